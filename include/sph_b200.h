@@ -1,0 +1,184 @@
+/*
+ * sph_b200.h -- C-ABI of libsph_b200, the B200 (sm_100a) weakly-compressible
+ * SPH time step of SPH-2D.
+ *
+ * The reference host (Fortran 90, one MPI rank per subdomain) calls
+ * argument-less subroutines that read and write module globals:
+ *   find_particle_pair()                          Taylor_Green_Vortex/find_particle_pair.f90:21-163
+ *   Define_freesurface_and_Normailized_derivates() Taylor_Green_Vortex/Define_freesurface_and_Normailized_derivates.f90:21-443
+ *   Solver_Normalized_*()                         Taylor_Green_Vortex/Solver_Normalized_Modified_Linear_Riemann_Delta_SPS.f90:23-639
+ *                                                 Taylor_Green_Vortex/Solver_Normalized_MUSCL_Linear_Riemann_Delta_SPS.f90
+ *   single_step_compute(i_time_step)              Taylor_Green_Vortex/single_step_compute.f90:19-301
+ *   time_iteration()  (Runge-Kutta branch)        Taylor_Green_Vortex/time_iteration.f90:781-1159
+ *   Shift_particle_position(i_time_step)          Taylor_Green_Vortex/Shift_particle_position.f90:21-137
+ *   Distribute_Period_Boundary_Particle(i)        Taylor_Green_Vortex/Distribute_Period_Boundary_Particle.f90:21-269
+ * Each entry point below replaces one of them (cited per function).  The
+ * Fortran shim passes its module arrays (column-major (n,2) = all x then all
+ * y), the particle counts and an sph_config filled from information_module.
+ *
+ * Conventions
+ *   - Every function returns int: 0 (SPH_OK) or a negative SPH_E_* code; the
+ *     library never aborts the process and never traps on the device.
+ *   - Host pointers are owned by the caller; the library copies from / to
+ *     them and never keeps them.
+ *   - Particle indices crossing the ABI are 1-based (Fortran) in pair lists.
+ *   - One handle per host thread; a handle is not thread-safe.
+ */
+#ifndef SPH_B200_H
+#define SPH_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define SPH_OK            0
+#define SPH_E_ARG        -1   /* null pointer, n <= 0, n > capacity, ...   */
+#define SPH_E_CAPACITY   -2   /* pair / particle / cell capacity exceeded   */
+#define SPH_E_NONFINITE  -3   /* NaN/Inf produced in the state               */
+#define SPH_E_CUDA       -5   /* a CUDA runtime call failed                  */
+#define SPH_E_TIMEOUT    -6   /* a bounded device wait gave up               */
+#define SPH_E_CONFIG     -7   /* unsupported configuration value             */
+#define SPH_E_DOMAIN     -8   /* a particle left the cell grid               */
+#define SPH_E_SKIN       -9   /* a particle moved further than the cell skin */
+#define SPH_E_NODEVICE  -10   /* no CUDA device / extension not usable       */
+
+/* ---- enumerations ------------------------------------------------------ */
+/* Kernel_function_model values of Moving_Square.../Compute_Kernel.f90:56-255 */
+#define SPH_KERNEL_GAUSSIAN   4   /* improved Gaussian, support 3h           */
+#define SPH_KERNEL_WENDLAND2  5   /* Wendland C2, support 2h                 */
+
+/* Solver_* variants (which `call Solver_...` line is live) */
+#define SPH_SOLVER_MODLR_DELTA_SPS  0 /* Solver_Normalized_Modified_Linear_Riemann_Delta_SPS (TGV default) */
+#define SPH_SOLVER_MUSCL_DELTA_SPS  1 /* Solver_Normalized_MUSCL_Linear_Riemann_Delta_SPS                 */
+
+#define SPH_EOS_TAIT    0   /* Status_Equation.f90:56-66  p = B((rho/rho0)^7-1) + pb */
+#define SPH_EOS_LINEAR  1   /* Status_Equation.f90:69-76  p = c0^2 (rho-rho0) + pb   */
+
+#define SPH_PAIRS_ONE_FLUID   0 /* TGV find_particle_pair.f90:76  keep if i or j is fluid     */
+#define SPH_PAIRS_NO_SAME_BND 1 /* MS  Find_particle_pair.f90:73-75 drop -2/-2, -3/-3, -201/-201 */
+
+#define SPH_PREC_FP64   0   /* every field and pair term in FP64                     */
+#define SPH_PREC_MIXED  1   /* FP32 pair arithmetic + compensated sums, FP64 state   */
+
+#define SPH_INTEGRATOR_RK4_REUSE 0 /* time_iteration.f90:781-1159 (3 RHS/step after step 1) */
+
+/* particle type labels (Information_Module.f90 of the moving-square case) */
+#define SPH_TYPE_WATER     2
+#define SPH_TYPE_PERIODIC  -101
+#define SPH_TYPE_ILL       120
+
+/* ---- configuration (filled once from information_module) ------------- */
+typedef struct sph_config {
+    int    kernel_model;      /* SPH_KERNEL_*                                        */
+    int    solver;            /* SPH_SOLVER_*                                        */
+    int    eos;               /* SPH_EOS_*                                           */
+    int    pair_rule;         /* SPH_PAIRS_*                                         */
+    int    precision;         /* SPH_PREC_*                                          */
+    int    renormalize;       /* 0: reference (inverse replaced by I), 1: true inverse */
+    int    reference_literals;/* 1: default-real literals of the reference (PI, 1e-7..) */
+    int    periodic;          /* 1: device-generated periodic images each step       */
+    int    shifting;          /* 1: Shift_particle_position after each step          */
+    int    integrator;        /* SPH_INTEGRATOR_*                                    */
+    double kernel_scale;      /* kernel_scale (support = kernel_scale * h)           */
+    double h;                 /* smooth_length (uniform)                             */
+    double dx;                /* interior_dx (SPS filter width, shift cap unit)      */
+    double rho0;              /* water_rho_0                                         */
+    double c0sq;              /* square_c_0                                          */
+    double background_p;      /* Background_Pressure                                 */
+    double nu;                /* water_kinematic_viscosity (Morris Laplacian)        */
+    double alpha, beta, fai;  /* Monaghan artificial viscosity alpha, beta, fai_coefficient */
+    double delta;             /* delta-SPH density diffusion coefficient             */
+    double delta_alpha;       /* Delta_alpha (artificial internal acceleration)      */
+    double xsph_eps;          /* epsilon (XSPH)                                      */
+    double shift_beta, shift_R, shift_max; /* shift_belta, shift_R, max_shift        */
+    int    shift_n;           /* shift_n                                             */
+    double fs_threshold;      /* volume fraction at or below which a particle is a surface candidate (0.65) */
+    double box_lo[2], box_hi[2];   /* periodic box (Period_Boundary_*_Min/Max)       */
+    double grid_lo[2], grid_hi[2]; /* extent every particle must stay inside         */
+    double cell_skin;         /* extra cell width as a fraction of the support (>= 0) */
+} sph_config;
+
+/* diagnostics returned by sph_step (reductions in FP64) */
+typedef struct sph_diag {
+    double kinetic_energy;    /* sum 0.5 m |v|^2 over water particles (Sampling_subroutine.f90:346-349) */
+    double max_speed;         /* max |v| over water particles                       */
+    long long pair_count;     /* pairs seen by the last RHS evaluation              */
+    int    n_images;          /* periodic images generated at the last step start   */
+    int    n_surface;         /* free-surface particles at the last RHS evaluation  */
+} sph_diag;
+
+/* per-pass device times (CUDA events) accumulated since the last reset, ms */
+typedef struct sph_timings {
+    double sort_ms, pass_a_ms, surface_ms, pass_c_ms, update_ms, images_ms, total_ms;
+    long long rhs_evaluations, steps;
+} sph_timings;
+
+typedef struct sph_handle sph_handle;
+
+/* Allocate device buffers for up to n_capacity host particles (plus their
+ * periodic images) and validate the configuration.  No reference counterpart:
+ * the reference sizes static module arrays at compile time
+ * (Taylor_Green_Vortex/information_module.f90:96-97, 286-302). */
+int sph_init(const sph_config* cfg, int n_capacity, sph_handle** out);
+int sph_free(sph_handle* h);
+
+/* Upload the host particle state.  Replaces the copy of the global arrays
+ * into the subdomain arrays (Taylor_Green_Vortex/Devide_block_and_send_tasks.f90:670-701).
+ * pos, vel: [2n] column-major; rho, mass: [n]; type: [n] labels;
+ * sps_mass: [n] or NULL -- the mass array the SPS force indexes with the
+ * neighbour's subdomain index (Solver_..._SPS.f90:489-490 reads the global
+ * particle_mass(j)); NULL means the particle's own mass. */
+int sph_set_state(sph_handle* h, int n, const double* pos, const double* vel,
+                  const double* rho, const double* mass, const int* type,
+                  const double* sps_mass);
+
+/* Download the host particles (same order as set_state).  press is the
+ * equation of state evaluated at the returned density.  Any pointer may be NULL. */
+int sph_get_state(sph_handle* h, int n, double* pos, double* vel, double* rho, double* press);
+
+/* find_particle_pair (Taylor_Green_Vortex/find_particle_pair.f90:21-163) on the
+ * current state.  Writes up to pair_cap pairs (1-based, i<j in host/image index
+ * order; images are numbered n+1.. in generation order), their kernel value
+ * w and gradient dwdx ([2*pair_cap] column-major, may be NULL).  *pair_number
+ * receives the total count; SPH_E_CAPACITY if it exceeds pair_cap. */
+int sph_find_particle_pair(sph_handle* h, int pair_cap, int* pair_i, int* pair_j,
+                           double* w, double* dwdx, long long* pair_number);
+
+/* One right-hand-side evaluation, i.e. the body of single_step_compute
+ * (Taylor_Green_Vortex/single_step_compute.f90:62-171): EOS, pair search,
+ * Define_freesurface_and_Normailized_derivates and the configured Solver_*,
+ * then assembly.  Outputs for the n host particles (any may be NULL):
+ * drhodt [n], acc [2n] (particle_acceleration), avg_vel [2n] (average_velocity),
+ * fs [n] free-surface flag, near [n] near-free-surface flag. */
+int sph_rhs(sph_handle* h, double* drhodt, double* acc, double* avg_vel, int* fs, int* near_fs);
+
+/* nsteps time steps of the configured integrator (time_iteration,
+ * Taylor_Green_Vortex/time_iteration.f90:781-1073): periodic wrap and images,
+ * the stage updates, shifting.  The state stays on the device.  out may be NULL. */
+int sph_step(sph_handle* h, int nsteps, double dt, sph_diag* out);
+
+/* Kinetic energy and max |v| of the water particles
+ * (Taylor_Green_Vortex/Sampling_subroutine.f90:340-356), FP64 reduction. */
+int sph_diagnostics(sph_handle* h, sph_diag* out);
+
+/* Intermediate per-particle fields of the last sph_rhs / RHS evaluation, for
+ * the n host particles, column-major blocks.  They are the module arrays the
+ * reference fills in Define_freesurface_and_Normailized_derivates and the
+ * solvers (Taylor_Green_Vortex/Public_variable_module.f90): */
+#define SPH_FIELD_FRA_V  0  /* [n]  subdomain_fra_v                                   */
+#define SPH_FIELD_BINV   1  /* [4n] Tensor_dyadic_inverse_matrix (11,12,21,22 blocks)  */
+#define SPH_FIELD_TAU    2  /* [3n] tao_xx, tao_xy, tao_yy                            */
+#define SPH_FIELD_GRADS  3  /* [8n] grad_rho x,y; grad_pressure x,y; grad u x,y; grad v x,y */
+int sph_get_field(sph_handle* h, int field, double* out);
+
+int sph_get_timings(sph_handle* h, sph_timings* out);
+int sph_reset_timings(sph_handle* h);
+
+/* Human-readable message for a status code (static storage). */
+const char* sph_strerror(int code);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPH_B200_H */

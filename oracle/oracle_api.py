@@ -1,0 +1,161 @@
+"""ctypes binding of the CPU oracle (oracle/liboracle.so).
+
+TEST INFRASTRUCTURE: imported only by tests/, __graft_entry__.smoke() and the
+CPU-baseline legs of bench.py, as the checker.  The product path never loads it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+sys.path.insert(0, os.path.join(os.path.dirname(HERE), "sph-2d_b200"))
+from sph_b200 import SphConfig  # noqa: E402  (struct layout only)
+
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB):
+        build()
+    lib = ctypes.CDLL(LIB)
+    dp = ctypes.POINTER(ctypes.c_double)
+    ip = ctypes.POINTER(ctypes.c_int)
+    cp = ctypes.POINTER(SphConfig)
+    lib.oracle_threads.argtypes = [ctypes.c_int]
+    lib.oracle_threads.restype = ctypes.c_int
+    lib.oracle_tgv_init.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                    ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int, dp, dp, dp, dp, dp]
+    lib.oracle_find_particle_pair.argtypes = [cp, ctypes.c_int, dp, ip, ctypes.c_longlong, ip, ip, dp, dp]
+    lib.oracle_find_particle_pair.restype = ctypes.c_longlong
+    lib.oracle_periodic_images.argtypes = [cp, ctypes.c_int, ctypes.c_int, dp, dp, dp, dp, ip, ip]
+    lib.oracle_rhs.argtypes = [cp, ctypes.c_int, dp, dp, dp, dp, ip, dp, dp, dp, dp, ip, ip, dp, dp, dp, dp]
+    lib.oracle_rhs.restype = ctypes.c_longlong
+    lib.oracle_create.argtypes = [cp, ctypes.c_int, dp, dp, dp, dp, ip, dp]
+    lib.oracle_create.restype = ctypes.c_void_p
+    lib.oracle_run.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double]
+    lib.oracle_get_state.argtypes = [ctypes.c_void_p, ctypes.c_int, dp, dp, dp, dp]
+    lib.oracle_kinetic_energy.argtypes = [ctypes.c_void_p]
+    lib.oracle_kinetic_energy.restype = ctypes.c_double
+    lib.oracle_last_pair_count.argtypes = [ctypes.c_void_p]
+    lib.oracle_last_pair_count.restype = ctypes.c_longlong
+    lib.oracle_last_images.argtypes = [ctypes.c_void_p]
+    lib.oracle_destroy.argtypes = [ctypes.c_void_p]
+    _lib = lib
+    return lib
+
+
+def _p(a, t=ctypes.c_double):
+    return None if a is None else a.ctypes.data_as(ctypes.POINTER(t))
+
+
+def threads(n: int = 0) -> int:
+    return load().oracle_threads(n)
+
+
+def tgv_init(nx, ny, U=1.0, rho0=1000.0, c0sq=100.0, sign=1, reference_literals=True):
+    n = nx * ny
+    pos = np.empty(2 * n); vel = np.empty(2 * n); rho = np.empty(n); mass = np.empty(n); press = np.empty(n)
+    load().oracle_tgv_init(nx, ny, 1.0, 1.0, U, rho0, c0sq, sign, int(reference_literals),
+                           _p(pos), _p(vel), _p(rho), _p(mass), _p(press))
+    return pos, vel, rho, mass, press
+
+
+def find_particle_pair(cfg: SphConfig, pos, type_, pair_cap=None):
+    n = type_.shape[0]
+    if pair_cap is None:
+        pair_cap = 80 * n + 16
+    pi = np.zeros(pair_cap, np.int32); pj = np.zeros(pair_cap, np.int32)
+    w = np.zeros(pair_cap); dw = np.zeros(2 * pair_cap)
+    pos = np.ascontiguousarray(pos, np.float64); type_ = np.ascontiguousarray(type_, np.int32)
+    m = load().oracle_find_particle_pair(ctypes.byref(cfg), n, _p(pos), _p(type_, ctypes.c_int), pair_cap,
+                                         _p(pi, ctypes.c_int), _p(pj, ctypes.c_int), _p(w), _p(dw))
+    if m > pair_cap:
+        raise RuntimeError("pair capacity exceeded")
+    return {"pair_i": pi[:m], "pair_j": pj[:m], "w": w[:m],
+            "dwdx": np.stack([dw[:m], dw[pair_cap:pair_cap + m]]), "pair_number": m}
+
+
+def periodic_images(cfg: SphConfig, pos, vel, rho, mass, type_, cap=None):
+    n = rho.shape[0]
+    if cap is None:
+        cap = 2 * n + 64
+    P = np.zeros(2 * cap); V = np.zeros(2 * cap); R = np.zeros(cap); M = np.zeros(cap)
+    T = np.zeros(cap, np.int32); S = np.full(cap, -1, np.int32)
+    P[:n] = pos[:n]; P[cap:cap + n] = pos[n:]; V[:n] = vel[:n]; V[cap:cap + n] = vel[n:]
+    R[:n] = rho; M[:n] = mass; T[:n] = type_
+    m = load().oracle_periodic_images(ctypes.byref(cfg), n, cap, _p(P), _p(V), _p(R), _p(M),
+                                      _p(T, ctypes.c_int), _p(S, ctypes.c_int))
+    if m < 0:
+        raise RuntimeError("image capacity exceeded")
+    pos2 = np.concatenate([P[:m], P[cap:cap + m]]); vel2 = np.concatenate([V[:m], V[cap:cap + m]])
+    return pos2, vel2, R[:m].copy(), M[:m].copy(), T[:m].copy(), S[:m].copy()
+
+
+def rhs(cfg: SphConfig, pos, vel, rho, mass, type_, sps_mass=None):
+    n = rho.shape[0]
+    out = {k: np.zeros(n) for k in ("drhodt", "fra_v")}
+    out["acc"] = np.zeros(2 * n); out["avg_vel"] = np.zeros(2 * n)
+    out["fs"] = np.zeros(n, np.int32); out["near"] = np.zeros(n, np.int32)
+    out["binv"] = np.zeros(4 * n); out["tau"] = np.zeros(3 * n); out["grads"] = np.zeros(8 * n)
+    a = [np.ascontiguousarray(x, np.float64) for x in (pos, vel, rho, mass)]
+    t = np.ascontiguousarray(type_, np.int32)
+    sm = None if sps_mass is None else np.ascontiguousarray(sps_mass, np.float64)
+    m = load().oracle_rhs(ctypes.byref(cfg), n, _p(a[0]), _p(a[1]), _p(a[2]), _p(a[3]), _p(t, ctypes.c_int), _p(sm),
+                          _p(out["drhodt"]), _p(out["acc"]), _p(out["avg_vel"]), _p(out["fs"], ctypes.c_int),
+                          _p(out["near"], ctypes.c_int), _p(out["fra_v"]), _p(out["binv"]), _p(out["tau"]),
+                          _p(out["grads"]))
+    out["pair_number"] = m
+    return out
+
+
+class OracleSim:
+    """The oracle's time_iteration on a copy of the given state."""
+
+    def __init__(self, cfg: SphConfig, pos, vel, rho, mass, type_, sps_mass=None):
+        self.lib = load()
+        self.cfg = cfg.copy()
+        self.n = rho.shape[0]
+        a = [np.ascontiguousarray(x, np.float64) for x in (pos, vel, rho, mass)]
+        t = np.ascontiguousarray(type_, np.int32)
+        sm = None if sps_mass is None else np.ascontiguousarray(sps_mass, np.float64)
+        self.h = self.lib.oracle_create(ctypes.byref(self.cfg), self.n, _p(a[0]), _p(a[1]), _p(a[2]), _p(a[3]),
+                                        _p(t, ctypes.c_int), _p(sm))
+
+    def run(self, nsteps: int, dt: float):
+        self.lib.oracle_run(self.h, int(nsteps), float(dt))
+
+    def state(self):
+        n = self.n
+        pos = np.empty(2 * n); vel = np.empty(2 * n); rho = np.empty(n); press = np.empty(n)
+        self.lib.oracle_get_state(self.h, n, _p(pos), _p(vel), _p(rho), _p(press))
+        return pos, vel, rho, press
+
+    def kinetic_energy(self) -> float:
+        return self.lib.oracle_kinetic_energy(self.h)
+
+    def last_pair_count(self) -> int:
+        return self.lib.oracle_last_pair_count(self.h)
+
+    def last_images(self) -> int:
+        return self.lib.oracle_last_images(self.h)
+
+    def __del__(self):
+        try:
+            if self.h:
+                self.lib.oracle_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass

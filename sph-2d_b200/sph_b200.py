@@ -1,0 +1,387 @@
+"""Python binding of libsph_b200 (ctypes over the C-ABI in include/sph_b200.h).
+
+This module is the host-side mirror of the reference's Fortran driver for the
+weakly-compressible SPH step of SPH-2D:
+
+  * ``SphConfig`` is the ``sph_config`` struct, filled the way the Fortran shim
+    fills it from ``information_module`` (Taylor_Green_Vortex/information_module.f90).
+  * ``Simulation.find_particle_pair`` / ``single_step_compute`` / ``time_iteration``
+    mirror ``find_particle_pair()`` (Taylor_Green_Vortex/find_particle_pair.f90:21),
+    ``single_step_compute()`` (Taylor_Green_Vortex/single_step_compute.f90:19) and the
+    Runge-Kutta branch of ``time_iteration()`` (Taylor_Green_Vortex/time_iteration.f90:781).
+
+The CUDA library is mandatory: ``load()`` raises if ``libsph_b200.so`` is not
+built or no CUDA device is usable; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsph_b200.so")
+
+# ---- constants mirrored from include/sph_b200.h ---------------------------
+SPH_OK = 0
+ERRORS = {
+    -1: "SPH_E_ARG", -2: "SPH_E_CAPACITY", -3: "SPH_E_NONFINITE", -5: "SPH_E_CUDA",
+    -6: "SPH_E_TIMEOUT", -7: "SPH_E_CONFIG", -8: "SPH_E_DOMAIN", -9: "SPH_E_SKIN",
+    -10: "SPH_E_NODEVICE",
+}
+KERNEL_GAUSSIAN = 4
+KERNEL_WENDLAND2 = 5
+SOLVER_MODLR_DELTA_SPS = 0
+SOLVER_MUSCL_DELTA_SPS = 1
+EOS_TAIT = 0
+EOS_LINEAR = 1
+PAIRS_ONE_FLUID = 0
+PAIRS_NO_SAME_BND = 1
+PREC_FP64 = 0
+PREC_MIXED = 1
+TYPE_WATER = 2
+TYPE_PERIODIC = -101
+TYPE_ILL = 120
+
+EXPORTED_SYMBOLS = (
+    "sph_init", "sph_free", "sph_set_state", "sph_get_state", "sph_find_particle_pair",
+    "sph_rhs", "sph_step", "sph_diagnostics", "sph_get_timings", "sph_reset_timings",
+    "sph_strerror", "sph_get_field",
+)
+
+
+class SphConfig(ctypes.Structure):
+    _fields_ = [
+        ("kernel_model", ctypes.c_int), ("solver", ctypes.c_int), ("eos", ctypes.c_int),
+        ("pair_rule", ctypes.c_int), ("precision", ctypes.c_int), ("renormalize", ctypes.c_int),
+        ("reference_literals", ctypes.c_int), ("periodic", ctypes.c_int), ("shifting", ctypes.c_int),
+        ("integrator", ctypes.c_int),
+        ("kernel_scale", ctypes.c_double), ("h", ctypes.c_double), ("dx", ctypes.c_double),
+        ("rho0", ctypes.c_double), ("c0sq", ctypes.c_double), ("background_p", ctypes.c_double),
+        ("nu", ctypes.c_double), ("alpha", ctypes.c_double), ("beta", ctypes.c_double),
+        ("fai", ctypes.c_double), ("delta", ctypes.c_double), ("delta_alpha", ctypes.c_double),
+        ("xsph_eps", ctypes.c_double), ("shift_beta", ctypes.c_double), ("shift_R", ctypes.c_double),
+        ("shift_max", ctypes.c_double), ("shift_n", ctypes.c_int), ("fs_threshold", ctypes.c_double),
+        ("box_lo", ctypes.c_double * 2), ("box_hi", ctypes.c_double * 2),
+        ("grid_lo", ctypes.c_double * 2), ("grid_hi", ctypes.c_double * 2),
+        ("cell_skin", ctypes.c_double),
+    ]
+
+    def copy(self) -> "SphConfig":
+        c = SphConfig()
+        ctypes.pointer(c)[0] = self
+        return c
+
+
+class SphDiag(ctypes.Structure):
+    _fields_ = [
+        ("kinetic_energy", ctypes.c_double), ("max_speed", ctypes.c_double),
+        ("pair_count", ctypes.c_longlong), ("n_images", ctypes.c_int), ("n_surface", ctypes.c_int),
+    ]
+
+
+class SphTimings(ctypes.Structure):
+    _fields_ = [
+        ("sort_ms", ctypes.c_double), ("pass_a_ms", ctypes.c_double), ("surface_ms", ctypes.c_double),
+        ("pass_c_ms", ctypes.c_double), ("update_ms", ctypes.c_double), ("images_ms", ctypes.c_double),
+        ("total_ms", ctypes.c_double), ("rhs_evaluations", ctypes.c_longlong), ("steps", ctypes.c_longlong),
+    ]
+
+
+# ---------------------------------------------------------------------------
+# Configurations (values of information_module and of the benchmark cases)
+# ---------------------------------------------------------------------------
+def tgv_reference_config(n_side: int = 100) -> SphConfig:
+    """The Taylor-Green case exactly as shipped in Taylor_Green_Vortex/information_module.f90:
+    improved Gaussian (kernel_scale 3, :132-134), h = 1.2 dx, rho0 = 1000 (:30),
+    c0^2 = 100 U (:142), nu = 1.0E-2 as a default real (:37), alpha 0, beta 2, fai 0.1,
+    delta 0.1, Delta_alpha 0.02 (:245-256), shifting on (:346-350), renormalisation
+    discarded, the default-real literals, periodic unit box."""
+    dx = 1.0 / n_side
+    c = SphConfig()
+    c.kernel_model = KERNEL_GAUSSIAN
+    c.solver = SOLVER_MODLR_DELTA_SPS
+    c.eos = EOS_TAIT
+    c.pair_rule = PAIRS_ONE_FLUID
+    c.precision = PREC_FP64
+    c.renormalize = 0
+    c.reference_literals = 1
+    c.periodic = 1
+    c.shifting = 1
+    c.integrator = 0
+    c.kernel_scale = 3.0
+    c.h = 1.20 * dx
+    c.dx = dx
+    c.rho0 = 1000.0
+    c.c0sq = 100.0
+    c.background_p = 0.0
+    c.nu = float(np.float32(1.0e-2))
+    c.alpha, c.beta, c.fai = 0.0, 2.0, 0.1
+    c.delta, c.delta_alpha = 0.1, 0.02
+    c.xsph_eps = 0.0
+    c.shift_beta, c.shift_R, c.shift_max, c.shift_n = 0.5, 0.2, 0.25 * dx, 4
+    c.fs_threshold = 0.65
+    c.box_lo[:] = [0.0, 0.0]
+    c.box_hi[:] = [1.0, 1.0]
+    pad = 0.05
+    c.grid_lo[:] = [-pad, -pad]
+    c.grid_hi[:] = [1.0 + pad, 1.0 + pad]
+    c.cell_skin = 0.1
+    return c
+
+
+def tgv_baseline_config(n_side: int, solver: int = SOLVER_MUSCL_DELTA_SPS,
+                        precision: int = PREC_FP64) -> SphConfig:
+    """The Taylor-Green benchmark case: periodic unit square, Wendland C2 (support 2h,
+    model 5 of Moving_Square.../Compute_Kernel.f90:172-198), h = 1.3 dx, rho0 = 1, U0 = 1,
+    c0 = 10 U0, Re = 100 (nu = 0.01), Tait gamma 7, true 2x2 renormalisation,
+    exact double constants."""
+    dx = 1.0 / n_side
+    c = tgv_reference_config(n_side)
+    c.kernel_model = KERNEL_WENDLAND2
+    c.solver = solver
+    c.precision = precision
+    c.renormalize = 1
+    c.reference_literals = 0
+    c.kernel_scale = 2.0
+    c.h = 1.3 * dx
+    c.rho0 = 1.0
+    c.c0sq = 100.0
+    c.nu = 0.01
+    c.shift_max = 0.25 * dx
+    c.cell_skin = 0.1
+    return c
+
+
+def baseline_dt(cfg: SphConfig) -> float:
+    """CFL time step dt = 0.25 h / c0 of the benchmark case."""
+    return 0.25 * cfg.h / math.sqrt(cfg.c0sq)
+
+
+def tgv_lattice(n_side: int, U: float = 1.0, rho0: float = 1.0, c0sq: float = 100.0,
+                sign: int = -1, reference_literals: bool = False):
+    """Taylor-Green lattice of Taylor_Green_Vortex/Distribute_Initial_Particle.f90:206-231,
+    vectorised.  sign=+1 is the reference's field (u = U sin cos, p = +rho0 U^2/4 ...),
+    sign=-1 the benchmark's (u = -U cos sin, p = -rho0 U^2/4 ...).  Returns
+    (pos[2n], vel[2n], rho[n], mass[n], press[n]) in Fortran column-major order."""
+    PI = 3.14159265358979324
+    dx = 1.0 / n_side
+    j = np.arange(1, n_side + 1, dtype=np.float64)
+    i = np.arange(1, n_side + 1, dtype=np.float64)
+    X = (j - 1) * dx + dx / 2.0
+    Y = (i - 1) * dx + dx / 2.0
+    x = np.tile(X, n_side)
+    y = np.repeat(Y, n_side)
+    if sign > 0:
+        u = U * np.sin(2 * PI * x) * np.cos(2 * PI * y)
+        v = -U * np.cos(2 * PI * x) * np.sin(2 * PI * y)
+        p = 0.25 * rho0 * (U * U) * (np.cos(4 * PI * x) + np.cos(4 * PI * y))
+    else:
+        u = -U * np.cos(2 * PI * x) * np.sin(2 * PI * y)
+        v = U * np.sin(2 * PI * x) * np.cos(2 * PI * y)
+        p = -0.25 * rho0 * (U * U) * (np.cos(4 * PI * x) + np.cos(4 * PI * y))
+    ex = float(np.float32(0.142857142)) if reference_literals else 1.0 / 7.0
+    rho = rho0 * np.power(1 + 7 * p / (c0sq * rho0), ex)
+    mass = dx * dx * rho
+    pos = np.concatenate([x, y])
+    vel = np.concatenate([u, v])
+    return pos, vel, rho, mass, p
+
+
+# ---------------------------------------------------------------------------
+# Library loading
+# ---------------------------------------------------------------------------
+_lib = None
+
+
+class SphError(RuntimeError):
+    def __init__(self, code: int, where: str):
+        self.code = code
+        msg = ERRORS.get(code, str(code))
+        try:
+            if _lib is not None:
+                msg = _lib.sph_strerror(code).decode()
+        except Exception:
+            pass
+        super().__init__(f"{where}: {msg} ({code})")
+
+
+def _dp():
+    return ctypes.POINTER(ctypes.c_double)
+
+
+def load(path: str = LIB_PATH):
+    """Load libsph_b200.so (raises if it is missing: the CUDA path is the only path)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"libsph_b200.so not built ({path}); run __graft_entry__.build()")
+    lib = ctypes.CDLL(path)
+    P = ctypes.c_void_p
+    dp = _dp()
+    ip = ctypes.POINTER(ctypes.c_int)
+    lib.sph_init.argtypes = [ctypes.POINTER(SphConfig), ctypes.c_int, ctypes.POINTER(P)]
+    lib.sph_free.argtypes = [P]
+    lib.sph_set_state.argtypes = [P, ctypes.c_int, dp, dp, dp, dp, ip, dp]
+    lib.sph_get_state.argtypes = [P, ctypes.c_int, dp, dp, dp, dp]
+    lib.sph_find_particle_pair.argtypes = [P, ctypes.c_longlong, ip, ip, dp, dp, ctypes.POINTER(ctypes.c_longlong)]
+    lib.sph_rhs.argtypes = [P, dp, dp, dp, ip, ip]
+    lib.sph_step.argtypes = [P, ctypes.c_int, ctypes.c_double, ctypes.POINTER(SphDiag)]
+    lib.sph_diagnostics.argtypes = [P, ctypes.POINTER(SphDiag)]
+    lib.sph_get_timings.argtypes = [P, ctypes.POINTER(SphTimings)]
+    lib.sph_reset_timings.argtypes = [P]
+    lib.sph_get_field.argtypes = [P, ctypes.c_int, dp]
+    lib.sph_strerror.argtypes = [ctypes.c_int]
+    lib.sph_strerror.restype = ctypes.c_char_p
+    for name in EXPORTED_SYMBOLS:
+        if name != "sph_strerror":
+            getattr(lib, name).restype = ctypes.c_int
+    _lib = lib
+    return lib
+
+
+def _ptr(a, ctype=ctypes.c_double):
+    if a is None:
+        return None
+    return a.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+def _check(code: int, where: str):
+    if code != SPH_OK:
+        raise SphError(code, where)
+
+
+# field ids of sph_get_field
+FIELD_FRA_V, FIELD_BINV, FIELD_TAU, FIELD_GRADS = 0, 1, 2, 3
+_FIELD_WIDTH = {FIELD_FRA_V: 1, FIELD_BINV: 4, FIELD_TAU: 3, FIELD_GRADS: 8}
+
+
+class Simulation:
+    """One libsph_b200 handle: the device-resident state of the Fortran
+    subdomain arrays plus the configuration."""
+
+    def __init__(self, cfg: SphConfig, capacity: int):
+        self.lib = load()
+        self.cfg = cfg.copy()
+        self.capacity = int(capacity)
+        h = ctypes.c_void_p()
+        _check(self.lib.sph_init(ctypes.byref(self.cfg), self.capacity, ctypes.byref(h)), "sph_init")
+        self.h = h
+        self.n = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.sph_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # --- state --------------------------------------------------------------
+    def set_state(self, pos, vel, rho, mass, type_, sps_mass=None):
+        n = rho.shape[0]
+        pos = np.ascontiguousarray(pos, dtype=np.float64)
+        vel = np.ascontiguousarray(vel, dtype=np.float64)
+        rho = np.ascontiguousarray(rho, dtype=np.float64)
+        mass = np.ascontiguousarray(mass, dtype=np.float64)
+        type_ = np.ascontiguousarray(type_, dtype=np.int32)
+        sm = None if sps_mass is None else np.ascontiguousarray(sps_mass, dtype=np.float64)
+        _check(self.lib.sph_set_state(self.h, n, _ptr(pos), _ptr(vel), _ptr(rho), _ptr(mass),
+                                      _ptr(type_, ctypes.c_int), _ptr(sm)), "sph_set_state")
+        self.n = n
+
+    def get_state(self):
+        n = self.n
+        pos = np.empty(2 * n); vel = np.empty(2 * n); rho = np.empty(n); press = np.empty(n)
+        _check(self.lib.sph_get_state(self.h, n, _ptr(pos), _ptr(vel), _ptr(rho), _ptr(press)), "sph_get_state")
+        return pos, vel, rho, press
+
+    # --- reference-named entry points ----------------------------------------
+    def find_particle_pair(self, pair_cap: int, want_kernel: bool = True):
+        pi = np.zeros(pair_cap, np.int32); pj = np.zeros(pair_cap, np.int32)
+        w = np.zeros(pair_cap) if want_kernel else None
+        dw = np.zeros(2 * pair_cap) if want_kernel else None
+        cnt = ctypes.c_longlong(0)
+        code = self.lib.sph_find_particle_pair(self.h, pair_cap, _ptr(pi, ctypes.c_int), _ptr(pj, ctypes.c_int),
+                                               _ptr(w), _ptr(dw), ctypes.byref(cnt))
+        _check(code, "sph_find_particle_pair")
+        m = cnt.value
+        out = {"pair_i": pi[:m], "pair_j": pj[:m], "pair_number": m}
+        if want_kernel:
+            out["w"] = w[:m]
+            out["dwdx"] = np.stack([dw[:m], dw[pair_cap:pair_cap + m]])
+        return out
+
+    def single_step_compute(self):
+        n = self.n
+        drho = np.empty(n); acc = np.empty(2 * n); avg = np.empty(2 * n)
+        fs = np.empty(n, np.int32); near = np.empty(n, np.int32)
+        _check(self.lib.sph_rhs(self.h, _ptr(drho), _ptr(acc), _ptr(avg), _ptr(fs, ctypes.c_int),
+                                _ptr(near, ctypes.c_int)), "sph_rhs")
+        return {"drhodt": drho, "acc": acc, "avg_vel": avg, "fs": fs, "near": near}
+
+    def field(self, fid: int):
+        out = np.empty(_FIELD_WIDTH[fid] * self.n)
+        _check(self.lib.sph_get_field(self.h, fid, _ptr(out)), "sph_get_field")
+        return out
+
+    def time_iteration(self, nsteps: int, dt: float) -> SphDiag:
+        d = SphDiag()
+        _check(self.lib.sph_step(self.h, int(nsteps), float(dt), ctypes.byref(d)), "sph_step")
+        return d
+
+    def diagnostics(self) -> SphDiag:
+        d = SphDiag()
+        _check(self.lib.sph_diagnostics(self.h, ctypes.byref(d)), "sph_diagnostics")
+        return d
+
+    def timings(self) -> SphTimings:
+        t = SphTimings()
+        _check(self.lib.sph_get_timings(self.h, ctypes.byref(t)), "sph_get_timings")
+        return t
+
+    def reset_timings(self):
+        _check(self.lib.sph_reset_timings(self.h), "sph_reset_timings")
+
+
+@dataclass
+class TgvCase:
+    """A Taylor-Green initial state ready for Simulation.set_state."""
+    cfg: SphConfig
+    pos: np.ndarray
+    vel: np.ndarray
+    rho: np.ndarray
+    mass: np.ndarray
+    type: np.ndarray
+
+    @property
+    def n(self) -> int:
+        return self.rho.shape[0]
+
+
+def make_tgv(n_side: int, reference: bool = False, solver: int = SOLVER_MUSCL_DELTA_SPS,
+             precision: int = PREC_FP64, jitter: float = 0.0, seed: int = 0) -> TgvCase:
+    if reference:
+        cfg = tgv_reference_config(n_side)
+        pos, vel, rho, mass, _ = tgv_lattice(n_side, rho0=1000.0, c0sq=100.0, sign=+1, reference_literals=True)
+    else:
+        cfg = tgv_baseline_config(n_side, solver, precision)
+        pos, vel, rho, mass, _ = tgv_lattice(n_side, rho0=1.0, c0sq=100.0, sign=-1)
+    if jitter > 0.0:
+        rng = np.random.default_rng(seed)
+        pos = pos + rng.uniform(-jitter, jitter, pos.shape) * cfg.dx
+    typ = np.full(rho.shape[0], TYPE_WATER, np.int32)
+    return TgvCase(cfg, pos, vel, rho, mass, typ)
