@@ -142,7 +142,7 @@ int sph_get_state(sph_handle* h, int n, double* pos, double* vel, double* rho, d
  * order; images are numbered n+1.. in generation order), their kernel value
  * w and gradient dwdx ([2*pair_cap] column-major, may be NULL).  *pair_number
  * receives the total count; SPH_E_CAPACITY if it exceeds pair_cap. */
-int sph_find_particle_pair(sph_handle* h, int pair_cap, int* pair_i, int* pair_j,
+int sph_find_particle_pair(sph_handle* h, long long pair_cap, int* pair_i, int* pair_j,
                            double* w, double* dwdx, long long* pair_number);
 
 /* One right-hand-side evaluation, i.e. the body of single_step_compute

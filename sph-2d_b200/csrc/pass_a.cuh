@@ -1,0 +1,178 @@
+// pass_a.cuh -- neighbour pass A (one thread per particle, gather form):
+// volume fraction, renormalisation tensor and its inverse, normalised
+// gradients of rho / p / u / v, SPS strain and stress.
+//
+// Reference: Define_freesurface_and_Normailized_derivates.f90:79-188 (fra_v,
+// Tensor_dyadic_matrix, inverse), Solver_Normalized_Modified_Linear_Riemann_Delta_SPS.f90:
+// 126-139 (normalised dW), :144-182 and :256-296 (SPS), :508-526 (grad rho),
+// Solver_Normalized_MUSCL_Linear_Riemann_Delta_SPS.f90:151-185 (grad p, u, v).
+//
+// Gather form of the reference's pair scatter: for particle a and pair
+// neighbour b, grad_a W_ab = f(d) (x_a - x_b) is the reference's dwdx(k) when a
+// is pair_i and -dwdx(k) when a is pair_j, so every scatter term becomes
+// "sum over b of (phi_b - phi_a) V_b B_a^-1 grad_a W_ab".  Since B_a^-1 is the
+// same matrix for all b, the raw sums are accumulated first and multiplied by
+// B_a^-1 once (exact in real arithmetic).
+#pragma once
+#include "setup.cuh"
+
+namespace sph {
+
+template <typename R>
+__global__ void __launch_bounds__(128) k_pass_a(Params P, Sorted<R> D) {
+    using V4 = typename VT<R>::V4;
+    using A = typename Acc<R>::T;
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= P.n_tot) return;
+    const int ta = D.type[a];
+    const int nn = D.nnbr[a];
+    const double2 xa = D.pos[a];
+    const V4 ka = D.kin[a];
+    const R rho_a = Dens<R>::rho(ka.z, P.rho0);
+    A fra, b00, b01, b10, b11, g[8];
+    fra.init(); b00.init(); b01.init(); b10.init(); b11.init();
+    for (int c = 0; c < 8; ++c) g[c].init();
+    const R inv_sv = (R)(1.0 / P.sv);
+    for (int e = 0; e < nn; ++e) {
+        const unsigned ent = __ldg(&D.nbr[(size_t)e * P.nbr_stride + a]);
+        const int b = (int)(ent & 0x7fffffffu);
+        const double2 xb = __ldg(&D.pos[b]);
+        const double dxd = xa.x - xb.x, dyd = xa.y - xb.y;
+        double dd;
+        if (!in_support(P, dxd, dyd, dd)) continue;
+        const R d = (R)dd, dx = (R)dxd, dy = (R)dyd;
+        R w, gx, gy;
+        kernel_w_dw<R>(P, d, dx, dy, w, gx, gy);
+        const V4 kb = D.kin[b];
+        const R Vb = D.aux[b].y;
+        // volume fraction (:84-85)
+        if (sizeof(R) == 8) fra.add(Vb / (R)P.sv); else fra.add(Vb * inv_sv);
+        // B(l,o) += (x_b - x_a)_l grad_a W_o V_b (:151-152)
+        b00.add(-dx * gx * Vb); b01.add(-dx * gy * Vb);
+        b10.add(-dy * gx * Vb); b11.add(-dy * gy * Vb);
+        // raw gradient sums (phi_b - phi_a) V_b grad_a W
+        const R drho = Dens<R>::rho(kb.z, P.rho0) - rho_a;
+        const R drho_m = sizeof(R) == 8 ? drho : (kb.z - ka.z);
+        const R t0 = drho_m * Vb;
+        g[0].add(t0 * gx); g[1].add(t0 * gy);
+        const R tu = (kb.x - ka.x) * Vb, tv = (kb.y - ka.y) * Vb;
+        g[4].add(tu * gx); g[5].add(tu * gy);
+        g[6].add(tv * gx); g[7].add(tv * gy);
+        if (P.muscl) {
+            const R tp = (kb.w - ka.w) * Vb;
+            g[2].add(tp * gx); g[3].add(tp * gy);
+        }
+    }
+    // inverse of the 2x2 tensor in FP64 (matrix_inversion_less_three,
+    // function_module.f90:190-204); the reference keeps the identity on success
+    // (Define_freesurface...f90:180-186) unless renormalisation is switched on.
+    double i00 = 1.0, i01 = 0.0, i10 = 0.0, i11 = 1.0;
+    if (ta == SPH_TYPE_WATER && P.renorm) {
+        double a1 = (double)b00.val(), bb1 = (double)b01.val(), a2 = (double)b10.val(), bb2 = (double)b11.val();
+        double det = (a1 * bb2 - bb1 * a2);
+        if (det != 0) { i00 = bb2 / det; i01 = -bb1 / det; i10 = -a2 / det; i11 = a1 / det; }
+    }
+    const R m00 = (R)i00, m01 = (R)i01, m10 = (R)i10, m11 = (R)i11;
+    D.binv[a] = mk4<R>(m00, m01, m10, m11);
+    R gr[8];
+    for (int f = 0; f < 4; ++f) {
+        R x = g[2 * f].val(), y = g[2 * f + 1].val();
+        gr[2 * f] = m00 * x + m01 * y;
+        gr[2 * f + 1] = m10 * x + m11 * y;
+    }
+    // SPS stress for water particles (:256-296)
+    R txx = R(0), txy = R(0), tyy = R(0);
+    if (ta == SPH_TYPE_WATER) {
+        const double sxx = (double)gr[4], sxy = (double)gr[5] + (double)gr[6], syy = (double)gr[7];
+        const double abs2 = 2 * (sxx * sxx + syy * syy) + sxy * sxy;
+        const double DL = P.sps_dl;               // SPS_Delta_L = sqrt(2.0)/2.0*interior_dx (host-side product)
+        const double t = P.sps_c012 * DL;
+        const double nut = (t * t) * sqrt(abs2);
+        const double kk = P.sps_23 * nut * (sxx + syy);
+        const double blin = P.sps_blin * (DL * DL) * abs2;
+        const double rho = (double)rho_a;
+        txx = (R)((2 * nut * sxx - kk - blin) * rho);
+        txy = (R)((nut * sxy) * rho);
+        tyy = (R)((2 * nut * syy - kk - blin) * rho);
+    }
+    D.nb1[a] = mk4<R>(txx, txy, tyy, gr[0]);
+    D.nb2[a] = mk4<R>(gr[1], gr[2], gr[3], gr[4]);
+    D.nb3[a] = mk4<R>(gr[5], gr[6], gr[7], R(0));
+    const R fv = fra.val();
+    D.fra_v[a] = fv;
+    uint8_t fl = 0;
+    if (ta == SPH_TYPE_WATER && (double)fv <= P.fs_thr) fl = 4;   // surface candidate (:123)
+    D.flags[a] = fl;
+}
+
+// Geometric free-surface test of the candidates (Define_freesurface...f90:295-376):
+// normal n = -B^-1 sum(grad W V)/|.|; the candidate is interior as soon as one
+// water neighbour j satisfies  |x_j-x_i| >= 1.414h and |x_j - (x_i + h n)| < h,
+// or |x_j-x_i| < 1.414h and acos(n.(x_j-x_i)/|x_j-x_i|) <= pi/4.
+// Both criteria only accept j within 2h <= support, so the list covers them.
+template <typename R>
+__global__ void k_surface(Params P, Sorted<R> D) {
+    using V4 = typename VT<R>::V4;
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= P.n_tot) return;
+    uint8_t fl = D.flags[a];
+    if (!(fl & 4)) return;
+    const int nn = D.nnbr[a];
+    const double2 xa = D.pos[a];
+    // sum_dwdx (:155-156) recomputed here (candidates are rare)
+    double s0 = 0.0, s1 = 0.0;
+    for (int e = 0; e < nn; ++e) {
+        const int b = (int)(D.nbr[(size_t)e * P.nbr_stride + a] & 0x7fffffffu);
+        const double2 xb = D.pos[b];
+        double dx = xa.x - xb.x, dy = xa.y - xb.y, d;
+        if (!in_support(P, dx, dy, d)) continue;
+        double w, gx, gy;
+        kernel_w_dw<double>(P, d, dx, dy, w, gx, gy);
+        const double Vb = (double)D.aux[b].y;
+        s0 += gx * Vb; s1 += gy * Vb;
+    }
+    const V4 bi = D.binv[a];
+    double n0 = (double)bi.x * s0 + (double)bi.y * s1;
+    double n1 = (double)bi.z * s0 + (double)bi.w * s1;
+    double len = sqrt(n0 * n0 + n1 * n1);
+    bool surface = true;
+    if (isnan(len) || len == 0.0) surface = false;
+    else {
+        n0 = -n0 / len; n1 = -n1 / len;
+        const double h = P.h;
+        const double vx = xa.x + h * n0, vy = xa.y + h * n1;
+        for (int e = 0; e < nn && surface; ++e) {
+            const int b = (int)(D.nbr[(size_t)e * P.nbr_stride + a] & 0x7fffffffu);
+            if (D.type[b] != SPH_TYPE_WATER) continue;
+            const double2 xb = D.pos[b];
+            double p0 = xb.x - xa.x, p1 = xb.y - xa.y;
+            double ji = sqrt(p0 * p0 + p1 * p1);
+            double nd = n0 * p0 + n1 * p1;
+            double q0 = xb.x - vx, q1 = xb.y - vy;
+            double jt = sqrt(q0 * q0 + q1 * q1);
+            if (ji >= P.c1414 * h && jt < h) surface = false;
+            else if (ji < P.c1414 * h && acos(nd / ji) <= (P.pi / 4.0)) surface = false;
+        }
+    }
+    D.flags[a] = surface ? (uint8_t)(fl | 1) : (uint8_t)(fl & ~1);
+}
+
+// Near-free-surface flags (Define_freesurface...f90:418-440): every pair
+// neighbour of a surface particle.  Idempotent byte stores, no atomics needed.
+template <typename R>
+__global__ void k_near(Params P, Sorted<R> D) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= P.n_tot) return;
+    if (!(D.flags[a] & 1)) return;
+    const int nn = D.nnbr[a];
+    const double2 xa = D.pos[a];
+    for (int e = 0; e < nn; ++e) {
+        const int b = (int)(D.nbr[(size_t)e * P.nbr_stride + a] & 0x7fffffffu);
+        const double2 xb = D.pos[b];
+        double dx = xa.x - xb.x, dy = xa.y - xb.y, d;
+        if (!in_support(P, dx, dy, d)) continue;
+        D.flags[b] |= 2;
+    }
+}
+
+}  // namespace sph

@@ -1,0 +1,258 @@
+// setup.cuh -- per-step set-up kernels: periodic wrap and images, the
+// background-cell sort, cell ranges and the per-particle neighbour lists.
+#pragma once
+#include "common.cuh"
+
+namespace sph {
+
+// Particle arrays in id order ("staging"): the host particles 0..n_host-1
+// followed by the periodic images of this step, numbered as the reference
+// appends them (Distribute_Period_Boundary_Particle.f90:95-206).
+struct Staging {
+    double2* pos;     // x, y
+    double2* vel;     // u, v
+    double* rho;
+    double* mass;
+    double* smass;    // mass the SPS force multiplies with (quirk A.6), default = mass
+    int* type;
+    // rates of the last RHS of the previous step (the reused K1), host particles only
+    double* r_drho;
+    double2* r_acc;
+    double2* r_avg;
+    int* cnt;         // image counts / scan scratch
+    int* off;
+};
+
+// --- 1. periodic wrap (Distribute_Period_Boundary_Particle.f90:56-90) -------
+__global__ void k_wrap(Params P, Staging S) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.n_host || S.type[i] == SPH_TYPE_ILL) return;
+    double2 x = S.pos[i];
+    double Lx = P.box_hi[0] - P.box_lo[0], Ly = P.box_hi[1] - P.box_lo[1];
+    if (x.x > P.box_hi[0]) x.x = x.x - Lx;
+    else if (x.x < P.box_lo[0]) x.x = x.x + Lx;
+    if (x.y > P.box_hi[1]) x.y = x.y - Ly;
+    else if (x.y < P.box_lo[1]) x.y = x.y + Ly;
+    S.pos[i] = x;
+}
+
+// --- 2. images: count per source, then emit at scanned offsets -------------
+// axis 0: left/right images of the host particles (:98-148),
+// axis 1: bottom/top images of host particles and left/right images (:156-206).
+__global__ void k_img_count(Params P, Staging S, int n_src, int axis) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_src) return;
+    int c = 0;
+    if (S.type[i] != SPH_TYPE_ILL) {
+        double x = axis == 0 ? S.pos[i].x : S.pos[i].y;
+        double lo = P.box_lo[axis], hi = P.box_hi[axis];
+        if (x <= (lo + P.band) && x >= lo) c++;
+        if (x >= (hi - P.band) && x <= hi) c++;
+    }
+    S.cnt[i] = c;
+}
+
+__global__ void k_img_emit(Params P, Staging S, int n_src, int axis, int base, const int* off) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_src || S.type[i] == SPH_TYPE_ILL) return;
+    double2 x = S.pos[i];
+    double v = axis == 0 ? x.x : x.y;
+    double lo = P.box_lo[axis], hi = P.box_hi[axis], L = hi - lo;
+    int o = base + off[i];
+    for (int side = 0; side < 2; ++side) {
+        bool in = side == 0 ? (v <= (lo + P.band) && v >= lo) : (v >= (hi - P.band) && v <= hi);
+        if (!in) continue;
+        double2 y = x;
+        double sh = side == 0 ? L : -L;
+        if (axis == 0) y.x = x.x + sh; else y.y = x.y + sh;
+        S.pos[o] = y;
+        S.vel[o] = S.vel[i];
+        S.rho[o] = S.rho[i];
+        S.mass[o] = S.mass[i];
+        S.smass[o] = S.smass[i];
+        S.type[o] = SPH_TYPE_PERIODIC;
+        ++o;
+    }
+}
+
+// --- 3. cell keys (row-major cells of edge >= list radius) -----------------
+__global__ void k_cell_keys(Params P, const double2* pos, const int* type, unsigned* keys, unsigned* vals,
+                            unsigned* status, unsigned dead_key) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.n_tot) return;
+    vals[i] = (unsigned)i;
+    int t = type[i];
+    if (t == SPH_TYPE_ILL || t == 0) { keys[i] = dead_key; return; }   // not binned (Assign_boundary_particles.f90:82)
+    double2 x = pos[i];
+    double fx = floor((x.x - P.gx0) / P.cs), fy = floor((x.y - P.gy0) / P.cs);
+    int cx = (int)fx, cy = (int)fy;
+    if (!(fx >= 0.0 && fy >= 0.0 && cx < P.gnx && cy < P.gny)) {
+        atomicOr(status, ST_DOMAIN);
+        keys[i] = dead_key;
+        return;
+    }
+    keys[i] = (unsigned)(cy * P.gnx + cx);
+}
+
+// Device-side arrays in cell-sorted order (templated on the pair precision).
+template <typename R>
+struct Sorted {
+    using V2 = typename VT<R>::V2;
+    using V4 = typename VT<R>::V4;
+    int* id;          // id-order index (host index, or n_host + image number)
+    int* type;
+    double2* pos;     // current stage position (FP64)
+    double2* pos0;    // step-start (master) position, also the list-build position
+    double2* vel0;    // step-start velocity (FP64 master)
+    double* rho0;     // step-start density (FP64 master)
+    double* mass;
+    double* smass;
+    V4* kin;          // u, v, rho (FP64) or rho-rho0 (mixed), p     -- neighbour record 1
+    V4* aux;          // m, V = m/rho, c, smass                      -- neighbour record 2
+    V4* nb1;          // tau_xx, tau_xy, tau_yy, grad rho x          -- neighbour record 3
+    V4* nb2;          // grad rho y, grad p x, grad p y, grad u x     -- neighbour record 4
+    V4* nb3;          // grad u y, grad v x, grad v y, 0             -- neighbour record 5 (MUSCL)
+    V4* binv;         // B^-1 (11, 12, 21, 22)
+    R* fra_v;
+    uint8_t* flags;   // bit0 surface, bit1 near surface, bit2 surface candidate
+    // rates of the current RHS
+    R* drho;
+    V2* acc;
+    V2* avg;
+    V2* shift;        // shifting displacement sums (last RHS of a step)
+    // Runge-Kutta sums K1 + 2 K2 + 2 K3 (time_iteration.f90:1040-1045)
+    R* ks_r;
+    V2* ks_a;
+    V2* ks_v;
+    // rates carried to the next step (K1 reuse)
+    R* c_drho;
+    V2* c_acc;
+    V2* c_avg;
+    // neighbour lists: slot-major [max_nbr][stride], bit 31 = "this particle has the lower id"
+    unsigned* nbr;
+    int* nnbr;
+    // cell ranges
+    int* cell_start;
+    int* cell_end;
+};
+
+// --- 4. gather the id-ordered arrays into cell order -----------------------
+template <typename R>
+__global__ void k_gather_sorted(Params P, Staging S, Sorted<R> D, const unsigned* perm) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= P.n_tot) return;
+    int i = (int)perm[s];
+    D.id[s] = i;
+    D.type[s] = S.type[i];
+    double2 x = S.pos[i];
+    D.pos[s] = x;
+    D.pos0[s] = x;
+    D.vel0[s] = S.vel[i];
+    D.rho0[s] = S.rho[i];
+    D.mass[s] = S.mass[i];
+    D.smass[s] = S.smass[i];
+    if (i < P.n_host) {
+        D.c_drho[s] = (R)S.r_drho[i];
+        D.c_acc[s] = mk2<R>((R)S.r_acc[i].x, (R)S.r_acc[i].y);
+        D.c_avg[s] = mk2<R>((R)S.r_avg[i].x, (R)S.r_avg[i].y);
+    } else {
+        D.c_drho[s] = R(0);
+        D.c_acc[s] = mk2<R>(R(0), R(0));
+        D.c_avg[s] = mk2<R>(R(0), R(0));
+    }
+}
+
+// sorted master state -> id order (host particles only; images are dropped)
+template <typename R>
+__global__ void k_unsort(Params P, Staging S, Sorted<R> D) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= P.n_tot) return;
+    int i = D.id[s];
+    if (i >= P.n_host) return;
+    S.pos[i] = D.pos0[s];
+    S.vel[i] = D.vel0[s];
+    S.rho[i] = D.rho0[s];
+    S.mass[i] = D.mass[s];
+    S.smass[i] = D.smass[s];
+    S.type[i] = D.type[s];
+    S.r_drho[i] = (double)D.c_drho[s];
+    S.r_acc[i] = make_double2((double)D.c_acc[s].x, (double)D.c_acc[s].y);
+    S.r_avg[i] = make_double2((double)D.c_avg[s].x, (double)D.c_avg[s].y);
+}
+
+// --- 5. cell ranges from the sorted keys ----------------------------------
+__global__ void k_cell_ranges(int n, const unsigned* keys, int* start, int* end, unsigned dead_key) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    unsigned k = keys[s];
+    if (k == dead_key) return;
+    if (s == 0 || keys[s - 1] != k) start[k] = s;
+    if (s == n - 1 || keys[s + 1] != k) end[k] = s + 1;
+}
+
+// Pair-rule of find_particle_pair (TGV :76, MS :73-75).
+__device__ __forceinline__ bool pair_allowed(int rule, int ti, int tj) {
+    if (rule == SPH_PAIRS_ONE_FLUID) return ti == SPH_TYPE_WATER || tj == SPH_TYPE_WATER;
+    if (ti == -2 && tj == -2) return false;
+    if (ti == -3 && tj == -3) return false;
+    if (ti == -201 && tj == -201) return false;
+    return true;
+}
+
+// --- 6. neighbour lists ----------------------------------------------------
+// Every particle b != a in the 3x3 cells with |x_a - x_b|^2 <= (support*(1+skin))^2
+// and an allowed type pair.  The exact support test is repeated at every RHS on
+// the current positions, so the list only has to be a superset of the pairs of
+// the whole step; k_stage checks the displacement bound that guarantees it.
+template <typename R>
+__global__ void k_build_lists(Params P, Sorted<R> D, unsigned* status) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= P.n_tot) return;
+    int ta = D.type[a];
+    int cnt = 0;
+    if (ta != SPH_TYPE_ILL && ta != 0) {
+        double2 xa = D.pos[a];
+        int ida = D.id[a];
+        int cx = (int)floor((xa.x - P.gx0) / P.cs), cy = (int)floor((xa.y - P.gy0) / P.cs);
+        int x0 = max(cx - 1, 0), x1 = min(cx + 1, P.gnx - 1);
+        for (int gy = max(cy - 1, 0); gy <= min(cy + 1, P.gny - 1); ++gy) {
+            int row = gy * P.gnx;
+            for (int gx = x0; gx <= x1; ++gx) {
+                int c = row + gx;
+                int b0 = D.cell_start[c];
+                if (b0 < 0) continue;
+                int b1 = D.cell_end[c];
+                for (int b = b0; b < b1; ++b) {
+                    if (b == a) continue;
+                    if (!pair_allowed(P.pair_rule, ta, D.type[b])) continue;
+                    double2 xb = D.pos[b];
+                    double dx = xa.x - xb.x, dy = xa.y - xb.y;
+                    if (dx * dx + dy * dy > P.r2_list) continue;
+                    if (cnt < P.max_nbr) {
+                        unsigned lower = ida < D.id[b] ? 0x80000000u : 0u;
+                        D.nbr[(size_t)cnt * P.nbr_stride + a] = (unsigned)b | lower;
+                    }
+                    ++cnt;
+                }
+            }
+        }
+        if (cnt > P.max_nbr) { atomicOr(status, ST_NBR_OVERFLOW); cnt = P.max_nbr; }
+    }
+    D.nnbr[a] = cnt;
+}
+
+// --- 7. neighbour records of the step-start state (all particles) ---------
+template <typename R>
+__global__ void k_records(Params P, Sorted<R> D) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= P.n_tot) return;
+    double rho = D.rho0[s];
+    double p, c;
+    eos64(P, rho, p, c);
+    double2 v = D.vel0[s];
+    double m = D.mass[s];
+    D.kin[s] = mk4<R>((R)v.x, (R)v.y, Dens<R>::store(rho, P.rho0), (R)p);
+    D.aux[s] = mk4<R>((R)m, (R)(m / rho), (R)c, (R)D.smass[s]);
+}
+
+}  // namespace sph

@@ -1,0 +1,740 @@
+// sph_b200.cu -- libsph_b200: host orchestration and the C-ABI of
+// include/sph_b200.h.  Build: see sph-2d_b200/build.py (nvcc, sm_100a).
+//
+// One handle = the device-resident particle state of one Fortran subdomain
+// (now the whole domain: the MPI decomposition of Devide_block_and_send_tasks
+// and the halo exchanges of exchange_buffer_domain_information are gone).
+//
+// Per time step (time_iteration.f90:781-1073):
+//   prepare: periodic wrap + images (id order), cell keys, radix sort,
+//            cell ranges, neighbour lists with a skin, neighbour records
+//   RHS    : pass A (renormalisation, gradients, SPS) -> surface test ->
+//            near-surface flags -> pass C (fused forces)
+//   stages : k_stage 0..3, shifting fused into the last stage
+#include <cuda_runtime.h>
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "update.cuh"
+
+using namespace sph;
+
+namespace {
+
+const char* kMessages[] = {
+    "ok", "invalid argument", "capacity exceeded", "non-finite value in the state", "(unused)",
+    "CUDA runtime error", "device wait timed out", "unsupported configuration",
+    "a particle left the cell grid", "a particle moved further than the neighbour-list skin",
+    "no usable CUDA device",
+};
+
+#define CK(call)                                                                 \
+    do {                                                                         \
+        cudaError_t e_ = (call);                                                 \
+        if (e_ != cudaSuccess) {                                                 \
+            fprintf(stderr, "libsph_b200: %s failed: %s (%s:%d)\n", #call,     \
+                    cudaGetErrorString(e_), __FILE__, __LINE__);                 \
+            return SPH_E_CUDA;                                                   \
+        }                                                                        \
+    } while (0)
+
+inline int blocks(long long n, int t) { return (int)((n + t - 1) / t); }
+
+enum Phase { PH_SORT, PH_A, PH_SURF, PH_C, PH_UPDATE, PH_IMAGES, PH_COUNT };
+
+template <typename T>
+cudaError_t dalloc(T** p, size_t count) {
+    return cudaMalloc((void**)p, std::max<size_t>(count, 1) * sizeof(T));
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+struct sph_handle {
+    sph_config cfg;
+    Params P;
+    int device = 0;
+    int cap_host = 0, cap_img = 0, cap_tot = 0;
+    int n_host = 0, n_img = 0;
+    bool staging_valid = false;
+    bool sorted_valid = false;
+    bool have_rhs = false;
+    long long step_count = 0;
+    long long last_pairs = 0;
+    cudaStream_t stream = nullptr;
+    Staging S{};
+    Sorted<double> D64{};
+    Sorted<float> D32{};
+    bool mixed = false;
+    // sort
+    unsigned *keys_in = nullptr, *keys_out = nullptr, *vals_in = nullptr, *vals_out = nullptr;
+    void* cub_tmp = nullptr;
+    size_t cub_bytes = 0;
+    int key_bits = 0;
+    unsigned dead_key = 0;
+    int ncells = 0;
+    // misc device buffers
+    unsigned* d_status = nullptr;
+    int* d_int = nullptr;           // small int scratch
+    double* d_part = nullptr;       // reduction partials
+    double* d_diag = nullptr;
+    double* d_xfer = nullptr;       // column-major transfer scratch [cap_host * 4]
+    double* d_export = nullptr;     // k_export output (lazy)
+    long long* d_off64 = nullptr;   // pair offsets (lazy)
+    int* d_cnt_id = nullptr;
+    // timing
+    bool timing = true;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_used = 0;
+    std::vector<int> ev_phase;
+    double t_ms[PH_COUNT] = {0};
+    double t_total = 0;
+    long long n_rhs = 0, n_steps = 0;
+};
+
+namespace {
+
+// --- configuration -> kernel parameters (mirrors the oracle's constants) ---
+int derive_params(const sph_config& c, Params& P) {
+    if (c.kernel_model != SPH_KERNEL_GAUSSIAN && c.kernel_model != SPH_KERNEL_WENDLAND2) return SPH_E_CONFIG;
+    if (c.solver != SPH_SOLVER_MODLR_DELTA_SPS && c.solver != SPH_SOLVER_MUSCL_DELTA_SPS) return SPH_E_CONFIG;
+    if (c.eos != SPH_EOS_TAIT && c.eos != SPH_EOS_LINEAR) return SPH_E_CONFIG;
+    if (c.precision != SPH_PREC_FP64 && c.precision != SPH_PREC_MIXED) return SPH_E_CONFIG;
+    if (c.integrator != SPH_INTEGRATOR_RK4_REUSE) return SPH_E_CONFIG;
+    if (!(c.h > 0) || !(c.kernel_scale >= 2.0) || !(c.dx > 0) || !(c.rho0 > 0) || !(c.c0sq > 0)) return SPH_E_CONFIG;
+    if (c.cell_skin < 0 || c.cell_skin > 2) return SPH_E_CONFIG;
+    if (c.shift_n != 4) return SPH_E_CONFIG;
+    memset(&P, 0, sizeof(P));
+    const bool q = c.reference_literals != 0;
+    P.kernel_model = c.kernel_model;
+    P.solver = c.solver;
+    P.muscl = c.solver == SPH_SOLVER_MUSCL_DELTA_SPS;
+    P.xsph = (c.xsph_eps != 0.0 && !P.muscl) ? 1 : 0;
+    P.renorm = c.renormalize ? 1 : 0;
+    P.quirks = q ? 1 : 0;
+    P.pair_rule = c.pair_rule;
+    P.shifting = c.shifting;
+    P.eos = c.eos;
+    const double pi = 3.14159265358979324;
+    const double pi_k = q ? (double)3.14159265358f : pi;
+    P.pi = pi;
+    P.h = c.h;
+    const double hbar = (c.h + c.h) / 2.0;
+    P.r_cut = c.kernel_scale * hbar;
+    if (q) {
+        float e9 = expf(-9.0f);
+        P.gauss_e9 = (double)e9;
+        double den = (double)(1.0f - 10.0f * e9);
+        P.kfactor = c.kernel_model == SPH_KERNEL_GAUSSIAN ? 1.0 / (pi_k * (c.h * c.h) * den) : 7.0 / (4 * pi_k * (c.h * c.h));
+        P.cut_min = (double)1.0e-7f;
+        P.fs_thr = (double)(float)c.fs_threshold;
+        P.c1414 = (double)1.414f;
+        P.sps_dl = (double)(sqrtf(2.0f) / 2.0f) * c.dx;
+        P.sps_c012 = (double)0.12f;
+        P.sps_23 = (double)(2.0f / 3.0f);
+        P.sps_blin = (double)((2.0f / 3.0f) * 0.0066f);
+        P.q_zero = (double)1.0e-8f;
+    } else {
+        P.gauss_e9 = exp(-9.0);
+        double den = 1.0 - 10.0 * P.gauss_e9;
+        P.kfactor = c.kernel_model == SPH_KERNEL_GAUSSIAN ? 1.0 / (pi_k * (c.h * c.h) * den) : 7.0 / (4 * pi_k * (c.h * c.h));
+        P.cut_min = 1.0e-7;
+        P.fs_thr = c.fs_threshold;
+        P.c1414 = 1.414;
+        P.sps_dl = sqrt(2.0) / 2.0 * c.dx;
+        P.sps_c012 = 0.12;
+        P.sps_23 = 2.0 / 3.0;
+        P.sps_blin = 2.0 / 3.0 * 0.0066;
+        P.q_zero = 1.0e-8;
+    }
+    P.rho0 = c.rho0; P.c0sq = c.c0sq; P.sqrt_c0 = sqrt(c.c0sq); P.eos_b = c.c0sq * c.rho0 / 7.0; P.pb = c.background_p;
+    P.nu = c.nu; P.alpha = c.alpha; P.beta = c.beta; P.fai = c.fai;
+    P.delta = c.delta; P.delta_alpha = c.delta_alpha; P.eps = c.xsph_eps;
+    const double sr = c.kernel_scale * c.h;
+    P.sv = pi * (sr * sr);
+    P.shift_beta = c.shift_beta; P.shift_R = c.shift_R; P.shift_max = c.shift_max; P.shift_n = c.shift_n;
+    // W(dx) (Shift_particle_position.f90:56-68)
+    {
+        double qd = c.dx / c.h;
+        if (c.kernel_model == SPH_KERNEL_GAUSSIAN) P.w_dx = (exp(-(qd * qd)) - P.gauss_e9) * P.kfactor;
+        else { double t = 1 - qd / 2.0; double t2 = t * t; P.w_dx = P.kfactor * (1 + 2 * qd) * (t2 * t2); }
+    }
+    for (int k = 0; k < 2; ++k) { P.box_lo[k] = c.box_lo[k]; P.box_hi[k] = c.box_hi[k]; }
+    P.band = c.kernel_scale * c.h;
+    // cell grid: edge = list radius, one spare cell on every side
+    const double rl = P.r_cut * (1.0 + c.cell_skin);
+    P.r2_list = rl * rl;
+    const double skin = P.r_cut * c.cell_skin;
+    P.skin_half2 = (0.5 * skin) * (0.5 * skin);
+    P.cs = rl;
+    P.gx0 = c.grid_lo[0] - rl;
+    P.gy0 = c.grid_lo[1] - rl;
+    P.gnx = (int)ceil((c.grid_hi[0] - c.grid_lo[0]) / rl) + 3;
+    P.gny = (int)ceil((c.grid_hi[1] - c.grid_lo[1]) / rl) + 3;
+    if (!(c.grid_hi[0] > c.grid_lo[0]) || !(c.grid_hi[1] > c.grid_lo[1])) return SPH_E_CONFIG;
+    if ((long long)P.gnx * P.gny > (1LL << 30)) return SPH_E_CONFIG;
+    // neighbour-list capacity: twice the lattice count inside the list radius
+    const double lat = pi * (rl / c.dx) * (rl / c.dx);
+    int mn = (int)ceil(2.0 * lat) + 16;
+    mn = (mn + 3) & ~3;
+    P.max_nbr = std::min(mn, 256);
+    return SPH_OK;
+}
+
+int status_to_code(unsigned st) {
+    if (st & ST_DOMAIN) return SPH_E_DOMAIN;
+    if (st & (ST_NBR_OVERFLOW | ST_PAIR_OVERFLOW)) return SPH_E_CAPACITY;
+    if (st & ST_NONFINITE) return SPH_E_NONFINITE;
+    if (st & ST_SKIN) return SPH_E_SKIN;
+    return SPH_OK;
+}
+
+// --- timing helpers ---------------------------------------------------------
+void tic(sph_handle* h, int phase) {
+    if (!h->timing) return;
+    if (h->ev_used >= h->ev_pool.size()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        h->ev_pool.push_back(e);
+    }
+    cudaEventRecord(h->ev_pool[h->ev_used], h->stream);
+    h->ev_phase.push_back(phase);
+    h->ev_used++;
+}
+
+void timing_flush(sph_handle* h) {
+    if (!h->timing || h->ev_used == 0) return;
+    cudaEventSynchronize(h->ev_pool[h->ev_used - 1]);
+    for (size_t k = 0; k + 1 < h->ev_used; ++k) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, h->ev_pool[k], h->ev_pool[k + 1]);
+        int ph = h->ev_phase[k];
+        if (ph >= 0 && ph < PH_COUNT) h->t_ms[ph] += ms;
+        h->t_total += ms;
+    }
+    h->ev_used = 0;
+    h->ev_phase.clear();
+}
+
+template <typename R> Sorted<R>& sorted(sph_handle* h);
+template <> Sorted<double>& sorted<double>(sph_handle* h) { return h->D64; }
+template <> Sorted<float>& sorted<float>(sph_handle* h) { return h->D32; }
+
+template <typename R>
+int alloc_sorted(Sorted<R>& D, int cap, int max_nbr, int ncells) {
+    CK(dalloc(&D.id, cap)); CK(dalloc(&D.type, cap));
+    CK(dalloc(&D.pos, cap)); CK(dalloc(&D.pos0, cap)); CK(dalloc(&D.vel0, cap)); CK(dalloc(&D.rho0, cap));
+    CK(dalloc(&D.mass, cap)); CK(dalloc(&D.smass, cap));
+    CK(dalloc(&D.kin, cap)); CK(dalloc(&D.aux, cap));
+    CK(dalloc(&D.nb1, cap)); CK(dalloc(&D.nb2, cap)); CK(dalloc(&D.nb3, cap)); CK(dalloc(&D.binv, cap));
+    CK(dalloc(&D.fra_v, cap)); CK(dalloc(&D.flags, cap));
+    CK(dalloc(&D.drho, cap)); CK(dalloc(&D.acc, cap)); CK(dalloc(&D.avg, cap)); CK(dalloc(&D.shift, cap));
+    CK(dalloc(&D.ks_r, cap)); CK(dalloc(&D.ks_a, cap)); CK(dalloc(&D.ks_v, cap));
+    CK(dalloc(&D.c_drho, cap)); CK(dalloc(&D.c_acc, cap)); CK(dalloc(&D.c_avg, cap));
+    CK(dalloc(&D.nbr, (size_t)cap * max_nbr)); CK(dalloc(&D.nnbr, cap));
+    CK(dalloc(&D.cell_start, ncells)); CK(dalloc(&D.cell_end, ncells));
+    CK(cudaMemset(D.nb3, 0, sizeof(*D.nb3) * (size_t)cap));
+    CK(cudaMemset(D.flags, 0, (size_t)cap));
+    return SPH_OK;
+}
+
+template <typename R>
+void free_sorted(Sorted<R>& D) {
+    void* ptrs[] = {D.id, D.type, D.pos, D.pos0, D.vel0, D.rho0, D.mass, D.smass, D.kin, D.aux, D.nb1, D.nb2, D.nb3,
+                    D.binv, D.fra_v, D.flags, D.drho, D.acc, D.avg, D.shift, D.ks_r, D.ks_a, D.ks_v, D.c_drho,
+                    D.c_acc, D.c_avg, D.nbr, D.nnbr, D.cell_start, D.cell_end};
+    for (void* p : ptrs) if (p) cudaFree(p);
+    D = Sorted<R>{};
+}
+
+// sorted master state -> staging (id order)
+template <typename R>
+int unsort(sph_handle* h) {
+    if (h->staging_valid) return SPH_OK;
+    if (!h->sorted_valid) return SPH_E_ARG;
+    Params P = h->P;
+    k_unsort<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, h->S, sorted<R>(h));
+    CK(cudaGetLastError());
+    h->staging_valid = true;
+    return SPH_OK;
+}
+
+// One exclusive scan of cnt[0..n) into off, returning the total on the host.
+int scan_total(sph_handle* h, const int* cnt, int* off, int n, int* total) {
+    if (n <= 0) { *total = 0; return SPH_OK; }
+    size_t bytes = 0;
+    CK(cub::DeviceScan::ExclusiveSum(nullptr, bytes, cnt, off, n, h->stream));
+    if (bytes > h->cub_bytes) return SPH_E_CAPACITY;
+    CK(cub::DeviceScan::ExclusiveSum(h->cub_tmp, bytes, cnt, off, n, h->stream));
+    int last[2];
+    CK(cudaMemcpyAsync(&last[0], off + n - 1, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(&last[1], cnt + n - 1, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    *total = last[0] + last[1];
+    return SPH_OK;
+}
+
+// Step-start set-up: wrap + periodic images, sort, cell ranges, lists, records.
+template <typename R>
+int prepare(sph_handle* h) {
+    int rc = unsort<R>(h);
+    if (rc) return rc;
+    Params& P = h->P;
+    P.n_host = h->n_host;
+    tic(h, PH_IMAGES);
+    int n_img = 0;
+    if (h->cfg.periodic) {
+        k_wrap<<<blocks(h->n_host, 256), 256, 0, h->stream>>>(P, h->S);
+        // left/right images of the host particles
+        k_img_count<<<blocks(h->n_host, 256), 256, 0, h->stream>>>(P, h->S, h->n_host, 0);
+        int n_lr = 0;
+        rc = scan_total(h, h->S.cnt, h->S.off, h->n_host, &n_lr);
+        if (rc) return rc;
+        if (h->n_host + n_lr > h->cap_tot) return SPH_E_CAPACITY;
+        k_img_emit<<<blocks(h->n_host, 256), 256, 0, h->stream>>>(P, h->S, h->n_host, 0, h->n_host, h->S.off);
+        // bottom/top images of host particles and left/right images
+        const int n_src = h->n_host + n_lr;
+        k_img_count<<<blocks(n_src, 256), 256, 0, h->stream>>>(P, h->S, n_src, 1);
+        int n_tb = 0;
+        rc = scan_total(h, h->S.cnt, h->S.off, n_src, &n_tb);
+        if (rc) return rc;
+        if (n_src + n_tb > h->cap_tot) return SPH_E_CAPACITY;
+        k_img_emit<<<blocks(n_src, 256), 256, 0, h->stream>>>(P, h->S, n_src, 1, n_src, h->S.off);
+        n_img = n_lr + n_tb;
+        CK(cudaGetLastError());
+    }
+    h->n_img = n_img;
+    P.n_tot = h->n_host + n_img;
+    tic(h, PH_SORT);
+    Sorted<R>& D = sorted<R>(h);
+    k_cell_keys<<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, h->S.pos, h->S.type, h->keys_in, h->vals_in,
+                                                              h->d_status, h->dead_key);
+    size_t bytes = h->cub_bytes;
+    CK(cub::DeviceRadixSort::SortPairs(h->cub_tmp, bytes, h->keys_in, h->keys_out, h->vals_in, h->vals_out,
+                                       P.n_tot, 0, h->key_bits, h->stream));
+    k_gather_sorted<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, h->S, D, h->vals_out);
+    CK(cudaMemsetAsync(D.cell_start, 0xff, sizeof(int) * (size_t)h->ncells, h->stream));
+    CK(cudaMemsetAsync(D.cell_end, 0xff, sizeof(int) * (size_t)h->ncells, h->stream));
+    k_cell_ranges<<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P.n_tot, h->keys_out, D.cell_start, D.cell_end,
+                                                                h->dead_key);
+    k_build_lists<R><<<blocks(P.n_tot, 128), 128, 0, h->stream>>>(P, D, h->d_status);
+    k_records<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, D);
+    CK(cudaGetLastError());
+    h->sorted_valid = true;
+    h->staging_valid = false;   // the master state now lives in the sorted arrays
+    return SPH_OK;
+}
+
+// One RHS evaluation on the current stage state.
+template <typename R>
+int rhs(sph_handle* h, int last) {
+    const Params& P = h->P;
+    Sorted<R>& D = sorted<R>(h);
+    const int nb = blocks(P.n_tot, 128);
+    tic(h, PH_A);
+    k_pass_a<R><<<nb, 128, 0, h->stream>>>(P, D);
+    tic(h, PH_SURF);
+    k_surface<R><<<nb, 128, 0, h->stream>>>(P, D);
+    k_near<R><<<nb, 128, 0, h->stream>>>(P, D);
+    tic(h, PH_C);
+    if (P.muscl) k_pass_c<R, true><<<nb, 128, 0, h->stream>>>(P, D, last);
+    else k_pass_c<R, false><<<nb, 128, 0, h->stream>>>(P, D, last);
+    CK(cudaGetLastError());
+    h->n_rhs++;
+    h->have_rhs = true;
+    return SPH_OK;
+}
+
+template <typename R>
+int stage(sph_handle* h, int st, double dt, int use_carried, int do_shift) {
+    const Params& P = h->P;
+    tic(h, PH_UPDATE);
+    k_stage<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, sorted<R>(h), st, dt, use_carried, do_shift,
+                                                             h->d_status);
+    CK(cudaGetLastError());
+    return SPH_OK;
+}
+
+int read_status(sph_handle* h) {
+    unsigned st = 0;
+    CK(cudaMemcpyAsync(&st, h->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (st) CK(cudaMemsetAsync(h->d_status, 0, sizeof(unsigned), h->stream));
+    return status_to_code(st);
+}
+
+template <typename R>
+int run_steps(sph_handle* h, int nsteps, double dt) {
+    for (int s = 0; s < nsteps; ++s) {
+        int rc = prepare<R>(h);
+        if (rc) return rc;
+        const int first = h->step_count == 0;
+        if (first) { rc = rhs<R>(h, 0); if (rc) return rc; }
+        rc = stage<R>(h, 0, dt, first ? 0 : 1, 0); if (rc) return rc;
+        rc = rhs<R>(h, 0); if (rc) return rc;
+        rc = stage<R>(h, 1, dt, 0, 0); if (rc) return rc;
+        rc = rhs<R>(h, 0); if (rc) return rc;
+        rc = stage<R>(h, 2, dt, 0, 0); if (rc) return rc;
+        rc = rhs<R>(h, 1); if (rc) return rc;
+        rc = stage<R>(h, 3, dt, 0, h->cfg.shifting); if (rc) return rc;
+        tic(h, -1);
+        h->step_count++;
+        h->n_steps++;
+        if (h->ev_used > 4096) timing_flush(h);
+    }
+    timing_flush(h);
+    return read_status(h);
+}
+
+template <typename R>
+int diagnostics(sph_handle* h, sph_diag* out) {
+    memset(out, 0, sizeof(*out));
+    if (!h->sorted_valid) {
+        // state only in staging: sort it once to reduce over the same arrays
+        int rc = prepare<R>(h);
+        if (rc) return rc;
+    }
+    const Params& P = h->P;
+    const int nparts = 148 * 4;
+    k_diag_partial<R><<<nparts, kRedThreads, 0, h->stream>>>(P, sorted<R>(h), h->d_part, h->d_part + nparts);
+    k_diag_final<<<1, kRedThreads, 0, h->stream>>>(nparts, h->d_part, h->d_part + nparts, h->d_diag);
+    CK(cudaMemsetAsync(h->d_int, 0, sizeof(int), h->stream));
+    k_count_surface<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, sorted<R>(h), h->d_int);
+    double v[2];
+    int nsurf = 0;
+    CK(cudaMemcpyAsync(v, h->d_diag, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(&nsurf, h->d_int, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    out->kinetic_energy = v[0];
+    out->max_speed = v[1];
+    out->n_images = h->n_img;
+    out->n_surface = h->have_rhs ? nsurf : 0;
+    out->pair_count = h->last_pairs;
+    return SPH_OK;
+}
+
+__global__ void k_to_ll(int n, const int* in, long long* out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = in[i];
+}
+
+// find_particle_pair on the current (prepared) state.
+template <typename R>
+int find_pairs(sph_handle* h, long long pair_cap, int* pi, int* pj, double* w, double* dwdx, long long* total) {
+    const Params& P = h->P;
+    const int n = P.n_tot;
+    if (!h->d_cnt_id) CK(dalloc(&h->d_cnt_id, h->cap_tot));
+    if (!h->d_off64) CK(dalloc(&h->d_off64, 2 * ((size_t)h->cap_tot + 1)));
+    long long* cnt64 = h->d_off64 + (h->cap_tot + 1);
+    k_pair_count<R><<<blocks(n, 128), 128, 0, h->stream>>>(P, sorted<R>(h), h->d_cnt_id);
+    k_to_ll<<<blocks(n, 256), 256, 0, h->stream>>>(n, h->d_cnt_id, cnt64);
+    size_t bytes = 0;
+    CK(cub::DeviceScan::ExclusiveSum(nullptr, bytes, cnt64, h->d_off64, n, h->stream));
+    if (bytes > h->cub_bytes) return SPH_E_CAPACITY;
+    CK(cub::DeviceScan::ExclusiveSum(h->cub_tmp, bytes, cnt64, h->d_off64, n, h->stream));
+    long long last[2];
+    CK(cudaMemcpyAsync(&last[0], h->d_off64 + n - 1, sizeof(long long), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(&last[1], cnt64 + n - 1, sizeof(long long), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    *total = last[0] + last[1];
+    h->last_pairs = *total;
+    if (pi == nullptr || pair_cap <= 0) return SPH_OK;
+    const long long m = std::min(*total, pair_cap);
+    int *dpi = nullptr, *dpj = nullptr;
+    double *dw = nullptr, *ddw = nullptr;
+    CK(dalloc(&dpi, m)); CK(dalloc(&dpj, m));
+    if (w) CK(dalloc(&dw, m));
+    if (dwdx) CK(dalloc(&ddw, 2 * m));
+    k_pair_emit<R><<<blocks(n, 128), 128, 0, h->stream>>>(P, sorted<R>(h), h->d_off64, m, dpi, dpj, dw, ddw);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(pi, dpi, sizeof(int) * m, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(pj, dpj, sizeof(int) * m, cudaMemcpyDeviceToHost, h->stream));
+    if (w) CK(cudaMemcpyAsync(w, dw, sizeof(double) * m, cudaMemcpyDeviceToHost, h->stream));
+    if (dwdx) {
+        CK(cudaMemcpyAsync(dwdx, ddw, sizeof(double) * m, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(dwdx + pair_cap, ddw + m, sizeof(double) * m, cudaMemcpyDeviceToHost, h->stream));
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    cudaFree(dpi); cudaFree(dpj);
+    if (dw) cudaFree(dw);
+    if (ddw) cudaFree(ddw);
+    return *total > pair_cap ? SPH_E_CAPACITY : SPH_OK;
+}
+
+template <typename R>
+int export_fields(sph_handle* h) {
+    if (!h->have_rhs || !h->sorted_valid) return SPH_E_ARG;
+    if (!h->d_export) CK(dalloc(&h->d_export, (size_t)kExportFields * h->cap_host));
+    const Params& P = h->P;
+    k_export<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, sorted<R>(h), h->d_export);
+    CK(cudaGetLastError());
+    return SPH_OK;
+}
+
+// Dispatch on the pair precision of the handle.
+#define DISPATCH(h, fn, ...) ((h)->mixed ? fn<float>(__VA_ARGS__) : fn<double>(__VA_ARGS__))
+
+void destroy(sph_handle* h) {
+    if (!h) return;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    free_sorted(h->D64);
+    free_sorted(h->D32);
+    void* ptrs[] = {h->S.pos, h->S.vel, h->S.rho, h->S.mass, h->S.smass, h->S.type, h->S.r_drho, h->S.r_acc,
+                    h->S.r_avg, h->S.cnt, h->S.off, h->keys_in, h->keys_out, h->vals_in, h->vals_out, h->cub_tmp,
+                    h->d_status, h->d_int, h->d_part, h->d_diag, h->d_xfer, h->d_export, h->d_off64, h->d_cnt_id};
+    for (void* p : ptrs) if (p) cudaFree(p);
+    for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+int init_impl(const sph_config* cfg, int n_capacity, sph_handle** out) {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return SPH_E_NODEVICE;
+    sph_handle* h = new (std::nothrow) sph_handle();
+    if (!h) return SPH_E_CAPACITY;
+    h->cfg = *cfg;
+    int rc = derive_params(*cfg, h->P);
+    if (rc) { delete h; return rc; }
+    CK(cudaGetDevice(&h->device));
+    h->mixed = cfg->precision == SPH_PREC_MIXED;
+    h->cap_host = n_capacity;
+    // periodic image capacity: the edge bands, 1.5x the uniform-density estimate
+    if (cfg->periodic) {
+        const double fx = h->P.band / (cfg->box_hi[0] - cfg->box_lo[0]);
+        const double fy = h->P.band / (cfg->box_hi[1] - cfg->box_lo[1]);
+        const double est = (double)n_capacity * (2 * fx + 2 * fy + 4 * fx * fy);
+        h->cap_img = (int)(1.5 * est) + 256;
+    }
+    h->cap_tot = h->cap_host + h->cap_img;
+    const int cap = h->cap_tot;
+    h->ncells = h->P.gnx * h->P.gny;
+    h->key_bits = 1;
+    while ((1LL << h->key_bits) <= (long long)h->ncells) h->key_bits++;
+    h->dead_key = (unsigned)((1ULL << h->key_bits) - 1);
+    h->P.nbr_stride = cap;
+    CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    // staging
+    CK(dalloc(&h->S.pos, cap)); CK(dalloc(&h->S.vel, cap)); CK(dalloc(&h->S.rho, cap));
+    CK(dalloc(&h->S.mass, cap)); CK(dalloc(&h->S.smass, cap)); CK(dalloc(&h->S.type, cap));
+    CK(dalloc(&h->S.r_drho, h->cap_host)); CK(dalloc(&h->S.r_acc, h->cap_host)); CK(dalloc(&h->S.r_avg, h->cap_host));
+    CK(dalloc(&h->S.cnt, cap)); CK(dalloc(&h->S.off, cap));
+    // sort
+    CK(dalloc(&h->keys_in, cap)); CK(dalloc(&h->keys_out, cap));
+    CK(dalloc(&h->vals_in, cap)); CK(dalloc(&h->vals_out, cap));
+    {
+        size_t b1 = 0, b2 = 0, b3 = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, b1, h->keys_in, h->keys_out, h->vals_in, h->vals_out, cap, 0,
+                                        h->key_bits, h->stream);
+        cub::DeviceScan::ExclusiveSum(nullptr, b2, h->S.cnt, h->S.off, cap, h->stream);
+        long long* dummy = nullptr;
+        cub::DeviceScan::ExclusiveSum(nullptr, b3, dummy, dummy, cap, h->stream);
+        h->cub_bytes = std::max(b1, std::max(b2, b3)) + 1024;
+        CK(cudaMalloc(&h->cub_tmp, h->cub_bytes));
+    }
+    CK(dalloc(&h->d_status, 1)); CK(cudaMemset(h->d_status, 0, sizeof(unsigned)));
+    CK(dalloc(&h->d_int, 4));
+    CK(dalloc(&h->d_part, 2 * 148 * 4)); CK(dalloc(&h->d_diag, 2));
+    CK(dalloc(&h->d_xfer, (size_t)4 * h->cap_host));
+    if (h->mixed) rc = alloc_sorted(h->D32, cap, h->P.max_nbr, h->ncells);
+    else rc = alloc_sorted(h->D64, cap, h->P.max_nbr, h->ncells);
+    if (rc) { destroy(h); return rc; }
+    *out = h;
+    return SPH_OK;
+}
+
+template <typename R>
+int get_state_impl(sph_handle* h, int n, double* pos, double* vel, double* rho, double* press) {
+    int rc = unsort<R>(h);
+    if (rc) return rc;
+    if (pos) {
+        k_deinterleave<<<blocks(n, 256), 256, 0, h->stream>>>(n, h->S.pos, h->d_xfer);
+        CK(cudaMemcpyAsync(pos, h->d_xfer, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    if (vel) {
+        k_deinterleave<<<blocks(n, 256), 256, 0, h->stream>>>(n, h->S.vel, h->d_xfer);
+        CK(cudaMemcpyAsync(vel, h->d_xfer, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    if (rho || press) {
+        std::vector<double> tmp;
+        double* r = rho;
+        if (!r) { tmp.resize(n); r = tmp.data(); }
+        CK(cudaMemcpyAsync(r, h->S.rho, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if (press) {
+            const Params& P = h->P;
+            for (int i = 0; i < n; ++i) {
+                double x = r[i] / P.rho0;
+                double x2 = x * x, x4 = x2 * x2;
+                press[i] = P.eos == SPH_EOS_TAIT ? P.eos_b * (x4 * x2 * x - 1.0) + P.pb : P.c0sq * (r[i] - P.rho0) + P.pb;
+            }
+        }
+    }
+    return SPH_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C-ABI
+// ===========================================================================
+extern "C" {
+
+const char* sph_strerror(int code) {
+    int k = -code;
+    if (k < 0 || k >= (int)(sizeof(kMessages) / sizeof(kMessages[0]))) return "unknown status";
+    return kMessages[k];
+}
+
+int sph_init(const sph_config* cfg, int n_capacity, sph_handle** out) {
+    if (!cfg || !out || n_capacity <= 0) return SPH_E_ARG;
+    *out = nullptr;
+    return init_impl(cfg, n_capacity, out);
+}
+
+int sph_free(sph_handle* h) {
+    if (!h) return SPH_E_ARG;
+    destroy(h);
+    return SPH_OK;
+}
+
+int sph_set_state(sph_handle* h, int n, const double* pos, const double* vel, const double* rho,
+                  const double* mass, const int* type, const double* sps_mass) {
+    if (!h || !pos || !vel || !rho || !mass || !type || n <= 0) return SPH_E_ARG;
+    if (n > h->cap_host) return SPH_E_CAPACITY;
+    CK(cudaSetDevice(h->device));
+    h->n_host = n;
+    CK(cudaMemcpyAsync(h->d_xfer, pos, sizeof(double) * 2 * n, cudaMemcpyHostToDevice, h->stream));
+    k_interleave<<<blocks(n, 256), 256, 0, h->stream>>>(n, h->d_xfer, h->S.pos);
+    CK(cudaMemcpyAsync(h->d_xfer + 2 * (size_t)n, vel, sizeof(double) * 2 * n, cudaMemcpyHostToDevice, h->stream));
+    k_interleave<<<blocks(n, 256), 256, 0, h->stream>>>(n, h->d_xfer + 2 * (size_t)n, h->S.vel);
+    CK(cudaMemcpyAsync(h->S.rho, rho, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->S.mass, mass, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->S.smass, sps_mass ? sps_mass : mass, sizeof(double) * n, cudaMemcpyHostToDevice,
+                       h->stream));
+    CK(cudaMemcpyAsync(h->S.type, type, sizeof(int) * n, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemsetAsync(h->S.r_drho, 0, sizeof(double) * n, h->stream));
+    CK(cudaMemsetAsync(h->S.r_acc, 0, sizeof(double2) * n, h->stream));
+    CK(cudaMemsetAsync(h->S.r_avg, 0, sizeof(double2) * n, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->staging_valid = true;
+    h->sorted_valid = false;
+    h->have_rhs = false;
+    h->step_count = 0;
+    return SPH_OK;
+}
+
+int sph_get_state(sph_handle* h, int n, double* pos, double* vel, double* rho, double* press) {
+    if (!h || n != h->n_host || n <= 0) return SPH_E_ARG;
+    CK(cudaSetDevice(h->device));
+    return DISPATCH(h, get_state_impl, h, n, pos, vel, rho, press);
+}
+
+int sph_find_particle_pair(sph_handle* h, long long pair_cap, int* pair_i, int* pair_j, double* w, double* dwdx,
+                           long long* pair_number) {
+    if (!h || !pair_number || h->n_host <= 0) return SPH_E_ARG;
+    if (pair_cap > 0 && (!pair_i || !pair_j)) return SPH_E_ARG;
+    CK(cudaSetDevice(h->device));
+    int rc = DISPATCH(h, prepare, h);
+    if (rc) return rc;
+    rc = read_status(h);
+    if (rc) return rc;
+    return DISPATCH(h, find_pairs, h, pair_cap, pair_i, pair_j, w, dwdx, pair_number);
+}
+
+int sph_rhs(sph_handle* h, double* drhodt, double* acc, double* avg_vel, int* fs, int* near_fs) {
+    if (!h || h->n_host <= 0) return SPH_E_ARG;
+    CK(cudaSetDevice(h->device));
+    int rc = DISPATCH(h, prepare, h);
+    if (rc) return rc;
+    rc = DISPATCH(h, rhs, h, 0);
+    if (rc) return rc;
+    timing_flush(h);
+    rc = read_status(h);
+    if (rc) return rc;
+    rc = DISPATCH(h, export_fields, h);
+    if (rc) return rc;
+    const size_t n = (size_t)h->n_host;
+    std::vector<double> buf(7 * n);
+    CK(cudaMemcpyAsync(buf.data(), h->d_export, sizeof(double) * 7 * n, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (size_t i = 0; i < n; ++i) {
+        if (drhodt) drhodt[i] = buf[i];
+        if (acc) { acc[i] = buf[n + i]; acc[n + i] = buf[2 * n + i]; }
+        if (avg_vel) { avg_vel[i] = buf[3 * n + i]; avg_vel[n + i] = buf[4 * n + i]; }
+        if (fs) fs[i] = (int)buf[5 * n + i];
+        if (near_fs) near_fs[i] = (int)buf[6 * n + i];
+    }
+    return SPH_OK;
+}
+
+int sph_get_field(sph_handle* h, int field, double* out) {
+    if (!h || !out || !h->have_rhs) return SPH_E_ARG;
+    CK(cudaSetDevice(h->device));
+    int first, count;
+    switch (field) {
+        case SPH_FIELD_FRA_V: first = 7; count = 1; break;
+        case SPH_FIELD_BINV: first = 8; count = 4; break;
+        case SPH_FIELD_TAU: first = 12; count = 3; break;
+        case SPH_FIELD_GRADS: first = 15; count = 8; break;
+        default: return SPH_E_ARG;
+    }
+    int rc = DISPATCH(h, export_fields, h);
+    if (rc) return rc;
+    const size_t n = (size_t)h->n_host;
+    CK(cudaMemcpyAsync(out, h->d_export + first * n, sizeof(double) * count * n, cudaMemcpyDeviceToHost,
+                       h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return SPH_OK;
+}
+
+int sph_step(sph_handle* h, int nsteps, double dt, sph_diag* out) {
+    if (!h || nsteps < 0 || !(dt > 0) || h->n_host <= 0) return SPH_E_ARG;
+    CK(cudaSetDevice(h->device));
+    int rc = DISPATCH(h, run_steps, h, nsteps, dt);
+    if (rc) return rc;
+    if (out) return DISPATCH(h, diagnostics, h, out);
+    return SPH_OK;
+}
+
+int sph_diagnostics(sph_handle* h, sph_diag* out) {
+    if (!h || !out || h->n_host <= 0) return SPH_E_ARG;
+    CK(cudaSetDevice(h->device));
+    return DISPATCH(h, diagnostics, h, out);
+}
+
+int sph_get_timings(sph_handle* h, sph_timings* out) {
+    if (!h || !out) return SPH_E_ARG;
+    timing_flush(h);
+    out->sort_ms = h->t_ms[PH_SORT];
+    out->pass_a_ms = h->t_ms[PH_A];
+    out->surface_ms = h->t_ms[PH_SURF];
+    out->pass_c_ms = h->t_ms[PH_C];
+    out->update_ms = h->t_ms[PH_UPDATE];
+    out->images_ms = h->t_ms[PH_IMAGES];
+    out->total_ms = h->t_total;
+    out->rhs_evaluations = h->n_rhs;
+    out->steps = h->n_steps;
+    return SPH_OK;
+}
+
+int sph_reset_timings(sph_handle* h) {
+    if (!h) return SPH_E_ARG;
+    timing_flush(h);
+    for (double& t : h->t_ms) t = 0;
+    h->t_total = 0;
+    h->n_rhs = 0;
+    h->n_steps = 0;
+    return SPH_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,234 @@
+// update.cuh -- integrator stages, shifting, diagnostics reductions, pair
+// enumeration for the find_particle_pair entry point, and layout conversions.
+#pragma once
+#include "pass_c.cuh"
+
+namespace sph {
+
+// Runge-Kutta stages of time_iteration.f90 (water particles only; images and
+// boundary particles keep their step-start state, as the reference only
+// updates type 2 at :944, :978, :1008, :1038):
+//   stage 0  rho = rho0 + drhodt*dt/2, v = v0 + 0.5 dt a + avg, x = x0 + 0.5 dt v    K = K1
+//   stage 1  same with the second RHS                                          K += 2 K2
+//   stage 2  full dt with the third RHS                                        K += 2 K3
+//   stage 3  rho = rho0 + (K + drhodt) dt/6, v = v0 + (K_a + a) dt/6 + avg,
+//            x = x0 + (K_v + v) dt/6 + 0.5 dt^2 a; then Shift_particle_position.
+// Stage 0 uses the rates carried from the previous step (K1 reuse, :940-965)
+// unless this is the first step, when a fresh RHS precedes it (:821).
+template <typename R>
+__global__ void k_stage(Params P, Sorted<R> D, int stage, double dt, int use_carried, int do_shift,
+                        unsigned* status) {
+    using V2 = typename VT<R>::V2;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= P.n_tot) return;
+    if (D.type[s] != SPH_TYPE_WATER) return;
+    const double2 x0 = D.pos0[s];
+    const double2 v0 = D.vel0[s];
+    const double r0 = D.rho0[s];
+    double dr, ax, ay, gx, gy;
+    if (stage == 0 && use_carried) {
+        dr = (double)D.c_drho[s]; V2 a = D.c_acc[s], g = D.c_avg[s];
+        ax = (double)a.x; ay = (double)a.y; gx = (double)g.x; gy = (double)g.y;
+    } else {
+        dr = (double)D.drho[s]; V2 a = D.acc[s], g = D.avg[s];
+        ax = (double)a.x; ay = (double)a.y; gx = (double)g.x; gy = (double)g.y;
+    }
+    double rho, u, v, x, y;
+    if (stage < 3) {
+        const double f = stage < 2 ? 0.5 * dt : dt;
+        rho = stage < 2 ? r0 + dr * dt / 2 : r0 + dr * dt;
+        u = v0.x + f * ax + gx;
+        x = x0.x + f * u;
+        v = v0.y + f * ay + gy;
+        y = x0.y + f * v;
+        if (stage == 0) {
+            D.ks_r[s] = (R)dr;
+            D.ks_a[s] = mk2<R>((R)ax, (R)ay);
+            D.ks_v[s] = mk2<R>((R)u, (R)v);
+        } else {
+            D.ks_r[s] = D.ks_r[s] + R(2) * (R)dr;
+            V2 ka = D.ks_a[s], kv = D.ks_v[s];
+            D.ks_a[s] = mk2<R>(ka.x + R(2) * (R)ax, ka.y + R(2) * (R)ay);
+            D.ks_v[s] = mk2<R>(kv.x + R(2) * (R)u, kv.y + R(2) * (R)v);
+        }
+    } else {
+        const V2 ka = D.ks_a[s], kv = D.ks_v[s];
+        rho = r0 + ((double)D.ks_r[s] + dr) * dt / 6.0;
+        u = v0.x + ((double)ka.x + ax) * dt / 6.0 + gx;
+        x = x0.x + ((double)kv.x + u) * dt / 6.0 + 0.5 * dt * dt * ax;
+        v = v0.y + ((double)ka.y + ay) * dt / 6.0 + gy;
+        y = x0.y + ((double)kv.y + v) * dt / 6.0 + 0.5 * dt * dt * ay;
+        // rates of this last RHS become next step's K1
+        D.c_drho[s] = (R)dr;
+        D.c_acc[s] = mk2<R>((R)ax, (R)ay);
+        D.c_avg[s] = mk2<R>((R)gx, (R)gy);
+    }
+    // the neighbour lists stay exact while nobody moved more than half the skin
+    const double ddx = x - x0.x, ddy = y - x0.y;
+    if (ddx * ddx + ddy * ddy > P.skin_half2) atomicOr(status, ST_SKIN);
+    if (stage == 3) {
+        if (do_shift && !(D.flags[s] & 2)) {
+            // Shift_particle_position.f90:108-131
+            const V2 sh = D.shift[s];
+            double s0 = (double)sh.x, s1 = (double)sh.y;
+            const double amp = sqrt(s0 * s0 + s1 * s1);
+            if (amp > P.shift_max) { s0 = s0 / amp * P.shift_max; s1 = s1 / amp * P.shift_max; }
+            x = x + s0;
+            y = y + s1;
+            rho = rho + (double)D.nb1[s].w * s0;
+            rho = rho + (double)D.nb2[s].x * s1;
+        }
+        if (!(isfinite(x) && isfinite(y) && isfinite(u) && isfinite(v) && isfinite(rho))) atomicOr(status, ST_NONFINITE);
+        D.pos0[s] = make_double2(x, y);
+        D.vel0[s] = make_double2(u, v);
+        D.rho0[s] = rho;
+        D.pos[s] = make_double2(x, y);
+    } else {
+        D.pos[s] = make_double2(x, y);
+    }
+    double p, c;
+    eos64(P, rho, p, c);
+    const double m = D.mass[s];
+    D.kin[s] = mk4<R>((R)u, (R)v, Dens<R>::store(rho, P.rho0), (R)p);
+    D.aux[s] = mk4<R>((R)m, (R)(m / rho), (R)c, (R)D.smass[s]);
+}
+
+// Kinetic energy and max |v| of the water host particles
+// (Sampling_subroutine.f90:346-356): deterministic two-level reduction in FP64.
+constexpr int kRedThreads = 256;
+template <typename R>
+__global__ void k_diag_partial(Params P, Sorted<R> D, double* part_ke, double* part_max) {
+    __shared__ double ske[kRedThreads], smx[kRedThreads];
+    double ke = 0.0, mx = 0.0;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < P.n_tot; s += gridDim.x * blockDim.x) {
+        if (D.type[s] != SPH_TYPE_WATER || D.id[s] >= P.n_host) continue;
+        double2 v = D.vel0[s];
+        double vv = v.x * v.x + v.y * v.y;
+        ke += 0.5 * D.mass[s] * vv;
+        mx = fmax(mx, sqrt(vv));
+    }
+    ske[threadIdx.x] = ke; smx[threadIdx.x] = mx;
+    __syncthreads();
+    for (int w = kRedThreads / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) { ske[threadIdx.x] += ske[threadIdx.x + w]; smx[threadIdx.x] = fmax(smx[threadIdx.x], smx[threadIdx.x + w]); }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) { part_ke[blockIdx.x] = ske[0]; part_max[blockIdx.x] = smx[0]; }
+}
+
+__global__ void k_diag_final(int nparts, const double* part_ke, const double* part_max, double* out) {
+    __shared__ double ske[kRedThreads], smx[kRedThreads];
+    double ke = 0.0, mx = 0.0;
+    for (int i = threadIdx.x; i < nparts; i += blockDim.x) { ke += part_ke[i]; mx = fmax(mx, part_max[i]); }
+    ske[threadIdx.x] = ke; smx[threadIdx.x] = mx;
+    __syncthreads();
+    for (int w = kRedThreads / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) { ske[threadIdx.x] += ske[threadIdx.x + w]; smx[threadIdx.x] = fmax(smx[threadIdx.x], smx[threadIdx.x + w]); }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) { out[0] = ske[0]; out[1] = smx[0]; }
+}
+
+// Count of flagged surface particles (diagnostics).
+template <typename R>
+__global__ void k_count_surface(Params P, Sorted<R> D, int* out) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= P.n_tot) return;
+    if (D.flags[s] & 1) atomicAdd(out, 1);
+}
+
+// --- find_particle_pair entry point ---------------------------------------
+// Pairs are emitted once, by their pair_i (lower id), sorted by (i, j).
+template <typename R>
+__global__ void k_pair_count(Params P, Sorted<R> D, int* cnt_id) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= P.n_tot) return;
+    const int nn = D.nnbr[a];
+    const double2 xa = D.pos[a];
+    int c = 0;
+    for (int e = 0; e < nn; ++e) {
+        const unsigned ent = D.nbr[(size_t)e * P.nbr_stride + a];
+        if (!(ent >> 31)) continue;
+        const double2 xb = D.pos[ent & 0x7fffffffu];
+        double d;
+        if (in_support(P, xa.x - xb.x, xa.y - xb.y, d)) ++c;
+    }
+    cnt_id[D.id[a]] = c;
+}
+
+template <typename R>
+__global__ void k_pair_emit(Params P, Sorted<R> D, const long long* off_id, long long cap, int* pi, int* pj,
+                            double* w, double* dwdx) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= P.n_tot) return;
+    const int nn = D.nnbr[a];
+    const double2 xa = D.pos[a];
+    const int ida = D.id[a];
+    int bid[256];
+    int m = 0;
+    for (int e = 0; e < nn && m < 256; ++e) {
+        const unsigned ent = D.nbr[(size_t)e * P.nbr_stride + a];
+        if (!(ent >> 31)) continue;
+        const int b = (int)(ent & 0x7fffffffu);
+        const double2 xb = D.pos[b];
+        double d;
+        if (!in_support(P, xa.x - xb.x, xa.y - xb.y, d)) continue;
+        // insertion by neighbour id
+        const int idb = D.id[b];
+        int k = m++;
+        while (k > 0 && D.id[bid[k - 1]] > idb) { bid[k] = bid[k - 1]; --k; }
+        bid[k] = b;
+    }
+    long long o = off_id[ida];
+    for (int k = 0; k < m; ++k, ++o) {
+        if (o >= cap) return;
+        const int b = bid[k];
+        const double2 xb = D.pos[b];
+        double dx = xa.x - xb.x, dy = xa.y - xb.y, d;
+        in_support(P, dx, dy, d);
+        double ww, gx, gy;
+        kernel_w_dw<double>(P, d, dx, dy, ww, gx, gy);
+        pi[o] = ida + 1;
+        pj[o] = D.id[b] + 1;
+        if (w) w[o] = ww;
+        if (dwdx) { dwdx[o] = gx; dwdx[cap + o] = gy; }
+    }
+}
+
+// --- column-major (n,2) <-> interleaved conversions -----------------------
+__global__ void k_interleave(int n, const double* colmaj, double2* out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = make_double2(colmaj[i], colmaj[n + i]);
+}
+__global__ void k_deinterleave(int n, const double2* in, double* colmaj) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) { double2 v = in[i]; colmaj[i] = v.x; colmaj[n + i] = v.y; }
+}
+
+// Per-particle outputs of the last RHS in id order (host particles), as doubles.
+// Layout: [0] drho, [1,2] acc, [3,4] avg, [5] fs, [6] near, [7] fra_v,
+// [8..11] binv, [12..14] tau, [15..22] grads  (each block n long).
+constexpr int kExportFields = 23;
+template <typename R>
+__global__ void k_export(Params P, Sorted<R> D, double* out) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= P.n_tot) return;
+    int i = D.id[s];
+    if (i >= P.n_host) return;
+    const size_t n = (size_t)P.n_host;
+    out[0 * n + i] = (double)D.drho[s];
+    out[1 * n + i] = (double)D.acc[s].x; out[2 * n + i] = (double)D.acc[s].y;
+    out[3 * n + i] = (double)D.avg[s].x; out[4 * n + i] = (double)D.avg[s].y;
+    out[5 * n + i] = (D.flags[s] & 1) ? 1.0 : 0.0;
+    out[6 * n + i] = (D.flags[s] & 2) ? 1.0 : 0.0;
+    out[7 * n + i] = (double)D.fra_v[s];
+    auto bi = D.binv[s]; auto n1 = D.nb1[s]; auto n2 = D.nb2[s]; auto n3 = D.nb3[s];
+    out[8 * n + i] = (double)bi.x; out[9 * n + i] = (double)bi.y; out[10 * n + i] = (double)bi.z; out[11 * n + i] = (double)bi.w;
+    out[12 * n + i] = (double)n1.x; out[13 * n + i] = (double)n1.y; out[14 * n + i] = (double)n1.z;
+    out[15 * n + i] = (double)n1.w; out[16 * n + i] = (double)n2.x;
+    out[17 * n + i] = (double)n2.y; out[18 * n + i] = (double)n2.z;
+    out[19 * n + i] = (double)n2.w; out[20 * n + i] = (double)n3.x;
+    out[21 * n + i] = (double)n3.y; out[22 * n + i] = (double)n3.z;
+}
+
+}  // namespace sph
