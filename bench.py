@@ -1,0 +1,347 @@
+"""Benchmark of the weakly-compressible SPH time step (libsph_b200).
+
+Workload: the 2048 x 2048 Taylor-Green vortex (4,194,304 particles), MUSCL
+linear-Riemann + delta-SPH + SPS solver, Wendland C2 (h = 1.3 dx), true 2x2
+renormalisation, periodic images, RK4 with K1 reuse (3 RHS per step after the
+first), particle shifting.  A "step" is one time step of that integrator over
+all particles.  Synthetic data: the analytic Taylor-Green initial field.
+
+Headline value: particle-steps/s of the mixed-precision step (FP32 pair
+arithmetic, compensated sums, FP64 state), inputs resident on the device,
+device-timed with CUDA events on the library's stream; the FP64 step is
+reported beside it.  e2e: the same step through the C-ABI with host buffers:
+every step uploads x, v, rho (sph_update_state), advances (sph_step) and
+downloads x, v, rho (sph_get_state).
+
+Multi-GPU: the path does not shard (one GPU holds all particles), so
+--gpus N runs N independent replicas (weak scaling, no collective on the data
+path); value = particles x steps of all ranks / max-over-ranks time.
+
+--impl reference: the CPU restatement of the reference (oracle/, OpenMP over
+particles) on the host cores, on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "sph-2d_b200"))
+
+METRIC = "particle-steps/s at 4.2M TGV: mixed vs FP64 GPU at <=1e-5 L2; adjoint/fwd cost"
+UNIT = "particle-steps/s"
+N_SIDE = 2048
+WORKLOAD = ("Taylor-Green vortex 2048x2048 (4,194,304 particles), MUSCL linear-Riemann + delta-SPH + SPS, "
+            "Wendland C2 h=1.3dx, rho0=1, c0=10, Re=100, RK4 with K1 reuse (3 RHS/step), shifting, periodic images")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="native", choices=["native", "reference"])
+    ap.add_argument("--n-side", type=int, default=N_SIDE)
+    ap.add_argument("--skip-accuracy", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Clocks:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def roofline_traffic():
+    """Measured DRAM bytes per particle of the pass-C kernel (ncu capture summarised
+    in profiles/), or None when no capture has been committed."""
+    path = os.path.join(ROOT, "profiles", "pass_c_dram_bytes_per_particle.txt")
+    try:
+        for line in open(path):
+            line = line.strip()
+            if line and not line.startswith("#"):
+                return float(line.split()[0])
+    except OSError:
+        return None
+    return None
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+# Algorithmic bytes per particle of pass C (the dominant kernel): its own
+# records read once (pos 16 B, kin 16, aux 16, nb1..nb3 48, B^-1 16, flags 1)
+# and its outputs written once (drhodt 4, acc 8, avg 8, shift 8), FP32 records.
+PASS_C_BYTES_MIXED = 16 + 16 + 16 + 48 + 16 + 1 + 4 + 8 + 8 + 8
+PASS_C_BYTES_FP64 = 16 + 32 + 32 + 96 + 32 + 1 + 8 + 16 + 16 + 16
+
+
+def run_native(args, rank, world, local):
+    import torch
+    torch.cuda.set_device(local)
+    import sph_b200 as S
+    import build_lib as pkg_build
+    if rank == 0:
+        pkg_build.build()
+    if world > 1:
+        torch.distributed.barrier()
+    S.load()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+
+    n_side = args.n_side
+    results = {}
+    clocks_info = None
+    for prec in (S.PREC_MIXED, S.PREC_FP64):
+        case = S.make_tgv(n_side, solver=S.SOLVER_MUSCL_DELTA_SPS, precision=prec)
+        dt = S.baseline_dt(case.cfg)
+        sim = S.Simulation(case.cfg, case.n)
+        sim.set_state(case.pos, case.vel, case.rho, case.mass, case.type)
+        sim.time_iteration(args.warmup, dt)           # includes the 4-RHS first step
+        barrier()
+        sim.reset_timings()
+        clk = Clocks(local) if prec == S.PREC_MIXED else None
+        if clk:
+            clk.start()
+        barrier()
+        t0 = time.perf_counter()
+        diag = sim.time_iteration(args.steps, dt)
+        tm = sim.timings()
+        barrier()
+        wall = time.perf_counter() - t0
+        if clk:
+            clocks_info = clk.stop()
+        dev_ms = max_over_ranks(tm.total_ms)
+        results[prec] = dict(sim=sim, case=case, dt=dt, dev_ms=dev_ms, wall_s=wall, tm=tm, diag=diag)
+        if prec == S.PREC_FP64:
+            sim.close()
+
+    mixed = results[S.PREC_MIXED]
+    fp64 = results[S.PREC_FP64]
+    n = mixed["case"].n
+    steps = args.steps
+    value = world * n * steps / (mixed["dev_ms"] / 1e3)
+    value64 = world * n * steps / (fp64["dev_ms"] / 1e3)
+    tm = mixed["tm"]
+
+    # ---- e2e through the C-ABI with pinned host buffers ---------------------
+    sim = mixed["sim"]
+    pos_h = torch.empty(2 * n, dtype=torch.float64).pin_memory().numpy()
+    vel_h = torch.empty(2 * n, dtype=torch.float64).pin_memory().numpy()
+    rho_h = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
+    lib = S.load()
+    dp = ctypes.POINTER(ctypes.c_double)
+    P = lambda a: a.ctypes.data_as(dp)  # noqa: E731
+    rc = lib.sph_get_state(sim.h, n, P(pos_h), P(vel_h), P(rho_h), None)
+    assert rc == 0
+    e2e_steps = max(2, min(steps, 10))
+    diag = S.SphDiag()
+    barrier()
+    t0 = time.perf_counter()
+    launches0 = sim.timings().kernel_launches
+    for _ in range(e2e_steps):
+        assert lib.sph_update_state(sim.h, n, P(pos_h), P(vel_h), P(rho_h)) == 0
+        assert lib.sph_step(sim.h, 1, ctypes.c_double(mixed["dt"]), ctypes.byref(diag)) == 0
+        assert lib.sph_get_state(sim.h, n, P(pos_h), P(vel_h), P(rho_h), None) == 0
+    barrier()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_value = world * n * e2e_steps / e2e_s
+    h2d = 40 * n
+    d2h = 40 * n
+
+    # ---- accuracy: mixed vs FP64 on the jittered lattice ----------------------
+    accuracy = None
+    if not args.skip_accuracy and rank == 0:
+        acc_side = min(n_side, 1024)
+        acc_steps = 100
+        v = {}
+        for prec in (S.PREC_FP64, S.PREC_MIXED):
+            c = S.make_tgv(acc_side, solver=S.SOLVER_MUSCL_DELTA_SPS, precision=prec, jitter=0.1, seed=1)
+            with S.Simulation(c.cfg, c.n) as s2:
+                s2.set_state(c.pos, c.vel, c.rho, c.mass, c.type)
+                s2.time_iteration(acc_steps, S.baseline_dt(c.cfg))
+                v[prec] = s2.get_state()[1]
+        l2 = float(np.linalg.norm(v[S.PREC_MIXED] - v[S.PREC_FP64]) / np.linalg.norm(v[S.PREC_FP64]))
+        accuracy = {"velocity_l2_mixed_vs_fp64": l2, "steps": acc_steps,
+                    "case": f"TGV {acc_side}x{acc_side}, lattice jittered +-0.1dx (seed 1), same solver"}
+
+    # ---- roofline of the dominant kernel (pass C) ----------------------------
+    pk, pk_kind = peaks()
+    passc_ms = tm.pass_c_ms / max(tm.rhs_evaluations, 1)
+    n_tot = n + mixed["diag"].n_images
+    alg = PASS_C_BYTES_MIXED * n_tot
+    achieved = alg / (passc_ms / 1e3) / 1e9
+    tr = roofline_traffic()
+    roof = {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+            "frac": achieved / pk["hbm_gbs"], "traffic": (tr * n_tot if tr else None),
+            "kernel": "k_pass_c<float,MUSCL>", "launch_ms": passc_ms, "algorithmic_bytes": alg,
+            "peak_kind": pk_kind + " (burst copy)"}
+
+    # ---- CPU baseline (rank 0 only, N = 1) ----------------------------------
+    cpu = None
+    if rank == 0 and world == 1:
+        cpu = cpu_reference(steps=2, warmup=1)
+
+    mixed["sim"].close()
+    if rank != 0:
+        return None
+    return {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": mixed["dev_ms"] / steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 pair arithmetic + f64 state (mixed)", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "particles": n, "images": int(mixed["diag"].n_images),
+                   "rhs_per_step": 3, "dt": mixed["dt"], "precision": "mixed",
+                   "l2": "state (~1.4 GB) larger than L2 (126 MB), no flush needed",
+                   "parallelism": f"replicas x{world}"},
+        "fp64": {"value": value64, "unit": UNIT, "ms_per_step": fp64["dev_ms"] / steps,
+                 "mixed_over_fp64": value / value64},
+        "accuracy": accuracy,
+        "adjoint_over_forward": None,
+        "passes_ms_per_step": {
+            "images": tm.images_ms / steps, "sort_lists": tm.sort_ms / steps,
+            "pass_a": tm.pass_a_ms / steps, "surface": tm.surface_ms / steps,
+            "pass_c": tm.pass_c_ms / steps, "update": tm.update_ms / steps},
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "steps": e2e_steps, "api": "sph_update_state + sph_step(1) + sph_get_state, pinned host buffers"},
+        "gpu_launches": int(tm.kernel_launches),
+        "clocks": clocks_info,
+        "wall_s_timed": mixed["wall_s"],
+    }
+
+
+def cpu_reference(steps: int, warmup: int, n_side: int = 256):
+    """The oracle (CPU restatement of the reference, OpenMP) on a bounded sample:
+    the same solver and physics on a 256 x 256 lattice."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_api as O
+    import sph_b200 as S
+    O.build()
+    threads = O.threads(os.cpu_count() or 1)
+    case = S.make_tgv(n_side, solver=S.SOLVER_MUSCL_DELTA_SPS)
+    dt = S.baseline_dt(case.cfg)
+    sim = O.OracleSim(case.cfg, case.pos, case.vel, case.rho, case.mass, case.type)
+    sim.run(max(warmup, 1), dt)        # first step has 4 RHS: keep it out of the timing
+    t0 = time.perf_counter()
+    sim.run(steps, dt)
+    el = time.perf_counter() - t0
+    return {"value": case.n * steps / el, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"TGV {n_side}x{n_side} ({case.n} particles), {steps} steps after {max(warmup, 1)} warm-up, "
+                      f"same solver, FP64, {threads} OpenMP threads; per-particle cost is size-independent",
+            "seconds": el}
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        steps = max(1, min(args.steps, 4))
+        t0 = time.perf_counter()
+        cpu = cpu_reference(steps=steps, warmup=max(1, min(args.warmup, 2)))
+        el = time.perf_counter() - t0
+        line = {"metric": METRIC, "value": cpu["value"], "unit": UNIT, "n_gpus": world, "steps": steps,
+                "warmup": args.warmup, "ms_per_step": cpu["seconds"] / steps * 1e3, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+                "config": {"workload": WORKLOAD, "sample": cpu["sample"]},
+                "cpu_baseline": cpu,
+                "e2e": {"value": cpu["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                "wall_s": el}
+        print(json.dumps(line))
+        return 0
+    if world > 1:
+        import torch
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        torch.distributed.init_process_group("nccl", timeout=timedelta(seconds=120))
+    out = run_native(args, rank, world, local)
+    if world > 1:
+        import torch
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0 and out is not None:
+        print(json.dumps(out))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -112,6 +112,7 @@ typedef struct sph_diag {
 typedef struct sph_timings {
     double sort_ms, pass_a_ms, surface_ms, pass_c_ms, update_ms, images_ms, total_ms;
     long long rhs_evaluations, steps;
+    long long kernel_launches;  /* libsph_b200 kernels launched (library sort/scan calls not counted) */
 } sph_timings;
 
 typedef struct sph_handle sph_handle;
@@ -132,6 +133,13 @@ int sph_free(sph_handle* h);
 int sph_set_state(sph_handle* h, int n, const double* pos, const double* vel,
                   const double* rho, const double* mass, const int* type,
                   const double* sps_mass);
+
+/* Overwrite position, velocity and density of the n host particles between
+ * steps (the host's boundary / wave-maker modules own and may modify these
+ * arrays) while keeping the integrator history: the rates the next step reuses
+ * as K1 stay attached to their particles.  No reference counterpart: the
+ * Fortran host writes its module arrays directly. */
+int sph_update_state(sph_handle* h, int n, const double* pos, const double* vel, const double* rho);
 
 /* Download the host particles (same order as set_state).  press is the
  * equation of state evaluated at the returned density.  Any pointer may be NULL. */

@@ -1,6 +1,6 @@
 """Build libsph_b200.so in-tree with nvcc for sm_100a.
 
-Usage: python sph-2d_b200/build.py [--force]
+Usage: python sph-2d_b200/build_lib.py [--force]
 The shared library lands next to this file so it travels with the source tree.
 """
 from __future__ import annotations

@@ -1,5 +1,5 @@
 // sph_b200.cu -- libsph_b200: host orchestration and the C-ABI of
-// include/sph_b200.h.  Build: see sph-2d_b200/build.py (nvcc, sm_100a).
+// include/sph_b200.h.  Build: see sph-2d_b200/build_lib.py (nvcc, sm_100a).
 //
 // One handle = the device-resident particle state of one Fortran subdomain
 // (now the whole domain: the MPI decomposition of Devide_block_and_send_tasks
@@ -96,6 +96,7 @@ struct sph_handle {
     double t_ms[PH_COUNT] = {0};
     double t_total = 0;
     long long n_rhs = 0, n_steps = 0;
+    long long launches = 0;
 };
 
 namespace {
@@ -261,6 +262,7 @@ int unsort(sph_handle* h) {
     Params P = h->P;
     k_unsort<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, h->S, sorted<R>(h));
     CK(cudaGetLastError());
+    h->launches += 1;
     h->staging_valid = true;
     return SPH_OK;
 }
@@ -310,6 +312,7 @@ int prepare(sph_handle* h) {
         CK(cudaGetLastError());
     }
     h->n_img = n_img;
+    h->launches += h->cfg.periodic ? 5 : 0;
     P.n_tot = h->n_host + n_img;
     tic(h, PH_SORT);
     Sorted<R>& D = sorted<R>(h);
@@ -326,6 +329,7 @@ int prepare(sph_handle* h) {
     k_build_lists<R><<<blocks(P.n_tot, 128), 128, 0, h->stream>>>(P, D, h->d_status);
     k_records<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, D);
     CK(cudaGetLastError());
+    h->launches += 5;
     h->sorted_valid = true;
     h->staging_valid = false;   // the master state now lives in the sorted arrays
     return SPH_OK;
@@ -346,6 +350,7 @@ int rhs(sph_handle* h, int last) {
     if (P.muscl) k_pass_c<R, true><<<nb, 128, 0, h->stream>>>(P, D, last);
     else k_pass_c<R, false><<<nb, 128, 0, h->stream>>>(P, D, last);
     CK(cudaGetLastError());
+    h->launches += 4;
     h->n_rhs++;
     h->have_rhs = true;
     return SPH_OK;
@@ -358,6 +363,7 @@ int stage(sph_handle* h, int st, double dt, int use_carried, int do_shift) {
     k_stage<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, sorted<R>(h), st, dt, use_carried, do_shift,
                                                              h->d_status);
     CK(cudaGetLastError());
+    h->launches += 1;
     return SPH_OK;
 }
 
@@ -406,6 +412,7 @@ int diagnostics(sph_handle* h, sph_diag* out) {
     k_diag_final<<<1, kRedThreads, 0, h->stream>>>(nparts, h->d_part, h->d_part + nparts, h->d_diag);
     CK(cudaMemsetAsync(h->d_int, 0, sizeof(int), h->stream));
     k_count_surface<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, sorted<R>(h), h->d_int);
+    h->launches += 3;
     double v[2];
     int nsurf = 0;
     CK(cudaMemcpyAsync(v, h->d_diag, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
@@ -556,11 +563,13 @@ int get_state_impl(sph_handle* h, int n, double* pos, double* vel, double* rho, 
     if (rc) return rc;
     if (pos) {
         k_deinterleave<<<blocks(n, 256), 256, 0, h->stream>>>(n, h->S.pos, h->d_xfer);
+        h->launches += 1;
         CK(cudaMemcpyAsync(pos, h->d_xfer, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
     }
     if (vel) {
         k_deinterleave<<<blocks(n, 256), 256, 0, h->stream>>>(n, h->S.vel, h->d_xfer);
+        h->launches += 1;
         CK(cudaMemcpyAsync(vel, h->d_xfer, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
     }
@@ -630,6 +639,23 @@ int sph_set_state(sph_handle* h, int n, const double* pos, const double* vel, co
     h->sorted_valid = false;
     h->have_rhs = false;
     h->step_count = 0;
+    return SPH_OK;
+}
+
+int sph_update_state(sph_handle* h, int n, const double* pos, const double* vel, const double* rho) {
+    if (!h || n != h->n_host || n <= 0 || !pos || !vel || !rho) return SPH_E_ARG;
+    CK(cudaSetDevice(h->device));
+    int rc = h->mixed ? unsort<float>(h) : unsort<double>(h);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(h->d_xfer, pos, sizeof(double) * 2 * n, cudaMemcpyHostToDevice, h->stream));
+    k_interleave<<<blocks(n, 256), 256, 0, h->stream>>>(n, h->d_xfer, h->S.pos);
+    CK(cudaMemcpyAsync(h->d_xfer + 2 * (size_t)n, vel, sizeof(double) * 2 * n, cudaMemcpyHostToDevice, h->stream));
+    k_interleave<<<blocks(n, 256), 256, 0, h->stream>>>(n, h->d_xfer + 2 * (size_t)n, h->S.vel);
+    CK(cudaMemcpyAsync(h->S.rho, rho, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaGetLastError());
+    h->launches += 2;
+    h->staging_valid = true;
+    h->sorted_valid = false;
     return SPH_OK;
 }
 
@@ -724,6 +750,7 @@ int sph_get_timings(sph_handle* h, sph_timings* out) {
     out->total_ms = h->t_total;
     out->rhs_evaluations = h->n_rhs;
     out->steps = h->n_steps;
+    out->kernel_launches = h->launches;
     return SPH_OK;
 }
 
@@ -734,6 +761,7 @@ int sph_reset_timings(sph_handle* h) {
     h->t_total = 0;
     h->n_rhs = 0;
     h->n_steps = 0;
+    h->launches = 0;
     return SPH_OK;
 }
 

@@ -49,7 +49,7 @@ TYPE_ILL = 120
 EXPORTED_SYMBOLS = (
     "sph_init", "sph_free", "sph_set_state", "sph_get_state", "sph_find_particle_pair",
     "sph_rhs", "sph_step", "sph_diagnostics", "sph_get_timings", "sph_reset_timings",
-    "sph_strerror", "sph_get_field",
+    "sph_strerror", "sph_get_field", "sph_update_state",
 )
 
 
@@ -88,6 +88,7 @@ class SphTimings(ctypes.Structure):
         ("sort_ms", ctypes.c_double), ("pass_a_ms", ctypes.c_double), ("surface_ms", ctypes.c_double),
         ("pass_c_ms", ctypes.c_double), ("update_ms", ctypes.c_double), ("images_ms", ctypes.c_double),
         ("total_ms", ctypes.c_double), ("rhs_evaluations", ctypes.c_longlong), ("steps", ctypes.c_longlong),
+        ("kernel_launches", ctypes.c_longlong),
     ]
 
 
@@ -157,8 +158,12 @@ def tgv_baseline_config(n_side: int, solver: int = SOLVER_MUSCL_DELTA_SPS,
 
 
 def baseline_dt(cfg: SphConfig) -> float:
-    """CFL time step dt = 0.25 h / c0 of the benchmark case."""
-    return 0.25 * cfg.h / math.sqrt(cfg.c0sq)
+    """Time step of the benchmark case: the acoustic CFL dt = 0.25 h / c0, limited by
+    the viscous (Morris) criterion 0.125 h^2 / nu the reference combines it with
+    (Taylor_Green_Vortex/Initialize_SPH_Calculation.f90:452-463, there with a fixed
+    water viscosity).  At 2048^2 and Re = 100 the acoustic step alone gives
+    nu dt / h^2 = 0.39, outside the explicit stability range of the Laplacian."""
+    return min(0.25 * cfg.h / math.sqrt(cfg.c0sq), 0.125 * cfg.h * cfg.h / cfg.nu)
 
 
 def tgv_lattice(n_side: int, U: float = 1.0, rho0: float = 1.0, c0sq: float = 100.0,
@@ -228,6 +233,7 @@ def load(path: str = LIB_PATH):
     lib.sph_free.argtypes = [P]
     lib.sph_set_state.argtypes = [P, ctypes.c_int, dp, dp, dp, dp, ip, dp]
     lib.sph_get_state.argtypes = [P, ctypes.c_int, dp, dp, dp, dp]
+    lib.sph_update_state.argtypes = [P, ctypes.c_int, dp, dp, dp]
     lib.sph_find_particle_pair.argtypes = [P, ctypes.c_longlong, ip, ip, dp, dp, ctypes.POINTER(ctypes.c_longlong)]
     lib.sph_rhs.argtypes = [P, dp, dp, dp, ip, ip]
     lib.sph_step.argtypes = [P, ctypes.c_int, ctypes.c_double, ctypes.POINTER(SphDiag)]
@@ -302,6 +308,13 @@ class Simulation:
         _check(self.lib.sph_set_state(self.h, n, _ptr(pos), _ptr(vel), _ptr(rho), _ptr(mass),
                                       _ptr(type_, ctypes.c_int), _ptr(sm)), "sph_set_state")
         self.n = n
+
+    def update_state(self, pos, vel, rho):
+        """Host-side edit of x, v, rho between steps; keeps the K1 rates."""
+        n = self.n
+        _check(self.lib.sph_update_state(self.h, n, _ptr(np.ascontiguousarray(pos, np.float64)),
+                                         _ptr(np.ascontiguousarray(vel, np.float64)),
+                                         _ptr(np.ascontiguousarray(rho, np.float64))), "sph_update_state")
 
     def get_state(self):
         n = self.n

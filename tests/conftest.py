@@ -27,7 +27,7 @@ def lib():
     """The CUDA library; GPU tests fail (not skip) if it cannot be built or loaded."""
     if not _have_gpu():
         pytest.skip("no CUDA device")
-    import build as pkg_build
+    import build_lib as pkg_build
     pkg_build.build()
     import sph_b200
     return sph_b200.load()

@@ -22,7 +22,7 @@ def declared_functions():
 
 @pytest.fixture(scope="module")
 def built_lib():
-    import build as pkg_build
+    import build_lib as pkg_build
     pkg_build.build()
     return ctypes.CDLL(S.LIB_PATH)
 

@@ -72,8 +72,8 @@ def test_pair_capacity_error(lib):
 RHS_CASES = [
     ("reference", dict(n_side=60, reference=True)),
     ("reference-jitter", dict(n_side=60, reference=True, jitter=0.1, seed=5)),
-    ("muscl", dict(n_side=64, solver=S.SOLVER_MUSCL_DELTA_SPS)),
-    ("muscl-jitter", dict(n_side=64, solver=S.SOLVER_MUSCL_DELTA_SPS, jitter=0.1, seed=1)),
+    ("muscl-jitter-1", dict(n_side=64, solver=S.SOLVER_MUSCL_DELTA_SPS, jitter=0.1, seed=1)),
+    ("muscl-jitter-2", dict(n_side=50, solver=S.SOLVER_MUSCL_DELTA_SPS, jitter=0.05, seed=9)),
     ("modlr-renorm-jitter", dict(n_side=64, solver=S.SOLVER_MODLR_DELTA_SPS, jitter=0.1, seed=2)),
 ]
 
@@ -100,18 +100,23 @@ def test_rhs_fp64_parity(lib, oracle, name, kw):
     assert np.array_equal(got["fs"], ref["fs"][:n])
     assert np.array_equal(got["near"], ref["near"][:n])
     assert relerr(fra, ref["fra_v"][:n]) < 1e-12
-    for c in range(4):
-        assert relerr(binv[c * n:(c + 1) * n], ref["binv"][c * m:c * m + n]) < 1e-10
-    for c in range(3):
-        assert relerr(tau[c * n:(c + 1) * n], ref["tau"][c * m:c * m + n]) < 1e-10, c
-    nf = 8 if case.cfg.solver == S.SOLVER_MUSCL_DELTA_SPS else 2
-    for c in range(nf):
-        assert relerr(grads[c * n:(c + 1) * n], ref["grads"][c * m:c * m + n]) < 1e-10, c
+    # tensors and gradient vectors are compared against the scale of the whole
+    # tensor / vector: single components can vanish analytically (the lattice
+    # Taylor-Green field has S_xy = 0), leaving round-off on both sides
+    def host_blocks(arr, k):
+        return np.concatenate([arr[c * m:c * m + n] for c in k])
+    assert relerr(binv, host_blocks(ref["binv"], range(4))) < 1e-10
+    assert relerr(tau, host_blocks(ref["tau"], range(3))) < 1e-10
+    nf = 4 if case.cfg.solver == S.SOLVER_MUSCL_DELTA_SPS else 1
+    for f in range(nf):
+        got_f = grads[2 * f * n:(2 * f + 2) * n]
+        assert relerr(got_f, host_blocks(ref["grads"], (2 * f, 2 * f + 1))) < 1e-10, f
 
 
 STEP_CASES = [
     ("reference-100", dict(n_side=100, reference=True), 5, 1e-4),
-    ("muscl-48", dict(n_side=48, solver=S.SOLVER_MUSCL_DELTA_SPS), 10, None),
+    ("muscl-48-jitter", dict(n_side=48, solver=S.SOLVER_MUSCL_DELTA_SPS, jitter=0.1, seed=3), 10, None),
+    ("modlr-48-lattice", dict(n_side=48, solver=S.SOLVER_MODLR_DELTA_SPS), 10, None),
     ("modlr-48-jitter", dict(n_side=48, solver=S.SOLVER_MODLR_DELTA_SPS, jitter=0.1, seed=4), 10, None),
 ]
 
@@ -138,7 +143,7 @@ def test_time_iteration_fp64_parity(lib, oracle, name, kw, nsteps, dt):
 
 def test_steps_split_equal_single_call(lib):
     """sph_step(2) == sph_step(1); sph_step(1): the carried K1 rates survive calls."""
-    case = S.make_tgv(40, solver=S.SOLVER_MUSCL_DELTA_SPS)
+    case = S.make_tgv(40, solver=S.SOLVER_MUSCL_DELTA_SPS, jitter=0.1, seed=2)
     dt = S.baseline_dt(case.cfg)
     out = []
     for split in (False, True):
@@ -155,10 +160,12 @@ def test_steps_split_equal_single_call(lib):
 
 
 def test_mixed_precision_velocity_error(lib):
-    """FP32 pair arithmetic with compensated sums: velocity L2 error vs the FP64 GPU step."""
+    """FP32 pair arithmetic with compensated sums: velocity L2 error vs the FP64 GPU
+    step, on the jittered lattice (an exact lattice puts the MUSCL limiter on
+    branch ties that round-off decides; see test_oracle.py)."""
     res = {}
     for prec in (S.PREC_FP64, S.PREC_MIXED):
-        case = S.make_tgv(128, solver=S.SOLVER_MUSCL_DELTA_SPS, precision=prec)
+        case = S.make_tgv(128, solver=S.SOLVER_MUSCL_DELTA_SPS, precision=prec, jitter=0.1, seed=11)
         dt = S.baseline_dt(case.cfg)
         with S.Simulation(case.cfg, case.n) as sim:
             sim.set_state(case.pos, case.vel, case.rho, case.mass, case.type)
