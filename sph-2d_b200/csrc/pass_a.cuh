@@ -21,7 +21,7 @@ namespace sph {
 template <typename R>
 __global__ void __launch_bounds__(128) k_pass_a(Params P, Sorted<R> D) {
     using V4 = typename VT<R>::V4;
-    using A = typename Acc<R>::T;
+    constexpr bool F32 = sizeof(R) == 4;
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= P.n_tot) return;
     const int ta = D.type[a];
@@ -29,46 +29,69 @@ __global__ void __launch_bounds__(128) k_pass_a(Params P, Sorted<R> D) {
     const double2 xa = D.pos[a];
     const V4 ka = D.kin[a];
     const R rho_a = Dens<R>::rho(ka.z, P.rho0);
-    A fra, b00, b01, b10, b11, g[8];
-    fra.init(); b00.init(); b01.init(); b10.init(); b11.init();
-    for (int c = 0; c < 8; ++c) g[c].init();
-    const R inv_sv = (R)(1.0 / P.sv);
+    // the sums of this pass have no large cancellation (differences of smooth
+    // fields, or B ~ I), so FP32 accumulates them directly in the mixed path
+    R fra = R(0), b00 = R(0), b01 = R(0), b10 = R(0), b11 = R(0);
+    R g[8];
+    for (int c = 0; c < 8; ++c) g[c] = R(0);
+    const R inv_h = (R)(1.0 / P.h);
+    const R r2cut = (R)(P.r_cut * P.r_cut), r2min = (R)(P.cut_min * P.cut_min);
     for (int e = 0; e < nn; ++e) {
         const unsigned ent = __ldg(&D.nbr[(size_t)e * P.nbr_stride + a]);
         const int b = (int)(ent & 0x7fffffffu);
         const double2 xb = __ldg(&D.pos[b]);
         const double dxd = xa.x - xb.x, dyd = xa.y - xb.y;
-        double dd;
-        if (!in_support(P, dxd, dyd, dd)) continue;
-        const R d = (R)dd, dx = (R)dxd, dy = (R)dyd;
-        R w, gx, gy;
-        kernel_w_dw<R>(P, d, dx, dy, w, gx, gy);
+        R d, inv_d;
+        if (F32) {
+            const R s = (R)(dxd * dxd + dyd * dyd);
+            if (!(s <= r2cut) || s < r2min) continue;
+            inv_d = rsqrtf(s);
+            d = s * inv_d;
+        } else {
+            double dd;
+            if (!in_support(P, dxd, dyd, dd)) continue;
+            d = (R)dd;
+            inv_d = R(1) / d;
+        }
+        const R dx = (R)dxd, dy = (R)dyd;
+        // grad_a W = g(d) (x_a - x_b)  (compute_kernel)
+        R gs;
+        {
+            const R q = d * inv_h;
+            const R kf = (R)P.kfactor;
+            if (P.kernel_model == SPH_KERNEL_GAUSSIAN) {
+                gs = exp(-(q * q)) * (R(-2) * q) * inv_d * inv_h * kf;
+            } else {
+                const R t = R(1) - R(0.5) * q;
+                gs = kf * (R(-5) * q * (t * t * t)) * inv_d * inv_h;
+            }
+        }
         const V4 kb = D.kin[b];
         const R Vb = D.aux[b].y;
-        // volume fraction (:84-85)
-        if (sizeof(R) == 8) fra.add(Vb / (R)P.sv); else fra.add(Vb * inv_sv);
+        const R gx = gs * dx * Vb, gy = gs * dy * Vb;    // V_b grad_a W
+        // volume fraction (Define_freesurface...f90:84-85)
+        fra += Vb;
         // B(l,o) += (x_b - x_a)_l grad_a W_o V_b (:151-152)
-        b00.add(-dx * gx * Vb); b01.add(-dx * gy * Vb);
-        b10.add(-dy * gx * Vb); b11.add(-dy * gy * Vb);
+        b00 -= dx * gx; b01 -= dx * gy;
+        b10 -= dy * gx; b11 -= dy * gy;
         // raw gradient sums (phi_b - phi_a) V_b grad_a W
-        const R drho = Dens<R>::rho(kb.z, P.rho0) - rho_a;
-        const R drho_m = sizeof(R) == 8 ? drho : (kb.z - ka.z);
-        const R t0 = drho_m * Vb;
-        g[0].add(t0 * gx); g[1].add(t0 * gy);
-        const R tu = (kb.x - ka.x) * Vb, tv = (kb.y - ka.y) * Vb;
-        g[4].add(tu * gx); g[5].add(tu * gy);
-        g[6].add(tv * gx); g[7].add(tv * gy);
+        const R drho = F32 ? (kb.z - ka.z) : (Dens<R>::rho(kb.z, P.rho0) - rho_a);
+        g[0] += drho * gx; g[1] += drho * gy;
+        const R du = kb.x - ka.x, dv = kb.y - ka.y;
+        g[4] += du * gx; g[5] += du * gy;
+        g[6] += dv * gx; g[7] += dv * gy;
         if (P.muscl) {
-            const R tp = (kb.w - ka.w) * Vb;
-            g[2].add(tp * gx); g[3].add(tp * gy);
+            const R dp = kb.w - ka.w;
+            g[2] += dp * gx; g[3] += dp * gy;
         }
     }
+    fra = fra * (R)(1.0 / P.sv);
     // inverse of the 2x2 tensor in FP64 (matrix_inversion_less_three,
     // function_module.f90:190-204); the reference keeps the identity on success
     // (Define_freesurface...f90:180-186) unless renormalisation is switched on.
     double i00 = 1.0, i01 = 0.0, i10 = 0.0, i11 = 1.0;
     if (ta == SPH_TYPE_WATER && P.renorm) {
-        double a1 = (double)b00.val(), bb1 = (double)b01.val(), a2 = (double)b10.val(), bb2 = (double)b11.val();
+        double a1 = (double)b00, bb1 = (double)b01, a2 = (double)b10, bb2 = (double)b11;
         double det = (a1 * bb2 - bb1 * a2);
         if (det != 0) { i00 = bb2 / det; i01 = -bb1 / det; i10 = -a2 / det; i11 = a1 / det; }
     }
@@ -76,7 +99,7 @@ __global__ void __launch_bounds__(128) k_pass_a(Params P, Sorted<R> D) {
     D.binv[a] = mk4<R>(m00, m01, m10, m11);
     R gr[8];
     for (int f = 0; f < 4; ++f) {
-        R x = g[2 * f].val(), y = g[2 * f + 1].val();
+        R x = g[2 * f], y = g[2 * f + 1];
         gr[2 * f] = m00 * x + m01 * y;
         gr[2 * f + 1] = m10 * x + m11 * y;
     }
@@ -98,7 +121,7 @@ __global__ void __launch_bounds__(128) k_pass_a(Params P, Sorted<R> D) {
     D.nb1[a] = mk4<R>(txx, txy, tyy, gr[0]);
     D.nb2[a] = mk4<R>(gr[1], gr[2], gr[3], gr[4]);
     D.nb3[a] = mk4<R>(gr[5], gr[6], gr[7], R(0));
-    const R fv = fra.val();
+    const R fv = fra;
     D.fra_v[a] = fv;
     uint8_t fl = 0;
     if (ta == SPH_TYPE_WATER && (double)fv <= P.fs_thr) fl = 4;   // surface candidate (:123)

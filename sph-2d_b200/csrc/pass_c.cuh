@@ -13,9 +13,18 @@
 //
 // Every pair quantity is evaluated in the reference's own orientation
 // (pair_i = the particle with the lower id, bit 31 of the list entry), so the
-// flux seen by the two particles of a pair is computed by the identical
-// sequence of operations the Fortran uses; each thread then keeps the
-// pair_i or pair_j contribution that belongs to its particle.
+// flux seen by the two particles of a pair is computed by the same sequence
+// of operations; each thread then keeps the pair_i or pair_j contribution that
+// belongs to its particle.  The physical terms are summed per pair and then
+// accumulated (the reference sums each term over all pairs first); the two
+// orders agree to round-off.
+//
+// Precision: R = double is the FP64 path.  R = float is the mixed path: FP32
+// pair arithmetic with reciprocal/rsqrt instead of divisions, compensated
+// (TwoSum) sums for the acceleration and the density rate, and the shifting
+// sum in FP64 (its terms are O(h/10) each and cancel to a displacement that
+// is orders of magnitude smaller, so FP32 rounding there would inject position
+// noise every step into the unstable lattice modes the shifting excites).
 #pragma once
 #include "pass_a.cuh"
 
@@ -41,7 +50,10 @@ __device__ __forceinline__ void muscl_limiter(R di, R dj, R dij, R& li, R& lj) {
     }
 }
 
-// Per-particle state a thread needs for "its" side of a pair.
+__device__ __forceinline__ double rcp(double x) { return 1.0 / x; }
+__device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
+
+// Per-particle state a thread needs for one side of a pair.
 template <typename R>
 struct Side {
     using V4 = typename VT<R>::V4;
@@ -52,10 +64,10 @@ struct Side {
 };
 
 template <typename R, bool MUSCL>
-__global__ void __launch_bounds__(128) k_pass_c(Params P, Sorted<R> D, int last_rhs) {
+__global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_pass_c(Params P, Sorted<R> D, int last_rhs) {
     using V4 = typename VT<R>::V4;
-    using V2 = typename VT<R>::V2;
     using A = typename Acc<R>::T;
+    constexpr bool F32 = sizeof(R) == 4;
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= P.n_tot) return;
     const int ta = D.type[a];
@@ -69,17 +81,22 @@ __global__ void __launch_bounds__(128) k_pass_c(Params P, Sorted<R> D, int last_
     const bool near_a = (D.flags[a] & 2) != 0;
 
     const R hbar = (R)P.h;
-    const R sqc0 = (R)P.sqrt_c0;
-    const R nu = (R)P.nu, alpha = (R)P.alpha, beta = (R)P.beta, fai = (R)P.fai;
-    const R dlt = (R)P.delta, dla = (R)P.delta_alpha, rho0 = (R)P.rho0, eps = (R)P.eps;
-    const R wdx_inv = (R)(1.0 / P.w_dx);
-    const R shf = (R)(P.shift_beta * (P.h * P.h));
-    const R shR = (R)P.shift_R;
+    const R inv_h = (R)(1.0 / P.h);
+    const R sqc0 = (R)P.sqrt_c0, inv_sqc0 = (R)(1.0 / P.sqrt_c0);
+    const R nu2 = (R)(2.0 * P.nu), alpha = (R)P.alpha, beta = (R)P.beta;
+    const R fh2 = (R)((P.fai * P.h) * (P.fai * P.h));
+    const R dlt2h = (R)(2.0 * P.delta * P.h);
+    const R dla_h = (R)(P.delta_alpha * P.h);
+    const R eps2 = (R)(2.0 * P.eps);
+    const R inv_rho_a = rcp(S.rho);
+    const R rho0_over_rho_a = (R)P.rho0 * inv_rho_a;
+    const R r2cut = (R)(P.r_cut * P.r_cut);
+    const bool water = ta == SPH_TYPE_WATER;   // delta-SPH only enters water rates (Solver :627-635)
 
-    // accumulators: continuity, delta-SPH, internal, AV, laplacian, art. internal, SPS, XSPH, shift
-    A cont, corr, ix, iy, avx, avy, lpx, lpy, arx, ary, spx, spy, xsx, xsy, shx, shy;
-    cont.init(); corr.init(); ix.init(); iy.init(); avx.init(); avy.init(); lpx.init(); lpy.init();
-    arx.init(); ary.init(); spx.init(); spy.init(); xsx.init(); xsy.init(); shx.init(); shy.init();
+    A cont, accx, accy;
+    cont.init(); accx.init(); accy.init();
+    R xsx = R(0), xsy = R(0);
+    double shx = 0.0, shy = 0.0;   // shifting sum, FP64 in both paths
 
     for (int e = 0; e < nn; ++e) {
         const unsigned ent = __ldg(&D.nbr[(size_t)e * P.nbr_stride + a]);
@@ -87,43 +104,68 @@ __global__ void __launch_bounds__(128) k_pass_c(Params P, Sorted<R> D, int last_
         const bool a_is_i = (ent >> 31) != 0;
         const double2 xb = __ldg(&D.pos[b]);
         const double dxd = xa.x - xb.x, dyd = xa.y - xb.y;
-        double dd;
-        if (!in_support(P, dxd, dyd, dd)) continue;
+        R d, inv_d;
+        double dd = 0.0;
+        if (F32) {
+            // the mixed path does not need the reference's exact sqrt test: a
+            // pair within one ulp of the support radius has W = grad W = 0
+            const R s = (R)(dxd * dxd + dyd * dyd);
+            if (!(s <= r2cut) || s < (R)(P.cut_min * P.cut_min)) continue;
+            inv_d = rsqrtf(s);
+            d = s * inv_d;
+        } else {
+            if (!in_support(P, dxd, dyd, dd)) continue;
+            d = (R)dd;
+            inv_d = R(1) / d;
+        }
         Side<R> T;
         T.kin = D.kin[b]; T.aux = D.aux[b]; T.nb1 = D.nb1[b]; T.nb2 = D.nb2[b];
         if (MUSCL) T.nb3 = D.nb3[b];
         T.rho = Dens<R>::rho(T.kin.z, P.rho0);
-        // canonical orientation: I = pair_i, J = pair_j
         const Side<R>& I = a_is_i ? S : T;
         const Side<R>& J = a_is_i ? T : S;
-        const R sgn = a_is_i ? R(1) : R(-1);
-        // position_difference_ij = x_i - x_j, distance, w, dwdx (find_particle_pair.f90:79-107)
+        // position_difference_ij = x_i - x_j (find_particle_pair.f90:79-107)
         const R xij0 = (R)(a_is_i ? dxd : -dxd), xij1 = (R)(a_is_i ? dyd : -dyd);
-        const R d = (R)dd;
-        R w, dw0, dw1;
-        kernel_w_dw<R>(P, d, xij0, xij1, w, dw0, dw1);
+        // compute_kernel: W and dwdx(k) = grad_i W (x_i - x_j)
+        R w, g;
+        {
+            const R q = d * inv_h;
+            const R kf = (R)P.kfactor;
+            if (P.kernel_model == SPH_KERNEL_GAUSSIAN) {
+                const R ex = exp(-(q * q));
+                w = (ex - (R)P.gauss_e9) * kf;
+                g = ex * (R(-2) * q) * inv_d * inv_h * kf;
+            } else {
+                const R t = R(1) - R(0.5) * q;
+                const R t3 = t * t * t;
+                w = kf * (R(1) + R(2) * q) * (t3 * t);
+                g = kf * (R(-5) * q * t3) * inv_d * inv_h;
+            }
+        }
+        const R dw0 = g * xij0, dw1 = g * xij1;
         // Normalized_dwdx of this particle's side: B_a^-1 dwdx(k)
         const R nd0 = bi.x * dw0 + bi.y * dw1;
         const R nd1 = bi.z * dw0 + bi.w * dw1;
-        const R cbar = (I.aux.z + J.aux.z) / R(2);
-        const R rbar = (I.rho + J.rho) / R(2);
+        const R cbar = R(0.5) * (I.aux.z + J.aux.z);
+        const R rbar = R(0.5) * (I.rho + J.rho);
+        const R inv_rbar = rcp(rbar);
         const R ui = I.kin.x, vi = I.kin.y, uj = J.kin.x, vj = J.kin.y;
         const R pi_ = I.kin.w, pj_ = J.kin.w;
         R PL, PR, Pbar, vI0, vI1, vJ0, vJ1, vb0, vb1, e0, e1;
         if (!MUSCL) {
-            PL = pi_; PR = pj_; Pbar = (PL + PR) / R(2);
+            PL = pi_; PR = pj_; Pbar = R(0.5) * (PL + PR);
             vI0 = ui; vI1 = vi; vJ0 = uj; vJ1 = vj;
-            vb0 = (vI0 + vJ0) / R(2); vb1 = (vI1 + vJ1) / R(2);
-            e0 = -xij0 / d; e1 = -xij1 / d;
+            vb0 = R(0.5) * (vI0 + vJ0); vb1 = R(0.5) * (vI1 + vJ1);
+            e0 = -xij0 * inv_d; e1 = -xij1 * inv_d;
         } else {
             const R x0 = -xij0, x1 = -xij1;          // j - i
-            e0 = x0 / d; e1 = x1 / d;
+            e0 = x0 * inv_d; e1 = x1 * inv_d;
             R li, lj;
-            // I.nb2 = (grad rho y, grad p x, grad p y, grad u x), I.nb3 = (grad u y, grad v x, grad v y, 0)
+            // nb2 = (grad rho y, grad p x, grad p y, grad u x), nb3 = (grad u y, grad v x, grad v y, 0)
             R Di = R(0.5) * (I.nb2.y * x0 + I.nb2.z * x1);
             R Dj = R(-0.5) * (J.nb2.y * x0 + J.nb2.z * x1);
             muscl_limiter<R>(Di, Dj, pj_ - pi_, li, lj);
-            PL = pi_ + li; PR = pj_ - lj; Pbar = (pi_ + pj_) / R(2);
+            PL = pi_ + li; PR = pj_ - lj; Pbar = R(0.5) * (pi_ + pj_);
             const R vd0 = -(ui - uj), vd1 = -(vi - vj);
             Di = R(0.5) * (I.nb2.w * x0 + I.nb3.x * x1);
             Dj = R(-0.5) * (J.nb2.w * x0 + J.nb3.x * x1);
@@ -133,12 +175,12 @@ __global__ void __launch_bounds__(128) k_pass_c(Params P, Sorted<R> D, int last_
             Dj = R(-0.5) * (J.nb3.y * x0 + J.nb3.z * x1);
             muscl_limiter<R>(Di, Dj, vd1, li, lj);
             vI1 = vi + li; vJ1 = vj - lj;
-            vb0 = (ui + uj) / R(2); vb1 = (vi + vj) / R(2);
+            vb0 = R(0.5) * (ui + uj); vb1 = R(0.5) * (vi + vj);
         }
         const R UL = vI0 * e0 + vI1 * e1;
         const R UR = vJ0 * e0 + vJ1 * e1;
-        const R Ubar = (UL + UR) / R(2);
-        const R Us = Ubar + R(0.5) * (PL - PR) / (rbar * sqc0);
+        const R Ubar = R(0.5) * (UL + UR);
+        const R Us = Ubar + R(0.5) * (PL - PR) * (inv_rbar * inv_sqc0);
         const R vs0 = (Us - Ubar) * e0 + vb0, vs1 = (Us - Ubar) * e1 + vb1;
         const R bR = min(R(3) * (max((UL - UR), R(0))), cbar);
         const R Ps = Pbar + R(0.5) * bR * rbar * (UL - UR);
@@ -146,77 +188,98 @@ __global__ void __launch_bounds__(128) k_pass_c(Params P, Sorted<R> D, int last_
         const R vA0 = near_a ? vb0 : vs0, vA1 = near_a ? vb1 : vs1, PA = near_a ? Pbar : Ps;
         const R va0 = a_is_i ? vI0 : vJ0, va1 = a_is_i ? vI1 : vJ1;
         const R Vb = T.aux.y, mb = T.aux.x;
+        const R sgn = a_is_i ? R(1) : R(-1);
         // continuity (:360-369)
         R tm = (va0 - vA0) * nd0 + (va1 - vA1) * nd1;
         if (!a_is_i) tm = -tm;
-        cont.add(R(2) * S.rho * Vb * tm);
+        R dr = R(2) * S.rho * Vb * tm;
         // pressure force (:374-388)
-        const R rho_ij = R(1) / (I.rho * J.rho);
-        ix.add(sgn * (mb * (R(-2) * PA * nd0 * rho_ij)));
-        iy.add(sgn * (mb * (R(-2) * PA * nd1 * rho_ij)));
+        const R rho_ij = inv_rho_a * rcp(T.rho);
+        const R fp = R(-2) * PA * rho_ij * mb;
+        R tx = fp * nd0, ty = fp * nd1;
         // artificial viscosity (:392-417)
         const R vij0 = ui - uj, vij1 = vi - vj;
-        const R r2 = xij0 * xij0 + xij1 * xij1;
+        const R inv_r2 = inv_d * inv_d;
         const R vx = vij0 * xij0 + vij1 * xij1;
         if (vx < R(0)) {
-            const R fh = fai * hbar;
-            const R phi1 = hbar * vx / (r2 + fh * fh);
-            const R Pi = (-alpha * cbar * phi1 + beta * (phi1 * phi1)) / rbar;
-            avx.add(sgn * (mb * (-Pi * nd0)));
-            avy.add(sgn * (mb * (-Pi * nd1)));
+            const R phi1 = hbar * vx / (d * d + fh2);
+            const R Pi = (-alpha * cbar * phi1 + beta * (phi1 * phi1)) * inv_rbar;
+            tx += mb * (-Pi * nd0);
+            ty += mb * (-Pi * nd1);
         }
         // Morris laplacian (:432-436)
-        const R rd = xij0 * nd0 + xij1 * nd1;
-        const R lf = Vb * R(2) * nu * rd / r2;
-        lpx.add(sgn * (lf * vij0));
-        lpy.add(sgn * (lf * vij1));
+        const R lf = Vb * nu2 * (xij0 * nd0 + xij1 * nd1) * inv_r2;
+        tx += lf * vij0;
+        ty += lf * vij1;
         // delta-alpha artificial internal acceleration (:442-446)
-        const R tt = dla * hbar * cbar * vx / r2;
-        arx.add(sgn * (tt * nd0 * rho0 / S.rho * Vb));
-        ary.add(sgn * (tt * nd1 * rho0 / S.rho * Vb));
-        // SPS force, unnormalised dwdx and the neighbour's SPS mass (:450-492)
+        const R tt = dla_h * cbar * vx * inv_r2 * rho0_over_rho_a * Vb;
+        tx += tt * nd0;
+        ty += tt * nd1;
+        // SPS force, unnormalised dwdx and the neighbour's SPS mass (:450-492);
+        // the reference does not reset temp_p between x and y (kept with quirks)
         const R sxx = I.nb1.x + J.nb1.x, sxy = I.nb1.y + J.nb1.y, syy = I.nb1.z + J.nb1.z;
         R tp = (sxx * dw0 + sxy * dw1) * rho_ij;
         const R smb = T.aux.w;
-        spx.add(sgn * (smb * tp));
+        tx += smb * tp;
         if (!P.quirks) tp = R(0);
         tp = (tp + syy * dw1 + sxy * dw0) * rho_ij;
-        spy.add(sgn * (smb * tp));
+        ty += smb * tp;
+        accx.add(sgn * tx);
+        accy.add(sgn * ty);
         // XSPH average velocity (:495-500; modified solver only)
         if (!MUSCL && P.xsph) {
-            const R f = eps * R(2) * mb / (I.rho + J.rho) * w;
-            xsx.add(-sgn * (f * vij0));
-            xsy.add(-sgn * (f * vij1));
+            const R f = eps2 * mb * rcp(I.rho + J.rho) * w;
+            xsx -= sgn * (f * vij0);
+            xsy -= sgn * (f * vij1);
         }
         // delta-SPH density diffusion (:552-583), x_j - x_i and grad rho of both
-        {
-            const R p0 = -xij0, p1 = -xij1;
-            const R drho = sizeof(R) == 8 ? (J.rho - I.rho) : (J.kin.z - I.kin.z);
+        if (water) {
+            const R drho = F32 ? (J.kin.z - I.kin.z) : (J.rho - I.rho);
             const R sg0 = I.nb1.w + J.nb1.w, sg1 = I.nb2.x + J.nb2.x;
-            const R psi = drho - R(0.5) * (sg0 * p0 + sg1 * p1);
-            const R tma = (p0 * nd0 + p1 * nd1) / r2;
-            corr.add(sgn * (R(2) * dlt * hbar * cbar * psi * tma * Vb));
+            const R psi = drho + R(0.5) * (sg0 * xij0 + sg1 * xij1);
+            const R tma = -(xij0 * nd0 + xij1 * nd1) * inv_r2;
+            dr += sgn * (dlt2h * cbar * psi * tma * Vb);
         }
-        // particle shifting sum (Shift_particle_position.f90:97-100)
+        cont.add(dr);
+        // particle shifting sum (Shift_particle_position.f90:97-100), FP64:
+        // shift_a = -beta h^2 B_a^-1 sum_b (1 + R (W/W(dx))^n) grad_a W_ab V_b
         if (last_rhs) {
-            const R r = w * wdx_inv;
-            const R f = shf * (R(1) + shR * pw4(r));
-            shx.add(-sgn * (f * nd0 * Vb));
-            shy.add(-sgn * (f * nd1 * Vb));
+            double gd, wd, Vd;
+            if (F32) {
+                double dd2 = sqrt(dxd * dxd + dyd * dyd);
+                const double q = dd2 / P.h;
+                if (P.kernel_model == SPH_KERNEL_GAUSSIAN) {
+                    const double ex = exp(-(q * q));
+                    wd = (ex - P.gauss_e9) * P.kfactor;
+                    gd = ex * (-2 * q) / (dd2 * P.h) * P.kfactor;
+                } else {
+                    const double t = 1 - q / 2.0;
+                    const double t3 = t * t * t;
+                    wd = P.kfactor * (1 + 2 * q) * (t3 * t);
+                    gd = P.kfactor * (-5 * q * t3) / (dd2 * P.h);
+                }
+                Vd = D.mass[b] / (P.rho0 + (double)T.kin.z);
+            } else {
+                wd = (double)w; gd = (double)g; Vd = (double)Vb;
+            }
+            const double r = wd / P.w_dx;
+            const double r2 = r * r;
+            const double f = (1 + P.shift_R * (r2 * r2)) * Vd * gd;
+            shx += f * dxd;
+            shy += f * dyd;
         }
     }
-    // assembly (single_step_compute.f90:152-171, Solver :627-635)
-    R drho = cont.val();
-    R ax = R(0), ay = R(0);
-    if (ta == SPH_TYPE_WATER) {
-        ax = ix.val() + R(0) + avx.val() + arx.val() + spx.val() + lpx.val();
-        ay = iy.val() + R(0) + avy.val() + ary.val() + spy.val() + lpy.val();
-        drho = drho + corr.val();
+    // assembly (single_step_compute.f90:152-171, Solver :627-635); the delta-SPH
+    // term only enters the rate of water particles
+    D.drho[a] = cont.val();
+    D.acc[a] = water ? mk2<R>(accx.val(), accy.val()) : mk2<R>(R(0), R(0));
+    D.avg[a] = mk2<R>(xsx, xsy);
+    if (last_rhs) {
+        const double c = -P.shift_beta * (P.h * P.h);
+        const double s0 = c * ((double)bi.x * shx + (double)bi.y * shy);
+        const double s1 = c * ((double)bi.z * shx + (double)bi.w * shy);
+        D.shift[a] = mk2<R>((R)s0, (R)s1);
     }
-    D.drho[a] = drho;
-    D.acc[a] = mk2<R>(ax, ay);
-    D.avg[a] = mk2<R>(xsx.val(), xsy.val());
-    if (last_rhs) D.shift[a] = mk2<R>(shx.val(), shy.val());
 }
 
 }  // namespace sph
