@@ -57,19 +57,6 @@ template <typename R> __host__ __device__ inline typename VT<R>::V4 mk4(R a, R b
 template <> __host__ __device__ inline double4 mk4<double>(double a, double b, double c, double d) { return make_double4(a, b, c, d); }
 template <> __host__ __device__ inline float4 mk4<float>(float a, float b, float c, float d) { return make_float4(a, b, c, d); }
 
-// Density in the kinematic record: FP64 stores rho, the mixed path stores
-// rho - rho0 (FP32 keeps ~1e-9 absolute on the small deviation instead of
-// ~1e-7 on rho itself, which would otherwise dominate the pressure error).
-template <typename R> struct Dens;
-template <> struct Dens<double> {
-    __device__ static double rho(double stored, double) { return stored; }
-    __device__ static double store(double rho, double) { return rho; }
-};
-template <> struct Dens<float> {
-    __device__ static float rho(float stored, double rho0) { return (float)rho0 + stored; }
-    __device__ static float store(double rho, double rho0) { return (float)(rho - rho0); }
-};
-
 __device__ __forceinline__ double pw3(double x) { return x * x * x; }
 __device__ __forceinline__ double pw4(double x) { double x2 = x * x; return x2 * x2; }
 __device__ __forceinline__ double pw7(double x) { double x2 = x * x; double x4 = x2 * x2; return x4 * x2 * x; }

@@ -27,8 +27,8 @@ __global__ void __launch_bounds__(128) k_pass_a(Params P, Sorted<R> D) {
     const int ta = D.type[a];
     const int nn = D.nnbr[a];
     const double2 xa = D.pos[a];
-    const V4 ka = D.kin[a];
-    const R rho_a = Dens<R>::rho(ka.z, P.rho0);
+    const double4 ka = D.kin[a];
+    const double rho_a = ka.z;
     // the sums of this pass have no large cancellation (differences of smooth
     // fields, or B ~ I), so FP32 accumulates them directly in the mixed path
     R fra = R(0), b00 = R(0), b01 = R(0), b10 = R(0), b11 = R(0);
@@ -66,7 +66,7 @@ __global__ void __launch_bounds__(128) k_pass_a(Params P, Sorted<R> D) {
                 gs = kf * (R(-5) * q * (t * t * t)) * inv_d * inv_h;
             }
         }
-        const V4 kb = D.kin[b];
+        const double4 kb = D.kin[b];
         const R Vb = D.aux[b].y;
         const R gx = gs * dx * Vb, gy = gs * dy * Vb;    // V_b grad_a W
         // volume fraction (Define_freesurface...f90:84-85)
@@ -75,13 +75,14 @@ __global__ void __launch_bounds__(128) k_pass_a(Params P, Sorted<R> D) {
         b00 -= dx * gx; b01 -= dx * gy;
         b10 -= dy * gx; b11 -= dy * gy;
         // raw gradient sums (phi_b - phi_a) V_b grad_a W
-        const R drho = F32 ? (kb.z - ka.z) : (Dens<R>::rho(kb.z, P.rho0) - rho_a);
+        // differences of the FP64 records, then FP32 arithmetic in the mixed path
+        const R drho = (R)(kb.z - ka.z);
         g[0] += drho * gx; g[1] += drho * gy;
-        const R du = kb.x - ka.x, dv = kb.y - ka.y;
+        const R du = (R)(kb.x - ka.x), dv = (R)(kb.y - ka.y);
         g[4] += du * gx; g[5] += du * gy;
         g[6] += dv * gx; g[7] += dv * gy;
         if (P.muscl) {
-            const R dp = kb.w - ka.w;
+            const R dp = (R)(kb.w - ka.w);
             g[2] += dp * gx; g[3] += dp * gy;
         }
     }

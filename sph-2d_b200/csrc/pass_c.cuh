@@ -57,12 +57,15 @@ __device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
 template <typename R>
 struct Side {
     using V4 = typename VT<R>::V4;
-    V4 kin;     // u, v, rho-ish, p
-    V4 aux;     // m, V, c, smass
+    double4 kin;   // u, v, rho, p (FP64)
+    V4 aux;        // m, V, c, smass
     V4 nb1, nb2, nb3;
-    R rho;
 };
 
+// The pair terms are written with the pair differences du = u_i - u_j,
+// dv = v_i - v_j, dp = p_i - p_j, drho = rho_j - rho_i formed in FP64 from the
+// kinematic records; in real arithmetic this is the reference's expression,
+// e.g. v_i - v* = (v_i - v_j)/2 - (U* - Ubar) e for the modified solver.
 template <typename R, bool MUSCL>
 __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_pass_c(Params P, Sorted<R> D, int last_rhs) {
     using V4 = typename VT<R>::V4;
@@ -76,22 +79,23 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_pass_c(Params P
     Side<R> S;
     S.kin = D.kin[a]; S.aux = D.aux[a]; S.nb1 = D.nb1[a]; S.nb2 = D.nb2[a];
     if (MUSCL) S.nb3 = D.nb3[a];
-    S.rho = Dens<R>::rho(S.kin.z, P.rho0);
+    const R rho_a = (R)S.kin.z;
     const V4 bi = D.binv[a];
     const bool near_a = (D.flags[a] & 2) != 0;
+    const bool water = ta == SPH_TYPE_WATER;   // delta-SPH only enters water rates (Solver :627-635)
 
     const R hbar = (R)P.h;
     const R inv_h = (R)(1.0 / P.h);
-    const R sqc0 = (R)P.sqrt_c0, inv_sqc0 = (R)(1.0 / P.sqrt_c0);
+    const R inv_sqc0 = (R)(1.0 / P.sqrt_c0);
     const R nu2 = (R)(2.0 * P.nu), alpha = (R)P.alpha, beta = (R)P.beta;
     const R fh2 = (R)((P.fai * P.h) * (P.fai * P.h));
     const R dlt2h = (R)(2.0 * P.delta * P.h);
     const R dla_h = (R)(P.delta_alpha * P.h);
     const R eps2 = (R)(2.0 * P.eps);
-    const R inv_rho_a = rcp(S.rho);
+    const R inv_rho_a = rcp(rho_a);
     const R rho0_over_rho_a = (R)P.rho0 * inv_rho_a;
     const R r2cut = (R)(P.r_cut * P.r_cut);
-    const bool water = ta == SPH_TYPE_WATER;   // delta-SPH only enters water rates (Solver :627-635)
+    const R r2min = (R)(P.cut_min * P.cut_min);
 
     A cont, accx, accy;
     cont.init(); accx.init(); accy.init();
@@ -105,15 +109,15 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_pass_c(Params P
         const double2 xb = __ldg(&D.pos[b]);
         const double dxd = xa.x - xb.x, dyd = xa.y - xb.y;
         R d, inv_d;
-        double dd = 0.0;
         if (F32) {
             // the mixed path does not need the reference's exact sqrt test: a
             // pair within one ulp of the support radius has W = grad W = 0
             const R s = (R)(dxd * dxd + dyd * dyd);
-            if (!(s <= r2cut) || s < (R)(P.cut_min * P.cut_min)) continue;
+            if (!(s <= r2cut) || s < r2min) continue;
             inv_d = rsqrtf(s);
             d = s * inv_d;
         } else {
+            double dd;
             if (!in_support(P, dxd, dyd, dd)) continue;
             d = (R)dd;
             inv_d = R(1) / d;
@@ -121,12 +125,18 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_pass_c(Params P
         Side<R> T;
         T.kin = D.kin[b]; T.aux = D.aux[b]; T.nb1 = D.nb1[b]; T.nb2 = D.nb2[b];
         if (MUSCL) T.nb3 = D.nb3[b];
-        T.rho = Dens<R>::rho(T.kin.z, P.rho0);
         const Side<R>& I = a_is_i ? S : T;
         const Side<R>& J = a_is_i ? T : S;
+        const R sgn = a_is_i ? R(1) : R(-1);
         // position_difference_ij = x_i - x_j (find_particle_pair.f90:79-107)
         const R xij0 = (R)(a_is_i ? dxd : -dxd), xij1 = (R)(a_is_i ? dyd : -dyd);
-        // compute_kernel: W and dwdx(k) = grad_i W (x_i - x_j)
+        // FP64 pair differences
+        const R du = (R)(I.kin.x - J.kin.x), dv = (R)(I.kin.y - J.kin.y);
+        const R dp = (R)(I.kin.w - J.kin.w);
+        const R drho_ji = (R)(J.kin.z - I.kin.z);
+        const R rho_i = (R)I.kin.z, rho_j = (R)J.kin.z;
+        const R rho_b = (R)T.kin.z;
+        // compute_kernel: W and dwdx(k) = g (x_i - x_j)
         R w, g;
         {
             const R q = d * inv_h;
@@ -147,60 +157,45 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_pass_c(Params P
         const R nd0 = bi.x * dw0 + bi.y * dw1;
         const R nd1 = bi.z * dw0 + bi.w * dw1;
         const R cbar = R(0.5) * (I.aux.z + J.aux.z);
-        const R rbar = R(0.5) * (I.rho + J.rho);
+        const R rbar = R(0.5) * (rho_i + rho_j);
         const R inv_rbar = rcp(rbar);
-        const R ui = I.kin.x, vi = I.kin.y, uj = J.kin.x, vj = J.kin.y;
-        const R pi_ = I.kin.w, pj_ = J.kin.w;
-        R PL, PR, Pbar, vI0, vI1, vJ0, vJ1, vb0, vb1, e0, e1;
-        if (!MUSCL) {
-            PL = pi_; PR = pj_; Pbar = R(0.5) * (PL + PR);
-            vI0 = ui; vI1 = vi; vJ0 = uj; vJ1 = vj;
-            vb0 = R(0.5) * (vI0 + vJ0); vb1 = R(0.5) * (vI1 + vJ1);
-            e0 = -xij0 * inv_d; e1 = -xij1 * inv_d;
-        } else {
+        const R e0 = -xij0 * inv_d, e1 = -xij1 * inv_d;     // x_j - x_i direction (both solvers)
+        // Riemann states.  li/lj are the MUSCL reconstruction increments
+        // (function_module.f90:34-80); the modified solver has none.
+        R lpi = R(0), lpj = R(0), lui = R(0), luj = R(0), lvi = R(0), lvj = R(0);
+        if (MUSCL) {
             const R x0 = -xij0, x1 = -xij1;          // j - i
-            e0 = x0 * inv_d; e1 = x1 * inv_d;
-            R li, lj;
             // nb2 = (grad rho y, grad p x, grad p y, grad u x), nb3 = (grad u y, grad v x, grad v y, 0)
-            R Di = R(0.5) * (I.nb2.y * x0 + I.nb2.z * x1);
-            R Dj = R(-0.5) * (J.nb2.y * x0 + J.nb2.z * x1);
-            muscl_limiter<R>(Di, Dj, pj_ - pi_, li, lj);
-            PL = pi_ + li; PR = pj_ - lj; Pbar = R(0.5) * (pi_ + pj_);
-            const R vd0 = -(ui - uj), vd1 = -(vi - vj);
-            Di = R(0.5) * (I.nb2.w * x0 + I.nb3.x * x1);
-            Dj = R(-0.5) * (J.nb2.w * x0 + J.nb3.x * x1);
-            muscl_limiter<R>(Di, Dj, vd0, li, lj);
-            vI0 = ui + li; vJ0 = uj - lj;
-            Di = R(0.5) * (I.nb3.y * x0 + I.nb3.z * x1);
-            Dj = R(-0.5) * (J.nb3.y * x0 + J.nb3.z * x1);
-            muscl_limiter<R>(Di, Dj, vd1, li, lj);
-            vI1 = vi + li; vJ1 = vj - lj;
-            vb0 = R(0.5) * (ui + uj); vb1 = R(0.5) * (vi + vj);
+            muscl_limiter<R>(R(0.5) * (I.nb2.y * x0 + I.nb2.z * x1), R(-0.5) * (J.nb2.y * x0 + J.nb2.z * x1), -dp,
+                             lpi, lpj);
+            muscl_limiter<R>(R(0.5) * (I.nb2.w * x0 + I.nb3.x * x1), R(-0.5) * (J.nb2.w * x0 + J.nb3.x * x1), -du,
+                             lui, luj);
+            muscl_limiter<R>(R(0.5) * (I.nb3.y * x0 + I.nb3.z * x1), R(-0.5) * (J.nb3.y * x0 + J.nb3.z * x1), -dv,
+                             lvi, lvj);
         }
-        const R UL = vI0 * e0 + vI1 * e1;
-        const R UR = vJ0 * e0 + vJ1 * e1;
-        const R Ubar = R(0.5) * (UL + UR);
-        const R Us = Ubar + R(0.5) * (PL - PR) * (inv_rbar * inv_sqc0);
-        const R vs0 = (Us - Ubar) * e0 + vb0, vs1 = (Us - Ubar) * e1 + vb1;
-        const R bR = min(R(3) * (max((UL - UR), R(0))), cbar);
-        const R Ps = Pbar + R(0.5) * bR * rbar * (UL - UR);
-        // this side's star state (near-free-surface particles use the averages)
-        const R vA0 = near_a ? vb0 : vs0, vA1 = near_a ? vb1 : vs1, PA = near_a ? Pbar : Ps;
-        const R va0 = a_is_i ? vI0 : vJ0, va1 = a_is_i ? vI1 : vJ1;
+        // U_L - U_R and P_L - P_R from the differences
+        const R dU = (du + lui + luj) * e0 + (dv + lvi + lvj) * e1;
+        const R dP = dp + lpi + lpj;
+        const R sU = R(0.5) * dP * (inv_rbar * inv_sqc0);               // U* - Ubar
+        const R bR = min(R(3) * (max(dU, R(0))), cbar);
+        const R Pbar = R(0.5) * ((R)I.kin.w + (R)J.kin.w);
+        const R Ps = Pbar + R(0.5) * bR * rbar * dU;
+        const R PA = near_a ? Pbar : Ps;
+        // this side's velocity minus its star velocity (near-surface: the average)
+        R wa0, wa1;
+        if (a_is_i) { wa0 = R(0.5) * du + lui; wa1 = R(0.5) * dv + lvi; }
+        else { wa0 = R(-0.5) * du - luj; wa1 = R(-0.5) * dv - lvj; }
+        if (!near_a) { wa0 -= sU * e0; wa1 -= sU * e1; }
         const R Vb = T.aux.y, mb = T.aux.x;
-        const R sgn = a_is_i ? R(1) : R(-1);
         // continuity (:360-369)
-        R tm = (va0 - vA0) * nd0 + (va1 - vA1) * nd1;
-        if (!a_is_i) tm = -tm;
-        R dr = R(2) * S.rho * Vb * tm;
+        R dr = R(2) * rho_a * Vb * (sgn * (wa0 * nd0 + wa1 * nd1));
         // pressure force (:374-388)
-        const R rho_ij = inv_rho_a * rcp(T.rho);
+        const R rho_ij = inv_rho_a * rcp(rho_b);
         const R fp = R(-2) * PA * rho_ij * mb;
         R tx = fp * nd0, ty = fp * nd1;
         // artificial viscosity (:392-417)
-        const R vij0 = ui - uj, vij1 = vi - vj;
         const R inv_r2 = inv_d * inv_d;
-        const R vx = vij0 * xij0 + vij1 * xij1;
+        const R vx = du * xij0 + dv * xij1;
         if (vx < R(0)) {
             const R phi1 = hbar * vx / (d * d + fh2);
             const R Pi = (-alpha * cbar * phi1 + beta * (phi1 * phi1)) * inv_rbar;
@@ -209,8 +204,8 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_pass_c(Params P
         }
         // Morris laplacian (:432-436)
         const R lf = Vb * nu2 * (xij0 * nd0 + xij1 * nd1) * inv_r2;
-        tx += lf * vij0;
-        ty += lf * vij1;
+        tx += lf * du;
+        ty += lf * dv;
         // delta-alpha artificial internal acceleration (:442-446)
         const R tt = dla_h * cbar * vx * inv_r2 * rho0_over_rho_a * Vb;
         tx += tt * nd0;
@@ -228,15 +223,14 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_pass_c(Params P
         accy.add(sgn * ty);
         // XSPH average velocity (:495-500; modified solver only)
         if (!MUSCL && P.xsph) {
-            const R f = eps2 * mb * rcp(I.rho + J.rho) * w;
-            xsx -= sgn * (f * vij0);
-            xsy -= sgn * (f * vij1);
+            const R f = eps2 * mb * rcp(rho_i + rho_j) * w;
+            xsx -= sgn * (f * du);
+            xsy -= sgn * (f * dv);
         }
-        // delta-SPH density diffusion (:552-583), x_j - x_i and grad rho of both
+        // delta-SPH density diffusion (:552-583): psi = (rho_j - rho_i) - 0.5 (grad rho_i + grad rho_j).(x_j - x_i)
         if (water) {
-            const R drho = F32 ? (J.kin.z - I.kin.z) : (J.rho - I.rho);
             const R sg0 = I.nb1.w + J.nb1.w, sg1 = I.nb2.x + J.nb2.x;
-            const R psi = drho + R(0.5) * (sg0 * xij0 + sg1 * xij1);
+            const R psi = drho_ji + R(0.5) * (sg0 * xij0 + sg1 * xij1);
             const R tma = -(xij0 * nd0 + xij1 * nd1) * inv_r2;
             dr += sgn * (dlt2h * cbar * psi * tma * Vb);
         }
@@ -246,7 +240,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_pass_c(Params P
         if (last_rhs) {
             double gd, wd, Vd;
             if (F32) {
-                double dd2 = sqrt(dxd * dxd + dyd * dyd);
+                const double dd2 = sqrt(dxd * dxd + dyd * dyd);
                 const double q = dd2 / P.h;
                 if (P.kernel_model == SPH_KERNEL_GAUSSIAN) {
                     const double ex = exp(-(q * q));
@@ -258,7 +252,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_pass_c(Params P
                     wd = P.kfactor * (1 + 2 * q) * (t3 * t);
                     gd = P.kfactor * (-5 * q * t3) / (dd2 * P.h);
                 }
-                Vd = D.mass[b] / (P.rho0 + (double)T.kin.z);
+                Vd = D.mass[b] / T.kin.z;
             } else {
                 wd = (double)w; gd = (double)g; Vd = (double)Vb;
             }
@@ -269,8 +263,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_pass_c(Params P
             shy += f * dyd;
         }
     }
-    // assembly (single_step_compute.f90:152-171, Solver :627-635); the delta-SPH
-    // term only enters the rate of water particles
+    // assembly (single_step_compute.f90:152-171, Solver :627-635)
     D.drho[a] = cont.val();
     D.acc[a] = water ? mk2<R>(accx.val(), accy.val()) : mk2<R>(R(0), R(0));
     D.avg[a] = mk2<R>(xsx, xsy);

@@ -107,7 +107,8 @@ struct Sorted {
     double* rho0;     // step-start density (FP64 master)
     double* mass;
     double* smass;
-    V4* kin;          // u, v, rho (FP64) or rho-rho0 (mixed), p     -- neighbour record 1
+    double4* kin;     // u, v, rho, p (FP64 in both paths: pair differences are  -- neighbour record 1
+                      // formed from it in FP64 before the FP32 arithmetic)
     V4* aux;          // m, V = m/rho, c, smass                      -- neighbour record 2
     V4* nb1;          // tau_xx, tau_xy, tau_yy, grad rho x          -- neighbour record 3
     V4* nb2;          // grad rho y, grad p x, grad p y, grad u x     -- neighbour record 4
@@ -123,7 +124,7 @@ struct Sorted {
     // Runge-Kutta sums K1 + 2 K2 + 2 K3 (time_iteration.f90:1040-1045)
     R* ks_r;
     V2* ks_a;
-    V2* ks_v;
+    double2* ks_v;    // velocity sums in FP64 (they move the FP64 positions)
     // rates carried to the next step (K1 reuse)
     R* c_drho;
     V2* c_acc;
@@ -251,7 +252,7 @@ __global__ void k_records(Params P, Sorted<R> D) {
     eos64(P, rho, p, c);
     double2 v = D.vel0[s];
     double m = D.mass[s];
-    D.kin[s] = mk4<R>((R)v.x, (R)v.y, Dens<R>::store(rho, P.rho0), (R)p);
+    D.kin[s] = make_double4(v.x, v.y, rho, p);
     D.aux[s] = mk4<R>((R)m, (R)(m / rho), (R)c, (R)D.smass[s]);
 }
 

@@ -44,15 +44,17 @@ __global__ void k_stage(Params P, Sorted<R> D, int stage, double dt, int use_car
         if (stage == 0) {
             D.ks_r[s] = (R)dr;
             D.ks_a[s] = mk2<R>((R)ax, (R)ay);
-            D.ks_v[s] = mk2<R>((R)u, (R)v);
+            D.ks_v[s] = make_double2(u, v);
         } else {
             D.ks_r[s] = D.ks_r[s] + R(2) * (R)dr;
-            V2 ka = D.ks_a[s], kv = D.ks_v[s];
+            V2 ka = D.ks_a[s];
+            double2 kv = D.ks_v[s];
             D.ks_a[s] = mk2<R>(ka.x + R(2) * (R)ax, ka.y + R(2) * (R)ay);
-            D.ks_v[s] = mk2<R>(kv.x + R(2) * (R)u, kv.y + R(2) * (R)v);
+            D.ks_v[s] = make_double2(kv.x + 2 * u, kv.y + 2 * v);
         }
     } else {
-        const V2 ka = D.ks_a[s], kv = D.ks_v[s];
+        const V2 ka = D.ks_a[s];
+        const double2 kv = D.ks_v[s];
         rho = r0 + ((double)D.ks_r[s] + dr) * dt / 6.0;
         u = v0.x + ((double)ka.x + ax) * dt / 6.0 + gx;
         x = x0.x + ((double)kv.x + u) * dt / 6.0 + 0.5 * dt * dt * ax;
@@ -89,7 +91,7 @@ __global__ void k_stage(Params P, Sorted<R> D, int stage, double dt, int use_car
     double p, c;
     eos64(P, rho, p, c);
     const double m = D.mass[s];
-    D.kin[s] = mk4<R>((R)u, (R)v, Dens<R>::store(rho, P.rho0), (R)p);
+    D.kin[s] = make_double4(u, v, rho, p);
     D.aux[s] = mk4<R>((R)m, (R)(m / rho), (R)c, (R)D.smass[s]);
 }
 
