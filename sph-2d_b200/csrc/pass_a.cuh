@@ -98,6 +98,7 @@ __global__ void __launch_bounds__(128) k_pass_a(Params P, Sorted<R> D) {
     }
     const R m00 = (R)i00, m01 = (R)i01, m10 = (R)i10, m11 = (R)i11;
     D.binv[a] = mk4<R>(m00, m01, m10, m11);
+    D.binv64[a] = make_double4(i00, i01, i10, i11);
     R gr[8];
     for (int f = 0; f < 4; ++f) {
         R x = g[2 * f], y = g[2 * f + 1];

@@ -268,10 +268,9 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_pass_c(Params P
     D.acc[a] = water ? mk2<R>(accx.val(), accy.val()) : mk2<R>(R(0), R(0));
     D.avg[a] = mk2<R>(xsx, xsy);
     if (last_rhs) {
+        const double4 b64 = D.binv64[a];
         const double c = -P.shift_beta * (P.h * P.h);
-        const double s0 = c * ((double)bi.x * shx + (double)bi.y * shy);
-        const double s1 = c * ((double)bi.z * shx + (double)bi.w * shy);
-        D.shift[a] = mk2<R>((R)s0, (R)s1);
+        D.shift[a] = make_double2(c * (b64.x * shx + b64.y * shy), c * (b64.z * shx + b64.w * shy));
     }
 }
 

@@ -113,14 +113,15 @@ struct Sorted {
     V4* nb1;          // tau_xx, tau_xy, tau_yy, grad rho x          -- neighbour record 3
     V4* nb2;          // grad rho y, grad p x, grad p y, grad u x     -- neighbour record 4
     V4* nb3;          // grad u y, grad v x, grad v y, 0             -- neighbour record 5 (MUSCL)
-    V4* binv;         // B^-1 (11, 12, 21, 22)
+    V4* binv;         // B^-1 (11, 12, 21, 22) in the pair precision
+    double4* binv64;  // B^-1 in FP64 (applied to the FP64 shifting sum)
     R* fra_v;
     uint8_t* flags;   // bit0 surface, bit1 near surface, bit2 surface candidate
     // rates of the current RHS
     R* drho;
     V2* acc;
     V2* avg;
-    V2* shift;        // shifting displacement sums (last RHS of a step)
+    double2* shift;   // shifting displacement (last RHS of a step), FP64
     // Runge-Kutta sums K1 + 2 K2 + 2 K3 (time_iteration.f90:1040-1045)
     R* ks_r;
     V2* ks_a;

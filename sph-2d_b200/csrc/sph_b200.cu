@@ -234,6 +234,7 @@ int alloc_sorted(Sorted<R>& D, int cap, int max_nbr, int ncells) {
     CK(dalloc(&D.mass, cap)); CK(dalloc(&D.smass, cap));
     CK(dalloc(&D.kin, cap)); CK(dalloc(&D.aux, cap));
     CK(dalloc(&D.nb1, cap)); CK(dalloc(&D.nb2, cap)); CK(dalloc(&D.nb3, cap)); CK(dalloc(&D.binv, cap));
+    CK(dalloc(&D.binv64, cap));
     CK(dalloc(&D.fra_v, cap)); CK(dalloc(&D.flags, cap));
     CK(dalloc(&D.drho, cap)); CK(dalloc(&D.acc, cap)); CK(dalloc(&D.avg, cap)); CK(dalloc(&D.shift, cap));
     CK(dalloc(&D.ks_r, cap)); CK(dalloc(&D.ks_a, cap)); CK(dalloc(&D.ks_v, cap));
@@ -248,7 +249,7 @@ int alloc_sorted(Sorted<R>& D, int cap, int max_nbr, int ncells) {
 template <typename R>
 void free_sorted(Sorted<R>& D) {
     void* ptrs[] = {D.id, D.type, D.pos, D.pos0, D.vel0, D.rho0, D.mass, D.smass, D.kin, D.aux, D.nb1, D.nb2, D.nb3,
-                    D.binv, D.fra_v, D.flags, D.drho, D.acc, D.avg, D.shift, D.ks_r, D.ks_a, D.ks_v, D.c_drho,
+                    D.binv, D.binv64, D.fra_v, D.flags, D.drho, D.acc, D.avg, D.shift, D.ks_r, D.ks_a, D.ks_v, D.c_drho,
                     D.c_acc, D.c_avg, D.nbr, D.nnbr, D.cell_start, D.cell_end};
     for (void* p : ptrs) if (p) cudaFree(p);
     D = Sorted<R>{};

@@ -71,8 +71,8 @@ __global__ void k_stage(Params P, Sorted<R> D, int stage, double dt, int use_car
     if (stage == 3) {
         if (do_shift && !(D.flags[s] & 2)) {
             // Shift_particle_position.f90:108-131
-            const V2 sh = D.shift[s];
-            double s0 = (double)sh.x, s1 = (double)sh.y;
+            const double2 sh = D.shift[s];
+            double s0 = sh.x, s1 = sh.y;
             const double amp = sqrt(s0 * s0 + s1 * s1);
             if (amp > P.shift_max) { s0 = s0 / amp * P.shift_max; s1 = s1 / amp * P.shift_max; }
             x = x + s0;
