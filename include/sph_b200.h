@@ -183,6 +183,25 @@ int sph_get_field(sph_handle* h, int field, double* out);
 int sph_get_timings(sph_handle* h, sph_timings* out);
 int sph_reset_timings(sph_handle* h);
 
+/* find_particle_pair for callers that cannot allocate GPU memory.  No
+ * counterpart in the reference.  Hosts whose GPU memory is owned and pooled by
+ * another framework, or that run where allocation is not allowed, pass their
+ * own device buffers: d_pos [2n] column-major and d_type [n] as inputs,
+ * d_pair_i/d_pair_j [pair_cap], d_w [pair_cap] and d_dwdx [2*pair_cap] (may be
+ * NULL) as outputs -- the same contents and order sph_find_particle_pair
+ * returns for a non-periodic configuration -- and *pair_number (host) receives
+ * the pair count.  stream is a cudaStream_t (NULL: the legacy default stream).
+ * The search works in a fixed static device array (about 2.4 MiB per GPU that
+ * loads the library, held until exit) and calls no cudaMalloc / cudaFree:
+ * at most 65536 particles and 65536 background cells of edge kernel_scale*h
+ * over grid_lo..grid_hi; larger inputs return SPH_E_CAPACITY.  Calls share that
+ * array: GPU work of two calls must not overlap.  The first call on a device
+ * resolves the array's address (cudaGetSymbolAddress); make it before any
+ * stream capture.  cfg->periodic is ignored (no images are generated). */
+int sph_find_particle_pair_noalloc(const sph_config* cfg, int n, const double* d_pos, const int* d_type,
+                                   long long pair_cap, int* d_pair_i, int* d_pair_j, double* d_w,
+                                   double* d_dwdx, long long* pair_number, void* stream);
+
 /* Human-readable message for a status code (static storage). */
 const char* sph_strerror(int code);
 

@@ -46,7 +46,8 @@ def nvcc() -> str:
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not needs_build():
         return OUT
-    cmd = [nvcc(), *NVCC_FLAGS, "-o", OUT + ".tmp", os.path.join(CSRC, "sph_b200.cu")]
+    cmd = [nvcc(), *NVCC_FLAGS, "-o", OUT + ".tmp", os.path.join(CSRC, "sph_b200.cu"),
+           os.path.join(CSRC, "sph_noalloc.cu")]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True, cwd=CSRC)

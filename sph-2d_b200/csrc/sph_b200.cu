@@ -594,6 +594,11 @@ int get_state_impl(sph_handle* h, int n, double* pos, double* vel, double* rho, 
 
 }  // namespace
 
+// The configuration-to-parameter mapping, shared with sph_noalloc.cu.
+namespace sph {
+int derive_params_shared(const sph_config& c, Params& P) { return derive_params(c, P); }
+}  // namespace sph
+
 // ===========================================================================
 // C-ABI
 // ===========================================================================

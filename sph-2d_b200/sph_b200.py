@@ -49,7 +49,7 @@ TYPE_ILL = 120
 EXPORTED_SYMBOLS = (
     "sph_init", "sph_free", "sph_set_state", "sph_get_state", "sph_find_particle_pair",
     "sph_rhs", "sph_step", "sph_diagnostics", "sph_get_timings", "sph_reset_timings",
-    "sph_strerror", "sph_get_field", "sph_update_state",
+    "sph_strerror", "sph_get_field", "sph_update_state", "sph_find_particle_pair_noalloc",
 )
 
 
@@ -241,6 +241,10 @@ def load(path: str = LIB_PATH):
     lib.sph_get_timings.argtypes = [P, ctypes.POINTER(SphTimings)]
     lib.sph_reset_timings.argtypes = [P]
     lib.sph_get_field.argtypes = [P, ctypes.c_int, dp]
+    lib.sph_find_particle_pair_noalloc.argtypes = [ctypes.POINTER(SphConfig), ctypes.c_int, ctypes.c_void_p,
+                                                   ctypes.c_void_p, ctypes.c_longlong, ctypes.c_void_p,
+                                                   ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                   ctypes.POINTER(ctypes.c_longlong), ctypes.c_void_p]
     lib.sph_strerror.argtypes = [ctypes.c_int]
     lib.sph_strerror.restype = ctypes.c_char_p
     for name in EXPORTED_SYMBOLS:
