@@ -137,9 +137,9 @@ def peaks():
 
 
 # Algorithmic bytes per particle of pass C (the dominant kernel): its own
-# records read once (pos 16 B, kin 16, aux 16, nb1..nb3 48, B^-1 16, flags 1)
-# and its outputs written once (drhodt 4, acc 8, avg 8, shift 8), FP32 records.
-PASS_C_BYTES_MIXED = 16 + 16 + 16 + 48 + 16 + 1 + 4 + 8 + 8 + 8
+# records read once (pos 16 B, kin 32 (FP64 in both paths), aux, nb1..nb3,
+# B^-1, flags 1) and its outputs written once (drhodt, acc, avg, shift 16).
+PASS_C_BYTES_MIXED = 16 + 32 + 16 + 48 + 16 + 1 + 4 + 8 + 8 + 16
 PASS_C_BYTES_FP64 = 16 + 32 + 32 + 96 + 32 + 1 + 8 + 16 + 16 + 16
 
 

@@ -36,10 +36,18 @@ __global__ void __launch_bounds__(128) k_pass_a(Params P, Sorted<R> D) {
     for (int c = 0; c < 8; ++c) g[c] = R(0);
     const R inv_h = (R)(1.0 / P.h);
     const R r2cut = (R)(P.r_cut * P.r_cut), r2min = (R)(P.cut_min * P.cut_min);
+    int np = 0;
+    // the next entry and its position are loaded one iteration ahead
+    unsigned ent_n = nn > 0 ? __ldg(&D.nbr[a]) : 0u;
+    double2 xb_n = nn > 0 ? __ldg(&D.pos[ent_n & 0x7fffffffu]) : make_double2(0.0, 0.0);
     for (int e = 0; e < nn; ++e) {
-        const unsigned ent = __ldg(&D.nbr[(size_t)e * P.nbr_stride + a]);
+        const unsigned ent = ent_n;
         const int b = (int)(ent & 0x7fffffffu);
-        const double2 xb = __ldg(&D.pos[b]);
+        const double2 xb = xb_n;
+        if (e + 1 < nn) {
+            ent_n = __ldg(&D.nbr[(size_t)(e + 1) * P.nbr_stride + a]);
+            xb_n = __ldg(&D.pos[ent_n & 0x7fffffffu]);
+        }
         const double dxd = xa.x - xb.x, dyd = xa.y - xb.y;
         R d, inv_d;
         if (F32) {
@@ -53,6 +61,8 @@ __global__ void __launch_bounds__(128) k_pass_a(Params P, Sorted<R> D) {
             d = (R)dd;
             inv_d = R(1) / d;
         }
+        D.pairs[(size_t)np * P.nbr_stride + a] = ent;
+        ++np;
         const R dx = (R)dxd, dy = (R)dyd;
         // grad_a W = g(d) (x_a - x_b)  (compute_kernel)
         R gs;
@@ -86,6 +96,7 @@ __global__ void __launch_bounds__(128) k_pass_a(Params P, Sorted<R> D) {
             g[2] += dp * gx; g[3] += dp * gy;
         }
     }
+    D.npairs[a] = np;
     fra = fra * (R)(1.0 / P.sv);
     // inverse of the 2x2 tensor in FP64 (matrix_inversion_less_three,
     // function_module.f90:190-204); the reference keeps the identity on success
@@ -142,12 +153,12 @@ __global__ void k_surface(Params P, Sorted<R> D) {
     if (a >= P.n_tot) return;
     uint8_t fl = D.flags[a];
     if (!(fl & 4)) return;
-    const int nn = D.nnbr[a];
+    const int nn = D.npairs[a];
     const double2 xa = D.pos[a];
     // sum_dwdx (:155-156) recomputed here (candidates are rare)
     double s0 = 0.0, s1 = 0.0;
     for (int e = 0; e < nn; ++e) {
-        const int b = (int)(D.nbr[(size_t)e * P.nbr_stride + a] & 0x7fffffffu);
+        const int b = (int)(D.pairs[(size_t)e * P.nbr_stride + a] & 0x7fffffffu);
         const double2 xb = D.pos[b];
         double dx = xa.x - xb.x, dy = xa.y - xb.y, d;
         if (!in_support(P, dx, dy, d)) continue;
@@ -167,7 +178,7 @@ __global__ void k_surface(Params P, Sorted<R> D) {
         const double h = P.h;
         const double vx = xa.x + h * n0, vy = xa.y + h * n1;
         for (int e = 0; e < nn && surface; ++e) {
-            const int b = (int)(D.nbr[(size_t)e * P.nbr_stride + a] & 0x7fffffffu);
+            const int b = (int)(D.pairs[(size_t)e * P.nbr_stride + a] & 0x7fffffffu);
             if (D.type[b] != SPH_TYPE_WATER) continue;
             const double2 xb = D.pos[b];
             double p0 = xb.x - xa.x, p1 = xb.y - xa.y;
@@ -189,13 +200,9 @@ __global__ void k_near(Params P, Sorted<R> D) {
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= P.n_tot) return;
     if (!(D.flags[a] & 1)) return;
-    const int nn = D.nnbr[a];
-    const double2 xa = D.pos[a];
+    const int nn = D.npairs[a];
     for (int e = 0; e < nn; ++e) {
-        const int b = (int)(D.nbr[(size_t)e * P.nbr_stride + a] & 0x7fffffffu);
-        const double2 xb = D.pos[b];
-        double dx = xa.x - xb.x, dy = xa.y - xb.y, d;
-        if (!in_support(P, dx, dy, d)) continue;
+        const int b = (int)(D.pairs[(size_t)e * P.nbr_stride + a] & 0x7fffffffu);
         D.flags[b] |= 2;
     }
 }

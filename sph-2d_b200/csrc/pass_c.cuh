@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_pass_c(Params P
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= P.n_tot) return;
     const int ta = D.type[a];
-    const int nn = D.nnbr[a];
+    const int nn = D.npairs[a];
     const double2 xa = D.pos[a];
     Side<R> S;
     S.kin = D.kin[a]; S.aux = D.aux[a]; S.nb1 = D.nb1[a]; S.nb2 = D.nb2[a];
@@ -94,32 +94,32 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_pass_c(Params P
     const R eps2 = (R)(2.0 * P.eps);
     const R inv_rho_a = rcp(rho_a);
     const R rho0_over_rho_a = (R)P.rho0 * inv_rho_a;
-    const R r2cut = (R)(P.r_cut * P.r_cut);
-    const R r2min = (R)(P.cut_min * P.cut_min);
 
     A cont, accx, accy;
     cont.init(); accx.init(); accy.init();
     R xsx = R(0), xsy = R(0);
     double shx = 0.0, shy = 0.0;   // shifting sum, FP64 in both paths
 
+    // the pairs pass A found inside the support at this RHS
+    unsigned ent_n = nn > 0 ? __ldg(&D.pairs[a]) : 0u;
+    double2 xb_n = nn > 0 ? __ldg(&D.pos[ent_n & 0x7fffffffu]) : make_double2(0.0, 0.0);
     for (int e = 0; e < nn; ++e) {
-        const unsigned ent = __ldg(&D.nbr[(size_t)e * P.nbr_stride + a]);
+        const unsigned ent = ent_n;
         const int b = (int)(ent & 0x7fffffffu);
         const bool a_is_i = (ent >> 31) != 0;
-        const double2 xb = __ldg(&D.pos[b]);
+        const double2 xb = xb_n;
+        if (e + 1 < nn) {
+            ent_n = __ldg(&D.pairs[(size_t)(e + 1) * P.nbr_stride + a]);
+            xb_n = __ldg(&D.pos[ent_n & 0x7fffffffu]);
+        }
         const double dxd = xa.x - xb.x, dyd = xa.y - xb.y;
         R d, inv_d;
         if (F32) {
-            // the mixed path does not need the reference's exact sqrt test: a
-            // pair within one ulp of the support radius has W = grad W = 0
             const R s = (R)(dxd * dxd + dyd * dyd);
-            if (!(s <= r2cut) || s < r2min) continue;
             inv_d = rsqrtf(s);
             d = s * inv_d;
         } else {
-            double dd;
-            if (!in_support(P, dxd, dyd, dd)) continue;
-            d = (R)dd;
+            d = (R)sqrt(dxd * dxd + dyd * dyd);
             inv_d = R(1) / d;
         }
         Side<R> T;

@@ -133,6 +133,10 @@ struct Sorted {
     // neighbour lists: slot-major [max_nbr][stride], bit 31 = "this particle has the lower id"
     unsigned* nbr;
     int* nnbr;
+    // the pairs of the current RHS (list entries inside the support), same layout,
+    // written by pass A and read by the passes that follow it
+    unsigned* pairs;
+    int* npairs;
     // cell ranges
     int* cell_start;
     int* cell_end;
