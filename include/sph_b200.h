@@ -51,6 +51,8 @@ extern "C" {
 /* Solver_* variants (which `call Solver_...` line is live) */
 #define SPH_SOLVER_MODLR_DELTA_SPS  0 /* Solver_Normalized_Modified_Linear_Riemann_Delta_SPS (TGV default) */
 #define SPH_SOLVER_MUSCL_DELTA_SPS  1 /* Solver_Normalized_MUSCL_Linear_Riemann_Delta_SPS                 */
+#define SPH_SOLVER_MS_MODLR_DELTA   2 /* Moving_Square.../Solver_Normalized_Modified_Linear_Riemann_Delta (MS default) */
+#define SPH_SOLVER_MS_HLLC_DELTA    3 /* Moving_Square.../Solver_Normalized_HLLC_Riemann_Delta                     */
 
 #define SPH_EOS_TAIT    0   /* Status_Equation.f90:56-66  p = B((rho/rho0)^7-1) + pb */
 #define SPH_EOS_LINEAR  1   /* Status_Equation.f90:69-76  p = c0^2 (rho-rho0) + pb   */
@@ -62,11 +64,15 @@ extern "C" {
 #define SPH_PREC_MIXED  1   /* FP32 pair arithmetic + compensated sums, FP64 state   */
 
 #define SPH_INTEGRATOR_RK4_REUSE 0 /* time_iteration.f90:781-1159 (3 RHS/step after step 1) */
+#define SPH_INTEGRATOR_EULER_PC  1 /* Moving_Square.../SPH_Time_Iteration.f90:304-334, Iteration_Method 2 (1 RHS/step) */
 
 /* particle type labels (Information_Module.f90 of the moving-square case) */
 #define SPH_TYPE_WATER     2
 #define SPH_TYPE_PERIODIC  -101
 #define SPH_TYPE_ILL       120
+#define SPH_TYPE_FIX_GHOST  -3
+#define SPH_TYPE_BODY       -4   /* Body_Particle_Label: an initial type (body force) */
+#define SPH_TYPE_INLET    -201
 
 /* ---- configuration (filled once from information_module) ------------- */
 typedef struct sph_config {
@@ -97,6 +103,8 @@ typedef struct sph_config {
     double box_lo[2], box_hi[2];   /* periodic box (Period_Boundary_*_Min/Max)       */
     double grid_lo[2], grid_hi[2]; /* extent every particle must stay inside         */
     double cell_skin;         /* extra cell width as a fraction of the support (>= 0) */
+    int    laplacian;         /* laplacianTerm: 1 Morris, 0 Monaghan (moving-square solvers) */
+    int    free_surface;      /* Has_FreeSurface_Or_Not: 1 detect free-surface particles, 0 none */
 } sph_config;
 
 /* diagnostics returned by sph_step (reductions in FP64) */
@@ -106,6 +114,9 @@ typedef struct sph_diag {
     long long pair_count;     /* pairs seen by the last RHS evaluation              */
     int    n_images;          /* periodic images generated at the last step start   */
     int    n_surface;         /* free-surface particles at the last RHS evaluation  */
+    double body_force[6];     /* pressure x,y; viscous x,y; total x,y of the last RHS (FP64,
+                                 Moving_Square.../Calculate_Body_Force.f90:53-142 and
+                                 Single_step_compute.f90:228-243); zero without body particles */
 } sph_diag;
 
 /* per-pass device times (CUDA events) accumulated since the last reset, ms */
@@ -140,6 +151,12 @@ int sph_set_state(sph_handle* h, int n, const double* pos, const double* vel,
  * as K1 stay attached to their particles.  No reference counterpart: the
  * Fortran host writes its module arrays directly. */
 int sph_update_state(sph_handle* h, int n, const double* pos, const double* vel, const double* rho);
+
+/* subdomain_particle_initial_type for the n host particles: particles whose
+ * initial type is SPH_TYPE_BODY form the body of the body-force integral
+ * (Moving_Square.../Calculate_Body_Force.f90:60).  Without this call no body
+ * force is computed. */
+int sph_set_initial_type(sph_handle* h, int n, const int* initial_type);
 
 /* Download the host particles (same order as set_state).  press is the
  * equation of state evaluated at the returned density.  Any pointer may be NULL. */

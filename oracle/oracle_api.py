@@ -53,6 +53,9 @@ def load():
     lib.oracle_last_pair_count.restype = ctypes.c_longlong
     lib.oracle_last_images.argtypes = [ctypes.c_void_p]
     lib.oracle_destroy.argtypes = [ctypes.c_void_p]
+    lib.oracle_set_initial_type.argtypes = [ctypes.c_void_p, ctypes.c_int, ip]
+    lib.oracle_body_force.argtypes = [ctypes.c_void_p, dp]
+    lib.oracle_rhs_body_force.argtypes = [cp, ctypes.c_int, dp, dp, dp, dp, ip, ip, dp]
     _lib = lib
     return lib
 
@@ -143,6 +146,15 @@ class OracleSim:
         self.lib.oracle_get_state(self.h, n, _p(pos), _p(vel), _p(rho), _p(press))
         return pos, vel, rho, press
 
+    def set_initial_type(self, itype):
+        it = np.ascontiguousarray(itype, np.int32)
+        self.lib.oracle_set_initial_type(self.h, self.n, _p(it, ctypes.c_int))
+
+    def body_force(self):
+        out = np.zeros(6)
+        self.lib.oracle_body_force(self.h, _p(out))
+        return out
+
     def kinetic_energy(self) -> float:
         return self.lib.oracle_kinetic_energy(self.h)
 
@@ -159,3 +171,13 @@ class OracleSim:
                 self.h = None
         except Exception:
             pass
+
+
+def rhs_body_force(cfg: SphConfig, pos, vel, rho, mass, type_, itype):
+    out = np.zeros(6)
+    a = [np.ascontiguousarray(x, np.float64) for x in (pos, vel, rho, mass)]
+    t = np.ascontiguousarray(type_, np.int32)
+    it = np.ascontiguousarray(itype, np.int32)
+    load().oracle_rhs_body_force(ctypes.byref(cfg), rho.shape[0], _p(a[0]), _p(a[1]), _p(a[2]), _p(a[3]),
+                                 _p(t, ctypes.c_int), _p(it, ctypes.c_int), _p(out))
+    return out

@@ -180,11 +180,12 @@ struct Particles {
     int n = 0;
     std::vector<double> x, y, u, v, rho, mass, smass;
     std::vector<int> type;
+    std::vector<int> itype;    // subdomain_particle_initial_type (body force)
     std::vector<int> src;      // image source (host index) or -1
     void resize(int m) {
         n = m;
         x.resize(m); y.resize(m); u.resize(m); v.resize(m); rho.resize(m); mass.resize(m);
-        smass.resize(m); type.resize(m); src.resize(m);
+        smass.resize(m); type.resize(m); itype.resize(m); src.resize(m);
     }
 };
 
@@ -237,6 +238,13 @@ void build_grid(const Particles& P, Grid& G) {
 // Stencil order of Taylor_Green_Vortex/Distribute_Backgroud_Grid.f90:104-112:
 // self, left, right, up-left, up, up-right, down-left, down, down-right.
 const int kStencil[9][2] = {{0, 0}, {-1, 0}, {1, 0}, {-1, 1}, {0, 1}, {1, 1}, {-1, -1}, {0, -1}, {1, -1}};
+
+inline bool ms_solver() { return g_cfg.solver == SPH_SOLVER_MS_MODLR_DELTA || g_cfg.solver == SPH_SOLVER_MS_HLLC_DELTA; }
+
+// Particles whose rates are assembled and integrated: water; the moving-square
+// driver also integrates inlet/outlet particles (Single_step_compute.f90:273,
+// SPH_Time_Iteration.f90:316).
+inline bool integrated(int t) { return t == SPH_TYPE_WATER || (ms_solver() && t <= SPH_TYPE_INLET); }
 
 inline bool pair_allowed(int ti, int tj) {
     if (g_cfg.pair_rule == SPH_PAIRS_ONE_FLUID) return !(ti != SPH_TYPE_WATER && tj != SPH_TYPE_WATER);
@@ -365,8 +373,9 @@ void define_free_surface(const Particles& P, Rhs& R) {
         scatter<1>(n, R.I, &ti, &tj, &R.fra_v);
     }
     R.fs.assign(n, 0);
-    for (int i = 0; i < n; ++i)       // :119-131
-        if (P.type[i] == SPH_TYPE_WATER && R.fra_v[i] <= g_K.fs_thr) R.fs[i] = 1;
+    if (g_cfg.free_surface)           // :119-131 (MS: only with Has_FreeSurface_Or_Not)
+        for (int i = 0; i < n; ++i)
+            if (P.type[i] == SPH_TYPE_WATER && R.fra_v[i] <= g_K.fs_thr) R.fs[i] = 1;
     {   // :137-159  B(L,o) += (x_j-x_i)_L dwdx_o V ; sum_dwdx
         std::vector<double> ti[6], tj[6];
         for (int c = 0; c < 6; ++c) { ti[c].resize(np); tj[c].resize(np); }
@@ -394,7 +403,8 @@ void define_free_surface(const Particles& P, Rhs& R) {
     for (int c = 0; c < 4; ++c) R.binv[c].assign(n, (c == 0 || c == 3) ? 1.0 : 0.0);
     R.n_singular = 0;
     for (int i = 0; i < n; ++i) {
-        if (P.type[i] != SPH_TYPE_WATER) continue;
+        // MS also inverts for outlet particles (MS Define_freesurface...f90:131)
+        if (!(P.type[i] == SPH_TYPE_WATER || (ms_solver() && P.type[i] == -202))) continue;
         double A[2][2] = {{R.B[0][i], R.B[1][i]}, {R.B[2][i], R.B[3][i]}}, Rm[2][2];
         int ok = inv2(A, Rm);
         if (!ok) { R.n_singular++; continue; }
@@ -695,6 +705,215 @@ void riemann_solver(const Particles& P, Rhs& R, bool muscl) {
     }
 }
 
+// The moving-square solvers: Moving_Square.../Solver_Normalized_Modified_Linear_Riemann_Delta.f90
+// and Solver_Normalized_HLLC_Riemann_Delta.f90 (no SPS; XSPH average velocity
+// computed first and added to the continuity flux; laplacianTerm switch), with
+// the assembly of Moving_Square.../Single_step_compute.f90:253-283.
+void ms_riemann_solver(const Particles& P, Rhs& R, bool hllc) {
+    const int n = P.n;
+    const PairList& L = R.L;
+    const size_t np = L.size();
+    const sph_config& C = g_cfg;
+    const double hbar = (C.h + C.h) / 2.0;
+    gradients(P, R, false);                        // grad rho with the normalised gradients (:100-112)
+    {   // XSPH average velocity (:114-121)
+        std::vector<double> ti[2], tj[2];
+        for (int c = 0; c < 2; ++c) { ti[c].resize(np); tj[c].resize(np); resize_zero(R.avg[c], n); }
+        #pragma omp parallel for
+        for (size_t k = 0; k < np; ++k) {
+            const int i = L.pi[k], j = L.pj[k];
+            const double vd[2] = {P.u[i] - P.u[j], P.v[i] - P.v[j]};
+            for (int a = 0; a < 2; ++a) {
+                ti[a][k] = -(C.xsph_eps * P.mass[j] * vd[a] / (P.rho[i] + P.rho[j]) * L.w[k]);
+                tj[a][k] = C.xsph_eps * P.mass[i] * vd[a] / (P.rho[i] + P.rho[j]) * L.w[k];
+            }
+        }
+        scatter<2>(n, R.I, ti, tj, R.avg);
+    }
+    // channels: 0 cont, 1-2 internal, 3-4 AV, 5-6 laplacian, 7-8 art_int
+    const int NT = 9;
+    std::vector<double> ti[NT], tj[NT];
+    for (int c = 0; c < NT; ++c) { ti[c].assign(np, 0.0); tj[c].assign(np, 0.0); }
+    #pragma omp parallel for schedule(static)
+    for (size_t k = 0; k < np; ++k) {
+        const int i = L.pi[k], j = L.pj[k];
+        const double Vi = R.vol[i], Vj = R.vol[j];
+        const double ri = P.rho[i], rj = P.rho[j];
+        const double ndi[2] = {R.ndwi0[k], R.ndwi1[k]}, ndj[2] = {R.ndwj0[k], R.ndwj1[k]};
+        const double cbar = (R.c[i] + R.c[j]) / 2.0;
+        const double rbar = (ri + rj) / 2.0;
+        const double PL = R.p[i], PR = R.p[j], Pbar = (PL + PR) / 2.0;
+        const double vI[2] = {P.u[i], P.v[i]}, vJ[2] = {P.u[j], P.v[j]};
+        const double vbar[2] = {(vI[0] + vJ[0]) / 2.0, (vI[1] + vJ[1]) / 2.0};
+        const double xij[2] = {L.dx0[k], L.dx1[k]};
+        const double d = std::sqrt(xij[0] * xij[0] + xij[1] * xij[1]);
+        const double e[2] = {-xij[0] / d, -xij[1] / d};
+        double vs[2], Ps;
+        if (!hllc) {
+            double UL = vI[0] * e[0] + vI[1] * e[1];
+            double UR = vJ[0] * e[0] + vJ[1] * e[1];
+            double Ubar = (UL + UR) / 2.0;
+            double Us = Ubar + 0.5 * (PL - PR) / (rbar * g_K.sqrt_c0);
+            vs[0] = (Us - Ubar) * e[0] + vbar[0]; vs[1] = (Us - Ubar) * e[1] + vbar[1];
+            double bR = std::min(3.0 * (std::max((UL - UR), 0.0)), cbar);
+            Ps = Pbar + 0.5 * bR * rbar * (UL - UR);
+        } else {
+            // Solver_Normalized_HLLC_Riemann_Delta.f90:207-322
+            const double T[2][2] = {{e[0], e[1]}, {-e[1], e[0]}};
+            const double VL[2] = {T[0][0] * vI[0] + T[0][1] * vI[1], T[1][0] * vI[0] + T[1][1] * vI[1]};
+            const double VR[2] = {T[0][0] * vJ[0] + T[0][1] * vJ[1], T[1][0] * vJ[0] + T[1][1] * vJ[1]};
+            const double V0 = T[0][0] * vbar[0] + T[0][1] * vbar[1];
+            const double rL = ri, rR = rj, cL = R.c[i], cR = R.c[j];
+            const double Us = (VR[0] * cL * rL + VL[0] * cR * rR + PL - PR) / (rL * cL + rR * cR);
+            double Pst = (PR * cL * rL + PL * cR * rR - cL * rL * cR * rR * (VR[0] - VL[0])) / (rL * cL + rR * cR);
+            const double rst = (Pst - C.background_p) / C.c0sq + C.rho0;
+            double QL = 1.0, QR = 1.0;
+            if (!(Pst <= PL) && rL > rst) QL = std::sqrt((rst / rL) * (Pst - PL) / (rL - rst)) / cL;
+            const double SL = VL[0] - cL * QL;
+            if (!(Pst <= PR) && rR > rst) QR = std::sqrt((rst / rR) * (Pst - PR) / (rR - rst)) / cR;
+            const double SR = VR[0] + cR * QR;
+            const double Sst = Us, xt = V0;
+            double rH, VH[2];
+            if (SL > xt) { rH = rL; VH[0] = VL[0]; VH[1] = VL[1]; }
+            else if (Sst >= xt && xt >= SL) {
+                double q = rL * ((SL - VL[0]) / (SL - Sst));
+                rH = q; VH[0] = (Sst * q) / rH; VH[1] = (VL[1] * q) / rH;
+            } else if (SR >= xt && xt >= Sst) {
+                double q = rR * ((SR - VR[0]) / (SR - Sst));
+                rH = q; VH[0] = (Sst * q) / rH; VH[1] = (VR[1] * q) / rH;
+            } else { rH = rR; VH[0] = VR[0]; VH[1] = VR[1]; }
+            vs[0] = T[0][0] * VH[0] + T[1][0] * VH[1];
+            vs[1] = T[0][1] * VH[0] + T[1][1] * VH[1];
+            Ps = C.c0sq * (rH - C.rho0) + C.background_p;
+        }
+        double vIs[2], vJs[2], IPs, JPs;
+        if (R.near[i] == 1) { vIs[0] = vbar[0]; vIs[1] = vbar[1]; IPs = Pbar; }
+        else { vIs[0] = vs[0]; vIs[1] = vs[1]; IPs = Ps; }
+        if (R.near[j] == 1) { vJs[0] = vbar[0]; vJs[1] = vbar[1]; JPs = Pbar; }
+        else { vJs[0] = vs[0]; vJs[1] = vs[1]; JPs = Ps; }
+        double vdi[2] = {vI[0] - vIs[0] + R.avg[0][i] - R.avg[0][j], vI[1] - vIs[1] + R.avg[1][i] - R.avg[1][j]};
+        double vdj[2] = {vJ[0] - vJs[0] + R.avg[0][j] - R.avg[0][i], vJ[1] - vJs[1] + R.avg[1][j] - R.avg[1][i]};
+        double tmi = vdi[0] * ndi[0] + vdi[1] * ndi[1];
+        double tmj = -(vdj[0] * ndj[0] + vdj[1] * ndj[1]);
+        ti[0][k] = 2 * ri * Vj * tmi;
+        tj[0][k] = 2 * rj * Vi * tmj;
+        double rho_ij = 1.0 / (ri * rj);
+        for (int a = 0; a < 2; ++a) {
+            ti[1 + a][k] = P.mass[j] * (-2 * IPs * ndi[a] * rho_ij);
+            tj[1 + a][k] = -(P.mass[i] * (-2 * JPs * ndj[a] * rho_ij));
+        }
+        double vij[2] = {P.u[i] - P.u[j], P.v[i] - P.v[j]};
+        double r2 = xij[0] * xij[0] + xij[1] * xij[1];
+        double vx = vij[0] * xij[0] + vij[1] * xij[1];
+        if (vx < 0.0) {
+            double fh = C.fai * hbar;
+            double phi1 = hbar * vx / (r2 + fh * fh);
+            double Pi = (-C.alpha * cbar * phi1 + C.beta * (phi1 * phi1)) / rbar;
+            for (int a = 0; a < 2; ++a) {
+                ti[3 + a][k] = P.mass[j] * (-Pi * ndi[a]);
+                tj[3 + a][k] = -(P.mass[i] * (-Pi * ndj[a]));
+            }
+        }
+        if (C.laplacian == 1) {
+            double rdi = xij[0] * ndi[0] + xij[1] * ndi[1];
+            double rdj = xij[0] * ndj[0] + xij[1] * ndj[1];
+            for (int a = 0; a < 2; ++a) {
+                ti[5 + a][k] = Vj * 2 * C.nu * rdi / r2 * vij[a];
+                tj[5 + a][k] = -(Vi * 2 * C.nu * rdj / r2 * vij[a]);
+            }
+        } else {
+            for (int a = 0; a < 2; ++a) {
+                ti[5 + a][k] = Vj * 2 * (2 + 2) * C.nu * vx / r2 * ndi[a];
+                tj[5 + a][k] = -(Vi * 2 * (2 + 2) * C.nu * vx / r2 * ndj[a]);
+            }
+        }
+        double tt = C.delta_alpha * hbar * cbar * vx / r2;
+        for (int a = 0; a < 2; ++a) {
+            ti[7 + a][k] = tt * ndi[a] * C.rho0 / ri * Vj;
+            tj[7 + a][k] = -(tt * ndj[a] * C.rho0 / rj * Vi);
+        }
+    }
+    std::vector<double> cont(n, 0.0), accs[8];
+    for (int c = 0; c < 8; ++c) resize_zero(accs[c], n);
+    scatter<1>(n, R.I, &ti[0], &tj[0], &cont);
+    scatter<8>(n, R.I, &ti[1], &tj[1], accs);
+    // delta-SPH (:531-545)
+    std::vector<double> dti(np), dtj(np), corr(n, 0.0);
+    #pragma omp parallel for schedule(static)
+    for (size_t k = 0; k < np; ++k) {
+        const int i = L.pi[k], j = L.pj[k];
+        double pd[2] = {-L.dx0[k], -L.dx1[k]};
+        double r2 = pd[0] * pd[0] + pd[1] * pd[1];
+        double drho = -(P.rho[i] - P.rho[j]);
+        double sg0 = R.grho[0][i] + R.grho[0][j], sg1 = R.grho[1][i] + R.grho[1][j];
+        double psi = drho - 0.5 * (sg0 * pd[0] + sg1 * pd[1]);
+        double tmi = (pd[0] * R.ndwi0[k] + pd[1] * R.ndwi1[k]) / r2;
+        double tmj = (pd[0] * R.ndwj0[k] + pd[1] * R.ndwj1[k]) / r2;
+        double cbar = (R.c[i] + R.c[j]) / 2.0;
+        dti[k] = 2 * C.delta * hbar * cbar * psi * tmi * R.vol[j];
+        dtj[k] = -(2 * C.delta * hbar * cbar * psi * tmj * R.vol[i]);
+    }
+    scatter<1>(n, R.I, &dti, &dtj, &corr);
+    R.drho.assign(n, 0.0);
+    for (int a = 0; a < 2; ++a) R.acc[a].assign(n, 0.0);
+    for (int i = 0; i < n; ++i) {
+        R.drho[i] = cont[i];
+        if (!integrated(P.type[i])) continue;
+        for (int a = 0; a < 2; ++a)
+            R.acc[a][i] = accs[0 + a][i] + 0.0 + accs[2 + a][i] + accs[6 + a][i] + 0.0 + accs[4 + a][i];
+        R.drho[i] = R.drho[i] + corr[i];
+    }
+}
+
+// Calculate_Body_Force (Moving_Square.../Calculate_Body_Force.f90:53-142) and the
+// sums of Moving_Square.../Single_step_compute.f90:228-243 (no gravity).
+void body_force(const Particles& P, const Rhs& R, double out[6]) {
+    const int n = P.n;
+    const PairList& L = R.L;
+    std::vector<double> bp[2], bv[2];
+    for (int c = 0; c < 2; ++c) { bp[c].assign(n, 0.0); bv[c].assign(n, 0.0); }
+    std::vector<int> nearb(n, 0);
+    const double nu = g_cfg.nu;
+    for (size_t k = 0; k < L.size(); ++k) {
+        const int i = L.pi[k], j = L.pj[k];
+        if (P.itype[i] != SPH_TYPE_BODY && P.itype[j] != SPH_TYPE_BODY) continue;
+        double vij[2] = {P.u[i] - P.u[j], P.v[i] - P.v[j]};
+        double xij[2] = {L.dx0[k], L.dx1[k]};
+        double r2 = xij[0] * xij[0] + xij[1] * xij[1];
+        double vx = vij[0] * xij[0] + vij[1] * xij[1];
+        double ndi[2] = {R.ndwi0[k], R.ndwi1[k]}, ndj[2] = {R.ndwj0[k], R.ndwj1[k]};
+        if (P.itype[j] == SPH_TYPE_BODY) {
+            nearb[i] = 1;
+            for (int a = 0; a < 2; ++a) bp[a][i] = bp[a][i] - R.vol[j] * (R.p[i] + R.p[j]) * ndi[a];
+            if (g_cfg.laplacian == 1) {
+                double rd = xij[0] * ndi[0] + xij[1] * ndi[1];
+                for (int a = 0; a < 2; ++a) bv[a][i] = bv[a][i] + P.rho[i] * R.vol[j] * 2 * nu * rd / r2 * vij[a];
+            } else {
+                for (int a = 0; a < 2; ++a) bv[a][i] = bv[a][i] + P.rho[i] * R.vol[j] * 2 * (2 + 2) * nu * vx / r2 * ndi[a];
+            }
+        }
+        if (P.itype[i] == SPH_TYPE_BODY) {
+            nearb[j] = 1;
+            for (int a = 0; a < 2; ++a) bp[a][j] = bp[a][j] + R.vol[i] * (R.p[i] + R.p[j]) * ndj[a];
+            if (g_cfg.laplacian == 1) {
+                double rd = xij[0] * ndj[0] + xij[1] * ndj[1];
+                for (int a = 0; a < 2; ++a) bv[a][j] = bv[a][j] - P.rho[j] * R.vol[i] * 2 * nu * rd / r2 * vij[a];
+            } else {
+                for (int a = 0; a < 2; ++a) bv[a][j] = bv[a][j] - P.rho[j] * R.vol[i] * 2 * (2 + 2) * nu * vx / r2 * ndj[a];
+            }
+        }
+    }
+    for (int c = 0; c < 6; ++c) out[c] = 0.0;
+    for (int i = 0; i < n; ++i) {
+        if (!nearb[i]) continue;
+        for (int a = 0; a < 2; ++a) {
+            out[0 + a] = out[0 + a] + R.vol[i] * bp[a][i];
+            out[2 + a] = out[2 + a] + R.vol[i] * bv[a][i];
+            out[4 + a] = out[4 + a] + R.vol[i] * (bp[a][i] + bv[a][i] + 0.0);
+        }
+    }
+}
+
 // single_step_compute (Taylor_Green_Vortex/single_step_compute.f90:62-171).
 void single_step_compute(const Particles& P, Rhs& R) {
     const int n = P.n;
@@ -710,6 +929,11 @@ void single_step_compute(const Particles& P, Rhs& R) {
     build_incidence(n, R.L, R.I);
     define_free_surface(P, R);
     normalized_gradients(R);
+    if (ms_solver()) {
+        for (int c = 0; c < 3; ++c) { resize_zero(R.S[c], n); resize_zero(R.tau[c], n); }
+        ms_riemann_solver(P, R, g_cfg.solver == SPH_SOLVER_MS_HLLC_DELTA);
+        return;
+    }
     const bool muscl = g_cfg.solver == SPH_SOLVER_MUSCL_DELTA_SPS;
     if (muscl) gradients(P, R, true);
     sps_stress(P, R);
@@ -762,7 +986,7 @@ void periodic_images(const Particles& H, Particles& P) {
         P.resize(m + 1);
         P.x[m] = nx; P.y[m] = ny; P.u[m] = P.u[i]; P.v[m] = P.v[i];
         P.rho[m] = P.rho[i]; P.mass[m] = P.mass[i]; P.smass[m] = P.smass[i];
-        P.type[m] = SPH_TYPE_PERIODIC;
+        P.type[m] = SPH_TYPE_PERIODIC; P.itype[m] = SPH_TYPE_PERIODIC;
         P.src[m] = (i < H.n) ? i : P.src[i];
     };
     for (int i = 0; i < H.n; ++i) {
@@ -797,7 +1021,63 @@ struct Sim {
     long long step = 0;               // completed steps
     Rhs last;
     int last_images = 0;
+    double bf[6] = {0, 0, 0, 0, 0, 0};   // body force of the last RHS
 };
+
+// Euler predictor-corrector of Moving_Square.../SPH_Time_Iteration.f90:304-334
+// (Iteration_Method 2): one RHS per step after the first, rates of the last RHS
+// reused for the predictor.
+void run_step_euler_pc(Sim& S, double dt) {
+    const int n = S.H.n;
+    if (g_cfg.periodic) wrap_periodic(S.H);
+    Particles P;
+    if (g_cfg.periodic) periodic_images(S.H, P);
+    else { P = S.H; for (int i = 0; i < n; ++i) P.src[i] = -1; }
+    S.last_images = P.n - n;
+    const Particles B0 = P;
+    Rhs R;
+    if (S.step == 0) {
+        single_step_compute(P, R);
+    } else {
+        R.drho.assign(P.n, 0.0);
+        for (int a = 0; a < 2; ++a) { R.acc[a].assign(P.n, 0.0); R.avg[a].assign(P.n, 0.0); }
+        for (int i = 0; i < n; ++i) {
+            R.drho[i] = S.rdrho[i]; R.acc[0][i] = S.racc0[i]; R.acc[1][i] = S.racc1[i];
+            R.avg[0][i] = S.ravg0[i]; R.avg[1][i] = S.ravg1[i];
+        }
+    }
+    std::vector<double> td(n), ta0(n), ta1(n), tv0(n), tv1(n);
+    for (int i = 0; i < n; ++i) { td[i] = R.drho[i]; ta0[i] = R.acc[0][i]; ta1[i] = R.acc[1][i]; tv0[i] = P.u[i]; tv1[i] = P.v[i]; }
+    for (int i = 0; i < n; ++i) {
+        if (!integrated(P.type[i])) continue;
+        P.rho[i] = B0.rho[i] + R.drho[i] * dt;
+        P.x[i] = B0.x[i] + dt * (P.u[i] + R.avg[0][i]) + 0.5 * R.acc[0][i] * (dt * dt);
+        P.y[i] = B0.y[i] + dt * (P.v[i] + R.avg[1][i]) + 0.5 * R.acc[1][i] * (dt * dt);
+        P.u[i] = B0.u[i] + dt * R.acc[0][i];
+        P.v[i] = B0.v[i] + dt * R.acc[1][i];
+    }
+    single_step_compute(P, R);
+    if (g_cfg.solver == SPH_SOLVER_MS_MODLR_DELTA || g_cfg.solver == SPH_SOLVER_MS_HLLC_DELTA) body_force(P, R, S.bf);
+    for (int i = 0; i < n; ++i) {
+        if (!integrated(P.type[i])) continue;
+        P.rho[i] = B0.rho[i] + 0.5 * (R.drho[i] + td[i]) * dt;
+        P.x[i] = B0.x[i] + 0.5 * dt * (P.u[i] + tv0[i]) + R.avg[0][i] * dt + 0.5 * R.acc[0][i] * (dt * dt);
+        P.y[i] = B0.y[i] + 0.5 * dt * (P.v[i] + tv1[i]) + R.avg[1][i] * dt + 0.5 * R.acc[1][i] * (dt * dt);
+        P.u[i] = B0.u[i] + 0.5 * dt * (R.acc[0][i] + ta0[i]);
+        P.v[i] = B0.v[i] + 0.5 * dt * (R.acc[1][i] + ta1[i]);
+    }
+    S.rdrho.assign(R.drho.begin(), R.drho.begin() + n);
+    S.racc0.assign(R.acc[0].begin(), R.acc[0].begin() + n);
+    S.racc1.assign(R.acc[1].begin(), R.acc[1].begin() + n);
+    S.ravg0.assign(R.avg[0].begin(), R.avg[0].begin() + n);
+    S.ravg1.assign(R.avg[1].begin(), R.avg[1].begin() + n);
+    if (g_cfg.shifting) shift_particles(P, n, R);
+    for (int i = 0; i < n; ++i) {
+        S.H.x[i] = P.x[i]; S.H.y[i] = P.y[i]; S.H.u[i] = P.u[i]; S.H.v[i] = P.v[i]; S.H.rho[i] = P.rho[i];
+    }
+    S.last = std::move(R);
+    S.step++;
+}
 
 // One time step of time_iteration.f90:781-1073 (Runge-Kutta branch): stage
 // updates :942-1047, then Shift_particle_position with the last RHS pair data.
@@ -862,6 +1142,7 @@ void run_step(Sim& S, double dt) {
     }
     save(K3r, K3a0, K3a1, K3v0, K3v1, R.drho, R.acc[0], R.acc[1]);
     single_step_compute(P, R);
+    if (ms_solver()) body_force(P, R, S.bf);
     for (int i = 0; i < n; ++i) {
         if (P.type[i] != SPH_TYPE_WATER) continue;
         P.rho[i] = B0.rho[i] + (K1r[i] + 2 * K2r[i] + 2 * K3r[i] + R.drho[i]) * dt / 6.0;
@@ -894,7 +1175,7 @@ Particles make_particles(int n, const double* pos, const double* vel, const doub
         H.u[i] = vel[i]; H.v[i] = vel[n + i];
         H.rho[i] = rho[i]; H.mass[i] = mass[i];
         H.smass[i] = smass ? smass[i] : mass[i];
-        H.type[i] = type[i]; H.src[i] = -1;
+        H.type[i] = type[i]; H.itype[i] = type[i]; H.src[i] = -1;
     }
     return H;
 }
@@ -1039,7 +1320,35 @@ int oracle_run(void* h, int nsteps, double dt) {
     Sim* S = (Sim*)h;
     g_cfg = S->cfg;
     derive_consts(S->cfg);
-    for (int s = 0; s < nsteps; ++s) run_step(*S, dt);
+    for (int s = 0; s < nsteps; ++s) {
+        if (S->cfg.integrator == SPH_INTEGRATOR_EULER_PC) run_step_euler_pc(*S, dt);
+        else run_step(*S, dt);
+    }
+    return 0;
+}
+
+int oracle_set_initial_type(void* h, int n, const int* itype) {
+    Sim* S = (Sim*)h;
+    if (n != S->H.n) return -1;
+    for (int i = 0; i < n; ++i) S->H.itype[i] = itype[i];
+    return 0;
+}
+
+void oracle_body_force(void* h, double* out) {
+    Sim* S = (Sim*)h;
+    for (int c = 0; c < 6; ++c) out[c] = S->bf[c];
+}
+
+// Body force of one RHS on exactly the given particles (itype: initial types).
+int oracle_rhs_body_force(const sph_config* cfg, int n, const double* pos, const double* vel, const double* rho,
+                          const double* mass, const int* type, const int* itype, double* out) {
+    g_cfg = *cfg;
+    derive_consts(*cfg);
+    Particles P = make_particles(n, pos, vel, rho, mass, type, nullptr);
+    for (int i = 0; i < n; ++i) P.itype[i] = itype[i];
+    Rhs R;
+    single_step_compute(P, R);
+    body_force(P, R, out);
     return 0;
 }
 

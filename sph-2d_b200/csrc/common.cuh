@@ -22,6 +22,7 @@ enum : unsigned {
 struct Params {
     // switches
     int kernel_model, solver, renorm, quirks, pair_rule, shifting, muscl, xsph;
+    int ms, hllc, laplacian, free_surface, integrator, has_body;
     // kernel / pair search
     double h, r_cut, cut_min, kfactor, gauss_e9, q_zero;
     double r2_list;          // squared neighbour-list radius (support * (1 + skin))
@@ -56,6 +57,13 @@ template <> __host__ __device__ inline float2 mk2<float>(float a, float b) { ret
 template <typename R> __host__ __device__ inline typename VT<R>::V4 mk4(R a, R b, R c, R d);
 template <> __host__ __device__ inline double4 mk4<double>(double a, double b, double c, double d) { return make_double4(a, b, c, d); }
 template <> __host__ __device__ inline float4 mk4<float>(float a, float b, float c, float d) { return make_float4(a, b, c, d); }
+
+// Particles whose rates are assembled and integrated: water; the moving-square
+// driver also integrates inlet/outlet particles (Moving_Square.../Single_step_compute.f90:273,
+// SPH_Time_Iteration.f90:316).
+__device__ __forceinline__ bool integrated(const Params& P, int t) {
+    return t == SPH_TYPE_WATER || (P.ms && t <= SPH_TYPE_INLET);
+}
 
 __device__ __forceinline__ double pw3(double x) { return x * x * x; }
 __device__ __forceinline__ double pw4(double x) { double x2 = x * x; return x2 * x2; }

@@ -34,6 +34,10 @@ __global__ void __launch_bounds__(128) k_pass_a(Params P, Sorted<R> D) {
     R fra = R(0), b00 = R(0), b01 = R(0), b10 = R(0), b11 = R(0);
     R g[8];
     for (int c = 0; c < 8; ++c) g[c] = R(0);
+    // moving-square solvers: XSPH average velocity, computed before their main
+    // loop (Solver_Normalized_..._Delta.f90:114-121):
+    //   avg_a = -epsilon sum_b m_b (v_a - v_b) / (rho_a + rho_b) W_ab
+    R xs0 = R(0), xs1 = R(0);
     const R inv_h = (R)(1.0 / P.h);
     const R r2cut = (R)(P.r_cut * P.r_cut), r2min = (R)(P.cut_min * P.cut_min);
     int np = 0;
@@ -65,18 +69,27 @@ __global__ void __launch_bounds__(128) k_pass_a(Params P, Sorted<R> D) {
         ++np;
         const R dx = (R)dxd, dy = (R)dyd;
         // grad_a W = g(d) (x_a - x_b)  (compute_kernel)
-        R gs;
+        R gs, wk;
         {
             const R q = d * inv_h;
             const R kf = (R)P.kfactor;
             if (P.kernel_model == SPH_KERNEL_GAUSSIAN) {
-                gs = exp(-(q * q)) * (R(-2) * q) * inv_d * inv_h * kf;
+                const R ex = exp(-(q * q));
+                wk = (ex - (R)P.gauss_e9) * kf;
+                gs = ex * (R(-2) * q) * inv_d * inv_h * kf;
             } else {
                 const R t = R(1) - R(0.5) * q;
-                gs = kf * (R(-5) * q * (t * t * t)) * inv_d * inv_h;
+                const R t3 = t * t * t;
+                wk = kf * (R(1) + R(2) * q) * (t3 * t);
+                gs = kf * (R(-5) * q * t3) * inv_d * inv_h;
             }
         }
         const double4 kb = D.kin[b];
+        if (P.ms) {
+            const R f = (R)P.eps * D.aux[b].x / (R)(ka.z + kb.z) * wk;
+            xs0 -= f * (R)(ka.x - kb.x);
+            xs1 -= f * (R)(ka.y - kb.y);
+        }
         const R Vb = D.aux[b].y;
         const R gx = gs * dx * Vb, gy = gs * dy * Vb;    // V_b grad_a W
         // volume fraction (Define_freesurface...f90:84-85)
@@ -102,7 +115,8 @@ __global__ void __launch_bounds__(128) k_pass_a(Params P, Sorted<R> D) {
     // function_module.f90:190-204); the reference keeps the identity on success
     // (Define_freesurface...f90:180-186) unless renormalisation is switched on.
     double i00 = 1.0, i01 = 0.0, i10 = 0.0, i11 = 1.0;
-    if (ta == SPH_TYPE_WATER && P.renorm) {
+    // the moving-square variant also inverts for outlet particles (MS Define_freesurface...f90:131)
+    if ((ta == SPH_TYPE_WATER || (P.ms && ta == -202)) && P.renorm) {
         double a1 = (double)b00, bb1 = (double)b01, a2 = (double)b10, bb2 = (double)b11;
         double det = (a1 * bb2 - bb1 * a2);
         if (det != 0) { i00 = bb2 / det; i01 = -bb1 / det; i10 = -a2 / det; i11 = a1 / det; }
@@ -118,7 +132,7 @@ __global__ void __launch_bounds__(128) k_pass_a(Params P, Sorted<R> D) {
     }
     // SPS stress for water particles (:256-296)
     R txx = R(0), txy = R(0), tyy = R(0);
-    if (ta == SPH_TYPE_WATER) {
+    if (ta == SPH_TYPE_WATER && !P.ms) {
         const double sxx = (double)gr[4], sxy = (double)gr[5] + (double)gr[6], syy = (double)gr[7];
         const double abs2 = 2 * (sxx * sxx + syy * syy) + sxy * sxy;
         const double DL = P.sps_dl;               // SPS_Delta_L = sqrt(2.0)/2.0*interior_dx (host-side product)
@@ -137,8 +151,9 @@ __global__ void __launch_bounds__(128) k_pass_a(Params P, Sorted<R> D) {
     const R fv = fra;
     D.fra_v[a] = fv;
     uint8_t fl = 0;
-    if (ta == SPH_TYPE_WATER && (double)fv <= P.fs_thr) fl = 4;   // surface candidate (:123)
+    if (P.free_surface && ta == SPH_TYPE_WATER && (double)fv <= P.fs_thr) fl = 4;   // surface candidate (:123)
     D.flags[a] = fl;
+    if (P.ms) D.avg[a] = mk2<R>(xs0, xs1);
 }
 
 // Geometric free-surface test of the candidates (Define_freesurface...f90:295-376):

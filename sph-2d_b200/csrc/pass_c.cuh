@@ -82,7 +82,11 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_pass_c(Params P
     const R rho_a = (R)S.kin.z;
     const V4 bi = D.binv[a];
     const bool near_a = (D.flags[a] & 2) != 0;
-    const bool water = ta == SPH_TYPE_WATER;   // delta-SPH only enters water rates (Solver :627-635)
+    // delta-SPH and the assembly only apply to integrated particles (Solver :627-635,
+    // Moving_Square.../Single_step_compute.f90:273-281)
+    const bool water = integrated(P, ta);
+    typename VT<R>::V2 avg_a = mk2<R>(R(0), R(0));
+    if (P.ms) avg_a = D.avg[a];
 
     const R hbar = (R)P.h;
     const R inv_h = (R)(1.0 / P.h);
@@ -175,17 +179,59 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_pass_c(Params P
         }
         // U_L - U_R and P_L - P_R from the differences
         const R dU = (du + lui + luj) * e0 + (dv + lvi + lvj) * e1;
-        const R dP = dp + lpi + lpj;
-        const R sU = R(0.5) * dP * (inv_rbar * inv_sqc0);               // U* - Ubar
-        const R bR = min(R(3) * (max(dU, R(0))), cbar);
         const R Pbar = R(0.5) * ((R)I.kin.w + (R)J.kin.w);
-        const R Ps = Pbar + R(0.5) * bR * rbar * dU;
-        const R PA = near_a ? Pbar : Ps;
-        // this side's velocity minus its star velocity (near-surface: the average)
-        R wa0, wa1;
+        R PA, wa0, wa1;          // this side's star pressure and velocity minus star velocity
         if (a_is_i) { wa0 = R(0.5) * du + lui; wa1 = R(0.5) * dv + lvi; }
         else { wa0 = R(-0.5) * du - luj; wa1 = R(-0.5) * dv - lvj; }
-        if (!near_a) { wa0 -= sU * e0; wa1 -= sU * e1; }
+        if (!P.hllc) {
+            const R dP = dp + lpi + lpj;
+            const R sU = R(0.5) * dP * (inv_rbar * inv_sqc0);               // U* - Ubar
+            const R bR = min(R(3) * (max(dU, R(0))), cbar);
+            const R Ps = Pbar + R(0.5) * bR * rbar * dU;
+            PA = near_a ? Pbar : Ps;
+            if (!near_a) { wa0 -= sU * e0; wa1 -= sU * e1; }
+        } else if (near_a) {
+            PA = Pbar;
+        } else {
+            // HLLC in the pair frame (Moving_Square.../Solver_Normalized_HLLC_Riemann_Delta.f90:207-322),
+            // in FP64 in both paths: rho* and P* = c0^2 (rho_HLLC - rho0) are differences of O(1) numbers
+            const double ed0 = -(a_is_i ? dxd : -dxd) / sqrt(dxd * dxd + dyd * dyd);
+            const double ed1 = -(a_is_i ? dyd : -dyd) / sqrt(dxd * dxd + dyd * dyd);
+            const double uI = I.kin.x, vI = I.kin.y, uJ = J.kin.x, vJ = J.kin.y;
+            const double VL0 = ed0 * uI + ed1 * vI, VL1 = -ed1 * uI + ed0 * vI;
+            const double VR0 = ed0 * uJ + ed1 * vJ, VR1 = -ed1 * uJ + ed0 * vJ;
+            const double V0 = ed0 * (0.5 * (uI + uJ)) + ed1 * (0.5 * (vI + vJ));
+            const double rL = I.kin.z, rR = J.kin.z, cL = (double)I.aux.z, cR = (double)J.aux.z;
+            const double PLd = I.kin.w, PRd = J.kin.w;
+            const double den = rL * cL + rR * cR;
+            const double Us = (VR0 * cL * rL + VL0 * cR * rR + PLd - PRd) / den;
+            const double Pst = (PRd * cL * rL + PLd * cR * rR - cL * rL * cR * rR * (VR0 - VL0)) / den;
+            const double rst = (Pst - P.pb) / P.c0sq + P.rho0;
+            double QL = 1.0, QR = 1.0;
+            if (!(Pst <= PLd) && rL > rst) QL = sqrt((rst / rL) * (Pst - PLd) / (rL - rst)) / cL;
+            const double SL = VL0 - cL * QL;
+            if (!(Pst <= PRd) && rR > rst) QR = sqrt((rst / rR) * (Pst - PRd) / (rR - rst)) / cR;
+            const double SR = VR0 + cR * QR;
+            double rH, VH0, VH1;
+            if (SL > V0) { rH = rL; VH0 = VL0; VH1 = VL1; }
+            else if (Us >= V0 && V0 >= SL) {
+                const double q = rL * ((SL - VL0) / (SL - Us));
+                rH = q; VH0 = (Us * q) / rH; VH1 = (VL1 * q) / rH;
+            } else if (SR >= V0 && V0 >= Us) {
+                const double q = rR * ((SR - VR0) / (SR - Us));
+                rH = q; VH0 = (Us * q) / rH; VH1 = (VR1 * q) / rH;
+            } else { rH = rR; VH0 = VR0; VH1 = VR1; }
+            const double vs0 = ed0 * VH0 - ed1 * VH1, vs1 = ed1 * VH0 + ed0 * VH1;
+            PA = (R)(P.c0sq * (rH - P.rho0) + P.pb);
+            const double4& K = a_is_i ? I.kin : J.kin;
+            wa0 = (R)(K.x - vs0);
+            wa1 = (R)(K.y - vs1);
+        }
+        if (P.ms) {      // XSPH velocities inside the continuity flux (MS solvers :199-202)
+            const typename VT<R>::V2 avg_b = D.avg[b];
+            wa0 += avg_a.x - avg_b.x;
+            wa1 += avg_a.y - avg_b.y;
+        }
         const R Vb = T.aux.y, mb = T.aux.x;
         // continuity (:360-369)
         R dr = R(2) * rho_a * Vb * (sgn * (wa0 * nd0 + wa1 * nd1));
@@ -202,27 +248,36 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_pass_c(Params P
             tx += mb * (-Pi * nd0);
             ty += mb * (-Pi * nd1);
         }
-        // Morris laplacian (:432-436)
-        const R lf = Vb * nu2 * (xij0 * nd0 + xij1 * nd1) * inv_r2;
-        tx += lf * du;
-        ty += lf * dv;
+        if (!P.ms || P.laplacian == 1) {
+            // Morris laplacian (:432-436)
+            const R lf = Vb * nu2 * (xij0 * nd0 + xij1 * nd1) * inv_r2;
+            tx += lf * du;
+            ty += lf * dv;
+        } else {
+            // laplacianTerm 0 (Moving_Square.../Solver_..._Delta.f90:315-318): 2 (dim+2) nu V (v.x)/r^2 grad W
+            const R lf = Vb * R(4) * nu2 * vx * inv_r2;
+            tx += lf * nd0;
+            ty += lf * nd1;
+        }
         // delta-alpha artificial internal acceleration (:442-446)
         const R tt = dla_h * cbar * vx * inv_r2 * rho0_over_rho_a * Vb;
         tx += tt * nd0;
         ty += tt * nd1;
         // SPS force, unnormalised dwdx and the neighbour's SPS mass (:450-492);
         // the reference does not reset temp_p between x and y (kept with quirks)
-        const R sxx = I.nb1.x + J.nb1.x, sxy = I.nb1.y + J.nb1.y, syy = I.nb1.z + J.nb1.z;
-        R tp = (sxx * dw0 + sxy * dw1) * rho_ij;
-        const R smb = T.aux.w;
-        tx += smb * tp;
-        if (!P.quirks) tp = R(0);
-        tp = (tp + syy * dw1 + sxy * dw0) * rho_ij;
-        ty += smb * tp;
+        if (!P.ms) {
+            const R sxx = I.nb1.x + J.nb1.x, sxy = I.nb1.y + J.nb1.y, syy = I.nb1.z + J.nb1.z;
+            R tp = (sxx * dw0 + sxy * dw1) * rho_ij;
+            const R smb = T.aux.w;
+            tx += smb * tp;
+            if (!P.quirks) tp = R(0);
+            tp = (tp + syy * dw1 + sxy * dw0) * rho_ij;
+            ty += smb * tp;
+        }
         accx.add(sgn * tx);
         accy.add(sgn * ty);
         // XSPH average velocity (:495-500; modified solver only)
-        if (!MUSCL && P.xsph) {
+        if (!MUSCL && P.xsph && !P.ms) {
             const R f = eps2 * mb * rcp(rho_i + rho_j) * w;
             xsx -= sgn * (f * du);
             xsy -= sgn * (f * dv);
@@ -266,7 +321,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_pass_c(Params P
     // assembly (single_step_compute.f90:152-171, Solver :627-635)
     D.drho[a] = cont.val();
     D.acc[a] = water ? mk2<R>(accx.val(), accy.val()) : mk2<R>(R(0), R(0));
-    D.avg[a] = mk2<R>(xsx, xsy);
+    if (!P.ms) D.avg[a] = mk2<R>(xsx, xsy);
     if (last_rhs) {
         const double4 b64 = D.binv64[a];
         const double c = -P.shift_beta * (P.h * P.h);

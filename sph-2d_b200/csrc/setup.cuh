@@ -15,6 +15,7 @@ struct Staging {
     double* mass;
     double* smass;    // mass the SPS force multiplies with (quirk A.6), default = mass
     int* type;
+    int* itype;       // initial type (body force), images get SPH_TYPE_PERIODIC
     // rates of the last RHS of the previous step (the reused K1), host particles only
     double* r_drho;
     double2* r_acc;
@@ -71,6 +72,7 @@ __global__ void k_img_emit(Params P, Staging S, int n_src, int axis, int base, c
         S.mass[o] = S.mass[i];
         S.smass[o] = S.smass[i];
         S.type[o] = SPH_TYPE_PERIODIC;
+        S.itype[o] = SPH_TYPE_PERIODIC;
         ++o;
     }
 }
@@ -101,6 +103,7 @@ struct Sorted {
     using V4 = typename VT<R>::V4;
     int* id;          // id-order index (host index, or n_host + image number)
     int* type;
+    int* itype;       // initial type (SPH_TYPE_BODY marks the body)
     double2* pos;     // current stage position (FP64)
     double2* pos0;    // step-start (master) position, also the list-build position
     double2* vel0;    // step-start velocity (FP64 master)
@@ -150,6 +153,7 @@ __global__ void k_gather_sorted(Params P, Staging S, Sorted<R> D, const unsigned
     int i = (int)perm[s];
     D.id[s] = i;
     D.type[s] = S.type[i];
+    D.itype[s] = S.itype[i];
     double2 x = S.pos[i];
     D.pos[s] = x;
     D.pos0[s] = x;
@@ -181,6 +185,7 @@ __global__ void k_unsort(Params P, Staging S, Sorted<R> D) {
     S.mass[i] = D.mass[s];
     S.smass[i] = D.smass[s];
     S.type[i] = D.type[s];
+    S.itype[i] = D.itype[s];
     S.r_drho[i] = (double)D.c_drho[s];
     S.r_acc[i] = make_double2((double)D.c_acc[s].x, (double)D.c_acc[s].y);
     S.r_avg[i] = make_double2((double)D.c_avg[s].x, (double)D.c_avg[s].y);

@@ -97,6 +97,9 @@ struct sph_handle {
     double t_total = 0;
     long long n_rhs = 0, n_steps = 0;
     long long launches = 0;
+    double bf[6] = {0, 0, 0, 0, 0, 0};   // body force of the last RHS
+    double* d_bf = nullptr;               // [6 * blocks(cap_tot) partials + 6]
+    bool bf_every_rhs = false;            // sph_rhs also reports it
 };
 
 namespace {
@@ -104,10 +107,11 @@ namespace {
 // --- configuration -> kernel parameters (mirrors the oracle's constants) ---
 int derive_params(const sph_config& c, Params& P) {
     if (c.kernel_model != SPH_KERNEL_GAUSSIAN && c.kernel_model != SPH_KERNEL_WENDLAND2) return SPH_E_CONFIG;
-    if (c.solver != SPH_SOLVER_MODLR_DELTA_SPS && c.solver != SPH_SOLVER_MUSCL_DELTA_SPS) return SPH_E_CONFIG;
+    if (c.solver < SPH_SOLVER_MODLR_DELTA_SPS || c.solver > SPH_SOLVER_MS_HLLC_DELTA) return SPH_E_CONFIG;
+    if (c.laplacian != 0 && c.laplacian != 1) return SPH_E_CONFIG;
     if (c.eos != SPH_EOS_TAIT && c.eos != SPH_EOS_LINEAR) return SPH_E_CONFIG;
     if (c.precision != SPH_PREC_FP64 && c.precision != SPH_PREC_MIXED) return SPH_E_CONFIG;
-    if (c.integrator != SPH_INTEGRATOR_RK4_REUSE) return SPH_E_CONFIG;
+    if (c.integrator != SPH_INTEGRATOR_RK4_REUSE && c.integrator != SPH_INTEGRATOR_EULER_PC) return SPH_E_CONFIG;
     if (!(c.h > 0) || !(c.kernel_scale >= 2.0) || !(c.dx > 0) || !(c.rho0 > 0) || !(c.c0sq > 0)) return SPH_E_CONFIG;
     if (c.cell_skin < 0 || c.cell_skin > 2) return SPH_E_CONFIG;
     if (c.shift_n != 4) return SPH_E_CONFIG;
@@ -117,6 +121,12 @@ int derive_params(const sph_config& c, Params& P) {
     P.solver = c.solver;
     P.muscl = c.solver == SPH_SOLVER_MUSCL_DELTA_SPS;
     P.xsph = (c.xsph_eps != 0.0 && !P.muscl) ? 1 : 0;
+    P.ms = (c.solver == SPH_SOLVER_MS_MODLR_DELTA || c.solver == SPH_SOLVER_MS_HLLC_DELTA) ? 1 : 0;
+    P.hllc = c.solver == SPH_SOLVER_MS_HLLC_DELTA ? 1 : 0;
+    P.laplacian = c.laplacian;
+    P.free_surface = c.free_surface ? 1 : 0;
+    P.integrator = c.integrator;
+    P.has_body = 0;
     P.renorm = c.renormalize ? 1 : 0;
     P.quirks = q ? 1 : 0;
     P.pair_rule = c.pair_rule;
@@ -229,7 +239,7 @@ template <> Sorted<float>& sorted<float>(sph_handle* h) { return h->D32; }
 
 template <typename R>
 int alloc_sorted(Sorted<R>& D, int cap, int max_nbr, int ncells) {
-    CK(dalloc(&D.id, cap)); CK(dalloc(&D.type, cap));
+    CK(dalloc(&D.id, cap)); CK(dalloc(&D.type, cap)); CK(dalloc(&D.itype, cap));
     CK(dalloc(&D.pos, cap)); CK(dalloc(&D.pos0, cap)); CK(dalloc(&D.vel0, cap)); CK(dalloc(&D.rho0, cap));
     CK(dalloc(&D.mass, cap)); CK(dalloc(&D.smass, cap));
     CK(dalloc(&D.kin, cap)); CK(dalloc(&D.aux, cap));
@@ -249,7 +259,7 @@ int alloc_sorted(Sorted<R>& D, int cap, int max_nbr, int ncells) {
 
 template <typename R>
 void free_sorted(Sorted<R>& D) {
-    void* ptrs[] = {D.id, D.type, D.pos, D.pos0, D.vel0, D.rho0, D.mass, D.smass, D.kin, D.aux, D.nb1, D.nb2, D.nb3,
+    void* ptrs[] = {D.id, D.type, D.itype, D.pos, D.pos0, D.vel0, D.rho0, D.mass, D.smass, D.kin, D.aux, D.nb1, D.nb2, D.nb3,
                     D.binv, D.binv64, D.fra_v, D.flags, D.drho, D.acc, D.avg, D.shift, D.ks_r, D.ks_a, D.ks_v, D.c_drho,
                     D.c_acc, D.c_avg, D.nbr, D.nnbr, D.pairs, D.npairs, D.cell_start, D.cell_end};
     for (void* p : ptrs) if (p) cudaFree(p);
@@ -353,6 +363,14 @@ int rhs(sph_handle* h, int last) {
     else k_pass_c<R, false><<<nb, 128, 0, h->stream>>>(P, D, last);
     CK(cudaGetLastError());
     h->launches += 4;
+    if (P.has_body && (last || h->bf_every_rhs)) {
+        const int nbf = blocks(P.n_tot, kRedThreads);      // <= blocks(cap_tot), the partial buffer size
+        double* fin = h->d_bf + (size_t)6 * blocks(h->cap_tot, kRedThreads);
+        k_body_force<R><<<nbf, kRedThreads, 0, h->stream>>>(P, D, h->d_bf);
+        k_body_force_final<<<1, kRedThreads, 0, h->stream>>>(nbf, h->d_bf, fin);
+        CK(cudaMemcpyAsync(h->bf, fin, 6 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        h->launches += 2;
+    }
     h->n_rhs++;
     h->have_rhs = true;
     return SPH_OK;
@@ -384,13 +402,19 @@ int run_steps(sph_handle* h, int nsteps, double dt) {
         if (rc) return rc;
         const int first = h->step_count == 0;
         if (first) { rc = rhs<R>(h, 0); if (rc) return rc; }
-        rc = stage<R>(h, 0, dt, first ? 0 : 1, 0); if (rc) return rc;
-        rc = rhs<R>(h, 0); if (rc) return rc;
-        rc = stage<R>(h, 1, dt, 0, 0); if (rc) return rc;
-        rc = rhs<R>(h, 0); if (rc) return rc;
-        rc = stage<R>(h, 2, dt, 0, 0); if (rc) return rc;
-        rc = rhs<R>(h, 1); if (rc) return rc;
-        rc = stage<R>(h, 3, dt, 0, h->cfg.shifting); if (rc) return rc;
+        if (h->cfg.integrator == SPH_INTEGRATOR_EULER_PC) {
+            rc = stage<R>(h, 10, dt, first ? 0 : 1, 0); if (rc) return rc;
+            rc = rhs<R>(h, 1); if (rc) return rc;
+            rc = stage<R>(h, 11, dt, 0, h->cfg.shifting); if (rc) return rc;
+        } else {
+            rc = stage<R>(h, 0, dt, first ? 0 : 1, 0); if (rc) return rc;
+            rc = rhs<R>(h, 0); if (rc) return rc;
+            rc = stage<R>(h, 1, dt, 0, 0); if (rc) return rc;
+            rc = rhs<R>(h, 0); if (rc) return rc;
+            rc = stage<R>(h, 2, dt, 0, 0); if (rc) return rc;
+            rc = rhs<R>(h, 1); if (rc) return rc;
+            rc = stage<R>(h, 3, dt, 0, h->cfg.shifting); if (rc) return rc;
+        }
         tic(h, -1);
         h->step_count++;
         h->n_steps++;
@@ -425,6 +449,7 @@ int diagnostics(sph_handle* h, sph_diag* out) {
     out->n_images = h->n_img;
     out->n_surface = h->have_rhs ? nsurf : 0;
     out->pair_count = h->last_pairs;
+    for (int c = 0; c < 6; ++c) out->body_force[c] = h->bf[c];
     return SPH_OK;
 }
 
@@ -495,7 +520,8 @@ void destroy(sph_handle* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     free_sorted(h->D64);
     free_sorted(h->D32);
-    void* ptrs[] = {h->S.pos, h->S.vel, h->S.rho, h->S.mass, h->S.smass, h->S.type, h->S.r_drho, h->S.r_acc,
+    void* ptrs[] = {h->S.pos, h->S.vel, h->S.rho, h->S.mass, h->S.smass, h->S.type, h->S.itype, h->d_bf,
+                    h->S.r_drho, h->S.r_acc,
                     h->S.r_avg, h->S.cnt, h->S.off, h->keys_in, h->keys_out, h->vals_in, h->vals_out, h->cub_tmp,
                     h->d_status, h->d_int, h->d_part, h->d_diag, h->d_xfer, h->d_export, h->d_off64, h->d_cnt_id};
     for (void* p : ptrs) if (p) cudaFree(p);
@@ -533,6 +559,8 @@ int init_impl(const sph_config* cfg, int n_capacity, sph_handle** out) {
     // staging
     CK(dalloc(&h->S.pos, cap)); CK(dalloc(&h->S.vel, cap)); CK(dalloc(&h->S.rho, cap));
     CK(dalloc(&h->S.mass, cap)); CK(dalloc(&h->S.smass, cap)); CK(dalloc(&h->S.type, cap));
+    CK(dalloc(&h->S.itype, cap));
+    CK(dalloc(&h->d_bf, (size_t)6 * blocks(cap, kRedThreads) + 6));
     CK(dalloc(&h->S.r_drho, h->cap_host)); CK(dalloc(&h->S.r_acc, h->cap_host)); CK(dalloc(&h->S.r_avg, h->cap_host));
     CK(dalloc(&h->S.cnt, cap)); CK(dalloc(&h->S.off, cap));
     // sort
@@ -638,6 +666,9 @@ int sph_set_state(sph_handle* h, int n, const double* pos, const double* vel, co
     CK(cudaMemcpyAsync(h->S.smass, sps_mass ? sps_mass : mass, sizeof(double) * n, cudaMemcpyHostToDevice,
                        h->stream));
     CK(cudaMemcpyAsync(h->S.type, type, sizeof(int) * n, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->S.itype, type, sizeof(int) * n, cudaMemcpyHostToDevice, h->stream));
+    h->P.has_body = 0;
+    for (int c = 0; c < 6; ++c) h->bf[c] = 0.0;
     CK(cudaMemsetAsync(h->S.r_drho, 0, sizeof(double) * n, h->stream));
     CK(cudaMemsetAsync(h->S.r_acc, 0, sizeof(double2) * n, h->stream));
     CK(cudaMemsetAsync(h->S.r_avg, 0, sizeof(double2) * n, h->stream));
@@ -666,6 +697,20 @@ int sph_update_state(sph_handle* h, int n, const double* pos, const double* vel,
     return SPH_OK;
 }
 
+int sph_set_initial_type(sph_handle* h, int n, const int* initial_type) {
+    if (!h || n != h->n_host || n <= 0 || !initial_type) return SPH_E_ARG;
+    CK(cudaSetDevice(h->device));
+    int rc = h->mixed ? unsort<float>(h) : unsort<double>(h);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(h->S.itype, initial_type, sizeof(int) * n, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    int body = 0;
+    for (int i = 0; i < n; ++i) body |= initial_type[i] == SPH_TYPE_BODY;
+    h->P.has_body = body;
+    h->sorted_valid = false;
+    return SPH_OK;
+}
+
 int sph_get_state(sph_handle* h, int n, double* pos, double* vel, double* rho, double* press) {
     if (!h || n != h->n_host || n <= 0) return SPH_E_ARG;
     CK(cudaSetDevice(h->device));
@@ -689,7 +734,9 @@ int sph_rhs(sph_handle* h, double* drhodt, double* acc, double* avg_vel, int* fs
     CK(cudaSetDevice(h->device));
     int rc = DISPATCH(h, prepare, h);
     if (rc) return rc;
+    h->bf_every_rhs = true;
     rc = DISPATCH(h, rhs, h, 0);
+    h->bf_every_rhs = false;
     if (rc) return rc;
     timing_flush(h);
     rc = read_status(h);

@@ -15,13 +15,19 @@ namespace sph {
 //            x = x0 + (K_v + v) dt/6 + 0.5 dt^2 a; then Shift_particle_position.
 // Stage 0 uses the rates carried from the previous step (K1 reuse, :940-965)
 // unless this is the first step, when a fresh RHS precedes it (:821).
+//
+// With SPH_INTEGRATOR_EULER_PC (Moving_Square.../SPH_Time_Iteration.f90:304-334) the
+// stages are 10 (predictor) and 11 (corrector):
+//   predictor  rho = rho0 + drhodt dt, x = x0 + dt (v0 + avg) + 0.5 a dt^2, v = v0 + dt a
+//   corrector  rho = rho0 + 0.5 (drhodt + drhodt_p) dt,
+//              x = x0 + 0.5 dt (v_p + v0) + avg dt + 0.5 a dt^2, v = v0 + 0.5 dt (a + a_p)
 template <typename R>
 __global__ void k_stage(Params P, Sorted<R> D, int stage, double dt, int use_carried, int do_shift,
                         unsigned* status) {
     using V2 = typename VT<R>::V2;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= P.n_tot) return;
-    if (D.type[s] != SPH_TYPE_WATER) return;
+    if (!integrated(P, D.type[s])) return;
     const double2 x0 = D.pos0[s];
     const double2 v0 = D.vel0[s];
     const double r0 = D.rho0[s];
@@ -34,7 +40,28 @@ __global__ void k_stage(Params P, Sorted<R> D, int stage, double dt, int use_car
         ax = (double)a.x; ay = (double)a.y; gx = (double)g.x; gy = (double)g.y;
     }
     double rho, u, v, x, y;
-    if (stage < 3) {
+    if (stage == 10) {
+        rho = r0 + dr * dt;
+        x = x0.x + dt * (v0.x + gx) + 0.5 * ax * (dt * dt);
+        y = x0.y + dt * (v0.y + gy) + 0.5 * ay * (dt * dt);
+        u = v0.x + dt * ax;
+        v = v0.y + dt * ay;
+        D.ks_r[s] = (R)dr;
+        D.ks_a[s] = mk2<R>((R)ax, (R)ay);
+        D.ks_v[s] = v0;
+    } else if (stage == 11) {
+        const double4 kp = D.kin[s];          // predicted velocity
+        const V2 ka = D.ks_a[s];
+        const double2 kv = D.ks_v[s];
+        rho = r0 + 0.5 * (dr + (double)D.ks_r[s]) * dt;
+        x = x0.x + 0.5 * dt * (kp.x + kv.x) + gx * dt + 0.5 * ax * (dt * dt);
+        y = x0.y + 0.5 * dt * (kp.y + kv.y) + gy * dt + 0.5 * ay * (dt * dt);
+        u = v0.x + 0.5 * dt * (ax + (double)ka.x);
+        v = v0.y + 0.5 * dt * (ay + (double)ka.y);
+        D.c_drho[s] = (R)dr;
+        D.c_acc[s] = mk2<R>((R)ax, (R)ay);
+        D.c_avg[s] = mk2<R>((R)gx, (R)gy);
+    } else if (stage < 3) {
         const double f = stage < 2 ? 0.5 * dt : dt;
         rho = stage < 2 ? r0 + dr * dt / 2 : r0 + dr * dt;
         u = v0.x + f * ax + gx;
@@ -68,8 +95,9 @@ __global__ void k_stage(Params P, Sorted<R> D, int stage, double dt, int use_car
     // the neighbour lists stay exact while nobody moved more than half the skin
     const double ddx = x - x0.x, ddy = y - x0.y;
     if (ddx * ddx + ddy * ddy > P.skin_half2) atomicOr(status, ST_SKIN);
-    if (stage == 3) {
-        if (do_shift && !(D.flags[s] & 2)) {
+    const bool final_stage = stage == 3 || stage == 11;
+    if (final_stage) {
+        if (do_shift && D.type[s] == SPH_TYPE_WATER && !(D.flags[s] & 2)) {
             // Shift_particle_position.f90:108-131
             const double2 sh = D.shift[s];
             double s0 = sh.x, s1 = sh.y;
@@ -129,6 +157,81 @@ __global__ void k_diag_final(int nparts, const double* part_ke, const double* pa
         __syncthreads();
     }
     if (threadIdx.x == 0) { out[0] = ske[0]; out[1] = smx[0]; }
+}
+
+// Body force of the last RHS (Moving_Square.../Calculate_Body_Force.f90:53-142 and
+// Single_step_compute.f90:228-243), gather form in FP64: for a particle with body
+// neighbours b (initial type SPH_TYPE_BODY)
+//   BFP_a = -sum_b V_b (p_a + p_b) B_a^-1 grad_a W_ab
+//   BFV_a =  sum_b rho_a V_b 2 nu ((x_a - x_b).B_a^-1 grad_a W_ab) / r^2 (v_a - v_b)   (Morris)
+//       or   sum_b rho_a V_b 2 (dim+2) nu ((v_a-v_b).(x_a-x_b)) / r^2 B_a^-1 grad_a W_ab
+// and the forces are sum_a V_a BFP_a, sum_a V_a BFV_a and their sum (no gravity).
+template <typename R>
+__global__ void k_body_force(Params P, Sorted<R> D, double* part) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    double f[6] = {0, 0, 0, 0, 0, 0};
+    if (a < P.n_tot) {
+        const int nn = D.npairs[a];
+        const double2 xa = D.pos[a];
+        const double4 ka = D.kin[a];
+        const double4 bi = D.binv64[a];
+        double bp0 = 0, bp1 = 0, bv0 = 0, bv1 = 0;
+        bool near_body = false;
+        for (int e = 0; e < nn; ++e) {
+            const int b = (int)(D.pairs[(size_t)e * P.nbr_stride + a] & 0x7fffffffu);
+            if (D.itype[b] != SPH_TYPE_BODY) continue;
+            near_body = true;
+            const double2 xb = D.pos[b];
+            const double4 kb = D.kin[b];
+            const double dx = xa.x - xb.x, dy = xa.y - xb.y;
+            const double r2 = dx * dx + dy * dy, d = sqrt(r2);
+            double w, gx, gy;
+            kernel_w_dw<double>(P, d, dx, dy, w, gx, gy);
+            const double n0 = bi.x * gx + bi.y * gy, n1 = bi.z * gx + bi.w * gy;
+            const double Vb = D.mass[b] / kb.z;
+            bp0 -= Vb * (ka.w + kb.w) * n0;
+            bp1 -= Vb * (ka.w + kb.w) * n1;
+            const double du = ka.x - kb.x, dv = ka.y - kb.y;
+            if (P.laplacian == 1) {
+                const double fv = ka.z * Vb * 2 * P.nu * (dx * n0 + dy * n1) / r2;
+                bv0 += fv * du; bv1 += fv * dv;
+            } else {
+                const double fv = ka.z * Vb * 2 * (2 + 2) * P.nu * (du * dx + dv * dy) / r2;
+                bv0 += fv * n0; bv1 += fv * n1;
+            }
+        }
+        if (near_body) {
+            const double Va = D.mass[a] / ka.z;
+            f[0] = Va * bp0; f[1] = Va * bp1; f[2] = Va * bv0; f[3] = Va * bv1;
+            f[4] = Va * (bp0 + bv0); f[5] = Va * (bp1 + bv1);
+        }
+    }
+    __shared__ double sh[6][kRedThreads];
+    for (int c = 0; c < 6; ++c) sh[c][threadIdx.x] = f[c];
+    __syncthreads();
+    for (int w = kRedThreads / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w)
+            for (int c = 0; c < 6; ++c) sh[c][threadIdx.x] += sh[c][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int c = 0; c < 6; ++c) part[(size_t)c * gridDim.x + blockIdx.x] = sh[c][0];
+}
+
+__global__ void k_body_force_final(int nparts, const double* part, double* out) {
+    __shared__ double sh[kRedThreads];
+    for (int c = 0; c < 6; ++c) {
+        double s = 0.0;
+        for (int i = threadIdx.x; i < nparts; i += blockDim.x) s += part[(size_t)c * nparts + i];
+        sh[threadIdx.x] = s;
+        __syncthreads();
+        for (int w = kRedThreads / 2; w > 0; w >>= 1) {
+            if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) out[c] = sh[0];
+        __syncthreads();
+    }
 }
 
 // Count of flagged surface particles (diagnostics).

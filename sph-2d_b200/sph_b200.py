@@ -36,6 +36,10 @@ KERNEL_GAUSSIAN = 4
 KERNEL_WENDLAND2 = 5
 SOLVER_MODLR_DELTA_SPS = 0
 SOLVER_MUSCL_DELTA_SPS = 1
+SOLVER_MS_MODLR_DELTA = 2
+SOLVER_MS_HLLC_DELTA = 3
+INTEGRATOR_RK4_REUSE = 0
+INTEGRATOR_EULER_PC = 1
 EOS_TAIT = 0
 EOS_LINEAR = 1
 PAIRS_ONE_FLUID = 0
@@ -45,11 +49,14 @@ PREC_MIXED = 1
 TYPE_WATER = 2
 TYPE_PERIODIC = -101
 TYPE_ILL = 120
+TYPE_FIX_GHOST = -3
+TYPE_BODY = -4
 
 EXPORTED_SYMBOLS = (
     "sph_init", "sph_free", "sph_set_state", "sph_get_state", "sph_find_particle_pair",
     "sph_rhs", "sph_step", "sph_diagnostics", "sph_get_timings", "sph_reset_timings",
     "sph_strerror", "sph_get_field", "sph_update_state", "sph_find_particle_pair_noalloc",
+    "sph_set_initial_type",
 )
 
 
@@ -67,7 +74,7 @@ class SphConfig(ctypes.Structure):
         ("shift_max", ctypes.c_double), ("shift_n", ctypes.c_int), ("fs_threshold", ctypes.c_double),
         ("box_lo", ctypes.c_double * 2), ("box_hi", ctypes.c_double * 2),
         ("grid_lo", ctypes.c_double * 2), ("grid_hi", ctypes.c_double * 2),
-        ("cell_skin", ctypes.c_double),
+        ("cell_skin", ctypes.c_double), ("laplacian", ctypes.c_int), ("free_surface", ctypes.c_int),
     ]
 
     def copy(self) -> "SphConfig":
@@ -80,6 +87,7 @@ class SphDiag(ctypes.Structure):
     _fields_ = [
         ("kinetic_energy", ctypes.c_double), ("max_speed", ctypes.c_double),
         ("pair_count", ctypes.c_longlong), ("n_images", ctypes.c_int), ("n_surface", ctypes.c_int),
+        ("body_force", ctypes.c_double * 6),
     ]
 
 
@@ -131,6 +139,8 @@ def tgv_reference_config(n_side: int = 100) -> SphConfig:
     c.grid_lo[:] = [-pad, -pad]
     c.grid_hi[:] = [1.0 + pad, 1.0 + pad]
     c.cell_skin = 0.1
+    c.laplacian = 1
+    c.free_surface = 1
     return c
 
 
@@ -234,6 +244,7 @@ def load(path: str = LIB_PATH):
     lib.sph_set_state.argtypes = [P, ctypes.c_int, dp, dp, dp, dp, ip, dp]
     lib.sph_get_state.argtypes = [P, ctypes.c_int, dp, dp, dp, dp]
     lib.sph_update_state.argtypes = [P, ctypes.c_int, dp, dp, dp]
+    lib.sph_set_initial_type.argtypes = [P, ctypes.c_int, ip]
     lib.sph_find_particle_pair.argtypes = [P, ctypes.c_longlong, ip, ip, dp, dp, ctypes.POINTER(ctypes.c_longlong)]
     lib.sph_rhs.argtypes = [P, dp, dp, dp, ip, ip]
     lib.sph_step.argtypes = [P, ctypes.c_int, ctypes.c_double, ctypes.POINTER(SphDiag)]
@@ -320,6 +331,11 @@ class Simulation:
                                          _ptr(np.ascontiguousarray(vel, np.float64)),
                                          _ptr(np.ascontiguousarray(rho, np.float64))), "sph_update_state")
 
+    def set_initial_type(self, itype):
+        """subdomain_particle_initial_type (SPH_TYPE_BODY marks the body for the body force)."""
+        it = np.ascontiguousarray(itype, dtype=np.int32)
+        _check(self.lib.sph_set_initial_type(self.h, self.n, _ptr(it, ctypes.c_int)), "sph_set_initial_type")
+
     def get_state(self):
         n = self.n
         pos = np.empty(2 * n); vel = np.empty(2 * n); rho = np.empty(n); press = np.empty(n)
@@ -402,3 +418,89 @@ def make_tgv(n_side: int, reference: bool = False, solver: int = SOLVER_MUSCL_DE
         pos = pos + rng.uniform(-jitter, jitter, pos.shape) * cfg.dx
     typ = np.full(rho.shape[0], TYPE_WATER, np.int32)
     return TgvCase(cfg, pos, vel, rho, mass, typ)
+
+
+# ---------------------------------------------------------------------------
+# Moving-square layout (SPHERIC test 6 geometry of Moving_Square.../Information_Module.f90,
+# scaled): a water-filled tank with fixed ghost walls and a square body made of
+# ghost particles whose initial type marks the body.
+# ---------------------------------------------------------------------------
+def moving_square_config(dx: float, lx: float, ly: float, solver: int = SOLVER_MS_HLLC_DELTA,
+                         precision: int = PREC_FP64, re: float = 100.0, U: float = 1.0, D: float = 1.0,
+                         c0: float = 10.0) -> SphConfig:
+    """Improved Gaussian (model 4, kernel_scale 3) with h = 1.15 dx as the moving-square case
+    ships (Information_Module.f90:615-616), linear (Tammann) EOS (:305), alpha 0.03, beta 2,
+    epsilon 0.1 (:630-644), Morris laplacian (:303), no free surface (:285), Euler
+    predictor-corrector (:699), max shift 0.15 dx (:679); rho0 = 1 and nu = U D / Re."""
+    c = SphConfig()
+    c.kernel_model = KERNEL_GAUSSIAN
+    c.solver = solver
+    c.eos = EOS_LINEAR
+    c.pair_rule = PAIRS_NO_SAME_BND
+    c.precision = precision
+    c.renormalize = 0
+    c.reference_literals = 1
+    c.periodic = 0
+    c.shifting = 1
+    c.integrator = INTEGRATOR_EULER_PC
+    c.kernel_scale = 3.0
+    c.h = 1.15 * dx
+    c.dx = dx
+    c.rho0 = 1.0
+    c.c0sq = c0 * c0
+    c.background_p = 0.0
+    c.nu = U * D / re
+    c.alpha, c.beta, c.fai = 0.03, 2.0, 0.1
+    c.delta, c.delta_alpha = 0.1, 0.02
+    c.xsph_eps = 0.1
+    c.shift_beta, c.shift_R, c.shift_max, c.shift_n = 0.5, 0.2, 0.15 * dx, 4
+    c.fs_threshold = 0.65
+    c.box_lo[:] = [0.0, 0.0]
+    c.box_hi[:] = [lx, ly]
+    pad = 6 * dx
+    c.grid_lo[:] = [-pad, -pad]
+    c.grid_hi[:] = [lx + pad, ly + pad]
+    c.cell_skin = 0.1
+    c.laplacian = 1
+    c.free_surface = 0
+    return c
+
+
+def make_moving_square(dx: float = 0.05, lx: float = 4.0, ly: float = 2.0, D: float = 0.5, U: float = 1.0,
+                       layers: int = 4, solver: int = SOLVER_MS_HLLC_DELTA, precision: int = PREC_FP64,
+                       jitter: float = 0.0, seed: int = 0):
+    """Water lattice in [0,lx]x[0,ly] at rest (rho = rho0), `layers` rows of fixed ghost
+    particles outside the walls, and a square body of side D centred at (lx/4, ly/2)
+    whose ghost particles move with velocity (U, 0).  Returns (case, initial_type)."""
+    cfg = moving_square_config(dx, lx, ly, solver, precision, U=U, D=D)
+    xs = (np.arange(int(round(lx / dx))) + 0.5) * dx
+    ys = (np.arange(int(round(ly / dx))) + 0.5) * dx
+    X, Y = np.meshgrid(xs, ys)
+    cx, cy = lx / 4, ly / 2
+    inside = (np.abs(X - cx) < D / 2) & (np.abs(Y - cy) < D / 2)
+    wx, wy = X[~inside], Y[~inside]
+    gx = (np.arange(-layers, int(round(lx / dx)) + layers) + 0.5) * dx
+    gy = (np.arange(-layers, int(round(ly / dx)) + layers) + 0.5) * dx
+    GX, GY = np.meshgrid(gx, gy)
+    wall = (GX < 0) | (GX > lx) | (GY < 0) | (GY > ly)
+    bx, by = X[inside], Y[inside]
+    x = np.concatenate([wx, GX[wall], bx])
+    y = np.concatenate([wy, GY[wall], by])
+    nw, ng, nb = wx.size, int(wall.sum()), bx.size
+    typ = np.concatenate([np.full(nw, TYPE_WATER), np.full(ng + nb, TYPE_FIX_GHOST)]).astype(np.int32)
+    ityp = np.concatenate([np.full(nw + ng, 0), np.full(nb, TYPE_BODY)]).astype(np.int32)
+    ityp[:nw] = TYPE_WATER
+    ityp[nw:nw + ng] = TYPE_FIX_GHOST
+    if jitter > 0.0:
+        rng = np.random.default_rng(seed)
+        x[:nw] += rng.uniform(-jitter, jitter, nw) * dx
+        y[:nw] += rng.uniform(-jitter, jitter, nw) * dx
+    n = x.size
+    u = np.zeros(n)
+    v = np.zeros(n)
+    u[nw + ng:] = U
+    rho = np.full(n, cfg.rho0)
+    mass = rho * dx * dx
+    pos = np.concatenate([x, y])
+    vel = np.concatenate([u, v])
+    return TgvCase(cfg, pos, vel, rho, mass, typ), ityp
