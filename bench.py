@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--n-side", type=int, default=N_SIDE)
     ap.add_argument("--skip-accuracy", action="store_true")
+    ap.add_argument("--skip-adjoint", action="store_true")
     return ap.parse_args()
 
 
@@ -256,6 +257,11 @@ def run_native(args, rank, world, local):
             "kernel": "k_pass_c<float,MUSCL>", "launch_ms": passc_ms, "algorithmic_bytes": alg,
             "peak_kind": pk_kind + " (burst copy)"}
 
+    # ---- adjoint cost (rank 0) -------------------------------------------------
+    adj = None
+    if rank == 0 and not args.skip_adjoint:
+        adj = adjoint_report(S)
+
     # ---- CPU baseline (rank 0 only, N = 1) ----------------------------------
     cpu = None
     if rank == 0 and world == 1:
@@ -275,7 +281,8 @@ def run_native(args, rank, world, local):
         "fp64": {"value": value64, "unit": UNIT, "ms_per_step": fp64["dev_ms"] / steps,
                  "mixed_over_fp64": value / value64},
         "accuracy": accuracy,
-        "adjoint_over_forward": None,
+        "adjoint_over_forward": adj["adjoint_over_forward"] if adj else None,
+        "adjoint": adj,
         "passes_ms_per_step": {
             "images": tm.images_ms / steps, "sort_lists": tm.sort_ms / steps,
             "pass_a": tm.pass_a_ms / steps, "surface": tm.surface_ms / steps,
@@ -287,6 +294,81 @@ def run_native(args, rank, world, local):
         "gpu_launches": int(tm.kernel_launches),
         "clocks": clocks_info,
         "wall_s_timed": mixed["wall_s"],
+    }
+
+
+ADJ_SIDE, ADJ_STEPS, ADJ_EVERY = 256, 500, 32
+
+
+def adjoint_leg(S, precision):
+    """Cost of the discrete adjoint on the adjoint Taylor-Green case: 256 x 256
+    particles, 500 steps, a checkpoint every 32 steps, loss = squared velocity
+    misfit at the end against a target from a forward run whose initial
+    velocity carries 8 seeded Fourier modes of amplitude 0.05 U0.  Solver:
+    modified linear Riemann + delta-SPH + SPS, Wendland C2, renormalised, no
+    shifting.  Both calls return only when their device work is done, so the
+    host clock around each is its cost; the device-event sums are beside it."""
+    case = S.make_tgv(ADJ_SIDE, solver=S.SOLVER_MODLR_DELTA_SPS, precision=precision)
+    case.cfg.shifting = 0
+    dt = S.baseline_dt(case.cfg)
+    dv = S.fourier_perturbation(case.pos, n_modes=8, amp=0.05, seed=2024)
+    with S.Simulation(case.cfg, case.n) as sim:
+        sim.set_state(case.pos, case.vel + dv, case.rho, case.mass, case.type)
+        sim.time_iteration(ADJ_STEPS, dt)
+        target = sim.get_state()[1]
+    out = {}
+    with S.Simulation(case.cfg, case.n) as sim:
+        for rep in range(2):         # the first round warms up allocations and module loading
+            sim.set_state(case.pos, case.vel, case.rho, case.mass, case.type)
+            sim.reset_timings()
+            t0 = time.perf_counter()
+            sim.time_iteration(ADJ_STEPS, dt)
+            t_fwd = time.perf_counter() - t0
+            dev_fwd = sim.timings().total_ms
+            sim.set_state(case.pos, case.vel, case.rho, case.mass, case.type)
+            sim.reset_timings()
+            t0 = time.perf_counter()
+            loss = sim.adjoint_forward(ADJ_STEPS, dt, checkpoint_every=ADJ_EVERY, target_vel=target)
+            t_fck = time.perf_counter() - t0
+            sim.reset_timings()
+            t0 = time.perf_counter()
+            g = sim.adjoint_backward(1.0)
+            t_bwd = time.perf_counter() - t0
+            tb = sim.timings()
+        out = {"loss": loss, "forward_s": t_fwd, "forward_checkpointed_s": t_fck, "backward_s": t_bwd,
+               "adjoint_over_forward": t_bwd / t_fwd,
+               "forward_device_ms": dev_fwd, "backward_device_ms": tb.total_ms,
+               "backward_reverse_kernels_ms": tb.adjoint_ms, "grad": g}
+    return case, dt, target, out
+
+
+def adjoint_report(S):
+    casem, dt, target, m = adjoint_leg(S, S.PREC_MIXED)
+    case, _, _, d = adjoint_leg(S, S.PREC_FP64)
+    # central differences of the FP64 forward along two seeded directions
+    fd_err = []
+    for k in range(2):
+        dirv = np.random.default_rng(300 + k).standard_normal(2 * case.n)
+        eps = 1e-6
+        ls = []
+        for sgn in (1.0, -1.0):
+            with S.Simulation(case.cfg, case.n) as sim:
+                sim.set_state(case.pos, case.vel + sgn * eps * dirv, case.rho, case.mass, case.type)
+                ls.append(sim.adjoint_forward(ADJ_STEPS, dt, checkpoint_every=ADJ_STEPS, target_vel=target))
+        fd = (ls[0] - ls[1]) / (2 * eps)
+        fd_err.append(abs(float(d["grad"]["vel0"] @ dirv) - fd) / abs(fd))
+    gm, g64 = m["grad"]["vel0"], d["grad"]["vel0"]
+    keep = ("loss", "forward_s", "forward_checkpointed_s", "backward_s", "adjoint_over_forward",
+            "forward_device_ms", "backward_device_ms", "backward_reverse_kernels_ms")
+    return {
+        "case": f"TGV {ADJ_SIDE}x{ADJ_SIDE} ({case.n} particles), {ADJ_STEPS} steps, checkpoint every {ADJ_EVERY}, "
+                "velocity-misfit loss vs a target from 8 seeded Fourier modes (0.05 U0); modified linear Riemann "
+                "+ delta-SPH + SPS, Wendland C2, renormalised, no shifting",
+        "mixed": {k: m[k] for k in keep}, "fp64": {k: d[k] for k in keep},
+        "adjoint_over_forward": m["adjoint_over_forward"],
+        "grad_vel0_l2_mixed_vs_fp64": float(np.linalg.norm(gm - g64) / np.linalg.norm(g64)),
+        "dnu_mixed": m["grad"]["nu"], "dnu_fp64": d["grad"]["nu"],
+        "fd_rel_err_fp64": fd_err, "fd": "central differences eps=1e-6, FP64 forward, 2 seeded directions",
     }
 
 

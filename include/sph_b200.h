@@ -124,6 +124,7 @@ typedef struct sph_timings {
     double sort_ms, pass_a_ms, surface_ms, pass_c_ms, update_ms, images_ms, total_ms;
     long long rhs_evaluations, steps;
     long long kernel_launches;  /* libsph_b200 kernels launched (library sort/scan calls not counted) */
+    double adjoint_ms;          /* reverse kernels of sph_adjoint_backward */
 } sph_timings;
 
 typedef struct sph_handle sph_handle;
@@ -218,6 +219,46 @@ int sph_reset_timings(sph_handle* h);
 int sph_find_particle_pair_noalloc(const sph_config* cfg, int n, const double* d_pos, const int* d_type,
                                    long long pair_cap, int* d_pair_i, int* d_pair_j, double* d_w,
                                    double* d_dwdx, long long* pair_number, void* stream);
+
+/* ---- discrete adjoint of the time step (no counterpart in the reference) --
+ * A forward/backward pair with the contract of an autograd function, for a
+ * Fortran host that has no automatic differentiation: sph_adjoint_forward
+ * runs nsteps steps from the handle's current state, keeps checkpoints of the
+ * state every checkpoint_every steps inside the handle (the saved context)
+ * and returns the loss; sph_adjoint_backward takes dL/dloss and returns the
+ * gradient of the loss with respect to the state the forward started from
+ * and to the viscosity.  The backward pass re-runs each checkpoint segment,
+ * rebuilds every step's pair set from the recomputed positions and holds it
+ * fixed while the reverse kernels run (the pair set is piecewise constant in
+ * the positions; the gradient is that of the taken branches of max/min and
+ * of the artificial-viscosity switch).  The handle's state after the backward
+ * pass is the forward's final state.
+ *
+ * Supported configurations: the normalised modified linear Riemann
+ * delta-SPH + SPS solver (SPH_SOLVER_MODLR_DELTA_SPS) with the RK4 driver,
+ * either kernel, with or without renormalisation, without particle shifting
+ * and without XSPH; other configurations return SPH_E_CONFIG.  The reverse
+ * kernels compute in FP64 for both precisions of the forward step. */
+#define SPH_LOSS_VELOCITY_MISFIT 0  /* sum over water particles of |v - v_target|^2 */
+#define SPH_LOSS_KINETIC_ENERGY  1  /* sum over water particles of m |v|^2 / 2       */
+#define SPH_ADJ_NPARAMS 1           /* g_params[0] = dL/dnu                          */
+
+typedef struct sph_adj_config {
+    int nsteps;             /* time steps of the forward run                          */
+    int checkpoint_every;   /* steps between state checkpoints (>= 1)                 */
+    int loss;               /* SPH_LOSS_*                                             */
+    int reserved;
+    double dt;
+    const double* target_vel;  /* [2*n] column-major (u block, v block); copied; misfit only */
+} sph_adj_config;
+
+int sph_adjoint_forward(sph_handle* h, const sph_adj_config* cfg, double* loss);
+
+/* Any output pointer may be NULL.  g_vel0 and g_pos0 are [2*n] column-major,
+ * g_rho0 is [n], g_params is [SPH_ADJ_NPARAMS].  Returns SPH_E_ARG when no
+ * forward context is held. */
+int sph_adjoint_backward(sph_handle* h, double dloss, double* g_vel0, double* g_rho0, double* g_pos0,
+                         double* g_params);
 
 /* Human-readable message for a status code (static storage). */
 const char* sph_strerror(int code);

@@ -22,7 +22,19 @@ struct Staging {
     double2* r_avg;
     int* cnt;         // image counts / scan scratch
     int* off;
+    // image counts and offsets of this step, kept for routing image adjoints:
+    // left/right images of host i sit at n_host + lr_off[i] + k (k < lr_cnt[i]),
+    // bottom/top images of source s at n_host + n_lr + tb_off[s] + k (k < tb_cnt[s])
+    int* lr_cnt;
+    int* lr_off;
+    int* tb_cnt;
+    int* tb_off;
 };
+
+__global__ void k_copy_int2(int n, const int* a, const int* b, int* a2, int* b2) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) { a2[i] = a[i]; b2[i] = b[i]; }
+}
 
 // --- 1. periodic wrap (Distribute_Period_Boundary_Particle.f90:56-90) -------
 __global__ void k_wrap(Params P, Staging S) {

@@ -21,7 +21,7 @@
 #include <new>
 #include <vector>
 
-#include "update.cuh"
+#include "adjoint.cuh"
 
 using namespace sph;
 
@@ -46,7 +46,7 @@ const char* kMessages[] = {
 
 inline int blocks(long long n, int t) { return (int)((n + t - 1) / t); }
 
-enum Phase { PH_SORT, PH_A, PH_SURF, PH_C, PH_UPDATE, PH_IMAGES, PH_COUNT };
+enum Phase { PH_SORT, PH_A, PH_SURF, PH_C, PH_UPDATE, PH_IMAGES, PH_ADJ, PH_COUNT };
 
 template <typename T>
 cudaError_t dalloc(T** p, size_t count) {
@@ -61,7 +61,7 @@ struct sph_handle {
     Params P;
     int device = 0;
     int cap_host = 0, cap_img = 0, cap_tot = 0;
-    int n_host = 0, n_img = 0;
+    int n_host = 0, n_img = 0, n_lr = 0;
     bool staging_valid = false;
     bool sorted_valid = false;
     bool have_rhs = false;
@@ -100,6 +100,7 @@ struct sph_handle {
     double bf[6] = {0, 0, 0, 0, 0, 0};   // body force of the last RHS
     double* d_bf = nullptr;               // [6 * blocks(cap_tot) partials + 6]
     bool bf_every_rhs = false;            // sph_rhs also reports it
+    struct AdjCtx* adj = nullptr;         // saved context of sph_adjoint_forward
 };
 
 namespace {
@@ -312,6 +313,8 @@ int prepare(sph_handle* h) {
         if (rc) return rc;
         if (h->n_host + n_lr > h->cap_tot) return SPH_E_CAPACITY;
         k_img_emit<<<blocks(h->n_host, 256), 256, 0, h->stream>>>(P, h->S, h->n_host, 0, h->n_host, h->S.off);
+        k_copy_int2<<<blocks(h->n_host, 256), 256, 0, h->stream>>>(h->n_host, h->S.cnt, h->S.off, h->S.lr_cnt,
+                                                                    h->S.lr_off);
         // bottom/top images of host particles and left/right images
         const int n_src = h->n_host + n_lr;
         k_img_count<<<blocks(n_src, 256), 256, 0, h->stream>>>(P, h->S, n_src, 1);
@@ -320,11 +323,13 @@ int prepare(sph_handle* h) {
         if (rc) return rc;
         if (n_src + n_tb > h->cap_tot) return SPH_E_CAPACITY;
         k_img_emit<<<blocks(n_src, 256), 256, 0, h->stream>>>(P, h->S, n_src, 1, n_src, h->S.off);
+        k_copy_int2<<<blocks(n_src, 256), 256, 0, h->stream>>>(n_src, h->S.cnt, h->S.off, h->S.tb_cnt, h->S.tb_off);
+        h->n_lr = n_lr;
         n_img = n_lr + n_tb;
         CK(cudaGetLastError());
     }
     h->n_img = n_img;
-    h->launches += h->cfg.periodic ? 5 : 0;
+    h->launches += h->cfg.periodic ? 7 : 0;
     P.n_tot = h->n_host + n_img;
     tic(h, PH_SORT);
     Sorted<R>& D = sorted<R>(h);
@@ -511,6 +516,335 @@ int export_fields(sph_handle* h) {
     return SPH_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Discrete adjoint: checkpointed forward run and the reverse sweep.
+// ---------------------------------------------------------------------------
+
+// Host-particle state in id order: what a step starts from.
+struct Snap {
+    double2 *pos = nullptr, *vel = nullptr, *r_acc = nullptr, *r_avg = nullptr;
+    double *rho = nullptr, *r_drho = nullptr;
+};
+
+}  // namespace
+
+struct AdjCtx {
+    bool valid = false;
+    int nsteps = 0, every = 0, loss = 0, nseg = 0;
+    double dt = 0.0;
+    long long step0 = 0;       // handle step count when the forward started
+    int n_host = 0;
+    int cap_ck = 0, cap_seg = 0, cap_host = 0, cap_tot = 0;
+    Snap ck;                   // checkpoints [nseg + 1] (the last: the final state)
+    Snap seg;                  // step-start states of the segment being reversed
+    // stage states S1..S3 in sorted order, [stage_slots][3][cap_tot]: one slot per
+    // step of the segment when memory allows (kept while the segment is re-run),
+    // else one slot that each reversed step recomputes
+    int stage_slots = 0;
+    double2* st_pos = nullptr;
+    double4* st_kin = nullptr;
+    double4* st_aux = nullptr;  // V4 of the pair precision (float4 uses the first half)
+    std::vector<int> seg_ntot;  // particles + images of each step of the segment
+    double2* target = nullptr;
+    double* loss_part = nullptr;
+    Adj A{};
+    std::vector<void*> owned;
+};
+
+namespace {
+
+template <typename T>
+int adj_alloc(AdjCtx* X, T** p, size_t count) {
+    CK(dalloc(p, count));
+    X->owned.push_back((void*)*p);
+    return SPH_OK;
+}
+
+void adj_free_all(AdjCtx* X) {
+    for (void* p : X->owned) cudaFree(p);
+    X->owned.clear();
+}
+
+int snap_alloc(AdjCtx* X, Snap& s, size_t n) {
+    int rc;
+    if ((rc = adj_alloc(X, &s.pos, n)) || (rc = adj_alloc(X, &s.vel, n)) || (rc = adj_alloc(X, &s.r_acc, n)) ||
+        (rc = adj_alloc(X, &s.r_avg, n)) || (rc = adj_alloc(X, &s.rho, n)) || (rc = adj_alloc(X, &s.r_drho, n)))
+        return rc;
+    return SPH_OK;
+}
+
+// staging (id order) <-> snapshot slot k
+int snap_io(sph_handle* h, const Snap& s, int k, int n, bool save) {
+    const size_t o = (size_t)k * n;
+    const SnapPtrs slot{s.pos + o, s.vel + o, s.r_acc + o, s.r_avg + o, s.rho + o, s.r_drho + o};
+    const SnapPtrs stg{h->S.pos, h->S.vel, h->S.r_acc, h->S.r_avg, h->S.rho, h->S.r_drho};
+    k_snap_copy<<<blocks(n, 256), 256, 0, h->stream>>>(n, save ? slot : stg, save ? stg : slot);
+    CK(cudaGetLastError());
+    h->launches += 1;
+    if (!save) {
+        h->staging_valid = true;
+        h->sorted_valid = false;
+    }
+    return SPH_OK;
+}
+
+int adj_config_ok(const sph_handle* h) {
+    const Params& P = h->P;
+    if (h->cfg.solver != SPH_SOLVER_MODLR_DELTA_SPS || P.muscl || P.ms || P.xsph) return SPH_E_CONFIG;
+    if (h->cfg.integrator != SPH_INTEGRATOR_RK4_REUSE || h->cfg.shifting) return SPH_E_CONFIG;
+    return SPH_OK;
+}
+
+int adj_prepare_ctx(sph_handle* h, const sph_adj_config* ac) {
+    AdjCtx* X = h->adj;
+    const int nseg = (ac->nsteps + ac->checkpoint_every - 1) / ac->checkpoint_every;
+    const int every = std::min(ac->checkpoint_every, ac->nsteps);
+    if (X && (X->cap_ck < nseg + 1 || X->cap_seg < every || X->cap_host < h->n_host || X->cap_tot < h->cap_tot)) {
+        adj_free_all(X);
+        delete X;
+        X = h->adj = nullptr;
+    }
+    if (!X) {
+        X = new (std::nothrow) AdjCtx();
+        if (!X) return SPH_E_CAPACITY;
+        h->adj = X;
+        const size_t nh = (size_t)h->cap_host, nt = (size_t)h->cap_tot;
+        X->cap_ck = nseg + 1; X->cap_seg = every; X->cap_host = h->cap_host; X->cap_tot = h->cap_tot;
+        int rc;
+        if ((rc = snap_alloc(X, X->ck, nh * (nseg + 1))) || (rc = snap_alloc(X, X->seg, nh * every))) return rc;
+        if ((rc = adj_alloc(X, &X->target, nh)) || (rc = adj_alloc(X, &X->loss_part, 148 * 4))) return rc;
+        Adj& A = X->A;
+        for (int k = 0; k < 4; ++k)
+            if ((rc = adj_alloc(X, &A.lr[k], nt)) || (rc = adj_alloc(X, &A.la[k], nt))) return rc;
+        if ((rc = adj_alloc(X, &A.lxe, nt)) || (rc = adj_alloc(X, &A.ax0, nt)) || (rc = adj_alloc(X, &A.av0, nt)) ||
+            (rc = adj_alloc(X, &A.ar0, nt)) || (rc = adj_alloc(X, &A.sx, nt)) || (rc = adj_alloc(X, &A.su, nt)) ||
+            (rc = adj_alloc(X, &A.sr, nt)) || (rc = adj_alloc(X, &A.gbinv, nt)) || (rc = adj_alloc(X, &A.ggr, nt)) ||
+            (rc = adj_alloc(X, &A.gtau, nt)) || (rc = adj_alloc(X, &A.mu1, nt)) || (rc = adj_alloc(X, &A.mu2, nt)) ||
+            (rc = adj_alloc(X, &A.mu3, nt)) ||
+            (rc = adj_alloc(X, &A.nu_part, (size_t)4 * blocks((long long)nt * kAdjLanes, kAdjThreads))) ||
+            (rc = adj_alloc(X, &A.nu_acc, 1)) || (rc = adj_alloc(X, &A.lx, nt)) || (rc = adj_alloc(X, &A.lv, nt)) ||
+            (rc = adj_alloc(X, &A.lrho, nt)) || (rc = adj_alloc(X, &A.lk_r, nh)) || (rc = adj_alloc(X, &A.lk_a, nh)))
+            return rc;
+        // stage states: every step of a segment if that leaves 1 GiB free, else one
+        const size_t per_slot = 3 * nt * (sizeof(double2) + 2 * sizeof(double4));
+        size_t free_b = 0, total_b = 0;
+        CK(cudaMemGetInfo(&free_b, &total_b));
+        X->stage_slots = (per_slot * every + (size_t(1) << 30) <= free_b) ? every : 1;
+        const size_t ns = (size_t)X->stage_slots * 3 * nt;
+        if ((rc = adj_alloc(X, &X->st_pos, ns)) || (rc = adj_alloc(X, &X->st_kin, ns)) ||
+            (rc = adj_alloc(X, &X->st_aux, ns)))
+            return rc;
+    }
+    X->valid = false;
+    X->nsteps = ac->nsteps; X->every = every; X->nseg = nseg; X->loss = ac->loss; X->dt = ac->dt;
+    X->n_host = h->n_host;
+    X->seg_ntot.assign(every, 0);
+    return SPH_OK;
+}
+
+template <typename R>
+int adjoint_forward(sph_handle* h, const sph_adj_config* ac, double* loss) {
+    int rc = adj_prepare_ctx(h, ac);
+    if (rc) return rc;
+    AdjCtx* X = h->adj;
+    const int n = h->n_host;
+    if (ac->loss == SPH_LOSS_VELOCITY_MISFIT) {
+        CK(cudaMemcpyAsync(h->d_xfer, ac->target_vel, sizeof(double) * 2 * n, cudaMemcpyHostToDevice, h->stream));
+        k_interleave<<<blocks(n, 256), 256, 0, h->stream>>>(n, h->d_xfer, X->target);
+        h->launches += 1;
+    }
+    X->step0 = h->step_count;
+    for (int c = 0; c < X->nseg; ++c) {
+        if ((rc = unsort<R>(h)) || (rc = snap_io(h, X->ck, c, n, true))) return rc;
+        const int ns = std::min(X->every, X->nsteps - c * X->every);
+        if ((rc = run_steps<R>(h, ns, X->dt))) return rc;
+    }
+    if ((rc = unsort<R>(h)) || (rc = snap_io(h, X->ck, X->nseg, n, true))) return rc;
+    const int nparts = 148 * 4;
+    k_adj_loss<<<nparts, 256, 0, h->stream>>>(n, X->loss, h->S.type, h->S.vel, h->S.mass, X->target, X->loss_part);
+    h->launches += 2;
+    CK(cudaMemsetAsync(h->d_diag, 0, sizeof(double), h->stream));
+    k_adj_nu_sum<<<1, 256, 0, h->stream>>>(nparts, X->loss_part, h->d_diag);
+    double v = 0.0;
+    CK(cudaMemcpyAsync(&v, h->d_diag, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (loss) *loss = v;
+    X->valid = true;
+    return SPH_OK;
+}
+
+// The sorted arrays with the positions and records of stage state k of stage slot j.
+template <typename R>
+Sorted<R> stage_view(sph_handle* h, int j, int k) {
+    AdjCtx* X = h->adj;
+    Sorted<R> V = sorted<R>(h);
+    const size_t o = ((size_t)j * 3 + k) * (size_t)X->cap_tot;
+    V.pos = X->st_pos + o;
+    V.kin = X->st_kin + o;
+    V.aux = reinterpret_cast<typename VT<R>::V4*>(X->st_aux + o);
+    return V;
+}
+
+// Copy the current stage state into stage slot j, state k.
+template <typename R>
+int keep_stage(sph_handle* h, int j, int k) {
+    Sorted<R> V = stage_view<R>(h, j, k);
+    const int nt = h->P.n_tot;
+    k_keep_stage<R><<<blocks(nt, 256), 256, 0, h->stream>>>(nt, sorted<R>(h), V.pos, V.kin, V.aux);
+    CK(cudaGetLastError());
+    h->launches += 1;
+    return SPH_OK;
+}
+
+// One RK4 step exactly as run_steps takes it, keeping S1..S3 in stage slot j;
+// with full = false the step stops after S3 (all the reverse needs).
+template <typename R>
+int step_keep(sph_handle* h, double dt, int j, bool full) {
+    int rc = prepare<R>(h);
+    if (rc) return rc;
+    h->adj->seg_ntot[j] = h->P.n_tot;
+    const int first = h->step_count == 0;
+    if (first && (rc = rhs<R>(h, 0))) return rc;
+    if ((rc = stage<R>(h, 0, dt, first ? 0 : 1, 0)) || (rc = keep_stage<R>(h, j, 0))) return rc;
+    if ((rc = rhs<R>(h, 0)) || (rc = stage<R>(h, 1, dt, 0, 0)) || (rc = keep_stage<R>(h, j, 1))) return rc;
+    if ((rc = rhs<R>(h, 0)) || (rc = stage<R>(h, 2, dt, 0, 0)) || (rc = keep_stage<R>(h, j, 2))) return rc;
+    if (full) {
+        if ((rc = rhs<R>(h, 1)) || (rc = stage<R>(h, 3, dt, 0, h->cfg.shifting))) return rc;
+        h->step_count++;
+        h->n_steps++;
+    }
+    tic(h, -1);
+    if (h->ev_used > 4096) timing_flush(h);
+    return SPH_OK;
+}
+
+// Reverse of one RHS evaluation on the stage state V, with the rate adjoints
+// of RHS k of the step; stage = the stage that produced V (-1: the step start).
+template <typename R>
+int adj_rhs(sph_handle* h, const Sorted<R>& V, int k, int stage) {
+    const Params& P = h->P;
+    AdjCtx* X = h->adj;
+    Adj& A = X->A;
+    const int nb = blocks(P.n_tot, kAdjThreads);
+    const int nbc = blocks((long long)P.n_tot * kAdjLanes, kAdjThreads);
+    tic(h, PH_A);
+    k_pass_a<R><<<nb, 128, 0, h->stream>>>(P, V);
+    k_surface<R><<<nb, 128, 0, h->stream>>>(P, V);
+    k_near<R><<<nb, 128, 0, h->stream>>>(P, V);
+    tic(h, PH_ADJ);
+    k_adj_c<R><<<nbc, kAdjThreads, 0, h->stream>>>(P, V, A, A.lr[k], A.la[k], A.nu_part + (size_t)k * nbc);
+    k_adj_point<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, V, A);
+    k_adj_a<R><<<nb, kAdjThreads, 0, h->stream>>>(P, V, A, stage, X->dt);
+    CK(cudaGetLastError());
+    h->launches += 6;
+    return SPH_OK;
+}
+
+// Reverse of one time step from the staged step-start state: rebuild the
+// images, the sort and the lists (the same permutation as in the forward
+// run), take S1..S3 from stage slot j (or recompute them into slot 0 when
+// j < 0), then run the reverse kernels from the step end to its start.
+template <typename R>
+int adj_step(sph_handle* h, bool first, int j) {
+    AdjCtx* X = h->adj;
+    Adj& A = X->A;
+    const double dt = X->dt;
+    int rc;
+    if (j < 0) {
+        if ((rc = step_keep<R>(h, dt, 0, false))) return rc;
+        j = 0;
+    } else {
+        if ((rc = prepare<R>(h))) return rc;
+        if (h->P.n_tot != X->seg_ntot[j]) return SPH_E_ARG;
+    }
+    const Params& P = h->P;
+    Sorted<R>& D = sorted<R>(h);
+    const int nb = blocks(P.n_tot, 256);
+    tic(h, PH_ADJ);
+    k_adj_stage3<R><<<nb, 256, 0, h->stream>>>(P, D, A, dt);
+    h->launches += 1;
+    for (int k = 2; k >= 0; --k)
+        if ((rc = adj_rhs<R>(h, stage_view<R>(h, j, k), k + 1, k))) return rc;
+    if (first) {
+        // the fresh K1 of the first step was evaluated on the step-start state
+        k_adj_load<R><<<nb, 256, 0, h->stream>>>(P, D, nullptr, nullptr);
+        h->launches += 1;
+        if ((rc = adj_rhs<R>(h, D, 0, -1))) return rc;
+    }
+    tic(h, PH_ADJ);
+    const int nba = blocks((long long)P.n_tot * kAdjLanes, kAdjThreads);
+    k_adj_nu_sum<<<1, 256, 0, h->stream>>>((first ? 4 : 3) * nba, A.nu_part + (first ? 0 : nba), A.nu_acc);
+    k_adj_scatter<R><<<nb, 256, 0, h->stream>>>(P, D, A, first ? 1 : 0);
+    h->launches += 2;
+    if (h->cfg.periodic) {
+        const int n_src = h->n_host + h->n_lr;
+        k_adj_route<<<blocks(n_src, 256), 256, 0, h->stream>>>(n_src, n_src, h->S.tb_cnt, h->S.tb_off, A);
+        k_adj_route<<<blocks(h->n_host, 256), 256, 0, h->stream>>>(h->n_host, h->n_host, h->S.lr_cnt, h->S.lr_off,
+                                                                     A);
+        h->launches += 2;
+    }
+    CK(cudaGetLastError());
+    tic(h, -1);
+    if (h->ev_used > 4096) timing_flush(h);
+    return SPH_OK;
+}
+
+template <typename R>
+int adjoint_backward(sph_handle* h, double dloss, double* g_vel0, double* g_rho0, double* g_pos0,
+                     double* g_params) {
+    AdjCtx* X = h->adj;
+    if (!X || !X->valid || X->n_host != h->n_host) return SPH_E_ARG;
+    Adj& A = X->A;
+    const int n = h->n_host;
+    const bool stored = X->stage_slots >= X->every;
+    int rc;
+    // seed from the final state
+    if ((rc = unsort<R>(h)) || (rc = snap_io(h, X->ck, X->nseg, n, false))) return rc;
+    k_adj_seed<<<blocks(n, 256), 256, 0, h->stream>>>(n, X->loss, dloss, h->S.type, h->S.vel, h->S.mass, X->target,
+                                                     A);
+    h->launches += 1;
+    CK(cudaMemsetAsync(A.nu_acc, 0, sizeof(double), h->stream));
+    for (int c = X->nseg - 1; c >= 0; --c) {
+        const int s0 = c * X->every, s1 = std::min(s0 + X->every, X->nsteps);
+        // re-run the segment from its checkpoint, keeping every step-start state
+        // (and the stage states when they fit)
+        if ((rc = snap_io(h, X->ck, c, n, false))) return rc;
+        h->step_count = X->step0 + s0;
+        for (int j = s0; j < s1; ++j) {
+            if ((rc = unsort<R>(h)) || (rc = snap_io(h, X->seg, j - s0, n, true))) return rc;
+            if (stored) rc = step_keep<R>(h, X->dt, j - s0, j + 1 < s1);
+            else if (j + 1 < s1) rc = run_steps<R>(h, 1, X->dt);
+            if (rc) return rc;
+        }
+        for (int j = s1 - 1; j >= s0; --j) {
+            if ((rc = snap_io(h, X->seg, j - s0, n, false))) return rc;
+            h->step_count = X->step0 + j;
+            if ((rc = adj_step<R>(h, X->step0 + j == 0, stored ? j - s0 : -1))) return rc;
+        }
+    }
+    timing_flush(h);
+    if ((rc = read_status(h))) return rc;
+    // gradients with respect to the state the forward started from (id order)
+    if (g_vel0) {
+        k_deinterleave<<<blocks(n, 256), 256, 0, h->stream>>>(n, A.lv, h->d_xfer);
+        CK(cudaMemcpyAsync(g_vel0, h->d_xfer, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    if (g_pos0) {
+        k_deinterleave<<<blocks(n, 256), 256, 0, h->stream>>>(n, A.lx, h->d_xfer);
+        CK(cudaMemcpyAsync(g_pos0, h->d_xfer, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    if (g_rho0) CK(cudaMemcpyAsync(g_rho0, A.lrho, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+    if (g_params) CK(cudaMemcpyAsync(g_params, A.nu_acc, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    // the handle continues from the forward's final state
+    if ((rc = snap_io(h, X->ck, X->nseg, n, false))) return rc;
+    h->step_count = X->step0 + X->nsteps;
+    h->have_rhs = false;
+    return SPH_OK;
+}
+
 // Dispatch on the pair precision of the handle.
 #define DISPATCH(h, fn, ...) ((h)->mixed ? fn<float>(__VA_ARGS__) : fn<double>(__VA_ARGS__))
 
@@ -520,9 +854,10 @@ void destroy(sph_handle* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     free_sorted(h->D64);
     free_sorted(h->D32);
+    if (h->adj) { adj_free_all(h->adj); delete h->adj; }
     void* ptrs[] = {h->S.pos, h->S.vel, h->S.rho, h->S.mass, h->S.smass, h->S.type, h->S.itype, h->d_bf,
                     h->S.r_drho, h->S.r_acc,
-                    h->S.r_avg, h->S.cnt, h->S.off, h->keys_in, h->keys_out, h->vals_in, h->vals_out, h->cub_tmp,
+                    h->S.r_avg, h->S.cnt, h->S.off, h->S.lr_cnt, h->S.lr_off, h->S.tb_cnt, h->S.tb_off, h->keys_in, h->keys_out, h->vals_in, h->vals_out, h->cub_tmp,
                     h->d_status, h->d_int, h->d_part, h->d_diag, h->d_xfer, h->d_export, h->d_off64, h->d_cnt_id};
     for (void* p : ptrs) if (p) cudaFree(p);
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
@@ -563,6 +898,8 @@ int init_impl(const sph_config* cfg, int n_capacity, sph_handle** out) {
     CK(dalloc(&h->d_bf, (size_t)6 * blocks(cap, kRedThreads) + 6));
     CK(dalloc(&h->S.r_drho, h->cap_host)); CK(dalloc(&h->S.r_acc, h->cap_host)); CK(dalloc(&h->S.r_avg, h->cap_host));
     CK(dalloc(&h->S.cnt, cap)); CK(dalloc(&h->S.off, cap));
+    CK(dalloc(&h->S.lr_cnt, cap)); CK(dalloc(&h->S.lr_off, cap));
+    CK(dalloc(&h->S.tb_cnt, cap)); CK(dalloc(&h->S.tb_off, cap));
     // sort
     CK(dalloc(&h->keys_in, cap)); CK(dalloc(&h->keys_out, cap));
     CK(dalloc(&h->vals_in, cap)); CK(dalloc(&h->vals_out, cap));
@@ -792,6 +1129,24 @@ int sph_diagnostics(sph_handle* h, sph_diag* out) {
     return DISPATCH(h, diagnostics, h, out);
 }
 
+int sph_adjoint_forward(sph_handle* h, const sph_adj_config* cfg, double* loss) {
+    if (!h || !cfg || h->n_host <= 0 || cfg->nsteps <= 0 || cfg->checkpoint_every <= 0 || !(cfg->dt > 0))
+        return SPH_E_ARG;
+    if (cfg->loss != SPH_LOSS_VELOCITY_MISFIT && cfg->loss != SPH_LOSS_KINETIC_ENERGY) return SPH_E_ARG;
+    if (cfg->loss == SPH_LOSS_VELOCITY_MISFIT && !cfg->target_vel) return SPH_E_ARG;
+    int rc = adj_config_ok(h);
+    if (rc) return rc;
+    CK(cudaSetDevice(h->device));
+    return DISPATCH(h, adjoint_forward, h, cfg, loss);
+}
+
+int sph_adjoint_backward(sph_handle* h, double dloss, double* g_vel0, double* g_rho0, double* g_pos0,
+                         double* g_params) {
+    if (!h) return SPH_E_ARG;
+    CK(cudaSetDevice(h->device));
+    return DISPATCH(h, adjoint_backward, h, dloss, g_vel0, g_rho0, g_pos0, g_params);
+}
+
 int sph_get_timings(sph_handle* h, sph_timings* out) {
     if (!h || !out) return SPH_E_ARG;
     timing_flush(h);
@@ -805,6 +1160,7 @@ int sph_get_timings(sph_handle* h, sph_timings* out) {
     out->rhs_evaluations = h->n_rhs;
     out->steps = h->n_steps;
     out->kernel_launches = h->launches;
+    out->adjoint_ms = h->t_ms[PH_ADJ];
     return SPH_OK;
 }
 

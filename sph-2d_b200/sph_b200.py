@@ -51,12 +51,15 @@ TYPE_PERIODIC = -101
 TYPE_ILL = 120
 TYPE_FIX_GHOST = -3
 TYPE_BODY = -4
+LOSS_VELOCITY_MISFIT = 0
+LOSS_KINETIC_ENERGY = 1
+ADJ_NPARAMS = 1
 
 EXPORTED_SYMBOLS = (
     "sph_init", "sph_free", "sph_set_state", "sph_get_state", "sph_find_particle_pair",
     "sph_rhs", "sph_step", "sph_diagnostics", "sph_get_timings", "sph_reset_timings",
     "sph_strerror", "sph_get_field", "sph_update_state", "sph_find_particle_pair_noalloc",
-    "sph_set_initial_type",
+    "sph_set_initial_type", "sph_adjoint_forward", "sph_adjoint_backward",
 )
 
 
@@ -91,12 +94,19 @@ class SphDiag(ctypes.Structure):
     ]
 
 
+class SphAdjConfig(ctypes.Structure):
+    _fields_ = [
+        ("nsteps", ctypes.c_int), ("checkpoint_every", ctypes.c_int), ("loss", ctypes.c_int),
+        ("reserved", ctypes.c_int), ("dt", ctypes.c_double), ("target_vel", ctypes.POINTER(ctypes.c_double)),
+    ]
+
+
 class SphTimings(ctypes.Structure):
     _fields_ = [
         ("sort_ms", ctypes.c_double), ("pass_a_ms", ctypes.c_double), ("surface_ms", ctypes.c_double),
         ("pass_c_ms", ctypes.c_double), ("update_ms", ctypes.c_double), ("images_ms", ctypes.c_double),
         ("total_ms", ctypes.c_double), ("rhs_evaluations", ctypes.c_longlong), ("steps", ctypes.c_longlong),
-        ("kernel_launches", ctypes.c_longlong),
+        ("kernel_launches", ctypes.c_longlong), ("adjoint_ms", ctypes.c_double),
     ]
 
 
@@ -252,6 +262,8 @@ def load(path: str = LIB_PATH):
     lib.sph_get_timings.argtypes = [P, ctypes.POINTER(SphTimings)]
     lib.sph_reset_timings.argtypes = [P]
     lib.sph_get_field.argtypes = [P, ctypes.c_int, dp]
+    lib.sph_adjoint_forward.argtypes = [P, ctypes.POINTER(SphAdjConfig), dp]
+    lib.sph_adjoint_backward.argtypes = [P, ctypes.c_double, dp, dp, dp, dp]
     lib.sph_find_particle_pair_noalloc.argtypes = [ctypes.POINTER(SphConfig), ctypes.c_int, ctypes.c_void_p,
                                                    ctypes.c_void_p, ctypes.c_longlong, ctypes.c_void_p,
                                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
@@ -389,6 +401,31 @@ class Simulation:
     def reset_timings(self):
         _check(self.lib.sph_reset_timings(self.h), "sph_reset_timings")
 
+    def adjoint_forward(self, nsteps: int, dt: float, checkpoint_every: int = 32,
+                        loss: int = LOSS_VELOCITY_MISFIT, target_vel=None) -> float:
+        """nsteps time steps with state checkpoints every checkpoint_every steps;
+        returns the loss of the final state (sph_adjoint_forward)."""
+        a = SphAdjConfig()
+        a.nsteps, a.checkpoint_every, a.loss, a.dt = int(nsteps), int(checkpoint_every), int(loss), float(dt)
+        keep = None
+        if target_vel is not None:
+            keep = np.ascontiguousarray(target_vel, np.float64)
+            if keep.shape != (2 * self.n,):
+                raise ValueError("target_vel must hold 2n values (u block, v block)")
+            a.target_vel = keep.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        out = ctypes.c_double(0.0)
+        _check(self.lib.sph_adjoint_forward(self.h, ctypes.byref(a), ctypes.byref(out)), "sph_adjoint_forward")
+        return out.value
+
+    def adjoint_backward(self, dloss: float = 1.0) -> dict:
+        """Gradient of dloss * loss with respect to the state the last
+        adjoint_forward started from and to the viscosity."""
+        n = self.n
+        gv = np.zeros(2 * n); gx = np.zeros(2 * n); gr = np.zeros(n); gp = np.zeros(ADJ_NPARAMS)
+        _check(self.lib.sph_adjoint_backward(self.h, float(dloss), _ptr(gv), _ptr(gr), _ptr(gx), _ptr(gp)),
+               "sph_adjoint_backward")
+        return {"vel0": gv, "rho0": gr, "pos0": gx, "nu": float(gp[0])}
+
 
 @dataclass
 class TgvCase:
@@ -418,6 +455,29 @@ def make_tgv(n_side: int, reference: bool = False, solver: int = SOLVER_MUSCL_DE
         pos = pos + rng.uniform(-jitter, jitter, pos.shape) * cfg.dx
     typ = np.full(rho.shape[0], TYPE_WATER, np.int32)
     return TgvCase(cfg, pos, vel, rho, mass, typ)
+
+
+def fourier_perturbation(pos, n_modes: int = 8, amp: float = 0.05, seed: int = 0, kmax: int = 4,
+                         box: float = 1.0) -> np.ndarray:
+    """A divergence-free velocity perturbation on the periodic box: the curl of
+    a sum of n_modes stream-function modes sin(2 pi (kx x + ky y)/L + phase)
+    with random integer wave numbers 1..kmax, random phases and weights,
+    scaled so that its largest speed is amp.  pos is the 2n column-major
+    position array; returns 2n values (u block, v block)."""
+    n = pos.shape[0] // 2
+    x, y = pos[:n], pos[n:]
+    rng = np.random.default_rng(seed)
+    u = np.zeros(n); v = np.zeros(n)
+    for _ in range(n_modes):
+        kx, ky = rng.integers(1, kmax + 1, 2) * rng.choice([-1, 1], 2)
+        ph = rng.uniform(0.0, 2.0 * np.pi)
+        wgt = rng.uniform(0.5, 1.0)
+        arg = 2.0 * np.pi * (kx * x + ky * y) / box + ph
+        c = np.cos(arg) * wgt * 2.0 * np.pi / box
+        u += c * ky          # d psi / dy
+        v -= c * kx          # -d psi / dx
+    scale = amp / max(np.sqrt(u * u + v * v).max(), 1e-300)
+    return np.concatenate([u, v]) * scale
 
 
 # ---------------------------------------------------------------------------

@@ -1,0 +1,173 @@
+"""The discrete adjoint of the time step (sph_adjoint_forward / sph_adjoint_backward)
+against central finite differences of the FP64 forward step on the GPU.
+
+The adjoint's directional derivative g.delta must match
+(L(x + eps delta) - L(x - eps delta)) / (2 eps) to 1e-4 relative for seeded
+directions in the initial velocity, density and position fields and for the
+viscosity, on the Wendland/renormalised case and on the reference's own
+Taylor-Green parameters (Gaussian kernel, inverse discarded, default-real
+literals).  Gradients must not depend on the checkpoint interval, and the
+handle must hold the forward's final state after the backward pass.
+
+The step size: eps = 1e-6 for Wendland C2, whose gradient goes to zero at the
+support radius, so the loss is smooth in the state.  The improved Gaussian
+is cut off at 3h with a gradient of exp(-9) times its scale left at the cut,
+so every pair that crosses the support radius puts a kink into the loss; a
+difference quotient whose interval straddles one is off by up to 1e-2
+relative at eps = 1e-6 (and exact again at 1e-7).  The Gaussian cases use
+eps ten times smaller, which keeps the interval clear of kinks while the
+rounding error of the FP64 loss stays below 1e-8 relative.
+"""
+import numpy as np
+import pytest
+
+import sph_b200 as S
+
+pytestmark = pytest.mark.gpu
+
+NSTEPS = 12
+REL_TOL = 1e-4
+
+
+def _case(kind):
+    if kind == "wendland-renorm":
+        case = S.make_tgv(32, solver=S.SOLVER_MODLR_DELTA_SPS, jitter=0.05, seed=11)
+    else:
+        case = S.make_tgv(32, reference=True, jitter=0.05, seed=12)
+    case.cfg.shifting = 0
+    return case
+
+
+def _target(case, dt, seed=5):
+    dv = S.fourier_perturbation(case.pos, n_modes=8, amp=0.05, seed=seed)
+    with S.Simulation(case.cfg, case.n) as sim:
+        sim.set_state(case.pos, case.vel + dv, case.rho, case.mass, case.type)
+        sim.time_iteration(NSTEPS, dt)
+        return sim.get_state()[1]
+
+
+def _loss(case, dt, target, pos=None, vel=None, rho=None, nu=None, loss=S.LOSS_VELOCITY_MISFIT, pre_steps=0):
+    cfg = case.cfg.copy()
+    if nu is not None:
+        cfg.nu = nu
+    with S.Simulation(cfg, case.n) as sim:
+        sim.set_state(case.pos, case.vel, case.rho, case.mass, case.type)
+        if pre_steps:
+            sim.time_iteration(pre_steps, dt)
+            p0, v0, r0, _ = sim.get_state()
+            sim.update_state(p0 if pos is None else p0 + pos, v0 if vel is None else v0 + vel,
+                             r0 if rho is None else r0 + rho)
+        else:
+            sim.update_state(case.pos if pos is None else case.pos + pos, case.vel if vel is None else case.vel + vel,
+                             case.rho if rho is None else case.rho + rho)
+        return sim.adjoint_forward(NSTEPS, dt, checkpoint_every=NSTEPS, loss=loss, target_vel=target)
+
+
+def _grad(case, dt, target, every=5, loss=S.LOSS_VELOCITY_MISFIT, pre_steps=0):
+    with S.Simulation(case.cfg, case.n) as sim:
+        sim.set_state(case.pos, case.vel, case.rho, case.mass, case.type)
+        if pre_steps:
+            sim.time_iteration(pre_steps, dt)
+        L = sim.adjoint_forward(NSTEPS, dt, checkpoint_every=every, loss=loss, target_vel=target)
+        end = sim.get_state()
+        g = sim.adjoint_backward(1.0)
+        after = sim.get_state()
+    return L, g, end, after
+
+
+def _eps_scale(case):
+    return 1.0 if case.cfg.kernel_model == S.KERNEL_WENDLAND2 else 0.1
+
+
+def _check(ad, fd, what):
+    assert abs(ad - fd) <= REL_TOL * abs(fd), (what, ad, fd, abs(ad - fd) / abs(fd))
+
+
+@pytest.mark.parametrize("kind", ["wendland-renorm", "reference-gaussian"])
+@pytest.mark.parametrize("pre_steps", [0, 3])
+def test_adjoint_matches_central_differences(lib, kind, pre_steps):
+    case = _case(kind)
+    dt = S.baseline_dt(case.cfg)
+    target = _target(case, dt)
+    L, g, end, after = _grad(case, dt, target, pre_steps=pre_steps)
+    assert np.isfinite(L) and L > 0
+    assert all(np.array_equal(a, b) for a, b in zip(end, after))
+    n = case.n
+    sc = _eps_scale(case)
+    for k in range(3):
+        rng = np.random.default_rng(100 + k)
+        d = rng.standard_normal(2 * n)
+        eps = 1e-6 * sc
+        fd = (_loss(case, dt, target, vel=eps * d, pre_steps=pre_steps)
+              - _loss(case, dt, target, vel=-eps * d, pre_steps=pre_steps)) / (2 * eps)
+        _check(float(g["vel0"] @ d), fd, f"velocity direction {k}")
+    rng = np.random.default_rng(200)
+    d = rng.standard_normal(n) * case.cfg.rho0
+    eps = 1e-7 * sc
+    fd = (_loss(case, dt, target, rho=eps * d, pre_steps=pre_steps)
+          - _loss(case, dt, target, rho=-eps * d, pre_steps=pre_steps)) / (2 * eps)
+    _check(float(g["rho0"] @ d), fd, "density direction")
+    d = rng.standard_normal(2 * n) * case.cfg.dx
+    eps = 1e-6 * sc
+    fd = (_loss(case, dt, target, pos=eps * d, pre_steps=pre_steps)
+          - _loss(case, dt, target, pos=-eps * d, pre_steps=pre_steps)) / (2 * eps)
+    _check(float(g["pos0"] @ d), fd, "position direction")
+    if pre_steps == 0:
+        nu = case.cfg.nu
+        e = 1e-4 * sc * nu
+        fd = (_loss(case, dt, target, nu=nu + e) - _loss(case, dt, target, nu=nu - e)) / (2 * e)
+        _check(g["nu"], fd, "viscosity")
+
+
+def test_adjoint_kinetic_energy_loss(lib):
+    case = _case("wendland-renorm")
+    dt = S.baseline_dt(case.cfg)
+    L, g, end, _ = _grad(case, dt, None, loss=S.LOSS_KINETIC_ENERGY)
+    v = end[1]
+    n = case.n
+    assert L == pytest.approx(0.5 * float(np.sum(case.mass * (v[:n] ** 2 + v[n:] ** 2))), rel=1e-12)
+    rng = np.random.default_rng(7)
+    d = rng.standard_normal(2 * n)
+    eps = 1e-6
+    fd = (_loss(case, dt, None, vel=eps * d, loss=S.LOSS_KINETIC_ENERGY)
+          - _loss(case, dt, None, vel=-eps * d, loss=S.LOSS_KINETIC_ENERGY)) / (2 * eps)
+    _check(float(g["vel0"] @ d), fd, "kinetic energy, velocity direction")
+
+
+def test_adjoint_independent_of_checkpoint_interval(lib):
+    case = _case("reference-gaussian")
+    dt = S.baseline_dt(case.cfg)
+    target = _target(case, dt)
+    ref = _grad(case, dt, target, every=NSTEPS)[1]
+    for every in (1, 5):
+        g = _grad(case, dt, target, every=every)[1]
+        for key in ("vel0", "rho0", "pos0"):
+            assert np.array_equal(g[key], ref[key]), (every, key)
+        assert g["nu"] == ref["nu"]
+
+
+def test_adjoint_rejects_unsupported_configurations(lib):
+    case = S.make_tgv(16, solver=S.SOLVER_MUSCL_DELTA_SPS)
+    with S.Simulation(case.cfg, case.n) as sim:
+        sim.set_state(case.pos, case.vel, case.rho, case.mass, case.type)
+        with pytest.raises(S.SphError) as e:
+            sim.adjoint_forward(2, 1e-4, loss=S.LOSS_KINETIC_ENERGY)
+        assert e.value.code == -7
+        with pytest.raises(S.SphError) as e:
+            sim.adjoint_backward()
+        assert e.value.code == -1
+
+
+def test_adjoint_of_the_mixed_precision_step(lib):
+    """Forward and recomputation in the mixed path, reverse kernels in FP64: the
+    gradient stays within 1e-4 (L2, relative) of the FP64 path's gradient."""
+    case = _case("wendland-renorm")
+    dt = S.baseline_dt(case.cfg)
+    target = _target(case, dt)
+    g64 = _grad(case, dt, target)[1]
+    case.cfg.precision = S.PREC_MIXED
+    gm = _grad(case, dt, target)[1]
+    for key in ("vel0", "rho0", "pos0"):
+        err = np.linalg.norm(gm[key] - g64[key]) / np.linalg.norm(g64[key])
+        assert err < 1e-4, (key, err)
+    assert abs(gm["nu"] - g64["nu"]) <= 1e-4 * abs(g64["nu"])
