@@ -56,6 +56,8 @@ def load():
     lib.oracle_set_initial_type.argtypes = [ctypes.c_void_p, ctypes.c_int, ip]
     lib.oracle_body_force.argtypes = [ctypes.c_void_p, dp]
     lib.oracle_rhs_body_force.argtypes = [cp, ctypes.c_int, dp, dp, dp, dp, ip, ip, dp]
+    lib.oracle_tangent.argtypes = [cp, ctypes.c_int, dp, dp, dp, dp, ip, dp, dp, dp, ctypes.c_double, ctypes.c_int,
+                                   ctypes.c_double, ctypes.c_int, dp, dp, dp, dp, dp]
     _lib = lib
     return lib
 
@@ -181,3 +183,23 @@ def rhs_body_force(cfg: SphConfig, pos, vel, rho, mass, type_, itype):
     load().oracle_rhs_body_force(ctypes.byref(cfg), rho.shape[0], _p(a[0]), _p(a[1]), _p(a[2]), _p(a[3]),
                                  _p(t, ctypes.c_int), _p(it, ctypes.c_int), _p(out))
     return out
+
+
+def tangent(cfg: SphConfig, pos, vel, rho, mass, type_, nsteps: int, dt: float, dpos=None, dvel=None, drho=None,
+            dnu: float = 0.0, loss: int = 0, target_vel=None):
+    """FP64 tangent-linear model (sph_tangent.cpp): the loss of the state after
+    nsteps steps, its derivative along (dpos, dvel, drho, dnu), and the final
+    state.  loss 0: squared velocity misfit against target_vel, 1: kinetic energy."""
+    n = rho.shape[0]
+    a = [np.ascontiguousarray(x, np.float64) for x in (pos, vel, rho, mass)]
+    t = np.ascontiguousarray(type_, np.int32)
+    d = [None if x is None else np.ascontiguousarray(x, np.float64) for x in (dpos, dvel, drho)]
+    tg = None if target_vel is None else np.ascontiguousarray(target_vel, np.float64)
+    out = np.zeros(2)
+    P = np.zeros(2 * n); V = np.zeros(2 * n); R = np.zeros(n)
+    rc = load().oracle_tangent(ctypes.byref(cfg), n, _p(a[0]), _p(a[1]), _p(a[2]), _p(a[3]), _p(t, ctypes.c_int),
+                               _p(d[0]), _p(d[1]), _p(d[2]), float(dnu), int(nsteps), float(dt), int(loss), _p(tg),
+                               _p(out), _p(P), _p(V), _p(R))
+    if rc != 0:
+        raise RuntimeError(f"oracle_tangent failed ({rc})")
+    return out[0], out[1], (P, V, R)

@@ -1,0 +1,469 @@
+// sph_tangent.cpp -- FP64 tangent-linear model of the Taylor-Green time step.
+//
+// TEST INFRASTRUCTURE ONLY: the CPU reference the GPU adjoint
+// (sph_adjoint_forward / sph_adjoint_backward) is checked against.  Never
+// linked into, loaded by or called from the product path.
+//
+// The step is written once, templated on the scalar type: with double it is a
+// second restatement of the oracle's Taylor-Green step (the pair loops of
+// Solver_Normalized_Modified_Linear_Riemann_Delta_SPS.f90:126-583 and the
+// Runge-Kutta stages of time_iteration.f90:781-1073, in the oracle's pair
+// orientation and term order), pinned against sph_oracle.cpp by the tests;
+// with Dual (value + one directional derivative, forward-mode differentiation)
+// it returns the loss and its derivative along a chosen direction of the
+// initial position, velocity, density and viscosity: the tangent-linear model.
+// Branches (support test, max/min of the Riemann dissipation, the artificial-
+// viscosity switch, periodic wrap and images) are taken on the values, so the
+// derivative is that of the taken branch with the pair set held fixed, which
+// is what the adjoint differentiates too.
+//
+// Scope: the modified linear Riemann delta-SPH + SPS solver, RK4 with the K1
+// reuse, periodic images, either kernel, with or without renormalisation,
+// no shifting, no XSPH, no free-surface particles.  Other inputs return
+// SPH_E_CONFIG.  The pair search is a plain double loop (small cases only).
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "../include/sph_b200.h"
+
+namespace {
+
+struct Dual {
+    double v, d;
+    Dual(double a = 0.0, double b = 0.0) : v(a), d(b) {}
+};
+inline Dual operator+(Dual a, Dual b) { return {a.v + b.v, a.d + b.d}; }
+inline Dual operator-(Dual a, Dual b) { return {a.v - b.v, a.d - b.d}; }
+inline Dual operator-(Dual a) { return {-a.v, -a.d}; }
+inline Dual operator*(Dual a, Dual b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
+inline Dual operator/(Dual a, Dual b) { return {a.v / b.v, (a.d * b.v - a.v * b.d) / (b.v * b.v)}; }
+inline Dual operator+(Dual a, double b) { return {a.v + b, a.d}; }
+inline Dual operator+(double a, Dual b) { return {a + b.v, b.d}; }
+inline Dual operator-(Dual a, double b) { return {a.v - b, a.d}; }
+inline Dual operator-(double a, Dual b) { return {a - b.v, -b.d}; }
+inline Dual operator*(Dual a, double b) { return {a.v * b, a.d * b}; }
+inline Dual operator*(double a, Dual b) { return {a * b.v, a * b.d}; }
+inline Dual operator/(Dual a, double b) { return {a.v / b, a.d / b}; }
+inline Dual operator/(double a, Dual b) { return {a / b.v, -a * b.d / (b.v * b.v)}; }
+inline Dual& operator+=(Dual& a, Dual b) { a = a + b; return a; }
+inline Dual& operator-=(Dual& a, Dual b) { a = a - b; return a; }
+inline Dual sqrt(Dual a) { double s = std::sqrt(a.v); return {s, s > 0.0 ? a.d / (2.0 * s) : 0.0}; }
+inline Dual exp(Dual a) { double e = std::exp(a.v); return {e, e * a.d}; }
+inline double val(double a) { return a; }
+inline double val(const Dual& a) { return a.v; }
+using std::exp;
+using std::sqrt;
+
+// Constants of the configuration (the same derivation as the oracle's).
+struct TConsts {
+    double pi_k, pi, e9, den, cut_min, fs_thr, dl, c012, c23, cblin, sqrt_c0, eos_b, sv, q_zero;
+};
+
+TConsts derive(const sph_config& c) {
+    TConsts K;
+    const bool q = c.reference_literals != 0;
+    K.pi = 3.14159265358979324;
+    K.pi_k = q ? (double)3.14159265358f : K.pi;
+    if (q) {
+        float e9 = std::exp(-9.0f);
+        K.e9 = (double)e9;
+        K.den = (double)(1.0f - 10.0f * e9);
+        K.cut_min = (double)1.0e-7f;
+        K.fs_thr = (double)(float)c.fs_threshold;
+        K.dl = (double)(std::sqrt(2.0f) / 2.0f);
+        K.c012 = (double)0.12f;
+        K.c23 = (double)(2.0f / 3.0f);
+        K.cblin = (double)((2.0f / 3.0f) * 0.0066f);
+        K.q_zero = (double)1.0e-8f;
+    } else {
+        K.e9 = std::exp(-9.0);
+        K.den = 1.0 - 10.0 * K.e9;
+        K.cut_min = 1.0e-7;
+        K.fs_thr = c.fs_threshold;
+        K.dl = std::sqrt(2.0) / 2.0;
+        K.c012 = 0.12;
+        K.c23 = 2.0 / 3.0;
+        K.cblin = 2.0 / 3.0 * 0.0066;
+        K.q_zero = 1.0e-8;
+    }
+    K.sqrt_c0 = std::sqrt(c.c0sq);
+    K.eos_b = c.c0sq * c.rho0 / 7.0;
+    const double sr = c.kernel_scale * c.h;
+    K.sv = K.pi * (sr * sr);
+    return K;
+}
+
+// All particles of one step (hosts, then periodic images).
+template <class T>
+struct Parts {
+    std::vector<T> x, y, u, v, rho;
+    std::vector<double> mass, smass;
+    std::vector<int> type;
+    int n = 0;
+    void push(const T& x_, const T& y_, const T& u_, const T& v_, const T& r_, double m, double sm, int t) {
+        x.push_back(x_); y.push_back(y_); u.push_back(u_); v.push_back(v_); rho.push_back(r_);
+        mass.push_back(m); smass.push_back(sm); type.push_back(t);
+        ++n;
+    }
+};
+
+template <class T>
+struct Model {
+    sph_config C;
+    TConsts K;
+    T nu;
+
+    // compute_kernel (Taylor_Green_Vortex/compute_kernel.f90:120-142; Wendland C2 of
+    // Moving_Square.../Compute_Kernel.f90:179-193)
+    void kernel(const T& d, const T& p0, const T& p1, double h, T& w, T& g0, T& g1) const {
+        const T q = d / h;
+        w = T(0.0); g0 = T(0.0); g1 = T(0.0);
+        if (C.kernel_model == SPH_KERNEL_GAUSSIAN) {
+            const double factor = 1.0 / (K.pi_k * (h * h) * K.den);
+            if (val(d) <= 3.0 * h) {
+                const T e = exp(-(q * q));
+                w = (e - K.e9) * factor;
+                g0 = (e * (-2.0 * q)) * p0 / (d * h) * factor;
+                g1 = (e * (-2.0 * q)) * p1 / (d * h) * factor;
+            }
+        } else {
+            const double factor = 7.0 / (4 * K.pi_k * (h * h));
+            if (val(d) <= 2.0 * h) {
+                const T t = 1.0 - q / 2.0;
+                const T t2 = t * t;
+                w = factor * (1.0 + 2.0 * q) * (t2 * t2);
+                g0 = factor * (-5.0 * q * (t2 * t)) * p0 / (d * h);
+                g1 = factor * (-5.0 * q * (t2 * t)) * p1 / (d * h);
+            }
+        }
+        if (val(q) <= K.q_zero) { g0 = T(0.0); g1 = T(0.0); }
+    }
+
+    // status_equation (Taylor_Green_Vortex/status_equation.f90:60-63)
+    void eos(const T& rho, T& p, T& c) const {
+        const T r = rho / C.rho0;
+        const T r3 = r * r * r;
+        if (C.eos == SPH_EOS_TAIT) p = K.eos_b * (r3 * r3 * r - 1.0) + C.background_p;
+        else p = C.c0sq * (rho - C.rho0) + C.background_p;
+        c = K.sqrt_c0 * r3;
+    }
+
+    // single_step_compute with the modified linear Riemann solver: drho and acc
+    // of every particle (zero acceleration for non-water particles).
+    int rhs(const Parts<T>& P, std::vector<T>& drho, std::vector<T>& acc0, std::vector<T>& acc1) const {
+        const int n = P.n;
+        std::vector<T> p(n), c(n), vol(n);
+        for (int i = 0; i < n; ++i) { eos(P.rho[i], p[i], c[i]); vol[i] = P.mass[i] / P.rho[i]; }
+        const double hb = (C.h + C.h) / 2.0;
+        const double rcut = C.kernel_scale * hb;
+        // find_particle_pair (find_particle_pair.f90:64-123): every i < j within the support
+        std::vector<int> pi, pj;
+        for (int i = 0; i < n - 1; ++i)
+            for (int j = i + 1; j < n; ++j) {
+                if (P.type[i] != SPH_TYPE_WATER && P.type[j] != SPH_TYPE_WATER) continue;
+                const double a = val(P.x[i]) - val(P.x[j]), b = val(P.y[i]) - val(P.y[j]);
+                if (std::fabs(a) > rcut || std::fabs(b) > rcut) continue;
+                const double d = std::sqrt(a * a + b * b);
+                if (d <= rcut && d >= K.cut_min) { pi.push_back(i); pj.push_back(j); }
+            }
+        const size_t np = pi.size();
+        std::vector<T> dx0(np), dx1(np), w(np), dw0(np), dw1(np);
+        for (size_t k = 0; k < np; ++k) {
+            const int i = pi[k], j = pj[k];
+            dx0[k] = P.x[i] - P.x[j]; dx1[k] = P.y[i] - P.y[j];
+            const T d = sqrt(dx0[k] * dx0[k] + dx1[k] * dx1[k]);
+            kernel(d, dx0[k], dx1[k], hb, w[k], dw0[k], dw1[k]);
+        }
+        // volume fraction: free-surface candidates are outside this model's scope
+        if (C.free_surface) {
+            std::vector<double> fra(n, 0.0);
+            for (size_t k = 0; k < np; ++k) {
+                fra[pi[k]] += val(vol[pj[k]]) / K.sv;
+                fra[pj[k]] += val(vol[pi[k]]) / K.sv;
+            }
+            for (int i = 0; i < n; ++i)
+                if (P.type[i] == SPH_TYPE_WATER && fra[i] <= K.fs_thr) return SPH_E_CONFIG;
+        }
+        // B(L,o) += (x_j - x_i)_L dwdx_o V (Define_freesurface...f90:137-159) and its inverse
+        std::vector<T> bi[4];
+        for (int q = 0; q < 4; ++q) bi[q].assign(n, T(q == 0 || q == 3 ? 1.0 : 0.0));
+        if (C.renormalize) {
+            std::vector<T> B[4];
+            for (int q = 0; q < 4; ++q) B[q].assign(n, T(0.0));
+            for (size_t k = 0; k < np; ++k) {
+                const int i = pi[k], j = pj[k];
+                const T pd[2] = {-dx0[k], -dx1[k]}, dw[2] = {dw0[k], dw1[k]};
+                for (int a = 0; a < 2; ++a)
+                    for (int o = 0; o < 2; ++o) {
+                        B[a * 2 + o][i] += pd[a] * dw[o] * vol[j];
+                        B[a * 2 + o][j] += pd[a] * dw[o] * vol[i];
+                    }
+            }
+            for (int i = 0; i < n; ++i) {
+                if (P.type[i] != SPH_TYPE_WATER) continue;
+                const T det = B[0][i] * B[3][i] - B[1][i] * B[2][i];
+                if (val(det) == 0.0) continue;
+                bi[0][i] = B[3][i] / det; bi[1][i] = -B[1][i] / det;
+                bi[2][i] = -B[2][i] / det; bi[3][i] = B[0][i] / det;
+            }
+        }
+        std::vector<T> ni0(np), ni1(np), nj0(np), nj1(np);
+        for (size_t k = 0; k < np; ++k) {
+            const int i = pi[k], j = pj[k];
+            ni0[k] = bi[0][i] * dw0[k] + bi[1][i] * dw1[k];
+            ni1[k] = bi[2][i] * dw0[k] + bi[3][i] * dw1[k];
+            nj0[k] = bi[0][j] * dw0[k] + bi[1][j] * dw1[k];
+            nj1[k] = bi[2][j] * dw0[k] + bi[3][j] * dw1[k];
+        }
+        // SPS strain and stress (Solver_..._SPS.f90:144-182, 256-296)
+        std::vector<T> S[3], tau[3];
+        for (int q = 0; q < 3; ++q) { S[q].assign(n, T(0.0)); tau[q].assign(n, T(0.0)); }
+        for (size_t k = 0; k < np; ++k) {
+            const int i = pi[k], j = pj[k];
+            const T vd0 = -(P.u[i] - P.u[j]), vd1 = -(P.v[i] - P.v[j]);
+            S[0][i] += vd0 * ni0[k] * vol[j];
+            S[1][i] += (vd0 * ni1[k] + vd1 * ni0[k]) * vol[j];
+            S[2][i] += vd1 * ni1[k] * vol[j];
+            S[0][j] += vd0 * nj0[k] * vol[i];
+            S[1][j] += (vd0 * nj1[k] + vd1 * nj0[k]) * vol[i];
+            S[2][j] += vd1 * nj1[k] * vol[i];
+        }
+        const double dl = K.dl * C.dx;
+        for (int i = 0; i < n; ++i) {
+            if (P.type[i] != SPH_TYPE_WATER) continue;
+            const T sxx = S[0][i], sxy = S[1][i], syy = S[2][i];
+            const T abs2 = 2.0 * (sxx * sxx + syy * syy) + sxy * sxy;
+            const double t = K.c012 * dl;
+            const T nut = (t * t) * sqrt(abs2);
+            const T kk = K.c23 * nut * (sxx + syy);
+            const T blin = K.cblin * (dl * dl) * abs2;
+            tau[0][i] = (2.0 * nut * sxx - kk - blin) * P.rho[i];
+            tau[1][i] = (nut * sxy) * P.rho[i];
+            tau[2][i] = (2.0 * nut * syy - kk - blin) * P.rho[i];
+        }
+        // main pair loop (Solver_..._SPS.f90:300-502)
+        std::vector<T> cont(n, T(0.0)), a0(n, T(0.0)), a1(n, T(0.0));
+        for (size_t k = 0; k < np; ++k) {
+            const int i = pi[k], j = pj[k];
+            const T Vi = vol[i], Vj = vol[j], ri = P.rho[i], rj = P.rho[j];
+            const T cbar = (c[i] + c[j]) / 2.0, rbar = (ri + rj) / 2.0;
+            const T Pbar = (p[i] + p[j]) / 2.0;
+            const T vbar0 = (P.u[i] + P.u[j]) / 2.0, vbar1 = (P.v[i] + P.v[j]) / 2.0;
+            const T r2 = dx0[k] * dx0[k] + dx1[k] * dx1[k];
+            const T d = sqrt(r2);
+            const T e0 = -dx0[k] / d, e1 = -dx1[k] / d;
+            const T UL = P.u[i] * e0 + P.v[i] * e1, UR = P.u[j] * e0 + P.v[j] * e1;
+            const T Ubar = (UL + UR) / 2.0;
+            const T Us = Ubar + 0.5 * (p[i] - p[j]) / (rbar * K.sqrt_c0);
+            const T vs0 = (Us - Ubar) * e0 + vbar0, vs1 = (Us - Ubar) * e1 + vbar1;
+            const T dU = UL - UR;
+            const T m3 = val(dU) > 0.0 ? 3.0 * dU : T(0.0);
+            const T bR = val(m3) < val(cbar) ? m3 : cbar;
+            const T Ps = Pbar + 0.5 * bR * rbar * dU;
+            const T tmi = (P.u[i] - vs0) * ni0[k] + (P.v[i] - vs1) * ni1[k];
+            const T tmj = -((P.u[j] - vs0) * nj0[k] + (P.v[j] - vs1) * nj1[k]);
+            cont[i] += 2.0 * ri * Vj * tmi;
+            cont[j] += 2.0 * rj * Vi * tmj;
+            const T rij = 1.0 / (ri * rj);
+            a0[i] += P.mass[j] * (-2.0 * Ps * ni0[k] * rij);
+            a1[i] += P.mass[j] * (-2.0 * Ps * ni1[k] * rij);
+            a0[j] -= P.mass[i] * (-2.0 * Ps * nj0[k] * rij);
+            a1[j] -= P.mass[i] * (-2.0 * Ps * nj1[k] * rij);
+            const T vij0 = P.u[i] - P.u[j], vij1 = P.v[i] - P.v[j];
+            const T vx = vij0 * dx0[k] + vij1 * dx1[k];
+            if (val(vx) < 0.0) {       // artificial viscosity (:392-417)
+                const double fh = C.fai * hb;
+                const T phi = hb * vx / (r2 + fh * fh);
+                const T Pi = (-C.alpha * cbar * phi + C.beta * (phi * phi)) / rbar;
+                a0[i] += P.mass[j] * (-Pi * ni0[k]); a1[i] += P.mass[j] * (-Pi * ni1[k]);
+                a0[j] -= P.mass[i] * (-Pi * nj0[k]); a1[j] -= P.mass[i] * (-Pi * nj1[k]);
+            }
+            // Morris laplacian (:432-436)
+            const T rdi = dx0[k] * ni0[k] + dx1[k] * ni1[k], rdj = dx0[k] * nj0[k] + dx1[k] * nj1[k];
+            a0[i] += Vj * 2.0 * nu * rdi / r2 * vij0; a1[i] += Vj * 2.0 * nu * rdi / r2 * vij1;
+            a0[j] -= Vi * 2.0 * nu * rdj / r2 * vij0; a1[j] -= Vi * 2.0 * nu * rdj / r2 * vij1;
+            // delta-alpha artificial internal acceleration (:442-446)
+            const T tt = C.delta_alpha * hb * cbar * vx / r2;
+            a0[i] += tt * ni0[k] * C.rho0 / ri * Vj; a1[i] += tt * ni1[k] * C.rho0 / ri * Vj;
+            a0[j] -= tt * nj0[k] * C.rho0 / rj * Vi; a1[j] -= tt * nj1[k] * C.rho0 / rj * Vi;
+            // SPS force with the unnormalised gradient (:450-492), temp_p carried with the literals
+            T tp = ((tau[0][i] + tau[0][j]) * dw0[k] + (tau[1][i] + tau[1][j]) * dw1[k]) * rij;
+            a0[i] += P.smass[j] * tp; a0[j] -= P.smass[i] * tp;
+            if (!C.reference_literals) tp = T(0.0);
+            tp = (tp + (tau[2][i] + tau[2][j]) * dw1[k] + (tau[1][i] + tau[1][j]) * dw0[k]) * rij;
+            a1[i] += P.smass[j] * tp; a1[j] -= P.smass[i] * tp;
+        }
+        // grad rho (:508-526) and delta-SPH (:552-583)
+        std::vector<T> g0(n, T(0.0)), g1(n, T(0.0)), corr(n, T(0.0));
+        for (size_t k = 0; k < np; ++k) {
+            const int i = pi[k], j = pj[k];
+            const T dr = -(P.rho[i] - P.rho[j]);
+            g0[i] += dr * vol[j] * ni0[k]; g1[i] += dr * vol[j] * ni1[k];
+            g0[j] += dr * vol[i] * nj0[k]; g1[j] += dr * vol[i] * nj1[k];
+        }
+        for (size_t k = 0; k < np; ++k) {
+            const int i = pi[k], j = pj[k];
+            const T pd0 = -dx0[k], pd1 = -dx1[k];
+            const T r2 = pd0 * pd0 + pd1 * pd1;
+            const T dr = -(P.rho[i] - P.rho[j]);
+            const T psi = dr - 0.5 * ((g0[i] + g0[j]) * pd0 + (g1[i] + g1[j]) * pd1);
+            const T tmi = (pd0 * ni0[k] + pd1 * ni1[k]) / r2, tmj = (pd0 * nj0[k] + pd1 * nj1[k]) / r2;
+            const T cbar = (c[i] + c[j]) / 2.0;
+            corr[i] += 2.0 * C.delta * hb * cbar * psi * tmi * vol[j];
+            corr[j] -= 2.0 * C.delta * hb * cbar * psi * tmj * vol[i];
+        }
+        drho.assign(n, T(0.0)); acc0.assign(n, T(0.0)); acc1.assign(n, T(0.0));
+        for (int i = 0; i < n; ++i) {
+            drho[i] = cont[i];
+            if (P.type[i] != SPH_TYPE_WATER) continue;
+            drho[i] = drho[i] + corr[i];
+            acc0[i] = a0[i]; acc1[i] = a1[i];
+        }
+        return SPH_OK;
+    }
+
+    // Distribute_Period_Boundary_Particle (:56-206): wrap, then left/right images
+    // of the hosts and bottom/top images of hosts and left/right images.
+    void images(std::vector<T>& hx, std::vector<T>& hy, const std::vector<T>& hu, const std::vector<T>& hv,
+                const std::vector<T>& hr, const std::vector<double>& mass, const std::vector<double>& smass,
+                const std::vector<int>& type, Parts<T>& P) const {
+        const int n = (int)hx.size();
+        const double Lx = C.box_hi[0] - C.box_lo[0], Ly = C.box_hi[1] - C.box_lo[1];
+        for (int i = 0; i < n && C.periodic; ++i) {
+            if (val(hx[i]) > C.box_hi[0]) hx[i] = hx[i] - Lx;
+            else if (val(hx[i]) < C.box_lo[0]) hx[i] = hx[i] + Lx;
+            if (val(hy[i]) > C.box_hi[1]) hy[i] = hy[i] - Ly;
+            else if (val(hy[i]) < C.box_lo[1]) hy[i] = hy[i] + Ly;
+        }
+        P = Parts<T>();
+        for (int i = 0; i < n; ++i) P.push(hx[i], hy[i], hu[i], hv[i], hr[i], mass[i], smass[i], type[i]);
+        if (!C.periodic) return;
+        const double band = C.kernel_scale * C.h;
+        for (int i = 0; i < n; ++i) {
+            const double x = val(P.x[i]);
+            if (x <= C.box_lo[0] + band && x >= C.box_lo[0])
+                P.push(P.x[i] + Lx, P.y[i], P.u[i], P.v[i], P.rho[i], P.mass[i], P.smass[i], SPH_TYPE_PERIODIC);
+            if (x >= C.box_hi[0] - band && x <= C.box_hi[0])
+                P.push(P.x[i] - Lx, P.y[i], P.u[i], P.v[i], P.rho[i], P.mass[i], P.smass[i], SPH_TYPE_PERIODIC);
+        }
+        const int nlr = P.n;
+        for (int i = 0; i < nlr; ++i) {
+            const double y = val(P.y[i]);
+            if (y <= C.box_lo[1] + band && y >= C.box_lo[1])
+                P.push(P.x[i], P.y[i] + Ly, P.u[i], P.v[i], P.rho[i], P.mass[i], P.smass[i], SPH_TYPE_PERIODIC);
+            if (y >= C.box_hi[1] - band && y <= C.box_hi[1])
+                P.push(P.x[i], P.y[i] - Ly, P.u[i], P.v[i], P.rho[i], P.mass[i], P.smass[i], SPH_TYPE_PERIODIC);
+        }
+    }
+};
+
+template <class T>
+int run(const sph_config& cfg, int n, const T* x0, const T* y0, const T* u0, const T* v0, const T* r0,
+        const double* mass, const int* type, const T& nu, int nsteps, double dt, std::vector<T>* out) {
+    Model<T> M;
+    M.C = cfg;
+    M.K = derive(cfg);
+    M.nu = nu;
+    std::vector<T> hx(x0, x0 + n), hy(y0, y0 + n), hu(u0, u0 + n), hv(v0, v0 + n), hr(r0, r0 + n);
+    std::vector<double> ms(mass, mass + n);
+    std::vector<int> ty(type, type + n);
+    std::vector<T> cr(n), ca0(n), ca1(n);
+    for (int s = 0; s < nsteps; ++s) {
+        Parts<T> P, B0;
+        M.images(hx, hy, hu, hv, hr, ms, ms, ty, P);
+        B0 = P;
+        std::vector<T> dr, a0, a1;
+        int rc;
+        if (s == 0) {
+            if ((rc = M.rhs(P, dr, a0, a1))) return rc;
+        } else {
+            dr.assign(P.n, T(0.0)); a0.assign(P.n, T(0.0)); a1.assign(P.n, T(0.0));
+            for (int i = 0; i < n; ++i) { dr[i] = cr[i]; a0[i] = ca0[i]; a1[i] = ca1[i]; }
+        }
+        std::vector<T> Kr(n), Ka0(n), Ka1(n), Kv0(n), Kv1(n);
+        // stages (time_iteration.f90:942-1047): water particles only
+        for (int st = 0; st < 3; ++st) {
+            const double f = st < 2 ? 0.5 * dt : dt;
+            const double wgt = st == 0 ? 1.0 : 2.0;
+            for (int i = 0; i < n; ++i) {
+                if (P.type[i] != SPH_TYPE_WATER) continue;
+                P.rho[i] = st < 2 ? B0.rho[i] + dr[i] * dt / 2 : B0.rho[i] + dr[i] * dt;
+                P.u[i] = B0.u[i] + f * a0[i];
+                P.x[i] = B0.x[i] + f * P.u[i];
+                P.v[i] = B0.v[i] + f * a1[i];
+                P.y[i] = B0.y[i] + f * P.v[i];
+                Kr[i] += wgt * dr[i]; Ka0[i] += wgt * a0[i]; Ka1[i] += wgt * a1[i];
+                Kv0[i] += wgt * P.u[i]; Kv1[i] += wgt * P.v[i];
+            }
+            if ((rc = M.rhs(P, dr, a0, a1))) return rc;
+        }
+        for (int i = 0; i < n; ++i) {
+            if (P.type[i] != SPH_TYPE_WATER) continue;
+            P.rho[i] = B0.rho[i] + (Kr[i] + dr[i]) * dt / 6.0;
+            P.u[i] = B0.u[i] + (Ka0[i] + a0[i]) * dt / 6.0;
+            P.x[i] = B0.x[i] + (Kv0[i] + P.u[i]) * dt / 6.0 + 0.5 * dt * dt * a0[i];
+            P.v[i] = B0.v[i] + (Ka1[i] + a1[i]) * dt / 6.0;
+            P.y[i] = B0.y[i] + (Kv1[i] + P.v[i]) * dt / 6.0 + 0.5 * dt * dt * a1[i];
+        }
+        for (int i = 0; i < n; ++i) {
+            cr[i] = dr[i]; ca0[i] = a0[i]; ca1[i] = a1[i];
+            hx[i] = P.x[i]; hy[i] = P.y[i]; hu[i] = P.u[i]; hv[i] = P.v[i]; hr[i] = P.rho[i];
+        }
+    }
+    out[0] = hx; out[1] = hy; out[2] = hu; out[3] = hv; out[4] = hr;
+    return SPH_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+// nsteps time steps from (pos, vel, rho) along the tangent direction
+// (dpos, dvel, drho, dnu) (any of the arrays may be NULL = zero).  out[0] = loss
+// of the final state (SPH_LOSS_*; target_vel for the misfit), out[1] = its
+// directional derivative.  The final state (values) goes to pos_out, vel_out,
+// rho_out when they are given.  Arrays are column-major (n,2) like the ABI's.
+int oracle_tangent(const sph_config* cfg, int n, const double* pos, const double* vel, const double* rho,
+                   const double* mass, const int* type, const double* dpos, const double* dvel, const double* drho,
+                   double dnu, int nsteps, double dt, int loss, const double* target_vel, double* out,
+                   double* pos_out, double* vel_out, double* rho_out) {
+    if (!cfg || !pos || !vel || !rho || !mass || !type || !out || n <= 0 || nsteps <= 0) return SPH_E_ARG;
+    if (cfg->solver != SPH_SOLVER_MODLR_DELTA_SPS || cfg->integrator != SPH_INTEGRATOR_RK4_REUSE ||
+        cfg->shifting || cfg->xsph_eps != 0.0 || cfg->pair_rule != SPH_PAIRS_ONE_FLUID)
+        return SPH_E_CONFIG;
+    if (loss == SPH_LOSS_VELOCITY_MISFIT && !target_vel) return SPH_E_ARG;
+    std::vector<Dual> x(n), y(n), u(n), v(n), r(n);
+    for (int i = 0; i < n; ++i) {
+        x[i] = Dual(pos[i], dpos ? dpos[i] : 0.0);
+        y[i] = Dual(pos[n + i], dpos ? dpos[n + i] : 0.0);
+        u[i] = Dual(vel[i], dvel ? dvel[i] : 0.0);
+        v[i] = Dual(vel[n + i], dvel ? dvel[n + i] : 0.0);
+        r[i] = Dual(rho[i], drho ? drho[i] : 0.0);
+    }
+    std::vector<Dual> st[5];
+    int rc = run<Dual>(*cfg, n, x.data(), y.data(), u.data(), v.data(), r.data(), mass, type, Dual(cfg->nu, dnu),
+                       nsteps, dt, st);
+    if (rc) return rc;
+    Dual L(0.0, 0.0);
+    for (int i = 0; i < n; ++i) {
+        if (type[i] != SPH_TYPE_WATER) continue;
+        if (loss == SPH_LOSS_VELOCITY_MISFIT) {
+            const Dual a = st[2][i] - target_vel[i], b = st[3][i] - target_vel[n + i];
+            L += a * a + b * b;
+        } else {
+            L += 0.5 * mass[i] * (st[2][i] * st[2][i] + st[3][i] * st[3][i]);
+        }
+    }
+    out[0] = L.v;
+    out[1] = L.d;
+    for (int i = 0; i < n; ++i) {
+        if (pos_out) { pos_out[i] = st[0][i].v; pos_out[n + i] = st[1][i].v; }
+        if (vel_out) { vel_out[i] = st[2][i].v; vel_out[n + i] = st[3][i].v; }
+        if (rho_out) rho_out[i] = st[4][i].v;
+    }
+    return SPH_OK;
+}
+
+}  // extern "C"

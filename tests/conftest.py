@@ -36,5 +36,6 @@ def lib():
 @pytest.fixture(scope="session")
 def oracle():
     import oracle_api
+    oracle_api.build()          # incremental: rebuilds only when a source changed
     oracle_api.load()
     return oracle_api

@@ -171,3 +171,26 @@ def test_adjoint_of_the_mixed_precision_step(lib):
         err = np.linalg.norm(gm[key] - g64[key]) / np.linalg.norm(g64[key])
         assert err < 1e-4, (key, err)
     assert abs(gm["nu"] - g64["nu"]) <= 1e-4 * abs(g64["nu"])
+
+
+@pytest.mark.parametrize("kind", ["wendland-renorm", "reference-gaussian"])
+def test_adjoint_matches_cpu_tangent_linear_reference(lib, oracle, kind):
+    """g.delta from the GPU adjoint against the FP64 CPU tangent-linear model of
+    the same steps (oracle/sph_tangent.cpp, forward-mode derivative with the
+    pair set fixed by the values): both are exact derivatives of the same
+    discrete map, so they agree to rounding (1e-8 relative)."""
+    case = _case(kind)
+    dt = S.baseline_dt(case.cfg)
+    target = _target(case, dt)
+    L, g, _, _ = _grad(case, dt, target)
+    n = case.n
+    rng = np.random.default_rng(400)
+    dirs = [dict(dvel=rng.standard_normal(2 * n)), dict(drho=rng.standard_normal(n) * case.cfg.rho0),
+            dict(dpos=rng.standard_normal(2 * n) * case.cfg.dx), dict(dnu=1.0)]
+    for d in dirs:
+        Lt, dLt, _ = oracle.tangent(case.cfg, case.pos, case.vel, case.rho, case.mass, case.type, NSTEPS, dt,
+                                    loss=S.LOSS_VELOCITY_MISFIT, target_vel=target, **d)
+        assert Lt == pytest.approx(L, rel=1e-10)
+        ad = (float(g["vel0"] @ d["dvel"]) if "dvel" in d else float(g["rho0"] @ d["drho"]) if "drho" in d
+              else float(g["pos0"] @ d["dpos"]) if "dpos" in d else g["nu"] * d["dnu"])
+        assert abs(ad - dLt) <= 1e-8 * abs(dLt), (list(d)[0], ad, dLt)

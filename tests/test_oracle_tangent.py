@@ -1,0 +1,56 @@
+"""The FP64 tangent-linear model (oracle/sph_tangent.cpp), the CPU reference of
+the adjoint: its value path must reproduce the oracle's time steps, and its
+directional derivative must match central differences of its own value path."""
+import numpy as np
+import pytest
+
+import sph_b200 as S
+
+
+def _case(kind):
+    if kind == "wendland-renorm":
+        case = S.make_tgv(24, solver=S.SOLVER_MODLR_DELTA_SPS, jitter=0.05, seed=3)
+    else:
+        case = S.make_tgv(24, reference=True, jitter=0.05, seed=4)
+    case.cfg.shifting = 0
+    return case
+
+
+@pytest.mark.parametrize("kind", ["wendland-renorm", "reference-gaussian"])
+def test_tangent_value_path_reproduces_the_oracle(oracle, kind):
+    case = _case(kind)
+    dt = S.baseline_dt(case.cfg)
+    _, _, (pos, vel, rho) = oracle.tangent(case.cfg, case.pos, case.vel, case.rho, case.mass, case.type, 5, dt, loss=1)
+    sim = oracle.OracleSim(case.cfg, case.pos, case.vel, case.rho, case.mass, case.type)
+    sim.run(5, dt)
+    rpos, rvel, rrho, _ = sim.state()
+    assert np.abs(pos - rpos).max() < 1e-14
+    assert np.abs(vel - rvel).max() <= 1e-12 * np.abs(rvel).max()
+    assert np.abs(rho - rrho).max() <= 1e-10 * np.abs(rrho - case.cfg.rho0).max()
+
+
+@pytest.mark.parametrize("kind", ["wendland-renorm", "reference-gaussian"])
+def test_tangent_matches_its_central_differences(oracle, kind):
+    case = _case(kind)
+    dt = S.baseline_dt(case.cfg)
+    d = np.random.default_rng(1).standard_normal(2 * case.n)
+    args = (case.pos, case.vel, case.rho, case.mass, case.type, 5, dt)
+    _, dL, _ = oracle.tangent(case.cfg, *args, dvel=d, loss=1)
+    eps = 1e-6 if kind == "wendland-renorm" else 1e-7
+    Lp = oracle.tangent(case.cfg, case.pos, case.vel + eps * d, *args[2:], loss=1)[0]
+    Lm = oracle.tangent(case.cfg, case.pos, case.vel - eps * d, *args[2:], loss=1)[0]
+    assert abs(dL - (Lp - Lm) / (2 * eps)) <= 1e-6 * abs(dL)
+    _, dLn, _ = oracle.tangent(case.cfg, *args, dnu=1.0, loss=1)
+    c2 = case.cfg.copy()
+    e = 1e-5 * c2.nu
+    c2.nu = case.cfg.nu + e
+    Lp = oracle.tangent(c2, *args, loss=1)[0]
+    c2.nu = case.cfg.nu - e
+    Lm = oracle.tangent(c2, *args, loss=1)[0]
+    assert abs(dLn - (Lp - Lm) / (2 * e)) <= 1e-6 * abs(dLn)
+
+
+def test_tangent_rejects_configurations_outside_its_scope(oracle):
+    case = S.make_tgv(8, solver=S.SOLVER_MUSCL_DELTA_SPS)
+    with pytest.raises(RuntimeError):
+        oracle.tangent(case.cfg, case.pos, case.vel, case.rho, case.mass, case.type, 1, 1e-4, loss=1)
