@@ -66,8 +66,12 @@ struct Side {
 // dv = v_i - v_j, dp = p_i - p_j, drho = rho_j - rho_i formed in FP64 from the
 // kinematic records; in real arithmetic this is the reference's expression,
 // e.g. v_i - v* = (v_i - v_j)/2 - (U* - Ubar) e for the modified solver.
-template <typename R, bool MUSCL>
-__global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_pass_c(Params P, Sorted<R> D, int last_rhs) {
+// MS: the moving-square solvers (HLLC or modified linear with XSPH in the
+// continuity flux, laplacian switch, no SPS); SHIFT: the last RHS of a step with
+// shifting on, which also forms the shifting sum.  Both are compile-time so that
+// each launch carries only the registers of the terms it evaluates.
+template <typename R, bool MUSCL, bool MS, bool SHIFT>
+__global__ void __launch_bounds__(128, sizeof(R) == 4 ? (MS ? 4 : 5) : 3) k_pass_c(Params P, Sorted<R> D) {
     using V4 = typename VT<R>::V4;
     using A = typename Acc<R>::T;
     constexpr bool F32 = sizeof(R) == 4;
@@ -86,7 +90,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_pass_c(Params P
     // Moving_Square.../Single_step_compute.f90:273-281)
     const bool water = integrated(P, ta);
     typename VT<R>::V2 avg_a = mk2<R>(R(0), R(0));
-    if (P.ms) avg_a = D.avg[a];
+    if (MS) avg_a = D.avg[a];
 
     const R hbar = (R)P.h;
     const R inv_h = (R)(1.0 / P.h);
@@ -183,7 +187,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_pass_c(Params P
         R PA, wa0, wa1;          // this side's star pressure and velocity minus star velocity
         if (a_is_i) { wa0 = R(0.5) * du + lui; wa1 = R(0.5) * dv + lvi; }
         else { wa0 = R(-0.5) * du - luj; wa1 = R(-0.5) * dv - lvj; }
-        if (!P.hllc) {
+        if (!MS || !P.hllc) {
             const R dP = dp + lpi + lpj;
             const R sU = R(0.5) * dP * (inv_rbar * inv_sqc0);               // U* - Ubar
             const R bR = min(R(3) * (max(dU, R(0))), cbar);
@@ -227,7 +231,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_pass_c(Params P
             wa0 = (R)(K.x - vs0);
             wa1 = (R)(K.y - vs1);
         }
-        if (P.ms) {      // XSPH velocities inside the continuity flux (MS solvers :199-202)
+        if (MS) {        // XSPH velocities inside the continuity flux (MS solvers :199-202)
             const typename VT<R>::V2 avg_b = D.avg[b];
             wa0 += avg_a.x - avg_b.x;
             wa1 += avg_a.y - avg_b.y;
@@ -248,7 +252,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_pass_c(Params P
             tx += mb * (-Pi * nd0);
             ty += mb * (-Pi * nd1);
         }
-        if (!P.ms || P.laplacian == 1) {
+        if (!MS || P.laplacian == 1) {
             // Morris laplacian (:432-436)
             const R lf = Vb * nu2 * (xij0 * nd0 + xij1 * nd1) * inv_r2;
             tx += lf * du;
@@ -265,7 +269,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_pass_c(Params P
         ty += tt * nd1;
         // SPS force, unnormalised dwdx and the neighbour's SPS mass (:450-492);
         // the reference does not reset temp_p between x and y (kept with quirks)
-        if (!P.ms) {
+        if (!MS) {
             const R sxx = I.nb1.x + J.nb1.x, sxy = I.nb1.y + J.nb1.y, syy = I.nb1.z + J.nb1.z;
             R tp = (sxx * dw0 + sxy * dw1) * rho_ij;
             const R smb = T.aux.w;
@@ -277,7 +281,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_pass_c(Params P
         accx.add(sgn * tx);
         accy.add(sgn * ty);
         // XSPH average velocity (:495-500; modified solver only)
-        if (!MUSCL && P.xsph && !P.ms) {
+        if (!MUSCL && !MS && P.xsph) {
             const R f = eps2 * mb * rcp(rho_i + rho_j) * w;
             xsx -= sgn * (f * du);
             xsy -= sgn * (f * dv);
@@ -292,7 +296,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_pass_c(Params P
         cont.add(dr);
         // particle shifting sum (Shift_particle_position.f90:97-100), FP64:
         // shift_a = -beta h^2 B_a^-1 sum_b (1 + R (W/W(dx))^n) grad_a W_ab V_b
-        if (last_rhs) {
+        if (SHIFT) {
             double gd, wd, Vd;
             if (F32) {
                 const double dd2 = sqrt(dxd * dxd + dyd * dyd);
@@ -321,8 +325,8 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_pass_c(Params P
     // assembly (single_step_compute.f90:152-171, Solver :627-635)
     D.drho[a] = cont.val();
     D.acc[a] = water ? mk2<R>(accx.val(), accy.val()) : mk2<R>(R(0), R(0));
-    if (!P.ms) D.avg[a] = mk2<R>(xsx, xsy);
-    if (last_rhs) {
+    if (!MS) D.avg[a] = mk2<R>(xsx, xsy);
+    if (SHIFT) {
         const double4 b64 = D.binv64[a];
         const double c = -P.shift_beta * (P.h * P.h);
         D.shift[a] = make_double2(c * (b64.x * shx + b64.y * shy), c * (b64.z * shx + b64.w * shy));

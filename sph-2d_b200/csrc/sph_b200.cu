@@ -364,8 +364,17 @@ int rhs(sph_handle* h, int last) {
     k_surface<R><<<nb, 128, 0, h->stream>>>(P, D);
     k_near<R><<<nb, 128, 0, h->stream>>>(P, D);
     tic(h, PH_C);
-    if (P.muscl) k_pass_c<R, true><<<nb, 128, 0, h->stream>>>(P, D, last);
-    else k_pass_c<R, false><<<nb, 128, 0, h->stream>>>(P, D, last);
+    const bool sh = last && h->cfg.shifting;
+    if (P.ms) {
+        if (sh) k_pass_c<R, false, true, true><<<nb, 128, 0, h->stream>>>(P, D);
+        else k_pass_c<R, false, true, false><<<nb, 128, 0, h->stream>>>(P, D);
+    } else if (P.muscl) {
+        if (sh) k_pass_c<R, true, false, true><<<nb, 128, 0, h->stream>>>(P, D);
+        else k_pass_c<R, true, false, false><<<nb, 128, 0, h->stream>>>(P, D);
+    } else {
+        if (sh) k_pass_c<R, false, false, true><<<nb, 128, 0, h->stream>>>(P, D);
+        else k_pass_c<R, false, false, false><<<nb, 128, 0, h->stream>>>(P, D);
+    }
     CK(cudaGetLastError());
     h->launches += 4;
     if (P.has_body && (last || h->bf_every_rhs)) {
