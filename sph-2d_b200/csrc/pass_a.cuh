@@ -19,7 +19,7 @@
 namespace sph {
 
 template <typename R>
-__global__ void __launch_bounds__(128) k_pass_a(Params P, Sorted<R> D) {
+__global__ void __launch_bounds__(128, sizeof(R) == 4 ? 8 : 6) k_pass_a(Params P, Sorted<R> D) {
     using V4 = typename VT<R>::V4;
     constexpr bool F32 = sizeof(R) == 4;
     const int a = blockIdx.x * blockDim.x + threadIdx.x;

@@ -58,6 +58,7 @@ template <typename R>
 struct Side {
     using V4 = typename VT<R>::V4;
     double4 kin;   // u, v, rho, p (FP64)
+    float4 kh, kl; // the same, hi + lo (mixed Taylor-Green variants)
     V4 aux;        // m, V, c, smass
     V4 nb1, nb2, nb3;
 };
@@ -75,15 +76,21 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (MS ? 4 : 5) : 3) k_pass
     using V4 = typename VT<R>::V4;
     using A = typename Acc<R>::T;
     constexpr bool F32 = sizeof(R) == 4;
+    // hi/lo records: the mixed Taylor-Green variants (the moving-square ones keep
+    // the FP64 records, which their FP64 HLLC state needs)
+    constexpr bool HL = F32 && !MS;
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= P.n_tot) return;
     const int ta = D.type[a];
     const int nn = D.npairs[a];
-    const double2 xa = D.pos[a];
+    const double2 xa = (!HL || SHIFT) ? D.pos[a] : make_double2(0.0, 0.0);
+    float4 xa_hl = make_float4(0.f, 0.f, 0.f, 0.f);
     Side<R> S;
-    S.kin = D.kin[a]; S.aux = D.aux[a]; S.nb1 = D.nb1[a]; S.nb2 = D.nb2[a];
+    if (HL) { S.kh = D.kh[a]; S.kl = D.kl[a]; xa_hl = D.xhl[a]; }
+    else S.kin = D.kin[a];
+    S.aux = D.aux[a]; S.nb1 = D.nb1[a]; S.nb2 = D.nb2[a];
     if (MUSCL) S.nb3 = D.nb3[a];
-    const R rho_a = (R)S.kin.z;
+    const R rho_a = HL ? (R)S.kh.z : (R)S.kin.z;
     const V4 bi = D.binv[a];
     const bool near_a = (D.flags[a] & 2) != 0;
     // delta-SPH and the assembly only apply to integrated particles (Solver :627-635,
@@ -110,20 +117,35 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (MS ? 4 : 5) : 3) k_pass
 
     // the pairs pass A found inside the support at this RHS
     unsigned ent_n = nn > 0 ? __ldg(&D.pairs[a]) : 0u;
-    double2 xb_n = nn > 0 ? __ldg(&D.pos[ent_n & 0x7fffffffu]) : make_double2(0.0, 0.0);
+    double2 xb_n = make_double2(0.0, 0.0);
+    float4 xbhl_n = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (nn > 0) {
+        if (HL) xbhl_n = __ldg(&D.xhl[ent_n & 0x7fffffffu]);
+        else xb_n = __ldg(&D.pos[ent_n & 0x7fffffffu]);
+    }
     for (int e = 0; e < nn; ++e) {
         const unsigned ent = ent_n;
         const int b = (int)(ent & 0x7fffffffu);
         const bool a_is_i = (ent >> 31) != 0;
         const double2 xb = xb_n;
+        const float4 xbhl = xbhl_n;
         if (e + 1 < nn) {
             ent_n = __ldg(&D.pairs[(size_t)(e + 1) * P.nbr_stride + a]);
-            xb_n = __ldg(&D.pos[ent_n & 0x7fffffffu]);
+            if (HL) xbhl_n = __ldg(&D.xhl[ent_n & 0x7fffffffu]);
+            else xb_n = __ldg(&D.pos[ent_n & 0x7fffffffu]);
         }
-        const double dxd = xa.x - xb.x, dyd = xa.y - xb.y;
+        // x_a - x_b: FP64, or hi/lo in FP32 (the shifting sum still reads the FP64 positions)
+        double dxd = 0.0, dyd = 0.0;
+        if (!HL) { dxd = xa.x - xb.x; dyd = xa.y - xb.y; }
+        else if (SHIFT) {
+            const double2 xb64 = __ldg(&D.pos[b]);
+            dxd = xa.x - xb64.x; dyd = xa.y - xb64.y;
+        }
+        const float dxf = HL ? (xa_hl.x - xbhl.x) + (xa_hl.z - xbhl.z) : 0.f;
+        const float dyf = HL ? (xa_hl.y - xbhl.y) + (xa_hl.w - xbhl.w) : 0.f;
         R d, inv_d;
         if (F32) {
-            const R s = (R)(dxd * dxd + dyd * dyd);
+            const R s = HL ? (R)(dxf * dxf + dyf * dyf) : (R)(dxd * dxd + dyd * dyd);
             inv_d = rsqrtf(s);
             d = s * inv_d;
         } else {
@@ -131,19 +153,32 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (MS ? 4 : 5) : 3) k_pass
             inv_d = R(1) / d;
         }
         Side<R> T;
-        T.kin = D.kin[b]; T.aux = D.aux[b]; T.nb1 = D.nb1[b]; T.nb2 = D.nb2[b];
+        if (HL) { T.kh = D.kh[b]; T.kl = D.kl[b]; }
+        else T.kin = D.kin[b];
+        T.aux = D.aux[b]; T.nb1 = D.nb1[b]; T.nb2 = D.nb2[b];
         if (MUSCL) T.nb3 = D.nb3[b];
         const Side<R>& I = a_is_i ? S : T;
         const Side<R>& J = a_is_i ? T : S;
         const R sgn = a_is_i ? R(1) : R(-1);
         // position_difference_ij = x_i - x_j (find_particle_pair.f90:79-107)
-        const R xij0 = (R)(a_is_i ? dxd : -dxd), xij1 = (R)(a_is_i ? dyd : -dyd);
-        // FP64 pair differences
-        const R du = (R)(I.kin.x - J.kin.x), dv = (R)(I.kin.y - J.kin.y);
-        const R dp = (R)(I.kin.w - J.kin.w);
-        const R drho_ji = (R)(J.kin.z - I.kin.z);
-        const R rho_i = (R)I.kin.z, rho_j = (R)J.kin.z;
-        const R rho_b = (R)T.kin.z;
+        R xij0, xij1;
+        if (HL) { xij0 = (R)(a_is_i ? dxf : -dxf); xij1 = (R)(a_is_i ? dyf : -dyf); }
+        else { xij0 = (R)(a_is_i ? dxd : -dxd); xij1 = (R)(a_is_i ? dyd : -dyd); }
+        // pair differences: FP64, or hi/lo in FP32
+        R du, dv, dp, drho_ji, rho_i, rho_j, rho_b;
+        if (HL) {
+            du = (R)((I.kh.x - J.kh.x) + (I.kl.x - J.kl.x));
+            dv = (R)((I.kh.y - J.kh.y) + (I.kl.y - J.kl.y));
+            dp = (R)((I.kh.w - J.kh.w) + (I.kl.w - J.kl.w));
+            drho_ji = (R)((J.kh.z - I.kh.z) + (J.kl.z - I.kl.z));
+            rho_i = (R)I.kh.z; rho_j = (R)J.kh.z; rho_b = (R)T.kh.z;
+        } else {
+            du = (R)(I.kin.x - J.kin.x); dv = (R)(I.kin.y - J.kin.y);
+            dp = (R)(I.kin.w - J.kin.w);
+            drho_ji = (R)(J.kin.z - I.kin.z);
+            rho_i = (R)I.kin.z; rho_j = (R)J.kin.z;
+            rho_b = (R)T.kin.z;
+        }
         // compute_kernel: W and dwdx(k) = g (x_i - x_j)
         R w, g;
         {
@@ -183,7 +218,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (MS ? 4 : 5) : 3) k_pass
         }
         // U_L - U_R and P_L - P_R from the differences
         const R dU = (du + lui + luj) * e0 + (dv + lvi + lvj) * e1;
-        const R Pbar = R(0.5) * ((R)I.kin.w + (R)J.kin.w);
+        const R Pbar = HL ? R(0.5) * ((R)I.kh.w + (R)J.kh.w) : R(0.5) * ((R)I.kin.w + (R)J.kin.w);
         R PA, wa0, wa1;          // this side's star pressure and velocity minus star velocity
         if (a_is_i) { wa0 = R(0.5) * du + lui; wa1 = R(0.5) * dv + lvi; }
         else { wa0 = R(-0.5) * du - luj; wa1 = R(-0.5) * dv - lvj; }
@@ -311,7 +346,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (MS ? 4 : 5) : 3) k_pass
                     wd = P.kfactor * (1 + 2 * q) * (t3 * t);
                     gd = P.kfactor * (-5 * q * t3) / (dd2 * P.h);
                 }
-                Vd = D.mass[b] / T.kin.z;
+                Vd = D.mass[b] / (HL ? __ldg(&D.kin[b].z) : T.kin.z);
             } else {
                 wd = (double)w; gd = (double)g; Vd = (double)Vb;
             }

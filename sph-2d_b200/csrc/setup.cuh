@@ -155,7 +155,26 @@ struct Sorted {
     // cell ranges
     int* cell_start;
     int* cell_end;
+    // mixed path only: the kinematic record and the position split into float
+    // hi + lo parts (v = hi + lo, hi = (float)v), so pass C forms pair
+    // differences (hi_i - hi_j) + (lo_i - lo_j) in FP32 with the accuracy of the
+    // FP64 difference rounded to FP32, without FP64 arithmetic or conversions
+    float4* kh;       // u, v, rho, p  (hi)
+    float4* kl;       //               (lo)
+    float4* xhl;      // x hi, y hi, x lo, y lo
 };
+
+// Hi/lo split of the records a particle's pass-C neighbours read (mixed path).
+template <typename R>
+__device__ __forceinline__ void store_split(Sorted<R>& D, int s, double2 x, double4 k) {
+    if (sizeof(R) != 4) return;
+    const float uh = (float)k.x, vh = (float)k.y, rh = (float)k.z, ph = (float)k.w;
+    D.kh[s] = make_float4(uh, vh, rh, ph);
+    D.kl[s] = make_float4((float)(k.x - (double)uh), (float)(k.y - (double)vh), (float)(k.z - (double)rh),
+                          (float)(k.w - (double)ph));
+    const float xh = (float)x.x, yh = (float)x.y;
+    D.xhl[s] = make_float4(xh, yh, (float)(x.x - (double)xh), (float)(x.y - (double)yh));
+}
 
 // --- 4. gather the id-ordered arrays into cell order -----------------------
 template <typename R>
@@ -238,25 +257,30 @@ __global__ void k_build_lists(Params P, Sorted<R> D, unsigned* status) {
         int ida = D.id[a];
         int cx = (int)floor((xa.x - P.gx0) / P.cs), cy = (int)floor((xa.y - P.gy0) / P.cs);
         int x0 = max(cx - 1, 0), x1 = min(cx + 1, P.gnx - 1);
+        // with the one-fluid rule every pair of a water particle is allowed
+        const bool check_type = !(P.pair_rule == SPH_PAIRS_ONE_FLUID && ta == SPH_TYPE_WATER);
         for (int gy = max(cy - 1, 0); gy <= min(cy + 1, P.gny - 1); ++gy) {
-            int row = gy * P.gnx;
+            // the cells x0..x1 of a row are consecutive keys, so their particles
+            // form one contiguous range of the sorted order
+            const int row = gy * P.gnx;
+            int b0 = -1, b1 = -1;
             for (int gx = x0; gx <= x1; ++gx) {
-                int c = row + gx;
-                int b0 = D.cell_start[c];
-                if (b0 < 0) continue;
-                int b1 = D.cell_end[c];
-                for (int b = b0; b < b1; ++b) {
-                    if (b == a) continue;
-                    if (!pair_allowed(P.pair_rule, ta, D.type[b])) continue;
-                    double2 xb = D.pos[b];
-                    double dx = xa.x - xb.x, dy = xa.y - xb.y;
-                    if (dx * dx + dy * dy > P.r2_list) continue;
-                    if (cnt < P.max_nbr) {
-                        unsigned lower = ida < D.id[b] ? 0x80000000u : 0u;
-                        D.nbr[(size_t)cnt * P.nbr_stride + a] = (unsigned)b | lower;
-                    }
-                    ++cnt;
+                const int st = D.cell_start[row + gx];
+                if (st < 0) continue;
+                if (b0 < 0) b0 = st;
+                b1 = D.cell_end[row + gx];
+            }
+            for (int b = b0; b < b1; ++b) {
+                if (b == a) continue;
+                if (check_type && !pair_allowed(P.pair_rule, ta, D.type[b])) continue;
+                const double2 xb = D.pos[b];
+                const double dx = xa.x - xb.x, dy = xa.y - xb.y;
+                if (dx * dx + dy * dy > P.r2_list) continue;
+                if (cnt < P.max_nbr) {
+                    const unsigned lower = ida < D.id[b] ? 0x80000000u : 0u;
+                    D.nbr[(size_t)cnt * P.nbr_stride + a] = (unsigned)b | lower;
                 }
+                ++cnt;
             }
         }
         if (cnt > P.max_nbr) { atomicOr(status, ST_NBR_OVERFLOW); cnt = P.max_nbr; }
@@ -276,6 +300,7 @@ __global__ void k_records(Params P, Sorted<R> D) {
     double m = D.mass[s];
     D.kin[s] = make_double4(v.x, v.y, rho, p);
     D.aux[s] = mk4<R>((R)m, (R)(m / rho), (R)c, (R)D.smass[s]);
+    store_split(D, s, D.pos[s], make_double4(v.x, v.y, rho, p));
 }
 
 }  // namespace sph

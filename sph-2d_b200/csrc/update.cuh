@@ -121,6 +121,7 @@ __global__ void k_stage(Params P, Sorted<R> D, int stage, double dt, int use_car
     const double m = D.mass[s];
     D.kin[s] = make_double4(u, v, rho, p);
     D.aux[s] = mk4<R>((R)m, (R)(m / rho), (R)c, (R)D.smass[s]);
+    store_split(D, s, make_double2(x, y), make_double4(u, v, rho, p));
 }
 
 // Kinetic energy and max |v| of the water host particles
