@@ -32,22 +32,19 @@ namespace sph {
 
 template <typename R>
 __device__ __forceinline__ void muscl_limiter(R di, R dj, R dij, R& li, R& lj) {
-    const R beta_lim = R(1.3);
-    const R diff = R(0.5);
-    R fi, fj, lim;
-    if (dj > R(0)) {
-        lim = max(R(0), max(min(beta_lim * di, dj), min(di, beta_lim * dj)));
-        if (lim > R(0.5) * dij && fabs(lim) > R(0)) {
-            if (di > dj) { fi = diff; fj = R(0); } else { fi = R(0); fj = diff; }
-            li = dij * fi; lj = dij * fj;
-        } else { li = lim; lj = lim; }
-    } else {
-        lim = min(R(0), min(max(beta_lim * di, dj), max(di, beta_lim * dj)));
-        if (lim < R(0.5) * dij && fabs(lim) > R(0)) {
-            if (di < dj) { fi = diff; fj = R(0); } else { fi = R(0); fj = diff; }
-            li = dij * fi; lj = dij * fj;
-        } else { li = lim; lj = lim; }
-    }
+    // the two sign branches of the reference written with selects (the same
+    // values, bit for bit, including the sign of the zero increments), so the
+    // lanes of a warp do not diverge
+    const R b = R(1.3);
+    const R bdi = b * di, bdj = b * dj;
+    const bool pos = dj > R(0);
+    const R lim = pos ? max(R(0), max(min(bdi, dj), min(di, bdj))) : min(R(0), min(max(bdi, dj), max(di, bdj)));
+    const R half = R(0.5) * dij;
+    const bool big = (pos ? (lim > half) : (lim < half)) && fabs(lim) > R(0);
+    const bool first = pos ? (di > dj) : (di < dj);
+    const R on = dij * R(0.5), off = dij * R(0);
+    li = big ? (first ? on : off) : lim;
+    lj = big ? (first ? off : on) : lim;
 }
 
 __device__ __forceinline__ double rcp(double x) { return 1.0 / x; }
