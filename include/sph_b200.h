@@ -105,6 +105,15 @@ typedef struct sph_config {
     double cell_skin;         /* extra cell width as a fraction of the support (>= 0) */
     int    laplacian;         /* laplacianTerm: 1 Morris, 0 Monaghan (moving-square solvers) */
     int    free_surface;      /* Has_FreeSurface_Or_Not: 1 detect free-surface particles, 0 none */
+    /* MLS density re-initialisation (Reinitialize_particle_density), run after the
+     * integrator update and before shifting of every mls_every-th step:
+     * mls_order 0 off, 3 linear or 6 quadratic moving least squares
+     * (RefreshDensity_MLS_Order; order 1 is not built and returns SPH_E_CONFIG),
+     * mls_every = MLS_time_step / RefreshDensity_time_step,
+     * mls_alpha = slighted_modified_alpha (the moment matrix gets alpha^3 on its diagonal). */
+    int    mls_order;
+    int    mls_every;
+    double mls_alpha;
 } sph_config;
 
 /* diagnostics returned by sph_step (reductions in FP64) */

@@ -56,6 +56,7 @@ def load():
     lib.oracle_set_initial_type.argtypes = [ctypes.c_void_p, ctypes.c_int, ip]
     lib.oracle_body_force.argtypes = [ctypes.c_void_p, dp]
     lib.oracle_rhs_body_force.argtypes = [cp, ctypes.c_int, dp, dp, dp, dp, ip, ip, dp]
+    lib.oracle_mls_reinit.argtypes = [cp, ctypes.c_int, dp, dp, dp, ip, dp]
     lib.oracle_tangent.argtypes = [cp, ctypes.c_int, dp, dp, dp, dp, ip, dp, dp, dp, ctypes.c_double, ctypes.c_int,
                                    ctypes.c_double, ctypes.c_int, dp, dp, dp, dp, dp]
     _lib = lib
@@ -203,3 +204,15 @@ def tangent(cfg: SphConfig, pos, vel, rho, mass, type_, nsteps: int, dt: float, 
     if rc != 0:
         raise RuntimeError(f"oracle_tangent failed ({rc})")
     return out[0], out[1], (P, V, R)
+
+
+def mls_reinit(cfg: SphConfig, pos, rho, mass, type_):
+    """Reinitialize_particle_density applied once to the given particles."""
+    n = rho.shape[0]
+    out = np.zeros(n)
+    a = [np.ascontiguousarray(x, np.float64) for x in (pos, rho, mass)]
+    t = np.ascontiguousarray(type_, np.int32)
+    rc = load().oracle_mls_reinit(ctypes.byref(cfg), n, _p(a[0]), _p(a[1]), _p(a[2]), _p(t, ctypes.c_int), _p(out))
+    if rc != 0:
+        raise RuntimeError("oracle_mls_reinit failed")
+    return out

@@ -1014,6 +1014,140 @@ void wrap_periodic(Particles& H) {
     }
 }
 
+// Matrix inverse by Gauss-Jordan elimination with full pivoting, in place,
+// the method of BRINV (Taylor_Green_Vortex/function_module.f90:568-639).
+// Returns false when the largest remaining pivot is negligible (d + 1 == 1).
+bool gauss_jordan_inverse(std::vector<double>& A, int n) {
+    std::vector<int> rowp(n), colp(n);
+    auto at = [&](int i, int j) -> double& { return A[(size_t)i * n + j]; };
+    for (int k = 0; k < n; ++k) {
+        double d = 0.0;
+        for (int i = k; i < n; ++i)
+            for (int j = k; j < n; ++j)
+                if (std::fabs(at(i, j)) > d) { d = std::fabs(at(i, j)); rowp[k] = i; colp[k] = j; }
+        if (d + 1.0 == 1.0) return false;
+        for (int j = 0; j < n; ++j) std::swap(at(k, j), at(rowp[k], j));
+        for (int i = 0; i < n; ++i) std::swap(at(i, k), at(i, colp[k]));
+        at(k, k) = 1.0 / at(k, k);
+        for (int j = 0; j < n; ++j) if (j != k) at(k, j) = at(k, j) * at(k, k);
+        for (int i = 0; i < n; ++i)
+            if (i != k)
+                for (int j = 0; j < n; ++j)
+                    if (j != k) at(i, j) = at(i, j) - at(i, k) * at(k, j);
+        for (int i = 0; i < n; ++i) if (i != k) at(i, k) = -at(i, k) * at(k, k);
+    }
+    for (int k = n - 1; k >= 0; --k) {
+        for (int j = 0; j < n; ++j) std::swap(at(k, j), at(colp[k], j));
+        for (int i = 0; i < n; ++i) std::swap(at(i, k), at(i, rowp[k]));
+    }
+    return true;
+}
+
+// matrix_inversion_less_three, n = 3 (Taylor_Green_Vortex/function_module.f90:157-249):
+// the adjugate over the determinant; false when the determinant is zero.
+bool inverse3(std::vector<double>& A) {
+    auto a = [&](int i, int j) { return A[(size_t)i * 3 + j]; };
+    const double det = a(0, 0) * (a(1, 1) * a(2, 2) - a(1, 2) * a(2, 1)) - a(0, 1) * (a(1, 0) * a(2, 2) - a(1, 2) * a(2, 0)) +
+                       a(0, 2) * (a(1, 0) * a(2, 1) - a(1, 1) * a(2, 0));
+    if (det == 0.0) return false;
+    std::vector<double> R(9);
+    R[0] = (a(1, 1) * a(2, 2) - a(1, 2) * a(2, 1)) / det;
+    R[1] = -(a(0, 1) * a(2, 2) - a(0, 2) * a(2, 1)) / det;
+    R[2] = (a(0, 1) * a(1, 2) - a(0, 2) * a(1, 1)) / det;
+    R[3] = -(a(1, 0) * a(2, 2) - a(1, 2) * a(2, 0)) / det;
+    R[4] = (a(0, 0) * a(2, 2) - a(0, 2) * a(2, 0)) / det;
+    R[5] = -(a(0, 0) * a(1, 2) - a(0, 2) * a(1, 0)) / det;
+    R[6] = (a(1, 0) * a(2, 1) - a(1, 1) * a(2, 0)) / det;
+    R[7] = -(a(0, 0) * a(2, 1) - a(0, 1) * a(2, 0)) / det;
+    R[8] = (a(0, 0) * a(1, 1) - a(0, 1) * a(1, 0)) / det;
+    A = R;
+    return true;
+}
+
+// Reinitialize_particle_density (Taylor_Green_Vortex/Reinitialize_particle_density.f90:98-181,
+// MLS_Interpolation_In_Subdomain_Domain.f90:96-285; the moving-square variant
+// Moving_Square.../Reinitialize_particle_density.f90:92-200 includes the particle
+// itself, weights the kernel by the neighbour volume, has no order-6 fallback and
+// keeps the old density on NaN).  Candidates: the 3x3 background cells in stencil
+// order (the effect list of Assign_boundary_particles), on the current positions.
+void mls_reinit(Particles& P, int n_host) {
+    const int m = g_cfg.mls_order;
+    const bool ms = ms_solver();
+    const double hb = (g_cfg.h + g_cfg.h) / 2.0;
+    const double alpha = g_cfg.mls_alpha;
+    Grid G;
+    build_grid(P, G);
+    const std::vector<double> rho_old = P.rho;
+    std::vector<double> rho_new(n_host);
+    #pragma omp parallel for schedule(dynamic, 64)
+    for (int i = 0; i < n_host; ++i) {
+        rho_new[i] = rho_old[i];
+        if (P.type[i] != SPH_TYPE_WATER) continue;
+        std::vector<int> nb;
+        std::vector<double> W;
+        const int ci = G.cell[i];
+        const int cx = ci % G.nx, cy = ci / G.nx;
+        for (int s = 0; s < 9; ++s) {
+            const int gx = cx + kStencil[s][0], gy = cy + kStencil[s][1];
+            if (gx < 0 || gy < 0 || gx >= G.nx || gy >= G.ny) continue;
+            const int c = gy * G.nx + gx;
+            for (int t = G.start[c]; t < G.start[c + 1]; ++t) {
+                const int j = G.items[t];
+                double pd[2] = {P.x[i] - P.x[j], P.y[i] - P.y[j]};
+                const double d = std::sqrt(pd[0] * pd[0] + pd[1] * pd[1]);
+                if (!(d <= g_cfg.kernel_scale * hb)) continue;
+                if (!ms && !(d >= g_K.cut_min)) continue;
+                double w, dw[2];
+                kernel(d, pd, hb, w, dw);
+                if (ms) w = w * (P.mass[j] / rho_old[j]);
+                nb.push_back(j);
+                W.push_back(w);
+            }
+        }
+        const int k = (int)nb.size();
+        std::vector<double> fai(k);
+        double sw = 0.0;
+        for (int q = 0; q < k; ++q) sw += W[q];
+        bool shepard = false;
+        // P (m x k), augmented by alpha I with weights alpha (:155-172)
+        std::vector<double> Pm((size_t)m * (k + m), 0.0), Wd(k + m, 0.0);
+        for (int q = 0; q < k; ++q) {
+            const int j = nb[q];
+            const double dx = (P.x[j] - P.x[i]) / g_cfg.h, dy = (P.y[j] - P.y[i]) / g_cfg.h;
+            double pv[6] = {1.0, dx, dy, dx * dx, dx * dy, dy * dy};
+            for (int r = 0; r < m; ++r) Pm[(size_t)r * (k + m) + q] = pv[r];
+            Wd[q] = W[q];
+        }
+        for (int L = 0; L < m; ++L) { Pm[(size_t)L * (k + m) + k + L] = alpha; Wd[k + L] = alpha; }
+        // B = P W, A = B P^T (:176-180)
+        std::vector<double> B((size_t)m * (k + m)), A((size_t)m * m, 0.0);
+        for (int r = 0; r < m; ++r)
+            for (int q = 0; q < k + m; ++q) B[(size_t)r * (k + m) + q] = Pm[(size_t)r * (k + m) + q] * Wd[q];
+        for (int r = 0; r < m; ++r)
+            for (int c = 0; c < m; ++c) {
+                double a = 0.0;
+                for (int q = 0; q < k + m; ++q) a += B[(size_t)r * (k + m) + q] * Pm[(size_t)c * (k + m) + q];
+                A[(size_t)r * m + c] = a;
+            }
+        const bool ok = m == 6 ? gauss_jordan_inverse(A, 6) : inverse3(A);
+        if (!ok) shepard = true;
+        if (!ms && m == 6 && k <= 8) shepard = true;
+        double rho = 0.0;
+        for (int q = 0; q < k; ++q) {
+            double f;
+            if (shepard) f = W[q] / sw;
+            else {   // Fai = row 1 of A^-1 B  (P_i = e_1)
+                f = 0.0;
+                for (int r = 0; r < m; ++r) f += A[(size_t)0 * m + r] * B[(size_t)r * (k + m) + q];
+            }
+            rho += rho_old[nb[q]] * f;
+        }
+        if (ms && std::isnan(rho)) rho = rho_old[i];
+        rho_new[i] = rho;
+    }
+    for (int i = 0; i < n_host; ++i) P.rho[i] = rho_new[i];
+}
+
 struct Sim {
     sph_config cfg;
     Particles H;                      // host particles
@@ -1071,6 +1205,7 @@ void run_step_euler_pc(Sim& S, double dt) {
     S.racc1.assign(R.acc[1].begin(), R.acc[1].begin() + n);
     S.ravg0.assign(R.avg[0].begin(), R.avg[0].begin() + n);
     S.ravg1.assign(R.avg[1].begin(), R.avg[1].begin() + n);
+    if (g_cfg.mls_order && (S.step + 1) % g_cfg.mls_every == 0) mls_reinit(P, n);
     if (g_cfg.shifting) shift_particles(P, n, R);
     for (int i = 0; i < n; ++i) {
         S.H.x[i] = P.x[i]; S.H.y[i] = P.y[i]; S.H.u[i] = P.u[i]; S.H.v[i] = P.v[i]; S.H.rho[i] = P.rho[i];
@@ -1157,6 +1292,8 @@ void run_step(Sim& S, double dt) {
     S.racc1.assign(R.acc[1].begin(), R.acc[1].begin() + n);
     S.ravg0.assign(R.avg[0].begin(), R.avg[0].begin() + n);
     S.ravg1.assign(R.avg[1].begin(), R.avg[1].begin() + n);
+    // Reinitialize_particle_density every MLS_time_step steps, before shifting (:673-682)
+    if (g_cfg.mls_order && (S.step + 1) % g_cfg.mls_every == 0) mls_reinit(P, n);
     if (g_cfg.shifting) shift_particles(P, n, R);
     // copy the host particles back (images are discarded)
     for (int i = 0; i < n; ++i) {
@@ -1187,6 +1324,20 @@ Particles make_particles(int n, const double* pos, const double* vel, const doub
 // like the Fortran module arrays.
 // ===========================================================================
 extern "C" {
+
+// Reinitialize_particle_density alone on the given particles (no images):
+// rho_out = the re-initialised densities of the n particles.
+int oracle_mls_reinit(const sph_config* cfg, int n, const double* pos, const double* rho, const double* mass,
+                      const int* type, double* rho_out) {
+    if (!cfg || n <= 0 || !(cfg->mls_order == 3 || cfg->mls_order == 6)) return -1;
+    g_cfg = *cfg;
+    derive_consts(*cfg);
+    std::vector<double> zero(2 * (size_t)n, 0.0);
+    Particles P = make_particles(n, pos, zero.data(), rho, mass, type, nullptr);
+    mls_reinit(P, n);
+    for (int i = 0; i < n; ++i) rho_out[i] = P.rho[i];
+    return 0;
+}
 
 int oracle_threads(int nthreads) {
 #ifdef _OPENMP

@@ -19,7 +19,7 @@
 //
 // Scope: the modified linear Riemann delta-SPH + SPS solver, RK4 with the K1
 // reuse, periodic images, either kernel, with or without renormalisation,
-// no shifting, no XSPH, no free-surface particles.  Other inputs return
+// no shifting, no XSPH, no density re-initialisation, no free-surface particles.  Other inputs return
 // SPH_E_CONFIG.  The pair search is a plain double loop (small cases only).
 
 #include <cmath>
@@ -431,7 +431,7 @@ int oracle_tangent(const sph_config* cfg, int n, const double* pos, const double
                    double* pos_out, double* vel_out, double* rho_out) {
     if (!cfg || !pos || !vel || !rho || !mass || !type || !out || n <= 0 || nsteps <= 0) return SPH_E_ARG;
     if (cfg->solver != SPH_SOLVER_MODLR_DELTA_SPS || cfg->integrator != SPH_INTEGRATOR_RK4_REUSE ||
-        cfg->shifting || cfg->xsph_eps != 0.0 || cfg->pair_rule != SPH_PAIRS_ONE_FLUID)
+        cfg->shifting || cfg->xsph_eps != 0.0 || cfg->pair_rule != SPH_PAIRS_ONE_FLUID || cfg->mls_order != 0)
         return SPH_E_CONFIG;
     if (loss == SPH_LOSS_VELOCITY_MISFIT && !target_vel) return SPH_E_ARG;
     std::vector<Dual> x(n), y(n), u(n), v(n), r(n);

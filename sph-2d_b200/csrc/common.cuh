@@ -23,6 +23,8 @@ struct Params {
     // switches
     int kernel_model, solver, renorm, quirks, pair_rule, shifting, muscl, xsph;
     int ms, hllc, laplacian, free_surface, integrator, has_body;
+    int mls_order, mls_every;     // density re-initialisation (0: off)
+    double mls_alpha3;            // alpha^3 added to the moment matrix diagonal
     // kernel / pair search
     double h, r_cut, cut_min, kfactor, gauss_e9, q_zero;
     double r2_list;          // squared neighbour-list radius (support * (1 + skin))

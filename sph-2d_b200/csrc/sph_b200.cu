@@ -101,6 +101,7 @@ struct sph_handle {
     double* d_bf = nullptr;               // [6 * blocks(cap_tot) partials + 6]
     bool bf_every_rhs = false;            // sph_rhs also reports it
     struct AdjCtx* adj = nullptr;         // saved context of sph_adjoint_forward
+    double* d_mls = nullptr;              // re-initialised densities [cap_tot]
 };
 
 namespace {
@@ -116,6 +117,8 @@ int derive_params(const sph_config& c, Params& P) {
     if (!(c.h > 0) || !(c.kernel_scale >= 2.0) || !(c.dx > 0) || !(c.rho0 > 0) || !(c.c0sq > 0)) return SPH_E_CONFIG;
     if (c.cell_skin < 0 || c.cell_skin > 2) return SPH_E_CONFIG;
     if (c.shift_n != 4) return SPH_E_CONFIG;
+    if (c.mls_order != 0 && c.mls_order != 3 && c.mls_order != 6) return SPH_E_CONFIG;
+    if (c.mls_order != 0 && (c.mls_every < 1 || !(c.mls_alpha >= 0))) return SPH_E_CONFIG;
     memset(&P, 0, sizeof(P));
     const bool q = c.reference_literals != 0;
     P.kernel_model = c.kernel_model;
@@ -127,6 +130,9 @@ int derive_params(const sph_config& c, Params& P) {
     P.laplacian = c.laplacian;
     P.free_surface = c.free_surface ? 1 : 0;
     P.integrator = c.integrator;
+    P.mls_order = c.mls_order;
+    P.mls_every = c.mls_order ? c.mls_every : 1;
+    P.mls_alpha3 = c.mls_alpha * c.mls_alpha * c.mls_alpha;
     P.has_body = 0;
     P.renorm = c.renormalize ? 1 : 0;
     P.quirks = q ? 1 : 0;
@@ -411,17 +417,36 @@ int read_status(sph_handle* h) {
     return status_to_code(st);
 }
 
+// Reinitialize_particle_density on the state after the integrator update of a
+// step, then the step's shift (time_iteration.f90:673-682).
+template <typename R>
+int reinit_density(sph_handle* h, int do_shift) {
+    const Params& P = h->P;
+    Sorted<R>& D = sorted<R>(h);
+    const int nb = blocks(P.n_tot, 128);
+    tic(h, PH_UPDATE);
+    if (P.mls_order == 6) k_mls<R, 6><<<nb, 128, 0, h->stream>>>(P, D, h->d_mls);
+    else k_mls<R, 3><<<nb, 128, 0, h->stream>>>(P, D, h->d_mls);
+    k_finish_mls<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, D, h->d_mls, do_shift, h->d_status);
+    CK(cudaGetLastError());
+    h->launches += 2;
+    return SPH_OK;
+}
+
 template <typename R>
 int run_steps(sph_handle* h, int nsteps, double dt) {
     for (int s = 0; s < nsteps; ++s) {
         int rc = prepare<R>(h);
         if (rc) return rc;
         const int first = h->step_count == 0;
+        // density re-initialisation after every mls_every-th step (1-based step number)
+        const bool mls = h->P.mls_order != 0 && (h->step_count + 1) % h->P.mls_every == 0;
+        const int shift_now = mls ? 0 : h->cfg.shifting;
         if (first) { rc = rhs<R>(h, 0); if (rc) return rc; }
         if (h->cfg.integrator == SPH_INTEGRATOR_EULER_PC) {
             rc = stage<R>(h, 10, dt, first ? 0 : 1, 0); if (rc) return rc;
             rc = rhs<R>(h, 1); if (rc) return rc;
-            rc = stage<R>(h, 11, dt, 0, h->cfg.shifting); if (rc) return rc;
+            rc = stage<R>(h, 11, dt, 0, shift_now); if (rc) return rc;
         } else {
             rc = stage<R>(h, 0, dt, first ? 0 : 1, 0); if (rc) return rc;
             rc = rhs<R>(h, 0); if (rc) return rc;
@@ -429,8 +454,9 @@ int run_steps(sph_handle* h, int nsteps, double dt) {
             rc = rhs<R>(h, 0); if (rc) return rc;
             rc = stage<R>(h, 2, dt, 0, 0); if (rc) return rc;
             rc = rhs<R>(h, 1); if (rc) return rc;
-            rc = stage<R>(h, 3, dt, 0, h->cfg.shifting); if (rc) return rc;
+            rc = stage<R>(h, 3, dt, 0, shift_now); if (rc) return rc;
         }
+        if (mls && (rc = reinit_density<R>(h, h->cfg.shifting))) return rc;
         tic(h, -1);
         h->step_count++;
         h->n_steps++;
@@ -602,7 +628,7 @@ int snap_io(sph_handle* h, const Snap& s, int k, int n, bool save) {
 int adj_config_ok(const sph_handle* h) {
     const Params& P = h->P;
     if (h->cfg.solver != SPH_SOLVER_MODLR_DELTA_SPS || P.muscl || P.ms || P.xsph) return SPH_E_CONFIG;
-    if (h->cfg.integrator != SPH_INTEGRATOR_RK4_REUSE || h->cfg.shifting) return SPH_E_CONFIG;
+    if (h->cfg.integrator != SPH_INTEGRATOR_RK4_REUSE || h->cfg.shifting || P.mls_order) return SPH_E_CONFIG;
     return SPH_OK;
 }
 
@@ -869,7 +895,8 @@ void destroy(sph_handle* h) {
     void* ptrs[] = {h->S.pos, h->S.vel, h->S.rho, h->S.mass, h->S.smass, h->S.type, h->S.itype, h->d_bf,
                     h->S.r_drho, h->S.r_acc,
                     h->S.r_avg, h->S.cnt, h->S.off, h->S.lr_cnt, h->S.lr_off, h->S.tb_cnt, h->S.tb_off, h->keys_in, h->keys_out, h->vals_in, h->vals_out, h->cub_tmp,
-                    h->d_status, h->d_int, h->d_part, h->d_diag, h->d_xfer, h->d_export, h->d_off64, h->d_cnt_id};
+                    h->d_status, h->d_int, h->d_part, h->d_diag, h->d_xfer, h->d_export, h->d_off64, h->d_cnt_id,
+                    h->d_mls};
     for (void* p : ptrs) if (p) cudaFree(p);
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -928,6 +955,7 @@ int init_impl(const sph_config* cfg, int n_capacity, sph_handle** out) {
     CK(dalloc(&h->d_int, 4));
     CK(dalloc(&h->d_part, 2 * 148 * 4)); CK(dalloc(&h->d_diag, 2));
     CK(dalloc(&h->d_xfer, (size_t)4 * h->cap_host));
+    if (cfg->mls_order) CK(dalloc(&h->d_mls, cap));
     if (h->mixed) rc = alloc_sorted(h->D32, cap, h->P.max_nbr, h->ncells);
     else rc = alloc_sorted(h->D64, cap, h->P.max_nbr, h->ncells);
     if (rc) { destroy(h); return rc; }

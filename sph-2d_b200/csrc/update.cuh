@@ -21,6 +21,23 @@ namespace sph {
 //   predictor  rho = rho0 + drhodt dt, x = x0 + dt (v0 + avg) + 0.5 a dt^2, v = v0 + dt a
 //   corrector  rho = rho0 + 0.5 (drhodt + drhodt_p) dt,
 //              x = x0 + 0.5 dt (v_p + v0) + avg dt + 0.5 a dt^2, v = v0 + 0.5 dt (a + a_p)
+// Shift_particle_position.f90:108-131: the capped displacement of the last RHS's
+// shifting sum and the first-order density correction, for water particles
+// that are not near the free surface.
+template <typename R>
+__device__ __forceinline__ void apply_shift(const Params& P, const Sorted<R>& D, int s, double& x, double& y,
+                                            double& rho) {
+    if (D.type[s] != SPH_TYPE_WATER || (D.flags[s] & 2)) return;
+    const double2 sh = D.shift[s];
+    double s0 = sh.x, s1 = sh.y;
+    const double amp = sqrt(s0 * s0 + s1 * s1);
+    if (amp > P.shift_max) { s0 = s0 / amp * P.shift_max; s1 = s1 / amp * P.shift_max; }
+    x = x + s0;
+    y = y + s1;
+    rho = rho + (double)D.nb1[s].w * s0;
+    rho = rho + (double)D.nb2[s].x * s1;
+}
+
 template <typename R>
 __global__ void k_stage(Params P, Sorted<R> D, int stage, double dt, int use_carried, int do_shift,
                         unsigned* status) {
@@ -97,17 +114,7 @@ __global__ void k_stage(Params P, Sorted<R> D, int stage, double dt, int use_car
     if (ddx * ddx + ddy * ddy > P.skin_half2) atomicOr(status, ST_SKIN);
     const bool final_stage = stage == 3 || stage == 11;
     if (final_stage) {
-        if (do_shift && D.type[s] == SPH_TYPE_WATER && !(D.flags[s] & 2)) {
-            // Shift_particle_position.f90:108-131
-            const double2 sh = D.shift[s];
-            double s0 = sh.x, s1 = sh.y;
-            const double amp = sqrt(s0 * s0 + s1 * s1);
-            if (amp > P.shift_max) { s0 = s0 / amp * P.shift_max; s1 = s1 / amp * P.shift_max; }
-            x = x + s0;
-            y = y + s1;
-            rho = rho + (double)D.nb1[s].w * s0;
-            rho = rho + (double)D.nb2[s].x * s1;
-        }
+        if (do_shift) apply_shift(P, D, s, x, y, rho);
         if (!(isfinite(x) && isfinite(y) && isfinite(u) && isfinite(v) && isfinite(rho))) atomicOr(status, ST_NONFINITE);
         D.pos0[s] = make_double2(x, y);
         D.vel0[s] = make_double2(u, v);
@@ -122,6 +129,145 @@ __global__ void k_stage(Params P, Sorted<R> D, int stage, double dt, int use_car
     D.kin[s] = make_double4(u, v, rho, p);
     D.aux[s] = mk4<R>((R)m, (R)(m / rho), (R)c, (R)D.smass[s]);
     store_split(D, s, make_double2(x, y), make_double4(u, v, rho, p));
+}
+
+// Density re-initialisation by moving least squares (Reinitialize_particle_density:
+// Taylor_Green_Vortex/Reinitialize_particle_density.f90:98-181 with
+// MLS_Interpolation_In_Subdomain_Domain.f90:96-285; moving-square variant
+// Moving_Square.../Reinitialize_particle_density.f90:92-200 with
+// SPH_Subroutine_Module.f90:2565-2792), FP64, on the state after the integrator
+// update (images keep the step-start state).  For a water particle i and its
+// neighbours j within the support, with W_j the kernel value (the moving-square
+// variant: W_j V_j, and i itself counts as a neighbour),
+//   p_j = (1, dx, dy[, dx^2, dx dy, dy^2]),  (dx, dy) = (x_j - x_i)/h,
+//   A   = sum_j W_j p_j p_j^T + alpha^3 I,
+//   rho_i = sum_j rho_j W_j (A^-1 e_1).p_j = c.r,  A c = e_1,  r = sum_j rho_j W_j p_j.
+// The reference inverts A (BRINV / the 3x3 adjugate) and forms the same weights;
+// here A c = e_1 is solved by an FP64 Cholesky factorisation (A is symmetric and
+// positive definite away from degenerate neighbourhoods).  A failed factorisation,
+// and with order 6 at most 8 neighbours (Taylor-Green variant), fall back to the
+// Shepard weights W_j / sum W, as the reference does.  Non-water particles keep
+// their density (the Taylor-Green routine zeroes its periodic images, which are
+// regenerated at the next step start).
+template <int M>
+__device__ __forceinline__ bool chol_solve_e1(double (&A)[M * (M + 1) / 2], double (&c)[M]) {
+    // packed lower triangle, row-major: A[i(i+1)/2 + j], j <= i
+    double L[M * (M + 1) / 2];
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+#pragma unroll
+        for (int j = 0; j <= i; ++j) {
+            double sum = A[i * (i + 1) / 2 + j];
+#pragma unroll
+            for (int k = 0; k < j; ++k) sum -= L[i * (i + 1) / 2 + k] * L[j * (j + 1) / 2 + k];
+            if (i == j) {
+                if (!(sum > 0.0)) return false;
+                L[i * (i + 1) / 2 + i] = sqrt(sum);
+            } else {
+                L[i * (i + 1) / 2 + j] = sum / L[j * (j + 1) / 2 + j];
+            }
+        }
+    }
+    // L y = e_1, L^T c = y
+    double y[M];
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+        double sum = i == 0 ? 1.0 : 0.0;
+#pragma unroll
+        for (int k = 0; k < i; ++k) sum -= L[i * (i + 1) / 2 + k] * y[k];
+        y[i] = sum / L[i * (i + 1) / 2 + i];
+    }
+#pragma unroll
+    for (int i = M - 1; i >= 0; --i) {
+        double sum = y[i];
+#pragma unroll
+        for (int k = i + 1; k < M; ++k) sum -= L[k * (k + 1) / 2 + i] * c[k];
+        c[i] = sum / L[i * (i + 1) / 2 + i];
+    }
+    return true;
+}
+
+template <typename R, int M>
+__global__ void k_mls(Params P, Sorted<R> D, double* rho_new) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= P.n_tot) return;
+    const double rho_a = D.kin[a].z;
+    if (D.type[a] != SPH_TYPE_WATER || D.id[a] >= P.n_host) { rho_new[a] = rho_a; return; }
+    const double2 xa = D.pos[a];
+    const double inv_h = 1.0 / P.h;
+    double A[M * (M + 1) / 2], r[M];
+#pragma unroll
+    for (int k = 0; k < M * (M + 1) / 2; ++k) A[k] = 0.0;
+#pragma unroll
+    for (int k = 0; k < M; ++k) r[k] = 0.0;
+    double sw = 0.0, srw = 0.0;
+    int cnt = 0;
+    const int nn = D.nnbr[a];
+    // the moving-square variant includes the particle itself (distance 0)
+    for (int e = (P.ms ? -1 : 0); e < nn; ++e) {
+        const int b = e < 0 ? a : (int)(D.nbr[(size_t)e * P.nbr_stride + a] & 0x7fffffffu);
+        const double2 xb = D.pos[b];
+        const double px = xa.x - xb.x, py = xa.y - xb.y;
+        double d;
+        const bool in = in_support(P, px, py, d);
+        if (P.ms ? !(d <= P.r_cut) : !in) continue;
+        double w, gx, gy;
+        kernel_w_dw<double>(P, d, px, py, w, gx, gy);
+        const double rho_b = D.kin[b].z;
+        if (P.ms) w *= D.mass[b] / rho_b;
+        double p[M];
+        const double dx = -px * inv_h, dy = -py * inv_h;
+        p[0] = 1.0; p[1] = dx; p[2] = dy;
+        if (M == 6) { p[3 % M] = dx * dx; p[4 % M] = dx * dy; p[5 % M] = dy * dy; }
+#pragma unroll
+        for (int i = 0; i < M; ++i) {
+            const double wp = w * p[i];
+#pragma unroll
+            for (int j = 0; j <= i; ++j) A[i * (i + 1) / 2 + j] += wp * p[j];
+            r[i] += rho_b * wp;
+        }
+        sw += w;
+        srw += rho_b * w;
+        ++cnt;
+    }
+#pragma unroll
+    for (int i = 0; i < M; ++i) A[i * (i + 1) / 2 + i] += P.mls_alpha3;
+    double c[M];
+    double out;
+    const bool few = !P.ms && M == 6 && cnt <= 8;
+    if (!few && chol_solve_e1<M>(A, c)) {
+        out = 0.0;
+#pragma unroll
+        for (int i = 0; i < M; ++i) out += c[i] * r[i];
+    } else {
+        out = srw / sw;
+    }
+    if (P.ms && isnan(out)) out = rho_a;
+    rho_new[a] = out;
+}
+
+// The re-initialised density replaces the integrated one; then the shift of the
+// step (when on) is applied, as the reference's driver calls the two in turn.
+template <typename R>
+__global__ void k_finish_mls(Params P, Sorted<R> D, const double* rho_new, int do_shift, unsigned* status) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= P.n_tot) return;
+    if (!integrated(P, D.type[s]) || D.id[s] >= P.n_host) return;
+    const double2 x0 = D.pos0[s];
+    double x = x0.x, y = x0.y;
+    double rho = D.type[s] == SPH_TYPE_WATER ? rho_new[s] : D.rho0[s];
+    if (do_shift) apply_shift(P, D, s, x, y, rho);
+    if (!(isfinite(x) && isfinite(y) && isfinite(rho))) atomicOr(status, ST_NONFINITE);
+    D.pos0[s] = make_double2(x, y);
+    D.pos[s] = make_double2(x, y);
+    D.rho0[s] = rho;
+    double p, c;
+    eos64(P, rho, p, c);
+    const double2 v = D.vel0[s];
+    const double m = D.mass[s];
+    D.kin[s] = make_double4(v.x, v.y, rho, p);
+    D.aux[s] = mk4<R>((R)m, (R)(m / rho), (R)c, (R)D.smass[s]);
+    store_split(D, s, make_double2(x, y), make_double4(v.x, v.y, rho, p));
 }
 
 // Kinetic energy and max |v| of the water host particles

@@ -78,6 +78,7 @@ class SphConfig(ctypes.Structure):
         ("box_lo", ctypes.c_double * 2), ("box_hi", ctypes.c_double * 2),
         ("grid_lo", ctypes.c_double * 2), ("grid_hi", ctypes.c_double * 2),
         ("cell_skin", ctypes.c_double), ("laplacian", ctypes.c_int), ("free_surface", ctypes.c_int),
+        ("mls_order", ctypes.c_int), ("mls_every", ctypes.c_int), ("mls_alpha", ctypes.c_double),
     ]
 
     def copy(self) -> "SphConfig":
@@ -151,6 +152,9 @@ def tgv_reference_config(n_side: int = 100) -> SphConfig:
     c.cell_skin = 0.1
     c.laplacian = 1
     c.free_surface = 1
+    # Reinitialize_particle_density: quadratic MLS every 20 steps (:324-332),
+    # slighted_modified_alpha = 0.0001 as a default real (:359)
+    c.mls_order, c.mls_every, c.mls_alpha = 6, 20, float(np.float32(1.0e-4))
     return c
 
 
@@ -174,6 +178,7 @@ def tgv_baseline_config(n_side: int, solver: int = SOLVER_MUSCL_DELTA_SPS,
     c.nu = 0.01
     c.shift_max = 0.25 * dx
     c.cell_skin = 0.1
+    c.mls_order = 0              # the benchmark case: no density re-initialisation
     return c
 
 
@@ -523,6 +528,9 @@ def moving_square_config(dx: float, lx: float, ly: float, solver: int = SOLVER_M
     c.cell_skin = 0.1
     c.laplacian = 1
     c.free_surface = 0
+    # Reinitialize_particle_density: linear MLS every 40 steps (:662-671),
+    # Slighted_modified_alpha = 1e-5 (:782)
+    c.mls_order, c.mls_every, c.mls_alpha = 3, 40, 1.0e-5
     return c
 
 

@@ -35,6 +35,7 @@ def _case(kind):
     else:
         case = S.make_tgv(32, reference=True, jitter=0.05, seed=12)
     case.cfg.shifting = 0
+    case.cfg.mls_order = 0
     return case
 
 

@@ -13,6 +13,7 @@ def _case(kind):
     else:
         case = S.make_tgv(24, reference=True, jitter=0.05, seed=4)
     case.cfg.shifting = 0
+    case.cfg.mls_order = 0
     return case
 
 
