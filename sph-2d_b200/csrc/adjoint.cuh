@@ -644,6 +644,7 @@ __global__ void k_adj_load(Params P, Sorted<R> D, const double2* pos, const doub
     D.pos[s] = x;
     D.kin[s] = k;
     D.aux[s] = mk4<R>((R)m, (R)(m / k.z), (R)c, (R)D.smass[s]);
+    store_split(D, s, x, k);
 }
 
 // Copies of the state a step starts from (id order, host particles) into or out

@@ -111,6 +111,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (MS ? 4 : 5) : 3) k_pass
     cont.init(); accx.init(); accy.init();
     R xsx = R(0), xsy = R(0);
     double shx = 0.0, shy = 0.0;   // shifting sum, FP64 in both paths
+    const double inv_h64 = 1.0 / P.h, inv_h2_64 = inv_h64 * inv_h64, inv_wdx = 1.0 / P.w_dx;
 
     // the pairs pass A found inside the support at this RHS
     unsigned ent_n = nn > 0 ? __ldg(&D.pairs[a]) : 0u;
@@ -331,23 +332,25 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (MS ? 4 : 5) : 3) k_pass
         if (SHIFT) {
             double gd, wd, Vd;
             if (F32) {
+                // FP64 without divisions: q = d/h, grad factor G = g/(d h) = -5 k t^3/h^2
+                // (Wendland) or -2 k e^{-q^2}/h^2 (Gaussian), V_b from the FP64 volume record
                 const double dd2 = sqrt(dxd * dxd + dyd * dyd);
-                const double q = dd2 / P.h;
+                const double q = dd2 * inv_h64;
                 if (P.kernel_model == SPH_KERNEL_GAUSSIAN) {
                     const double ex = exp(-(q * q));
                     wd = (ex - P.gauss_e9) * P.kfactor;
-                    gd = ex * (-2 * q) / (dd2 * P.h) * P.kfactor;
+                    gd = -2.0 * P.kfactor * ex * inv_h2_64;
                 } else {
-                    const double t = 1 - q / 2.0;
-                    const double t3 = t * t * t;
-                    wd = P.kfactor * (1 + 2 * q) * (t3 * t);
-                    gd = P.kfactor * (-5 * q * t3) / (dd2 * P.h);
+                    const double t = 1.0 - 0.5 * q;
+                    const double t2 = t * t;
+                    wd = P.kfactor * (1.0 + 2.0 * q) * (t2 * t2);
+                    gd = -5.0 * P.kfactor * (t2 * t) * inv_h2_64;
                 }
-                Vd = D.mass[b] / (HL ? __ldg(&D.kin[b].z) : T.kin.z);
+                Vd = __ldg(&D.vol64[b]);
             } else {
                 wd = (double)w; gd = (double)g; Vd = (double)Vb;
             }
-            const double r = wd / P.w_dx;
+            const double r = wd * inv_wdx;
             const double r2 = r * r;
             const double f = (1 + P.shift_R * (r2 * r2)) * Vd * gd;
             shx += f * dxd;

@@ -159,6 +159,7 @@ struct Sorted {
     // hi + lo parts (v = hi + lo, hi = (float)v), so pass C forms pair
     // differences (hi_i - hi_j) + (lo_i - lo_j) in FP32 with the accuracy of the
     // FP64 difference rounded to FP32, without FP64 arithmetic or conversions
+    double* vol64;    // m / rho in FP64 (the mixed path's FP64 shifting sum)
     float4* kh;       // u, v, rho, p  (hi)
     float4* kl;       //               (lo)
     float4* xhl;      // x hi, y hi, x lo, y lo
@@ -168,6 +169,7 @@ struct Sorted {
 template <typename R>
 __device__ __forceinline__ void store_split(Sorted<R>& D, int s, double2 x, double4 k) {
     if (sizeof(R) != 4) return;
+    D.vol64[s] = D.mass[s] / k.z;
     const float uh = (float)k.x, vh = (float)k.y, rh = (float)k.z, ph = (float)k.w;
     D.kh[s] = make_float4(uh, vh, rh, ph);
     D.kl[s] = make_float4((float)(k.x - (double)uh), (float)(k.y - (double)vh), (float)(k.z - (double)rh),

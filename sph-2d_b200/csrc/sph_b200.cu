@@ -259,7 +259,9 @@ int alloc_sorted(Sorted<R>& D, int cap, int max_nbr, int ncells) {
     CK(dalloc(&D.nbr, (size_t)cap * max_nbr)); CK(dalloc(&D.nnbr, cap));
     CK(dalloc(&D.pairs, (size_t)cap * max_nbr)); CK(dalloc(&D.npairs, cap));
     CK(dalloc(&D.cell_start, ncells)); CK(dalloc(&D.cell_end, ncells));
-    if (sizeof(R) == 4) { CK(dalloc(&D.kh, cap)); CK(dalloc(&D.kl, cap)); CK(dalloc(&D.xhl, cap)); }
+    if (sizeof(R) == 4) {
+        CK(dalloc(&D.kh, cap)); CK(dalloc(&D.kl, cap)); CK(dalloc(&D.xhl, cap)); CK(dalloc(&D.vol64, cap));
+    }
     CK(cudaMemset(D.nb3, 0, sizeof(*D.nb3) * (size_t)cap));
     CK(cudaMemset(D.flags, 0, (size_t)cap));
     return SPH_OK;
@@ -270,7 +272,7 @@ void free_sorted(Sorted<R>& D) {
     void* ptrs[] = {D.id, D.type, D.itype, D.pos, D.pos0, D.vel0, D.rho0, D.mass, D.smass, D.kin, D.aux, D.nb1, D.nb2, D.nb3,
                     D.binv, D.binv64, D.fra_v, D.flags, D.drho, D.acc, D.avg, D.shift, D.ks_r, D.ks_a, D.ks_v, D.c_drho,
                     D.c_acc, D.c_avg, D.nbr, D.nnbr, D.pairs, D.npairs, D.cell_start, D.cell_end, D.kh, D.kl,
-                    D.xhl};
+                    D.xhl, D.vol64};
     for (void* p : ptrs) if (p) cudaFree(p);
     D = Sorted<R>{};
 }
