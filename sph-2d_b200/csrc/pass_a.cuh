@@ -19,7 +19,7 @@
 namespace sph {
 
 template <typename R>
-__global__ void __launch_bounds__(128, sizeof(R) == 4 ? 8 : 6) k_pass_a(Params P, Sorted<R> D) {
+__global__ void __launch_bounds__(128, sizeof(R) == 4 ? 6 : 4) k_pass_a(Params P, Sorted<R> D) {
     using V4 = typename VT<R>::V4;
     constexpr bool F32 = sizeof(R) == 4;
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
@@ -41,16 +41,33 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 8 : 6) k_pass_a(Params P
     const R inv_h = (R)(1.0 / P.h);
     const R r2cut = (R)(P.r_cut * P.r_cut), r2min = (R)(P.cut_min * P.cut_min);
     int np = 0;
-    // the next entry and its position are loaded one iteration ahead
+    // two-deep software pipeline: the list entry two iterations ahead, the
+    // neighbour's position and records (kin, volume) one iteration ahead, so the
+    // loads of the next neighbour are in flight while this one is evaluated
     unsigned ent_n = nn > 0 ? __ldg(&D.nbr[a]) : 0u;
-    double2 xb_n = nn > 0 ? __ldg(&D.pos[ent_n & 0x7fffffffu]) : make_double2(0.0, 0.0);
+    unsigned ent_nn = nn > 1 ? __ldg(&D.nbr[(size_t)P.nbr_stride + a]) : 0u;
+    double2 xb_n = make_double2(0.0, 0.0);
+    double4 kb_n = make_double4(0.0, 0.0, 0.0, 0.0);
+    R vb_n = R(0);
+    if (nn > 0) {
+        const int b0 = (int)(ent_n & 0x7fffffffu);
+        xb_n = __ldg(&D.pos[b0]);
+        kb_n = D.kin[b0];
+        vb_n = D.aux[b0].y;
+    }
     for (int e = 0; e < nn; ++e) {
         const unsigned ent = ent_n;
         const int b = (int)(ent & 0x7fffffffu);
         const double2 xb = xb_n;
+        const double4 kb = kb_n;
+        const R Vb = vb_n;
         if (e + 1 < nn) {
-            ent_n = __ldg(&D.nbr[(size_t)(e + 1) * P.nbr_stride + a]);
-            xb_n = __ldg(&D.pos[ent_n & 0x7fffffffu]);
+            ent_n = ent_nn;
+            const int b1 = (int)(ent_n & 0x7fffffffu);
+            xb_n = __ldg(&D.pos[b1]);
+            kb_n = D.kin[b1];
+            vb_n = D.aux[b1].y;
+            if (e + 2 < nn) ent_nn = __ldg(&D.nbr[(size_t)(e + 2) * P.nbr_stride + a]);
         }
         const double dxd = xa.x - xb.x, dyd = xa.y - xb.y;
         R d, inv_d;
@@ -84,13 +101,11 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 8 : 6) k_pass_a(Params P
                 gs = kf * (R(-5) * q * t3) * inv_d * inv_h;
             }
         }
-        const double4 kb = D.kin[b];
         if (P.ms) {
             const R f = (R)P.eps * D.aux[b].x / (R)(ka.z + kb.z) * wk;
             xs0 -= f * (R)(ka.x - kb.x);
             xs1 -= f * (R)(ka.y - kb.y);
         }
-        const R Vb = D.aux[b].y;
         const R gx = gs * dx * Vb, gy = gs * dy * Vb;    // V_b grad_a W
         // volume fraction (Define_freesurface...f90:84-85)
         fra += Vb;
