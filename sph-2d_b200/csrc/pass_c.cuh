@@ -69,7 +69,7 @@ struct Side {
 // shifting on, which also forms the shifting sum.  Both are compile-time so that
 // each launch carries only the registers of the terms it evaluates.
 template <typename R, bool MUSCL, bool MS, bool SHIFT>
-__global__ void __launch_bounds__(128, sizeof(R) == 4 ? (MS ? 4 : 5) : 3) k_pass_c(Params P, Sorted<R> D) {
+__global__ void __launch_bounds__(128, sizeof(R) == 4 ? 4 : 3) k_pass_c(Params P, Sorted<R> D) {
     using V4 = typename VT<R>::V4;
     using A = typename Acc<R>::T;
     constexpr bool F32 = sizeof(R) == 4;
@@ -115,11 +115,24 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (MS ? 4 : 5) : 3) k_pass
 
     // the pairs pass A found inside the support at this RHS
     unsigned ent_n = nn > 0 ? __ldg(&D.pairs[a]) : 0u;
+    // software pipeline: the pair entry two iterations ahead; the neighbour's
+    // position and (mixed path) its records one iteration ahead
+    constexpr bool PRE = HL;
+    unsigned ent_nn = nn > 1 ? __ldg(&D.pairs[(size_t)P.nbr_stride + a]) : 0u;
     double2 xb_n = make_double2(0.0, 0.0);
     float4 xbhl_n = make_float4(0.f, 0.f, 0.f, 0.f);
+    Side<R> T_n;
+    auto load_records = [&](int bb, Side<R>& t) {
+        if (HL) { t.kh = D.kh[bb]; t.kl = D.kl[bb]; }
+        else t.kin = D.kin[bb];
+        t.aux = D.aux[bb]; t.nb1 = D.nb1[bb]; t.nb2 = D.nb2[bb];
+        if (MUSCL) t.nb3 = D.nb3[bb];
+    };
     if (nn > 0) {
-        if (HL) xbhl_n = __ldg(&D.xhl[ent_n & 0x7fffffffu]);
-        else xb_n = __ldg(&D.pos[ent_n & 0x7fffffffu]);
+        const int b0 = (int)(ent_n & 0x7fffffffu);
+        if (HL) xbhl_n = __ldg(&D.xhl[b0]);
+        else xb_n = __ldg(&D.pos[b0]);
+        if (PRE) load_records(b0, T_n);
     }
     for (int e = 0; e < nn; ++e) {
         const unsigned ent = ent_n;
@@ -127,10 +140,15 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (MS ? 4 : 5) : 3) k_pass
         const bool a_is_i = (ent >> 31) != 0;
         const double2 xb = xb_n;
         const float4 xbhl = xbhl_n;
+        Side<R> T;
+        if (PRE) T = T_n;
         if (e + 1 < nn) {
-            ent_n = __ldg(&D.pairs[(size_t)(e + 1) * P.nbr_stride + a]);
-            if (HL) xbhl_n = __ldg(&D.xhl[ent_n & 0x7fffffffu]);
-            else xb_n = __ldg(&D.pos[ent_n & 0x7fffffffu]);
+            ent_n = ent_nn;
+            const int b1 = (int)(ent_n & 0x7fffffffu);
+            if (HL) xbhl_n = __ldg(&D.xhl[b1]);
+            else xb_n = __ldg(&D.pos[b1]);
+            if (PRE) load_records(b1, T_n);
+            if (e + 2 < nn) ent_nn = __ldg(&D.pairs[(size_t)(e + 2) * P.nbr_stride + a]);
         }
         // x_a - x_b: FP64, or hi/lo in FP32 (the shifting sum still reads the FP64 positions)
         double dxd = 0.0, dyd = 0.0;
@@ -150,11 +168,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (MS ? 4 : 5) : 3) k_pass
             d = (R)sqrt(dxd * dxd + dyd * dyd);
             inv_d = R(1) / d;
         }
-        Side<R> T;
-        if (HL) { T.kh = D.kh[b]; T.kl = D.kl[b]; }
-        else T.kin = D.kin[b];
-        T.aux = D.aux[b]; T.nb1 = D.nb1[b]; T.nb2 = D.nb2[b];
-        if (MUSCL) T.nb3 = D.nb3[b];
+        if (!PRE) load_records(b, T);
         const Side<R>& I = a_is_i ? S : T;
         const Side<R>& J = a_is_i ? T : S;
         const R sgn = a_is_i ? R(1) : R(-1);
