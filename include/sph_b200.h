@@ -114,6 +114,18 @@ typedef struct sph_config {
     int    mls_order;
     int    mls_every;
     double mls_alpha;
+    /* Fixed-ghost and body-ghost assignment of the moving-square driver
+     * (Moving_Square.../Assign_boundary_particles.f90:611-941), run at the start of
+     * every right-hand side when ghost_assign = 1; 0 leaves the ghost states to
+     * the host.  Shepard interpolation (MLS_order_Boundary = 1) over the non-ghost
+     * particles within kernel_scale * ghost_h_factor * h (ghost_h_factor = 1.2),
+     * mirrored velocities by wall label (sph_set_boundary_labels), the body's
+     * prescribed velocity (sph_set_body_motion). */
+    int    ghost_assign;
+    int    wall_bc;               /* ExternalBoundaryCondition: 1 free slip, 0 no slip  */
+    double ghost_h_factor;
+    double shock_release_time;    /* Shock_wave_release_time                           */
+    double gravity[2];            /* Gravity_grad                                      */
 } sph_config;
 
 /* diagnostics returned by sph_step (reductions in FP64) */
@@ -167,6 +179,25 @@ int sph_update_state(sph_handle* h, int n, const double* pos, const double* vel,
  * (Moving_Square.../Calculate_Body_Force.f90:60).  Without this call no body
  * force is computed. */
 int sph_set_initial_type(sph_handle* h, int n, const int* initial_type);
+
+/* subdomain_Boundary_particle_type for the n host particles: -6 horizontal
+ * wall, -7 corner ("center"), -8 vertical wall, 0 anything else
+ * (Moving_Square.../Initial_Particle_From_First_Step.f90:220-300).  Used by the
+ * ghost assignment; the radius free-slip label -9 (cylinder walls) is not
+ * supported (SPH_E_CONFIG). */
+int sph_set_boundary_labels(sph_handle* h, int n, const int* labels);
+
+/* Custom_velocity and Custom_accleration of Body_Motion_Solver
+ * (Moving_Square.../Body_Motion_Solver.f90:150-195) for the following steps: the
+ * body particles (initial type SPH_TYPE_BODY) are translated by vel * dt at the
+ * start of every step, their ghosts take vel, and acc enters the pressure
+ * extrapolation onto them.  A host with a non-constant motion calls this before
+ * every sph_step(h, 1, ...). */
+int sph_set_body_motion(sph_handle* h, const double vel[2], const double acc[2]);
+
+/* Real_physical_time of the next step's start, before its dt increment
+ * (SPH_Time_Iteration.f90:71-72); sph_set_state resets it to 0. */
+int sph_set_time(sph_handle* h, double t);
 
 /* Download the host particles (same order as set_state).  press is the
  * equation of state evaluated at the returned density.  Any pointer may be NULL. */

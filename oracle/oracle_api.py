@@ -57,6 +57,7 @@ def load():
     lib.oracle_body_force.argtypes = [ctypes.c_void_p, dp]
     lib.oracle_rhs_body_force.argtypes = [cp, ctypes.c_int, dp, dp, dp, dp, ip, ip, dp]
     lib.oracle_mls_reinit.argtypes = [cp, ctypes.c_int, dp, dp, dp, ip, dp]
+    lib.oracle_set_ghost_state.argtypes = [ctypes.c_int, ip, dp, dp, ctypes.c_double]
     lib.oracle_tangent.argtypes = [cp, ctypes.c_int, dp, dp, dp, dp, ip, dp, dp, dp, ctypes.c_double, ctypes.c_int,
                                    ctypes.c_double, ctypes.c_int, dp, dp, dp, dp, dp]
     _lib = lib
@@ -216,3 +217,12 @@ def mls_reinit(cfg: SphConfig, pos, rho, mass, type_):
     if rc != 0:
         raise RuntimeError("oracle_mls_reinit failed")
     return out
+
+
+def set_ghost_state(labels, body_vel=(0.0, 0.0), body_acc=(0.0, 0.0), t: float = 0.0):
+    """Wall labels, body velocity / acceleration and physical time for the
+    oracle's ghost assignment (used when the configuration has ghost_assign = 1)."""
+    lb = np.ascontiguousarray(labels, np.int32)
+    bv = np.ascontiguousarray(body_vel, np.float64)
+    ba = np.ascontiguousarray(body_acc, np.float64)
+    load().oracle_set_ghost_state(lb.shape[0], _p(lb, ctypes.c_int), _p(bv), _p(ba), float(t))

@@ -914,8 +914,99 @@ void body_force(const Particles& P, const Rhs& R, double out[6]) {
     }
 }
 
+// Ghost-assignment inputs of the moving-square driver: the wall labels
+// (Boundary_particle_type, host index order), the body's Custom_velocity and
+// Custom_accleration, and Real_physical_time.
+std::vector<int> g_labels;
+double g_bvel[2] = {0.0, 0.0}, g_bacc[2] = {0.0, 0.0};
+double g_time = 0.0;
+int g_n_host = 0;
+
+// Assign_boundary_particles, fixed-ghost part (Moving_Square.../Assign_boundary_particles.f90:
+// 611-941) with MLS_order_Boundary = 1: Fai_j = W_j V_j / sum W V over the
+// non-ghost particles within kernel_scale * 1.2 h; pressure, velocity and mass
+// interpolated (pressure with the gravity / body-acceleration term), body ghosts
+// take the body velocity, wall ghosts the characteristic-variable branch during
+// the shock release time (labels -6, -7; other labels keep the zero pressure
+// they start from) and the mirrored velocity; then the density from the
+// linear equation of state, or the rest state without neighbours.
+void assign_ghosts(Particles& P, Rhs& R) {
+    const sph_config& C = g_cfg;
+    const bool q = C.reference_literals != 0;
+    const double hg = (q ? (double)(float)C.ghost_h_factor : C.ghost_h_factor) * C.h;
+    const double rg = C.kernel_scale * hg;
+    const int n_host = std::min(g_n_host, P.n);
+    // every ghost reads only non-ghost particles, so the order of assignment is free
+    for (int i = 0; i < n_host; ++i) {
+        if (P.type[i] != SPH_TYPE_FIX_GHOST) continue;
+        const bool body = P.itype[i] == SPH_TYPE_BODY;
+        const double ge[2] = {C.gravity[0] + (body ? g_bacc[0] : 0.0), C.gravity[1] + (body ? g_bacc[1] : 0.0)};
+        std::vector<int> nb;
+        std::vector<double> W;
+        for (int j = 0; j < P.n; ++j) {
+            if (P.type[j] == SPH_TYPE_FIX_GHOST || P.type[j] == SPH_TYPE_ILL || P.type[j] == 0) continue;
+            double pd[2] = {P.x[i] - P.x[j], P.y[i] - P.y[j]};
+            const double d = std::sqrt(pd[0] * pd[0] + pd[1] * pd[1]);
+            if (!(d <= rg)) continue;
+            double w, dw[2];
+            kernel(d, pd, hg, w, dw);
+            nb.push_back(j);
+            W.push_back(w * P.mass[j] / P.rho[j]);
+        }
+        double pint = 0.0, uint = 0.0, vint = 0.0, m = 0.0;
+        if (nb.size() >= 3) {
+            double A = 0.0;
+            for (double w : W) A += w;
+            const double ainv = 1.0 / A;
+            for (size_t k = 0; k < nb.size(); ++k) {
+                const int j = nb[k];
+                const double fai = ainv * W[k];
+                const double pd0 = P.x[i] - P.x[j], pd1 = P.y[i] - P.y[j];
+                pint = pint + R.p[j] * fai + P.rho[j] * fai * (ge[0] * pd0 + ge[1] * pd1);
+                uint = uint + P.u[j] * fai;
+                vint = vint + P.v[j] * fai;
+                m = m + P.mass[j] * fai;
+            }
+        }
+        double u, v, p = 0.0;
+        const int lab = i < (int)g_labels.size() ? g_labels[i] : 0;
+        if (body) {
+            u = g_bvel[0]; v = g_bvel[1]; p = pint;
+        } else {
+            if (0.0 < g_time && g_time <= C.shock_release_time) {
+                const double ri = (pint - C.background_p) / C.c0sq + C.rho0;
+                const double c = g_K.sqrt_c0 * pw3(ri / C.rho0);
+                u = uint; v = vint;
+                if (lab == -6) {
+                    const double J2 = ri * c * (vint - 0.0) + (pint - 0.0), J3 = -ri * c * (vint - 0.0) + (pint - 0.0);
+                    v = 0.0 + (J2 - J3) / (2 * ri * c);
+                    p = 0.0 + 0.5 * (J2 + J3);
+                } else if (lab == -7) {
+                    const double J2 = ri * c * (uint - 0.0) + (pint - 0.0), J3 = -ri * c * (uint - 0.0) + (pint - 0.0);
+                    u = 0.0 + (J2 - J3) / (2 * ri * c);
+                    p = 0.0 + 0.5 * (J2 + J3);
+                }
+            } else {
+                u = uint; v = vint; p = pint;
+            }
+            if (lab == -6) { if (C.wall_bc == 1) v = -v; else { u = -u; v = -v; } }
+            else if (lab == -7) { u = -u; v = -v; }
+            else if (lab == -8) { if (C.wall_bc == 1) u = -u; else { u = -u; v = -v; } }
+        }
+        double rho, c;
+        if (m != 0.0) {
+            rho = (p - C.background_p) / C.c0sq + C.rho0;
+            c = g_K.sqrt_c0 * pw3(rho / C.rho0);
+        } else {
+            u = 0.0; v = 0.0; p = 0.0; rho = C.rho0; m = 0.0; c = g_K.sqrt_c0;
+        }
+        P.u[i] = u; P.v[i] = v; P.rho[i] = rho; P.mass[i] = m; P.smass[i] = m;
+        R.p[i] = p; R.c[i] = c; R.vol[i] = m / rho;
+    }
+}
+
 // single_step_compute (Taylor_Green_Vortex/single_step_compute.f90:62-171).
-void single_step_compute(const Particles& P, Rhs& R) {
+void single_step_compute(Particles& P, Rhs& R) {
     const int n = P.n;
     R.p.assign(n, 0.0); R.c.assign(n, 0.0); R.vol.assign(n, 0.0);
     for (int i = 0; i < n; ++i) {
@@ -923,6 +1014,7 @@ void single_step_compute(const Particles& P, Rhs& R) {
         eos(P.rho[i], R.p[i], R.c[i]);
     }
     for (int i = 0; i < n; ++i) R.vol[i] = P.mass[i] / P.rho[i];   // Assign_boundary_particles.f90:303-308
+    if (g_cfg.ghost_assign) assign_ghosts(P, R);    // MS Single_step_compute.f90:73
     build_grid(P, R.G);
     R.L = PairList();
     find_pairs(P, R.G, R.L);
@@ -1161,8 +1253,19 @@ struct Sim {
 // Euler predictor-corrector of Moving_Square.../SPH_Time_Iteration.f90:304-334
 // (Iteration_Method 2): one RHS per step after the first, rates of the last RHS
 // reused for the predictor.
+// Real_time = Real_time + dt and Body_Motion_Solver at the start of a step
+// (MS SPH_Time_Iteration.f90:71-114): the body moves with Custom_velocity.
+void advance_time_and_body(Sim& S, double dt) {
+    g_time += dt;
+    g_n_host = S.H.n;
+    if (!g_cfg.ghost_assign) return;
+    for (int i = 0; i < S.H.n; ++i)
+        if (S.H.itype[i] == SPH_TYPE_BODY) { S.H.x[i] += g_bvel[0] * dt; S.H.y[i] += g_bvel[1] * dt; }
+}
+
 void run_step_euler_pc(Sim& S, double dt) {
     const int n = S.H.n;
+    advance_time_and_body(S, dt);
     if (g_cfg.periodic) wrap_periodic(S.H);
     Particles P;
     if (g_cfg.periodic) periodic_images(S.H, P);
@@ -1218,6 +1321,7 @@ void run_step_euler_pc(Sim& S, double dt) {
 // updates :942-1047, then Shift_particle_position with the last RHS pair data.
 void run_step(Sim& S, double dt) {
     const int n = S.H.n;
+    advance_time_and_body(S, dt);
     if (g_cfg.periodic) wrap_periodic(S.H);
     Particles P;
     if (g_cfg.periodic) periodic_images(S.H, P);
@@ -1337,6 +1441,15 @@ int oracle_mls_reinit(const sph_config* cfg, int n, const double* pos, const dou
     mls_reinit(P, n);
     for (int i = 0; i < n; ++i) rho_out[i] = P.rho[i];
     return 0;
+}
+
+// Inputs of the ghost assignment for the following oracle calls.
+void oracle_set_ghost_state(int n, const int* labels, const double* bvel, const double* bacc, double t) {
+    g_labels.assign(labels ? labels : nullptr, labels ? labels + n : nullptr);
+    if (!labels) g_labels.assign(n, 0);
+    for (int k = 0; k < 2; ++k) { g_bvel[k] = bvel ? bvel[k] : 0.0; g_bacc[k] = bacc ? bacc[k] : 0.0; }
+    g_time = t;
+    g_n_host = n;
 }
 
 int oracle_threads(int nthreads) {

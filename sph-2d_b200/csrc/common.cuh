@@ -25,6 +25,9 @@ struct Params {
     int ms, hllc, laplacian, free_surface, integrator, has_body;
     int mls_order, mls_every;     // density re-initialisation (0: off)
     double mls_alpha3;            // alpha^3 added to the moment matrix diagonal
+    // ghost assignment (moving-square driver)
+    int ghost_assign, wall_bc, ghost_cells;
+    double ghost_h, ghost_r, ghost_kf, shock_t, grav[2];
     // kernel / pair search
     double h, r_cut, cut_min, kfactor, gauss_e9, q_zero;
     double r2_list;          // squared neighbour-list radius (support * (1 + skin))

@@ -16,6 +16,7 @@ struct Staging {
     double* smass;    // mass the SPS force multiplies with (quirk A.6), default = mass
     int* type;
     int* itype;       // initial type (body force), images get SPH_TYPE_PERIODIC
+    int* blabel;      // wall label of the ghost assignment (host particles)
     // rates of the last RHS of the previous step (the reused K1), host particles only
     double* r_drho;
     double2* r_acc;
@@ -116,6 +117,7 @@ struct Sorted {
     int* id;          // id-order index (host index, or n_host + image number)
     int* type;
     int* itype;       // initial type (SPH_TYPE_BODY marks the body)
+    int* blabel;      // wall label of the ghost assignment (0 for images)
     double2* pos;     // current stage position (FP64)
     double2* pos0;    // step-start (master) position, also the list-build position
     double2* vel0;    // step-start velocity (FP64 master)
@@ -187,6 +189,7 @@ __global__ void k_gather_sorted(Params P, Staging S, Sorted<R> D, const unsigned
     D.id[s] = i;
     D.type[s] = S.type[i];
     D.itype[s] = S.itype[i];
+    D.blabel[s] = i < P.n_host ? S.blabel[i] : 0;
     double2 x = S.pos[i];
     D.pos[s] = x;
     D.pos0[s] = x;

@@ -102,6 +102,9 @@ struct sph_handle {
     bool bf_every_rhs = false;            // sph_rhs also reports it
     struct AdjCtx* adj = nullptr;         // saved context of sph_adjoint_forward
     double* d_mls = nullptr;              // re-initialised densities [cap_tot]
+    double t_phys = 0.0;                  // Real_physical_time (ghost assignment)
+    double body_vel[2] = {0.0, 0.0};      // Custom_velocity
+    double body_acc[2] = {0.0, 0.0};      // Custom_accleration
 };
 
 namespace {
@@ -119,6 +122,8 @@ int derive_params(const sph_config& c, Params& P) {
     if (c.shift_n != 4) return SPH_E_CONFIG;
     if (c.mls_order != 0 && c.mls_order != 3 && c.mls_order != 6) return SPH_E_CONFIG;
     if (c.mls_order != 0 && (c.mls_every < 1 || !(c.mls_alpha >= 0))) return SPH_E_CONFIG;
+    if (c.ghost_assign != 0 && c.ghost_assign != 1) return SPH_E_CONFIG;
+    if (c.ghost_assign && (!(c.ghost_h_factor > 0) || (c.wall_bc != 0 && c.wall_bc != 1))) return SPH_E_CONFIG;
     memset(&P, 0, sizeof(P));
     const bool q = c.reference_literals != 0;
     P.kernel_model = c.kernel_model;
@@ -202,6 +207,21 @@ int derive_params(const sph_config& c, Params& P) {
     int mn = (int)ceil(2.0 * lat) + 16;
     mn = (mn + 3) & ~3;
     P.max_nbr = std::min(mn, 256);
+    // ghost assignment: average_smooth_length = 1.2*smooth_length (a default-real
+    // literal under reference_literals), support kernel_scale times that, cells
+    // covering it plus the half skin the neighbours may move within a step
+    P.ghost_assign = c.ghost_assign;
+    P.wall_bc = c.wall_bc;
+    P.ghost_h = (q ? (double)(float)c.ghost_h_factor : c.ghost_h_factor) * c.h;
+    P.ghost_r = c.kernel_scale * P.ghost_h;
+    P.ghost_kf = c.kernel_model == SPH_KERNEL_GAUSSIAN
+                     ? 1.0 / (pi_k * (P.ghost_h * P.ghost_h) * (q ? (double)(1.0f - 10.0f * expf(-9.0f))
+                                                                  : 1.0 - 10.0 * exp(-9.0)))
+                     : 7.0 / (4 * pi_k * (P.ghost_h * P.ghost_h));
+    P.ghost_cells = c.ghost_assign ? (int)ceil((P.ghost_r + 0.5 * skin) / P.cs) : 1;
+    P.shock_t = c.shock_release_time;
+    P.grav[0] = c.gravity[0];
+    P.grav[1] = c.gravity[1];
     return SPH_OK;
 }
 
@@ -246,7 +266,7 @@ template <> Sorted<float>& sorted<float>(sph_handle* h) { return h->D32; }
 
 template <typename R>
 int alloc_sorted(Sorted<R>& D, int cap, int max_nbr, int ncells) {
-    CK(dalloc(&D.id, cap)); CK(dalloc(&D.type, cap)); CK(dalloc(&D.itype, cap));
+    CK(dalloc(&D.id, cap)); CK(dalloc(&D.type, cap)); CK(dalloc(&D.itype, cap)); CK(dalloc(&D.blabel, cap));
     CK(dalloc(&D.pos, cap)); CK(dalloc(&D.pos0, cap)); CK(dalloc(&D.vel0, cap)); CK(dalloc(&D.rho0, cap));
     CK(dalloc(&D.mass, cap)); CK(dalloc(&D.smass, cap));
     CK(dalloc(&D.kin, cap)); CK(dalloc(&D.aux, cap));
@@ -269,7 +289,7 @@ int alloc_sorted(Sorted<R>& D, int cap, int max_nbr, int ncells) {
 
 template <typename R>
 void free_sorted(Sorted<R>& D) {
-    void* ptrs[] = {D.id, D.type, D.itype, D.pos, D.pos0, D.vel0, D.rho0, D.mass, D.smass, D.kin, D.aux, D.nb1, D.nb2, D.nb3,
+    void* ptrs[] = {D.id, D.type, D.itype, D.blabel, D.pos, D.pos0, D.vel0, D.rho0, D.mass, D.smass, D.kin, D.aux, D.nb1, D.nb2, D.nb3,
                     D.binv, D.binv64, D.fra_v, D.flags, D.drho, D.acc, D.avg, D.shift, D.ks_r, D.ks_a, D.ks_v, D.c_drho,
                     D.c_acc, D.c_avg, D.nbr, D.nnbr, D.pairs, D.npairs, D.cell_start, D.cell_end, D.kh, D.kl,
                     D.xhl, D.vol64};
@@ -368,6 +388,13 @@ int rhs(sph_handle* h, int last) {
     const Params& P = h->P;
     Sorted<R>& D = sorted<R>(h);
     const int nb = blocks(P.n_tot, 128);
+    if (P.ghost_assign) {
+        // Assign_boundary_particles at the start of single_step_compute (MS Single_step_compute.f90:73)
+        tic(h, PH_UPDATE);
+        k_assign_ghosts<R><<<nb, 128, 0, h->stream>>>(P, D, h->t_phys, h->body_vel[0], h->body_vel[1],
+                                                       h->body_acc[0], h->body_acc[1]);
+        h->launches += 1;
+    }
     tic(h, PH_A);
     k_pass_a<R><<<nb, 128, 0, h->stream>>>(P, D);
     tic(h, PH_SURF);
@@ -438,6 +465,17 @@ int reinit_density(sph_handle* h, int do_shift) {
 template <typename R>
 int run_steps(sph_handle* h, int nsteps, double dt) {
     for (int s = 0; s < nsteps; ++s) {
+        // Real_time = Real_time + dt, then Body_Motion_Solver (MS SPH_Time_Iteration.f90:71-114)
+        h->t_phys += dt;
+        if (h->P.ghost_assign && (h->body_vel[0] != 0.0 || h->body_vel[1] != 0.0)) {
+            int rc = unsort<R>(h);
+            if (rc) return rc;
+            k_translate_body<<<blocks(h->n_host, 256), 256, 0, h->stream>>>(h->n_host, h->S.itype, h->S.pos,
+                                                                              h->body_vel[0] * dt, h->body_vel[1] * dt);
+            CK(cudaGetLastError());
+            h->launches += 1;
+            h->sorted_valid = false;
+        }
         int rc = prepare<R>(h);
         if (rc) return rc;
         const int first = h->step_count == 0;
@@ -894,7 +932,7 @@ void destroy(sph_handle* h) {
     free_sorted(h->D64);
     free_sorted(h->D32);
     if (h->adj) { adj_free_all(h->adj); delete h->adj; }
-    void* ptrs[] = {h->S.pos, h->S.vel, h->S.rho, h->S.mass, h->S.smass, h->S.type, h->S.itype, h->d_bf,
+    void* ptrs[] = {h->S.pos, h->S.vel, h->S.rho, h->S.mass, h->S.smass, h->S.type, h->S.itype, h->S.blabel, h->d_bf,
                     h->S.r_drho, h->S.r_acc,
                     h->S.r_avg, h->S.cnt, h->S.off, h->S.lr_cnt, h->S.lr_off, h->S.tb_cnt, h->S.tb_off, h->keys_in, h->keys_out, h->vals_in, h->vals_out, h->cub_tmp,
                     h->d_status, h->d_int, h->d_part, h->d_diag, h->d_xfer, h->d_export, h->d_off64, h->d_cnt_id,
@@ -935,6 +973,7 @@ int init_impl(const sph_config* cfg, int n_capacity, sph_handle** out) {
     CK(dalloc(&h->S.pos, cap)); CK(dalloc(&h->S.vel, cap)); CK(dalloc(&h->S.rho, cap));
     CK(dalloc(&h->S.mass, cap)); CK(dalloc(&h->S.smass, cap)); CK(dalloc(&h->S.type, cap));
     CK(dalloc(&h->S.itype, cap));
+    CK(dalloc(&h->S.blabel, cap)); CK(cudaMemset(h->S.blabel, 0, sizeof(int) * (size_t)cap));
     CK(dalloc(&h->d_bf, (size_t)6 * blocks(cap, kRedThreads) + 6));
     CK(dalloc(&h->S.r_drho, h->cap_host)); CK(dalloc(&h->S.r_acc, h->cap_host)); CK(dalloc(&h->S.r_avg, h->cap_host));
     CK(dalloc(&h->S.cnt, cap)); CK(dalloc(&h->S.off, cap));
@@ -1055,6 +1094,9 @@ int sph_set_state(sph_handle* h, int n, const double* pos, const double* vel, co
     h->sorted_valid = false;
     h->have_rhs = false;
     h->step_count = 0;
+    h->t_phys = 0.0;
+    CK(cudaMemsetAsync(h->S.blabel, 0, sizeof(int) * (size_t)n, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
     return SPH_OK;
 }
 
@@ -1086,6 +1128,31 @@ int sph_set_initial_type(sph_handle* h, int n, const int* initial_type) {
     for (int i = 0; i < n; ++i) body |= initial_type[i] == SPH_TYPE_BODY;
     h->P.has_body = body;
     h->sorted_valid = false;
+    return SPH_OK;
+}
+
+int sph_set_boundary_labels(sph_handle* h, int n, const int* labels) {
+    if (!h || n != h->n_host || n <= 0 || !labels) return SPH_E_ARG;
+    for (int i = 0; i < n; ++i)
+        if (labels[i] == -9) return SPH_E_CONFIG;     // radius free slip: not built
+    CK(cudaSetDevice(h->device));
+    int rc = h->mixed ? unsort<float>(h) : unsort<double>(h);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(h->S.blabel, labels, sizeof(int) * n, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->sorted_valid = false;
+    return SPH_OK;
+}
+
+int sph_set_body_motion(sph_handle* h, const double vel[2], const double acc[2]) {
+    if (!h || !vel || !acc) return SPH_E_ARG;
+    for (int k = 0; k < 2; ++k) { h->body_vel[k] = vel[k]; h->body_acc[k] = acc[k]; }
+    return SPH_OK;
+}
+
+int sph_set_time(sph_handle* h, double t) {
+    if (!h) return SPH_E_ARG;
+    h->t_phys = t;
     return SPH_OK;
 }
 

@@ -49,7 +49,7 @@ __global__ void k_stage(Params P, Sorted<R> D, int stage, double dt, int use_car
     const double2 v0 = D.vel0[s];
     const double r0 = D.rho0[s];
     double dr, ax, ay, gx, gy;
-    if (stage == 0 && use_carried) {
+    if ((stage == 0 || stage == 10) && use_carried) {   // the first stage of either driver
         dr = (double)D.c_drho[s]; V2 a = D.c_acc[s], g = D.c_avg[s];
         ax = (double)a.x; ay = (double)a.y; gx = (double)g.x; gy = (double)g.y;
     } else {
@@ -268,6 +268,118 @@ __global__ void k_finish_mls(Params P, Sorted<R> D, const double* rho_new, int d
     D.kin[s] = make_double4(v.x, v.y, rho, p);
     D.aux[s] = mk4<R>((R)m, (R)(m / rho), (R)c, (R)D.smass[s]);
     store_split(D, s, make_double2(x, y), make_double4(v.x, v.y, rho, p));
+}
+
+// Body_Motion_Solver (Moving_Square.../Body_Motion_Solver.f90:187-193): the body
+// particles (initial type SPH_TYPE_BODY) move by the step's displacement.
+__global__ void k_translate_body(int n, const int* itype, double2* pos, double dx, double dy) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || itype[i] != SPH_TYPE_BODY) return;
+    const double2 x = pos[i];
+    pos[i] = make_double2(x.x + dx, x.y + dy);
+}
+
+// Fixed-ghost assignment of the moving-square driver (Moving_Square.../
+// Assign_boundary_particles.f90:611-941, with MLS_order_Boundary = 1, i.e.
+// Shepard weights Fai_j = W_j V_j / sum W V), at the start of every RHS, from the
+// current state of the non-ghost particles within kernel_scale * 1.2 h:
+//   p = sum Fai (p_j + rho_j g.(x - x_j)),  u = sum Fai u_j,  m = sum Fai m_j
+// (g: gravity, plus the body acceleration for body ghosts), at least 3
+// neighbours or nothing.  Body ghosts take the body velocity; wall ghosts, during
+// 0 < t <= Shock_wave_release_time, go through the characteristic variables for
+// labels -6 / -7 (which return the interpolated values) and keep the zero
+// pressure they start from for other labels, as the reference's branch does;
+// then the wall velocity is mirrored by label and wall condition.  Finally
+// rho = (p - pb)/c0^2 + rho0, or the rest state when m = 0.
+template <typename R>
+__global__ void k_assign_ghosts(Params P, Sorted<R> D, double t, double bvx, double bvy, double bax, double bay) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= P.n_tot) return;
+    if (D.type[s] != SPH_TYPE_FIX_GHOST || D.id[s] >= P.n_host) return;
+    const double2 x = D.pos[s];
+    const bool body = D.itype[s] == SPH_TYPE_BODY;
+    const double gxe = P.grav[0] + (body ? bax : 0.0), gye = P.grav[1] + (body ? bay : 0.0);
+    const int cx = (int)floor((x.x - P.gx0) / P.cs), cy = (int)floor((x.y - P.gy0) / P.cs);
+    double sw = 0.0, sp = 0.0, su = 0.0, sv = 0.0, sm = 0.0;
+    int cnt = 0;
+    const double hg = P.ghost_h;
+    for (int gy = max(cy - P.ghost_cells, 0); gy <= min(cy + P.ghost_cells, P.gny - 1); ++gy) {
+        const int row = gy * P.gnx;
+        for (int gx = max(cx - P.ghost_cells, 0); gx <= min(cx + P.ghost_cells, P.gnx - 1); ++gx) {
+            const int b0 = D.cell_start[row + gx];
+            if (b0 < 0) continue;
+            const int b1 = D.cell_end[row + gx];
+            for (int b = b0; b < b1; ++b) {
+                if (D.type[b] == SPH_TYPE_FIX_GHOST) continue;     // no other boundary particles
+                const double2 xb = D.pos[b];
+                const double dx = x.x - xb.x, dy = x.y - xb.y;
+                const double d = sqrt(dx * dx + dy * dy);
+                if (!(d <= P.ghost_r)) continue;
+                const double q = d / hg;
+                double w;
+                if (P.kernel_model == SPH_KERNEL_GAUSSIAN) {
+                    w = (exp(-(q * q)) - P.gauss_e9) * P.ghost_kf;
+                } else {
+                    const double tq = 1.0 - q / 2.0;
+                    const double t2 = tq * tq;
+                    w = P.ghost_kf * (1.0 + 2.0 * q) * (t2 * t2);
+                }
+                const double4 kb = D.kin[b];
+                const double mb = D.mass[b];
+                const double W = w * (mb / kb.z);
+                sw += W;
+                sp += kb.w * W + kb.z * W * (gxe * dx + gye * dy);
+                su += kb.x * W;
+                sv += kb.y * W;
+                sm += mb * W;
+                ++cnt;
+            }
+        }
+    }
+    double uint = 0.0, vint = 0.0, pint = 0.0, m = 0.0;
+    if (cnt >= 3) {
+        const double inv = 1.0 / sw;
+        pint = sp * inv; uint = su * inv; vint = sv * inv; m = sm * inv;
+    }
+    double u, v, p = 0.0;
+    if (body) {
+        u = bvx; v = bvy; p = pint;
+    } else {
+        const int lab = D.blabel[s];
+        if (0.0 < t && t <= P.shock_t) {
+            const double ri = (pint - P.pb) / P.c0sq + P.rho0;
+            const double r = ri / P.rho0;
+            const double c = P.sqrt_c0 * (r * r * r);
+            u = uint; v = vint;
+            if (lab == -6 || lab == -7) {
+                const double vn = lab == -6 ? vint : uint;
+                const double J2 = ri * c * vn + pint, J3 = -ri * c * vn + pint;
+                const double vs = (J2 - J3) / (2 * ri * c);
+                if (lab == -6) v = vs; else u = vs;
+                p = 0.5 * (J2 + J3);
+            }
+        } else {
+            u = uint; v = vint; p = pint;
+        }
+        if (lab == -6) { if (P.wall_bc == 1) v = -v; else { u = -u; v = -v; } }
+        else if (lab == -7) { u = -u; v = -v; }
+        else if (lab == -8) { if (P.wall_bc == 1) u = -u; else { u = -u; v = -v; } }
+    }
+    double rho, c;
+    if (m != 0.0) {
+        rho = (p - P.pb) / P.c0sq + P.rho0;
+        const double r = rho / P.rho0;
+        c = P.sqrt_c0 * (r * r * r);
+    } else {
+        u = 0.0; v = 0.0; p = 0.0; rho = P.rho0; m = 0.0; c = P.sqrt_c0;
+    }
+    D.mass[s] = m;
+    D.smass[s] = m;
+    D.vel0[s] = make_double2(u, v);
+    D.rho0[s] = rho;
+    D.kin[s] = make_double4(u, v, rho, p);
+    D.aux[s] = mk4<R>((R)m, (R)(m / rho), (R)c, (R)m);
+    store_split(D, s, x, make_double4(u, v, rho, p));
 }
 
 // Kinetic energy and max |v| of the water host particles

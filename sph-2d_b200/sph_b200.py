@@ -60,6 +60,7 @@ EXPORTED_SYMBOLS = (
     "sph_rhs", "sph_step", "sph_diagnostics", "sph_get_timings", "sph_reset_timings",
     "sph_strerror", "sph_get_field", "sph_update_state", "sph_find_particle_pair_noalloc",
     "sph_set_initial_type", "sph_adjoint_forward", "sph_adjoint_backward",
+    "sph_set_boundary_labels", "sph_set_body_motion", "sph_set_time",
 )
 
 
@@ -79,6 +80,8 @@ class SphConfig(ctypes.Structure):
         ("grid_lo", ctypes.c_double * 2), ("grid_hi", ctypes.c_double * 2),
         ("cell_skin", ctypes.c_double), ("laplacian", ctypes.c_int), ("free_surface", ctypes.c_int),
         ("mls_order", ctypes.c_int), ("mls_every", ctypes.c_int), ("mls_alpha", ctypes.c_double),
+        ("ghost_assign", ctypes.c_int), ("wall_bc", ctypes.c_int), ("ghost_h_factor", ctypes.c_double),
+        ("shock_release_time", ctypes.c_double), ("gravity", ctypes.c_double * 2),
     ]
 
     def copy(self) -> "SphConfig":
@@ -267,6 +270,9 @@ def load(path: str = LIB_PATH):
     lib.sph_get_timings.argtypes = [P, ctypes.POINTER(SphTimings)]
     lib.sph_reset_timings.argtypes = [P]
     lib.sph_get_field.argtypes = [P, ctypes.c_int, dp]
+    lib.sph_set_boundary_labels.argtypes = [P, ctypes.c_int, ip]
+    lib.sph_set_body_motion.argtypes = [P, dp, dp]
+    lib.sph_set_time.argtypes = [P, ctypes.c_double]
     lib.sph_adjoint_forward.argtypes = [P, ctypes.POINTER(SphAdjConfig), dp]
     lib.sph_adjoint_backward.argtypes = [P, ctypes.c_double, dp, dp, dp, dp]
     lib.sph_find_particle_pair_noalloc.argtypes = [ctypes.POINTER(SphConfig), ctypes.c_int, ctypes.c_void_p,
@@ -352,6 +358,20 @@ class Simulation:
         """subdomain_particle_initial_type (SPH_TYPE_BODY marks the body for the body force)."""
         it = np.ascontiguousarray(itype, dtype=np.int32)
         _check(self.lib.sph_set_initial_type(self.h, self.n, _ptr(it, ctypes.c_int)), "sph_set_initial_type")
+
+    def set_boundary_labels(self, labels):
+        """subdomain_Boundary_particle_type (-6 horizontal wall, -7 corner, -8 vertical wall, 0 other)."""
+        lb = np.ascontiguousarray(labels, dtype=np.int32)
+        _check(self.lib.sph_set_boundary_labels(self.h, self.n, _ptr(lb, ctypes.c_int)), "sph_set_boundary_labels")
+
+    def set_body_motion(self, vel, acc=(0.0, 0.0)):
+        """Custom_velocity / Custom_accleration of the body for the following steps."""
+        v = np.ascontiguousarray(vel, np.float64)
+        a = np.ascontiguousarray(acc, np.float64)
+        _check(self.lib.sph_set_body_motion(self.h, _ptr(v), _ptr(a)), "sph_set_body_motion")
+
+    def set_time(self, t: float):
+        _check(self.lib.sph_set_time(self.h, float(t)), "sph_set_time")
 
     def get_state(self):
         n = self.n
@@ -531,7 +551,31 @@ def moving_square_config(dx: float, lx: float, ly: float, solver: int = SOLVER_M
     # Reinitialize_particle_density: linear MLS every 40 steps (:662-671),
     # Slighted_modified_alpha = 1e-5 (:782)
     c.mls_order, c.mls_every, c.mls_alpha = 3, 40, 1.0e-5
+    # Assign_boundary_particles parameters: no slip (ExternalBoundaryCondition 0, :301),
+    # average smoothing length 1.2 h, Shock_wave_release_time 10 (:715), no gravity.
+    # ghost_assign = 0: the ghost states are the caller's (set ghost_assign = 1, the
+    # labels and the body motion to let the library assign them every RHS).
+    c.ghost_assign, c.wall_bc, c.ghost_h_factor, c.shock_release_time = 0, 0, 1.2, 10.0
+    c.gravity[:] = [0.0, 0.0]
     return c
+
+
+def moving_square_labels(case, itype) -> np.ndarray:
+    """subdomain_Boundary_particle_type of a make_moving_square layout: wall ghosts
+    below/above the tank within 0 <= x <= lx are horizontal (-6), left/right of it
+    within 0 <= y <= ly vertical (-8), the corner blocks -7 (Initial_Particle_From_First_Step.f90:
+    220-300); water and body particles 0 (the body's ghosts take its velocity)."""
+    n = case.n
+    x, y = case.pos[:n], case.pos[n:]
+    lx, ly = case.cfg.box_hi[0], case.cfg.box_hi[1]
+    lab = np.zeros(n, np.int32)
+    wall = (case.type == TYPE_FIX_GHOST) & (np.asarray(itype) != TYPE_BODY)
+    inx = (x >= 0.0) & (x <= lx)
+    iny = (y >= 0.0) & (y <= ly)
+    lab[wall & inx] = -6
+    lab[wall & ~inx & iny] = -8
+    lab[wall & ~inx & ~iny] = -7
+    return lab
 
 
 def make_moving_square(dx: float = 0.05, lx: float = 4.0, ly: float = 2.0, D: float = 0.5, U: float = 1.0,
