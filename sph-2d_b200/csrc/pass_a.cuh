@@ -18,16 +18,24 @@
 
 namespace sph {
 
-template <typename R>
+// HLREC: in the mixed path, read the hi/lo float records (position, u, v, rho, p)
+// instead of the FP64 ones and form the pair differences in FP32 from them
+// (see store_split); the adjoint, which runs this pass on stored stage states
+// that carry only the FP64 records, uses HLREC = false.
+template <typename R, bool HLREC>
 __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 6 : 4) k_pass_a(Params P, Sorted<R> D) {
     using V4 = typename VT<R>::V4;
     constexpr bool F32 = sizeof(R) == 4;
+    constexpr bool HL = HLREC && F32;
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= P.n_tot) return;
     const int ta = D.type[a];
     const int nn = D.nnbr[a];
-    const double2 xa = D.pos[a];
-    const double4 ka = D.kin[a];
+    const double2 xa = HL ? make_double2(0.0, 0.0) : D.pos[a];
+    const double4 ka = HL ? make_double4(0.0, 0.0, __ldg(&D.kin[a].z), 0.0) : D.kin[a];
+    const float4 xa_hl = HL ? D.xhl[a] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 kah = HL ? D.kh[a] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 kal = HL ? D.kl[a] : make_float4(0.f, 0.f, 0.f, 0.f);
     const double rho_a = ka.z;
     // the sums of this pass have no large cancellation (differences of smooth
     // fields, or B ~ I), so FP32 accumulates them directly in the mixed path
@@ -48,31 +56,32 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 6 : 4) k_pass_a(Params P
     unsigned ent_nn = nn > 1 ? __ldg(&D.nbr[(size_t)P.nbr_stride + a]) : 0u;
     double2 xb_n = make_double2(0.0, 0.0);
     double4 kb_n = make_double4(0.0, 0.0, 0.0, 0.0);
+    float4 xbhl_n = make_float4(0.f, 0.f, 0.f, 0.f), kbh_n = xbhl_n, kbl_n = xbhl_n;
     R vb_n = R(0);
-    if (nn > 0) {
-        const int b0 = (int)(ent_n & 0x7fffffffu);
-        xb_n = __ldg(&D.pos[b0]);
-        kb_n = D.kin[b0];
-        vb_n = D.aux[b0].y;
-    }
+    auto fetch = [&](int bb) {
+        if (HL) { xbhl_n = __ldg(&D.xhl[bb]); kbh_n = __ldg(&D.kh[bb]); kbl_n = __ldg(&D.kl[bb]); }
+        else { xb_n = __ldg(&D.pos[bb]); kb_n = D.kin[bb]; }
+        vb_n = D.aux[bb].y;
+    };
+    if (nn > 0) fetch((int)(ent_n & 0x7fffffffu));
     for (int e = 0; e < nn; ++e) {
         const unsigned ent = ent_n;
         const int b = (int)(ent & 0x7fffffffu);
         const double2 xb = xb_n;
         const double4 kb = kb_n;
+        const float4 xbhl = xbhl_n, kbh = kbh_n, kbl = kbl_n;
         const R Vb = vb_n;
         if (e + 1 < nn) {
             ent_n = ent_nn;
-            const int b1 = (int)(ent_n & 0x7fffffffu);
-            xb_n = __ldg(&D.pos[b1]);
-            kb_n = D.kin[b1];
-            vb_n = D.aux[b1].y;
+            fetch((int)(ent_n & 0x7fffffffu));
             if (e + 2 < nn) ent_nn = __ldg(&D.nbr[(size_t)(e + 2) * P.nbr_stride + a]);
         }
-        const double dxd = xa.x - xb.x, dyd = xa.y - xb.y;
+        const double dxd = HL ? 0.0 : xa.x - xb.x, dyd = HL ? 0.0 : xa.y - xb.y;
+        const float dxf = HL ? (xa_hl.x - xbhl.x) + (xa_hl.z - xbhl.z) : 0.f;
+        const float dyf = HL ? (xa_hl.y - xbhl.y) + (xa_hl.w - xbhl.w) : 0.f;
         R d, inv_d;
         if (F32) {
-            const R s = (R)(dxd * dxd + dyd * dyd);
+            const R s = HL ? (R)(dxf * dxf + dyf * dyf) : (R)(dxd * dxd + dyd * dyd);
             if (!(s <= r2cut) || s < r2min) continue;
             inv_d = rsqrtf(s);
             d = s * inv_d;
@@ -84,7 +93,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 6 : 4) k_pass_a(Params P
         }
         D.pairs[(size_t)np * P.nbr_stride + a] = ent;
         ++np;
-        const R dx = (R)dxd, dy = (R)dyd;
+        const R dx = HL ? (R)dxf : (R)dxd, dy = HL ? (R)dyf : (R)dyd;
         // grad_a W = g(d) (x_a - x_b)  (compute_kernel)
         R gs, wk;
         {
@@ -101,10 +110,23 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 6 : 4) k_pass_a(Params P
                 gs = kf * (R(-5) * q * t3) * inv_d * inv_h;
             }
         }
+        // differences of the records (b minus a): FP64, or hi/lo in FP32
+        R drho, du, dv, dp;
+        if (HL) {
+            drho = (R)((kbh.z - kah.z) + (kbl.z - kal.z));
+            du = (R)((kbh.x - kah.x) + (kbl.x - kal.x));
+            dv = (R)((kbh.y - kah.y) + (kbl.y - kal.y));
+            dp = (R)((kbh.w - kah.w) + (kbl.w - kal.w));
+        } else {
+            drho = (R)(kb.z - ka.z);
+            du = (R)(kb.x - ka.x); dv = (R)(kb.y - ka.y);
+            dp = (R)(kb.w - ka.w);
+        }
         if (P.ms) {
-            const R f = (R)P.eps * D.aux[b].x / (R)(ka.z + kb.z) * wk;
-            xs0 -= f * (R)(ka.x - kb.x);
-            xs1 -= f * (R)(ka.y - kb.y);
+            const R rsum = HL ? (R)(kah.z + kbh.z) : (R)(ka.z + kb.z);
+            const R f = (R)P.eps * D.aux[b].x / rsum * wk;
+            xs0 += f * du;
+            xs1 += f * dv;
         }
         const R gx = gs * dx * Vb, gy = gs * dy * Vb;    // V_b grad_a W
         // volume fraction (Define_freesurface...f90:84-85)
@@ -113,16 +135,10 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 6 : 4) k_pass_a(Params P
         b00 -= dx * gx; b01 -= dx * gy;
         b10 -= dy * gx; b11 -= dy * gy;
         // raw gradient sums (phi_b - phi_a) V_b grad_a W
-        // differences of the FP64 records, then FP32 arithmetic in the mixed path
-        const R drho = (R)(kb.z - ka.z);
         g[0] += drho * gx; g[1] += drho * gy;
-        const R du = (R)(kb.x - ka.x), dv = (R)(kb.y - ka.y);
         g[4] += du * gx; g[5] += du * gy;
         g[6] += dv * gx; g[7] += dv * gy;
-        if (P.muscl) {
-            const R dp = (R)(kb.w - ka.w);
-            g[2] += dp * gx; g[3] += dp * gy;
-        }
+        if (P.muscl) { g[2] += dp * gx; g[3] += dp * gy; }
     }
     D.npairs[a] = np;
     fra = fra * (R)(1.0 / P.sv);

@@ -396,7 +396,7 @@ int rhs(sph_handle* h, int last) {
         h->launches += 1;
     }
     tic(h, PH_A);
-    k_pass_a<R><<<nb, 128, 0, h->stream>>>(P, D);
+    k_pass_a<R, true><<<nb, 128, 0, h->stream>>>(P, D);
     tic(h, PH_SURF);
     k_surface<R><<<nb, 128, 0, h->stream>>>(P, D);
     k_near<R><<<nb, 128, 0, h->stream>>>(P, D);
@@ -805,7 +805,7 @@ int adj_rhs(sph_handle* h, const Sorted<R>& V, int k, int stage) {
     const int nb = blocks(P.n_tot, kAdjThreads);
     const int nbc = blocks((long long)P.n_tot * kAdjLanes, kAdjThreads);
     tic(h, PH_A);
-    k_pass_a<R><<<nb, 128, 0, h->stream>>>(P, V);
+    k_pass_a<R, false><<<nb, 128, 0, h->stream>>>(P, V);
     k_surface<R><<<nb, 128, 0, h->stream>>>(P, V);
     k_near<R><<<nb, 128, 0, h->stream>>>(P, V);
     tic(h, PH_ADJ);
