@@ -59,10 +59,8 @@ def parse():
 
 # ---------------------------------------------------------------------------
 def dist_env():
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return rank, world, local
+    import replicas
+    return replicas.dist_env()
 
 
 class Clocks:
@@ -155,17 +153,13 @@ def run_native(args, rank, world, local):
         torch.distributed.barrier()
     S.load()
 
+    import replicas
+
     def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(x, world, device=f"cuda:{local}")
 
     def barrier():
-        torch.cuda.synchronize()
-        if world > 1:
-            torch.distributed.barrier()
+        replicas.barrier(world, sync=torch.cuda.synchronize)
 
     n_side = args.n_side
     results = {}
@@ -200,8 +194,8 @@ def run_native(args, rank, world, local):
     fp64 = results[S.PREC_FP64]
     n = mixed["case"].n
     steps = args.steps
-    value = world * n * steps / (mixed["dev_ms"] / 1e3)
-    value64 = world * n * steps / (fp64["dev_ms"] / 1e3)
+    value = replicas.aggregate_rate(n * steps, world, mixed["dev_ms"] / 1e3)
+    value64 = replicas.aggregate_rate(n * steps, world, fp64["dev_ms"] / 1e3)
     tm = mixed["tm"]
 
     # ---- e2e through the C-ABI with pinned host buffers ---------------------
@@ -225,7 +219,7 @@ def run_native(args, rank, world, local):
         assert lib.sph_get_state(sim.h, n, P(pos_h), P(vel_h), P(rho_h), None) == 0
     barrier()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
-    e2e_value = world * n * e2e_steps / e2e_s
+    e2e_value = replicas.aggregate_rate(n * e2e_steps, world, e2e_s)
     h2d = 40 * n
     d2h = 40 * n
 
@@ -412,16 +406,13 @@ def main():
                 "wall_s": el}
         print(json.dumps(line))
         return 0
+    import replicas
     if world > 1:
         import torch
-        from datetime import timedelta
         torch.cuda.set_device(local)
-        torch.distributed.init_process_group("nccl", timeout=timedelta(seconds=120))
+    replicas.init(world, "nccl")
     out = run_native(args, rank, world, local)
-    if world > 1:
-        import torch
-        torch.distributed.barrier()
-        torch.distributed.destroy_process_group()
+    replicas.shutdown(world)
     if rank == 0 and out is not None:
         print(json.dumps(out))
     return 0
