@@ -274,13 +274,31 @@ int sph_find_particle_pair_noalloc(const sph_config* cfg, int n, const double* d
  * of the artificial-viscosity switch).  The handle's state after the backward
  * pass is the forward's final state.
  *
- * Supported configurations: the normalised modified linear Riemann
- * delta-SPH + SPS solver (SPH_SOLVER_MODLR_DELTA_SPS) with the RK4 driver,
- * either kernel, with or without renormalisation, without particle shifting
- * and without XSPH; other configurations return SPH_E_CONFIG.  The reverse
- * kernels compute in FP64 for both precisions of the forward step. */
+ * Supported configurations (others return SPH_E_CONFIG), either kernel, with
+ * or without renormalisation, without particle shifting and without MLS
+ * density re-initialisation:
+ *  - the normalised modified linear Riemann delta-SPH + SPS solver
+ *    (SPH_SOLVER_MODLR_DELTA_SPS) with the RK4 driver, without XSPH;
+ *  - the moving-square modified linear Riemann solver (SPH_SOLVER_MS_MODLR_DELTA,
+ *    Morris laplacian, XSPH velocities in the continuity flux) with the Euler
+ *    predictor-corrector driver, with the library's ghost assignment
+ *    (ghost_assign = 1: the reverse runs through the Shepard interpolation onto
+ *    the wall and body ghosts) or with caller-given ghost states.
+ * The reverse kernels compute in FP64 for both precisions of the forward step.
+ *
+ * Body motion: with body_motion set, step k of the forward run (k = 0 ..
+ * nsteps-1) moves the body with velocity (body_motion[4k], body_motion[4k+1])
+ * and acceleration (body_motion[4k+2], body_motion[4k+3]) (Custom_velocity and
+ * Custom_accleration of Body_Motion_Solver at time t0 + (k+1) dt); NULL keeps
+ * the handle's sph_set_body_motion values for every step.  After the backward
+ * pass sph_adjoint_motion_gradient returns dL/d(body_motion), from which the
+ * gradient with respect to any parametrisation of the motion (an amplitude,
+ * Fourier coefficients) follows by the chain rule on the host. */
 #define SPH_LOSS_VELOCITY_MISFIT 0  /* sum over water particles of |v - v_target|^2 */
 #define SPH_LOSS_KINETIC_ENERGY  1  /* sum over water particles of m |v|^2 / 2       */
+#define SPH_LOSS_DRAG            2  /* sum over the steps of dt * F_x, F = the total body force
+                                       of the step's last RHS (sph_diag.body_force[4]);
+                                       needs a body (sph_set_initial_type)             */
 #define SPH_ADJ_NPARAMS 1           /* g_params[0] = dL/dnu                          */
 
 typedef struct sph_adj_config {
@@ -290,6 +308,8 @@ typedef struct sph_adj_config {
     int reserved;
     double dt;
     const double* target_vel;  /* [2*n] column-major (u block, v block); copied; misfit only */
+    const double* body_motion; /* [4*nsteps] per-step body velocity and acceleration; copied;
+                                  NULL: the handle's constant body motion            */
 } sph_adj_config;
 
 int sph_adjoint_forward(sph_handle* h, const sph_adj_config* cfg, double* loss);
@@ -299,6 +319,11 @@ int sph_adjoint_forward(sph_handle* h, const sph_adj_config* cfg, double* loss);
  * forward context is held. */
 int sph_adjoint_backward(sph_handle* h, double dloss, double* g_vel0, double* g_rho0, double* g_pos0,
                          double* g_params);
+
+/* dL/d(body_motion) of the last backward pass, [4*nsteps] in the layout of
+ * sph_adj_config.body_motion (zero when the run has no body or no ghost
+ * assignment).  Returns SPH_E_ARG when no backward pass has completed. */
+int sph_adjoint_motion_gradient(sph_handle* h, double* g_motion);
 
 /* Human-readable message for a status code (static storage). */
 const char* sph_strerror(int code);

@@ -58,6 +58,15 @@ struct Adj {
     double* lrho;
     double* lk_r;
     double2* lk_a;
+    // moving-square path (Euler predictor-corrector, ghost assignment)
+    double2* lg[2];      // adjoint of the XSPH velocity of RHS k of the step
+    double2* lk_g;       // id order: of the carried XSPH velocity
+    double2* gavg;       // adjoint of avg from the pass C reverse
+    double* sm;          // adjoint of the mass of the state the reversed RHS was evaluated on
+    double4* glam;       // ghost Shepard multipliers (p, u, v, m) / sum W
+    double* glamw;       //   and of the normalisation
+    double* mo_part;     // per-block partials of the body-motion adjoints
+    double* g_motion;    // [4 nsteps] dL/d(body velocity, body acceleration) of each step
 };
 
 constexpr int kAdjThreads = 128;
@@ -77,6 +86,15 @@ __device__ __forceinline__ void kernel_g(const Params& P, double d, double& G, d
     }
 }
 
+// Kernel value W(d) of compute_kernel (its d-derivative is G(d) d).
+__device__ __forceinline__ double kernel_w(const Params& P, double d) {
+    const double q = d / P.h;
+    if (P.kernel_model == SPH_KERNEL_GAUSSIAN) return (exp(-(q * q)) - P.gauss_e9) * P.kfactor;
+    const double t = 1.0 - 0.5 * q;
+    const double t2 = t * t;
+    return P.kfactor * (1.0 + 2.0 * q) * (t2 * t2);
+}
+
 // dp/drho and dc/drho of eos64.
 __device__ __forceinline__ void eos_deriv(const Params& P, double rho, double& dp, double& dc) {
     const double r = rho / P.rho0;
@@ -91,11 +109,12 @@ struct PSide {
     double u, v, rho, p, c, V, m, sm;
     double t0, t1, t2;    // tau xx, xy, yy
     double g0, g1;        // grad rho
+    double ax, ay;        // XSPH average velocity (moving-square solver)
     double4 bi;           // B^-1
     bool water, near;
 };
 
-template <typename R>
+template <typename R, bool MS = false>
 __device__ __forceinline__ PSide load_side(const Sorted<R>& D, int s) {
     PSide o;
     o.x = D.pos[s];
@@ -112,6 +131,11 @@ __device__ __forceinline__ PSide load_side(const Sorted<R>& D, int s) {
     o.bi = D.binv64[s];
     o.water = D.type[s] == SPH_TYPE_WATER;
     o.near = (D.flags[s] & 2) != 0;
+    o.ax = o.ay = 0.0;
+    if (MS) {
+        const typename VT<R>::V2 g = D.avg[s];
+        o.ax = (double)g.x; o.ay = (double)g.y;
+    }
     return o;
 }
 
@@ -124,10 +148,15 @@ struct PBar {
     double t0, t1, t2, g0, g1;
     double bi0, bi1, bi2, bi3;
     double nu;
+    double avg0, avg1;    // of avg_a - avg_b (MS)
+    double mb;            // of m_b (explicit; V_b = m_b/rho_b is in Vb)
 };
 
 // Reverse of the contribution of b to particle a (a water particle) with the
-// adjoints lr (of drho_a) and (l0, l1) (of acc_a).
+// adjoints lr (of drho_a) and (l0, l1) (of acc_a).  MS: the moving-square
+// modified solver (Moving_Square.../Solver_Normalized_Modified_Linear_Riemann_Delta.f90
+// :169-230): w also carries avg_a - avg_b (XSPH inside the continuity flux), no SPS.
+template <bool MS = false>
 __device__ __forceinline__ void rev_pair(const Params& P, const PSide& A, const PSide& B, double lr, double l0,
                                          double l1, PBar& o) {
     const double r0 = A.x.x - B.x.x, r1 = A.x.y - B.x.y;
@@ -155,6 +184,7 @@ __device__ __forceinline__ void rev_pair(const Params& P, const PSide& A, const 
         kk = dp / (2.0 * rbar * c0 * d);
         w0 = 0.5 * du0 + kk * r0; w1 = 0.5 * du1 + kk * r1;
     }
+    if (MS) { w0 += A.ax - B.ax; w1 += A.ay - B.ay; }
     const double rhoij = 1.0 / (A.rho * B.rho);
     const double fp = -2.0 * PA * B.m * rhoij;
     const bool av = vx < 0.0;
@@ -176,11 +206,12 @@ __device__ __forceinline__ void rev_pair(const Params& P, const PSide& A, const 
     o.t0 = o.t1 = o.t2 = o.g0 = o.g1 = 0.0;
     // acc = Cn G n + lf (u_a - u_b) + SPS
     const double Cnb = G * Ln;
+    o.mb = Cnb * (-2.0 * PA * rhoij - (av ? Pi : 0.0));
     Gb += Cn * Ln;
     n0b += Cn * G * l0; n1b += Cn * G * l1;
     const double lfb = l0 * du0 + l1 * du1;
     du0b += lf * l0; du1b += lf * l1;
-    {
+    if (!MS) {
         // SPS: acc_x += sm rho_ij G Q, acc_y += sm rho_ij G (q rho_ij Q + Rr), q = 1 with the
         // reference's temp_p carry-over
         const double sxx = A.t0 + B.t0, sxy = A.t1 + B.t1, syy = A.t2 + B.t2;
@@ -245,6 +276,7 @@ __device__ __forceinline__ void rev_pair(const Params& P, const PSide& A, const 
         }
     }
     du0b += 0.5 * w0b; du1b += 0.5 * w1b;
+    o.avg0 = w0b; o.avg1 = w1b;
     Pbarb += PAb0;
     if (!A.near) {
         const double kkb = w0b * r0 + w1b * r1;
@@ -294,7 +326,7 @@ __device__ __forceinline__ void rev_pair(const Params& P, const PSide& A, const 
 #define SPH_ADJ_C_MIN_BLOCKS 3       // 168 registers: 3 blocks of 128 per SM
 #endif
 constexpr int kAdjLanes = SPH_ADJ_LANES;     // 2 or 4
-template <typename R>
+template <typename R, bool MS = false>
 __global__ void __launch_bounds__(kAdjThreads, SPH_ADJ_C_MIN_BLOCKS) k_adj_c(Params P, Sorted<R> D, Adj A, const double* lr,
                                                         const double2* la, double* nu_part) {
     __shared__ double red[kAdjThreads];
@@ -304,9 +336,11 @@ __global__ void __launch_bounds__(kAdjThreads, SPH_ADJ_C_MIN_BLOCKS) k_adj_c(Par
     double nu_sum = 0.0;
     // every lane of the warp takes part in the shuffles below
     const bool live = c < P.n_tot;
-    double v[19];
+    // 0-16 as below; MS: 17-18 avg, 19 mass
+    constexpr int NV = MS ? 20 : 17;
+    double v[20];
 #pragma unroll
-    for (int q = 0; q < 19; ++q) v[q] = 0.0;
+    for (int q = 0; q < 20; ++q) v[q] = 0.0;
     if (live) {
         const int nn = D.npairs[c];
         // both roles run the same instructions: the two sides are loaded by
@@ -320,10 +354,10 @@ __global__ void __launch_bounds__(kAdjThreads, SPH_ADJ_C_MIN_BLOCKS) k_adj_c(Par
             const double l_r = lr[acc_at];
             const double2 l_a = la[acc_at];
             if (l_r == 0.0 && l_a.x == 0.0 && l_a.y == 0.0) continue;
-            const PSide Sa = load_side(D, acc_at);
-            const PSide Sb = load_side(D, other);
+            const PSide Sa = load_side<R, MS>(D, acc_at);
+            const PSide Sb = load_side<R, MS>(D, other);
             PBar o;
-            rev_pair(P, Sa, Sb, l_r, l_a.x, l_a.y, o);
+            rev_pair<MS>(P, Sa, Sb, l_r, l_a.x, l_a.y, o);
             v[0] += sg * o.x0; v[1] += sg * o.x1; v[2] += sg * o.u; v[3] += sg * o.v;
             v[4] += role ? o.pb : o.pa;
             v[5] += role ? o.cb : o.ca;
@@ -334,10 +368,14 @@ __global__ void __launch_bounds__(kAdjThreads, SPH_ADJ_C_MIN_BLOCKS) k_adj_c(Par
                 v[13] += o.bi0; v[14] += o.bi1; v[15] += o.bi2; v[16] += o.bi3;
                 nu_sum += o.nu;
             }
+            if (MS) {
+                v[17] += sg * o.avg0; v[18] += sg * o.avg1;
+                v[19] += role ? o.mb : 0.0;
+            }
         }
     }
 #pragma unroll
-    for (int q = 0; q < 17; ++q) {
+    for (int q = 0; q < NV; ++q) {
         v[q] += __shfl_xor_sync(0xffffffffu, v[q], 1);
         if (kAdjLanes == 4) v[q] += __shfl_xor_sync(0xffffffffu, v[q], 2);
     }
@@ -352,6 +390,10 @@ __global__ void __launch_bounds__(kAdjThreads, SPH_ADJ_C_MIN_BLOCKS) k_adj_c(Par
         A.gbinv[c] = make_double4(v[13], v[14], v[15], v[16]);
         A.ggr[c] = make_double2(v[11], v[12]);
         A.gtau[c] = make_double4(v[8], v[9], v[10], 0.0);
+        if (MS) {
+            A.gavg[c] = make_double2(v[17], v[18]);
+            A.sm[c] = v[19] + v[7] / rho;       // V = m / rho
+        }
     }
     red[threadIdx.x] = nu_sum;
     __syncthreads();
@@ -509,23 +551,60 @@ __device__ __forceinline__ void rev_rawsum(const Params& P, double r0, double r1
 }
 
 // Reverse of pass A's raw pair sums, then of the stage that produced the
-// state this RHS was evaluated on.
-template <typename R>
-__global__ void __launch_bounds__(kAdjThreads) k_adj_a(Params P, Sorted<R> D, Adj A, int stage, double dt) {
+// state this RHS was evaluated on.  MS: also the reverse of the XSPH velocity
+//   avg_a = eps sum_b m_b (v_b - v_a) W_ab / (rho_a + rho_b)
+// (Moving_Square.../Solver_Normalized_Modified_Linear_Riemann_Delta.f90:114-121)
+// with the adjoint lg + gavg of avg; the totals of the state adjoint (x, u, rho,
+// m) are written to sx, su, sr, sm for the ghost reverse and the stage reverse
+// that follow.
+template <typename R, bool MS = false>
+__global__ void __launch_bounds__(kAdjThreads) k_adj_a(Params P, Sorted<R> D, Adj A, int stage, double dt,
+                                                       const double2* lg) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.n_tot) return;
     const double2 xc = D.pos[c];
     const double4 kc = D.kin[c];
-    const double Vc = D.mass[c] / kc.z;
+    const double mc = D.mass[c];
+    const double Vc = mc / kc.z;
     const double4 mc1 = A.mu1[c], mc2 = A.mu2[c];
     const double2 mc3 = A.mu3[c];
-    double x0b = 0, x1b = 0, ub = 0, vb = 0, rb = 0, Vb = 0;
+    double x0b = 0, x1b = 0, ub = 0, vb = 0, rb = 0, Vb = 0, mb_ = 0;
+    double2 lac = make_double2(0.0, 0.0);
+    if (MS) {
+        const double2 g = A.gavg[c], l = lg[c];
+        lac = make_double2(g.x + l.x, g.y + l.y);
+    }
     const int nn = D.npairs[c];
     for (int e = 0; e < nn; ++e) {
         const int b = (int)(D.pairs[(size_t)e * P.nbr_stride + c] & 0x7fffffffu);
         const double2 xb = D.pos[b];
         const double4 kb = D.kin[b];
         const double r0 = xc.x - xb.x, r1 = xc.y - xb.y;
+        if (MS) {
+            const double d = sqrt(r0 * r0 + r1 * r1);
+            double G, dG;
+            kernel_g(P, d, G, dG);
+            const double W = kernel_w(P, d);
+            const double mb = D.mass[b];
+            const double rs = kc.z + kb.z, irs = 1.0 / rs;
+            const double2 g = A.gavg[b], l = lg[b];
+            const double lb0 = g.x + l.x, lb1 = g.y + l.y;
+            // own sum: f = eps m_b W / rs times (v_b - v_c)
+            const double f = P.eps * mb * W * irs;
+            const double S = lac.x * (kb.x - kc.x) + lac.y * (kb.y - kc.y);
+            ub -= f * lac.x; vb -= f * lac.y;
+            rb -= S * f * irs;
+            const double Wb = S * P.eps * mb * irs;
+            // the neighbour's sum: f' = eps m_c W / rs times (v_c - v_b)
+            const double f2 = P.eps * mc * W * irs;
+            const double S2 = lb0 * (kc.x - kb.x) + lb1 * (kc.y - kb.y);
+            ub += f2 * lb0; vb += f2 * lb1;
+            rb -= S2 * f2 * irs;
+            mb_ += S2 * P.eps * W * irs;
+            const double Wb2 = S2 * P.eps * mc * irs;
+            // dW/dx_c = G r
+            x0b += (Wb + Wb2) * G * r0; x1b += (Wb + Wb2) * G * r1;
+        }
         // own sums: phi_b - phi_c, weight V_b
         {
             const double Vbn = D.mass[b] / kb.z;
@@ -550,6 +629,13 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_a(Params P, Sorted<R> D, Ad
         }
     }
     const double2 sx = A.sx[c], su = A.su[c];
+    if (MS) {
+        A.sx[c] = make_double2(sx.x + x0b, sx.y + x1b);
+        A.su[c] = make_double2(su.x + ub, su.y + vb);
+        A.sr[c] += rb - Vc / kc.z * Vb;
+        A.sm[c] += mb_ + Vb / kc.z;
+        return;
+    }
     stage_reverse(P, D, A, c, stage, dt, make_double2(sx.x + x0b, sx.y + x1b), make_double2(su.x + ub, su.y + vb),
                   A.sr[c] + rb - Vc / kc.z * Vb);
 }
@@ -603,6 +689,7 @@ __global__ void k_adj_scatter(Params P, Sorted<R> D, Adj A, int first) {
     if (i < P.n_host) {
         A.lk_r[i] = first ? 0.0 : A.lr[0][s];
         A.lk_a[i] = first ? make_double2(0, 0) : A.la[0][s];
+        if (A.lk_g) A.lk_g[i] = first ? make_double2(0, 0) : A.lg[0][s];
     }
 }
 
@@ -674,7 +761,7 @@ __global__ void k_adj_loss(int n, int kind, const int* type, const double2* vel,
     __shared__ double red[256];
     double s = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        if (type[i] != SPH_TYPE_WATER) continue;
+        if (type[i] != SPH_TYPE_WATER || kind == SPH_LOSS_DRAG) continue;
         const double2 v = vel[i];
         if (kind == SPH_LOSS_VELOCITY_MISFIT) {
             const double2 t = target[i];
@@ -693,13 +780,14 @@ __global__ void k_adj_loss(int n, int kind, const int* type, const double2* vel,
 }
 
 // Adjoint of the final state: dL/dv scaled by dloss; the positions, densities
-// and carried rates do not enter the loss.
+// and carried rates do not enter the loss (nor the final state the drag loss,
+// whose terms enter step by step in the reverse sweep).
 __global__ void k_adj_seed(int n, int kind, double dloss, const int* type, const double2* vel, const double* mass,
                            const double2* target, Adj A) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double2 g = make_double2(0, 0);
-    if (type[i] == SPH_TYPE_WATER) {
+    if (type[i] == SPH_TYPE_WATER && kind != SPH_LOSS_DRAG) {
         const double2 v = vel[i];
         if (kind == SPH_LOSS_VELOCITY_MISFIT) {
             const double2 t = target[i];
@@ -713,6 +801,362 @@ __global__ void k_adj_seed(int n, int kind, double dloss, const int* type, const
     A.lrho[i] = 0.0;
     A.lk_r[i] = 0.0;
     A.lk_a[i] = make_double2(0, 0);
+    if (A.lk_g) A.lk_g[i] = make_double2(0, 0);
+}
+
+// ---------------------------------------------------------------------------
+// Moving-square path: Euler predictor-corrector with carried rates, ghost
+// assignment, body motion and the drag loss.
+// ---------------------------------------------------------------------------
+
+// Reverse of the drag loss term w * F_x of one RHS, F = the total body force of
+// k_body_force (Calculate_Body_Force.f90:53-142, Morris laplacian):
+//   F_x = sum_a V_a sum_{b in body} T_ab,
+//   T_ab = V_b [ -(p_a + p_b) G L0 + 2 nu rho_a G Q (u_a - u_b) / d^2 ],
+// r = x_a - x_b, L = B_a^-1 r, Q = r.L.  Thread c adds the derivative with
+// respect to its inputs as particle a (its body neighbours b) and, for a body
+// particle, as particle b (its neighbours a), to the state adjoints of the RHS;
+// dL/dnu partials per block into nu_part.
+template <typename R>
+__global__ void __launch_bounds__(kAdjThreads) k_adj_drag(Params P, Sorted<R> D, Adj A, double w, double* nu_part) {
+    __shared__ double red[kAdjThreads];
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    double nu_sum = 0.0;
+    if (c < P.n_tot) {
+        const bool cbody = D.itype[c] == SPH_TYPE_BODY;
+        const double2 xc = D.pos[c];
+        const double4 kc = D.kin[c];
+        const double Vc = D.mass[c] / kc.z;
+        const double4 bic = D.binv64[c];
+        double x0b = 0, x1b = 0, ub = 0, pb = 0, rb = 0, Vb_ = 0;
+        double4 gb = make_double4(0, 0, 0, 0);
+        const int nn = D.npairs[c];
+        for (int e = 0; e < nn; ++e) {
+            const int b = (int)(D.pairs[(size_t)e * P.nbr_stride + c] & 0x7fffffffu);
+            const bool bbody = D.itype[b] == SPH_TYPE_BODY;
+            if (!bbody && !cbody) continue;
+            const double2 xb = D.pos[b];
+            const double4 kb = D.kin[b];
+            const double Vb = D.mass[b] / kb.z;
+            // the term of pair (a, b): a = c when b is the body particle, else a = b
+            const bool c_is_a = bbody;
+            const double4 bi = c_is_a ? bic : D.binv64[b];
+            const double4 ka = c_is_a ? kc : kb, kbb = c_is_a ? kb : kc;
+            const double Va = c_is_a ? Vc : Vb, Vbb = c_is_a ? Vb : Vc;
+            const double r0 = c_is_a ? xc.x - xb.x : xb.x - xc.x, r1 = c_is_a ? xc.y - xb.y : xb.y - xc.y;
+            const double d2 = r0 * r0 + r1 * r1, d = sqrt(d2), id2 = 1.0 / d2;
+            double G, dG;
+            kernel_g(P, d, G, dG);
+            const double L0 = bi.x * r0 + bi.y * r1, L1 = bi.z * r0 + bi.w * r1;
+            const double Q = r0 * L0 + r1 * L1;
+            const double P2 = ka.w + kbb.w, du = ka.x - kbb.x;
+            const double K = 2.0 * P.nu * ka.z;
+            const double Tin = -P2 * G * L0 + K * du * G * Q * id2;
+            const double wv = w * Va * Vbb;
+            // d/dr of Tin
+            const double gq0 = L0 + bi.x * r0 + bi.z * r1, gq1 = L1 + bi.y * r0 + bi.w * r1;
+            const double kd = dG / d;
+            const double t1 = K * du * id2;
+            const double Tr0 = -P2 * (kd * r0 * L0 + G * bi.x) + t1 * (kd * r0 * Q + G * gq0 - 2.0 * G * Q * r0 * id2);
+            const double Tr1 = -P2 * (kd * r1 * L0 + G * bi.y) + t1 * (kd * r1 * Q + G * gq1 - 2.0 * G * Q * r1 * id2);
+            const double sg = c_is_a ? 1.0 : -1.0;
+            x0b += sg * wv * Tr0; x1b += sg * wv * Tr1;
+            ub += sg * wv * K * G * Q * id2;
+            pb += -wv * G * L0;
+            if (c_is_a) {
+                rb += wv * 2.0 * P.nu * G * Q * du * id2;
+                Vb_ += w * Vbb * Tin;
+                nu_sum += wv * 2.0 * ka.z * G * Q * du * id2;
+                gb.x += wv * (-P2 * G * r0 + t1 * G * r0 * r0);
+                gb.y += wv * (-P2 * G * r1 + t1 * G * r0 * r1);
+                gb.z += wv * (t1 * G * r1 * r0);
+                gb.w += wv * (t1 * G * r1 * r1);
+            } else {
+                Vb_ += w * Va * Tin;
+            }
+        }
+        if (nn > 0) {
+            double dp, dc;
+            eos_deriv(P, kc.z, dp, dc);
+            const double2 sx = A.sx[c], su = A.su[c];
+            A.sx[c] = make_double2(sx.x + x0b, sx.y + x1b);
+            A.su[c] = make_double2(su.x + ub, su.y);
+            A.sr[c] += rb + dp * pb - Vc / kc.z * Vb_;
+            if (A.sm) A.sm[c] += Vb_ / kc.z;
+            const double4 g = A.gbinv[c];
+            A.gbinv[c] = make_double4(g.x + gb.x, g.y + gb.y, g.z + gb.z, g.w + gb.w);
+        }
+    }
+    red[threadIdx.x] = nu_sum;
+    __syncthreads();
+    for (int k = kAdjThreads / 2; k > 0; k >>= 1) {
+        if (threadIdx.x < k) red[threadIdx.x] += red[threadIdx.x + k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) nu_part[blockIdx.x] = red[0];
+}
+
+// Reverse of k_assign_ghosts, ghost side.  For ghost s with the adjoints of its
+// assigned state (u, v from su; rho from sr, i.e. p through rho = (p - pb)/c0^2
+// + rho0; m from sm) form the multipliers of the Shepard sums
+//   lam_phi = phibar_int / sum W  (phi = p, u, v, m),
+//   lam_w   = -sum_phi lam_phi phi_int        (the normalisation),
+// after the reverse of the label mirror and of the shock-release branch (whose
+// characteristic form returns the interpolated values for labels -6/-7 and
+// pressure 0 for other labels).  Body ghosts: u, v are the body velocity, whose
+// adjoint is summed per block with the adjoint of the body acceleration (the
+// g.(x - x_j) pressure term) into part[4 blocks].  A second gather gives the
+// ghost's position adjoint.  The ghost's su, sr, sm are consumed (the ghost
+// state a step starts from is overwritten before use).  Without library ghost
+// assignment the ghost states are the caller's, constant from step to step, and
+// their adjoints pass through to the step start untouched.
+template <typename R>
+__global__ void __launch_bounds__(kAdjThreads) k_adj_ghost_lambda(Params P, Sorted<R> D, Adj A, double t,
+                                                                  double bax, double bay, double* part) {
+    __shared__ double red[4][kAdjThreads];
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    double bu = 0, bv = 0, ba0 = 0, ba1 = 0;
+    if (s < P.n_tot && D.type[s] == SPH_TYPE_FIX_GHOST && P.ghost_assign) {
+        double lp = 0, lu = 0, lv = 0, lm = 0, lw = 0;
+        double2 xs = make_double2(0, 0);
+        if (D.id[s] < P.n_host) {
+            const bool body = D.itype[s] == SPH_TYPE_BODY;
+            const double gxe = P.grav[0] + (body ? bax : 0.0), gye = P.grav[1] + (body ? bay : 0.0);
+            double sw = 0.0, sp = 0.0, su = 0.0, sv = 0.0, sm = 0.0;
+            int cnt = 0;
+            ghost_visit(P, D, s, [&](int b, double dx, double dy, double, double w) {
+                const double4 kb = D.kin[b];
+                const double mb = D.mass[b];
+                const double W = w * (mb / kb.z);
+                sw += W;
+                sp += kb.w * W + kb.z * W * (gxe * dx + gye * dy);
+                su += kb.x * W;
+                sv += kb.y * W;
+                sm += mb * W;
+                ++cnt;
+            });
+            double pint = 0.0, uint = 0.0, vint = 0.0, m = 0.0;
+            if (cnt >= 3) {
+                const double inv = 1.0 / sw;
+                pint = sp * inv; uint = su * inv; vint = sv * inv; m = sm * inv;
+            }
+            if (m != 0.0) {
+                const double2 ou = A.su[s];
+                double pbar = A.sr[s] / P.c0sq, ubar = 0.0, vbar = 0.0;
+                if (body) {
+                    bu = ou.x; bv = ou.y;
+                } else {
+                    const int lab = D.blabel[s];
+                    double fu = 1.0, fv = 1.0;
+                    if (lab == -6) { if (P.wall_bc == 1) fv = -1.0; else { fu = -1.0; fv = -1.0; } }
+                    else if (lab == -7) { fu = -1.0; fv = -1.0; }
+                    else if (lab == -8) { if (P.wall_bc == 1) fu = -1.0; else { fu = -1.0; fv = -1.0; } }
+                    ubar = fu * ou.x; vbar = fv * ou.y;
+                    if (0.0 < t && t <= P.shock_t && lab != -6 && lab != -7) pbar = 0.0;
+                }
+                const double inv = 1.0 / sw;
+                lp = pbar * inv; lu = ubar * inv; lv = vbar * inv; lm = A.sm[s] * inv;
+                lw = -(lp * pint + lu * uint + lv * vint + lm * m);
+                ghost_visit(P, D, s, [&](int b, double dx, double dy, double q, double w) {
+                    const double4 kb = D.kin[b];
+                    const double mb = D.mass[b];
+                    const double Vb = mb / kb.z, W = w * Vb;
+                    const double Wb = lp * (kb.w + kb.z * (gxe * dx + gye * dy)) + lu * kb.x + lv * kb.y + lm * mb + lw;
+                    const double k = Wb * Vb * ghost_dw_over_d(P, q);
+                    const double cg = lp * kb.z * W;
+                    xs.x += k * dx + cg * gxe;
+                    xs.y += k * dy + cg * gye;
+                    if (body) { ba0 += cg * dx; ba1 += cg * dy; }
+                });
+            }
+        }
+        A.glam[s] = make_double4(lp, lu, lv, lm);
+        A.glamw[s] = lw;
+        const double2 sx = A.sx[s];
+        A.sx[s] = make_double2(sx.x + xs.x, sx.y + xs.y);
+        A.su[s] = make_double2(0, 0);
+        A.sr[s] = 0.0;
+        A.sm[s] = 0.0;
+    }
+    red[0][threadIdx.x] = bu; red[1][threadIdx.x] = bv; red[2][threadIdx.x] = ba0; red[3][threadIdx.x] = ba1;
+    __syncthreads();
+    for (int k = kAdjThreads / 2; k > 0; k >>= 1) {
+        if (threadIdx.x < k)
+            for (int q = 0; q < 4; ++q) red[q][threadIdx.x] += red[q][threadIdx.x + k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 4; ++q) part[(size_t)q * gridDim.x + blockIdx.x] = red[q][0];
+}
+
+// Reverse of k_assign_ghosts, interpolated side: particle j gathers the ghosts
+// whose window and radius it falls in (the same cells and the same distance test
+// as the forward: j's list-build cell within ghost_cells of the ghost's cell) and
+// adds d(sum_s lam_s . sums_s)/d(x_j, u_j, v_j, rho_j); p_j enters through the
+// equation of state, V_j = m_j / rho_j.
+template <typename R>
+__global__ void __launch_bounds__(kAdjThreads) k_adj_ghost_water(Params P, Sorted<R> D, Adj A, double bax,
+                                                                 double bay) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= P.n_tot || D.type[j] == SPH_TYPE_FIX_GHOST) return;
+    const double2 xj = D.pos[j], x0 = D.pos0[j];
+    const int cx = (int)floor((x0.x - P.gx0) / P.cs), cy = (int)floor((x0.y - P.gy0) / P.cs);
+    const double4 kj = D.kin[j];
+    const double mj = D.mass[j], Vj = mj / kj.z;
+    const double hg = P.ghost_h;
+    double x0b = 0, x1b = 0, ub = 0, vb = 0, pb = 0, rb = 0;
+    for (int gy = max(cy - P.ghost_cells, 0); gy <= min(cy + P.ghost_cells, P.gny - 1); ++gy) {
+        const int row = gy * P.gnx;
+        for (int gx = max(cx - P.ghost_cells, 0); gx <= min(cx + P.ghost_cells, P.gnx - 1); ++gx) {
+            const int s0 = D.cell_start[row + gx];
+            if (s0 < 0) continue;
+            const int s1 = D.cell_end[row + gx];
+            for (int s = s0; s < s1; ++s) {
+                if (D.type[s] != SPH_TYPE_FIX_GHOST || D.id[s] >= P.n_host) continue;
+                const double2 x = D.pos[s];
+                const double dx = x.x - xj.x, dy = x.y - xj.y;
+                const double d = sqrt(dx * dx + dy * dy);
+                if (!(d <= P.ghost_r)) continue;
+                const double4 lam = A.glam[s];
+                const double lw = A.glamw[s];
+                if (lam.x == 0.0 && lam.y == 0.0 && lam.z == 0.0 && lam.w == 0.0 && lw == 0.0) continue;
+                const double q = d / hg;
+                double w;
+                if (P.kernel_model == SPH_KERNEL_GAUSSIAN) {
+                    w = (exp(-(q * q)) - P.gauss_e9) * P.ghost_kf;
+                } else {
+                    const double tq = 1.0 - q / 2.0;
+                    const double t2 = tq * tq;
+                    w = P.ghost_kf * (1.0 + 2.0 * q) * (t2 * t2);
+                }
+                const bool body = D.itype[s] == SPH_TYPE_BODY;
+                const double gxe = P.grav[0] + (body ? bax : 0.0), gye = P.grav[1] + (body ? bay : 0.0);
+                const double ge = gxe * dx + gye * dy;
+                const double W = w * Vj;
+                ub += lam.y * W; vb += lam.z * W; pb += lam.x * W;
+                rb += lam.x * W * ge;
+                const double Wb = lam.x * (kj.w + kj.z * ge) + lam.y * kj.x + lam.z * kj.y + lam.w * mj + lw;
+                rb -= Wb * W / kj.z;
+                const double k = Wb * Vj * ghost_dw_over_d(P, q);
+                const double cg = lam.x * kj.z * W;
+                x0b -= k * dx + cg * gxe;
+                x1b -= k * dy + cg * gye;
+            }
+        }
+    }
+    double dp, dc;
+    eos_deriv(P, kj.z, dp, dc);
+    const double2 sx = A.sx[j], su = A.su[j];
+    A.sx[j] = make_double2(sx.x + x0b, sx.y + x1b);
+    A.su[j] = make_double2(su.x + ub, su.y + vb);
+    A.sr[j] += rb + dp * pb;
+}
+
+// Reverse of the step end of the Euler predictor-corrector (stage 11,
+// SPH_Time_Iteration.f90:313-394) from the id-order adjoints of the end state
+// and of the carried rates:
+//   rho' = rho0 + (d1 + d2) dt/2,  u' = v0 + (a1 + a2) dt/2,
+//   x'   = x0 + (up + v0) dt/2 + g2 dt + a2 dt^2/2,   carried (d2, a2, g2),
+// up the predicted velocity.  Rates of RHS 0 (the predictor's, K1) and RHS 1
+// (the corrector's); lxe keeps the adjoint of up for the predictor reverse.
+template <typename R>
+__global__ void k_adj_stage_end_ms(Params P, Sorted<R> D, Adj A, double dt) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= P.n_tot) return;
+    const int i = D.id[s];
+    double2 lx = make_double2(0, 0), lv = make_double2(0, 0);
+    double lrho = 0.0;
+    if (i < P.n_host) { lx = A.lx[i]; lv = A.lv[i]; lrho = A.lrho[i]; }
+    for (int k = 0; k < 2; ++k) {
+        A.lr[k][s] = 0.0; A.la[k][s] = make_double2(0, 0); A.lg[k][s] = make_double2(0, 0);
+    }
+    A.lxe[s] = make_double2(0, 0);
+    A.ax0[s] = lx;
+    A.ar0[s] = lrho;
+    if (i < P.n_host && integrated(P, D.type[s])) {
+        const double h2 = 0.5 * dt;
+        A.av0[s] = make_double2(lv.x + h2 * lx.x, lv.y + h2 * lx.y);
+        A.lxe[s] = make_double2(h2 * lx.x, h2 * lx.y);
+        const double2 lka = A.lk_a[i], lkg = A.lk_g[i];
+        A.lr[0][s] = h2 * lrho;
+        A.la[0][s] = make_double2(h2 * lv.x, h2 * lv.y);
+        A.lr[1][s] = h2 * lrho + A.lk_r[i];
+        A.la[1][s] = make_double2(h2 * lv.x + h2 * dt * lx.x + lka.x, h2 * lv.y + h2 * dt * lx.y + lka.y);
+        A.lg[1][s] = make_double2(dt * lx.x + lkg.x, dt * lx.y + lkg.y);
+    } else {
+        A.av0[s] = lv;
+    }
+}
+
+// Reverse of the predictor (stage 10) with the adjoint (sx, su, sr) of the
+// predicted state:  xp = x0 + (v0 + g1) dt + a1 dt^2/2,  up = v0 + a1 dt,
+// rho_p = rho0 + d1 dt (pred = 1); or, for the state a step starts from (the
+// first step's fresh RHS, pred = 0), the plain accumulation.
+template <typename R>
+__global__ void k_adj_stage_ms(Params P, Sorted<R> D, Adj A, int pred, double dt) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= P.n_tot) return;
+    const double2 sx = A.sx[s], su = A.su[s];
+    const double sr = A.sr[s];
+    double2 ax = A.ax0[s], av = A.av0[s];
+    double ar = A.ar0[s];
+    ax.x += sx.x; ax.y += sx.y;
+    ar += sr;
+    if (pred && D.id[s] < P.n_host && integrated(P, D.type[s])) {
+        const double2 le = A.lxe[s];
+        const double lu0 = su.x + le.x, lu1 = su.y + le.y;
+        av.x += dt * sx.x + lu0; av.y += dt * sx.y + lu1;
+        const double2 la = A.la[0][s], lg = A.lg[0][s];
+        const double q = 0.5 * dt * dt;
+        A.la[0][s] = make_double2(la.x + q * sx.x + dt * lu0, la.y + q * sx.y + dt * lu1);
+        A.lg[0][s] = make_double2(lg.x + dt * sx.x, lg.y + dt * sx.y);
+        A.lr[0][s] += dt * sr;
+    } else {
+        av.x += su.x; av.y += su.y;
+    }
+    A.ax0[s] = ax; A.av0[s] = av; A.ar0[s] = ar;
+}
+
+// Per-block sums of the step-start position adjoint of the body particles
+// (the body moves by u_body dt at the step start, so dL/du_body += dt times this).
+template <typename R>
+__global__ void k_adj_body_pos(Params P, Sorted<R> D, Adj A, double* part) {
+    __shared__ double red[2][256];
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    double x = 0.0, y = 0.0;
+    if (s < P.n_tot && D.itype[s] == SPH_TYPE_BODY && D.id[s] < P.n_host) {
+        const double2 a = A.ax0[s];
+        x = a.x; y = a.y;
+    }
+    red[0][threadIdx.x] = x; red[1][threadIdx.x] = y;
+    __syncthreads();
+    for (int k = 128; k > 0; k >>= 1) {
+        if (threadIdx.x < k) { red[0][threadIdx.x] += red[0][threadIdx.x + k]; red[1][threadIdx.x] += red[1][threadIdx.x + k]; }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) { part[blockIdx.x] = red[0][0]; part[gridDim.x + blockIdx.x] = red[1][0]; }
+}
+
+// out[q] += scale * sum_i part[q nparts + i], q < nq, in block order.
+__global__ void k_adj_motion_sum(int nparts, int nq, const double* part, double scale, double* out) {
+    __shared__ double red[256];
+    for (int q = 0; q < nq; ++q) {
+        double s = 0.0;
+        for (int i = threadIdx.x; i < nparts; i += blockDim.x) s += part[(size_t)q * nparts + i];
+        red[threadIdx.x] = s;
+        __syncthreads();
+        for (int w = 128; w > 0; w >>= 1) {
+            if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) out[q] += scale * red[0];
+        __syncthreads();
+    }
+}
+
+// Drag loss accumulation of the forward run: acc += w * F_x.
+__global__ void k_drag_acc(const double* force, double w, double* acc) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) acc[0] += w * force[4];
 }
 
 }  // namespace sph

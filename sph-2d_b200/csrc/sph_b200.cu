@@ -105,6 +105,13 @@ struct sph_handle {
     double t_phys = 0.0;                  // Real_physical_time (ghost assignment)
     double body_vel[2] = {0.0, 0.0};      // Custom_velocity
     double body_acc[2] = {0.0, 0.0};      // Custom_accleration
+    // per-step body motion of an adjoint run: step (step_count - sched_step0)
+    // takes sched[4k .. 4k+3] (velocity, acceleration) when 0 <= k < sched_n
+    const double* sched = nullptr;
+    long long sched_step0 = 0;
+    int sched_n = 0;
+    double* drag_acc = nullptr;           // adjoint forward: += drag_w * F_x at each step's last RHS
+    double drag_w = 0.0;
 };
 
 namespace {
@@ -421,6 +428,10 @@ int rhs(sph_handle* h, int last) {
         k_body_force_final<<<1, kRedThreads, 0, h->stream>>>(nbf, h->d_bf, fin);
         CK(cudaMemcpyAsync(h->bf, fin, 6 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
         h->launches += 2;
+        if (h->drag_acc && last) {
+            k_drag_acc<<<1, 32, 0, h->stream>>>(fin, h->drag_w, h->drag_acc);
+            h->launches += 1;
+        }
     }
     h->n_rhs++;
     h->have_rhs = true;
@@ -462,21 +473,37 @@ int reinit_density(sph_handle* h, int do_shift) {
     return SPH_OK;
 }
 
+// Start of a step: Real_time = Real_time + dt, then Body_Motion_Solver (MS
+// SPH_Time_Iteration.f90:71-114): the body motion of the step (an adjoint run's
+// schedule, else the handle's), and the body moved by its velocity times dt.
+template <typename R>
+int step_begin(sph_handle* h, double dt) {
+    h->t_phys += dt;
+    if (h->sched) {
+        const long long k = h->step_count - h->sched_step0;
+        if (k >= 0 && k < h->sched_n) {
+            const double* m = h->sched + 4 * k;
+            h->body_vel[0] = m[0]; h->body_vel[1] = m[1]; h->body_acc[0] = m[2]; h->body_acc[1] = m[3];
+        }
+    }
+    if (h->P.ghost_assign && (h->body_vel[0] != 0.0 || h->body_vel[1] != 0.0)) {
+        int rc = unsort<R>(h);
+        if (rc) return rc;
+        k_translate_body<<<blocks(h->n_host, 256), 256, 0, h->stream>>>(h->n_host, h->S.itype, h->S.pos,
+                                                                          h->body_vel[0] * dt, h->body_vel[1] * dt);
+        CK(cudaGetLastError());
+        h->launches += 1;
+        h->sorted_valid = false;
+    }
+    return SPH_OK;
+}
+
 template <typename R>
 int run_steps(sph_handle* h, int nsteps, double dt) {
     for (int s = 0; s < nsteps; ++s) {
-        // Real_time = Real_time + dt, then Body_Motion_Solver (MS SPH_Time_Iteration.f90:71-114)
-        h->t_phys += dt;
-        if (h->P.ghost_assign && (h->body_vel[0] != 0.0 || h->body_vel[1] != 0.0)) {
-            int rc = unsort<R>(h);
-            if (rc) return rc;
-            k_translate_body<<<blocks(h->n_host, 256), 256, 0, h->stream>>>(h->n_host, h->S.itype, h->S.pos,
-                                                                              h->body_vel[0] * dt, h->body_vel[1] * dt);
-            CK(cudaGetLastError());
-            h->launches += 1;
-            h->sorted_valid = false;
-        }
-        int rc = prepare<R>(h);
+        int rc = step_begin<R>(h, dt);
+        if (rc) return rc;
+        rc = prepare<R>(h);
         if (rc) return rc;
         const int first = h->step_count == 0;
         // density re-initialisation after every mls_every-th step (1-based step number)
@@ -626,6 +653,13 @@ struct AdjCtx {
     double* loss_part = nullptr;
     Adj A{};
     std::vector<void*> owned;
+    // moving-square runs
+    int cap_steps = 0;          // capacity of A.g_motion in steps
+    double t0 = 0.0;            // physical time the forward started from
+    double dloss = 0.0;
+    bool have_grad = false;     // A.g_motion holds the last backward pass's result
+    std::vector<double> motion; // [4 nsteps] body motion schedule (empty: the handle's)
+    double* drag_acc = nullptr; // [1] drag loss of the forward run
 };
 
 namespace {
@@ -665,12 +699,26 @@ int snap_io(sph_handle* h, const Snap& s, int k, int n, bool save) {
     return SPH_OK;
 }
 
-int adj_config_ok(const sph_handle* h) {
+int adj_config_ok(const sph_handle* h, int loss) {
     const Params& P = h->P;
-    if (h->cfg.solver != SPH_SOLVER_MODLR_DELTA_SPS || P.muscl || P.ms || P.xsph) return SPH_E_CONFIG;
-    if (h->cfg.integrator != SPH_INTEGRATOR_RK4_REUSE || h->cfg.shifting || P.mls_order) return SPH_E_CONFIG;
+    if (h->cfg.shifting || P.mls_order || P.muscl) return SPH_E_CONFIG;
+    if (P.ms) {
+        // moving-square modified linear solver, Morris laplacian, Euler predictor-corrector
+        if (h->cfg.solver != SPH_SOLVER_MS_MODLR_DELTA || P.laplacian != 1) return SPH_E_CONFIG;
+        if (h->cfg.integrator != SPH_INTEGRATOR_EULER_PC || h->cfg.periodic) return SPH_E_CONFIG;
+    } else {
+        if (h->cfg.solver != SPH_SOLVER_MODLR_DELTA_SPS || P.xsph) return SPH_E_CONFIG;
+        if (h->cfg.integrator != SPH_INTEGRATOR_RK4_REUSE) return SPH_E_CONFIG;
+    }
+    if (loss == SPH_LOSS_DRAG && !P.has_body) return SPH_E_CONFIG;
     return SPH_OK;
 }
+
+// Clears the per-step schedule and the drag accumulation of the handle on exit.
+struct SchedGuard {
+    sph_handle* h;
+    ~SchedGuard() { h->sched = nullptr; h->sched_n = 0; h->drag_acc = nullptr; }
+};
 
 int adj_prepare_ctx(sph_handle* h, const sph_adj_config* ac) {
     AdjCtx* X = h->adj;
@@ -698,7 +746,7 @@ int adj_prepare_ctx(sph_handle* h, const sph_adj_config* ac) {
             (rc = adj_alloc(X, &A.sr, nt)) || (rc = adj_alloc(X, &A.gbinv, nt)) || (rc = adj_alloc(X, &A.ggr, nt)) ||
             (rc = adj_alloc(X, &A.gtau, nt)) || (rc = adj_alloc(X, &A.mu1, nt)) || (rc = adj_alloc(X, &A.mu2, nt)) ||
             (rc = adj_alloc(X, &A.mu3, nt)) ||
-            (rc = adj_alloc(X, &A.nu_part, (size_t)4 * blocks((long long)nt * kAdjLanes, kAdjThreads))) ||
+            (rc = adj_alloc(X, &A.nu_part, (size_t)5 * blocks((long long)nt * kAdjLanes, kAdjThreads))) ||
             (rc = adj_alloc(X, &A.nu_acc, 1)) || (rc = adj_alloc(X, &A.lx, nt)) || (rc = adj_alloc(X, &A.lv, nt)) ||
             (rc = adj_alloc(X, &A.lrho, nt)) || (rc = adj_alloc(X, &A.lk_r, nh)) || (rc = adj_alloc(X, &A.lk_a, nh)))
             return rc;
@@ -712,7 +760,24 @@ int adj_prepare_ctx(sph_handle* h, const sph_adj_config* ac) {
             (rc = adj_alloc(X, &X->st_aux, ns)))
             return rc;
     }
+    if (h->P.ms && !X->A.gavg) {
+        Adj& A = X->A;
+        const size_t nh = (size_t)X->cap_host, nt = (size_t)X->cap_tot;
+        int rc;
+        if ((rc = adj_alloc(X, &A.lg[0], nt)) || (rc = adj_alloc(X, &A.lg[1], nt)) ||
+            (rc = adj_alloc(X, &A.lk_g, nh)) || (rc = adj_alloc(X, &A.gavg, nt)) || (rc = adj_alloc(X, &A.sm, nt)) ||
+            (rc = adj_alloc(X, &A.glam, nt)) || (rc = adj_alloc(X, &A.glamw, nt)) ||
+            (rc = adj_alloc(X, &A.mo_part, (size_t)4 * blocks((long long)nt, kAdjThreads))) ||
+            (rc = adj_alloc(X, &X->drag_acc, 1)))
+            return rc;
+    }
+    if (X->cap_steps < ac->nsteps) {
+        int rc = adj_alloc(X, &X->A.g_motion, (size_t)4 * ac->nsteps);
+        if (rc) return rc;
+        X->cap_steps = ac->nsteps;
+    }
     X->valid = false;
+    X->have_grad = false;
     X->nsteps = ac->nsteps; X->every = every; X->nseg = nseg; X->loss = ac->loss; X->dt = ac->dt;
     X->n_host = h->n_host;
     X->seg_ntot.assign(every, 0);
@@ -731,19 +796,36 @@ int adjoint_forward(sph_handle* h, const sph_adj_config* ac, double* loss) {
         h->launches += 1;
     }
     X->step0 = h->step_count;
+    X->t0 = h->t_phys;
+    X->motion.clear();
+    if (ac->body_motion) X->motion.assign(ac->body_motion, ac->body_motion + 4 * (size_t)ac->nsteps);
+    SchedGuard guard{h};
+    if (!X->motion.empty()) {
+        h->sched = X->motion.data(); h->sched_step0 = X->step0; h->sched_n = X->nsteps;
+    }
+    if (ac->loss == SPH_LOSS_DRAG) {
+        CK(cudaMemsetAsync(X->drag_acc, 0, sizeof(double), h->stream));
+        h->drag_acc = X->drag_acc;
+        h->drag_w = ac->dt;
+    }
     for (int c = 0; c < X->nseg; ++c) {
         if ((rc = unsort<R>(h)) || (rc = snap_io(h, X->ck, c, n, true))) return rc;
         const int ns = std::min(X->every, X->nsteps - c * X->every);
         if ((rc = run_steps<R>(h, ns, X->dt))) return rc;
     }
     if ((rc = unsort<R>(h)) || (rc = snap_io(h, X->ck, X->nseg, n, true))) return rc;
-    const int nparts = 148 * 4;
-    k_adj_loss<<<nparts, 256, 0, h->stream>>>(n, X->loss, h->S.type, h->S.vel, h->S.mass, X->target, X->loss_part);
-    h->launches += 2;
-    CK(cudaMemsetAsync(h->d_diag, 0, sizeof(double), h->stream));
-    k_adj_nu_sum<<<1, 256, 0, h->stream>>>(nparts, X->loss_part, h->d_diag);
     double v = 0.0;
-    CK(cudaMemcpyAsync(&v, h->d_diag, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (ac->loss == SPH_LOSS_DRAG) {
+        CK(cudaMemcpyAsync(&v, X->drag_acc, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    } else {
+        const int nparts = 148 * 4;
+        k_adj_loss<<<nparts, 256, 0, h->stream>>>(n, X->loss, h->S.type, h->S.vel, h->S.mass, X->target,
+                                                 X->loss_part);
+        h->launches += 2;
+        CK(cudaMemsetAsync(h->d_diag, 0, sizeof(double), h->stream));
+        k_adj_nu_sum<<<1, 256, 0, h->stream>>>(nparts, X->loss_part, h->d_diag);
+        CK(cudaMemcpyAsync(&v, h->d_diag, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    }
     CK(cudaStreamSynchronize(h->stream));
     if (loss) *loss = v;
     X->valid = true;
@@ -773,15 +855,27 @@ int keep_stage(sph_handle* h, int j, int k) {
     return SPH_OK;
 }
 
-// One RK4 step exactly as run_steps takes it, keeping S1..S3 in stage slot j;
-// with full = false the step stops after S3 (all the reverse needs).
+// One step exactly as run_steps takes it, keeping the stage states in stage
+// slot j (RK4: S1..S3; Euler predictor-corrector: the predicted state); with
+// full = false the step stops after the last kept state (all the reverse needs).
 template <typename R>
 int step_keep(sph_handle* h, double dt, int j, bool full) {
-    int rc = prepare<R>(h);
-    if (rc) return rc;
+    int rc = step_begin<R>(h, dt);
+    if (rc || (rc = prepare<R>(h))) return rc;
     h->adj->seg_ntot[j] = h->P.n_tot;
     const int first = h->step_count == 0;
     if (first && (rc = rhs<R>(h, 0))) return rc;
+    if (h->cfg.integrator == SPH_INTEGRATOR_EULER_PC) {
+        if ((rc = stage<R>(h, 10, dt, first ? 0 : 1, 0)) || (rc = keep_stage<R>(h, j, 0))) return rc;
+        if (full) {
+            if ((rc = rhs<R>(h, 1)) || (rc = stage<R>(h, 11, dt, 0, 0))) return rc;
+            h->step_count++;
+            h->n_steps++;
+        }
+        tic(h, -1);
+        if (h->ev_used > 4096) timing_flush(h);
+        return SPH_OK;
+    }
     if ((rc = stage<R>(h, 0, dt, first ? 0 : 1, 0)) || (rc = keep_stage<R>(h, j, 0))) return rc;
     if ((rc = rhs<R>(h, 0)) || (rc = stage<R>(h, 1, dt, 0, 0)) || (rc = keep_stage<R>(h, j, 1))) return rc;
     if ((rc = rhs<R>(h, 0)) || (rc = stage<R>(h, 2, dt, 0, 0)) || (rc = keep_stage<R>(h, j, 2))) return rc;
@@ -811,7 +905,7 @@ int adj_rhs(sph_handle* h, const Sorted<R>& V, int k, int stage) {
     tic(h, PH_ADJ);
     k_adj_c<R><<<nbc, kAdjThreads, 0, h->stream>>>(P, V, A, A.lr[k], A.la[k], A.nu_part + (size_t)k * nbc);
     k_adj_point<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, V, A);
-    k_adj_a<R><<<nb, kAdjThreads, 0, h->stream>>>(P, V, A, stage, X->dt);
+    k_adj_a<R><<<nb, kAdjThreads, 0, h->stream>>>(P, V, A, stage, X->dt, nullptr);
     CK(cudaGetLastError());
     h->launches += 6;
     return SPH_OK;
@@ -866,6 +960,101 @@ int adj_step(sph_handle* h, bool first, int j) {
     return SPH_OK;
 }
 
+// Reverse of one moving-square RHS evaluation on the state V with the rate
+// adjoints of RHS k of the step (0: the predictor's K1, 1: the corrector's):
+// the ghost assignment and pass A are re-run on V (the same values as in the
+// forward run), then the reverse of pass C (and of the step's drag term), of the
+// per-particle end of pass A, of its pair sums and XSPH velocity, of the ghost
+// assignment, and of the predictor (pred = 1) or the step-start accumulation.
+// The body-motion adjoints of the RHS go to g_motion[4 jstep ..].
+template <typename R>
+int adj_rhs_ms(sph_handle* h, const Sorted<R>& V, int k, int pred, bool drag, int jstep) {
+    const Params& P = h->P;
+    AdjCtx* X = h->adj;
+    Adj& A = X->A;
+    const int nb = blocks(P.n_tot, kAdjThreads);
+    const int nbc = blocks((long long)P.n_tot * kAdjLanes, kAdjThreads);
+    tic(h, PH_A);
+    if (P.ghost_assign) {
+        k_assign_ghosts<R><<<nb, 128, 0, h->stream>>>(P, V, h->t_phys, h->body_vel[0], h->body_vel[1],
+                                                       h->body_acc[0], h->body_acc[1]);
+        h->launches += 1;
+    }
+    k_pass_a<R, false><<<nb, 128, 0, h->stream>>>(P, V);
+    k_surface<R><<<nb, 128, 0, h->stream>>>(P, V);
+    k_near<R><<<nb, 128, 0, h->stream>>>(P, V);
+    tic(h, PH_ADJ);
+    k_adj_c<R, true><<<nbc, kAdjThreads, 0, h->stream>>>(P, V, A, A.lr[k], A.la[k], A.nu_part + (size_t)k * nbc);
+    if (drag) {
+        double* part = A.nu_part + (size_t)4 * nbc;
+        k_adj_drag<R><<<nb, kAdjThreads, 0, h->stream>>>(P, V, A, X->dloss * X->dt, part);
+        k_adj_nu_sum<<<1, 256, 0, h->stream>>>(nb, part, A.nu_acc);
+        h->launches += 2;
+    }
+    k_adj_point<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, V, A);
+    k_adj_a<R, true><<<nb, kAdjThreads, 0, h->stream>>>(P, V, A, 0, X->dt, A.lg[k]);
+    k_adj_ghost_lambda<R><<<nb, kAdjThreads, 0, h->stream>>>(P, V, A, h->t_phys, h->body_acc[0], h->body_acc[1],
+                                                             A.mo_part);
+    k_adj_motion_sum<<<1, 256, 0, h->stream>>>(nb, 4, A.mo_part, 1.0, A.g_motion + 4 * (size_t)jstep);
+    if (P.ghost_assign) {
+        k_adj_ghost_water<R><<<nb, kAdjThreads, 0, h->stream>>>(P, V, A, h->body_acc[0], h->body_acc[1]);
+        h->launches += 1;
+    }
+    k_adj_stage_ms<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, V, A, pred, X->dt);
+    CK(cudaGetLastError());
+    h->launches += 10;
+    return SPH_OK;
+}
+
+// Reverse of one Euler predictor-corrector step (moving square) from the staged
+// step-start state (body not yet moved): the step's start (time, body motion,
+// translation) and sort are redone, the predicted state comes from stage slot j
+// (or is recomputed into slot 0 when j < 0).  jstep: the step's index in the
+// adjoint run.
+template <typename R>
+int adj_step_ms(sph_handle* h, bool first, int j, int jstep) {
+    AdjCtx* X = h->adj;
+    Adj& A = X->A;
+    const double dt = X->dt;
+    int rc;
+    if (j < 0) {
+        if ((rc = step_keep<R>(h, dt, 0, false))) return rc;
+        j = 0;
+    } else {
+        if ((rc = step_begin<R>(h, dt)) || (rc = prepare<R>(h))) return rc;
+        if (h->P.n_tot != X->seg_ntot[j]) return SPH_E_ARG;
+    }
+    const Params& P = h->P;
+    Sorted<R>& D = sorted<R>(h);
+    const int nb = blocks(P.n_tot, 256);
+    tic(h, PH_ADJ);
+    k_adj_stage_end_ms<R><<<nb, 256, 0, h->stream>>>(P, D, A, dt);
+    h->launches += 1;
+    if ((rc = adj_rhs_ms<R>(h, stage_view<R>(h, j, 0), 1, 1, X->loss == SPH_LOSS_DRAG, jstep))) return rc;
+    if (first) {
+        // the fresh K1 of the first step was evaluated on the step-start state
+        k_adj_load<R><<<nb, 256, 0, h->stream>>>(P, D, nullptr, nullptr);
+        h->launches += 1;
+        if ((rc = adj_rhs_ms<R>(h, D, 0, 0, false, jstep))) return rc;
+    }
+    tic(h, PH_ADJ);
+    const int nba = blocks((long long)P.n_tot * kAdjLanes, kAdjThreads);
+    k_adj_nu_sum<<<1, 256, 0, h->stream>>>((first ? 2 : 1) * nba, A.nu_part + (first ? 0 : nba), A.nu_acc);
+    // with library ghost assignment the body moved by u_body dt at the step start:
+    // dL/du_body += dt sum_body dL/dx
+    if (P.ghost_assign) {
+        k_adj_body_pos<R><<<nb, 256, 0, h->stream>>>(P, D, A, A.mo_part);
+        k_adj_motion_sum<<<1, 256, 0, h->stream>>>(nb, 2, A.mo_part, dt, A.g_motion + 4 * (size_t)jstep);
+        h->launches += 2;
+    }
+    k_adj_scatter<R><<<nb, 256, 0, h->stream>>>(P, D, A, first ? 1 : 0);
+    h->launches += 2;
+    CK(cudaGetLastError());
+    tic(h, -1);
+    if (h->ev_used > 4096) timing_flush(h);
+    return SPH_OK;
+}
+
 template <typename R>
 int adjoint_backward(sph_handle* h, double dloss, double* g_vel0, double* g_rho0, double* g_pos0,
                      double* g_params) {
@@ -875,6 +1064,14 @@ int adjoint_backward(sph_handle* h, double dloss, double* g_vel0, double* g_rho0
     const int n = h->n_host;
     const bool stored = X->stage_slots >= X->every;
     int rc;
+    X->dloss = dloss;
+    X->have_grad = false;
+    SchedGuard guard{h};
+    if (!X->motion.empty()) {
+        h->sched = X->motion.data(); h->sched_step0 = X->step0; h->sched_n = X->nsteps;
+    }
+    const bool ms = h->P.ms != 0;
+    if (ms) CK(cudaMemsetAsync(A.g_motion, 0, sizeof(double) * 4 * (size_t)X->nsteps, h->stream));
     // seed from the final state
     if ((rc = unsort<R>(h)) || (rc = snap_io(h, X->ck, X->nseg, n, false))) return rc;
     k_adj_seed<<<blocks(n, 256), 256, 0, h->stream>>>(n, X->loss, dloss, h->S.type, h->S.vel, h->S.mass, X->target,
@@ -887,6 +1084,7 @@ int adjoint_backward(sph_handle* h, double dloss, double* g_vel0, double* g_rho0
         // (and the stage states when they fit)
         if ((rc = snap_io(h, X->ck, c, n, false))) return rc;
         h->step_count = X->step0 + s0;
+        h->t_phys = X->t0 + s0 * X->dt;
         for (int j = s0; j < s1; ++j) {
             if ((rc = unsort<R>(h)) || (rc = snap_io(h, X->seg, j - s0, n, true))) return rc;
             if (stored) rc = step_keep<R>(h, X->dt, j - s0, j + 1 < s1);
@@ -896,7 +1094,10 @@ int adjoint_backward(sph_handle* h, double dloss, double* g_vel0, double* g_rho0
         for (int j = s1 - 1; j >= s0; --j) {
             if ((rc = snap_io(h, X->seg, j - s0, n, false))) return rc;
             h->step_count = X->step0 + j;
-            if ((rc = adj_step<R>(h, X->step0 + j == 0, stored ? j - s0 : -1))) return rc;
+            h->t_phys = X->t0 + j * X->dt;
+            if (ms) rc = adj_step_ms<R>(h, X->step0 + j == 0, stored ? j - s0 : -1, j);
+            else rc = adj_step<R>(h, X->step0 + j == 0, stored ? j - s0 : -1);
+            if (rc) return rc;
         }
     }
     timing_flush(h);
@@ -918,7 +1119,13 @@ int adjoint_backward(sph_handle* h, double dloss, double* g_vel0, double* g_rho0
     // the handle continues from the forward's final state
     if ((rc = snap_io(h, X->ck, X->nseg, n, false))) return rc;
     h->step_count = X->step0 + X->nsteps;
+    h->t_phys = X->t0 + X->nsteps * X->dt;
+    if (!X->motion.empty()) {
+        const double* m = X->motion.data() + 4 * (size_t)(X->nsteps - 1);
+        h->body_vel[0] = m[0]; h->body_vel[1] = m[1]; h->body_acc[0] = m[2]; h->body_acc[1] = m[3];
+    }
     h->have_rhs = false;
+    X->have_grad = true;
     return SPH_OK;
 }
 
@@ -1240,9 +1447,10 @@ int sph_diagnostics(sph_handle* h, sph_diag* out) {
 int sph_adjoint_forward(sph_handle* h, const sph_adj_config* cfg, double* loss) {
     if (!h || !cfg || h->n_host <= 0 || cfg->nsteps <= 0 || cfg->checkpoint_every <= 0 || !(cfg->dt > 0))
         return SPH_E_ARG;
-    if (cfg->loss != SPH_LOSS_VELOCITY_MISFIT && cfg->loss != SPH_LOSS_KINETIC_ENERGY) return SPH_E_ARG;
+    if (cfg->loss != SPH_LOSS_VELOCITY_MISFIT && cfg->loss != SPH_LOSS_KINETIC_ENERGY && cfg->loss != SPH_LOSS_DRAG)
+        return SPH_E_ARG;
     if (cfg->loss == SPH_LOSS_VELOCITY_MISFIT && !cfg->target_vel) return SPH_E_ARG;
-    int rc = adj_config_ok(h);
+    int rc = adj_config_ok(h, cfg->loss);
     if (rc) return rc;
     CK(cudaSetDevice(h->device));
     return DISPATCH(h, adjoint_forward, h, cfg, loss);
@@ -1253,6 +1461,20 @@ int sph_adjoint_backward(sph_handle* h, double dloss, double* g_vel0, double* g_
     if (!h) return SPH_E_ARG;
     CK(cudaSetDevice(h->device));
     return DISPATCH(h, adjoint_backward, h, dloss, g_vel0, g_rho0, g_pos0, g_params);
+}
+
+int sph_adjoint_motion_gradient(sph_handle* h, double* g_motion) {
+    if (!h || !g_motion || !h->adj || !h->adj->have_grad) return SPH_E_ARG;
+    CK(cudaSetDevice(h->device));
+    AdjCtx* X = h->adj;
+    const size_t bytes = sizeof(double) * 4 * (size_t)X->nsteps;
+    if (!h->P.ms) {
+        memset(g_motion, 0, bytes);
+        return SPH_OK;
+    }
+    CK(cudaMemcpyAsync(g_motion, X->A.g_motion, bytes, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return SPH_OK;
 }
 
 int sph_get_timings(sph_handle* h, sph_timings* out) {

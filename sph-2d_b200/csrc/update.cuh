@@ -279,29 +279,15 @@ __global__ void k_translate_body(int n, const int* itype, double2* pos, double d
     pos[i] = make_double2(x.x + dx, x.y + dy);
 }
 
-// Fixed-ghost assignment of the moving-square driver (Moving_Square.../
-// Assign_boundary_particles.f90:611-941, with MLS_order_Boundary = 1, i.e.
-// Shepard weights Fai_j = W_j V_j / sum W V), at the start of every RHS, from the
-// current state of the non-ghost particles within kernel_scale * 1.2 h:
-//   p = sum Fai (p_j + rho_j g.(x - x_j)),  u = sum Fai u_j,  m = sum Fai m_j
-// (g: gravity, plus the body acceleration for body ghosts), at least 3
-// neighbours or nothing.  Body ghosts take the body velocity; wall ghosts, during
-// 0 < t <= Shock_wave_release_time, go through the characteristic variables for
-// labels -6 / -7 (which return the interpolated values) and keep the zero
-// pressure they start from for other labels, as the reference's branch does;
-// then the wall velocity is mirrored by label and wall condition.  Finally
-// rho = (p - pb)/c0^2 + rho0, or the rest state when m = 0.
-template <typename R>
-__global__ void k_assign_ghosts(Params P, Sorted<R> D, double t, double bvx, double bvy, double bax, double bay) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= P.n_tot) return;
-    if (D.type[s] != SPH_TYPE_FIX_GHOST || D.id[s] >= P.n_host) return;
+// The neighbours the ghost assignment interpolates from for ghost slot s: the
+// non-ghost particles within kernel_scale * 1.2 h, visited cell by cell over the
+// window of s's cell (the list-build cells, so the window reaches ghost_r plus
+// half the skin).  fn(b, dx, dy, q, w) gets (dx, dy) = x_s - x_b, q = d / h_g and
+// the kernel value w with the ghost smoothing length h_g.
+template <typename R, typename F>
+__device__ __forceinline__ void ghost_visit(const Params& P, const Sorted<R>& D, int s, F&& fn) {
     const double2 x = D.pos[s];
-    const bool body = D.itype[s] == SPH_TYPE_BODY;
-    const double gxe = P.grav[0] + (body ? bax : 0.0), gye = P.grav[1] + (body ? bay : 0.0);
     const int cx = (int)floor((x.x - P.gx0) / P.cs), cy = (int)floor((x.y - P.gy0) / P.cs);
-    double sw = 0.0, sp = 0.0, su = 0.0, sv = 0.0, sm = 0.0;
-    int cnt = 0;
     const double hg = P.ghost_h;
     for (int gy = max(cy - P.ghost_cells, 0); gy <= min(cy + P.ghost_cells, P.gny - 1); ++gy) {
         const int row = gy * P.gnx;
@@ -324,18 +310,53 @@ __global__ void k_assign_ghosts(Params P, Sorted<R> D, double t, double bvx, dou
                     const double t2 = tq * tq;
                     w = P.ghost_kf * (1.0 + 2.0 * q) * (t2 * t2);
                 }
-                const double4 kb = D.kin[b];
-                const double mb = D.mass[b];
-                const double W = w * (mb / kb.z);
-                sw += W;
-                sp += kb.w * W + kb.z * W * (gxe * dx + gye * dy);
-                su += kb.x * W;
-                sv += kb.y * W;
-                sm += mb * W;
-                ++cnt;
+                fn(b, dx, dy, q, w);
             }
         }
     }
+}
+
+// (dw/dd) / d of the ghost kernel at q = d / h_g.
+__device__ __forceinline__ double ghost_dw_over_d(const Params& P, double q) {
+    const double hg2 = P.ghost_h * P.ghost_h;
+    if (P.kernel_model == SPH_KERNEL_GAUSSIAN) return -2.0 * exp(-(q * q)) * P.ghost_kf / hg2;
+    const double tq = 1.0 - q / 2.0;
+    return -5.0 * (tq * tq * tq) * P.ghost_kf / hg2;
+}
+
+// Fixed-ghost assignment of the moving-square driver (Moving_Square.../
+// Assign_boundary_particles.f90:611-941, with MLS_order_Boundary = 1, i.e.
+// Shepard weights Fai_j = W_j V_j / sum W V), at the start of every RHS, from the
+// current state of the non-ghost particles within kernel_scale * 1.2 h:
+//   p = sum Fai (p_j + rho_j g.(x - x_j)),  u = sum Fai u_j,  m = sum Fai m_j
+// (g: gravity, plus the body acceleration for body ghosts), at least 3
+// neighbours or nothing.  Body ghosts take the body velocity; wall ghosts, during
+// 0 < t <= Shock_wave_release_time, go through the characteristic variables for
+// labels -6 / -7 (which return the interpolated values) and keep the zero
+// pressure they start from for other labels, as the reference's branch does;
+// then the wall velocity is mirrored by label and wall condition.  Finally
+// rho = (p - pb)/c0^2 + rho0, or the rest state when m = 0.
+template <typename R>
+__global__ void k_assign_ghosts(Params P, Sorted<R> D, double t, double bvx, double bvy, double bax, double bay) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= P.n_tot) return;
+    if (D.type[s] != SPH_TYPE_FIX_GHOST || D.id[s] >= P.n_host) return;
+    const double2 x = D.pos[s];
+    const bool body = D.itype[s] == SPH_TYPE_BODY;
+    const double gxe = P.grav[0] + (body ? bax : 0.0), gye = P.grav[1] + (body ? bay : 0.0);
+    double sw = 0.0, sp = 0.0, su = 0.0, sv = 0.0, sm = 0.0;
+    int cnt = 0;
+    ghost_visit(P, D, s, [&](int b, double dx, double dy, double, double w) {
+        const double4 kb = D.kin[b];
+        const double mb = D.mass[b];
+        const double W = w * (mb / kb.z);
+        sw += W;
+        sp += kb.w * W + kb.z * W * (gxe * dx + gye * dy);
+        su += kb.x * W;
+        sv += kb.y * W;
+        sm += mb * W;
+        ++cnt;
+    });
     double uint = 0.0, vint = 0.0, pint = 0.0, m = 0.0;
     if (cnt >= 3) {
         const double inv = 1.0 / sw;

@@ -53,6 +53,7 @@ TYPE_FIX_GHOST = -3
 TYPE_BODY = -4
 LOSS_VELOCITY_MISFIT = 0
 LOSS_KINETIC_ENERGY = 1
+LOSS_DRAG = 2
 ADJ_NPARAMS = 1
 
 EXPORTED_SYMBOLS = (
@@ -60,7 +61,7 @@ EXPORTED_SYMBOLS = (
     "sph_rhs", "sph_step", "sph_diagnostics", "sph_get_timings", "sph_reset_timings",
     "sph_strerror", "sph_get_field", "sph_update_state", "sph_find_particle_pair_noalloc",
     "sph_set_initial_type", "sph_adjoint_forward", "sph_adjoint_backward",
-    "sph_set_boundary_labels", "sph_set_body_motion", "sph_set_time",
+    "sph_set_boundary_labels", "sph_set_body_motion", "sph_set_time", "sph_adjoint_motion_gradient",
 )
 
 
@@ -102,6 +103,7 @@ class SphAdjConfig(ctypes.Structure):
     _fields_ = [
         ("nsteps", ctypes.c_int), ("checkpoint_every", ctypes.c_int), ("loss", ctypes.c_int),
         ("reserved", ctypes.c_int), ("dt", ctypes.c_double), ("target_vel", ctypes.POINTER(ctypes.c_double)),
+        ("body_motion", ctypes.POINTER(ctypes.c_double)),
     ]
 
 
@@ -275,6 +277,7 @@ def load(path: str = LIB_PATH):
     lib.sph_set_time.argtypes = [P, ctypes.c_double]
     lib.sph_adjoint_forward.argtypes = [P, ctypes.POINTER(SphAdjConfig), dp]
     lib.sph_adjoint_backward.argtypes = [P, ctypes.c_double, dp, dp, dp, dp]
+    lib.sph_adjoint_motion_gradient.argtypes = [P, dp]
     lib.sph_find_particle_pair_noalloc.argtypes = [ctypes.POINTER(SphConfig), ctypes.c_int, ctypes.c_void_p,
                                                    ctypes.c_void_p, ctypes.c_longlong, ctypes.c_void_p,
                                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
@@ -316,6 +319,7 @@ class Simulation:
         _check(self.lib.sph_init(ctypes.byref(self.cfg), self.capacity, ctypes.byref(h)), "sph_init")
         self.h = h
         self.n = 0
+        self._adj_steps = 0
 
     def close(self):
         if getattr(self, "h", None):
@@ -427,19 +431,26 @@ class Simulation:
         _check(self.lib.sph_reset_timings(self.h), "sph_reset_timings")
 
     def adjoint_forward(self, nsteps: int, dt: float, checkpoint_every: int = 32,
-                        loss: int = LOSS_VELOCITY_MISFIT, target_vel=None) -> float:
+                        loss: int = LOSS_VELOCITY_MISFIT, target_vel=None, body_motion=None) -> float:
         """nsteps time steps with state checkpoints every checkpoint_every steps;
-        returns the loss of the final state (sph_adjoint_forward)."""
+        returns the loss (sph_adjoint_forward).  body_motion: (nsteps, 4) per-step
+        body velocity and acceleration, or None for the handle's constant motion."""
         a = SphAdjConfig()
         a.nsteps, a.checkpoint_every, a.loss, a.dt = int(nsteps), int(checkpoint_every), int(loss), float(dt)
-        keep = None
+        keep = motion = None
         if target_vel is not None:
             keep = np.ascontiguousarray(target_vel, np.float64)
             if keep.shape != (2 * self.n,):
                 raise ValueError("target_vel must hold 2n values (u block, v block)")
             a.target_vel = keep.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        if body_motion is not None:
+            motion = np.ascontiguousarray(body_motion, np.float64)
+            if motion.shape != (int(nsteps), 4):
+                raise ValueError("body_motion must have shape (nsteps, 4)")
+            a.body_motion = motion.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
         out = ctypes.c_double(0.0)
         _check(self.lib.sph_adjoint_forward(self.h, ctypes.byref(a), ctypes.byref(out)), "sph_adjoint_forward")
+        self._adj_steps = int(nsteps)
         return out.value
 
     def adjoint_backward(self, dloss: float = 1.0) -> dict:
@@ -450,6 +461,13 @@ class Simulation:
         _check(self.lib.sph_adjoint_backward(self.h, float(dloss), _ptr(gv), _ptr(gr), _ptr(gx), _ptr(gp)),
                "sph_adjoint_backward")
         return {"vel0": gv, "rho0": gr, "pos0": gx, "nu": float(gp[0])}
+
+    def adjoint_motion_gradient(self) -> np.ndarray:
+        """dL/d(body_motion) of the last backward pass, shape (nsteps, 4)
+        (sph_adjoint_motion_gradient)."""
+        g = np.zeros(4 * self._adj_steps)
+        _check(self.lib.sph_adjoint_motion_gradient(self.h, _ptr(g)), "sph_adjoint_motion_gradient")
+        return g.reshape(self._adj_steps, 4)
 
 
 @dataclass
@@ -480,6 +498,27 @@ def make_tgv(n_side: int, reference: bool = False, solver: int = SOLVER_MUSCL_DE
         pos = pos + rng.uniform(-jitter, jitter, pos.shape) * cfg.dx
     typ = np.full(rho.shape[0], TYPE_WATER, np.int32)
     return TgvCase(cfg, pos, vel, rho, mass, typ)
+
+
+def body_motion_schedule(coeffs, nsteps: int, dt: float, t0: float = 0.0, period: float = 1.0):
+    """Per-step body motion for Simulation.adjoint_forward(body_motion=...) and its
+    Jacobian with respect to the motion parameters.
+
+    The body moves in x with u(t) = a_0 + sum_{k=1..K} a_k sin(2 pi k t / period)
+    (a_0 alone is the impulsive start at constant speed; the reference's motion
+    table is not part of its source tree), v = 0, evaluated at the times the steps
+    use, t0 + (s + 1) dt.  Returns (schedule, jac): schedule[s] = (u, 0, du/dt, 0)
+    with shape (nsteps, 4), and jac[s, :, k] = d schedule[s] / d a_k, so that
+    dL/da = einsum('sq,sqk->k', adjoint_motion_gradient(), jac)."""
+    a = np.asarray(coeffs, np.float64)
+    t = t0 + (np.arange(int(nsteps)) + 1.0) * dt
+    w = 2.0 * np.pi / period
+    jac = np.zeros((int(nsteps), 4, a.size))
+    jac[:, 0, 0] = 1.0
+    for k in range(1, a.size):
+        jac[:, 0, k] = np.sin(k * w * t)
+        jac[:, 2, k] = k * w * np.cos(k * w * t)
+    return jac @ a, jac
 
 
 def fourier_perturbation(pos, n_modes: int = 8, amp: float = 0.05, seed: int = 0, kmax: int = 4,

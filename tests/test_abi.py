@@ -63,14 +63,15 @@ def test_init_without_device_fails_cleanly(built_lib):
 def test_struct_sizes_match_header(tmp_path):
     prog = tmp_path / "sz.c"
     prog.write_text('#include "sph_b200.h"\n#include <stdio.h>\n#include <stddef.h>\n'
-                    'int main(void){printf("%zu %zu %zu %zu %zu %zu\\n", sizeof(sph_config), sizeof(sph_diag),'
+                    'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu\\n", sizeof(sph_config), sizeof(sph_diag),'
                     ' sizeof(sph_timings), offsetof(sph_config, cell_skin), sizeof(sph_adj_config),'
-                    ' offsetof(sph_adj_config, target_vel));return 0;}\n')
+                    ' offsetof(sph_adj_config, target_vel), offsetof(sph_adj_config, body_motion));return 0;}\n')
     exe = tmp_path / "sz"
     subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(prog), "-o", str(exe)], check=True)
     vals = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()]
     assert vals == [ctypes.sizeof(S.SphConfig), ctypes.sizeof(S.SphDiag), ctypes.sizeof(S.SphTimings),
-                    S.SphConfig.cell_skin.offset, ctypes.sizeof(S.SphAdjConfig), S.SphAdjConfig.target_vel.offset]
+                    S.SphConfig.cell_skin.offset, ctypes.sizeof(S.SphAdjConfig), S.SphAdjConfig.target_vel.offset,
+                    S.SphAdjConfig.body_motion.offset]
 
 
 def test_config_validation_codes():

@@ -1,0 +1,182 @@
+"""The discrete adjoint of the moving-square step (sph_adjoint_forward /
+sph_adjoint_backward / sph_adjoint_motion_gradient) against central finite
+differences of the FP64 forward run on the GPU.
+
+The case: the moving-square modified linear Riemann solver (XSPH velocities in
+the continuity flux, Morris laplacian) with the Euler predictor-corrector, the
+library's ghost assignment at every RHS (Shepard interpolation onto the wall
+and body ghosts, mirrored wall velocities, the shock-release branch) and the
+body moved by a per-step schedule.  Losses: the drag impulse sum_s dt F_x and
+the final kinetic energy.  Parameters: the motion amplitude (impulsive start),
+four Fourier coefficients of the motion, the viscosity and the initial
+velocity field.  The improved Gaussian kernel is cut off with a kink at 3h
+(and the ghost kernel at 3 * 1.2h), so the difference steps are those of the
+Gaussian Taylor-Green checks (1e-7 relative).
+
+The water starts with a smooth velocity field rather than at rest: at rest
+every pair sits exactly on the artificial-viscosity switch v.r = 0, where the
+alpha term (alpha = 0.03 here, 0 in the Taylor-Green cases) has a kink, and a
+central difference straddling it measures the mean of the one-sided slopes
+while the adjoint takes the inactive branch."""
+import numpy as np
+import pytest
+
+import sph_b200 as S
+
+pytestmark = pytest.mark.gpu
+
+NSTEPS = 16
+REL_TOL = 1e-4
+
+
+def _case(jitter=0.05, seed=41, ghost_assign=1):
+    case, ity = S.make_moving_square(solver=S.SOLVER_MS_MODLR_DELTA, jitter=jitter, seed=seed)
+    water = np.r_[case.type, case.type] == S.TYPE_WATER
+    case.vel = case.vel + np.where(water, S.fourier_perturbation(case.pos, n_modes=6, amp=0.2, seed=seed), 0.0)
+    cfg = case.cfg
+    cfg.ghost_assign = ghost_assign
+    cfg.shifting = 0
+    cfg.mls_order = 0
+    lab = S.moving_square_labels(case, ity)
+    dt = 0.25 * cfg.h / np.sqrt(cfg.c0sq)
+    return case, ity, lab, dt
+
+
+def _sim(case, ity, lab, cfg=None, vel=None):
+    sim = S.Simulation(case.cfg if cfg is None else cfg, case.n)
+    sim.set_state(case.pos, case.vel if vel is None else case.vel + vel, case.rho, case.mass, case.type)
+    sim.set_initial_type(ity)
+    sim.set_boundary_labels(lab)
+    sim.set_time(0.0)
+    return sim
+
+
+def _loss(case, ity, lab, dt, motion, loss, cfg=None, vel=None):
+    with _sim(case, ity, lab, cfg, vel) as sim:
+        return sim.adjoint_forward(NSTEPS, dt, checkpoint_every=NSTEPS, loss=loss, body_motion=motion)
+
+
+def _grad(case, ity, lab, dt, motion, loss, every=5):
+    with _sim(case, ity, lab) as sim:
+        L = sim.adjoint_forward(NSTEPS, dt, checkpoint_every=every, loss=loss, body_motion=motion)
+        end = sim.get_state()
+        g = sim.adjoint_backward(1.0)
+        gm = sim.adjoint_motion_gradient()
+        after = sim.get_state()
+    return L, g, gm, end, after
+
+
+def _check(ad, fd, what):
+    assert abs(ad - fd) <= REL_TOL * abs(fd), (what, ad, fd, abs(ad - fd) / abs(fd))
+
+
+def test_drag_loss_is_the_sum_of_the_step_forces(lib):
+    """The forward drag loss equals sum_s dt * body_force[4] of time_iteration
+    with the same per-step motion."""
+    case, ity, lab, dt = _case()
+    motion, _ = S.body_motion_schedule([0.6, 0.3, 0.0, 0.1, 0.0], NSTEPS, dt, period=NSTEPS * dt)
+    L = _loss(case, ity, lab, dt, motion, S.LOSS_DRAG)
+    with _sim(case, ity, lab) as sim:
+        total = 0.0
+        for s in range(NSTEPS):
+            sim.set_body_motion(motion[s, :2], motion[s, 2:])
+            d = sim.time_iteration(1, dt)
+            total += dt * d.body_force[4]
+    assert L == pytest.approx(total, rel=1e-12, abs=0)
+    assert L != 0.0
+
+
+@pytest.mark.parametrize("loss", [S.LOSS_DRAG, S.LOSS_KINETIC_ENERGY])
+def test_motion_gradient_matches_central_differences(lib, loss):
+    """dL/d(amplitude) of the impulsive start and dL/d(Fourier coefficients)."""
+    case, ity, lab, dt = _case()
+    period = NSTEPS * dt
+    coeffs = np.array([0.5, 0.4, -0.2, 0.15, 0.1])
+    motion, jac = S.body_motion_schedule(coeffs, NSTEPS, dt, period=period)
+    L, g, gm, end, after = _grad(case, ity, lab, dt, motion, loss)
+    assert np.isfinite(L) and L != 0.0
+    assert all(np.array_equal(a, b) for a, b in zip(end, after))
+    assert np.all(np.isfinite(gm))
+    gc = np.einsum("sq,sqk->k", gm, jac)
+    for k in range(coeffs.size):
+        eps = 1e-7
+        cp, cm = coeffs.copy(), coeffs.copy()
+        cp[k] += eps
+        cm[k] -= eps
+        fd = (_loss(case, ity, lab, dt, S.body_motion_schedule(cp, NSTEPS, dt, period=period)[0], loss)
+              - _loss(case, ity, lab, dt, S.body_motion_schedule(cm, NSTEPS, dt, period=period)[0], loss)) / (2 * eps)
+        _check(gc[k], fd, f"motion coefficient {k}")
+
+
+def test_drag_gradient_velocity_and_viscosity(lib):
+    case, ity, lab, dt = _case()
+    motion, _ = S.body_motion_schedule([1.0], NSTEPS, dt)
+    L, g, gm, _, _ = _grad(case, ity, lab, dt, motion, S.LOSS_DRAG)
+    n = case.n
+    water = case.type == S.TYPE_WATER
+    # ghost velocities are overwritten before use: no gradient
+    assert np.all(g["vel0"][:n][~water] == 0) and np.all(g["vel0"][n:][~water] == 0)
+    for k in range(2):
+        rng = np.random.default_rng(300 + k)
+        d = rng.standard_normal(2 * n) * 0.1
+        eps = 1e-7
+        fd = (_loss(case, ity, lab, dt, motion, S.LOSS_DRAG, vel=eps * d)
+              - _loss(case, ity, lab, dt, motion, S.LOSS_DRAG, vel=-eps * d)) / (2 * eps)
+        _check(float(g["vel0"] @ d), fd, f"velocity direction {k}")
+    nu = case.cfg.nu
+    e = 1e-5 * nu
+    cp, cm = case.cfg.copy(), case.cfg.copy()
+    cp.nu, cm.nu = nu + e, nu - e
+    fd = (_loss(case, ity, lab, dt, motion, S.LOSS_DRAG, cfg=cp)
+          - _loss(case, ity, lab, dt, motion, S.LOSS_DRAG, cfg=cm)) / (2 * e)
+    _check(g["nu"], fd, "viscosity")
+
+
+def test_adjoint_with_caller_given_ghosts(lib):
+    """ghost_assign = 0: the ghost states are the caller's and stay constant, so
+    their initial velocities are live inputs; the body does not move."""
+    case, ity, lab, dt = _case(ghost_assign=0)
+    motion, _ = S.body_motion_schedule([1.0], NSTEPS, dt)
+    L, g, gm, _, _ = _grad(case, ity, lab, dt, motion, S.LOSS_DRAG)
+    assert np.all(gm == 0)
+    n = case.n
+    rng = np.random.default_rng(310)
+    d = rng.standard_normal(2 * n) * 0.1
+    eps = 1e-7
+    fd = (_loss(case, ity, lab, dt, motion, S.LOSS_DRAG, vel=eps * d)
+          - _loss(case, ity, lab, dt, motion, S.LOSS_DRAG, vel=-eps * d)) / (2 * eps)
+    _check(float(g["vel0"] @ d), fd, "velocity direction")
+    ghost = np.r_[case.type, case.type] != S.TYPE_WATER
+    assert np.any(g["vel0"][ghost] != 0)
+
+
+def test_moving_square_adjoint_independent_of_checkpoint_interval(lib):
+    case, ity, lab, dt = _case()
+    motion, _ = S.body_motion_schedule([0.5, 0.4], NSTEPS, dt, period=NSTEPS * dt)
+    ref = _grad(case, ity, lab, dt, motion, S.LOSS_DRAG, every=NSTEPS)
+    for every in (1, 7):
+        got = _grad(case, ity, lab, dt, motion, S.LOSS_DRAG, every=every)
+        assert got[0] == ref[0]
+        for key in ("vel0", "rho0", "pos0"):
+            assert np.array_equal(got[1][key], ref[1][key]), (every, key)
+        assert got[1]["nu"] == ref[1]["nu"]
+        assert np.array_equal(got[2], ref[2])
+
+
+def test_moving_square_adjoint_rejects_unsupported(lib):
+    case, ity, lab, dt = _case()
+    cfg = case.cfg.copy()
+    cfg.solver = S.SOLVER_MS_HLLC_DELTA
+    with _sim(case, ity, lab, cfg) as sim:
+        with pytest.raises(S.SphError) as e:
+            sim.adjoint_forward(2, dt, loss=S.LOSS_DRAG)
+        assert e.value.code == -7
+    # the drag loss needs a body
+    case2 = S.make_tgv(16, solver=S.SOLVER_MODLR_DELTA_SPS)
+    case2.cfg.shifting = 0
+    case2.cfg.mls_order = 0
+    with S.Simulation(case2.cfg, case2.n) as sim:
+        sim.set_state(case2.pos, case2.vel, case2.rho, case2.mass, case2.type)
+        with pytest.raises(S.SphError) as e:
+            sim.adjoint_forward(2, 1e-4, loss=S.LOSS_DRAG)
+        assert e.value.code == -7
