@@ -60,6 +60,8 @@ def load():
     lib.oracle_set_ghost_state.argtypes = [ctypes.c_int, ip, dp, dp, ctypes.c_double]
     lib.oracle_tangent.argtypes = [cp, ctypes.c_int, dp, dp, dp, dp, ip, dp, dp, dp, ctypes.c_double, ctypes.c_int,
                                    ctypes.c_double, ctypes.c_int, dp, dp, dp, dp, dp]
+    lib.oracle_tangent_ms.argtypes = [cp, ctypes.c_int, dp, dp, dp, dp, ip, ip, ip, ctypes.c_double, ctypes.c_int,
+                                      ctypes.c_double, dp, ctypes.c_int, dp, dp, dp, dp, ctypes.c_double, dp, dp]
     _lib = lib
     return lib
 
@@ -205,6 +207,27 @@ def tangent(cfg: SphConfig, pos, vel, rho, mass, type_, nsteps: int, dt: float, 
     if rc != 0:
         raise RuntimeError(f"oracle_tangent failed ({rc})")
     return out[0], out[1], (P, V, R)
+
+
+def tangent_ms(cfg: SphConfig, pos, vel, rho, mass, type_, itype, labels, t0: float, nsteps: int, dt: float,
+               motion, loss: int, target_vel=None, dpos=None, dvel=None, drho=None, dnu: float = 0.0, dmotion=None):
+    """Moving-square FP64 tangent-linear model (sph_tangent.cpp, oracle_tangent_ms):
+    the loss after nsteps Euler predictor-corrector steps with the per-step body
+    motion (nsteps, 4) and its derivative along (dpos, dvel, drho, dnu, dmotion)."""
+    n = rho.shape[0]
+    a = [np.ascontiguousarray(x, np.float64) for x in (pos, vel, rho, mass)]
+    ti = [np.ascontiguousarray(x, np.int32) for x in (type_, itype, labels)]
+    mo = np.ascontiguousarray(motion, np.float64).reshape(-1)
+    d = [None if x is None else np.ascontiguousarray(x, np.float64).reshape(-1) for x in (dpos, dvel, drho, dmotion)]
+    tg = None if target_vel is None else np.ascontiguousarray(target_vel, np.float64)
+    out = np.zeros(2)
+    rc = load().oracle_tangent_ms(ctypes.byref(cfg), n, _p(a[0]), _p(a[1]), _p(a[2]), _p(a[3]),
+                                  _p(ti[0], ctypes.c_int), _p(ti[1], ctypes.c_int), _p(ti[2], ctypes.c_int),
+                                  float(t0), int(nsteps), float(dt), _p(mo), int(loss), _p(tg), _p(d[0]), _p(d[1]),
+                                  _p(d[2]), float(dnu), _p(d[3]), _p(out))
+    if rc != 0:
+        raise RuntimeError(f"oracle_tangent_ms failed ({rc})")
+    return out[0], out[1]
 
 
 def mls_reinit(cfg: SphConfig, pos, rho, mass, type_):

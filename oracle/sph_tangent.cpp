@@ -17,10 +17,14 @@
 // derivative is that of the taken branch with the pair set held fixed, which
 // is what the adjoint differentiates too.
 //
-// Scope: the modified linear Riemann delta-SPH + SPS solver, RK4 with the K1
-// reuse, periodic images, either kernel, with or without renormalisation,
-// no shifting, no XSPH, no density re-initialisation, no free-surface particles.  Other inputs return
-// SPH_E_CONFIG.  The pair search is a plain double loop (small cases only).
+// Scope: (1) Taylor-Green: the modified linear Riemann delta-SPH + SPS solver,
+// RK4 with the K1 reuse, periodic images (oracle_tangent); (2) moving square:
+// the modified linear Riemann solver with XSPH in the continuity flux, the
+// fixed-ghost assignment, the body force and the Euler predictor-corrector with
+// a per-step body motion (oracle_tangent_ms).  Either kernel, with or without
+// renormalisation, no shifting, no density re-initialisation, no free-surface
+// particles.  Other inputs return SPH_E_CONFIG.  The pair search is a plain
+// double loop (small cases only).
 
 #include <cmath>
 #include <cstring>
@@ -416,6 +420,346 @@ int run(const sph_config& cfg, int n, const T* x0, const T* y0, const T* u0, con
     return SPH_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Moving-square step (Moving_Square_Cylinder_Flow/...): the modified linear
+// Riemann solver with the XSPH velocity inside the continuity flux
+// (Solver_Normalized_Modified_Linear_Riemann_Delta.f90:100-336), the fixed-ghost
+// assignment (Assign_boundary_particles.f90:611-941, MLS order 1), the body force
+// (Calculate_Body_Force.f90:53-142) and the Euler predictor-corrector with the
+// carried rates (SPH_Time_Iteration.f90:313-394), the body moved at each step
+// start by a per-step velocity (Body_Motion_Solver.f90:187-193).  The same
+// steps, in the same pair orientation and order, as sph_oracle.cpp's
+// ms_riemann_solver / assign_ghosts / body_force / run_step_euler_pc, with the
+// masses as scalars of type T (the ghost masses are interpolated).
+// ---------------------------------------------------------------------------
+template <class T>
+struct MSParts {
+    std::vector<T> x, y, u, v, rho, mass;
+    std::vector<int> type, itype, label;
+    int n = 0;
+};
+
+template <class T>
+struct MSModel {
+    Model<T> M;
+    double t = 0.0;          // Real_physical_time of the step
+    T bvel[2], bacc[2];      // Custom_velocity, Custom_accleration of the step
+
+    bool pair_allowed(int ti, int tj) const {
+        if (M.C.pair_rule == SPH_PAIRS_ONE_FLUID) return !(ti != SPH_TYPE_WATER && tj != SPH_TYPE_WATER);
+        if (ti == -2 && tj == -2) return false;
+        if (ti == -3 && tj == -3) return false;
+        if (ti == -201 && tj == -201) return false;
+        return true;
+    }
+
+    void assign_ghosts(MSParts<T>& P, std::vector<T>& p, std::vector<T>& c, std::vector<T>& vol) const {
+        const sph_config& C = M.C;
+        const bool q = C.reference_literals != 0;
+        const double hg = (q ? (double)(float)C.ghost_h_factor : C.ghost_h_factor) * C.h;
+        const double rg = C.kernel_scale * hg;
+        for (int i = 0; i < P.n; ++i) {
+            if (P.type[i] != SPH_TYPE_FIX_GHOST) continue;
+            const bool body = P.itype[i] == SPH_TYPE_BODY;
+            const T ge0 = body ? C.gravity[0] + bacc[0] : T(C.gravity[0]);
+            const T ge1 = body ? C.gravity[1] + bacc[1] : T(C.gravity[1]);
+            std::vector<int> nb;
+            std::vector<T> W;
+            for (int j = 0; j < P.n; ++j) {
+                if (P.type[j] == SPH_TYPE_FIX_GHOST || P.type[j] == SPH_TYPE_ILL || P.type[j] == 0) continue;
+                const T pd0 = P.x[i] - P.x[j], pd1 = P.y[i] - P.y[j];
+                const T d = sqrt(pd0 * pd0 + pd1 * pd1);
+                if (!(val(d) <= rg)) continue;
+                T w, g0, g1;
+                M.kernel(d, pd0, pd1, hg, w, g0, g1);
+                nb.push_back(j);
+                W.push_back(w * P.mass[j] / P.rho[j]);
+            }
+            T pint(0.0), uint(0.0), vint(0.0), m(0.0);
+            if (nb.size() >= 3) {
+                T A(0.0);
+                for (const T& w : W) A += w;
+                const T ainv = 1.0 / A;
+                for (size_t k = 0; k < nb.size(); ++k) {
+                    const int j = nb[k];
+                    const T fai = ainv * W[k];
+                    const T pd0 = P.x[i] - P.x[j], pd1 = P.y[i] - P.y[j];
+                    pint = pint + p[j] * fai + P.rho[j] * fai * (ge0 * pd0 + ge1 * pd1);
+                    uint = uint + P.u[j] * fai;
+                    vint = vint + P.v[j] * fai;
+                    m = m + P.mass[j] * fai;
+                }
+            }
+            T u, v, pr(0.0);
+            const int lab = P.label[i];
+            if (body) {
+                u = bvel[0]; v = bvel[1]; pr = pint;
+            } else {
+                if (0.0 < t && t <= C.shock_release_time) {
+                    const T ri = (pint - C.background_p) / C.c0sq + C.rho0;
+                    const T r = ri / C.rho0;
+                    const T cc = M.K.sqrt_c0 * (r * r * r);
+                    u = uint; v = vint;
+                    if (lab == -6 || lab == -7) {
+                        const T vn = lab == -6 ? vint : uint;
+                        const T J2 = ri * cc * vn + pint, J3 = -ri * cc * vn + pint;
+                        const T vsn = (J2 - J3) / (2.0 * ri * cc);
+                        if (lab == -6) v = vsn; else u = vsn;
+                        pr = 0.5 * (J2 + J3);
+                    }
+                } else {
+                    u = uint; v = vint; pr = pint;
+                }
+                if (lab == -6) { if (C.wall_bc == 1) v = -v; else { u = -u; v = -v; } }
+                else if (lab == -7) { u = -u; v = -v; }
+                else if (lab == -8) { if (C.wall_bc == 1) u = -u; else { u = -u; v = -v; } }
+            }
+            T rho, cc;
+            if (val(m) != 0.0) {
+                rho = (pr - C.background_p) / C.c0sq + C.rho0;
+                const T r = rho / C.rho0;
+                cc = M.K.sqrt_c0 * (r * r * r);
+            } else {
+                u = T(0.0); v = T(0.0); pr = T(0.0); rho = T(C.rho0); m = T(0.0); cc = T(M.K.sqrt_c0);
+            }
+            P.u[i] = u; P.v[i] = v; P.rho[i] = rho; P.mass[i] = m;
+            p[i] = pr; c[i] = cc; vol[i] = m / rho;
+        }
+    }
+
+    // single_step_compute of the moving square: the rates of every particle and,
+    // when fx is given, the x body force of this RHS.
+    int rhs(MSParts<T>& P, std::vector<T>& drho, std::vector<T>* acc, std::vector<T>* avg, T* fx) const {
+        const sph_config& C = M.C;
+        const TConsts& K = M.K;
+        const T& nu = M.nu;
+        const int n = P.n;
+        std::vector<T> p(n), c(n), vol(n);
+        for (int i = 0; i < n; ++i) {
+            if (P.type[i] == SPH_TYPE_ILL) continue;
+            M.eos(P.rho[i], p[i], c[i]);
+        }
+        for (int i = 0; i < n; ++i) vol[i] = P.mass[i] / P.rho[i];
+        if (C.ghost_assign) assign_ghosts(P, p, c, vol);
+        const double hb = (C.h + C.h) / 2.0;
+        const double rcut = C.kernel_scale * hb;
+        std::vector<int> pi, pj;
+        for (int i = 0; i < n - 1; ++i)
+            for (int j = i + 1; j < n; ++j) {
+                if (!pair_allowed(P.type[i], P.type[j])) continue;
+                const double a = val(P.x[i]) - val(P.x[j]), b = val(P.y[i]) - val(P.y[j]);
+                if (std::fabs(a) > rcut || std::fabs(b) > rcut) continue;
+                const double d = std::sqrt(a * a + b * b);
+                if (d <= rcut && d >= K.cut_min) { pi.push_back(i); pj.push_back(j); }
+            }
+        const size_t np = pi.size();
+        std::vector<T> dx0(np), dx1(np), w(np), dw0(np), dw1(np);
+        for (size_t k = 0; k < np; ++k) {
+            const int i = pi[k], j = pj[k];
+            dx0[k] = P.x[i] - P.x[j]; dx1[k] = P.y[i] - P.y[j];
+            const T d = sqrt(dx0[k] * dx0[k] + dx1[k] * dx1[k]);
+            M.kernel(d, dx0[k], dx1[k], hb, w[k], dw0[k], dw1[k]);
+        }
+        std::vector<T> bi[4];
+        for (int q = 0; q < 4; ++q) bi[q].assign(n, T(q == 0 || q == 3 ? 1.0 : 0.0));
+        if (C.renormalize) {
+            std::vector<T> B[4];
+            for (int q = 0; q < 4; ++q) B[q].assign(n, T(0.0));
+            for (size_t k = 0; k < np; ++k) {
+                const int i = pi[k], j = pj[k];
+                const T pd[2] = {-dx0[k], -dx1[k]}, dw[2] = {dw0[k], dw1[k]};
+                for (int a = 0; a < 2; ++a)
+                    for (int o = 0; o < 2; ++o) {
+                        B[a * 2 + o][i] += pd[a] * dw[o] * vol[j];
+                        B[a * 2 + o][j] += pd[a] * dw[o] * vol[i];
+                    }
+            }
+            for (int i = 0; i < n; ++i) {
+                if (P.type[i] != SPH_TYPE_WATER) continue;
+                const T det = B[0][i] * B[3][i] - B[1][i] * B[2][i];
+                if (val(det) == 0.0) continue;
+                bi[0][i] = B[3][i] / det; bi[1][i] = -B[1][i] / det;
+                bi[2][i] = -B[2][i] / det; bi[3][i] = B[0][i] / det;
+            }
+        }
+        std::vector<T> ni0(np), ni1(np), nj0(np), nj1(np);
+        for (size_t k = 0; k < np; ++k) {
+            const int i = pi[k], j = pj[k];
+            ni0[k] = bi[0][i] * dw0[k] + bi[1][i] * dw1[k];
+            ni1[k] = bi[2][i] * dw0[k] + bi[3][i] * dw1[k];
+            nj0[k] = bi[0][j] * dw0[k] + bi[1][j] * dw1[k];
+            nj1[k] = bi[2][j] * dw0[k] + bi[3][j] * dw1[k];
+        }
+        // grad rho (:100-112) and the XSPH average velocity (:114-121)
+        std::vector<T> g0(n, T(0.0)), g1(n, T(0.0));
+        for (int a = 0; a < 2; ++a) avg[a].assign(n, T(0.0));
+        for (size_t k = 0; k < np; ++k) {
+            const int i = pi[k], j = pj[k];
+            const T dr = -(P.rho[i] - P.rho[j]);
+            g0[i] += dr * vol[j] * ni0[k]; g1[i] += dr * vol[j] * ni1[k];
+            g0[j] += dr * vol[i] * nj0[k]; g1[j] += dr * vol[i] * nj1[k];
+            const T vd[2] = {P.u[i] - P.u[j], P.v[i] - P.v[j]};
+            for (int a = 0; a < 2; ++a) {
+                avg[a][i] += -(C.xsph_eps * P.mass[j] * vd[a] / (P.rho[i] + P.rho[j]) * w[k]);
+                avg[a][j] += C.xsph_eps * P.mass[i] * vd[a] / (P.rho[i] + P.rho[j]) * w[k];
+            }
+        }
+        // main pair loop (:169-336), no free surface
+        std::vector<T> cont(n, T(0.0)), a0(n, T(0.0)), a1(n, T(0.0));
+        for (size_t k = 0; k < np; ++k) {
+            const int i = pi[k], j = pj[k];
+            const T Vi = vol[i], Vj = vol[j], ri = P.rho[i], rj = P.rho[j];
+            const T cbar = (c[i] + c[j]) / 2.0, rbar = (ri + rj) / 2.0;
+            const T Pbar = (p[i] + p[j]) / 2.0;
+            const T vbar0 = (P.u[i] + P.u[j]) / 2.0, vbar1 = (P.v[i] + P.v[j]) / 2.0;
+            const T r2 = dx0[k] * dx0[k] + dx1[k] * dx1[k];
+            const T d = sqrt(r2);
+            const T e0 = -dx0[k] / d, e1 = -dx1[k] / d;
+            const T UL = P.u[i] * e0 + P.v[i] * e1, UR = P.u[j] * e0 + P.v[j] * e1;
+            const T Ubar = (UL + UR) / 2.0;
+            const T Us = Ubar + 0.5 * (p[i] - p[j]) / (rbar * K.sqrt_c0);
+            const T vs0 = (Us - Ubar) * e0 + vbar0, vs1 = (Us - Ubar) * e1 + vbar1;
+            const T dU = UL - UR;
+            const T m3 = val(dU) > 0.0 ? 3.0 * dU : T(0.0);
+            const T bR = val(m3) < val(cbar) ? m3 : cbar;
+            const T Ps = Pbar + 0.5 * bR * rbar * dU;
+            const T vdi0 = P.u[i] - vs0 + avg[0][i] - avg[0][j], vdi1 = P.v[i] - vs1 + avg[1][i] - avg[1][j];
+            const T vdj0 = P.u[j] - vs0 + avg[0][j] - avg[0][i], vdj1 = P.v[j] - vs1 + avg[1][j] - avg[1][i];
+            const T tmi = vdi0 * ni0[k] + vdi1 * ni1[k];
+            const T tmj = -(vdj0 * nj0[k] + vdj1 * nj1[k]);
+            cont[i] += 2.0 * ri * Vj * tmi;
+            cont[j] += 2.0 * rj * Vi * tmj;
+            const T rij = 1.0 / (ri * rj);
+            a0[i] += P.mass[j] * (-2.0 * Ps * ni0[k] * rij);
+            a1[i] += P.mass[j] * (-2.0 * Ps * ni1[k] * rij);
+            a0[j] += -(P.mass[i] * (-2.0 * Ps * nj0[k] * rij));
+            a1[j] += -(P.mass[i] * (-2.0 * Ps * nj1[k] * rij));
+            const T vij0 = P.u[i] - P.u[j], vij1 = P.v[i] - P.v[j];
+            const T vx = vij0 * dx0[k] + vij1 * dx1[k];
+            if (val(vx) < 0.0) {
+                const double fh = C.fai * hb;
+                const T phi = hb * vx / (r2 + fh * fh);
+                const T Pi = (-C.alpha * cbar * phi + C.beta * (phi * phi)) / rbar;
+                a0[i] += P.mass[j] * (-Pi * ni0[k]); a1[i] += P.mass[j] * (-Pi * ni1[k]);
+                a0[j] += -(P.mass[i] * (-Pi * nj0[k])); a1[j] += -(P.mass[i] * (-Pi * nj1[k]));
+            }
+            const T rdi = dx0[k] * ni0[k] + dx1[k] * ni1[k], rdj = dx0[k] * nj0[k] + dx1[k] * nj1[k];
+            a0[i] += Vj * 2.0 * nu * rdi / r2 * vij0; a1[i] += Vj * 2.0 * nu * rdi / r2 * vij1;
+            a0[j] += -(Vi * 2.0 * nu * rdj / r2 * vij0); a1[j] += -(Vi * 2.0 * nu * rdj / r2 * vij1);
+            const T tt = C.delta_alpha * hb * cbar * vx / r2;
+            a0[i] += tt * ni0[k] * C.rho0 / ri * Vj; a1[i] += tt * ni1[k] * C.rho0 / ri * Vj;
+            a0[j] += -(tt * nj0[k] * C.rho0 / rj * Vi); a1[j] += -(tt * nj1[k] * C.rho0 / rj * Vi);
+        }
+        // delta-SPH (:531-545)
+        std::vector<T> corr(n, T(0.0));
+        for (size_t k = 0; k < np; ++k) {
+            const int i = pi[k], j = pj[k];
+            const T pd0 = -dx0[k], pd1 = -dx1[k];
+            const T r2 = pd0 * pd0 + pd1 * pd1;
+            const T dr = -(P.rho[i] - P.rho[j]);
+            const T psi = dr - 0.5 * ((g0[i] + g0[j]) * pd0 + (g1[i] + g1[j]) * pd1);
+            const T tmi = (pd0 * ni0[k] + pd1 * ni1[k]) / r2, tmj = (pd0 * nj0[k] + pd1 * nj1[k]) / r2;
+            const T cbar = (c[i] + c[j]) / 2.0;
+            corr[i] += 2.0 * C.delta * hb * cbar * psi * tmi * vol[j];
+            corr[j] += -(2.0 * C.delta * hb * cbar * psi * tmj * vol[i]);
+        }
+        drho.assign(n, T(0.0)); acc[0].assign(n, T(0.0)); acc[1].assign(n, T(0.0));
+        for (int i = 0; i < n; ++i) {
+            drho[i] = cont[i];
+            if (P.type[i] != SPH_TYPE_WATER) continue;
+            acc[0][i] = a0[i]; acc[1][i] = a1[i];
+            drho[i] = drho[i] + corr[i];
+        }
+        if (fx) {
+            // Calculate_Body_Force, x component of the total (Morris laplacian)
+            std::vector<T> bp(n, T(0.0)), bv(n, T(0.0));
+            std::vector<int> nearb(n, 0);
+            for (size_t k = 0; k < np; ++k) {
+                const int i = pi[k], j = pj[k];
+                if (P.itype[i] != SPH_TYPE_BODY && P.itype[j] != SPH_TYPE_BODY) continue;
+                const T vij0 = P.u[i] - P.u[j];
+                const T r2 = dx0[k] * dx0[k] + dx1[k] * dx1[k];
+                if (P.itype[j] == SPH_TYPE_BODY) {
+                    nearb[i] = 1;
+                    bp[i] = bp[i] - vol[j] * (p[i] + p[j]) * ni0[k];
+                    const T rd = dx0[k] * ni0[k] + dx1[k] * ni1[k];
+                    bv[i] = bv[i] + P.rho[i] * vol[j] * 2.0 * nu * rd / r2 * vij0;
+                }
+                if (P.itype[i] == SPH_TYPE_BODY) {
+                    nearb[j] = 1;
+                    bp[j] = bp[j] + vol[i] * (p[i] + p[j]) * nj0[k];
+                    const T rd = dx0[k] * nj0[k] + dx1[k] * nj1[k];
+                    bv[j] = bv[j] - P.rho[j] * vol[i] * 2.0 * nu * rd / r2 * vij0;
+                }
+            }
+            T f(0.0);
+            for (int i = 0; i < n; ++i)
+                if (nearb[i]) f = f + vol[i] * (bp[i] + bv[i] + 0.0);
+            *fx = f;
+        }
+        return SPH_OK;
+    }
+};
+
+// nsteps Euler predictor-corrector steps of the moving square; motion[4s..4s+3]
+// is step s's body velocity and acceleration.  Returns the final state in H and
+// the drag impulse sum_s dt F_x(s) in drag.
+template <class T>
+int run_ms(const sph_config& cfg, MSParts<T>& H, const T& nu, const std::vector<T>& motion, double t0, int nsteps,
+           double dt, T& drag) {
+    MSModel<T> S;
+    S.M.C = cfg;
+    S.M.K = derive(cfg);
+    S.M.nu = nu;
+    const int n = H.n;
+    std::vector<T> rdrho, racc[2], ravg[2];
+    double t = t0;
+    drag = T(0.0);
+    for (int s = 0; s < nsteps; ++s) {
+        t += dt;
+        S.t = t;
+        S.bvel[0] = motion[4 * s]; S.bvel[1] = motion[4 * s + 1];
+        S.bacc[0] = motion[4 * s + 2]; S.bacc[1] = motion[4 * s + 3];
+        if (cfg.ghost_assign)
+            for (int i = 0; i < n; ++i)
+                if (H.itype[i] == SPH_TYPE_BODY) { H.x[i] = H.x[i] + S.bvel[0] * dt; H.y[i] = H.y[i] + S.bvel[1] * dt; }
+        MSParts<T> P = H;
+        const MSParts<T> B0 = H;
+        std::vector<T> dr, a[2], g[2];
+        int rc;
+        if (s == 0) {
+            if ((rc = S.rhs(P, dr, a, g, nullptr))) return rc;
+        } else {
+            dr = rdrho; a[0] = racc[0]; a[1] = racc[1]; g[0] = ravg[0]; g[1] = ravg[1];
+        }
+        const std::vector<T> td = dr, ta0 = a[0], ta1 = a[1], tv0 = P.u, tv1 = P.v;
+        for (int i = 0; i < n; ++i) {
+            if (P.type[i] != SPH_TYPE_WATER) continue;
+            P.rho[i] = B0.rho[i] + dr[i] * dt;
+            P.x[i] = B0.x[i] + dt * (P.u[i] + g[0][i]) + 0.5 * a[0][i] * (dt * dt);
+            P.y[i] = B0.y[i] + dt * (P.v[i] + g[1][i]) + 0.5 * a[1][i] * (dt * dt);
+            P.u[i] = B0.u[i] + dt * a[0][i];
+            P.v[i] = B0.v[i] + dt * a[1][i];
+        }
+        T fx;
+        if ((rc = S.rhs(P, dr, a, g, &fx))) return rc;
+        drag = drag + dt * fx;
+        for (int i = 0; i < n; ++i) {
+            if (P.type[i] != SPH_TYPE_WATER) continue;
+            P.rho[i] = B0.rho[i] + 0.5 * (dr[i] + td[i]) * dt;
+            P.x[i] = B0.x[i] + 0.5 * dt * (P.u[i] + tv0[i]) + g[0][i] * dt + 0.5 * a[0][i] * (dt * dt);
+            P.y[i] = B0.y[i] + 0.5 * dt * (P.v[i] + tv1[i]) + g[1][i] * dt + 0.5 * a[1][i] * (dt * dt);
+            P.u[i] = B0.u[i] + 0.5 * dt * (a[0][i] + ta0[i]);
+            P.v[i] = B0.v[i] + 0.5 * dt * (a[1][i] + ta1[i]);
+        }
+        rdrho = dr; racc[0] = a[0]; racc[1] = a[1]; ravg[0] = g[0]; ravg[1] = g[1];
+        for (int i = 0; i < n; ++i) {
+            H.x[i] = P.x[i]; H.y[i] = P.y[i]; H.u[i] = P.u[i]; H.v[i] = P.v[i]; H.rho[i] = P.rho[i];
+        }
+    }
+    return SPH_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -463,6 +807,61 @@ int oracle_tangent(const sph_config* cfg, int n, const double* pos, const double
         if (vel_out) { vel_out[i] = st[2][i].v; vel_out[n + i] = st[3][i].v; }
         if (rho_out) rho_out[i] = st[4][i].v;
     }
+    return SPH_OK;
+}
+
+// The moving-square tangent-linear model: nsteps steps from (pos, vel, rho) at
+// time t0 with the initial types, wall labels and per-step body motion
+// (motion[4*nsteps]), along the direction (dpos, dvel, drho, dnu, dmotion) (any
+// array may be NULL = zero).  out[0] = loss (SPH_LOSS_KINETIC_ENERGY,
+// SPH_LOSS_VELOCITY_MISFIT or SPH_LOSS_DRAG), out[1] = its directional derivative.
+int oracle_tangent_ms(const sph_config* cfg, int n, const double* pos, const double* vel, const double* rho,
+                      const double* mass, const int* type, const int* itype, const int* labels, double t0,
+                      int nsteps, double dt, const double* motion, int loss, const double* target_vel,
+                      const double* dpos, const double* dvel, const double* drho, double dnu, const double* dmotion,
+                      double* out) {
+    if (!cfg || !pos || !vel || !rho || !mass || !type || !itype || !motion || !out || n <= 0 || nsteps <= 0)
+        return SPH_E_ARG;
+    if (cfg->solver != SPH_SOLVER_MS_MODLR_DELTA || cfg->integrator != SPH_INTEGRATOR_EULER_PC || cfg->shifting ||
+        cfg->mls_order != 0 || cfg->laplacian != 1 || cfg->free_surface || cfg->periodic)
+        return SPH_E_CONFIG;
+    for (int i = 0; i < n; ++i)
+        if (type[i] <= SPH_TYPE_INLET) return SPH_E_CONFIG;
+    if (loss == SPH_LOSS_VELOCITY_MISFIT && !target_vel) return SPH_E_ARG;
+    MSParts<Dual> H;
+    H.n = n;
+    for (int i = 0; i < n; ++i) {
+        H.x.push_back(Dual(pos[i], dpos ? dpos[i] : 0.0));
+        H.y.push_back(Dual(pos[n + i], dpos ? dpos[n + i] : 0.0));
+        H.u.push_back(Dual(vel[i], dvel ? dvel[i] : 0.0));
+        H.v.push_back(Dual(vel[n + i], dvel ? dvel[n + i] : 0.0));
+        H.rho.push_back(Dual(rho[i], drho ? drho[i] : 0.0));
+        H.mass.push_back(Dual(mass[i], 0.0));
+        H.type.push_back(type[i]);
+        H.itype.push_back(itype[i]);
+        H.label.push_back(labels ? labels[i] : 0);
+    }
+    std::vector<Dual> mo(4 * (size_t)nsteps);
+    for (size_t k = 0; k < mo.size(); ++k) mo[k] = Dual(motion[k], dmotion ? dmotion[k] : 0.0);
+    Dual drag;
+    int rc = run_ms<Dual>(*cfg, H, Dual(cfg->nu, dnu), mo, t0, nsteps, dt, drag);
+    if (rc) return rc;
+    Dual L(0.0, 0.0);
+    if (loss == SPH_LOSS_DRAG) {
+        L = drag;
+    } else {
+        for (int i = 0; i < n; ++i) {
+            if (type[i] != SPH_TYPE_WATER) continue;
+            if (loss == SPH_LOSS_VELOCITY_MISFIT) {
+                const Dual a = H.u[i] - target_vel[i], b = H.v[i] - target_vel[n + i];
+                L += a * a + b * b;
+            } else {
+                L += 0.5 * mass[i] * (H.u[i] * H.u[i] + H.v[i] * H.v[i]);
+            }
+        }
+    }
+    out[0] = L.v;
+    out[1] = L.d;
     return SPH_OK;
 }
 

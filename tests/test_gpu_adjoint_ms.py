@@ -180,3 +180,38 @@ def test_moving_square_adjoint_rejects_unsupported(lib):
         with pytest.raises(S.SphError) as e:
             sim.adjoint_forward(2, 1e-4, loss=S.LOSS_DRAG)
         assert e.value.code == -7
+
+
+@pytest.mark.parametrize("loss", [S.LOSS_DRAG, S.LOSS_KINETIC_ENERGY])
+def test_moving_square_adjoint_matches_cpu_tangent_linear_reference(lib, oracle, loss):
+    """g.delta from the GPU adjoint against the FP64 CPU tangent-linear model of
+    the same steps (oracle/sph_tangent.cpp, oracle_tangent_ms) along directions
+    in the initial velocity, position and density, the viscosity and the body
+    motion: both are exact derivatives of the same discrete map (1e-8)."""
+    case, ity = S.make_moving_square(dx=0.1, lx=2.0, ly=1.0, D=0.4, solver=S.SOLVER_MS_MODLR_DELTA,
+                                     jitter=0.05, seed=8)
+    water = np.r_[case.type, case.type] == S.TYPE_WATER
+    case.vel = case.vel + np.where(water, S.fourier_perturbation(case.pos, n_modes=4, amp=0.2, seed=8), 0.0)
+    cfg = case.cfg
+    cfg.ghost_assign, cfg.shifting, cfg.mls_order = 1, 0, 0
+    lab = S.moving_square_labels(case, ity)
+    dt = 0.25 * cfg.h / np.sqrt(cfg.c0sq)
+    motion, _ = S.body_motion_schedule([0.5, 0.3, -0.1], NSTEPS, dt, period=NSTEPS * dt)
+    L, g, gm, _, _ = _grad(case, ity, lab, dt, motion, loss)
+    n = case.n
+    rng = np.random.default_rng(500)
+    dmo = np.zeros_like(motion)
+    dmo[:, 0] = rng.standard_normal(NSTEPS)
+    dmo[:, 1] = rng.standard_normal(NSTEPS)
+    dmo[:, 2] = rng.standard_normal(NSTEPS) * 10.0
+    dirs = [dict(dvel=rng.standard_normal(2 * n) * 0.1), dict(dpos=rng.standard_normal(2 * n) * 0.01 * cfg.dx),
+            dict(drho=rng.standard_normal(n) * 1e-3), dict(dnu=1.0), dict(dmotion=dmo)]
+    for d in dirs:
+        Lt, dLt = oracle.tangent_ms(cfg, case.pos, case.vel, case.rho, case.mass, case.type, ity, lab, 0.0, NSTEPS,
+                                    dt, motion, loss, **d)
+        assert Lt == pytest.approx(L, rel=1e-10)
+        key = list(d)[0]
+        ad = {"dvel": lambda: float(g["vel0"] @ d["dvel"]), "dpos": lambda: float(g["pos0"] @ d["dpos"]),
+              "drho": lambda: float(g["rho0"] @ d["drho"]), "dnu": lambda: g["nu"],
+              "dmotion": lambda: float(np.sum(gm * d["dmotion"]))}[key]()
+        assert abs(ad - dLt) <= 1e-8 * abs(dLt), (key, ad, dLt)
