@@ -252,9 +252,10 @@ def run_native(args, rank, world, local):
             "peak_kind": pk_kind + " (burst copy)"}
 
     # ---- adjoint cost (rank 0) -------------------------------------------------
-    adj = None
+    adj = adj_ms = None
     if rank == 0 and not args.skip_adjoint:
         adj = adjoint_report(S)
+        adj_ms = adjoint_ms_report(S)
 
     # ---- CPU baseline (rank 0 only, N = 1) ----------------------------------
     cpu = None
@@ -277,6 +278,7 @@ def run_native(args, rank, world, local):
         "accuracy": accuracy,
         "adjoint_over_forward": adj["adjoint_over_forward"] if adj else None,
         "adjoint": adj,
+        "adjoint_moving_square": adj_ms,
         "passes_ms_per_step": {
             "images": tm.images_ms / steps, "sort_lists": tm.sort_ms / steps,
             "pass_a": tm.pass_a_ms / steps, "surface": tm.surface_ms / steps,
@@ -363,6 +365,101 @@ def adjoint_report(S):
         "grad_vel0_l2_mixed_vs_fp64": float(np.linalg.norm(gm - g64) / np.linalg.norm(g64)),
         "dnu_mixed": m["grad"]["nu"], "dnu_fp64": d["grad"]["nu"],
         "fd_rel_err_fp64": fd_err, "fd": "central differences eps=1e-6, FP64 forward, 2 seeded directions",
+    }
+
+
+MS_DX, MS_STEPS, MS_EVERY, MS_FD_STEPS = 0.02, 2000, 64, 200
+MS_COEFFS = (1.0, 0.2, -0.1, 0.05, 0.02)
+
+
+def adjoint_ms_report(S):
+    """Cost and check of the moving-square adjoint: square of side D = 1 in a
+    [0,10] x [0,5] tank of still water, dx = D/50 (~125k particles with 4 ghost
+    layers), Re = 100, modified linear Riemann + delta-SPH (the adjoint's
+    moving-square solver), ghost assignment every RHS, Euler predictor-corrector,
+    FP64; 2,000 steps with a checkpoint every 64.  Motion u(t) = a0 + sum_k a_k
+    sin(2 pi k t / T) over the run time T; loss = time-averaged drag coefficient
+    sum_s dt F_x / (T F0), F0 = rho0 U^2 D / 2.  Forward = the same steps with
+    one checkpoint (sph_adjoint_forward, checkpoint_every = nsteps).  The
+    gradient with respect to a0 and a1 is checked by central differences on the
+    first 200 steps of the same case: the improved Gaussian's gradient does not
+    vanish at its 3h cut-off, so the right-hand side jumps whenever a pair
+    crosses the support, and over thousands of steps so many crossings move by
+    a step inside any difference interval that the difference quotient no
+    longer measures the derivative (the adjoint's is that of the taken pair
+    sets)."""
+    case, ity = S.make_moving_square(dx=MS_DX, lx=10.0, ly=5.0, D=1.0, U=1.0, solver=S.SOLVER_MS_MODLR_DELTA)
+    cfg = case.cfg
+    cfg.ghost_assign, cfg.shifting, cfg.mls_order = 1, 0, 0
+    lab = S.moving_square_labels(case, ity)
+    dt = 0.25 * cfg.h / np.sqrt(cfg.c0sq)
+    T = MS_STEPS * dt
+    scale = 1.0 / (T * 0.5 * cfg.rho0 * 1.0 * 1.0)
+    coeffs = np.array(MS_COEFFS)
+    motion, jac = S.body_motion_schedule(coeffs, MS_STEPS, dt, period=T)
+
+    def reset(sim):
+        # sph_set_state clears the body marks, the wall labels and the time
+        sim.set_state(case.pos, case.vel, case.rho, case.mass, case.type)
+        sim.set_initial_type(ity)
+        sim.set_boundary_labels(lab)
+        sim.set_time(0.0)
+
+    def new_sim():
+        sim = S.Simulation(cfg, case.n)
+        reset(sim)
+        return sim
+
+    def loss_of(mo, nsteps):
+        with new_sim() as sim:
+            return scale * sim.adjoint_forward(nsteps, dt, checkpoint_every=MS_EVERY, loss=S.LOSS_DRAG,
+                                               body_motion=mo)
+
+    out = {}
+    with new_sim() as sim:
+        for rep in range(2):          # the first round warms up allocations
+            reset(sim)
+            t0 = time.perf_counter()
+            sim.adjoint_forward(MS_STEPS, dt, checkpoint_every=MS_STEPS, loss=S.LOSS_DRAG, body_motion=motion)
+            t_fwd = time.perf_counter() - t0
+            reset(sim)
+            t0 = time.perf_counter()
+            L = sim.adjoint_forward(MS_STEPS, dt, checkpoint_every=MS_EVERY, loss=S.LOSS_DRAG, body_motion=motion)
+            t_fck = time.perf_counter() - t0
+            sim.reset_timings()
+            t0 = time.perf_counter()
+            g = sim.adjoint_backward(scale)
+            gm = sim.adjoint_motion_gradient()
+            t_bwd = time.perf_counter() - t0
+            tb = sim.timings()
+    gc = np.einsum("sq,sqk->k", gm, jac)
+    # the check on the first MS_FD_STEPS steps (same schedule, same scale)
+    nf = MS_FD_STEPS
+    with new_sim() as sim:
+        sim.adjoint_forward(nf, dt, checkpoint_every=MS_EVERY, loss=S.LOSS_DRAG, body_motion=motion[:nf])
+        sim.adjoint_backward(scale)
+        gcf = np.einsum("sq,sqk->k", sim.adjoint_motion_gradient(), jac[:nf])
+    fd = []
+    for k in (0, 1):
+        eps = 1e-6
+        cp, cm = coeffs.copy(), coeffs.copy()
+        cp[k] += eps
+        cm[k] -= eps
+        f = (loss_of(S.body_motion_schedule(cp, MS_STEPS, dt, period=T)[0][:nf], nf)
+             - loss_of(S.body_motion_schedule(cm, MS_STEPS, dt, period=T)[0][:nf], nf)) / (2 * eps)
+        fd.append({"coefficient": k, "adjoint": float(gcf[k]), "fd": f, "rel_err": abs(gcf[k] - f) / abs(f)})
+    return {
+        "case": f"moving square D=1 in [0,10]x[0,5], dx=D/50 ({case.n} particles incl. ghosts), Re=100, "
+                f"MS modified linear Riemann + delta-SPH, ghost assignment, Euler PC, FP64, {MS_STEPS} steps, "
+                f"checkpoint every {MS_EVERY}, motion a0 + 4 Fourier coefficients {list(MS_COEFFS)}",
+        "loss": "time-averaged drag coefficient", "mean_drag_coefficient": scale * L,
+        "forward_s": t_fwd, "forward_checkpointed_s": t_fck, "backward_s": t_bwd,
+        "adjoint_over_forward": t_bwd / t_fwd,
+        "forward_particle_steps_per_s": case.n * MS_STEPS / t_fwd,
+        "adjoint_particle_steps_per_s": case.n * MS_STEPS / t_bwd,
+        "backward_device_ms": tb.total_ms, "backward_reverse_kernels_ms": tb.adjoint_ms,
+        "dC_d_coeffs": [float(x) for x in gc], "dC_dnu": g["nu"], "fd": fd,
+        "fd_note": f"central differences eps=1e-6 of the FP64 forward over the first {MS_FD_STEPS} steps",
     }
 
 

@@ -86,13 +86,22 @@ __device__ __forceinline__ void kernel_g(const Params& P, double d, double& G, d
     }
 }
 
-// Kernel value W(d) of compute_kernel (its d-derivative is G(d) d).
-__device__ __forceinline__ double kernel_w(const Params& P, double d) {
-    const double q = d / P.h;
-    if (P.kernel_model == SPH_KERNEL_GAUSSIAN) return (exp(-(q * q)) - P.gauss_e9) * P.kfactor;
-    const double t = 1.0 - 0.5 * q;
-    const double t2 = t * t;
-    return P.kfactor * (1.0 + 2.0 * q) * (t2 * t2);
+// kernel_g and the kernel value W(d) of compute_kernel (whose d-derivative is
+// G(d) d) from one exponential.
+__device__ __forceinline__ void kernel_gw(const Params& P, double d, double& G, double& dG, double& W) {
+    const double h = P.h, q = d / h, kf = P.kfactor;
+    if (P.kernel_model == SPH_KERNEL_GAUSSIAN) {
+        const double ex = exp(-(q * q));
+        G = -2.0 * kf * ex / (h * h);
+        dG = 4.0 * kf * q * ex / (h * h * h);
+        W = (ex - P.gauss_e9) * kf;
+    } else {
+        const double t = 1.0 - 0.5 * q;
+        const double t2 = t * t;
+        G = -5.0 * kf * t2 * t / (h * h);
+        dG = 7.5 * kf * t2 / (h * h * h);
+        W = kf * (1.0 + 2.0 * q) * (t2 * t2);
+    }
 }
 
 // dp/drho and dc/drho of eos64.
@@ -531,14 +540,11 @@ __device__ __forceinline__ void stage_reverse(const Params& P, const Sorted<R>& 
 }
 
 // f = V_b G(d) [sum_phi (phi_b - phi_a) mu_phi.r - r^T M r]: the adjoint-weighted
-// pair term of pass A's raw sums at particle a.  Returns f / V_b and its
-// gradient with respect to r divided by V_b.
-__device__ __forceinline__ void rev_rawsum(const Params& P, double r0, double r1, double dr, double du, double dv,
-                                           const double4& m1, const double4& m2, const double2& m3, double& S_G,
-                                           double& fr0, double& fr1, double& G) {
-    const double d = sqrt(r0 * r0 + r1 * r1);
-    double dG;
-    kernel_g(P, d, G, dG);
+// pair term of pass A's raw sums at particle a, with G = G(d), dG = G'(d),
+// d = |r|.  Returns f / V_b and its gradient with respect to r divided by V_b.
+__device__ __forceinline__ void rev_rawsum(double r0, double r1, double d, double G, double dG, double dr,
+                                           double du, double dv, const double4& m1, const double4& m2,
+                                           const double2& m3, double& S_G, double& fr0, double& fr1) {
     const double c0 = dr * m1.x + du * m1.z + dv * m2.x;   // sum_phi dphi mu_phi (x)
     const double c1 = dr * m1.y + du * m1.w + dv * m2.y;
     const double Mr0 = m2.z * r0 + m2.w * r1, Mr1 = m3.x * r0 + m3.y * r1;
@@ -580,11 +586,10 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_a(Params P, Sorted<R> D, Ad
         const double2 xb = D.pos[b];
         const double4 kb = D.kin[b];
         const double r0 = xc.x - xb.x, r1 = xc.y - xb.y;
+        const double d = sqrt(r0 * r0 + r1 * r1);
+        double G, dG, W;
+        kernel_gw(P, d, G, dG, W);
         if (MS) {
-            const double d = sqrt(r0 * r0 + r1 * r1);
-            double G, dG;
-            kernel_g(P, d, G, dG);
-            const double W = kernel_w(P, d);
             const double mb = D.mass[b];
             const double rs = kc.z + kb.z, irs = 1.0 / rs;
             const double2 g = A.gavg[b], l = lg[b];
@@ -608,8 +613,8 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_a(Params P, Sorted<R> D, Ad
         // own sums: phi_b - phi_c, weight V_b
         {
             const double Vbn = D.mass[b] / kb.z;
-            double S, f0, f1, G;
-            rev_rawsum(P, r0, r1, kb.z - kc.z, kb.x - kc.x, kb.y - kc.y, mc1, mc2, mc3, S, f0, f1, G);
+            double S, f0, f1;
+            rev_rawsum(r0, r1, d, G, dG, kb.z - kc.z, kb.x - kc.x, kb.y - kc.y, mc1, mc2, mc3, S, f0, f1);
             x0b += Vbn * f0; x1b += Vbn * f1;
             rb -= Vbn * G * (mc1.x * r0 + mc1.y * r1);
             ub -= Vbn * G * (mc1.z * r0 + mc1.w * r1);
@@ -619,8 +624,8 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_a(Params P, Sorted<R> D, Ad
         {
             const double4 mb1 = A.mu1[b], mb2 = A.mu2[b];
             const double2 mb3 = A.mu3[b];
-            double S, f0, f1, G;
-            rev_rawsum(P, -r0, -r1, kc.z - kb.z, kc.x - kb.x, kc.y - kb.y, mb1, mb2, mb3, S, f0, f1, G);
+            double S, f0, f1;
+            rev_rawsum(-r0, -r1, d, G, dG, kc.z - kb.z, kc.x - kb.x, kc.y - kb.y, mb1, mb2, mb3, S, f0, f1);
             x0b -= Vc * f0; x1b -= Vc * f1;
             rb -= Vc * G * (mb1.x * r0 + mb1.y * r1);
             ub -= Vc * G * (mb1.z * r0 + mb1.w * r1);
@@ -816,13 +821,14 @@ __global__ void k_adj_seed(int n, int kind, double dloss, const int* type, const
 // r = x_a - x_b, L = B_a^-1 r, Q = r.L.  Thread c adds the derivative with
 // respect to its inputs as particle a (its body neighbours b) and, for a body
 // particle, as particle b (its neighbours a), to the state adjoints of the RHS;
-// dL/dnu partials per block into nu_part.
+// dL/dnu partials per block into nu_part.  Only body particles and the
+// particles k_mark_body_nbrs flagged (nflag == 2) have terms.
 template <typename R>
 __global__ void __launch_bounds__(kAdjThreads) k_adj_drag(Params P, Sorted<R> D, Adj A, double w, double* nu_part) {
     __shared__ double red[kAdjThreads];
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     double nu_sum = 0.0;
-    if (c < P.n_tot) {
+    if (c < P.n_tot && (D.itype[c] == SPH_TYPE_BODY || D.nflag[c] == 2)) {
         const bool cbody = D.itype[c] == SPH_TYPE_BODY;
         const double2 xc = D.pos[c];
         const double4 kc = D.kin[c];
@@ -896,9 +902,20 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_drag(Params P, Sorted<R> D,
     if (threadIdx.x == 0) nu_part[blockIdx.x] = red[0];
 }
 
-// Reverse of k_assign_ghosts, ghost side.  For ghost s with the adjoints of its
-// assigned state (u, v from su; rho from sr, i.e. p through rho = (p - pb)/c0^2
-// + rho0; m from sm) form the multipliers of the Shepard sums
+// Flags the pair neighbours of the body particles (nflag = 2; the flags are
+// cleared before and the ghost flags written after this kernel's use).
+template <typename R>
+__global__ void k_mark_body_nbrs(Params P, Sorted<R> D) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= P.n_tot || D.itype[b] != SPH_TYPE_BODY) return;
+    const int nn = D.npairs[b];
+    for (int e = 0; e < nn; ++e) D.nflag[(int)(D.pairs[(size_t)e * P.nbr_stride + b] & 0x7fffffffu)] = 2;
+}
+
+// Reverse of k_assign_ghosts, ghost side, one warp per ghost as in the forward
+// kernel.  For ghost s with the adjoints of its assigned state (u, v from su; rho
+// from sr, i.e. p through rho = (p - pb)/c0^2 + rho0; m from sm) form the
+// multipliers of the Shepard sums
 //   lam_phi = phibar_int / sum W  (phi = p, u, v, m),
 //   lam_w   = -sum_phi lam_phi phi_int        (the normalisation),
 // after the reverse of the label mirror and of the shock-release branch (whose
@@ -906,144 +923,161 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_drag(Params P, Sorted<R> D,
 // pressure 0 for other labels).  Body ghosts: u, v are the body velocity, whose
 // adjoint is summed per block with the adjoint of the body acceleration (the
 // g.(x - x_j) pressure term) into part[4 blocks].  A second gather gives the
-// ghost's position adjoint.  The ghost's su, sr, sm are consumed (the ghost
-// state a step starts from is overwritten before use).  Without library ghost
-// assignment the ghost states are the caller's, constant from step to step, and
-// their adjoints pass through to the step start untouched.
+// ghost's position adjoint and flags (nflag = 1) the particles it interpolates
+// from for k_adj_ghost_water.  The ghost's su, sr, sm are consumed (the ghost
+// state a step starts from is overwritten before use).  Only launched with the
+// library's ghost assignment: caller-given ghost states are constant from step
+// to step and their adjoints pass through to the step start untouched.
 template <typename R>
-__global__ void __launch_bounds__(kAdjThreads) k_adj_ghost_lambda(Params P, Sorted<R> D, Adj A, double t,
+__global__ void __launch_bounds__(kAdjThreads) k_adj_ghost_lambda(Params P, Sorted<R> D, Adj A,
+                                                                  const int* ghost_ids, int n_ghost, double t,
                                                                   double bax, double bay, double* part) {
-    __shared__ double red[4][kAdjThreads];
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ double red[4][kAdjThreads / 32];
+    const int wg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     double bu = 0, bv = 0, ba0 = 0, ba1 = 0;
-    if (s < P.n_tot && D.type[s] == SPH_TYPE_FIX_GHOST && P.ghost_assign) {
-        double lp = 0, lu = 0, lv = 0, lm = 0, lw = 0;
-        double2 xs = make_double2(0, 0);
-        if (D.id[s] < P.n_host) {
-            const bool body = D.itype[s] == SPH_TYPE_BODY;
-            const double gxe = P.grav[0] + (body ? bax : 0.0), gye = P.grav[1] + (body ? bay : 0.0);
-            double sw = 0.0, sp = 0.0, su = 0.0, sv = 0.0, sm = 0.0;
-            int cnt = 0;
-            ghost_visit(P, D, s, [&](int b, double dx, double dy, double, double w) {
+    if (wg < n_ghost) {
+        const int s = D.slot_of[ghost_ids[wg]];
+        const bool body = D.itype[s] == SPH_TYPE_BODY;
+        const double gxe = P.grav[0] + (body ? bax : 0.0), gye = P.grav[1] + (body ? bay : 0.0);
+        double sw = 0.0, sp = 0.0, su = 0.0, sv = 0.0, sm = 0.0;
+        int cnt = 0;
+        ghost_visit_warp(P, D, s, [&](int b, double dx, double dy, double, double w) {
+            const double4 kb = D.kin[b];
+            const double mb = D.mass[b];
+            const double W = w * (mb / kb.z);
+            sw += W;
+            sp += kb.w * W + kb.z * W * (gxe * dx + gye * dy);
+            su += kb.x * W;
+            sv += kb.y * W;
+            sm += mb * W;
+            ++cnt;
+        });
+        sw = warp_sum(sw); sp = warp_sum(sp); su = warp_sum(su); sv = warp_sum(sv); sm = warp_sum(sm);
+        cnt = warp_sum(cnt);
+        double pint = 0.0, uint = 0.0, vint = 0.0, m = 0.0;
+        if (cnt >= 3) {
+            const double inv = 1.0 / sw;
+            pint = sp * inv; uint = su * inv; vint = sv * inv; m = sm * inv;
+        }
+        double lp = 0, lu = 0, lv = 0, lm = 0, lw = 0, xs0 = 0, xs1 = 0;
+        if (m != 0.0) {
+            const double2 ou = A.su[s];
+            double pbar = A.sr[s] / P.c0sq, ubar = 0.0, vbar = 0.0;
+            if (body) {
+                bu = ou.x; bv = ou.y;
+            } else {
+                const int lab = D.blabel[s];
+                double fu = 1.0, fv = 1.0;
+                if (lab == -6) { if (P.wall_bc == 1) fv = -1.0; else { fu = -1.0; fv = -1.0; } }
+                else if (lab == -7) { fu = -1.0; fv = -1.0; }
+                else if (lab == -8) { if (P.wall_bc == 1) fu = -1.0; else { fu = -1.0; fv = -1.0; } }
+                ubar = fu * ou.x; vbar = fv * ou.y;
+                if (0.0 < t && t <= P.shock_t && lab != -6 && lab != -7) pbar = 0.0;
+            }
+            const double inv = 1.0 / sw;
+            lp = pbar * inv; lu = ubar * inv; lv = vbar * inv; lm = A.sm[s] * inv;
+            lw = -(lp * pint + lu * uint + lv * vint + lm * m);
+            double a0 = 0.0, a1 = 0.0;
+            ghost_visit_warp(P, D, s, [&](int b, double dx, double dy, double q, double w) {
                 const double4 kb = D.kin[b];
                 const double mb = D.mass[b];
-                const double W = w * (mb / kb.z);
-                sw += W;
-                sp += kb.w * W + kb.z * W * (gxe * dx + gye * dy);
-                su += kb.x * W;
-                sv += kb.y * W;
-                sm += mb * W;
-                ++cnt;
+                const double Vb = mb / kb.z, W = w * Vb;
+                const double Wb = lp * (kb.w + kb.z * (gxe * dx + gye * dy)) + lu * kb.x + lv * kb.y + lm * mb + lw;
+                const double k = Wb * Vb * ghost_dw_over_d(P, q);
+                const double cg = lp * kb.z * W;
+                xs0 += k * dx + cg * gxe;
+                xs1 += k * dy + cg * gye;
+                a0 += cg * dx; a1 += cg * dy;
+                D.nflag[b] = 1;
             });
-            double pint = 0.0, uint = 0.0, vint = 0.0, m = 0.0;
-            if (cnt >= 3) {
-                const double inv = 1.0 / sw;
-                pint = sp * inv; uint = su * inv; vint = sv * inv; m = sm * inv;
-            }
-            if (m != 0.0) {
-                const double2 ou = A.su[s];
-                double pbar = A.sr[s] / P.c0sq, ubar = 0.0, vbar = 0.0;
-                if (body) {
-                    bu = ou.x; bv = ou.y;
-                } else {
-                    const int lab = D.blabel[s];
-                    double fu = 1.0, fv = 1.0;
-                    if (lab == -6) { if (P.wall_bc == 1) fv = -1.0; else { fu = -1.0; fv = -1.0; } }
-                    else if (lab == -7) { fu = -1.0; fv = -1.0; }
-                    else if (lab == -8) { if (P.wall_bc == 1) fu = -1.0; else { fu = -1.0; fv = -1.0; } }
-                    ubar = fu * ou.x; vbar = fv * ou.y;
-                    if (0.0 < t && t <= P.shock_t && lab != -6 && lab != -7) pbar = 0.0;
-                }
-                const double inv = 1.0 / sw;
-                lp = pbar * inv; lu = ubar * inv; lv = vbar * inv; lm = A.sm[s] * inv;
-                lw = -(lp * pint + lu * uint + lv * vint + lm * m);
-                ghost_visit(P, D, s, [&](int b, double dx, double dy, double q, double w) {
-                    const double4 kb = D.kin[b];
-                    const double mb = D.mass[b];
-                    const double Vb = mb / kb.z, W = w * Vb;
-                    const double Wb = lp * (kb.w + kb.z * (gxe * dx + gye * dy)) + lu * kb.x + lv * kb.y + lm * mb + lw;
-                    const double k = Wb * Vb * ghost_dw_over_d(P, q);
-                    const double cg = lp * kb.z * W;
-                    xs.x += k * dx + cg * gxe;
-                    xs.y += k * dy + cg * gye;
-                    if (body) { ba0 += cg * dx; ba1 += cg * dy; }
-                });
-            }
+            xs0 = warp_sum(xs0); xs1 = warp_sum(xs1);
+            a0 = warp_sum(a0); a1 = warp_sum(a1);
+            if (body) { ba0 = a0; ba1 = a1; }
         }
-        A.glam[s] = make_double4(lp, lu, lv, lm);
-        A.glamw[s] = lw;
-        const double2 sx = A.sx[s];
-        A.sx[s] = make_double2(sx.x + xs.x, sx.y + xs.y);
-        A.su[s] = make_double2(0, 0);
-        A.sr[s] = 0.0;
-        A.sm[s] = 0.0;
+        if (lane == 0) {
+            A.glam[s] = make_double4(lp, lu, lv, lm);
+            A.glamw[s] = lw;
+            const double2 sx = A.sx[s];
+            A.sx[s] = make_double2(sx.x + xs0, sx.y + xs1);
+            A.su[s] = make_double2(0, 0);
+            A.sr[s] = 0.0;
+            A.sm[s] = 0.0;
+        }
     }
-    red[0][threadIdx.x] = bu; red[1][threadIdx.x] = bv; red[2][threadIdx.x] = ba0; red[3][threadIdx.x] = ba1;
+    if (lane == 0) { red[0][wib] = bu; red[1][wib] = bv; red[2][wib] = ba0; red[3][wib] = ba1; }
     __syncthreads();
-    for (int k = kAdjThreads / 2; k > 0; k >>= 1) {
-        if (threadIdx.x < k)
-            for (int q = 0; q < 4; ++q) red[q][threadIdx.x] += red[q][threadIdx.x + k];
-        __syncthreads();
-    }
     if (threadIdx.x == 0)
-        for (int q = 0; q < 4; ++q) part[(size_t)q * gridDim.x + blockIdx.x] = red[q][0];
+        for (int q = 0; q < 4; ++q) {
+            double acc = 0.0;
+            for (int w = 0; w < kAdjThreads / 32; ++w) acc += red[q][w];
+            part[(size_t)q * gridDim.x + blockIdx.x] = acc;
+        }
 }
 
-// Reverse of k_assign_ghosts, interpolated side: particle j gathers the ghosts
-// whose window and radius it falls in (the same cells and the same distance test
-// as the forward: j's list-build cell within ghost_cells of the ghost's cell) and
-// adds d(sum_s lam_s . sums_s)/d(x_j, u_j, v_j, rho_j); p_j enters through the
-// equation of state, V_j = m_j / rho_j.
+// Reverse of k_assign_ghosts, interpolated side, one warp per flagged particle j:
+// the lanes split the ghosts of the window around j's list-build cell whose own
+// window and radius j falls in (the same cells and the same distance test as the
+// forward), adding d(sum_s lam_s . sums_s)/d(x_j, u_j, v_j, rho_j); p_j enters
+// through the equation of state, V_j = m_j / rho_j.
 template <typename R>
 __global__ void __launch_bounds__(kAdjThreads) k_adj_ghost_water(Params P, Sorted<R> D, Adj A, double bax,
                                                                  double bay) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= P.n_tot || D.type[j] == SPH_TYPE_FIX_GHOST) return;
+    const int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (j >= P.n_tot || D.nflag[j] == 0 || D.type[j] == SPH_TYPE_FIX_GHOST) return;    // whole warps
+    const int lane = threadIdx.x & 31;
     const double2 xj = D.pos[j], x0 = D.pos0[j];
     const int cx = (int)floor((x0.x - P.gx0) / P.cs), cy = (int)floor((x0.y - P.gy0) / P.cs);
     const double4 kj = D.kin[j];
     const double mj = D.mass[j], Vj = mj / kj.z;
     const double hg = P.ghost_h;
     double x0b = 0, x1b = 0, ub = 0, vb = 0, pb = 0, rb = 0;
+    const int gx0 = max(cx - P.ghost_cells, 0), gx1 = min(cx + P.ghost_cells, P.gnx - 1);
     for (int gy = max(cy - P.ghost_cells, 0); gy <= min(cy + P.ghost_cells, P.gny - 1); ++gy) {
         const int row = gy * P.gnx;
-        for (int gx = max(cx - P.ghost_cells, 0); gx <= min(cx + P.ghost_cells, P.gnx - 1); ++gx) {
-            const int s0 = D.cell_start[row + gx];
-            if (s0 < 0) continue;
-            const int s1 = D.cell_end[row + gx];
-            for (int s = s0; s < s1; ++s) {
-                if (D.type[s] != SPH_TYPE_FIX_GHOST || D.id[s] >= P.n_host) continue;
-                const double2 x = D.pos[s];
-                const double dx = x.x - xj.x, dy = x.y - xj.y;
-                const double d = sqrt(dx * dx + dy * dy);
-                if (!(d <= P.ghost_r)) continue;
-                const double4 lam = A.glam[s];
-                const double lw = A.glamw[s];
-                if (lam.x == 0.0 && lam.y == 0.0 && lam.z == 0.0 && lam.w == 0.0 && lw == 0.0) continue;
-                const double q = d / hg;
-                double w;
-                if (P.kernel_model == SPH_KERNEL_GAUSSIAN) {
-                    w = (exp(-(q * q)) - P.gauss_e9) * P.ghost_kf;
-                } else {
-                    const double tq = 1.0 - q / 2.0;
-                    const double t2 = tq * tq;
-                    w = P.ghost_kf * (1.0 + 2.0 * q) * (t2 * t2);
-                }
-                const bool body = D.itype[s] == SPH_TYPE_BODY;
-                const double gxe = P.grav[0] + (body ? bax : 0.0), gye = P.grav[1] + (body ? bay : 0.0);
-                const double ge = gxe * dx + gye * dy;
-                const double W = w * Vj;
-                ub += lam.y * W; vb += lam.z * W; pb += lam.x * W;
-                rb += lam.x * W * ge;
-                const double Wb = lam.x * (kj.w + kj.z * ge) + lam.y * kj.x + lam.z * kj.y + lam.w * mj + lw;
-                rb -= Wb * W / kj.z;
-                const double k = Wb * Vj * ghost_dw_over_d(P, q);
-                const double cg = lam.x * kj.z * W;
-                x0b -= k * dx + cg * gxe;
-                x1b -= k * dy + cg * gye;
+        int lo = -1, hi = -1;
+        for (int gx = gx0; gx <= gx1; ++gx) {
+            const int b0 = D.cell_start[row + gx];
+            if (b0 < 0) continue;
+            if (lo < 0) lo = b0;
+            hi = D.cell_end[row + gx];
+        }
+        if (lo < 0) continue;
+        for (int s = lo + lane; s < hi; s += 32) {
+            if (D.type[s] != SPH_TYPE_FIX_GHOST || D.id[s] >= P.n_host) continue;
+            const double2 x = D.pos[s];
+            const double dx = x.x - xj.x, dy = x.y - xj.y;
+            const double d = sqrt(dx * dx + dy * dy);
+            if (!(d <= P.ghost_r)) continue;
+            const double4 lam = A.glam[s];
+            const double lw = A.glamw[s];
+            if (lam.x == 0.0 && lam.y == 0.0 && lam.z == 0.0 && lam.w == 0.0 && lw == 0.0) continue;
+            const double q = d / hg;
+            double w;
+            if (P.kernel_model == SPH_KERNEL_GAUSSIAN) {
+                w = (exp(-(q * q)) - P.gauss_e9) * P.ghost_kf;
+            } else {
+                const double tq = 1.0 - q / 2.0;
+                const double t2 = tq * tq;
+                w = P.ghost_kf * (1.0 + 2.0 * q) * (t2 * t2);
             }
+            const bool body = D.itype[s] == SPH_TYPE_BODY;
+            const double gxe = P.grav[0] + (body ? bax : 0.0), gye = P.grav[1] + (body ? bay : 0.0);
+            const double ge = gxe * dx + gye * dy;
+            const double W = w * Vj;
+            ub += lam.y * W; vb += lam.z * W; pb += lam.x * W;
+            rb += lam.x * W * ge;
+            const double Wb = lam.x * (kj.w + kj.z * ge) + lam.y * kj.x + lam.z * kj.y + lam.w * mj + lw;
+            rb -= Wb * W / kj.z;
+            const double k = Wb * Vj * ghost_dw_over_d(P, q);
+            const double cg = lam.x * kj.z * W;
+            x0b -= k * dx + cg * gxe;
+            x1b -= k * dy + cg * gye;
         }
     }
+    x0b = warp_sum(x0b); x1b = warp_sum(x1b); ub = warp_sum(ub); vb = warp_sum(vb);
+    pb = warp_sum(pb); rb = warp_sum(rb);
+    if (lane != 0) return;
     double dp, dc;
     eos_deriv(P, kj.z, dp, dc);
     const double2 sx = A.sx[j], su = A.su[j];

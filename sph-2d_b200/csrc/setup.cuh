@@ -115,6 +115,9 @@ struct Sorted {
     using V2 = typename VT<R>::V2;
     using V4 = typename VT<R>::V4;
     int* id;          // id-order index (host index, or n_host + image number)
+    int* slot_of;     // inverse: the sorted slot of id i
+    uint8_t* nflag;   // reverse sweep: bit 0 near a ghost (within its interpolation radius),
+                      // bit 1 a pair neighbour of a body particle
     int* type;
     int* itype;       // initial type (SPH_TYPE_BODY marks the body)
     int* blabel;      // wall label of the ghost assignment (0 for images)
@@ -187,6 +190,7 @@ __global__ void k_gather_sorted(Params P, Staging S, Sorted<R> D, const unsigned
     if (s >= P.n_tot) return;
     int i = (int)perm[s];
     D.id[s] = i;
+    D.slot_of[i] = s;
     D.type[s] = S.type[i];
     D.itype[s] = S.itype[i];
     D.blabel[s] = i < P.n_host ? S.blabel[i] : 0;

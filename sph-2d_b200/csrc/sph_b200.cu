@@ -100,6 +100,7 @@ struct sph_handle {
     double bf[6] = {0, 0, 0, 0, 0, 0};   // body force of the last RHS
     double* d_bf = nullptr;               // [6 * blocks(cap_tot) partials + 6]
     bool bf_every_rhs = false;            // sph_rhs also reports it
+    bool bf_pending = false;              // the device copy is newer than bf (read on demand)
     struct AdjCtx* adj = nullptr;         // saved context of sph_adjoint_forward
     double* d_mls = nullptr;              // re-initialised densities [cap_tot]
     double t_phys = 0.0;                  // Real_physical_time (ghost assignment)
@@ -112,6 +113,9 @@ struct sph_handle {
     int sched_n = 0;
     double* drag_acc = nullptr;           // adjoint forward: += drag_w * F_x at each step's last RHS
     double drag_w = 0.0;
+    // fixed-ghost host particles (type SPH_TYPE_FIX_GHOST) in id order, from sph_set_state
+    int* d_ghost_ids = nullptr;           // [cap_host]
+    int n_ghost = 0;
 };
 
 namespace {
@@ -274,6 +278,7 @@ template <> Sorted<float>& sorted<float>(sph_handle* h) { return h->D32; }
 template <typename R>
 int alloc_sorted(Sorted<R>& D, int cap, int max_nbr, int ncells) {
     CK(dalloc(&D.id, cap)); CK(dalloc(&D.type, cap)); CK(dalloc(&D.itype, cap)); CK(dalloc(&D.blabel, cap));
+    CK(dalloc(&D.slot_of, cap)); CK(dalloc(&D.nflag, cap));
     CK(dalloc(&D.pos, cap)); CK(dalloc(&D.pos0, cap)); CK(dalloc(&D.vel0, cap)); CK(dalloc(&D.rho0, cap));
     CK(dalloc(&D.mass, cap)); CK(dalloc(&D.smass, cap));
     CK(dalloc(&D.kin, cap)); CK(dalloc(&D.aux, cap));
@@ -299,7 +304,7 @@ void free_sorted(Sorted<R>& D) {
     void* ptrs[] = {D.id, D.type, D.itype, D.blabel, D.pos, D.pos0, D.vel0, D.rho0, D.mass, D.smass, D.kin, D.aux, D.nb1, D.nb2, D.nb3,
                     D.binv, D.binv64, D.fra_v, D.flags, D.drho, D.acc, D.avg, D.shift, D.ks_r, D.ks_a, D.ks_v, D.c_drho,
                     D.c_acc, D.c_avg, D.nbr, D.nnbr, D.pairs, D.npairs, D.cell_start, D.cell_end, D.kh, D.kl,
-                    D.xhl, D.vol64};
+                    D.xhl, D.vol64, D.slot_of, D.nflag};
     for (void* p : ptrs) if (p) cudaFree(p);
     D = Sorted<R>{};
 }
@@ -398,9 +403,12 @@ int rhs(sph_handle* h, int last) {
     if (P.ghost_assign) {
         // Assign_boundary_particles at the start of single_step_compute (MS Single_step_compute.f90:73)
         tic(h, PH_UPDATE);
-        k_assign_ghosts<R><<<nb, 128, 0, h->stream>>>(P, D, h->t_phys, h->body_vel[0], h->body_vel[1],
-                                                       h->body_acc[0], h->body_acc[1]);
-        h->launches += 1;
+        if (h->n_ghost > 0) {
+            k_assign_ghosts<R><<<blocks((long long)h->n_ghost * 32, 128), 128, 0, h->stream>>>(
+                P, D, h->d_ghost_ids, h->n_ghost, h->t_phys, h->body_vel[0], h->body_vel[1], h->body_acc[0],
+                h->body_acc[1]);
+            h->launches += 1;
+        }
     }
     tic(h, PH_A);
     k_pass_a<R, true><<<nb, 128, 0, h->stream>>>(P, D);
@@ -426,7 +434,7 @@ int rhs(sph_handle* h, int last) {
         double* fin = h->d_bf + (size_t)6 * blocks(h->cap_tot, kRedThreads);
         k_body_force<R><<<nbf, kRedThreads, 0, h->stream>>>(P, D, h->d_bf);
         k_body_force_final<<<1, kRedThreads, 0, h->stream>>>(nbf, h->d_bf, fin);
-        CK(cudaMemcpyAsync(h->bf, fin, 6 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        h->bf_pending = true;
         h->launches += 2;
         if (h->drag_acc && last) {
             k_drag_acc<<<1, 32, 0, h->stream>>>(fin, h->drag_w, h->drag_acc);
@@ -552,7 +560,12 @@ int diagnostics(sph_handle* h, sph_diag* out) {
     int nsurf = 0;
     CK(cudaMemcpyAsync(v, h->d_diag, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaMemcpyAsync(&nsurf, h->d_int, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    if (h->bf_pending) {
+        const double* fin = h->d_bf + (size_t)6 * blocks(h->cap_tot, kRedThreads);
+        CK(cudaMemcpyAsync(h->bf, fin, 6 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    }
     CK(cudaStreamSynchronize(h->stream));
+    h->bf_pending = false;
     out->kinetic_energy = v[0];
     out->max_speed = v[1];
     out->n_images = h->n_img;
@@ -767,7 +780,9 @@ int adj_prepare_ctx(sph_handle* h, const sph_adj_config* ac) {
         if ((rc = adj_alloc(X, &A.lg[0], nt)) || (rc = adj_alloc(X, &A.lg[1], nt)) ||
             (rc = adj_alloc(X, &A.lk_g, nh)) || (rc = adj_alloc(X, &A.gavg, nt)) || (rc = adj_alloc(X, &A.sm, nt)) ||
             (rc = adj_alloc(X, &A.glam, nt)) || (rc = adj_alloc(X, &A.glamw, nt)) ||
-            (rc = adj_alloc(X, &A.mo_part, (size_t)4 * blocks((long long)nt, kAdjThreads))) ||
+            // per-block partials: k_adj_ghost_lambda (4 per block of 4 ghosts), k_adj_body_pos (2 per block of 256)
+            (rc = adj_alloc(X, &A.mo_part, std::max((size_t)4 * blocks((long long)nh * 32, kAdjThreads),
+                                                    (size_t)2 * blocks((long long)nt, 256)))) ||
             (rc = adj_alloc(X, &X->drag_acc, 1)))
             return rc;
     }
@@ -974,35 +989,41 @@ int adj_rhs_ms(sph_handle* h, const Sorted<R>& V, int k, int pred, bool drag, in
     Adj& A = X->A;
     const int nb = blocks(P.n_tot, kAdjThreads);
     const int nbc = blocks((long long)P.n_tot * kAdjLanes, kAdjThreads);
+    const bool ghosts = P.ghost_assign && h->n_ghost > 0;
     tic(h, PH_A);
-    if (P.ghost_assign) {
-        k_assign_ghosts<R><<<nb, 128, 0, h->stream>>>(P, V, h->t_phys, h->body_vel[0], h->body_vel[1],
-                                                       h->body_acc[0], h->body_acc[1]);
+    if (ghosts) {
+        k_assign_ghosts<R><<<blocks((long long)h->n_ghost * 32, 128), 128, 0, h->stream>>>(
+            P, V, h->d_ghost_ids, h->n_ghost, h->t_phys, h->body_vel[0], h->body_vel[1], h->body_acc[0],
+            h->body_acc[1]);
         h->launches += 1;
     }
     k_pass_a<R, false><<<nb, 128, 0, h->stream>>>(P, V);
     k_surface<R><<<nb, 128, 0, h->stream>>>(P, V);
     k_near<R><<<nb, 128, 0, h->stream>>>(P, V);
     tic(h, PH_ADJ);
+    CK(cudaMemsetAsync(V.nflag, 0, (size_t)P.n_tot, h->stream));
     k_adj_c<R, true><<<nbc, kAdjThreads, 0, h->stream>>>(P, V, A, A.lr[k], A.la[k], A.nu_part + (size_t)k * nbc);
     if (drag) {
         double* part = A.nu_part + (size_t)4 * nbc;
+        k_mark_body_nbrs<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, V);
         k_adj_drag<R><<<nb, kAdjThreads, 0, h->stream>>>(P, V, A, X->dloss * X->dt, part);
         k_adj_nu_sum<<<1, 256, 0, h->stream>>>(nb, part, A.nu_acc);
-        h->launches += 2;
+        h->launches += 3;
     }
     k_adj_point<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, V, A);
     k_adj_a<R, true><<<nb, kAdjThreads, 0, h->stream>>>(P, V, A, 0, X->dt, A.lg[k]);
-    k_adj_ghost_lambda<R><<<nb, kAdjThreads, 0, h->stream>>>(P, V, A, h->t_phys, h->body_acc[0], h->body_acc[1],
-                                                             A.mo_part);
-    k_adj_motion_sum<<<1, 256, 0, h->stream>>>(nb, 4, A.mo_part, 1.0, A.g_motion + 4 * (size_t)jstep);
-    if (P.ghost_assign) {
-        k_adj_ghost_water<R><<<nb, kAdjThreads, 0, h->stream>>>(P, V, A, h->body_acc[0], h->body_acc[1]);
-        h->launches += 1;
+    if (ghosts) {
+        const int ngb = blocks((long long)h->n_ghost * 32, kAdjThreads);
+        k_adj_ghost_lambda<R><<<ngb, kAdjThreads, 0, h->stream>>>(P, V, A, h->d_ghost_ids, h->n_ghost, h->t_phys,
+                                                                  h->body_acc[0], h->body_acc[1], A.mo_part);
+        k_adj_motion_sum<<<1, 256, 0, h->stream>>>(ngb, 4, A.mo_part, 1.0, A.g_motion + 4 * (size_t)jstep);
+        k_adj_ghost_water<R><<<blocks((long long)P.n_tot * 32, kAdjThreads), kAdjThreads, 0, h->stream>>>(
+            P, V, A, h->body_acc[0], h->body_acc[1]);
+        h->launches += 3;
     }
     k_adj_stage_ms<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, V, A, pred, X->dt);
     CK(cudaGetLastError());
-    h->launches += 10;
+    h->launches += 5;
     return SPH_OK;
 }
 
@@ -1143,7 +1164,7 @@ void destroy(sph_handle* h) {
                     h->S.r_drho, h->S.r_acc,
                     h->S.r_avg, h->S.cnt, h->S.off, h->S.lr_cnt, h->S.lr_off, h->S.tb_cnt, h->S.tb_off, h->keys_in, h->keys_out, h->vals_in, h->vals_out, h->cub_tmp,
                     h->d_status, h->d_int, h->d_part, h->d_diag, h->d_xfer, h->d_export, h->d_off64, h->d_cnt_id,
-                    h->d_mls};
+                    h->d_mls, h->d_ghost_ids};
     for (void* p : ptrs) if (p) cudaFree(p);
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -1291,8 +1312,19 @@ int sph_set_state(sph_handle* h, int n, const double* pos, const double* vel, co
                        h->stream));
     CK(cudaMemcpyAsync(h->S.type, type, sizeof(int) * n, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->S.itype, type, sizeof(int) * n, cudaMemcpyHostToDevice, h->stream));
+    {
+        // the ghost assignment works one warp per ghost over this list
+        std::vector<int> g;
+        for (int i = 0; i < n; ++i)
+            if (type[i] == SPH_TYPE_FIX_GHOST) g.push_back(i);
+        if (!h->d_ghost_ids) CK(dalloc(&h->d_ghost_ids, h->cap_host));
+        h->n_ghost = (int)g.size();
+        if (!g.empty())
+            CK(cudaMemcpyAsync(h->d_ghost_ids, g.data(), sizeof(int) * g.size(), cudaMemcpyHostToDevice, h->stream));
+    }
     h->P.has_body = 0;
     for (int c = 0; c < 6; ++c) h->bf[c] = 0.0;
+    h->bf_pending = false;
     CK(cudaMemsetAsync(h->S.r_drho, 0, sizeof(double) * n, h->stream));
     CK(cudaMemsetAsync(h->S.r_acc, 0, sizeof(double2) * n, h->stream));
     CK(cudaMemsetAsync(h->S.r_avg, 0, sizeof(double2) * n, h->stream));

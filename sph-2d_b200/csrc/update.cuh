@@ -279,49 +279,67 @@ __global__ void k_translate_body(int n, const int* itype, double2* pos, double d
     pos[i] = make_double2(x.x + dx, x.y + dy);
 }
 
-// The neighbours the ghost assignment interpolates from for ghost slot s: the
-// non-ghost particles within kernel_scale * 1.2 h, visited cell by cell over the
-// window of s's cell (the list-build cells, so the window reaches ghost_r plus
-// half the skin).  fn(b, dx, dy, q, w) gets (dx, dy) = x_s - x_b, q = d / h_g and
-// the kernel value w with the ghost smoothing length h_g.
-template <typename R, typename F>
-__device__ __forceinline__ void ghost_visit(const Params& P, const Sorted<R>& D, int s, F&& fn) {
-    const double2 x = D.pos[s];
-    const int cx = (int)floor((x.x - P.gx0) / P.cs), cy = (int)floor((x.y - P.gy0) / P.cs);
-    const double hg = P.ghost_h;
-    for (int gy = max(cy - P.ghost_cells, 0); gy <= min(cy + P.ghost_cells, P.gny - 1); ++gy) {
-        const int row = gy * P.gnx;
-        for (int gx = max(cx - P.ghost_cells, 0); gx <= min(cx + P.ghost_cells, P.gnx - 1); ++gx) {
-            const int b0 = D.cell_start[row + gx];
-            if (b0 < 0) continue;
-            const int b1 = D.cell_end[row + gx];
-            for (int b = b0; b < b1; ++b) {
-                if (D.type[b] == SPH_TYPE_FIX_GHOST) continue;     // no other boundary particles
-                const double2 xb = D.pos[b];
-                const double dx = x.x - xb.x, dy = x.y - xb.y;
-                const double d = sqrt(dx * dx + dy * dy);
-                if (!(d <= P.ghost_r)) continue;
-                const double q = d / hg;
-                double w;
-                if (P.kernel_model == SPH_KERNEL_GAUSSIAN) {
-                    w = (exp(-(q * q)) - P.gauss_e9) * P.ghost_kf;
-                } else {
-                    const double tq = 1.0 - q / 2.0;
-                    const double t2 = tq * tq;
-                    w = P.ghost_kf * (1.0 + 2.0 * q) * (t2 * t2);
-                }
-                fn(b, dx, dy, q, w);
-            }
-        }
-    }
-}
-
 // (dw/dd) / d of the ghost kernel at q = d / h_g.
 __device__ __forceinline__ double ghost_dw_over_d(const Params& P, double q) {
     const double hg2 = P.ghost_h * P.ghost_h;
     if (P.kernel_model == SPH_KERNEL_GAUSSIAN) return -2.0 * exp(-(q * q)) * P.ghost_kf / hg2;
     const double tq = 1.0 - q / 2.0;
     return -5.0 * (tq * tq * tq) * P.ghost_kf / hg2;
+}
+
+// The neighbours the ghost assignment interpolates from for ghost slot s: the
+// non-ghost particles within kernel_scale * 1.2 h, found over the window of s's
+// cell (the list-build cells, so the window reaches ghost_r plus half the skin).
+// The 32 lanes of a warp split the candidates of each window row (the slots of
+// a row's window cells are contiguous in the cell-sorted order); fn(b, dx, dy,
+// q, w) gets (dx, dy) = x_s - x_b, q = d / h_g and the kernel value w with the
+// ghost smoothing length h_g, on the lane that visits b.
+template <typename R, typename F>
+__device__ __forceinline__ void ghost_visit_warp(const Params& P, const Sorted<R>& D, int s, F&& fn) {
+    const int lane = threadIdx.x & 31;
+    const double2 x = D.pos[s];
+    const int cx = (int)floor((x.x - P.gx0) / P.cs), cy = (int)floor((x.y - P.gy0) / P.cs);
+    const double hg = P.ghost_h;
+    const int gx0 = max(cx - P.ghost_cells, 0), gx1 = min(cx + P.ghost_cells, P.gnx - 1);
+    for (int gy = max(cy - P.ghost_cells, 0); gy <= min(cy + P.ghost_cells, P.gny - 1); ++gy) {
+        const int row = gy * P.gnx;
+        int lo = -1, hi = -1;
+        for (int gx = gx0; gx <= gx1; ++gx) {
+            const int b0 = D.cell_start[row + gx];
+            if (b0 < 0) continue;
+            if (lo < 0) lo = b0;
+            hi = D.cell_end[row + gx];
+        }
+        if (lo < 0) continue;
+        for (int b = lo + lane; b < hi; b += 32) {
+            if (D.type[b] == SPH_TYPE_FIX_GHOST) continue;
+            const double2 xb = D.pos[b];
+            const double dx = x.x - xb.x, dy = x.y - xb.y;
+            const double d = sqrt(dx * dx + dy * dy);
+            if (!(d <= P.ghost_r)) continue;
+            const double q = d / hg;
+            double w;
+            if (P.kernel_model == SPH_KERNEL_GAUSSIAN) {
+                w = (exp(-(q * q)) - P.gauss_e9) * P.ghost_kf;
+            } else {
+                const double tq = 1.0 - q / 2.0;
+                const double t2 = tq * tq;
+                w = P.ghost_kf * (1.0 + 2.0 * q) * (t2 * t2);
+            }
+            fn(b, dx, dy, q, w);
+        }
+    }
+}
+
+// Sum over the warp, lane 0's association order, broadcast to every lane (so
+// that all lanes continue with bit-identical values).
+__device__ __forceinline__ double warp_sum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return __shfl_sync(0xffffffffu, v, 0);
+}
+__device__ __forceinline__ int warp_sum(int v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return __shfl_sync(0xffffffffu, v, 0);
 }
 
 // Fixed-ghost assignment of the moving-square driver (Moving_Square.../
@@ -336,17 +354,20 @@ __device__ __forceinline__ double ghost_dw_over_d(const Params& P, double q) {
 // pressure they start from for other labels, as the reference's branch does;
 // then the wall velocity is mirrored by label and wall condition.  Finally
 // rho = (p - pb)/c0^2 + rho0, or the rest state when m = 0.
+// One warp per ghost (ghost_ids: the host ghosts in id order, n_ghost of them),
+// the lanes splitting the neighbours; the sums are reduced in a fixed order.
 template <typename R>
-__global__ void k_assign_ghosts(Params P, Sorted<R> D, double t, double bvx, double bvy, double bax, double bay) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= P.n_tot) return;
-    if (D.type[s] != SPH_TYPE_FIX_GHOST || D.id[s] >= P.n_host) return;
+__global__ void k_assign_ghosts(Params P, Sorted<R> D, const int* ghost_ids, int n_ghost, double t, double bvx,
+                                double bvy, double bax, double bay) {
+    const int wg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (wg >= n_ghost) return;                       // whole warps
+    const int s = D.slot_of[ghost_ids[wg]];
     const double2 x = D.pos[s];
     const bool body = D.itype[s] == SPH_TYPE_BODY;
     const double gxe = P.grav[0] + (body ? bax : 0.0), gye = P.grav[1] + (body ? bay : 0.0);
     double sw = 0.0, sp = 0.0, su = 0.0, sv = 0.0, sm = 0.0;
     int cnt = 0;
-    ghost_visit(P, D, s, [&](int b, double dx, double dy, double, double w) {
+    ghost_visit_warp(P, D, s, [&](int b, double dx, double dy, double, double w) {
         const double4 kb = D.kin[b];
         const double mb = D.mass[b];
         const double W = w * (mb / kb.z);
@@ -357,6 +378,9 @@ __global__ void k_assign_ghosts(Params P, Sorted<R> D, double t, double bvx, dou
         sm += mb * W;
         ++cnt;
     });
+    sw = warp_sum(sw); sp = warp_sum(sp); su = warp_sum(su); sv = warp_sum(sv); sm = warp_sum(sm);
+    cnt = warp_sum(cnt);
+    if ((threadIdx.x & 31) != 0) return;
     double uint = 0.0, vint = 0.0, pint = 0.0, m = 0.0;
     if (cnt >= 3) {
         const double inv = 1.0 / sw;
@@ -440,50 +464,46 @@ __global__ void k_diag_final(int nparts, const double* part_ke, const double* pa
 }
 
 // Body force of the last RHS (Moving_Square.../Calculate_Body_Force.f90:53-142 and
-// Single_step_compute.f90:228-243), gather form in FP64: for a particle with body
-// neighbours b (initial type SPH_TYPE_BODY)
+// Single_step_compute.f90:228-243), FP64: for a particle a with body neighbours b
+// (initial type SPH_TYPE_BODY)
 //   BFP_a = -sum_b V_b (p_a + p_b) B_a^-1 grad_a W_ab
 //   BFV_a =  sum_b rho_a V_b 2 nu ((x_a - x_b).B_a^-1 grad_a W_ab) / r^2 (v_a - v_b)   (Morris)
 //       or   sum_b rho_a V_b 2 (dim+2) nu ((v_a-v_b).(x_a-x_b)) / r^2 B_a^-1 grad_a W_ab
 // and the forces are sum_a V_a BFP_a, sum_a V_a BFV_a and their sum (no gravity).
+// Gathered from the body side: body particle b sums V_a times its terms over its
+// pair neighbours a (the pair set is symmetric), so only the body's threads loop.
 template <typename R>
 __global__ void k_body_force(Params P, Sorted<R> D, double* part) {
-    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
     double f[6] = {0, 0, 0, 0, 0, 0};
-    if (a < P.n_tot) {
-        const int nn = D.npairs[a];
-        const double2 xa = D.pos[a];
-        const double4 ka = D.kin[a];
-        const double4 bi = D.binv64[a];
-        double bp0 = 0, bp1 = 0, bv0 = 0, bv1 = 0;
-        bool near_body = false;
+    if (b < P.n_tot && D.itype[b] == SPH_TYPE_BODY) {
+        const int nn = D.npairs[b];
+        const double2 xb = D.pos[b];
+        const double4 kb = D.kin[b];
+        const double Vb = D.mass[b] / kb.z;
         for (int e = 0; e < nn; ++e) {
-            const int b = (int)(D.pairs[(size_t)e * P.nbr_stride + a] & 0x7fffffffu);
-            if (D.itype[b] != SPH_TYPE_BODY) continue;
-            near_body = true;
-            const double2 xb = D.pos[b];
-            const double4 kb = D.kin[b];
+            const int a = (int)(D.pairs[(size_t)e * P.nbr_stride + b] & 0x7fffffffu);
+            const double2 xa = D.pos[a];
+            const double4 ka = D.kin[a];
+            const double4 bi = D.binv64[a];
+            const double Va = D.mass[a] / ka.z;
             const double dx = xa.x - xb.x, dy = xa.y - xb.y;
             const double r2 = dx * dx + dy * dy, d = sqrt(r2);
             double w, gx, gy;
             kernel_w_dw<double>(P, d, dx, dy, w, gx, gy);
             const double n0 = bi.x * gx + bi.y * gy, n1 = bi.z * gx + bi.w * gy;
-            const double Vb = D.mass[b] / kb.z;
-            bp0 -= Vb * (ka.w + kb.w) * n0;
-            bp1 -= Vb * (ka.w + kb.w) * n1;
+            const double bp0 = -Vb * (ka.w + kb.w) * n0, bp1 = -Vb * (ka.w + kb.w) * n1;
             const double du = ka.x - kb.x, dv = ka.y - kb.y;
+            double bv0, bv1;
             if (P.laplacian == 1) {
                 const double fv = ka.z * Vb * 2 * P.nu * (dx * n0 + dy * n1) / r2;
-                bv0 += fv * du; bv1 += fv * dv;
+                bv0 = fv * du; bv1 = fv * dv;
             } else {
                 const double fv = ka.z * Vb * 2 * (2 + 2) * P.nu * (du * dx + dv * dy) / r2;
-                bv0 += fv * n0; bv1 += fv * n1;
+                bv0 = fv * n0; bv1 = fv * n1;
             }
-        }
-        if (near_body) {
-            const double Va = D.mass[a] / ka.z;
-            f[0] = Va * bp0; f[1] = Va * bp1; f[2] = Va * bv0; f[3] = Va * bv1;
-            f[4] = Va * (bp0 + bv0); f[5] = Va * (bp1 + bv1);
+            f[0] += Va * bp0; f[1] += Va * bp1; f[2] += Va * bv0; f[3] += Va * bv1;
+            f[4] += Va * (bp0 + bv0); f[5] += Va * (bp1 + bv1);
         }
     }
     __shared__ double sh[6][kRedThreads];
