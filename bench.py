@@ -256,6 +256,9 @@ def run_native(args, rank, world, local):
     if rank == 0 and not args.skip_adjoint:
         adj = adjoint_report(S)
         adj_ms = adjoint_ms_report(S)
+    ms = None
+    if rank == 0 and not args.skip_accuracy:
+        ms = moving_square_report(S)
 
     # ---- CPU baseline (rank 0 only, N = 1) ----------------------------------
     cpu = None
@@ -279,6 +282,7 @@ def run_native(args, rank, world, local):
         "adjoint_over_forward": adj["adjoint_over_forward"] if adj else None,
         "adjoint": adj,
         "adjoint_moving_square": adj_ms,
+        "moving_square": ms,
         "passes_ms_per_step": {
             "images": tm.images_ms / steps, "sort_lists": tm.sort_ms / steps,
             "pass_a": tm.pass_a_ms / steps, "surface": tm.surface_ms / steps,
@@ -379,8 +383,9 @@ def adjoint_ms_report(S):
     moving-square solver), ghost assignment every RHS, Euler predictor-corrector,
     FP64; 2,000 steps with a checkpoint every 64.  Motion u(t) = a0 + sum_k a_k
     sin(2 pi k t / T) over the run time T; loss = time-averaged drag coefficient
-    sum_s dt F_x / (T F0), F0 = rho0 U^2 D / 2.  Forward = the same steps with
-    one checkpoint (sph_adjoint_forward, checkpoint_every = nsteps).  The
+    sum_s dt F_x / (T F0), F0 = rho0 U^2 D / 2.  Forward = time_iteration over
+    the same number of steps with the body at its mean speed a0 (the same work
+    per step: translation, ghost assignment, RHS, body force).  The
     gradient with respect to a0 and a1 is checked by central differences on the
     first 200 steps of the same case: the improved Gaussian's gradient does not
     vanish at its 3h cut-off, so the right-hand side jumps whenever a pair
@@ -419,8 +424,9 @@ def adjoint_ms_report(S):
     with new_sim() as sim:
         for rep in range(2):          # the first round warms up allocations
             reset(sim)
+            sim.set_body_motion((coeffs[0], 0.0))
             t0 = time.perf_counter()
-            sim.adjoint_forward(MS_STEPS, dt, checkpoint_every=MS_STEPS, loss=S.LOSS_DRAG, body_motion=motion)
+            sim.time_iteration(MS_STEPS, dt)
             t_fwd = time.perf_counter() - t0
             reset(sim)
             t0 = time.perf_counter()
@@ -461,6 +467,49 @@ def adjoint_ms_report(S):
         "dC_d_coeffs": [float(x) for x in gc], "dC_dnu": g["nu"], "fd": fd,
         "fd_note": f"central differences eps=1e-6 of the FP64 forward over the first {MS_FD_STEPS} steps",
     }
+
+
+def moving_square_report(S, steps: int = 200, warmup: int = 3):
+    """The moving-square forward: square of side D = 1 in a [0,10] x [0,5] tank,
+    dx = D/100 (about 500k fluid particles, 4 ghost layers), HLLC + delta-SPH,
+    Re = 100, the square started impulsively at U = 1, ghost assignment and the
+    body force every step, Euler predictor-corrector with shifting and MLS
+    density re-initialisation every 40 steps (the shipped moving-square
+    settings).  Mixed and FP64 from the same state: device-timed particle-steps/s,
+    the velocity L2 difference after the run and the drag coefficient of the
+    last step (F0 = rho0 U^2 D / 2)."""
+    out = {}
+    vel = {}
+    for name, prec in (("mixed", S.PREC_MIXED), ("fp64", S.PREC_FP64)):
+        case, ity = S.make_moving_square(dx=0.01, lx=10.0, ly=5.0, D=1.0, U=1.0, solver=S.SOLVER_MS_HLLC_DELTA,
+                                         precision=prec)
+        cfg = case.cfg
+        cfg.ghost_assign = 1
+        lab = S.moving_square_labels(case, ity)
+        dt = 0.25 * cfg.h / np.sqrt(cfg.c0sq)
+        with S.Simulation(cfg, case.n) as sim:
+            sim.set_state(case.pos, case.vel, case.rho, case.mass, case.type)
+            sim.set_initial_type(ity)
+            sim.set_boundary_labels(lab)
+            sim.set_body_motion((1.0, 0.0))
+            sim.set_time(0.0)
+            sim.time_iteration(warmup, dt)
+            sim.reset_timings()
+            d = sim.time_iteration(steps, dt)
+            tm = sim.timings()
+            vel[name] = sim.get_state()[1]
+        out[name] = {"particle_steps_per_s": case.n * steps / (tm.total_ms / 1e3),
+                     "ms_per_step": tm.total_ms / steps,
+                     "drag_coefficient": d.body_force[4] / (0.5 * cfg.rho0)}
+        n = case.n
+    water = np.r_[case.type, case.type] == S.TYPE_WATER
+    dv = vel["mixed"][water] - vel["fp64"][water]
+    out["mixed_over_fp64"] = out["mixed"]["particle_steps_per_s"] / out["fp64"]["particle_steps_per_s"]
+    out["velocity_l2_mixed_vs_fp64"] = float(np.linalg.norm(dv) / np.linalg.norm(vel["fp64"][water]))
+    out["case"] = (f"moving square D=1 in [0,10]x[0,5], dx=D/100 ({n} particles incl. ghosts), HLLC + delta-SPH, "
+                   f"Re=100, impulsive U=1, ghost assignment, body force every step, Euler PC, shifting, MLS every "
+                   f"40 steps; {steps} steps after {warmup}, device-timed")
+    return out
 
 
 def cpu_reference(steps: int, warmup: int, n_side: int = 256):

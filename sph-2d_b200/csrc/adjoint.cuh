@@ -73,33 +73,34 @@ constexpr int kAdjThreads = 128;
 
 // G(d) of grad_a W = G(d) (x_a - x_b) and dG/dd.
 // Gaussian: G = -2 k exp(-q^2)/h^2; Wendland C2: G = -5 k (1 - q/2)^3 / h^2.
+// (1/h is loop-invariant: the compiler hoists it out of the pair loops.)
 __device__ __forceinline__ void kernel_g(const Params& P, double d, double& G, double& dG) {
-    const double h = P.h, q = d / h, kf = P.kfactor;
+    const double ih = 1.0 / P.h, q = d * ih, kf = P.kfactor, ih2 = ih * ih;
     if (P.kernel_model == SPH_KERNEL_GAUSSIAN) {
         const double ex = exp(-(q * q));
-        G = -2.0 * kf * ex / (h * h);
-        dG = 4.0 * kf * q * ex / (h * h * h);
+        G = -2.0 * kf * ex * ih2;
+        dG = 4.0 * kf * q * ex * (ih2 * ih);
     } else {
         const double t = 1.0 - 0.5 * q;
-        G = -5.0 * kf * t * t * t / (h * h);
-        dG = 7.5 * kf * t * t / (h * h * h);
+        G = -5.0 * kf * t * t * t * ih2;
+        dG = 7.5 * kf * t * t * (ih2 * ih);
     }
 }
 
 // kernel_g and the kernel value W(d) of compute_kernel (whose d-derivative is
 // G(d) d) from one exponential.
 __device__ __forceinline__ void kernel_gw(const Params& P, double d, double& G, double& dG, double& W) {
-    const double h = P.h, q = d / h, kf = P.kfactor;
+    const double ih = 1.0 / P.h, q = d * ih, kf = P.kfactor, ih2 = ih * ih;
     if (P.kernel_model == SPH_KERNEL_GAUSSIAN) {
         const double ex = exp(-(q * q));
-        G = -2.0 * kf * ex / (h * h);
-        dG = 4.0 * kf * q * ex / (h * h * h);
+        G = -2.0 * kf * ex * ih2;
+        dG = 4.0 * kf * q * ex * (ih2 * ih);
         W = (ex - P.gauss_e9) * kf;
     } else {
         const double t = 1.0 - 0.5 * q;
         const double t2 = t * t;
-        G = -5.0 * kf * t2 * t / (h * h);
-        dG = 7.5 * kf * t2 / (h * h * h);
+        G = -5.0 * kf * t2 * t * ih2;
+        dG = 7.5 * kf * t2 * (ih2 * ih);
         W = kf * (1.0 + 2.0 * q) * (t2 * t2);
     }
 }
@@ -116,6 +117,7 @@ __device__ __forceinline__ void eos_deriv(const Params& P, double rho, double& d
 struct PSide {
     double2 x;
     double u, v, rho, p, c, V, m, sm;
+    double ir;            // 1 / rho
     double t0, t1, t2;    // tau xx, xy, yy
     double g0, g1;        // grad rho
     double ax, ay;        // XSPH average velocity (moving-square solver)
@@ -131,7 +133,8 @@ __device__ __forceinline__ PSide load_side(const Sorted<R>& D, int s) {
     o.u = k.x; o.v = k.y; o.rho = k.z; o.p = k.w;
     const typename VT<R>::V4 ax = D.aux[s];
     o.m = D.mass[s];
-    o.V = o.m / o.rho;
+    o.ir = 1.0 / o.rho;
+    o.V = o.m * o.ir;
     o.c = (double)ax.z;
     o.sm = (double)ax.w;
     const typename VT<R>::V4 n1 = D.nb1[s];
@@ -178,7 +181,7 @@ __device__ __forceinline__ void rev_pair(const Params& P, const PSide& A, const 
     const double vx = du0 * r0 + du1 * r1;
     const double dU = -vx * id;
     const double rbar = 0.5 * (A.rho + B.rho), cbar = 0.5 * (A.c + B.c);
-    const double c0 = P.sqrt_c0;
+    const double irbar = 1.0 / rbar, ic0 = 1.0 / P.sqrt_c0;
     const double Pbar = 0.5 * (A.p + B.p);
     // Riemann state
     double PA, w0, w1, bR = 0.0, kk = 0.0;
@@ -190,22 +193,23 @@ __device__ __forceinline__ void rev_pair(const Params& P, const PSide& A, const 
         take_m3 = m3 < cbar;
         bR = take_m3 ? m3 : cbar;
         PA = Pbar + 0.5 * bR * rbar * dU;
-        kk = dp / (2.0 * rbar * c0 * d);
+        kk = dp * (0.5 * irbar * ic0) * id;
         w0 = 0.5 * du0 + kk * r0; w1 = 0.5 * du1 + kk * r1;
     }
     if (MS) { w0 += A.ax - B.ax; w1 += A.ay - B.ay; }
-    const double rhoij = 1.0 / (A.rho * B.rho);
+    const double rhoij = A.ir * B.ir;
     const double fp = -2.0 * PA * B.m * rhoij;
     const bool av = vx < 0.0;
     const double fh2 = (P.fai * P.h) * (P.fai * P.h);
     const double den_phi = d2 + fh2;
-    double phi = 0.0, Pi = 0.0;
+    double phi = 0.0, Pi = 0.0, iden = 0.0;
     if (av) {
-        phi = P.h * vx / den_phi;
-        Pi = (-P.alpha * cbar * phi + P.beta * (phi * phi)) / rbar;
+        iden = 1.0 / den_phi;
+        phi = P.h * vx * iden;
+        Pi = (-P.alpha * cbar * phi + P.beta * (phi * phi)) * irbar;
     }
     const double Kt = P.delta_alpha * P.h * P.rho0;
-    const double tt = Kt * cbar * vx * id2 / A.rho * B.V;
+    const double tt = Kt * cbar * vx * id2 * A.ir * B.V;
     const double Cn = fp - (av ? B.m * Pi : 0.0) + tt;
     const double lf = 2.0 * P.nu * B.V * G * s * id2;
     const double Ln = l0 * n0 + l1 * n1;
@@ -232,26 +236,26 @@ __device__ __forceinline__ void rev_pair(const Params& P, const PSide& A, const 
         const double rhoijb = B.sm * G * (l0 * Q + l1 * (2.0 * q * rhoij * Q + Rr));
         o.t0 = Qb * r0; o.t1 = Qb * r1 + Rb * r0; o.t2 = Rb * r1;
         r0b += Qb * sxx + Rb * sxy; r1b += Qb * sxy + Rb * syy;
-        rab -= rhoijb * rhoij / A.rho; rbb -= rhoijb * rhoij / B.rho;
+        rab -= rhoijb * rhoij * A.ir; rbb -= rhoijb * rhoij * B.ir;
     }
     // C = fp - [av] m_b Pi + tt
     const double PAb0 = -2.0 * B.m * rhoij * Cnb;
-    rab -= fp / A.rho * Cnb; rbb -= fp / B.rho * Cnb;
+    rab -= fp * A.ir * Cnb; rbb -= fp * B.ir * Cnb;
     if (av) {
         const double Pib = -B.m * Cnb;
-        cbarb += -P.alpha * phi / rbar * Pib;
-        const double phib = (-P.alpha * cbar + 2.0 * P.beta * phi) / rbar * Pib;
-        rbarb -= Pi / rbar * Pib;
-        vxb += P.h / den_phi * phib;
-        db -= phi * 2.0 * d / den_phi * phib;
+        cbarb += -P.alpha * phi * irbar * Pib;
+        const double phib = (-P.alpha * cbar + 2.0 * P.beta * phi) * irbar * Pib;
+        rbarb -= Pi * irbar * Pib;
+        vxb += P.h * iden * phib;
+        db -= phi * 2.0 * d * iden * phib;
     }
     {
-        const double base = Kt * id2 / A.rho;
+        const double base = Kt * id2 * A.ir;
         cbarb += base * vx * B.V * Cnb;
         vxb += base * cbar * B.V * Cnb;
         Vbb += base * cbar * vx * Cnb;
         db -= 2.0 * tt * id * Cnb;
-        rab -= tt / A.rho * Cnb;
+        rab -= tt * A.ir * Cnb;
     }
     // Morris laplacian factor lf = 2 nu V_b G s / d^2
     o.nu = 2.0 * B.V * G * s * id2 * lfb;
@@ -290,8 +294,8 @@ __device__ __forceinline__ void rev_pair(const Params& P, const PSide& A, const 
     if (!A.near) {
         const double kkb = w0b * r0 + w1b * r1;
         r0b += kk * w0b; r1b += kk * w1b;
-        dpb += kkb / (2.0 * rbar * c0 * d);
-        rbarb -= kk / rbar * kkb;
+        dpb += kkb * (0.5 * irbar * ic0) * id;
+        rbarb -= kk * irbar * kkb;
         db -= kk * id * kkb;
         const double bRb = 0.5 * rbar * dU * PAb0;
         rbarb += 0.5 * bR * dU * PAb0;
@@ -541,8 +545,8 @@ __device__ __forceinline__ void stage_reverse(const Params& P, const Sorted<R>& 
 
 // f = V_b G(d) [sum_phi (phi_b - phi_a) mu_phi.r - r^T M r]: the adjoint-weighted
 // pair term of pass A's raw sums at particle a, with G = G(d), dG = G'(d),
-// d = |r|.  Returns f / V_b and its gradient with respect to r divided by V_b.
-__device__ __forceinline__ void rev_rawsum(double r0, double r1, double d, double G, double dG, double dr,
+// id = 1/|r|.  Returns f / V_b and its gradient with respect to r divided by V_b.
+__device__ __forceinline__ void rev_rawsum(double r0, double r1, double id, double G, double dG, double dr,
                                            double du, double dv, const double4& m1, const double4& m2,
                                            const double2& m3, double& S_G, double& fr0, double& fr1) {
     const double c0 = dr * m1.x + du * m1.z + dv * m2.x;   // sum_phi dphi mu_phi (x)
@@ -551,7 +555,7 @@ __device__ __forceinline__ void rev_rawsum(double r0, double r1, double d, doubl
     const double MTr0 = m2.z * r0 + m3.x * r1, MTr1 = m2.w * r0 + m3.y * r1;
     const double S = c0 * r0 + c1 * r1 - (r0 * Mr0 + r1 * Mr1);
     S_G = S;
-    const double k = dG * S / d;
+    const double k = dG * S * id;
     fr0 = k * r0 + G * (c0 - Mr0 - MTr0);
     fr1 = k * r1 + G * (c1 - Mr1 - MTr1);
 }
@@ -586,7 +590,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_a(Params P, Sorted<R> D, Ad
         const double2 xb = D.pos[b];
         const double4 kb = D.kin[b];
         const double r0 = xc.x - xb.x, r1 = xc.y - xb.y;
-        const double d = sqrt(r0 * r0 + r1 * r1);
+        const double d = sqrt(r0 * r0 + r1 * r1), id = 1.0 / d;
         double G, dG, W;
         kernel_gw(P, d, G, dG, W);
         if (MS) {
@@ -614,7 +618,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_a(Params P, Sorted<R> D, Ad
         {
             const double Vbn = D.mass[b] / kb.z;
             double S, f0, f1;
-            rev_rawsum(r0, r1, d, G, dG, kb.z - kc.z, kb.x - kc.x, kb.y - kc.y, mc1, mc2, mc3, S, f0, f1);
+            rev_rawsum(r0, r1, id, G, dG, kb.z - kc.z, kb.x - kc.x, kb.y - kc.y, mc1, mc2, mc3, S, f0, f1);
             x0b += Vbn * f0; x1b += Vbn * f1;
             rb -= Vbn * G * (mc1.x * r0 + mc1.y * r1);
             ub -= Vbn * G * (mc1.z * r0 + mc1.w * r1);
@@ -625,7 +629,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_a(Params P, Sorted<R> D, Ad
             const double4 mb1 = A.mu1[b], mb2 = A.mu2[b];
             const double2 mb3 = A.mu3[b];
             double S, f0, f1;
-            rev_rawsum(-r0, -r1, d, G, dG, kc.z - kb.z, kc.x - kb.x, kc.y - kb.y, mb1, mb2, mb3, S, f0, f1);
+            rev_rawsum(-r0, -r1, id, G, dG, kc.z - kb.z, kc.x - kb.x, kc.y - kb.y, mb1, mb2, mb3, S, f0, f1);
             x0b -= Vc * f0; x1b -= Vc * f1;
             rb -= Vc * G * (mb1.x * r0 + mb1.y * r1);
             ub -= Vc * G * (mb1.z * r0 + mb1.w * r1);
