@@ -223,6 +223,11 @@ def run_native(args, rank, world, local):
     h2d = 40 * n
     d2h = 40 * n
 
+    # ---- output streaming: snapshots overlapped with the steps (rank 0) -------
+    streaming = None
+    if rank == 0 and not args.skip_accuracy:
+        streaming = streaming_report(S, sim, n, mixed["dt"])
+
     # ---- accuracy: mixed vs FP64 on the jittered lattice ----------------------
     accuracy = None
     if not args.skip_accuracy and rank == 0:
@@ -283,6 +288,7 @@ def run_native(args, rank, world, local):
         "adjoint": adj,
         "adjoint_moving_square": adj_ms,
         "moving_square": ms,
+        "output_streaming": streaming,
         "passes_ms_per_step": {
             "images": tm.images_ms / steps, "sort_lists": tm.sort_ms / steps,
             "pass_a": tm.pass_a_ms / steps, "surface": tm.surface_ms / steps,
@@ -370,6 +376,31 @@ def adjoint_report(S):
         "dnu_mixed": m["grad"]["nu"], "dnu_fp64": d["grad"]["nu"],
         "fd_rel_err_fp64": fd_err, "fd": "central differences eps=1e-6, FP64 forward, 2 seeded directions",
     }
+
+
+def streaming_report(S, sim, n, dt, chunks: int = 4, every: int = 5):
+    """Output every `every` steps on the benchmark state: wall time per step of
+    the same step calls with no output, with sph_snapshot_begin into page-locked
+    buffers before each chunk (the transfer of x, v, rho, p runs on the copy
+    stream while the next steps compute), and with a synchronous sph_get_state
+    before each chunk."""
+    bufs = [torch.empty(m * n, dtype=torch.float64).pin_memory().numpy() for m in (2, 2, 1, 1)]
+    res = {}
+    for mode in ("none", "snapshot", "get_state"):
+        sim.time_iteration(1, dt)
+        t0 = time.perf_counter()
+        for _ in range(chunks):
+            if mode == "snapshot":
+                sim.snapshot_begin(*bufs)
+            elif mode == "get_state":
+                sim.get_state()
+            sim.time_iteration(every, dt)
+        sim.snapshot_wait()
+        res[mode] = (time.perf_counter() - t0) * 1e3 / (chunks * every)
+    return {"ms_per_step": res, "every": every, "bytes_per_snapshot": 48 * n,
+            "snapshot_overhead_pct": 100.0 * (res["snapshot"] / res["none"] - 1.0),
+            "get_state_overhead_pct": 100.0 * (res["get_state"] / res["none"] - 1.0),
+            "note": "wall clock, mixed 2048^2 step; sph_step calls of `every` steps each"}
 
 
 MS_DX, MS_STEPS, MS_EVERY, MS_FD_STEPS = 0.02, 2000, 64, 200

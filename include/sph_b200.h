@@ -27,6 +27,8 @@
 #ifndef SPH_B200_H
 #define SPH_B200_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -202,6 +204,41 @@ int sph_set_time(sph_handle* h, double t);
 /* Download the host particles (same order as set_state).  press is the
  * equation of state evaluated at the returned density.  Any pointer may be NULL. */
 int sph_get_state(sph_handle* h, int n, double* pos, double* vel, double* rho, double* press);
+
+/* ---- snapshot streaming and restart (Output_for_tecplot.f90,
+ * Output_for_Restart_Calculation.f90: the host's output modules keep writing
+ * the files; the library delivers the state without stalling the step) -----
+ *
+ * sph_snapshot_begin queues a copy of the current state (the layout of
+ * sph_get_state) into the given host buffers and returns at once: the state is
+ * copied on the device in the step's stream order, and the transfer to the host
+ * runs on a separate copy stream while later sph_step calls proceed.  The
+ * buffers must stay valid until the snapshot completes; with page-locked
+ * (cudaHostAlloc'd) buffers the transfer overlaps the steps, with pageable ones
+ * it completes before the call returns.  A new snapshot first waits for the
+ * previous one.  sph_snapshot_query returns SPH_OK when the last snapshot is
+ * complete (or none was taken) and SPH_PENDING while it is in flight;
+ * sph_snapshot_wait blocks until it is complete. */
+#define SPH_PENDING 1
+int sph_snapshot_begin(sph_handle* h, int n, double* pos, double* vel, double* rho, double* press);
+int sph_snapshot_query(sph_handle* h);
+int sph_snapshot_wait(sph_handle* h);
+
+/* Exact restart: the whole per-particle and per-run state a later step depends
+ * on (positions, velocities, densities, masses, SPS masses, types, initial
+ * types, wall labels, the rates carried to the next step, the step count, the
+ * physical time and the body motion), so that a handle restored from it
+ * continues bit-identically to the one saved.  Little-endian binary: a 64-byte
+ * header (magic "SPHB200R", version 1, n, then the step count, the time and the
+ * body velocity and acceleration as doubles) followed by per-particle arrays in
+ * set_state order: pos, vel (x, y pairs), rho, mass, smass (double), type,
+ * itype, labels (int32), carried drho, acc, avg (double; acc and avg as x, y
+ * pairs).  sph_restart_load needs a handle of the same configuration with
+ * capacity for n; it replaces sph_set_state, sph_set_initial_type,
+ * sph_set_boundary_labels, sph_set_time and sph_set_body_motion. */
+size_t sph_restart_size(int n);
+int sph_restart_save(sph_handle* h, void* buf, size_t bytes);
+int sph_restart_load(sph_handle* h, const void* buf, size_t bytes);
 
 /* find_particle_pair (Taylor_Green_Vortex/find_particle_pair.f90:21-163) on the
  * current state.  Writes up to pair_cap pairs (1-based, i<j in host/image index

@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdint>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -116,6 +117,12 @@ struct sph_handle {
     // fixed-ghost host particles (type SPH_TYPE_FIX_GHOST) in id order, from sph_set_state
     int* d_ghost_ids = nullptr;           // [cap_host]
     int n_ghost = 0;
+    // snapshot streaming: the id-order copy is made in the step stream, the
+    // device-to-host transfer runs on copy_stream
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t snap_ready = nullptr, snap_done = nullptr;
+    double* d_snap = nullptr;             // [6 * cap_host]
+    bool snap_pending = false;
 };
 
 namespace {
@@ -1167,6 +1174,10 @@ void destroy(sph_handle* h) {
                     h->d_mls, h->d_ghost_ids};
     for (void* p : ptrs) if (p) cudaFree(p);
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
+    if (h->copy_stream) { cudaStreamSynchronize(h->copy_stream); cudaStreamDestroy(h->copy_stream); }
+    if (h->snap_ready) cudaEventDestroy(h->snap_ready);
+    if (h->snap_done) cudaEventDestroy(h->snap_done);
+    if (h->d_snap) cudaFree(h->d_snap);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }
@@ -1197,6 +1208,9 @@ int init_impl(const sph_config* cfg, int n_capacity, sph_handle** out) {
     h->dead_key = (unsigned)((1ULL << h->key_bits) - 1);
     h->P.nbr_stride = cap;
     CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&h->snap_ready, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&h->snap_done, cudaEventDisableTiming));
     // staging
     CK(dalloc(&h->S.pos, cap)); CK(dalloc(&h->S.vel, cap)); CK(dalloc(&h->S.rho, cap));
     CK(dalloc(&h->S.mass, cap)); CK(dalloc(&h->S.smass, cap)); CK(dalloc(&h->S.type, cap));
@@ -1392,6 +1406,156 @@ int sph_set_body_motion(sph_handle* h, const double vel[2], const double acc[2])
 int sph_set_time(sph_handle* h, double t) {
     if (!h) return SPH_E_ARG;
     h->t_phys = t;
+    return SPH_OK;
+}
+
+int sph_snapshot_wait(sph_handle* h) {
+    if (!h) return SPH_E_ARG;
+    if (h->snap_pending) {
+        CK(cudaSetDevice(h->device));
+        CK(cudaEventSynchronize(h->snap_done));
+        h->snap_pending = false;
+    }
+    return SPH_OK;
+}
+
+int sph_snapshot_query(sph_handle* h) {
+    if (!h) return SPH_E_ARG;
+    if (!h->snap_pending) return SPH_OK;
+    CK(cudaSetDevice(h->device));
+    const cudaError_t e = cudaEventQuery(h->snap_done);
+    if (e == cudaErrorNotReady) return SPH_PENDING;
+    CK(e);
+    h->snap_pending = false;
+    return SPH_OK;
+}
+
+int sph_snapshot_begin(sph_handle* h, int n, double* pos, double* vel, double* rho, double* press) {
+    if (!h || n != h->n_host || n <= 0) return SPH_E_ARG;
+    int rc = sph_snapshot_wait(h);               // the device buffer is reused
+    if (rc) return rc;
+    CK(cudaSetDevice(h->device));
+    if (!h->d_snap) CK(dalloc(&h->d_snap, (size_t)6 * h->cap_host));
+    rc = h->mixed ? unsort<float>(h) : unsort<double>(h);
+    if (rc) return rc;
+    k_snapshot<<<blocks(n, 256), 256, 0, h->stream>>>(h->P, n, h->S.pos, h->S.vel, h->S.rho, h->d_snap);
+    CK(cudaGetLastError());
+    h->launches += 1;
+    CK(cudaEventRecord(h->snap_ready, h->stream));
+    CK(cudaStreamWaitEvent(h->copy_stream, h->snap_ready, 0));
+    const size_t nn = (size_t)n;
+    if (pos) CK(cudaMemcpyAsync(pos, h->d_snap, sizeof(double) * 2 * nn, cudaMemcpyDeviceToHost, h->copy_stream));
+    if (vel)
+        CK(cudaMemcpyAsync(vel, h->d_snap + 2 * nn, sizeof(double) * 2 * nn, cudaMemcpyDeviceToHost, h->copy_stream));
+    if (rho) CK(cudaMemcpyAsync(rho, h->d_snap + 4 * nn, sizeof(double) * nn, cudaMemcpyDeviceToHost, h->copy_stream));
+    if (press)
+        CK(cudaMemcpyAsync(press, h->d_snap + 5 * nn, sizeof(double) * nn, cudaMemcpyDeviceToHost, h->copy_stream));
+    CK(cudaEventRecord(h->snap_done, h->copy_stream));
+    h->snap_pending = true;
+    return SPH_OK;
+}
+
+namespace {
+// Restart image: header, then the per-particle arrays in the order below.
+struct RestartHeader {
+    char magic[8];            // "SPHB200R"
+    int32_t version;          // 1
+    int32_t n;
+    int64_t step_count;
+    double t_phys;
+    double body_vel[2];
+    double body_acc[2];
+};
+static_assert(sizeof(RestartHeader) == 64, "restart header is 64 bytes");
+constexpr size_t kRestartPerParticle = 2 * 16 + 3 * 8 + 3 * 4 + 8 + 2 * 16;   // 108 bytes
+}  // namespace
+
+size_t sph_restart_size(int n) {
+    return n > 0 ? sizeof(RestartHeader) + kRestartPerParticle * (size_t)n : 0;
+}
+
+int sph_restart_save(sph_handle* h, void* buf, size_t bytes) {
+    if (!h || !buf || h->n_host <= 0) return SPH_E_ARG;
+    const int n = h->n_host;
+    if (bytes < sph_restart_size(n)) return SPH_E_CAPACITY;
+    CK(cudaSetDevice(h->device));
+    int rc = h->mixed ? unsort<float>(h) : unsort<double>(h);
+    if (rc) return rc;
+    RestartHeader hd{};
+    memcpy(hd.magic, "SPHB200R", 8);
+    hd.version = 1;
+    hd.n = n;
+    hd.step_count = h->step_count;
+    hd.t_phys = h->t_phys;
+    for (int k = 0; k < 2; ++k) { hd.body_vel[k] = h->body_vel[k]; hd.body_acc[k] = h->body_acc[k]; }
+    char* p = static_cast<char*>(buf);
+    memcpy(p, &hd, sizeof(hd));
+    p += sizeof(hd);
+    const size_t nn = (size_t)n;
+    auto get = [&](const void* src, size_t each) -> int {
+        CK(cudaMemcpyAsync(p, src, each * nn, cudaMemcpyDeviceToHost, h->stream));
+        p += each * nn;
+        return SPH_OK;
+    };
+    if ((rc = get(h->S.pos, 16)) || (rc = get(h->S.vel, 16)) || (rc = get(h->S.rho, 8)) || (rc = get(h->S.mass, 8)) ||
+        (rc = get(h->S.smass, 8)) || (rc = get(h->S.type, 4)) || (rc = get(h->S.itype, 4)) ||
+        (rc = get(h->S.blabel, 4)) || (rc = get(h->S.r_drho, 8)) || (rc = get(h->S.r_acc, 16)) ||
+        (rc = get(h->S.r_avg, 16)))
+        return rc;
+    CK(cudaStreamSynchronize(h->stream));
+    return SPH_OK;
+}
+
+int sph_restart_load(sph_handle* h, const void* buf, size_t bytes) {
+    if (!h || !buf || bytes < sizeof(RestartHeader)) return SPH_E_ARG;
+    RestartHeader hd;
+    memcpy(&hd, buf, sizeof(hd));
+    if (memcmp(hd.magic, "SPHB200R", 8) != 0 || hd.version != 1 || hd.n <= 0) return SPH_E_ARG;
+    const int n = hd.n;
+    if (bytes < sph_restart_size(n)) return SPH_E_ARG;
+    if (n > h->cap_host) return SPH_E_CAPACITY;
+    CK(cudaSetDevice(h->device));
+    int rc = sph_snapshot_wait(h);
+    if (rc) return rc;
+    const char* p = static_cast<const char*>(buf) + sizeof(hd);
+    const size_t nn = (size_t)n;
+    // host-side views of the arrays the host bookkeeping needs
+    const int* type = reinterpret_cast<const int*>(p + (2 * 16 + 3 * 8) * nn);
+    const int* itype = type + nn;
+    const int* labels = itype + nn;
+    for (size_t i = 0; i < nn; ++i)
+        if (labels[i] == -9) return SPH_E_CONFIG;     // radius free slip: not built
+    auto put = [&](void* dst, size_t each) -> int {
+        CK(cudaMemcpyAsync(dst, p, each * nn, cudaMemcpyHostToDevice, h->stream));
+        p += each * nn;
+        return SPH_OK;
+    };
+    if ((rc = put(h->S.pos, 16)) || (rc = put(h->S.vel, 16)) || (rc = put(h->S.rho, 8)) || (rc = put(h->S.mass, 8)) ||
+        (rc = put(h->S.smass, 8)) || (rc = put(h->S.type, 4)) || (rc = put(h->S.itype, 4)) ||
+        (rc = put(h->S.blabel, 4)) || (rc = put(h->S.r_drho, 8)) || (rc = put(h->S.r_acc, 16)) ||
+        (rc = put(h->S.r_avg, 16)))
+        return rc;
+    std::vector<int> g;
+    int body = 0;
+    for (size_t i = 0; i < nn; ++i) {
+        if (type[i] == SPH_TYPE_FIX_GHOST) g.push_back((int)i);
+        body |= itype[i] == SPH_TYPE_BODY;
+    }
+    if (!h->d_ghost_ids) CK(dalloc(&h->d_ghost_ids, h->cap_host));
+    h->n_ghost = (int)g.size();
+    if (!g.empty())
+        CK(cudaMemcpyAsync(h->d_ghost_ids, g.data(), sizeof(int) * g.size(), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->n_host = n;
+    h->P.has_body = body;
+    for (int c = 0; c < 6; ++c) h->bf[c] = 0.0;
+    h->bf_pending = false;
+    h->staging_valid = true;
+    h->sorted_valid = false;
+    h->have_rhs = false;
+    h->step_count = hd.step_count;
+    h->t_phys = hd.t_phys;
+    for (int k = 0; k < 2; ++k) { h->body_vel[k] = hd.body_vel[k]; h->body_acc[k] = hd.body_acc[k]; }
     return SPH_OK;
 }
 

@@ -610,6 +610,23 @@ __global__ void k_deinterleave(int n, const double2* in, double* colmaj) {
     if (i < n) { double2 v = in[i]; colmaj[i] = v.x; colmaj[n + i] = v.y; }
 }
 
+// Snapshot of the host particles' state (id order, staging arrays) in the
+// column-major layout of sph_get_state: [0, 2n) pos, [2n, 4n) vel, [4n, 5n) rho,
+// [5n, 6n) pressure from the equation of state.
+__global__ void k_snapshot(Params P, int n, const double2* pos, const double2* vel, const double* rho,
+                           double* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double2 x = pos[i], v = vel[i];
+    const double r = rho[i];
+    double p, c;
+    eos64(P, r, p, c);
+    out[i] = x.x; out[n + i] = x.y;
+    out[2 * (size_t)n + i] = v.x; out[3 * (size_t)n + i] = v.y;
+    out[4 * (size_t)n + i] = r;
+    out[5 * (size_t)n + i] = p;
+}
+
 // Per-particle outputs of the last RHS in id order (host particles), as doubles.
 // Layout: [0] drho, [1,2] acc, [3,4] avg, [5] fs, [6] near, [7] fra_v,
 // [8..11] binv, [12..14] tau, [15..22] grads  (each block n long).

@@ -62,6 +62,8 @@ EXPORTED_SYMBOLS = (
     "sph_strerror", "sph_get_field", "sph_update_state", "sph_find_particle_pair_noalloc",
     "sph_set_initial_type", "sph_adjoint_forward", "sph_adjoint_backward",
     "sph_set_boundary_labels", "sph_set_body_motion", "sph_set_time", "sph_adjoint_motion_gradient",
+    "sph_snapshot_begin", "sph_snapshot_query", "sph_snapshot_wait", "sph_restart_size", "sph_restart_save",
+    "sph_restart_load",
 )
 
 
@@ -278,6 +280,12 @@ def load(path: str = LIB_PATH):
     lib.sph_adjoint_forward.argtypes = [P, ctypes.POINTER(SphAdjConfig), dp]
     lib.sph_adjoint_backward.argtypes = [P, ctypes.c_double, dp, dp, dp, dp]
     lib.sph_adjoint_motion_gradient.argtypes = [P, dp]
+    lib.sph_snapshot_begin.argtypes = [P, ctypes.c_int, dp, dp, dp, dp]
+    lib.sph_snapshot_query.argtypes = [P]
+    lib.sph_snapshot_wait.argtypes = [P]
+    lib.sph_restart_size.argtypes = [ctypes.c_int]
+    lib.sph_restart_save.argtypes = [P, ctypes.c_void_p, ctypes.c_size_t]
+    lib.sph_restart_load.argtypes = [P, ctypes.c_void_p, ctypes.c_size_t]
     lib.sph_find_particle_pair_noalloc.argtypes = [ctypes.POINTER(SphConfig), ctypes.c_int, ctypes.c_void_p,
                                                    ctypes.c_void_p, ctypes.c_longlong, ctypes.c_void_p,
                                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
@@ -287,6 +295,7 @@ def load(path: str = LIB_PATH):
     for name in EXPORTED_SYMBOLS:
         if name != "sph_strerror":
             getattr(lib, name).restype = ctypes.c_int
+    lib.sph_restart_size.restype = ctypes.c_size_t
     _lib = lib
     return lib
 
@@ -376,6 +385,43 @@ class Simulation:
 
     def set_time(self, t: float):
         _check(self.lib.sph_set_time(self.h, float(t)), "sph_set_time")
+
+    def snapshot_begin(self, pos, vel, rho, press):
+        """Queue a copy of the state into the given float64 arrays (2n, 2n, n, n;
+        any may be None) and return at once (sph_snapshot_begin).  The arrays
+        must stay alive until snapshot_wait; page-locked arrays let the transfer
+        overlap the following steps."""
+        arrs = [pos, vel, rho, press]
+        for a, m in zip(arrs, (2, 2, 1, 1)):
+            if a is not None and (a.dtype != np.float64 or a.size != m * self.n or not a.flags.c_contiguous):
+                raise ValueError("snapshot buffers: contiguous float64 arrays of 2n, 2n, n, n values")
+        self._snap_keep = arrs
+        _check(self.lib.sph_snapshot_begin(self.h, self.n, *[_ptr(a) if a is not None else None for a in arrs]),
+               "sph_snapshot_begin")
+
+    def snapshot_query(self) -> bool:
+        """True when the last snapshot has arrived in its host buffers."""
+        rc = self.lib.sph_snapshot_query(self.h)
+        if rc < 0:
+            _check(rc, "sph_snapshot_query")
+        return rc == 0
+
+    def snapshot_wait(self):
+        _check(self.lib.sph_snapshot_wait(self.h), "sph_snapshot_wait")
+        self._snap_keep = None
+
+    def restart_save(self) -> bytes:
+        """The exact restart image of the handle (sph_restart_save)."""
+        size = self.lib.sph_restart_size(self.n)
+        buf = ctypes.create_string_buffer(size)
+        _check(self.lib.sph_restart_save(self.h, buf, size), "sph_restart_save")
+        return buf.raw
+
+    def restart_load(self, image: bytes):
+        """Restore a restart image (sph_restart_load); n comes from the image."""
+        buf = ctypes.create_string_buffer(image, len(image))
+        _check(self.lib.sph_restart_load(self.h, buf, len(image)), "sph_restart_load")
+        self.n = int(np.frombuffer(image[12:16], np.int32)[0])
 
     def get_state(self):
         n = self.n

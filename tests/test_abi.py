@@ -83,3 +83,13 @@ def test_config_validation_codes():
     assert abs(S.baseline_dt(c) - 0.25 * c.h / 10.0) < 1e-18
     r = S.tgv_reference_config(100)
     assert r.kernel_model == S.KERNEL_GAUSSIAN and r.kernel_scale == 3.0 and r.rho0 == 1000.0
+
+
+def test_restart_image_size(built_lib):
+    """sph_restart_size: a 64-byte header and 108 bytes per particle (pos, vel 16
+    each; rho, mass, smass 8 each; type, itype, label 4 each; carried drho 8,
+    acc and avg 16 each); no device needed."""
+    lib = S.load()
+    assert lib.sph_restart_size(0) == 0
+    assert lib.sph_restart_size(1) == 64 + 108
+    assert lib.sph_restart_size(1000) == 64 + 108 * 1000
