@@ -384,6 +384,7 @@ def streaming_report(S, sim, n, dt, chunks: int = 4, every: int = 5):
     buffers before each chunk (the transfer of x, v, rho, p runs on the copy
     stream while the next steps compute), and with a synchronous sph_get_state
     before each chunk."""
+    import torch
     bufs = [torch.empty(m * n, dtype=torch.float64).pin_memory().numpy() for m in (2, 2, 1, 1)]
     res = {}
     for mode in ("none", "snapshot", "get_state"):
