@@ -479,7 +479,7 @@ def adjoint_ms_report(S):
         gcf = np.einsum("sq,sqk->k", sim.adjoint_motion_gradient(), jac[:nf])
     fd = []
     for k in (0, 1):
-        eps = 1e-6
+        eps = 1e-7          # the moving-square tests' step (Gaussian: kinks at the cut-off)
         cp, cm = coeffs.copy(), coeffs.copy()
         cp[k] += eps
         cm[k] -= eps
@@ -497,7 +497,7 @@ def adjoint_ms_report(S):
         "adjoint_particle_steps_per_s": case.n * MS_STEPS / t_bwd,
         "backward_device_ms": tb.total_ms, "backward_reverse_kernels_ms": tb.adjoint_ms,
         "dC_d_coeffs": [float(x) for x in gc], "dC_dnu": g["nu"], "fd": fd,
-        "fd_note": f"central differences eps=1e-6 of the FP64 forward over the first {MS_FD_STEPS} steps",
+        "fd_note": f"central differences eps=1e-7 of the FP64 forward over the first {MS_FD_STEPS} steps",
     }
 
 
