@@ -51,6 +51,7 @@ struct Adj {
     double2* mu3;        //   (B 21, B 22)
     double* nu_part;     // per-block partial sums of dL/dnu, one block of slots per RHS of the step
     double* nu_acc;      // [1] dL/dnu
+    double* irho;        // 1/rho of the state the reversed RHS was evaluated on (k_adj_c)
     // id order, n_host + images: adjoint of the step-start state carried from
     // step to step, and (host particles) of the rates reused as K1
     double2* lx;
@@ -394,7 +395,8 @@ __global__ void __launch_bounds__(kAdjThreads, SPH_ADJ_C_MIN_BLOCKS) k_adj_c(Par
     }
     if (live && (t & (kAdjLanes - 1)) == 0) {
         const double4 k = D.kin[c];
-        const double rho = k.z, V = D.mass[c] / rho;
+        const double rho = k.z, ir = 1.0 / rho, V = D.mass[c] * ir;
+        A.irho[c] = ir;
         double dp, dc;
         eos_deriv(P, rho, dp, dc);
         A.sx[c] = make_double2(v[0], v[1]);
@@ -616,7 +618,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_a(Params P, Sorted<R> D, Ad
         }
         // own sums: phi_b - phi_c, weight V_b
         {
-            const double Vbn = D.mass[b] / kb.z;
+            const double Vbn = D.mass[b] * A.irho[b];
             double S, f0, f1;
             rev_rawsum(r0, r1, id, G, dG, kb.z - kc.z, kb.x - kc.x, kb.y - kc.y, mc1, mc2, mc3, S, f0, f1);
             x0b += Vbn * f0; x1b += Vbn * f1;
@@ -836,7 +838,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_drag(Params P, Sorted<R> D,
         const bool cbody = D.itype[c] == SPH_TYPE_BODY;
         const double2 xc = D.pos[c];
         const double4 kc = D.kin[c];
-        const double Vc = D.mass[c] / kc.z;
+        const double Vc = D.mass[c] * A.irho[c];
         const double4 bic = D.binv64[c];
         double x0b = 0, x1b = 0, ub = 0, pb = 0, rb = 0, Vb_ = 0;
         double4 gb = make_double4(0, 0, 0, 0);
@@ -847,14 +849,14 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_drag(Params P, Sorted<R> D,
             if (!bbody && !cbody) continue;
             const double2 xb = D.pos[b];
             const double4 kb = D.kin[b];
-            const double Vb = D.mass[b] / kb.z;
+            const double Vb = D.mass[b] * A.irho[b];
             // the term of pair (a, b): a = c when b is the body particle, else a = b
             const bool c_is_a = bbody;
             const double4 bi = c_is_a ? bic : D.binv64[b];
             const double4 ka = c_is_a ? kc : kb, kbb = c_is_a ? kb : kc;
             const double Va = c_is_a ? Vc : Vb, Vbb = c_is_a ? Vb : Vc;
             const double r0 = c_is_a ? xc.x - xb.x : xb.x - xc.x, r1 = c_is_a ? xc.y - xb.y : xb.y - xc.y;
-            const double d2 = r0 * r0 + r1 * r1, d = sqrt(d2), id2 = 1.0 / d2;
+            const double d2 = r0 * r0 + r1 * r1, d = sqrt(d2), id = 1.0 / d, id2 = id * id;
             double G, dG;
             kernel_g(P, d, G, dG);
             const double L0 = bi.x * r0 + bi.y * r1, L1 = bi.z * r0 + bi.w * r1;
@@ -865,7 +867,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_drag(Params P, Sorted<R> D,
             const double wv = w * Va * Vbb;
             // d/dr of Tin
             const double gq0 = L0 + bi.x * r0 + bi.z * r1, gq1 = L1 + bi.y * r0 + bi.w * r1;
-            const double kd = dG / d;
+            const double kd = dG * id;
             const double t1 = K * du * id2;
             const double Tr0 = -P2 * (kd * r0 * L0 + G * bi.x) + t1 * (kd * r0 * Q + G * gq0 - 2.0 * G * Q * r0 * id2);
             const double Tr1 = -P2 * (kd * r1 * L0 + G * bi.y) + t1 * (kd * r1 * Q + G * gq1 - 2.0 * G * Q * r1 * id2);
@@ -1019,16 +1021,10 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_ghost_lambda(Params P, Sort
         }
 }
 
-// Reverse of k_assign_ghosts, interpolated side, one warp per flagged particle j:
-// the lanes split the ghosts of the window around j's list-build cell whose own
-// window and radius j falls in (the same cells and the same distance test as the
-// forward), adding d(sum_s lam_s . sums_s)/d(x_j, u_j, v_j, rho_j); p_j enters
-// through the equation of state, V_j = m_j / rho_j.
+// k_adj_ghost_water for one flagged particle j (all 32 lanes of the warp).
 template <typename R>
-__global__ void __launch_bounds__(kAdjThreads) k_adj_ghost_water(Params P, Sorted<R> D, Adj A, double bax,
-                                                                 double bay) {
-    const int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (j >= P.n_tot || D.nflag[j] == 0 || D.type[j] == SPH_TYPE_FIX_GHOST) return;    // whole warps
+__device__ __forceinline__ void ghost_water_one(const Params& P, const Sorted<R>& D, const Adj& A, int j, double bax,
+                                                double bay) {
     const int lane = threadIdx.x & 31;
     const double2 xj = D.pos[j], x0 = D.pos0[j];
     const int cx = (int)floor((x0.x - P.gx0) / P.cs), cy = (int)floor((x0.y - P.gy0) / P.cs);
@@ -1088,6 +1084,23 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_ghost_water(Params P, Sorte
     A.sx[j] = make_double2(sx.x + x0b, sx.y + x1b);
     A.su[j] = make_double2(su.x + ub, su.y + vb);
     A.sr[j] += rb + dp * pb;
+}
+
+// Reverse of k_assign_ghosts, interpolated side, one warp per flagged particle j
+// (a fixed grid of warps strides over the slots and skips the unflagged ones):
+// the lanes split the ghosts of the window around j's list-build cell whose own
+// window and radius j falls in (the same cells and the same distance test as the
+// forward), adding d(sum_s lam_s . sums_s)/d(x_j, u_j, v_j, rho_j); p_j enters
+// through the equation of state, V_j = m_j / rho_j.
+template <typename R>
+__global__ void __launch_bounds__(kAdjThreads) k_adj_ghost_water(Params P, Sorted<R> D, Adj A, double bax,
+                                                                 double bay) {
+    // a fixed grid of warps strides over the slots; only the flagged ones work
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < P.n_tot; j += nw) {
+        if (D.nflag[j] == 0 || D.type[j] == SPH_TYPE_FIX_GHOST) continue;    // whole warps
+        ghost_water_one(P, D, A, j, bax, bay);
+    }
 }
 
 // Reverse of the step end of the Euler predictor-corrector (stage 11,

@@ -767,7 +767,7 @@ int adj_prepare_ctx(sph_handle* h, const sph_adj_config* ac) {
             (rc = adj_alloc(X, &A.gtau, nt)) || (rc = adj_alloc(X, &A.mu1, nt)) || (rc = adj_alloc(X, &A.mu2, nt)) ||
             (rc = adj_alloc(X, &A.mu3, nt)) ||
             (rc = adj_alloc(X, &A.nu_part, (size_t)5 * blocks((long long)nt * kAdjLanes, kAdjThreads))) ||
-            (rc = adj_alloc(X, &A.nu_acc, 1)) || (rc = adj_alloc(X, &A.lx, nt)) || (rc = adj_alloc(X, &A.lv, nt)) ||
+            (rc = adj_alloc(X, &A.nu_acc, 1)) || (rc = adj_alloc(X, &A.irho, nt)) || (rc = adj_alloc(X, &A.lx, nt)) || (rc = adj_alloc(X, &A.lv, nt)) ||
             (rc = adj_alloc(X, &A.lrho, nt)) || (rc = adj_alloc(X, &A.lk_r, nh)) || (rc = adj_alloc(X, &A.lk_a, nh)))
             return rc;
         // stage states: every step of a segment if that leaves 1 GiB free, else one
@@ -1024,8 +1024,7 @@ int adj_rhs_ms(sph_handle* h, const Sorted<R>& V, int k, int pred, bool drag, in
         k_adj_ghost_lambda<R><<<ngb, kAdjThreads, 0, h->stream>>>(P, V, A, h->d_ghost_ids, h->n_ghost, h->t_phys,
                                                                   h->body_acc[0], h->body_acc[1], A.mo_part);
         k_adj_motion_sum<<<1, 256, 0, h->stream>>>(ngb, 4, A.mo_part, 1.0, A.g_motion + 4 * (size_t)jstep);
-        k_adj_ghost_water<R><<<blocks((long long)P.n_tot * 32, kAdjThreads), kAdjThreads, 0, h->stream>>>(
-            P, V, A, h->body_acc[0], h->body_acc[1]);
+        k_adj_ghost_water<R><<<148 * 8, kAdjThreads, 0, h->stream>>>(P, V, A, h->body_acc[0], h->body_acc[1]);
         h->launches += 3;
     }
     k_adj_stage_ms<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, V, A, pred, X->dt);
