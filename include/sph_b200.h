@@ -312,15 +312,17 @@ int sph_find_particle_pair_noalloc(const sph_config* cfg, int n, const double* d
  * pass is the forward's final state.
  *
  * Supported configurations (others return SPH_E_CONFIG), either kernel, with
- * or without renormalisation, without particle shifting and without MLS
- * density re-initialisation:
+ * or without renormalisation, without MLS density re-initialisation:
  *  - the normalised modified linear Riemann delta-SPH + SPS solver
- *    (SPH_SOLVER_MODLR_DELTA_SPS) with the RK4 driver, without XSPH;
+ *    (SPH_SOLVER_MODLR_DELTA_SPS) with the RK4 driver, without XSPH, with or
+ *    without particle shifting (the capped shift and its density correction
+ *    are differentiated on the branch the forward took);
  *  - the moving-square modified linear Riemann solver (SPH_SOLVER_MS_MODLR_DELTA,
  *    Morris laplacian, XSPH velocities in the continuity flux) with the Euler
  *    predictor-corrector driver, with the library's ghost assignment
  *    (ghost_assign = 1: the reverse runs through the Shepard interpolation onto
- *    the wall and body ghosts) or with caller-given ghost states.
+ *    the wall and body ghosts) or with caller-given ghost states; without
+ *    particle shifting.
  * The reverse kernels compute in FP64 for both precisions of the forward step.
  *
  * Body motion: with body_motion set, step k of the forward run (k = 0 ..

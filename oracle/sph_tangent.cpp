@@ -7,7 +7,8 @@
 // The step is written once, templated on the scalar type: with double it is a
 // second restatement of the oracle's Taylor-Green step (the pair loops of
 // Solver_Normalized_Modified_Linear_Riemann_Delta_SPS.f90:126-583 and the
-// Runge-Kutta stages of time_iteration.f90:781-1073, in the oracle's pair
+// Runge-Kutta stages of time_iteration.f90:781-1073, with the particle shift
+// of Shift_particle_position.f90:56-136 when on, in the oracle's pair
 // orientation and term order), pinned against sph_oracle.cpp by the tests;
 // with Dual (value + one directional derivative, forward-mode differentiation)
 // it returns the loss and its derivative along a chosen direction of the
@@ -22,8 +23,8 @@
 // the modified linear Riemann solver with XSPH in the continuity flux, the
 // fixed-ghost assignment, the body force and the Euler predictor-corrector with
 // a per-step body motion (oracle_tangent_ms).  Either kernel, with or without
-// renormalisation, no shifting, no density re-initialisation, no free-surface
-// particles.  Other inputs return SPH_E_CONFIG.  The pair search is a plain
+// renormalisation, with or without shifting in (1) and without in (2), no
+// density re-initialisation, no free-surface particles.  Other inputs return SPH_E_CONFIG.  The pair search is a plain
 // double loop (small cases only).
 
 #include <cmath>
@@ -63,6 +64,7 @@ using std::sqrt;
 // Constants of the configuration (the same derivation as the oracle's).
 struct TConsts {
     double pi_k, pi, e9, den, cut_min, fs_thr, dl, c012, c23, cblin, sqrt_c0, eos_b, sv, q_zero;
+    double w_dx;      // kernel value at distance dx (Shift_particle_position.f90:56-68)
 };
 
 TConsts derive(const sph_config& c) {
@@ -96,6 +98,17 @@ TConsts derive(const sph_config& c) {
     K.eos_b = c.c0sq * c.rho0 / 7.0;
     const double sr = c.kernel_scale * c.h;
     K.sv = K.pi * (sr * sr);
+    {
+        const double h = c.h, q = c.dx / h;
+        if (c.kernel_model == SPH_KERNEL_GAUSSIAN) {
+            const double factor = 1.0 / (K.pi_k * (h * h) * K.den);
+            K.w_dx = c.dx <= 3.0 * h ? (std::exp(-(q * q)) - K.e9) * factor : 0.0;
+        } else {
+            const double factor = 7.0 / (4 * K.pi_k * (h * h));
+            const double t = 1.0 - q / 2.0, t2 = t * t;
+            K.w_dx = c.dx <= 2.0 * h ? factor * (1.0 + 2.0 * q) * (t2 * t2) : 0.0;
+        }
+    }
     return K;
 }
 
@@ -155,8 +168,12 @@ struct Model {
     }
 
     // single_step_compute with the modified linear Riemann solver: drho and acc
-    // of every particle (zero acceleration for non-water particles).
-    int rhs(const Parts<T>& P, std::vector<T>& drho, std::vector<T>& acc0, std::vector<T>& acc1) const {
+    // of every particle (zero acceleration for non-water particles).  With sh
+    // given, also the particle shift of Shift_particle_position.f90:56-100 on
+    // this RHS's pairs, sh[0..1][i] = -beta h^2 sum_j (1 + R (w/w_dx)^4) V_j
+    // B_i^-1 grad_i W, and the normalised density gradient gr[0..1].
+    int rhs(const Parts<T>& P, std::vector<T>& drho, std::vector<T>& acc0, std::vector<T>& acc1,
+            std::vector<T>* sh = nullptr, std::vector<T>* gr = nullptr) const {
         const int n = P.n;
         std::vector<T> p(n), c(n), vol(n);
         for (int i = 0; i < n; ++i) { eos(P.rho[i], p[i], c[i]); vol[i] = P.mass[i] / P.rho[i]; }
@@ -325,6 +342,19 @@ struct Model {
             drho[i] = drho[i] + corr[i];
             acc0[i] = a0[i]; acc1[i] = a1[i];
         }
+        if (sh) {
+            sh[0].assign(n, T(0.0)); sh[1].assign(n, T(0.0));
+            const double h2 = C.h * C.h;
+            for (size_t k = 0; k < np; ++k) {
+                const int i = pi[k], j = pj[k];
+                const T r = w[k] / K.w_dx;
+                const T r2 = r * r;
+                const T f = C.shift_beta * h2 * (1.0 + C.shift_R * (r2 * r2));
+                sh[0][i] += -(f * ni0[k] * vol[j]); sh[1][i] += -(f * ni1[k] * vol[j]);
+                sh[0][j] += f * nj0[k] * vol[i]; sh[1][j] += f * nj1[k] * vol[i];
+            }
+            gr[0] = g0; gr[1] = g1;
+        }
         return SPH_OK;
     }
 
@@ -387,6 +417,7 @@ int run(const sph_config& cfg, int n, const T* x0, const T* y0, const T* u0, con
             for (int i = 0; i < n; ++i) { dr[i] = cr[i]; a0[i] = ca0[i]; a1[i] = ca1[i]; }
         }
         std::vector<T> Kr(n), Ka0(n), Ka1(n), Kv0(n), Kv1(n);
+        std::vector<T> sh[2], gr[2];
         // stages (time_iteration.f90:942-1047): water particles only
         for (int st = 0; st < 3; ++st) {
             const double f = st < 2 ? 0.5 * dt : dt;
@@ -401,7 +432,7 @@ int run(const sph_config& cfg, int n, const T* x0, const T* y0, const T* u0, con
                 Kr[i] += wgt * dr[i]; Ka0[i] += wgt * a0[i]; Ka1[i] += wgt * a1[i];
                 Kv0[i] += wgt * P.u[i]; Kv1[i] += wgt * P.v[i];
             }
-            if ((rc = M.rhs(P, dr, a0, a1))) return rc;
+            if ((rc = M.rhs(P, dr, a0, a1, st == 2 && cfg.shifting ? sh : nullptr, gr))) return rc;
         }
         for (int i = 0; i < n; ++i) {
             if (P.type[i] != SPH_TYPE_WATER) continue;
@@ -410,6 +441,20 @@ int run(const sph_config& cfg, int n, const T* x0, const T* y0, const T* u0, con
             P.x[i] = B0.x[i] + (Kv0[i] + P.u[i]) * dt / 6.0 + 0.5 * dt * dt * a0[i];
             P.v[i] = B0.v[i] + (Ka1[i] + a1[i]) * dt / 6.0;
             P.y[i] = B0.y[i] + (Kv1[i] + P.v[i]) * dt / 6.0 + 0.5 * dt * dt * a1[i];
+        }
+        if (cfg.shifting) {
+            // Shift_particle_position.f90:97-136 on the last RHS's pairs: capped
+            // shift of the water particles (none is near a surface in this model's
+            // scope) and the first-order density correction
+            for (int i = 0; i < n; ++i) {
+                if (P.type[i] != SPH_TYPE_WATER) continue;
+                T s0 = sh[0][i], s1 = sh[1][i];
+                const T amp = sqrt(s0 * s0 + s1 * s1);
+                if (val(amp) > cfg.shift_max) { s0 = s0 / amp * cfg.shift_max; s1 = s1 / amp * cfg.shift_max; }
+                P.x[i] = P.x[i] + s0; P.y[i] = P.y[i] + s1;
+                P.rho[i] = P.rho[i] + gr[0][i] * s0;
+                P.rho[i] = P.rho[i] + gr[1][i] * s1;
+            }
         }
         for (int i = 0; i < n; ++i) {
             cr[i] = dr[i]; ca0[i] = a0[i]; ca1[i] = a1[i];
@@ -775,7 +820,7 @@ int oracle_tangent(const sph_config* cfg, int n, const double* pos, const double
                    double* pos_out, double* vel_out, double* rho_out) {
     if (!cfg || !pos || !vel || !rho || !mass || !type || !out || n <= 0 || nsteps <= 0) return SPH_E_ARG;
     if (cfg->solver != SPH_SOLVER_MODLR_DELTA_SPS || cfg->integrator != SPH_INTEGRATOR_RK4_REUSE ||
-        cfg->shifting || cfg->xsph_eps != 0.0 || cfg->pair_rule != SPH_PAIRS_ONE_FLUID || cfg->mls_order != 0)
+        cfg->xsph_eps != 0.0 || cfg->pair_rule != SPH_PAIRS_ONE_FLUID || cfg->mls_order != 0)
         return SPH_E_CONFIG;
     if (loss == SPH_LOSS_VELOCITY_MISFIT && !target_vel) return SPH_E_ARG;
     std::vector<Dual> x(n), y(n), u(n), v(n), r(n);

@@ -52,6 +52,11 @@ struct Adj {
     double* nu_part;     // per-block partial sums of dL/dnu, one block of slots per RHS of the step
     double* nu_acc;      // [1] dL/dnu
     double* irho;        // 1/rho of the state the reversed RHS was evaluated on (k_adj_c)
+    // particle shifting of the step end (last RHS of a step)
+    double2* ssum;       // the shifting sum s = sum_b (1 + R (W/W_dx)^4) V_b G r, recomputed
+    double2* smu;        // its adjoint
+    double2* shgr;       // adjoint of grad rho from the density correction
+    double4* shbi;       // adjoint of B^-1 from delta = -beta h^2 B^-1 s
     // id order, n_host + images: adjoint of the step-start state carried from
     // step to step, and (host particles) of the rates reused as K1
     double2* lx;
@@ -433,9 +438,11 @@ __global__ void k_adj_nu_sum(int nparts, const double* part, double* acc) {
     if (threadIdx.x == 0) acc[0] += red[0];
 }
 
-// Reverse of the per-particle end of pass A.
+// Reverse of the per-particle end of pass A.  shift: the RHS is the last of a
+// step with particle shifting, whose step-end reverse left adjoints of grad rho
+// and B^-1 in shgr / shbi.
 template <typename R>
-__global__ void k_adj_point(Params P, Sorted<R> D, Adj A) {
+__global__ void k_adj_point(Params P, Sorted<R> D, Adj A, int shift) {
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= P.n_tot) return;
     const int ta = D.type[a];
@@ -445,7 +452,13 @@ __global__ void k_adj_point(Params P, Sorted<R> D, Adj A) {
     const double gr0 = (double)n1.w, gr1 = (double)n2.x;
     const double gu0 = (double)n2.w, gu1 = (double)n3.x;
     const double gv0 = (double)n3.y, gv1 = (double)n3.z;
-    const double2 ggr = A.ggr[a];
+    double2 ggr = A.ggr[a];
+    double4 gbs = make_double4(0, 0, 0, 0);
+    if (shift) {
+        const double2 sg = A.shgr[a];
+        ggr.x += sg.x; ggr.y += sg.y;
+        gbs = A.shbi[a];
+    }
     double Gr0 = ggr.x, Gr1 = ggr.y, Gu0 = 0, Gu1 = 0, Gv0 = 0, Gv1 = 0;
     double rho_b = 0.0;
     if (ta == SPH_TYPE_WATER && !P.ms) {
@@ -496,7 +509,8 @@ __global__ void k_adj_point(Params P, Sorted<R> D, Adj A) {
         raw(gr0, gr1, qr0, qr1);
         raw(gu0, gu1, qu0, qu1);
         raw(gv0, gv1, qv0, qv1);
-        const double4 gb = A.gbinv[a];
+        double4 gb = A.gbinv[a];
+        gb.x += gbs.x; gb.y += gbs.y; gb.z += gbs.z; gb.w += gbs.w;
         // adjoint of B^-1: from pass C and from grad = B^-1 g
         const double Y00 = gb.x + Gr0 * qr0 + Gu0 * qu0 + Gv0 * qv0;
         const double Y01 = gb.y + Gr0 * qr1 + Gu0 * qu1 + Gv0 * qv1;
@@ -651,16 +665,116 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_a(Params P, Sorted<R> D, Ad
                   A.sr[c] + rb - Vc / kc.z * Vb);
 }
 
+// The shifting sum of particle a over the pairs of the RHS state D, in FP64
+// (the forward forms it in the last pass C of a step, k_pass_c<..., SHIFT>):
+//   s_a = sum_b phi(d) V_b r,  phi = (1 + R (W/W_dx)^4) G,  r = x_a - x_b.
+template <typename R>
+__global__ void k_shift_sum(Params P, Sorted<R> D, Adj A) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= P.n_tot) return;
+    const double2 xa = D.pos[a];
+    const double iwdx = 1.0 / P.w_dx;
+    double s0 = 0.0, s1 = 0.0;
+    const int nn = D.npairs[a];
+    for (int e = 0; e < nn; ++e) {
+        const int b = (int)(D.pairs[(size_t)e * P.nbr_stride + a] & 0x7fffffffu);
+        const double2 xb = D.pos[b];
+        const double r0 = xa.x - xb.x, r1 = xa.y - xb.y;
+        const double d = sqrt(r0 * r0 + r1 * r1);
+        double G, dG, W;
+        kernel_gw(P, d, G, dG, W);
+        const double q = W * iwdx, q2 = q * q;
+        const double f = (1.0 + P.shift_R * (q2 * q2)) * G * (D.mass[b] / D.kin[b].z);
+        s0 += f * r0; s1 += f * r1;
+    }
+    A.ssum[a] = make_double2(s0, s1);
+}
+
+// Reverse of the shifting sums with their adjoints mu (smu): particle c adds
+// d(mu_c . s_c)/dx_c (its own sum) and d(mu_b . s_b)/d(x_c, rho_c) over its pair
+// neighbours b (their sums, through r and V_c = m_c / rho_c) to sx, sr.
+template <typename R>
+__global__ void k_adj_shift(Params P, Sorted<R> D, Adj A) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= P.n_tot) return;
+    const double2 xc = D.pos[c];
+    const double2 mc = A.smu[c];
+    const double Vc = D.mass[c] * A.irho[c];
+    const double iwdx = 1.0 / P.w_dx;
+    double x0b = 0, x1b = 0, Vb_ = 0;
+    const int nn = D.npairs[c];
+    for (int e = 0; e < nn; ++e) {
+        const int b = (int)(D.pairs[(size_t)e * P.nbr_stride + c] & 0x7fffffffu);
+        const double2 mb = A.smu[b];
+        if (mc.x == 0.0 && mc.y == 0.0 && mb.x == 0.0 && mb.y == 0.0) continue;
+        const double2 xb = D.pos[b];
+        const double r0 = xc.x - xb.x, r1 = xc.y - xb.y;
+        const double d = sqrt(r0 * r0 + r1 * r1), id = 1.0 / d;
+        double G, dG, W;
+        kernel_gw(P, d, G, dG, W);
+        const double q = W * iwdx, q2 = q * q, q4 = q2 * q2;
+        const double phi = (1.0 + P.shift_R * q4) * G;
+        // dphi/dd: dW/dd = G d
+        const double dphi = 4.0 * P.shift_R * q2 * q * (G * d * iwdx) * G + (1.0 + P.shift_R * q4) * dG;
+        const double Vb = D.mass[b] * A.irho[b];
+        // own sum: mu_c . V_b phi r, r = x_c - x_b
+        const double rm = r0 * mc.x + r1 * mc.y;
+        x0b += Vb * (phi * mc.x + dphi * rm * r0 * id);
+        x1b += Vb * (phi * mc.y + dphi * rm * r1 * id);
+        // the neighbour's sum: mu_b . V_c phi r', r' = -r
+        const double rmb = -(r0 * mb.x + r1 * mb.y);
+        x0b -= Vc * (phi * mb.x - dphi * rmb * r0 * id);
+        x1b -= Vc * (phi * mb.y - dphi * rmb * r1 * id);
+        Vb_ += phi * rmb;
+    }
+    const double2 sx = A.sx[c];
+    A.sx[c] = make_double2(sx.x + x0b, sx.y + x1b);
+    A.sr[c] -= Vc * A.irho[c] * Vb_;
+}
+
 // Reverse of stage 3 (the step end) from the id-order adjoints of the end state
 // and of the carried rates.  Non-integrated host particles keep their state.
+// With shift: the step end also moved the water particles that are not near
+// the surface by the capped shift cap(delta), delta = -beta h^2 B^-1 s (s from
+// k_shift_sum), and corrected rho by grad rho . cap(delta)
+// (Shift_particle_position.f90:97-136): its reverse leaves the adjoints of s
+// (smu), grad rho (shgr) and B^-1 (shbi) of the last RHS; the cap is the branch
+// the forward took.
 template <typename R>
-__global__ void k_adj_stage3(Params P, Sorted<R> D, Adj A, double dt) {
+__global__ void k_adj_stage3(Params P, Sorted<R> D, Adj A, double dt, int shift) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= P.n_tot) return;
     const int i = D.id[s];
     double2 lx = make_double2(0, 0), lv = make_double2(0, 0);
     double lrho = 0.0;
     if (i < P.n_host) { lx = A.lx[i]; lv = A.lv[i]; lrho = A.lrho[i]; }
+    if (shift) {
+        double2 mu = make_double2(0, 0), sg = make_double2(0, 0);
+        double4 sb = make_double4(0, 0, 0, 0);
+        if (i < P.n_host && D.type[s] == SPH_TYPE_WATER && !(D.flags[s] & 2)) {
+            const double2 ss = A.ssum[s];
+            const double4 bi = D.binv64[s];
+            const double c = -P.shift_beta * (P.h * P.h);
+            const double d0 = c * (bi.x * ss.x + bi.y * ss.y), d1 = c * (bi.z * ss.x + bi.w * ss.y);
+            const double amp = sqrt(d0 * d0 + d1 * d1);
+            const bool capped = amp > P.shift_max;
+            const double dc0 = capped ? d0 / amp * P.shift_max : d0, dc1 = capped ? d1 / amp * P.shift_max : d1;
+            const double g0 = (double)D.nb1[s].w, g1 = (double)D.nb2[s].x;
+            // x' = x + dc, rho' = rho + g.dc
+            const double b0 = lx.x + lrho * g0, b1 = lx.y + lrho * g1;
+            sg = make_double2(lrho * dc0, lrho * dc1);
+            double e0 = b0, e1 = b1;
+            if (capped) {
+                const double k = P.shift_max / amp, h0 = d0 / amp, h1 = d1 / amp;
+                const double hb = h0 * b0 + h1 * b1;
+                e0 = k * (b0 - h0 * hb); e1 = k * (b1 - h1 * hb);
+            }
+            // delta = c B^-1 s
+            mu = make_double2(c * (bi.x * e0 + bi.z * e1), c * (bi.y * e0 + bi.w * e1));
+            sb = make_double4(c * e0 * ss.x, c * e0 * ss.y, c * e1 * ss.x, c * e1 * ss.y);
+        }
+        A.smu[s] = mu; A.shgr[s] = sg; A.shbi[s] = sb;
+    }
     for (int k = 0; k < 4; ++k) { A.lr[k][s] = 0.0; A.la[k][s] = make_double2(0, 0); }
     A.lxe[s] = make_double2(0, 0);
     if (i < P.n_host && integrated(P, D.type[s])) {

@@ -721,9 +721,10 @@ int snap_io(sph_handle* h, const Snap& s, int k, int n, bool save) {
 
 int adj_config_ok(const sph_handle* h, int loss) {
     const Params& P = h->P;
-    if (h->cfg.shifting || P.mls_order || P.muscl) return SPH_E_CONFIG;
+    if (P.mls_order || P.muscl) return SPH_E_CONFIG;
     if (P.ms) {
         // moving-square modified linear solver, Morris laplacian, Euler predictor-corrector
+        if (h->cfg.shifting) return SPH_E_CONFIG;
         if (h->cfg.solver != SPH_SOLVER_MS_MODLR_DELTA || P.laplacian != 1) return SPH_E_CONFIG;
         if (h->cfg.integrator != SPH_INTEGRATOR_EULER_PC || h->cfg.periodic) return SPH_E_CONFIG;
     } else {
@@ -767,7 +768,8 @@ int adj_prepare_ctx(sph_handle* h, const sph_adj_config* ac) {
             (rc = adj_alloc(X, &A.gtau, nt)) || (rc = adj_alloc(X, &A.mu1, nt)) || (rc = adj_alloc(X, &A.mu2, nt)) ||
             (rc = adj_alloc(X, &A.mu3, nt)) ||
             (rc = adj_alloc(X, &A.nu_part, (size_t)5 * blocks((long long)nt * kAdjLanes, kAdjThreads))) ||
-            (rc = adj_alloc(X, &A.nu_acc, 1)) || (rc = adj_alloc(X, &A.irho, nt)) || (rc = adj_alloc(X, &A.lx, nt)) || (rc = adj_alloc(X, &A.lv, nt)) ||
+            (rc = adj_alloc(X, &A.nu_acc, 1)) || (rc = adj_alloc(X, &A.irho, nt)) || (rc = adj_alloc(X, &A.ssum, nt)) ||
+            (rc = adj_alloc(X, &A.smu, nt)) || (rc = adj_alloc(X, &A.shgr, nt)) || (rc = adj_alloc(X, &A.shbi, nt)) || (rc = adj_alloc(X, &A.lx, nt)) || (rc = adj_alloc(X, &A.lv, nt)) ||
             (rc = adj_alloc(X, &A.lrho, nt)) || (rc = adj_alloc(X, &A.lk_r, nh)) || (rc = adj_alloc(X, &A.lk_a, nh)))
             return rc;
         // stage states: every step of a segment if that leaves 1 GiB free, else one
@@ -913,23 +915,32 @@ int step_keep(sph_handle* h, double dt, int j, bool full) {
 
 // Reverse of one RHS evaluation on the stage state V, with the rate adjoints
 // of RHS k of the step; stage = the stage that produced V (-1: the step start).
+// shift: the last RHS of a step with particle shifting (pass A already re-run by
+// adj_step, the step-end reverse left smu / shgr / shbi).
 template <typename R>
-int adj_rhs(sph_handle* h, const Sorted<R>& V, int k, int stage) {
+int adj_rhs(sph_handle* h, const Sorted<R>& V, int k, int stage, bool shift = false) {
     const Params& P = h->P;
     AdjCtx* X = h->adj;
     Adj& A = X->A;
     const int nb = blocks(P.n_tot, kAdjThreads);
     const int nbc = blocks((long long)P.n_tot * kAdjLanes, kAdjThreads);
-    tic(h, PH_A);
-    k_pass_a<R, false><<<nb, 128, 0, h->stream>>>(P, V);
-    k_surface<R><<<nb, 128, 0, h->stream>>>(P, V);
-    k_near<R><<<nb, 128, 0, h->stream>>>(P, V);
+    if (!shift) {
+        tic(h, PH_A);
+        k_pass_a<R, false><<<nb, 128, 0, h->stream>>>(P, V);
+        k_surface<R><<<nb, 128, 0, h->stream>>>(P, V);
+        k_near<R><<<nb, 128, 0, h->stream>>>(P, V);
+        h->launches += 3;
+    }
     tic(h, PH_ADJ);
     k_adj_c<R><<<nbc, kAdjThreads, 0, h->stream>>>(P, V, A, A.lr[k], A.la[k], A.nu_part + (size_t)k * nbc);
-    k_adj_point<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, V, A);
+    if (shift) {
+        k_adj_shift<R><<<nb, kAdjThreads, 0, h->stream>>>(P, V, A);
+        h->launches += 1;
+    }
+    k_adj_point<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, V, A, shift ? 1 : 0);
     k_adj_a<R><<<nb, kAdjThreads, 0, h->stream>>>(P, V, A, stage, X->dt, nullptr);
     CK(cudaGetLastError());
-    h->launches += 6;
+    h->launches += 3;
     return SPH_OK;
 }
 
@@ -953,11 +964,25 @@ int adj_step(sph_handle* h, bool first, int j) {
     const Params& P = h->P;
     Sorted<R>& D = sorted<R>(h);
     const int nb = blocks(P.n_tot, 256);
+    const bool shift = h->cfg.shifting != 0;
+    if (shift) {
+        // the step end's shift reads the last RHS's pass A (B^-1, grad rho, flags)
+        // and its shifting sum: re-form them on the kept state S3 first
+        const Sorted<R> V = stage_view<R>(h, j, 2);
+        const int nba = blocks(P.n_tot, 128);
+        tic(h, PH_A);
+        k_pass_a<R, false><<<nba, 128, 0, h->stream>>>(P, V);
+        k_surface<R><<<nba, 128, 0, h->stream>>>(P, V);
+        k_near<R><<<nba, 128, 0, h->stream>>>(P, V);
+        tic(h, PH_ADJ);
+        k_shift_sum<R><<<nb, 256, 0, h->stream>>>(P, V, A);
+        h->launches += 4;
+    }
     tic(h, PH_ADJ);
-    k_adj_stage3<R><<<nb, 256, 0, h->stream>>>(P, D, A, dt);
+    k_adj_stage3<R><<<nb, 256, 0, h->stream>>>(P, D, A, dt, shift ? 1 : 0);
     h->launches += 1;
     for (int k = 2; k >= 0; --k)
-        if ((rc = adj_rhs<R>(h, stage_view<R>(h, j, k), k + 1, k))) return rc;
+        if ((rc = adj_rhs<R>(h, stage_view<R>(h, j, k), k + 1, k, shift && k == 2))) return rc;
     if (first) {
         // the fresh K1 of the first step was evaluated on the step-start state
         k_adj_load<R><<<nb, 256, 0, h->stream>>>(P, D, nullptr, nullptr);
@@ -1017,7 +1042,7 @@ int adj_rhs_ms(sph_handle* h, const Sorted<R>& V, int k, int pred, bool drag, in
         k_adj_nu_sum<<<1, 256, 0, h->stream>>>(nb, part, A.nu_acc);
         h->launches += 3;
     }
-    k_adj_point<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, V, A);
+    k_adj_point<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, V, A, 0);
     k_adj_a<R, true><<<nb, kAdjThreads, 0, h->stream>>>(P, V, A, 0, X->dt, A.lg[k]);
     if (ghosts) {
         const int ngb = blocks((long long)h->n_ghost * 32, kAdjThreads);

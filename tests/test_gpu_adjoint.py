@@ -30,11 +30,13 @@ REL_TOL = 1e-4
 
 
 def _case(kind):
-    if kind == "wendland-renorm":
+    """"-shift" kinds keep the configuration's particle shifting (the reference
+    Taylor-Green case shifts every step); the others switch it off."""
+    if kind.startswith("wendland-renorm"):
         case = S.make_tgv(32, solver=S.SOLVER_MODLR_DELTA_SPS, jitter=0.05, seed=11)
     else:
         case = S.make_tgv(32, reference=True, jitter=0.05, seed=12)
-    case.cfg.shifting = 0
+    case.cfg.shifting = 1 if kind.endswith("-shift") else 0
     case.cfg.mls_order = 0
     return case
 
@@ -84,7 +86,8 @@ def _check(ad, fd, what):
     assert abs(ad - fd) <= REL_TOL * abs(fd), (what, ad, fd, abs(ad - fd) / abs(fd))
 
 
-@pytest.mark.parametrize("kind", ["wendland-renorm", "reference-gaussian"])
+@pytest.mark.parametrize("kind", ["wendland-renorm", "reference-gaussian", "wendland-renorm-shift",
+                                  "reference-gaussian-shift"])
 @pytest.mark.parametrize("pre_steps", [0, 3])
 def test_adjoint_matches_central_differences(lib, kind, pre_steps):
     case = _case(kind)
@@ -174,7 +177,8 @@ def test_adjoint_of_the_mixed_precision_step(lib):
     assert abs(gm["nu"] - g64["nu"]) <= 1e-4 * abs(g64["nu"])
 
 
-@pytest.mark.parametrize("kind", ["wendland-renorm", "reference-gaussian"])
+@pytest.mark.parametrize("kind", ["wendland-renorm", "reference-gaussian", "wendland-renorm-shift",
+                                  "reference-gaussian-shift"])
 def test_adjoint_matches_cpu_tangent_linear_reference(lib, oracle, kind):
     """g.delta from the GPU adjoint against the FP64 CPU tangent-linear model of
     the same steps (oracle/sph_tangent.cpp, forward-mode derivative with the

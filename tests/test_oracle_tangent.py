@@ -8,16 +8,19 @@ import sph_b200 as S
 
 
 def _case(kind):
-    if kind == "wendland-renorm":
+    if kind.startswith("wendland-renorm"):
         case = S.make_tgv(24, solver=S.SOLVER_MODLR_DELTA_SPS, jitter=0.05, seed=3)
     else:
         case = S.make_tgv(24, reference=True, jitter=0.05, seed=4)
-    case.cfg.shifting = 0
+    case.cfg.shifting = 1 if kind.endswith("-shift") else 0
     case.cfg.mls_order = 0
     return case
 
 
-@pytest.mark.parametrize("kind", ["wendland-renorm", "reference-gaussian"])
+KINDS = ["wendland-renorm", "reference-gaussian", "wendland-renorm-shift", "reference-gaussian-shift"]
+
+
+@pytest.mark.parametrize("kind", KINDS)
 def test_tangent_value_path_reproduces_the_oracle(oracle, kind):
     case = _case(kind)
     dt = S.baseline_dt(case.cfg)
@@ -30,14 +33,14 @@ def test_tangent_value_path_reproduces_the_oracle(oracle, kind):
     assert np.abs(rho - rrho).max() <= 1e-10 * np.abs(rrho - case.cfg.rho0).max()
 
 
-@pytest.mark.parametrize("kind", ["wendland-renorm", "reference-gaussian"])
+@pytest.mark.parametrize("kind", KINDS)
 def test_tangent_matches_its_central_differences(oracle, kind):
     case = _case(kind)
     dt = S.baseline_dt(case.cfg)
     d = np.random.default_rng(1).standard_normal(2 * case.n)
     args = (case.pos, case.vel, case.rho, case.mass, case.type, 5, dt)
     _, dL, _ = oracle.tangent(case.cfg, *args, dvel=d, loss=1)
-    eps = 1e-6 if kind == "wendland-renorm" else 1e-7
+    eps = 1e-6 if kind.startswith("wendland") else 1e-7
     Lp = oracle.tangent(case.cfg, case.pos, case.vel + eps * d, *args[2:], loss=1)[0]
     Lm = oracle.tangent(case.cfg, case.pos, case.vel - eps * d, *args[2:], loss=1)[0]
     assert abs(dL - (Lp - Lm) / (2 * eps)) <= 1e-6 * abs(dL)
