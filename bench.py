@@ -311,10 +311,16 @@ def adjoint_leg(S, precision):
     particles, 500 steps, a checkpoint every 32 steps, loss = squared velocity
     misfit at the end against a target from a forward run whose initial
     velocity carries 8 seeded Fourier modes of amplitude 0.05 U0.  Solver:
-    modified linear Riemann + delta-SPH + SPS, Wendland C2, renormalised,
-    particle shifting every step.  Both calls return only when their device work is done, so the
+    modified linear Riemann + delta-SPH + SPS, Wendland C2, renormalised, no
+    shifting: with shifting this solver amplifies lattice-scale perturbations
+    (the mixed and FP64 runs of the same start drift apart e-fold every few
+    steps until they saturate), so over 500 steps the exact gradient is
+    dominated by that growth and no difference check can confirm it; the
+    shifting reverse is checked on short horizons by the tests.  Both calls
+    return only when their device work is done, so the
     host clock around each is its cost; the device-event sums are beside it."""
     case = S.make_tgv(ADJ_SIDE, solver=S.SOLVER_MODLR_DELTA_SPS, precision=precision)
+    case.cfg.shifting = 0
     case.cfg.mls_order = 0      # density re-initialisation is outside the adjoint's scope
     dt = S.baseline_dt(case.cfg)
     dv = S.fourier_perturbation(case.pos, n_modes=8, amp=0.05, seed=2024)
@@ -369,7 +375,7 @@ def adjoint_report(S):
     return {
         "case": f"TGV {ADJ_SIDE}x{ADJ_SIDE} ({case.n} particles), {ADJ_STEPS} steps, checkpoint every {ADJ_EVERY}, "
                 "velocity-misfit loss vs a target from 8 seeded Fourier modes (0.05 U0); modified linear Riemann "
-                "+ delta-SPH + SPS, Wendland C2, renormalised, particle shifting every step",
+                "+ delta-SPH + SPS, Wendland C2, renormalised, no shifting",
         "mixed": {k: m[k] for k in keep}, "fp64": {k: d[k] for k in keep},
         "adjoint_over_forward": m["adjoint_over_forward"],
         "grad_vel0_l2_mixed_vs_fp64": float(np.linalg.norm(gm - g64) / np.linalg.norm(g64)),
