@@ -128,6 +128,20 @@ def roofline_traffic():
     return None
 
 
+def pass_c_instructions():
+    """Measured warp instructions per slot of the pass-C kernel (ncu capture
+    summarised in profiles/), or None."""
+    path = os.path.join(ROOT, "profiles", "pass_c_warp_instructions_per_slot.txt")
+    try:
+        for line in open(path):
+            line = line.strip()
+            if line and not line.startswith("#"):
+                return float(line.split()[0])
+    except OSError:
+        return None
+    return None
+
+
 def peaks():
     try:
         return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))), "measured"
@@ -255,6 +269,16 @@ def run_native(args, rank, world, local):
             "frac": achieved / pk["hbm_gbs"], "traffic": (tr * n_tot if tr else None),
             "kernel": "k_pass_c<float,MUSCL>", "launch_ms": passc_ms, "algorithmic_bytes": alg,
             "peak_kind": pk_kind + " (burst copy)"}
+    # pass C is bound by instruction issue, not bytes: the same launch against the
+    # issue limit of 4 warp instructions per SM per clock (148 SMs, sampled clock)
+    ipb = pass_c_instructions()
+    if ipb:
+        mhz = (clocks_info or {}).get("sm_mhz") or 1965.0
+        issue_peak = 4.0 * 148 * mhz * 1e6
+        issue_ach = ipb * n_tot / (passc_ms / 1e3)
+        roof["issue"] = {"achieved": issue_ach, "peak": issue_peak, "unit": "warp-instructions/s",
+                         "frac": issue_ach / issue_peak, "instructions_per_slot": ipb, "sm_mhz": mhz,
+                         "source": "ncu smsp__inst_executed.sum per slot (profiles/) x slots / live launch time"}
 
     # ---- adjoint cost (rank 0) -------------------------------------------------
     adj = adj_ms = None
