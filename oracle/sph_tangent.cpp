@@ -18,8 +18,9 @@
 // derivative is that of the taken branch with the pair set held fixed, which
 // is what the adjoint differentiates too.
 //
-// Scope: (1) Taylor-Green: the modified linear Riemann delta-SPH + SPS solver,
-// RK4 with the K1 reuse, periodic images (oracle_tangent); (2) moving square:
+// Scope: (1) Taylor-Green: the modified linear Riemann and the MUSCL linear
+// Riemann delta-SPH + SPS solvers, RK4 with the K1 reuse, periodic images
+// (oracle_tangent); (2) moving square:
 // the modified linear Riemann solver with XSPH in the continuity flux, the
 // fixed-ghost assignment, the body force and the Euler predictor-corrector with
 // a per-step body motion (oracle_tangent_ms).  Either kernel, with or without
@@ -110,6 +111,30 @@ TConsts derive(const sph_config& c) {
         }
     }
     return K;
+}
+
+// MUSCL_Limiter (Taylor_Green_Vortex/function_module.f90:34-80), branches taken on
+// the values, with std::min / std::max's choice of operand on ties.
+template <class T>
+inline T tmin(const T& a, const T& b) { return val(b) < val(a) ? b : a; }
+template <class T>
+inline T tmax(const T& a, const T& b) { return val(a) < val(b) ? b : a; }
+template <class T>
+void muscl_limiter_t(const T& di, const T& dj, const T& dij, T& li, T& lj) {
+    const double beta_lim = 1.3, diff = 0.5;
+    if (val(dj) > 0.0) {
+        const T lim = tmax(T(0.0), tmax(tmin(beta_lim * di, dj), tmin(di, beta_lim * dj)));
+        if (val(lim) > 0.5 * val(dij) && std::fabs(val(lim)) > 0.0) {
+            const bool first = val(di) > val(dj);
+            li = dij * (first ? diff : 0.0); lj = dij * (first ? 0.0 : diff);
+        } else { li = lim; lj = lim; }
+    } else {
+        const T lim = tmin(T(0.0), tmin(tmax(beta_lim * di, dj), tmax(di, beta_lim * dj)));
+        if (val(lim) < 0.5 * val(dij) && std::fabs(val(lim)) > 0.0) {
+            const bool first = val(di) < val(dj);
+            li = dij * (first ? diff : 0.0); lj = dij * (first ? 0.0 : diff);
+        } else { li = lim; lj = lim; }
+    }
 }
 
 // All particles of one step (hosts, then periodic images).
@@ -264,6 +289,22 @@ struct Model {
             tau[1][i] = (nut * sxy) * P.rho[i];
             tau[2][i] = (2.0 * nut * syy - kk - blin) * P.rho[i];
         }
+        // MUSCL: normalised gradients of p, u, v (Solver_Normalized_MUSCL_Linear_Riemann_Delta_SPS.f90:151-185)
+        const bool muscl = C.solver == SPH_SOLVER_MUSCL_DELTA_SPS;
+        std::vector<T> gp[2], gu[2], gv[2];
+        if (muscl) {
+            for (int q = 0; q < 2; ++q) { gp[q].assign(n, T(0.0)); gu[q].assign(n, T(0.0)); gv[q].assign(n, T(0.0)); }
+            for (size_t k = 0; k < np; ++k) {
+                const int i = pi[k], j = pj[k];
+                const T dpp = p[j] - p[i], dpu = -(P.u[i] - P.u[j]), dpv = -(P.v[i] - P.v[j]);
+                gp[0][i] += dpp * vol[j] * ni0[k]; gp[1][i] += dpp * vol[j] * ni1[k];
+                gp[0][j] += dpp * vol[i] * nj0[k]; gp[1][j] += dpp * vol[i] * nj1[k];
+                gu[0][i] += dpu * vol[j] * ni0[k]; gu[1][i] += dpu * vol[j] * ni1[k];
+                gu[0][j] += dpu * vol[i] * nj0[k]; gu[1][j] += dpu * vol[i] * nj1[k];
+                gv[0][i] += dpv * vol[j] * ni0[k]; gv[1][i] += dpv * vol[j] * ni1[k];
+                gv[0][j] += dpv * vol[i] * nj0[k]; gv[1][j] += dpv * vol[i] * nj1[k];
+            }
+        }
         // main pair loop (Solver_..._SPS.f90:300-502)
         std::vector<T> cont(n, T(0.0)), a0(n, T(0.0)), a1(n, T(0.0));
         for (size_t k = 0; k < np; ++k) {
@@ -275,16 +316,32 @@ struct Model {
             const T r2 = dx0[k] * dx0[k] + dx1[k] * dx1[k];
             const T d = sqrt(r2);
             const T e0 = -dx0[k] / d, e1 = -dx1[k] / d;
-            const T UL = P.u[i] * e0 + P.v[i] * e1, UR = P.u[j] * e0 + P.v[j] * e1;
+            // left / right states: the particles' own, or the MUSCL reconstructions
+            // (Solver_Normalized_MUSCL_Linear_Riemann_Delta_SPS.f90:470-502)
+            T PL = p[i], PR = p[j], uI = P.u[i], vI = P.v[i], uJ = P.u[j], vJ = P.v[j];
+            if (muscl) {
+                const T x0 = -dx0[k], x1 = -dx1[k];     // j - i
+                T li, lj;
+                muscl_limiter_t(0.5 * (gp[0][i] * x0 + gp[1][i] * x1), -0.5 * (gp[0][j] * x0 + gp[1][j] * x1),
+                                p[j] - p[i], li, lj);
+                PL = p[i] + li; PR = p[j] - lj;
+                muscl_limiter_t(0.5 * (gu[0][i] * x0 + gu[1][i] * x1), -0.5 * (gu[0][j] * x0 + gu[1][j] * x1),
+                                -(P.u[i] - P.u[j]), li, lj);
+                uI = P.u[i] + li; uJ = P.u[j] - lj;
+                muscl_limiter_t(0.5 * (gv[0][i] * x0 + gv[1][i] * x1), -0.5 * (gv[0][j] * x0 + gv[1][j] * x1),
+                                -(P.v[i] - P.v[j]), li, lj);
+                vI = P.v[i] + li; vJ = P.v[j] - lj;
+            }
+            const T UL = uI * e0 + vI * e1, UR = uJ * e0 + vJ * e1;
             const T Ubar = (UL + UR) / 2.0;
-            const T Us = Ubar + 0.5 * (p[i] - p[j]) / (rbar * K.sqrt_c0);
+            const T Us = Ubar + 0.5 * (PL - PR) / (rbar * K.sqrt_c0);
             const T vs0 = (Us - Ubar) * e0 + vbar0, vs1 = (Us - Ubar) * e1 + vbar1;
             const T dU = UL - UR;
             const T m3 = val(dU) > 0.0 ? 3.0 * dU : T(0.0);
             const T bR = val(m3) < val(cbar) ? m3 : cbar;
             const T Ps = Pbar + 0.5 * bR * rbar * dU;
-            const T tmi = (P.u[i] - vs0) * ni0[k] + (P.v[i] - vs1) * ni1[k];
-            const T tmj = -((P.u[j] - vs0) * nj0[k] + (P.v[j] - vs1) * nj1[k]);
+            const T tmi = (uI - vs0) * ni0[k] + (vI - vs1) * ni1[k];
+            const T tmj = -((uJ - vs0) * nj0[k] + (vJ - vs1) * nj1[k]);
             cont[i] += 2.0 * ri * Vj * tmi;
             cont[j] += 2.0 * rj * Vi * tmj;
             const T rij = 1.0 / (ri * rj);
@@ -819,7 +876,8 @@ int oracle_tangent(const sph_config* cfg, int n, const double* pos, const double
                    double dnu, int nsteps, double dt, int loss, const double* target_vel, double* out,
                    double* pos_out, double* vel_out, double* rho_out) {
     if (!cfg || !pos || !vel || !rho || !mass || !type || !out || n <= 0 || nsteps <= 0) return SPH_E_ARG;
-    if (cfg->solver != SPH_SOLVER_MODLR_DELTA_SPS || cfg->integrator != SPH_INTEGRATOR_RK4_REUSE ||
+    if ((cfg->solver != SPH_SOLVER_MODLR_DELTA_SPS && cfg->solver != SPH_SOLVER_MUSCL_DELTA_SPS) ||
+        cfg->integrator != SPH_INTEGRATOR_RK4_REUSE ||
         cfg->xsph_eps != 0.0 || cfg->pair_rule != SPH_PAIRS_ONE_FLUID || cfg->mls_order != 0)
         return SPH_E_CONFIG;
     if (loss == SPH_LOSS_VELOCITY_MISFIT && !target_vel) return SPH_E_ARG;

@@ -8,7 +8,9 @@ import sph_b200 as S
 
 
 def _case(kind):
-    if kind.startswith("wendland-renorm"):
+    if kind.startswith("muscl"):
+        case = S.make_tgv(24, solver=S.SOLVER_MUSCL_DELTA_SPS, jitter=0.05, seed=6)
+    elif kind.startswith("wendland-renorm"):
         case = S.make_tgv(24, solver=S.SOLVER_MODLR_DELTA_SPS, jitter=0.05, seed=3)
     else:
         case = S.make_tgv(24, reference=True, jitter=0.05, seed=4)
@@ -17,7 +19,8 @@ def _case(kind):
     return case
 
 
-KINDS = ["wendland-renorm", "reference-gaussian", "wendland-renorm-shift", "reference-gaussian-shift"]
+KINDS = ["wendland-renorm", "reference-gaussian", "wendland-renorm-shift", "reference-gaussian-shift", "muscl",
+         "muscl-shift"]
 
 
 @pytest.mark.parametrize("kind", KINDS)
@@ -40,6 +43,7 @@ def test_tangent_matches_its_central_differences(oracle, kind):
     d = np.random.default_rng(1).standard_normal(2 * case.n)
     args = (case.pos, case.vel, case.rho, case.mass, case.type, 5, dt)
     _, dL, _ = oracle.tangent(case.cfg, *args, dvel=d, loss=1)
+    # 1e-7 for the Gaussian (kink at its cut-off) and MUSCL (limiter branch switches)
     eps = 1e-6 if kind.startswith("wendland") else 1e-7
     Lp = oracle.tangent(case.cfg, case.pos, case.vel + eps * d, *args[2:], loss=1)[0]
     Lm = oracle.tangent(case.cfg, case.pos, case.vel - eps * d, *args[2:], loss=1)[0]
@@ -56,5 +60,6 @@ def test_tangent_matches_its_central_differences(oracle, kind):
 
 def test_tangent_rejects_configurations_outside_its_scope(oracle):
     case = S.make_tgv(8, solver=S.SOLVER_MUSCL_DELTA_SPS)
+    case.cfg.mls_order = 6
     with pytest.raises(RuntimeError):
         oracle.tangent(case.cfg, case.pos, case.vel, case.rho, case.mass, case.type, 1, 1e-4, loss=1)
