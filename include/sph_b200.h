@@ -313,10 +313,11 @@ int sph_find_particle_pair_noalloc(const sph_config* cfg, int n, const double* d
  *
  * Supported configurations (others return SPH_E_CONFIG), either kernel, with
  * or without renormalisation, without MLS density re-initialisation:
- *  - the normalised modified linear Riemann delta-SPH + SPS solver
- *    (SPH_SOLVER_MODLR_DELTA_SPS) with the RK4 driver, without XSPH, with or
- *    without particle shifting (the capped shift and its density correction
- *    are differentiated on the branch the forward took);
+ *  - the normalised modified linear Riemann and MUSCL linear Riemann delta-SPH
+ *    + SPS solvers (SPH_SOLVER_MODLR_DELTA_SPS without XSPH,
+ *    SPH_SOLVER_MUSCL_DELTA_SPS) with the RK4 driver, with or without particle
+ *    shifting (the limiter, the capped shift and its density correction are
+ *    differentiated on the branch the forward took);
  *  - the moving-square modified linear Riemann solver (SPH_SOLVER_MS_MODLR_DELTA,
  *    Morris laplacian, XSPH velocities in the continuity flux) with the Euler
  *    predictor-corrector driver, with the library's ghost assignment

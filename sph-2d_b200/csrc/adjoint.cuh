@@ -52,6 +52,12 @@ struct Adj {
     double* nu_part;     // per-block partial sums of dL/dnu, one block of slots per RHS of the step
     double* nu_acc;      // [1] dL/dnu
     double* irho;        // 1/rho of the state the reversed RHS was evaluated on (k_adj_c)
+    // MUSCL: adjoints of the normalised grad p, u, v from the pass C reverse, and
+    // the multipliers of pass A's raw grad p sums
+    double2* ggp;
+    double2* ggu;
+    double2* ggv;
+    double2* mu4;
     // particle shifting of the step end (last RHS of a step)
     double2* ssum;       // the shifting sum s = sum_b (1 + R (W/W_dx)^4) V_b G r, recomputed
     double2* smu;        // its adjoint
@@ -127,11 +133,12 @@ struct PSide {
     double t0, t1, t2;    // tau xx, xy, yy
     double g0, g1;        // grad rho
     double ax, ay;        // XSPH average velocity (moving-square solver)
+    double gp0, gp1, gu0, gu1, gv0, gv1;   // normalised grad p, u, v (MUSCL)
     double4 bi;           // B^-1
     bool water, near;
 };
 
-template <typename R, bool MS = false>
+template <typename R, bool MS = false, bool MUSCL = false>
 __device__ __forceinline__ PSide load_side(const Sorted<R>& D, int s) {
     PSide o;
     o.x = D.pos[s];
@@ -150,6 +157,13 @@ __device__ __forceinline__ PSide load_side(const Sorted<R>& D, int s) {
     o.water = D.type[s] == SPH_TYPE_WATER;
     o.near = (D.flags[s] & 2) != 0;
     o.ax = o.ay = 0.0;
+    o.gp0 = o.gp1 = o.gu0 = o.gu1 = o.gv0 = o.gv1 = 0.0;
+    if (MUSCL) {
+        // nb2 = (grad rho y, grad p x, grad p y, grad u x), nb3 = (grad u y, grad v x, grad v y, 0)
+        const typename VT<R>::V4 n2 = D.nb2[s], n3 = D.nb3[s];
+        o.gp0 = (double)n2.y; o.gp1 = (double)n2.z; o.gu0 = (double)n2.w; o.gu1 = (double)n3.x;
+        o.gv0 = (double)n3.y; o.gv1 = (double)n3.z;
+    }
     if (MS) {
         const typename VT<R>::V2 g = D.avg[s];
         o.ax = (double)g.x; o.ay = (double)g.y;
@@ -168,15 +182,63 @@ struct PBar {
     double nu;
     double avg0, avg1;    // of avg_a - avg_b (MS)
     double mb;            // of m_b (explicit; V_b = m_b/rho_b is in Vb)
+    // MUSCL: of the normalised grad p, u, v of a and of b
+    double gpa0, gpa1, gua0, gua1, gva0, gva1, gpb0, gpb1, gub0, gub1, gvb0, gvb1;
 };
+
+// Reverse of muscl_limiter on the branch the forward took: lim is one of 0,
+// 1.3 di, dj, di, 1.3 dj (the min / max chain), or the large-jump branch gives
+// dij/2 to one side.  From the adjoints (lib, ljb) of (li, lj), the adjoints of
+// (di, dj, dij).
+__device__ __forceinline__ void muscl_limiter_rev(double di, double dj, double dij, double lib, double ljb,
+                                                  double& dib, double& djb, double& dijb) {
+    const double b = 1.3, bdi = b * di, bdj = b * dj;
+    const bool pos = dj > 0.0;
+    double lim, cdi = 0.0, cdj = 0.0;            // lim = cdi di + cdj dj on the taken branch
+    if (pos) {
+        // max(0, max(min(bdi, dj), min(di, bdj)))
+        const bool m1a = bdi <= dj;
+        const double m1 = m1a ? bdi : dj, m1i = m1a ? b : 0.0, m1j = m1a ? 0.0 : 1.0;
+        const bool m2a = di <= bdj;
+        const double m2 = m2a ? di : bdj, m2i = m2a ? 1.0 : 0.0, m2j = m2a ? 0.0 : b;
+        const bool mm1 = m1 >= m2;
+        const double mm = mm1 ? m1 : m2;
+        lim = mm > 0.0 ? mm : 0.0;
+        if (mm > 0.0) { cdi = mm1 ? m1i : m2i; cdj = mm1 ? m1j : m2j; }
+    } else {
+        // min(0, min(max(bdi, dj), max(di, bdj)))
+        const bool m1a = bdi >= dj;
+        const double m1 = m1a ? bdi : dj, m1i = m1a ? b : 0.0, m1j = m1a ? 0.0 : 1.0;
+        const bool m2a = di >= bdj;
+        const double m2 = m2a ? di : bdj, m2i = m2a ? 1.0 : 0.0, m2j = m2a ? 0.0 : b;
+        const bool mm1 = m1 <= m2;
+        const double mm = mm1 ? m1 : m2;
+        lim = mm < 0.0 ? mm : 0.0;
+        if (mm < 0.0) { cdi = mm1 ? m1i : m2i; cdj = mm1 ? m1j : m2j; }
+    }
+    const double half = 0.5 * dij;
+    const bool big = (pos ? (lim > half) : (lim < half)) && fabs(lim) > 0.0;
+    dib = djb = dijb = 0.0;
+    if (big) {
+        const bool first = pos ? (di > dj) : (di < dj);
+        dijb = 0.5 * (first ? lib : ljb);
+    } else {
+        const double l = lib + ljb;
+        dib = cdi * l; djb = cdj * l;
+    }
+}
 
 // Reverse of the contribution of b to particle a (a water particle) with the
 // adjoints lr (of drho_a) and (l0, l1) (of acc_a).  MS: the moving-square
 // modified solver (Moving_Square.../Solver_Normalized_Modified_Linear_Riemann_Delta.f90
 // :169-230): w also carries avg_a - avg_b (XSPH inside the continuity flux), no SPS.
-template <bool MS = false>
+// MUSCL: the MUSCL linear-Riemann solver (Solver_Normalized_MUSCL_Linear_Riemann_Delta_SPS.f90:
+// 470-502): the limited reconstructions of p, u, v enter U_L - U_R, P_L - P_R and
+// this side's v - v*; a_lower: a is the reference's pair index i (the lower id),
+// which fixes the limiter's sides.
+template <bool MS = false, bool MUSCL = false>
 __device__ __forceinline__ void rev_pair(const Params& P, const PSide& A, const PSide& B, double lr, double l0,
-                                         double l1, PBar& o) {
+                                         double l1, PBar& o, bool a_lower = true) {
     const double r0 = A.x.x - B.x.x, r1 = A.x.y - B.x.y;
     const double d2 = r0 * r0 + r1 * r1, d = sqrt(d2), id = 1.0 / d, id2 = id * id;
     double G, dG;
@@ -185,22 +247,48 @@ __device__ __forceinline__ void rev_pair(const Params& P, const PSide& A, const 
     const double s = r0 * n0 + r1 * n1;
     const double du0 = A.u - B.u, du1 = A.v - B.v, dp = A.p - B.p, drho = A.rho - B.rho;
     const double vx = du0 * r0 + du1 * r1;
-    const double dU = -vx * id;
+    // MUSCL reconstruction increments on the reference's i / j sides
+    const double sI = a_lower ? 1.0 : -1.0;
+    double lpi = 0, lpj = 0, lui = 0, luj = 0, lvi = 0, lvj = 0;
+    double xj0 = 0, xj1 = 0, dpi = 0, dpj = 0, dui = 0, duj = 0, dvi = 0, dvj = 0;
+    double gIp0 = 0, gIp1 = 0, gJp0 = 0, gJp1 = 0, gIu0 = 0, gIu1 = 0, gJu0 = 0, gJu1 = 0;
+    double gIv0 = 0, gIv1 = 0, gJv0 = 0, gJv1 = 0;
+    if (MUSCL) {
+        xj0 = -sI * r0; xj1 = -sI * r1;                       // x_j - x_i
+        gIp0 = a_lower ? A.gp0 : B.gp0; gIp1 = a_lower ? A.gp1 : B.gp1;
+        gJp0 = a_lower ? B.gp0 : A.gp0; gJp1 = a_lower ? B.gp1 : A.gp1;
+        gIu0 = a_lower ? A.gu0 : B.gu0; gIu1 = a_lower ? A.gu1 : B.gu1;
+        gJu0 = a_lower ? B.gu0 : A.gu0; gJu1 = a_lower ? B.gu1 : A.gu1;
+        gIv0 = a_lower ? A.gv0 : B.gv0; gIv1 = a_lower ? A.gv1 : B.gv1;
+        gJv0 = a_lower ? B.gv0 : A.gv0; gJv1 = a_lower ? B.gv1 : A.gv1;
+        dpi = 0.5 * (gIp0 * xj0 + gIp1 * xj1); dpj = -0.5 * (gJp0 * xj0 + gJp1 * xj1);
+        dui = 0.5 * (gIu0 * xj0 + gIu1 * xj1); duj = -0.5 * (gJu0 * xj0 + gJu1 * xj1);
+        dvi = 0.5 * (gIv0 * xj0 + gIv1 * xj1); dvj = -0.5 * (gJv0 * xj0 + gJv1 * xj1);
+        muscl_limiter<double>(dpi, dpj, -sI * dp, lpi, lpj);
+        muscl_limiter<double>(dui, duj, -sI * du0, lui, luj);
+        muscl_limiter<double>(dvi, dvj, -sI * du1, lvi, lvj);
+    }
+    const double Su = lui + luj, Sv = lvi + lvj, Sp = lpi + lpj;
+    // U_L - U_R = -(v_a - v_b + sI (l_i + l_j)).r / d
+    const double vxm = MUSCL ? (du0 + sI * Su) * r0 + (du1 + sI * Sv) * r1 : vx;
+    const double dU = -vxm * id;
     const double rbar = 0.5 * (A.rho + B.rho), cbar = 0.5 * (A.c + B.c);
     const double irbar = 1.0 / rbar, ic0 = 1.0 / P.sqrt_c0;
     const double Pbar = 0.5 * (A.p + B.p);
     // Riemann state
     double PA, w0, w1, bR = 0.0, kk = 0.0;
     bool take_m3 = false;
+    // this side's reconstruction increment: + l_i as i, - l_j as j
+    const double su = MUSCL ? (a_lower ? lui : -luj) : 0.0, sv = MUSCL ? (a_lower ? lvi : -lvj) : 0.0;
     if (A.near) {
-        PA = Pbar; w0 = 0.5 * du0; w1 = 0.5 * du1;
+        PA = Pbar; w0 = 0.5 * du0 + su; w1 = 0.5 * du1 + sv;
     } else {
         const double m3 = 3.0 * fmax(dU, 0.0);
         take_m3 = m3 < cbar;
         bR = take_m3 ? m3 : cbar;
         PA = Pbar + 0.5 * bR * rbar * dU;
-        kk = dp * (0.5 * irbar * ic0) * id;
-        w0 = 0.5 * du0 + kk * r0; w1 = 0.5 * du1 + kk * r1;
+        kk = (MUSCL ? dp + sI * Sp : dp) * (0.5 * irbar * ic0) * id;
+        w0 = 0.5 * du0 + su + kk * r0; w1 = 0.5 * du1 + sv + kk * r1;
     }
     if (MS) { w0 += A.ax - B.ax; w1 += A.ay - B.ay; }
     const double rhoij = A.ir * B.ir;
@@ -296,11 +384,16 @@ __device__ __forceinline__ void rev_pair(const Params& P, const PSide& A, const 
     }
     du0b += 0.5 * w0b; du1b += 0.5 * w1b;
     o.avg0 = w0b; o.avg1 = w1b;
+    double luib = 0, lujb = 0, lvib = 0, lvjb = 0, Spb = 0, Sub = 0, Svb = 0;
+    if (MUSCL) {
+        if (a_lower) { luib += w0b; lvib += w1b; } else { lujb -= w0b; lvjb -= w1b; }
+    }
     Pbarb += PAb0;
     if (!A.near) {
         const double kkb = w0b * r0 + w1b * r1;
         r0b += kk * w0b; r1b += kk * w1b;
         dpb += kkb * (0.5 * irbar * ic0) * id;
+        if (MUSCL) Spb += sI * kkb * (0.5 * irbar * ic0) * id;
         rbarb -= kk * irbar * kkb;
         db -= kk * id * kkb;
         const double bRb = 0.5 * rbar * dU * PAb0;
@@ -309,11 +402,48 @@ __device__ __forceinline__ void rev_pair(const Params& P, const PSide& A, const 
         if (take_m3) { if (dU > 0.0) dUb += 3.0 * bRb; }
         else cbarb += bRb;
     }
-    // dU = -vx/d, vx = (u_a - u_b).r
-    vxb -= dUb * id;
-    db += vx * id2 * dUb;
+    // dU = -vxm/d
+    {
+        const double vxmb = -dUb * id;
+        db += vxm * id2 * dUb;
+        du0b += vxmb * r0; du1b += vxmb * r1;
+        if (MUSCL) {
+            r0b += vxmb * (du0 + sI * Su); r1b += vxmb * (du1 + sI * Sv);
+            Sub += sI * vxmb * r0; Svb += sI * vxmb * r1;
+        } else {
+            r0b += vxmb * du0; r1b += vxmb * du1;
+        }
+    }
+    // vx = (u_a - u_b).r (artificial viscosity, delta-alpha)
     du0b += vxb * r0; du1b += vxb * r1;
     r0b += vxb * du0; r1b += vxb * du1;
+    if (MUSCL) {
+        // the limiters: inputs di = (grad_i . x_ji)/2, dj = -(grad_j . x_ji)/2, dij = phi_j - phi_i
+        const double lpib = Spb, lpjb = Spb;
+        luib += Sub; lujb += Sub; lvib += Svb; lvjb += Svb;
+        double dib, djb, dijb, xjb0 = 0.0, xjb1 = 0.0;
+        double gIpb0, gIpb1, gJpb0, gJpb1, gIub0, gIub1, gJub0, gJub1, gIvb0, gIvb1, gJvb0, gJvb1;
+        muscl_limiter_rev(dpi, dpj, -sI * dp, lpib, lpjb, dib, djb, dijb);
+        dpb -= sI * dijb;
+        gIpb0 = 0.5 * dib * xj0; gIpb1 = 0.5 * dib * xj1; gJpb0 = -0.5 * djb * xj0; gJpb1 = -0.5 * djb * xj1;
+        xjb0 += 0.5 * dib * gIp0 - 0.5 * djb * gJp0; xjb1 += 0.5 * dib * gIp1 - 0.5 * djb * gJp1;
+        muscl_limiter_rev(dui, duj, -sI * du0, luib, lujb, dib, djb, dijb);
+        du0b -= sI * dijb;
+        gIub0 = 0.5 * dib * xj0; gIub1 = 0.5 * dib * xj1; gJub0 = -0.5 * djb * xj0; gJub1 = -0.5 * djb * xj1;
+        xjb0 += 0.5 * dib * gIu0 - 0.5 * djb * gJu0; xjb1 += 0.5 * dib * gIu1 - 0.5 * djb * gJu1;
+        muscl_limiter_rev(dvi, dvj, -sI * du1, lvib, lvjb, dib, djb, dijb);
+        du1b -= sI * dijb;
+        gIvb0 = 0.5 * dib * xj0; gIvb1 = 0.5 * dib * xj1; gJvb0 = -0.5 * djb * xj0; gJvb1 = -0.5 * djb * xj1;
+        xjb0 += 0.5 * dib * gIv0 - 0.5 * djb * gJv0; xjb1 += 0.5 * dib * gIv1 - 0.5 * djb * gJv1;
+        r0b -= sI * xjb0; r1b -= sI * xjb1;                   // x_j - x_i = -sI r
+        if (a_lower) {
+            o.gpa0 = gIpb0; o.gpa1 = gIpb1; o.gua0 = gIub0; o.gua1 = gIub1; o.gva0 = gIvb0; o.gva1 = gIvb1;
+            o.gpb0 = gJpb0; o.gpb1 = gJpb1; o.gub0 = gJub0; o.gub1 = gJub1; o.gvb0 = gJvb0; o.gvb1 = gJvb1;
+        } else {
+            o.gpa0 = gJpb0; o.gpa1 = gJpb1; o.gua0 = gJub0; o.gua1 = gJub1; o.gva0 = gJvb0; o.gva1 = gJvb1;
+            o.gpb0 = gIpb0; o.gpb1 = gIpb1; o.gub0 = gIub0; o.gub1 = gIub1; o.gvb0 = gIvb0; o.gvb1 = gIvb1;
+        }
+    }
     // s = r.n, n = B^-1 r
     r0b += sb * n0; r1b += sb * n1;
     n0b += sb * r0; n1b += sb * r1;
@@ -345,7 +475,7 @@ __device__ __forceinline__ void rev_pair(const Params& P, const PSide& A, const 
 #define SPH_ADJ_C_MIN_BLOCKS 3       // 168 registers: 3 blocks of 128 per SM
 #endif
 constexpr int kAdjLanes = SPH_ADJ_LANES;     // 2 or 4
-template <typename R, bool MS = false>
+template <typename R, bool MS = false, bool MUSCL = false>
 __global__ void __launch_bounds__(kAdjThreads, SPH_ADJ_C_MIN_BLOCKS) k_adj_c(Params P, Sorted<R> D, Adj A, const double* lr,
                                                         const double2* la, double* nu_part) {
     __shared__ double red[kAdjThreads];
@@ -355,28 +485,30 @@ __global__ void __launch_bounds__(kAdjThreads, SPH_ADJ_C_MIN_BLOCKS) k_adj_c(Par
     double nu_sum = 0.0;
     // every lane of the warp takes part in the shuffles below
     const bool live = c < P.n_tot;
-    // 0-16 as below; MS: 17-18 avg, 19 mass
-    constexpr int NV = MS ? 20 : 17;
-    double v[20];
+    // 0-16 as below; MS: 17-18 avg, 19 mass; MUSCL: 17-22 grad p, u, v
+    constexpr int NV = MS ? 20 : (MUSCL ? 23 : 17);
+    double v[23];
 #pragma unroll
-    for (int q = 0; q < 20; ++q) v[q] = 0.0;
+    for (int q = 0; q < 23; ++q) v[q] = 0.0;
     if (live) {
         const int nn = D.npairs[c];
         // both roles run the same instructions: the two sides are loaded by
         // index (c's records stay in L1), not branched on
         const double sg = role ? -1.0 : 1.0;
         for (int e = par; e < nn; e += kAdjLanes / 2) {
-            const int b = (int)(D.pairs[(size_t)e * P.nbr_stride + c] & 0x7fffffffu);
+            const unsigned ent = D.pairs[(size_t)e * P.nbr_stride + c];
+            const int b = (int)(ent & 0x7fffffffu);
             const int acc_at = role ? b : c;         // the particle whose sum is differentiated
+            const bool c_lower = (ent >> 31) != 0;  // c has the lower id of the pair
             const int other = role ? c : b;
             if (D.type[acc_at] != SPH_TYPE_WATER) continue;
             const double l_r = lr[acc_at];
             const double2 l_a = la[acc_at];
             if (l_r == 0.0 && l_a.x == 0.0 && l_a.y == 0.0) continue;
-            const PSide Sa = load_side<R, MS>(D, acc_at);
-            const PSide Sb = load_side<R, MS>(D, other);
+            const PSide Sa = load_side<R, MS, MUSCL>(D, acc_at);
+            const PSide Sb = load_side<R, MS, MUSCL>(D, other);
             PBar o;
-            rev_pair<MS>(P, Sa, Sb, l_r, l_a.x, l_a.y, o);
+            rev_pair<MS, MUSCL>(P, Sa, Sb, l_r, l_a.x, l_a.y, o, role ? !c_lower : c_lower);
             v[0] += sg * o.x0; v[1] += sg * o.x1; v[2] += sg * o.u; v[3] += sg * o.v;
             v[4] += role ? o.pb : o.pa;
             v[5] += role ? o.cb : o.ca;
@@ -390,6 +522,11 @@ __global__ void __launch_bounds__(kAdjThreads, SPH_ADJ_C_MIN_BLOCKS) k_adj_c(Par
             if (MS) {
                 v[17] += sg * o.avg0; v[18] += sg * o.avg1;
                 v[19] += role ? o.mb : 0.0;
+            }
+            if (MUSCL) {
+                v[17] += role ? o.gpb0 : o.gpa0; v[18] += role ? o.gpb1 : o.gpa1;
+                v[19] += role ? o.gub0 : o.gua0; v[20] += role ? o.gub1 : o.gua1;
+                v[21] += role ? o.gvb0 : o.gva0; v[22] += role ? o.gvb1 : o.gva1;
             }
         }
     }
@@ -413,6 +550,11 @@ __global__ void __launch_bounds__(kAdjThreads, SPH_ADJ_C_MIN_BLOCKS) k_adj_c(Par
         if (MS) {
             A.gavg[c] = make_double2(v[17], v[18]);
             A.sm[c] = v[19] + v[7] / rho;       // V = m / rho
+        }
+        if (MUSCL) {
+            A.ggp[c] = make_double2(v[17], v[18]);
+            A.ggu[c] = make_double2(v[19], v[20]);
+            A.ggv[c] = make_double2(v[21], v[22]);
         }
     }
     red[threadIdx.x] = nu_sum;
@@ -459,7 +601,11 @@ __global__ void k_adj_point(Params P, Sorted<R> D, Adj A, int shift) {
         ggr.x += sg.x; ggr.y += sg.y;
         gbs = A.shbi[a];
     }
-    double Gr0 = ggr.x, Gr1 = ggr.y, Gu0 = 0, Gu1 = 0, Gv0 = 0, Gv1 = 0;
+    double Gr0 = ggr.x, Gr1 = ggr.y, Gu0 = 0, Gu1 = 0, Gv0 = 0, Gv1 = 0, Gp0 = 0, Gp1 = 0;
+    if (P.muscl) {
+        const double2 gp = A.ggp[a], gu = A.ggu[a], gv = A.ggv[a];
+        Gp0 = gp.x; Gp1 = gp.y; Gu0 = gu.x; Gu1 = gu.y; Gv0 = gv.x; Gv1 = gv.y;
+    }
     double rho_b = 0.0;
     if (ta == SPH_TYPE_WATER && !P.ms) {
         // tau = SPS(grad u, grad v) rho (Solver_..._SPS.f90:256-296)
@@ -483,17 +629,19 @@ __global__ void k_adj_point(Params P, Sorted<R> D, Adj A, int shift) {
         double abs2b = P.sps_blin * (DL * DL) * blinb;
         if (sq > 0.0) abs2b += (t * t) * nutb / (2.0 * sq);
         sxxb += 4 * sxx * abs2b; syyb += 4 * syy * abs2b; sxyb += 2 * sxy * abs2b;
-        Gu0 = sxxb; Gu1 = sxyb; Gv0 = sxyb; Gv1 = syyb;
+        Gu0 += sxxb; Gu1 += sxyb; Gv0 += sxyb; Gv1 += syyb;
     }
     // grad = B^-1 g: adjoint of g = B^-T adjoint of grad
     auto mt = [&](double x, double y, double& ox, double& oy) {
         ox = bi.x * x + bi.z * y;
         oy = bi.y * x + bi.w * y;
     };
-    double m0, m1, m2, m3, m4, m5;
+    double m0, m1, m2, m3, m4, m5, m6 = 0.0, m7 = 0.0;
     mt(Gr0, Gr1, m0, m1);
     mt(Gu0, Gu1, m2, m3);
     mt(Gv0, Gv1, m4, m5);
+    if (P.muscl) mt(Gp0, Gp1, m6, m7);
+    const double gp0n = (double)n2.y, gp1n = (double)n2.z;    // normalised grad p (MUSCL)
     double M00 = 0, M01 = 0, M10 = 0, M11 = 0;
     const bool inverted = (ta == SPH_TYPE_WATER || (P.ms && ta == -202)) && P.renorm &&
                           !(bi.x == 1.0 && bi.y == 0.0 && bi.z == 0.0 && bi.w == 1.0);
@@ -505,17 +653,18 @@ __global__ void k_adj_point(Params P, Sorted<R> D, Adj A, int shift) {
             ox = B00 * x + B01 * y;
             oy = B10 * x + B11 * y;
         };
-        double qr0, qr1, qu0, qu1, qv0, qv1;
+        double qr0, qr1, qu0, qu1, qv0, qv1, qp0 = 0.0, qp1 = 0.0;
         raw(gr0, gr1, qr0, qr1);
         raw(gu0, gu1, qu0, qu1);
         raw(gv0, gv1, qv0, qv1);
+        if (P.muscl) raw(gp0n, gp1n, qp0, qp1);
         double4 gb = A.gbinv[a];
         gb.x += gbs.x; gb.y += gbs.y; gb.z += gbs.z; gb.w += gbs.w;
         // adjoint of B^-1: from pass C and from grad = B^-1 g
-        const double Y00 = gb.x + Gr0 * qr0 + Gu0 * qu0 + Gv0 * qv0;
-        const double Y01 = gb.y + Gr0 * qr1 + Gu0 * qu1 + Gv0 * qv1;
-        const double Y10 = gb.z + Gr1 * qr0 + Gu1 * qu0 + Gv1 * qv0;
-        const double Y11 = gb.w + Gr1 * qr1 + Gu1 * qu1 + Gv1 * qv1;
+        const double Y00 = gb.x + Gr0 * qr0 + Gu0 * qu0 + Gv0 * qv0 + Gp0 * qp0;
+        const double Y01 = gb.y + Gr0 * qr1 + Gu0 * qu1 + Gv0 * qv1 + Gp0 * qp1;
+        const double Y10 = gb.z + Gr1 * qr0 + Gu1 * qu0 + Gv1 * qv0 + Gp1 * qp0;
+        const double Y11 = gb.w + Gr1 * qr1 + Gu1 * qu1 + Gv1 * qv1 + Gp1 * qp1;
         // adjoint of B = -B^-T Y B^-T
         const double T00 = Y00 * bi.x + Y01 * bi.y, T01 = Y00 * bi.z + Y01 * bi.w;
         const double T10 = Y10 * bi.x + Y11 * bi.y, T11 = Y10 * bi.z + Y11 * bi.w;
@@ -527,6 +676,7 @@ __global__ void k_adj_point(Params P, Sorted<R> D, Adj A, int shift) {
     A.mu1[a] = make_double4(m0, m1, m2, m3);
     A.mu2[a] = make_double4(m4, m5, M00, M01);
     A.mu3[a] = make_double2(M10, M11);
+    if (P.muscl) A.mu4[a] = make_double2(m6, m7);
     A.sr[a] += rho_b;
 }
 
@@ -564,9 +714,11 @@ __device__ __forceinline__ void stage_reverse(const Params& P, const Sorted<R>& 
 // id = 1/|r|.  Returns f / V_b and its gradient with respect to r divided by V_b.
 __device__ __forceinline__ void rev_rawsum(double r0, double r1, double id, double G, double dG, double dr,
                                            double du, double dv, const double4& m1, const double4& m2,
-                                           const double2& m3, double& S_G, double& fr0, double& fr1) {
-    const double c0 = dr * m1.x + du * m1.z + dv * m2.x;   // sum_phi dphi mu_phi (x)
-    const double c1 = dr * m1.y + du * m1.w + dv * m2.y;
+                                           const double2& m3, double& S_G, double& fr0, double& fr1,
+                                           double dpp = 0.0, double2 m4 = make_double2(0.0, 0.0)) {
+    // sum_phi dphi mu_phi; MUSCL adds the grad p sum (dpp, m4)
+    const double c0 = dr * m1.x + du * m1.z + dv * m2.x + dpp * m4.x;
+    const double c1 = dr * m1.y + du * m1.w + dv * m2.y + dpp * m4.y;
     const double Mr0 = m2.z * r0 + m2.w * r1, Mr1 = m3.x * r0 + m3.y * r1;
     const double MTr0 = m2.z * r0 + m3.x * r1, MTr1 = m2.w * r0 + m3.y * r1;
     const double S = c0 * r0 + c1 * r1 - (r0 * Mr0 + r1 * Mr1);
@@ -583,7 +735,8 @@ __device__ __forceinline__ void rev_rawsum(double r0, double r1, double id, doub
 // with the adjoint lg + gavg of avg; the totals of the state adjoint (x, u, rho,
 // m) are written to sx, su, sr, sm for the ghost reverse and the stage reverse
 // that follow.
-template <typename R, bool MS = false>
+// MUSCL: also pass A's raw grad p sum, p = p(rho) by the equation of state.
+template <typename R, bool MS = false, bool MUSCL = false>
 __global__ void __launch_bounds__(kAdjThreads) k_adj_a(Params P, Sorted<R> D, Adj A, int stage, double dt,
                                                        const double2* lg) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -594,7 +747,8 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_a(Params P, Sorted<R> D, Ad
     const double Vc = mc / kc.z;
     const double4 mc1 = A.mu1[c], mc2 = A.mu2[c];
     const double2 mc3 = A.mu3[c];
-    double x0b = 0, x1b = 0, ub = 0, vb = 0, rb = 0, Vb = 0, mb_ = 0;
+    const double2 mc4 = MUSCL ? A.mu4[c] : make_double2(0.0, 0.0);
+    double x0b = 0, x1b = 0, ub = 0, vb = 0, rb = 0, Vb = 0, mb_ = 0, pb_ = 0;
     double2 lac = make_double2(0.0, 0.0);
     if (MS) {
         const double2 g = A.gavg[c], l = lg[c];
@@ -634,9 +788,11 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_a(Params P, Sorted<R> D, Ad
         {
             const double Vbn = D.mass[b] * A.irho[b];
             double S, f0, f1;
-            rev_rawsum(r0, r1, id, G, dG, kb.z - kc.z, kb.x - kc.x, kb.y - kc.y, mc1, mc2, mc3, S, f0, f1);
+            rev_rawsum(r0, r1, id, G, dG, kb.z - kc.z, kb.x - kc.x, kb.y - kc.y, mc1, mc2, mc3, S, f0, f1,
+                       MUSCL ? kb.w - kc.w : 0.0, mc4);
             x0b += Vbn * f0; x1b += Vbn * f1;
             rb -= Vbn * G * (mc1.x * r0 + mc1.y * r1);
+            if (MUSCL) pb_ -= Vbn * G * (mc4.x * r0 + mc4.y * r1);
             ub -= Vbn * G * (mc1.z * r0 + mc1.w * r1);
             vb -= Vbn * G * (mc2.x * r0 + mc2.y * r1);
         }
@@ -644,10 +800,13 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_a(Params P, Sorted<R> D, Ad
         {
             const double4 mb1 = A.mu1[b], mb2 = A.mu2[b];
             const double2 mb3 = A.mu3[b];
+            const double2 mb4 = MUSCL ? A.mu4[b] : make_double2(0.0, 0.0);
             double S, f0, f1;
-            rev_rawsum(-r0, -r1, id, G, dG, kc.z - kb.z, kc.x - kb.x, kc.y - kb.y, mb1, mb2, mb3, S, f0, f1);
+            rev_rawsum(-r0, -r1, id, G, dG, kc.z - kb.z, kc.x - kb.x, kc.y - kb.y, mb1, mb2, mb3, S, f0, f1,
+                       MUSCL ? kc.w - kb.w : 0.0, mb4);
             x0b -= Vc * f0; x1b -= Vc * f1;
             rb -= Vc * G * (mb1.x * r0 + mb1.y * r1);
+            if (MUSCL) pb_ -= Vc * G * (mb4.x * r0 + mb4.y * r1);
             ub -= Vc * G * (mb1.z * r0 + mb1.w * r1);
             vb -= Vc * G * (mb2.x * r0 + mb2.y * r1);
             Vb += G * S;
@@ -660,6 +819,11 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_a(Params P, Sorted<R> D, Ad
         A.sr[c] += rb - Vc / kc.z * Vb;
         A.sm[c] += mb_ + Vb / kc.z;
         return;
+    }
+    if (MUSCL) {
+        double dpd, dcd;
+        eos_deriv(P, kc.z, dpd, dcd);
+        rb += dpd * pb_;
     }
     stage_reverse(P, D, A, c, stage, dt, make_double2(sx.x + x0b, sx.y + x1b), make_double2(su.x + ub, su.y + vb),
                   A.sr[c] + rb - Vc / kc.z * Vb);

@@ -721,14 +721,15 @@ int snap_io(sph_handle* h, const Snap& s, int k, int n, bool save) {
 
 int adj_config_ok(const sph_handle* h, int loss) {
     const Params& P = h->P;
-    if (P.mls_order || P.muscl) return SPH_E_CONFIG;
+    if (P.mls_order) return SPH_E_CONFIG;
     if (P.ms) {
         // moving-square modified linear solver, Morris laplacian, Euler predictor-corrector
         if (h->cfg.shifting) return SPH_E_CONFIG;
         if (h->cfg.solver != SPH_SOLVER_MS_MODLR_DELTA || P.laplacian != 1) return SPH_E_CONFIG;
         if (h->cfg.integrator != SPH_INTEGRATOR_EULER_PC || h->cfg.periodic) return SPH_E_CONFIG;
     } else {
-        if (h->cfg.solver != SPH_SOLVER_MODLR_DELTA_SPS || P.xsph) return SPH_E_CONFIG;
+        if ((h->cfg.solver != SPH_SOLVER_MODLR_DELTA_SPS && h->cfg.solver != SPH_SOLVER_MUSCL_DELTA_SPS) || P.xsph)
+            return SPH_E_CONFIG;
         if (h->cfg.integrator != SPH_INTEGRATOR_RK4_REUSE) return SPH_E_CONFIG;
     }
     if (loss == SPH_LOSS_DRAG && !P.has_body) return SPH_E_CONFIG;
@@ -768,7 +769,8 @@ int adj_prepare_ctx(sph_handle* h, const sph_adj_config* ac) {
             (rc = adj_alloc(X, &A.gtau, nt)) || (rc = adj_alloc(X, &A.mu1, nt)) || (rc = adj_alloc(X, &A.mu2, nt)) ||
             (rc = adj_alloc(X, &A.mu3, nt)) ||
             (rc = adj_alloc(X, &A.nu_part, (size_t)5 * blocks((long long)nt * kAdjLanes, kAdjThreads))) ||
-            (rc = adj_alloc(X, &A.nu_acc, 1)) || (rc = adj_alloc(X, &A.irho, nt)) || (rc = adj_alloc(X, &A.ssum, nt)) ||
+            (rc = adj_alloc(X, &A.nu_acc, 1)) || (rc = adj_alloc(X, &A.irho, nt)) || (rc = adj_alloc(X, &A.ssum, nt)) || (rc = adj_alloc(X, &A.ggp, nt)) ||
+            (rc = adj_alloc(X, &A.ggu, nt)) || (rc = adj_alloc(X, &A.ggv, nt)) || (rc = adj_alloc(X, &A.mu4, nt)) ||
             (rc = adj_alloc(X, &A.smu, nt)) || (rc = adj_alloc(X, &A.shgr, nt)) || (rc = adj_alloc(X, &A.shbi, nt)) || (rc = adj_alloc(X, &A.lx, nt)) || (rc = adj_alloc(X, &A.lv, nt)) ||
             (rc = adj_alloc(X, &A.lrho, nt)) || (rc = adj_alloc(X, &A.lk_r, nh)) || (rc = adj_alloc(X, &A.lk_a, nh)))
             return rc;
@@ -932,13 +934,18 @@ int adj_rhs(sph_handle* h, const Sorted<R>& V, int k, int stage, bool shift = fa
         h->launches += 3;
     }
     tic(h, PH_ADJ);
-    k_adj_c<R><<<nbc, kAdjThreads, 0, h->stream>>>(P, V, A, A.lr[k], A.la[k], A.nu_part + (size_t)k * nbc);
+    if (P.muscl)
+        k_adj_c<R, false, true><<<nbc, kAdjThreads, 0, h->stream>>>(P, V, A, A.lr[k], A.la[k],
+                                                                     A.nu_part + (size_t)k * nbc);
+    else
+        k_adj_c<R><<<nbc, kAdjThreads, 0, h->stream>>>(P, V, A, A.lr[k], A.la[k], A.nu_part + (size_t)k * nbc);
     if (shift) {
         k_adj_shift<R><<<nb, kAdjThreads, 0, h->stream>>>(P, V, A);
         h->launches += 1;
     }
     k_adj_point<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, V, A, shift ? 1 : 0);
-    k_adj_a<R><<<nb, kAdjThreads, 0, h->stream>>>(P, V, A, stage, X->dt, nullptr);
+    if (P.muscl) k_adj_a<R, false, true><<<nb, kAdjThreads, 0, h->stream>>>(P, V, A, stage, X->dt, nullptr);
+    else k_adj_a<R><<<nb, kAdjThreads, 0, h->stream>>>(P, V, A, stage, X->dt, nullptr);
     CK(cudaGetLastError());
     h->launches += 3;
     return SPH_OK;

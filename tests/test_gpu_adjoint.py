@@ -4,9 +4,10 @@ against central finite differences of the FP64 forward step on the GPU.
 The adjoint's directional derivative g.delta must match
 (L(x + eps delta) - L(x - eps delta)) / (2 eps) to 1e-4 relative for seeded
 directions in the initial velocity, density and position fields and for the
-viscosity, on the Wendland/renormalised case and on the reference's own
+viscosity, on the Wendland/renormalised case, on the reference's own
 Taylor-Green parameters (Gaussian kernel, inverse discarded, default-real
-literals).  Gradients must not depend on the checkpoint interval, and the
+literals) and on the MUSCL linear-Riemann solver, each with and without
+particle shifting.  Gradients must not depend on the checkpoint interval, and the
 handle must hold the forward's final state after the backward pass.
 
 The step size: eps = 1e-6 for Wendland C2, whose gradient goes to zero at the
@@ -16,7 +17,13 @@ so every pair that crosses the support radius puts a kink into the loss; a
 difference quotient whose interval straddles one is off by up to 1e-2
 relative at eps = 1e-6 (and exact again at 1e-7).  The Gaussian cases use
 eps ten times smaller, which keeps the interval clear of kinks while the
-rounding error of the FP64 loss stays below 1e-8 relative.
+rounding error of the FP64 loss stays below 1e-8 relative.  The MUSCL
+limiter switches branches at |di|, |dj| thresholds and its large-jump branch
+jumps in value, so a 32x32 case over 12 steps has switches within 1e-7 of
+the seeded point in several directions (measured: 5e-3 to 4e-1 relative at
+eps = 1e-7 for density, 1e-6 for velocity and position, and 1e-8 or better
+one decade lower); the MUSCL cases use eps a hundred times smaller, where
+the quotient agrees with the adjoint to 1e-6 or better.
 """
 import numpy as np
 import pytest
@@ -32,7 +39,9 @@ REL_TOL = 1e-4
 def _case(kind):
     """"-shift" kinds keep the configuration's particle shifting (the reference
     Taylor-Green case shifts every step); the others switch it off."""
-    if kind.startswith("wendland-renorm"):
+    if kind.startswith("muscl"):
+        case = S.make_tgv(32, solver=S.SOLVER_MUSCL_DELTA_SPS, jitter=0.05, seed=13)
+    elif kind.startswith("wendland-renorm"):
         case = S.make_tgv(32, solver=S.SOLVER_MODLR_DELTA_SPS, jitter=0.05, seed=11)
     else:
         case = S.make_tgv(32, reference=True, jitter=0.05, seed=12)
@@ -79,6 +88,10 @@ def _grad(case, dt, target, every=5, loss=S.LOSS_VELOCITY_MISFIT, pre_steps=0):
 
 
 def _eps_scale(case):
+    # the MUSCL limiter switches branches (its large-jump branch even jumps in
+    # value) far more densely than the Gaussian's cut-off kinks
+    if case.cfg.solver == S.SOLVER_MUSCL_DELTA_SPS:
+        return 0.01
     return 1.0 if case.cfg.kernel_model == S.KERNEL_WENDLAND2 else 0.1
 
 
@@ -87,7 +100,7 @@ def _check(ad, fd, what):
 
 
 @pytest.mark.parametrize("kind", ["wendland-renorm", "reference-gaussian", "wendland-renorm-shift",
-                                  "reference-gaussian-shift"])
+                                  "reference-gaussian-shift", "muscl", "muscl-shift"])
 @pytest.mark.parametrize("pre_steps", [0, 3])
 def test_adjoint_matches_central_differences(lib, kind, pre_steps):
     case = _case(kind)
@@ -152,6 +165,7 @@ def test_adjoint_independent_of_checkpoint_interval(lib):
 
 def test_adjoint_rejects_unsupported_configurations(lib):
     case = S.make_tgv(16, solver=S.SOLVER_MUSCL_DELTA_SPS)
+    case.cfg.mls_order = 6                    # density re-initialisation: not differentiated
     with S.Simulation(case.cfg, case.n) as sim:
         sim.set_state(case.pos, case.vel, case.rho, case.mass, case.type)
         with pytest.raises(S.SphError) as e:
@@ -178,7 +192,7 @@ def test_adjoint_of_the_mixed_precision_step(lib):
 
 
 @pytest.mark.parametrize("kind", ["wendland-renorm", "reference-gaussian", "wendland-renorm-shift",
-                                  "reference-gaussian-shift"])
+                                  "reference-gaussian-shift", "muscl", "muscl-shift"])
 def test_adjoint_matches_cpu_tangent_linear_reference(lib, oracle, kind):
     """g.delta from the GPU adjoint against the FP64 CPU tangent-linear model of
     the same steps (oracle/sph_tangent.cpp, forward-mode derivative with the
