@@ -474,9 +474,12 @@ __device__ __forceinline__ void rev_pair(const Params& P, const PSide& A, const 
 #ifndef SPH_ADJ_C_MIN_BLOCKS
 #define SPH_ADJ_C_MIN_BLOCKS 3       // 168 registers: 3 blocks of 128 per SM
 #endif
+#ifndef SPH_ADJ_C_MUSCL_MIN_BLOCKS
+#define SPH_ADJ_C_MUSCL_MIN_BLOCKS 2 // the limiter reverses need more than 168
+#endif
 constexpr int kAdjLanes = SPH_ADJ_LANES;     // 2 or 4
 template <typename R, bool MS = false, bool MUSCL = false>
-__global__ void __launch_bounds__(kAdjThreads, SPH_ADJ_C_MIN_BLOCKS) k_adj_c(Params P, Sorted<R> D, Adj A, const double* lr,
+__global__ void __launch_bounds__(kAdjThreads, MUSCL ? SPH_ADJ_C_MUSCL_MIN_BLOCKS : SPH_ADJ_C_MIN_BLOCKS) k_adj_c(Params P, Sorted<R> D, Adj A, const double* lr,
                                                         const double2* la, double* nu_part) {
     __shared__ double red[kAdjThreads];
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
