@@ -68,22 +68,31 @@ struct Side {
 // continuity flux, laplacian switch, no SPS); SHIFT: the last RHS of a step with
 // shifting on, which also forms the shifting sum.  Both are compile-time so that
 // each launch carries only the registers of the terms it evaluates.
+#ifndef SPH_PASS_C_SHIFT_BLOCKS
+#define SPH_PASS_C_SHIFT_BLOCKS 4
+#endif
 template <typename R, bool MUSCL, bool MS, bool SHIFT>
-__global__ void __launch_bounds__(128, sizeof(R) == 4 ? 4 : 3) k_pass_c(Params P, Sorted<R> D) {
+__global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIFT_BLOCKS : 4) : 3)
+    k_pass_c(Params P, Sorted<R> D) {
     using V4 = typename VT<R>::V4;
     using A = typename Acc<R>::T;
     constexpr bool F32 = sizeof(R) == 4;
     // hi/lo records: the mixed Taylor-Green variants (the moving-square ones keep
     // the FP64 records, which their FP64 HLLC state needs)
     constexpr bool HL = F32 && !MS;
+    // the shifting sum needs the FP64 position differences: that launch reads the
+    // neighbour's FP64 position (and FP64 volume) instead of its hi/lo position
+    // and takes the FP32 difference as the rounding of the FP64 one
+    constexpr bool X64 = !HL || SHIFT;
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= P.n_tot) return;
     const int ta = D.type[a];
     const int nn = D.npairs[a];
-    const double2 xa = (!HL || SHIFT) ? D.pos[a] : make_double2(0.0, 0.0);
+    const double2 xa = X64 ? D.pos[a] : make_double2(0.0, 0.0);
     float4 xa_hl = make_float4(0.f, 0.f, 0.f, 0.f);
     Side<R> S;
-    if (HL) { S.kh = D.kh[a]; S.kl = D.kl[a]; xa_hl = D.xhl[a]; }
+    if (HL) { S.kh = D.kh[a]; S.kl = D.kl[a]; }
+    if (!X64) xa_hl = D.xhl[a];
     else S.kin = D.kin[a];
     S.aux = D.aux[a]; S.nb1 = D.nb1[a]; S.nb2 = D.nb2[a];
     if (MUSCL) S.nb3 = D.nb3[a];
@@ -121,6 +130,8 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 4 : 3) k_pass_c(Params P
     unsigned ent_nn = nn > 1 ? __ldg(&D.pairs[(size_t)P.nbr_stride + a]) : 0u;
     double2 xb_n = make_double2(0.0, 0.0);
     float4 xbhl_n = make_float4(0.f, 0.f, 0.f, 0.f);
+    double vd_n = 0.0;                 // FP64 volume, mixed SHIFT launch
+    constexpr bool VPRE = HL && SHIFT;
     Side<R> T_n;
     auto load_records = [&](int bb, Side<R>& t) {
         if (HL) { t.kh = D.kh[bb]; t.kl = D.kl[bb]; }
@@ -130,8 +141,9 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 4 : 3) k_pass_c(Params P
     };
     if (nn > 0) {
         const int b0 = (int)(ent_n & 0x7fffffffu);
-        if (HL) xbhl_n = __ldg(&D.xhl[b0]);
-        else xb_n = __ldg(&D.pos[b0]);
+        if (X64) xb_n = __ldg(&D.pos[b0]);
+        else xbhl_n = __ldg(&D.xhl[b0]);
+        if (VPRE) vd_n = __ldg(&D.vol64[b0]);
         if (PRE) load_records(b0, T_n);
     }
     for (int e = 0; e < nn; ++e) {
@@ -140,25 +152,24 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 4 : 3) k_pass_c(Params P
         const bool a_is_i = (ent >> 31) != 0;
         const double2 xb = xb_n;
         const float4 xbhl = xbhl_n;
+        const double vd_b = vd_n;
         Side<R> T;
         if (PRE) T = T_n;
         if (e + 1 < nn) {
             ent_n = ent_nn;
             const int b1 = (int)(ent_n & 0x7fffffffu);
-            if (HL) xbhl_n = __ldg(&D.xhl[b1]);
-            else xb_n = __ldg(&D.pos[b1]);
+            if (X64) xb_n = __ldg(&D.pos[b1]);
+            else xbhl_n = __ldg(&D.xhl[b1]);
+            if (VPRE) vd_n = __ldg(&D.vol64[b1]);
             if (PRE) load_records(b1, T_n);
             if (e + 2 < nn) ent_nn = __ldg(&D.pairs[(size_t)(e + 2) * P.nbr_stride + a]);
         }
-        // x_a - x_b: FP64, or hi/lo in FP32 (the shifting sum still reads the FP64 positions)
+        // x_a - x_b: FP64, or hi/lo in FP32 (the mixed SHIFT launch: the FP32
+        // rounding of the FP64 difference, which its shifting sum needs)
         double dxd = 0.0, dyd = 0.0;
-        if (!HL) { dxd = xa.x - xb.x; dyd = xa.y - xb.y; }
-        else if (SHIFT) {
-            const double2 xb64 = __ldg(&D.pos[b]);
-            dxd = xa.x - xb64.x; dyd = xa.y - xb64.y;
-        }
-        const float dxf = HL ? (xa_hl.x - xbhl.x) + (xa_hl.z - xbhl.z) : 0.f;
-        const float dyf = HL ? (xa_hl.y - xbhl.y) + (xa_hl.w - xbhl.w) : 0.f;
+        if (X64) { dxd = xa.x - xb.x; dyd = xa.y - xb.y; }
+        const float dxf = !HL ? 0.f : X64 ? (float)dxd : (xa_hl.x - xbhl.x) + (xa_hl.z - xbhl.z);
+        const float dyf = !HL ? 0.f : X64 ? (float)dyd : (xa_hl.y - xbhl.y) + (xa_hl.w - xbhl.w);
         R d, inv_d;
         if (F32) {
             const R s = HL ? (R)(dxf * dxf + dyf * dyf) : (R)(dxd * dxd + dyd * dyd);
@@ -347,8 +358,12 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 4 : 3) k_pass_c(Params P
             double gd, wd, Vd;
             if (F32) {
                 // FP64 without divisions: q = d/h, grad factor G = g/(d h) = -5 k t^3/h^2
-                // (Wendland) or -2 k e^{-q^2}/h^2 (Gaussian), V_b from the FP64 volume record
-                const double dd2 = sqrt(dxd * dxd + dyd * dyd);
+                // (Wendland) or -2 k e^{-q^2}/h^2 (Gaussian), V_b from the FP64 volume record.
+                // The distance: one Newton (Heron) step for sqrt(s) from the FP32
+                // distance d0 (relative error ~1e-7), d = d0 + (s - d0^2)/(2 d0),
+                // leaves a relative error of order 1e-14
+                const double d0 = (double)d;
+                const double dd2 = fma(fma(-d0, d0, dxd * dxd + dyd * dyd), 0.5 * (double)inv_d, d0);
                 const double q = dd2 * inv_h64;
                 if (P.kernel_model == SPH_KERNEL_GAUSSIAN) {
                     const double ex = exp(-(q * q));
@@ -360,7 +375,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 4 : 3) k_pass_c(Params P
                     wd = P.kfactor * (1.0 + 2.0 * q) * (t2 * t2);
                     gd = -5.0 * P.kfactor * (t2 * t) * inv_h2_64;
                 }
-                Vd = __ldg(&D.vol64[b]);
+                Vd = VPRE ? vd_b : __ldg(&D.vol64[b]);
             } else {
                 wd = (double)w; gd = (double)g; Vd = (double)Vb;
             }

@@ -279,7 +279,32 @@ __global__ void k_build_lists(Params P, Sorted<R> D, unsigned* status) {
                 if (b0 < 0) b0 = st;
                 b1 = D.cell_end[row + gx];
             }
-            for (int b = b0; b < b1; ++b) {
+            // candidates four at a time: their loads are issued together, then
+            // tested in order (the list is the same as a one-by-one scan)
+            int b = b0;
+            for (; b + 4 <= b1; b += 4) {
+                double2 xb[4];
+                int tb[4], ib[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    xb[k] = __ldg(&D.pos[b + k]);
+                    ib[k] = __ldg(&D.id[b + k]);
+                    tb[k] = check_type ? __ldg(&D.type[b + k]) : 0;
+                }
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    if (b + k == a) continue;
+                    if (check_type && !pair_allowed(P.pair_rule, ta, tb[k])) continue;
+                    const double dx = xa.x - xb[k].x, dy = xa.y - xb[k].y;
+                    if (dx * dx + dy * dy > P.r2_list) continue;
+                    if (cnt < P.max_nbr) {
+                        const unsigned lower = ida < ib[k] ? 0x80000000u : 0u;
+                        D.nbr[(size_t)cnt * P.nbr_stride + a] = (unsigned)(b + k) | lower;
+                    }
+                    ++cnt;
+                }
+            }
+            for (; b < b1; ++b) {
                 if (b == a) continue;
                 if (check_type && !pair_allowed(P.pair_rule, ta, D.type[b])) continue;
                 const double2 xb = D.pos[b];
