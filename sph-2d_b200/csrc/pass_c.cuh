@@ -397,4 +397,75 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIF
     }
 }
 
+// The particle shifting sum of the mixed Taylor-Green path as a gather of its
+// own, launched after pass C on the last RHS of a step (Shift_particle_position.f90:
+// 56-100): shift_a = -beta h^2 B_a^-1 sum_b (1 + R (W/W(dx))^4) grad_a W_ab V_b in
+// FP64, over the RHS's pair list, with the FP64 positions and volumes.  The same
+// sum inside mixed pass C holds its FP64 values at pass C's register bound and
+// stalls on their loads; here it runs at full occupancy.  Particles the shift
+// does not move (not water, or near the free surface) get 0.
+template <typename R>
+__global__ void __launch_bounds__(128) k_shift_gather(Params P, Sorted<R> D) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= P.n_tot) return;
+    if (D.type[a] != SPH_TYPE_WATER || (D.flags[a] & 2)) {
+        D.shift[a] = make_double2(0.0, 0.0);
+        return;
+    }
+    const int nn = D.npairs[a];
+    const double2 xa = D.pos[a];
+    const double inv_h64 = 1.0 / P.h, inv_h2_64 = inv_h64 * inv_h64, inv_wdx = 1.0 / P.w_dx;
+    double shx = 0.0, shy = 0.0;
+    // the pair entry two iterations ahead, the neighbour's position and volume one ahead
+    unsigned ent_n = nn > 0 ? __ldg(&D.pairs[a]) : 0u;
+    unsigned ent_nn = nn > 1 ? __ldg(&D.pairs[(size_t)P.nbr_stride + a]) : 0u;
+    double2 xb_n = make_double2(0.0, 0.0);
+    double vd_n = 0.0;
+    if (nn > 0) {
+        const int b0 = (int)(ent_n & 0x7fffffffu);
+        xb_n = __ldg(&D.pos[b0]);
+        vd_n = __ldg(&D.vol64[b0]);
+    }
+    for (int e = 0; e < nn; ++e) {
+        const double2 xb = xb_n;
+        const double Vd = vd_n;
+        if (e + 1 < nn) {
+            ent_n = ent_nn;
+            const int b1 = (int)(ent_n & 0x7fffffffu);
+            xb_n = __ldg(&D.pos[b1]);
+            vd_n = __ldg(&D.vol64[b1]);
+            if (e + 2 < nn) ent_nn = __ldg(&D.pairs[(size_t)(e + 2) * P.nbr_stride + a]);
+        }
+        const double dxd = xa.x - xb.x, dyd = xa.y - xb.y;
+        const double s2 = dxd * dxd + dyd * dyd;
+        // distance: FP32 estimate, then one Newton (Heron) step for sqrt(s2),
+        // d = d0 + (s2 - d0^2)/(2 d0): relative error of order 1e-14
+        const float sf = (float)s2;
+        const float yf = rsqrtf(sf);
+        const double d0 = (double)(sf * yf);
+        const double dd = fma(fma(-d0, d0, s2), 0.5 * (double)yf, d0);
+        const double q = dd * inv_h64;
+        // grad factor G = g/(d h) and W (compute_kernel), FP64 without divisions
+        double wd, gd;
+        if (P.kernel_model == SPH_KERNEL_GAUSSIAN) {
+            const double ex = exp(-(q * q));
+            wd = (ex - P.gauss_e9) * P.kfactor;
+            gd = -2.0 * P.kfactor * ex * inv_h2_64;
+        } else {
+            const double t = 1.0 - 0.5 * q;
+            const double t2 = t * t;
+            wd = P.kfactor * (1.0 + 2.0 * q) * (t2 * t2);
+            gd = -5.0 * P.kfactor * (t2 * t) * inv_h2_64;
+        }
+        const double r = wd * inv_wdx;
+        const double r2 = r * r;
+        const double f = (1 + P.shift_R * (r2 * r2)) * Vd * gd;
+        shx += f * dxd;
+        shy += f * dyd;
+    }
+    const double4 b64 = D.binv64[a];
+    const double c = -P.shift_beta * (P.h * P.h);
+    D.shift[a] = make_double2(c * (b64.x * shx + b64.y * shy), c * (b64.z * shx + b64.w * shy));
+}
+
 }  // namespace sph

@@ -423,16 +423,24 @@ int rhs(sph_handle* h, int last) {
     k_surface<R><<<nb, 128, 0, h->stream>>>(P, D);
     k_near<R><<<nb, 128, 0, h->stream>>>(P, D);
     tic(h, PH_C);
+    // the mixed Taylor-Green path forms the shifting sum in k_shift_gather after
+    // pass C; the FP64 and moving-square launches form it inside pass C
+    const bool sep = sizeof(R) == 4 && !P.ms;
     const bool sh = last && h->cfg.shifting;
+    const bool shc = sh && !sep;
     if (P.ms) {
-        if (sh) k_pass_c<R, false, true, true><<<nb, 128, 0, h->stream>>>(P, D);
+        if (shc) k_pass_c<R, false, true, true><<<nb, 128, 0, h->stream>>>(P, D);
         else k_pass_c<R, false, true, false><<<nb, 128, 0, h->stream>>>(P, D);
     } else if (P.muscl) {
-        if (sh) k_pass_c<R, true, false, true><<<nb, 128, 0, h->stream>>>(P, D);
+        if (shc) k_pass_c<R, true, false, true><<<nb, 128, 0, h->stream>>>(P, D);
         else k_pass_c<R, true, false, false><<<nb, 128, 0, h->stream>>>(P, D);
     } else {
-        if (sh) k_pass_c<R, false, false, true><<<nb, 128, 0, h->stream>>>(P, D);
+        if (shc) k_pass_c<R, false, false, true><<<nb, 128, 0, h->stream>>>(P, D);
         else k_pass_c<R, false, false, false><<<nb, 128, 0, h->stream>>>(P, D);
+    }
+    if (sh && sep) {
+        k_shift_gather<R><<<nb, 128, 0, h->stream>>>(P, D);
+        h->launches += 1;
     }
     CK(cudaGetLastError());
     h->launches += 4;
