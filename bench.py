@@ -149,10 +149,12 @@ def peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
-# Algorithmic bytes per particle of pass C (the dominant kernel): its own
-# records read once (pos 16 B, kin 32 (FP64 in both paths), aux, nb1..nb3,
-# B^-1, flags 1) and its outputs written once (drhodt, acc, avg, shift 16).
-PASS_C_BYTES_MIXED = 16 + 32 + 16 + 48 + 16 + 1 + 4 + 8 + 8 + 16
+# Algorithmic bytes per particle of mixed pass C (the dominant kernel): its own
+# records read once (hi/lo position 16 B, hi/lo kinematic record 32, aux 16,
+# nb1..nb3 48, B^-1 16, flags 1) and its outputs written once (drhodt 4, acc 8,
+# avg 8).  The mixed path forms the shifting sum in a separate gather
+# (k_shift_gather, timed with the update).
+PASS_C_BYTES_MIXED = 16 + 32 + 16 + 48 + 16 + 1 + 4 + 8 + 8
 PASS_C_BYTES_FP64 = 16 + 32 + 32 + 96 + 32 + 1 + 8 + 16 + 16 + 16
 
 

@@ -439,6 +439,8 @@ int rhs(sph_handle* h, int last) {
         else k_pass_c<R, false, false, false><<<nb, 128, 0, h->stream>>>(P, D);
     }
     if (sh && sep) {
+        // timed with the update: shifting is part of the step's second pass
+        tic(h, PH_UPDATE);
         k_shift_gather<R><<<nb, 128, 0, h->stream>>>(P, D);
         h->launches += 1;
     }
