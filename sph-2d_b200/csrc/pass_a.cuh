@@ -21,9 +21,14 @@ namespace sph {
 // HLREC: in the mixed path, read the hi/lo float records (position, u, v, rho, p)
 // instead of the FP64 ones and form the pair differences in FP32 from them
 // (see store_split); the adjoint, which runs this pass on stored stage states
-// that carry only the FP64 records, uses HLREC = false.
-template <typename R, bool HLREC>
-__global__ void __launch_bounds__(128, sizeof(R) == 4 ? 6 : 4) k_pass_a(Params P, Sorted<R> D) {
+// that carry only the FP64 records, uses HLREC = false.  MS: the moving-square
+// solvers (P.ms), whose XSPH sum is formed here; compile-time so that the
+// Taylor-Green launches carry none of its registers.
+#ifndef SPH_PASS_A_F32_BLOCKS
+#define SPH_PASS_A_F32_BLOCKS 7
+#endif
+template <typename R, bool HLREC, bool MS>
+__global__ void __launch_bounds__(128, sizeof(R) == 4 ? SPH_PASS_A_F32_BLOCKS : 4) k_pass_a(Params P, Sorted<R> D) {
     using V4 = typename VT<R>::V4;
     constexpr bool F32 = sizeof(R) == 4;
     constexpr bool HL = HLREC && F32;
@@ -122,7 +127,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 6 : 4) k_pass_a(Params P
             du = (R)(kb.x - ka.x); dv = (R)(kb.y - ka.y);
             dp = (R)(kb.w - ka.w);
         }
-        if (P.ms) {
+        if (MS) {
             const R rsum = HL ? (R)(kah.z + kbh.z) : (R)(ka.z + kb.z);
             const R f = (R)P.eps * D.aux[b].x / rsum * wk;
             xs0 += f * du;
@@ -147,7 +152,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 6 : 4) k_pass_a(Params P
     // (Define_freesurface...f90:180-186) unless renormalisation is switched on.
     double i00 = 1.0, i01 = 0.0, i10 = 0.0, i11 = 1.0;
     // the moving-square variant also inverts for outlet particles (MS Define_freesurface...f90:131)
-    if ((ta == SPH_TYPE_WATER || (P.ms && ta == -202)) && P.renorm) {
+    if ((ta == SPH_TYPE_WATER || (MS && ta == -202)) && P.renorm) {
         double a1 = (double)b00, bb1 = (double)b01, a2 = (double)b10, bb2 = (double)b11;
         double det = (a1 * bb2 - bb1 * a2);
         if (det != 0) { i00 = bb2 / det; i01 = -bb1 / det; i10 = -a2 / det; i11 = a1 / det; }
@@ -163,7 +168,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 6 : 4) k_pass_a(Params P
     }
     // SPS stress for water particles (:256-296)
     R txx = R(0), txy = R(0), tyy = R(0);
-    if (ta == SPH_TYPE_WATER && !P.ms) {
+    if (ta == SPH_TYPE_WATER && !MS) {
         const double sxx = (double)gr[4], sxy = (double)gr[5] + (double)gr[6], syy = (double)gr[7];
         const double abs2 = 2 * (sxx * sxx + syy * syy) + sxy * sxy;
         const double DL = P.sps_dl;               // SPS_Delta_L = sqrt(2.0)/2.0*interior_dx (host-side product)
@@ -184,7 +189,13 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 6 : 4) k_pass_a(Params P
     uint8_t fl = 0;
     if (P.free_surface && ta == SPH_TYPE_WATER && (double)fv <= P.fs_thr) fl = 4;   // surface candidate (:123)
     D.flags[a] = fl;
-    if (P.ms) D.avg[a] = mk2<R>(xs0, xs1);
+    if (MS) D.avg[a] = mk2<R>(xs0, xs1);
+}
+
+template <typename R, bool HLREC>
+void launch_pass_a(const Params& P, const Sorted<R>& D, int nb, cudaStream_t st) {
+    if (P.ms) k_pass_a<R, HLREC, true><<<nb, 128, 0, st>>>(P, D);
+    else k_pass_a<R, HLREC, false><<<nb, 128, 0, st>>>(P, D);
 }
 
 // Geometric free-surface test of the candidates (Define_freesurface...f90:295-376):

@@ -418,7 +418,7 @@ int rhs(sph_handle* h, int last) {
         }
     }
     tic(h, PH_A);
-    k_pass_a<R, true><<<nb, 128, 0, h->stream>>>(P, D);
+    launch_pass_a<R, true>(P, D, nb, h->stream);
     tic(h, PH_SURF);
     k_surface<R><<<nb, 128, 0, h->stream>>>(P, D);
     k_near<R><<<nb, 128, 0, h->stream>>>(P, D);
@@ -938,7 +938,7 @@ int adj_rhs(sph_handle* h, const Sorted<R>& V, int k, int stage, bool shift = fa
     const int nbc = blocks((long long)P.n_tot * kAdjLanes, kAdjThreads);
     if (!shift) {
         tic(h, PH_A);
-        k_pass_a<R, false><<<nb, 128, 0, h->stream>>>(P, V);
+        launch_pass_a<R, false>(P, V, nb, h->stream);
         k_surface<R><<<nb, 128, 0, h->stream>>>(P, V);
         k_near<R><<<nb, 128, 0, h->stream>>>(P, V);
         h->launches += 3;
@@ -988,7 +988,7 @@ int adj_step(sph_handle* h, bool first, int j) {
         const Sorted<R> V = stage_view<R>(h, j, 2);
         const int nba = blocks(P.n_tot, 128);
         tic(h, PH_A);
-        k_pass_a<R, false><<<nba, 128, 0, h->stream>>>(P, V);
+        launch_pass_a<R, false>(P, V, nba, h->stream);
         k_surface<R><<<nba, 128, 0, h->stream>>>(P, V);
         k_near<R><<<nba, 128, 0, h->stream>>>(P, V);
         tic(h, PH_ADJ);
@@ -1046,7 +1046,7 @@ int adj_rhs_ms(sph_handle* h, const Sorted<R>& V, int k, int pred, bool drag, in
             h->body_acc[1]);
         h->launches += 1;
     }
-    k_pass_a<R, false><<<nb, 128, 0, h->stream>>>(P, V);
+    launch_pass_a<R, false>(P, V, nb, h->stream);
     k_surface<R><<<nb, 128, 0, h->stream>>>(P, V);
     k_near<R><<<nb, 128, 0, h->stream>>>(P, V);
     tic(h, PH_ADJ);
