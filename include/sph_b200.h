@@ -55,6 +55,10 @@ extern "C" {
 #define SPH_SOLVER_MUSCL_DELTA_SPS  1 /* Solver_Normalized_MUSCL_Linear_Riemann_Delta_SPS                 */
 #define SPH_SOLVER_MS_MODLR_DELTA   2 /* Moving_Square.../Solver_Normalized_Modified_Linear_Riemann_Delta (MS default) */
 #define SPH_SOLVER_MS_HLLC_DELTA    3 /* Moving_Square.../Solver_Normalized_HLLC_Riemann_Delta                     */
+#define SPH_SOLVER_DELTA_SPS        4 /* Taylor_Green_Vortex/Solver_Normalized_Delta_SPH_SPS (no Riemann state:
+                                         pair-mean pressure and velocity, Antuono delta-SPH diffusion,
+                                         no XSPH; its energy equation, which nothing else reads under the
+                                         Tait EOS, is not integrated)                                   */
 
 #define SPH_EOS_TAIT    0   /* Status_Equation.f90:56-66  p = B((rho/rho0)^7-1) + pb */
 #define SPH_EOS_LINEAR  1   /* Status_Equation.f90:69-76  p = c0^2 (rho-rho0) + pb   */

@@ -549,8 +549,13 @@ void gradients(const Particles& P, Rhs& R, bool muscl) {
 // Main pair loop of the two linear-Riemann solvers
 // (Solver_Normalized_Modified_Linear_Riemann_Delta_SPS.f90:300-502,
 //  Solver_Normalized_MUSCL_Linear_Riemann_Delta_SPS.f90:458-682)
-// and the delta-SPH density diffusion (:552-583 / :690-721).
-void riemann_solver(const Particles& P, Rhs& R, bool muscl) {
+// and the delta-SPH density diffusion (:552-583 / :690-721).  dsph: the plain
+// method Solver_Normalized_Delta_SPH_SPS.f90, whose pair loop (:324-512) has no
+// Riemann state (continuity with v_i - v_j, pressure p_i + p_j), no XSPH
+// (:286-322 commented out, average_velocity zeroed by single_step_compute.f90:122)
+// and the Antuono density diffusion (:610-636); its energy equation (dedt,
+// :379-380, 435-468) feeds nothing else under the Tait EOS and is not formed.
+void riemann_solver(const Particles& P, Rhs& R, bool muscl, bool dsph) {
     const int n = P.n;
     const PairList& L = R.L;
     const size_t np = L.size();
@@ -609,16 +614,31 @@ void riemann_solver(const Particles& P, Rhs& R, bool muscl) {
         else { vIs[0] = vs[0]; vIs[1] = vs[1]; IPs = Ps; }
         if (R.near[j] == 1) { vJs[0] = vbar[0]; vJs[1] = vbar[1]; JPs = Pbar; }
         else { vJs[0] = vs[0]; vJs[1] = vs[1]; JPs = Ps; }
-        double tmi = (vI[0] - vIs[0]) * ndi[0] + (vI[1] - vIs[1]) * ndi[1];
-        double tmj = -((vJ[0] - vJs[0]) * ndj[0] + (vJ[1] - vJs[1]) * ndj[1]);
-        ti[0][k] = 2 * ri * Vj * tmi;
-        tj[0][k] = 2 * rj * Vi * tmj;
         double rho_ij = 1.0 / (ri * rj);
-        for (int a = 0; a < 2; ++a) {
-            double tpi = -2 * IPs * ndi[a] * rho_ij;
-            double tpj = -2 * JPs * ndj[a] * rho_ij;
-            ti[1 + a][k] = P.mass[j] * tpi;
-            tj[1 + a][k] = -(P.mass[i] * tpj);
+        if (dsph) {
+            // Solver_Normalized_Delta_SPH_SPS.f90:335-374
+            const double vd[2] = {P.u[i] - P.u[j], P.v[i] - P.v[j]};
+            double tmi = vd[0] * ndi[0] + vd[1] * ndi[1];
+            double tmj = vd[0] * ndj[0] + vd[1] * ndj[1];
+            ti[0][k] = ri * Vj * tmi;
+            tj[0][k] = rj * Vi * tmj;
+            for (int a = 0; a < 2; ++a) {
+                double tpi = -(R.p[i] + R.p[j]) * ndi[a] * rho_ij;
+                double tpj = -(R.p[i] + R.p[j]) * ndj[a] * rho_ij;
+                ti[1 + a][k] = P.mass[j] * tpi;
+                tj[1 + a][k] = -(P.mass[i] * tpj);
+            }
+        } else {
+            double tmi = (vI[0] - vIs[0]) * ndi[0] + (vI[1] - vIs[1]) * ndi[1];
+            double tmj = -((vJ[0] - vJs[0]) * ndj[0] + (vJ[1] - vJs[1]) * ndj[1]);
+            ti[0][k] = 2 * ri * Vj * tmi;
+            tj[0][k] = 2 * rj * Vi * tmj;
+            for (int a = 0; a < 2; ++a) {
+                double tpi = -2 * IPs * ndi[a] * rho_ij;
+                double tpj = -2 * JPs * ndj[a] * rho_ij;
+                ti[1 + a][k] = P.mass[j] * tpi;
+                tj[1 + a][k] = -(P.mass[i] * tpj);
+            }
         }
         // artificial viscosity (:392-417)
         double vij[2] = {P.u[i] - P.u[j], P.v[i] - P.v[j]};
@@ -660,7 +680,7 @@ void riemann_solver(const Particles& P, Rhs& R, bool muscl) {
         tp = tp * rho_ij;
         ti[10][k] = P.smass[j] * tp; tj[10][k] = -(P.smass[i] * tp);
         // XSPH average velocity (:495-500, modified linear Riemann solver only)
-        if (!muscl) {
+        if (!muscl && !dsph) {
             for (int a = 0; a < 2; ++a) {
                 ti[11 + a][k] = -(C.xsph_eps * 2 * P.mass[j] * vij[a] / (ri + rj) * L.w[k]);
                 tj[11 + a][k] = C.xsph_eps * 2 * P.mass[i] * vij[a] / (ri + rj) * L.w[k];
@@ -680,10 +700,19 @@ void riemann_solver(const Particles& P, Rhs& R, bool muscl) {
         double r2 = pd[0] * pd[0] + pd[1] * pd[1];
         double drho = -(P.rho[i] - P.rho[j]);
         double sg0 = R.grho[0][i] + R.grho[0][j], sg1 = R.grho[1][i] + R.grho[1][j];
+        double cbar = (R.c[i] + R.c[j]) / 2.0;
+        if (dsph) {
+            // Solver_Normalized_Delta_SPH_SPS.f90:610-636
+            double ps[2] = {2 * drho / r2 * pd[0] - sg0, 2 * drho / r2 * pd[1] - sg1};
+            double tmi = ps[0] * R.ndwi0[k] + ps[1] * R.ndwi1[k];
+            double tmj = ps[0] * R.ndwj0[k] + ps[1] * R.ndwj1[k];
+            ti[13][k] = C.delta * hbar * cbar * tmi * R.vol[j];
+            tj[13][k] = -(C.delta * hbar * cbar * tmj * R.vol[i]);
+            continue;
+        }
         double psi = drho - 0.5 * (sg0 * pd[0] + sg1 * pd[1]);
         double tmi = (pd[0] * R.ndwi0[k] + pd[1] * R.ndwi1[k]) / r2;
         double tmj = (pd[0] * R.ndwj0[k] + pd[1] * R.ndwj1[k]) / r2;
-        double cbar = (R.c[i] + R.c[j]) / 2.0;
         ti[13][k] = 2 * C.delta * hbar * cbar * psi * tmi * R.vol[j];
         tj[13][k] = -(2 * C.delta * hbar * cbar * psi * tmj * R.vol[i]);
     }
@@ -1029,7 +1058,7 @@ void single_step_compute(Particles& P, Rhs& R) {
     const bool muscl = g_cfg.solver == SPH_SOLVER_MUSCL_DELTA_SPS;
     if (muscl) gradients(P, R, true);
     sps_stress(P, R);
-    riemann_solver(P, R, muscl);
+    riemann_solver(P, R, muscl, g_cfg.solver == SPH_SOLVER_DELTA_SPS);
 }
 
 // Shift_particle_position: Taylor_Green_Vortex/Shift_particle_position.f90:56-136,

@@ -22,6 +22,7 @@ enum : unsigned {
 struct Params {
     // switches
     int kernel_model, solver, renorm, quirks, pair_rule, shifting, muscl, xsph;
+    int dsph;                     // Solver_Normalized_Delta_SPH_SPS (Taylor-Green)
     int ms, hllc, laplacian, free_surface, integrator, has_body;
     int mls_order, mls_every;     // density re-initialisation (0: off)
     double mls_alpha3;            // alpha^3 added to the moment matrix diagonal

@@ -98,7 +98,11 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIF
     if (MUSCL) S.nb3 = D.nb3[a];
     const R rho_a = HL ? (R)S.kh.z : (R)S.kin.z;
     const V4 bi = D.binv[a];
-    const bool near_a = (D.flags[a] & 2) != 0;
+    // Solver_Normalized_Delta_SPH_SPS has no Riemann state: its continuity and
+    // pressure terms (:333-374) are the pair-mean (v-bar, P-bar) form the Riemann
+    // solvers use near the free surface, so it takes that branch for every pair
+    const bool dsph = !MUSCL && !MS && P.dsph;
+    const bool near_a = dsph || (D.flags[a] & 2) != 0;
     // delta-SPH and the assembly only apply to integrated particles (Solver :627-635,
     // Moving_Square.../Single_step_compute.f90:273-281)
     const bool water = integrated(P, ta);
@@ -111,6 +115,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIF
     const R nu2 = (R)(2.0 * P.nu), alpha = (R)P.alpha, beta = (R)P.beta;
     const R fh2 = (R)((P.fai * P.h) * (P.fai * P.h));
     const R dlt2h = (R)(2.0 * P.delta * P.h);
+    const R dla_dh = (R)(P.delta * P.h);
     const R dla_h = (R)(P.delta_alpha * P.h);
     const R eps2 = (R)(2.0 * P.eps);
     const R inv_rho_a = rcp(rho_a);
@@ -347,9 +352,17 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIF
         // delta-SPH density diffusion (:552-583): psi = (rho_j - rho_i) - 0.5 (grad rho_i + grad rho_j).(x_j - x_i)
         if (water) {
             const R sg0 = I.nb1.w + J.nb1.w, sg1 = I.nb2.x + J.nb2.x;
-            const R psi = drho_ji + R(0.5) * (sg0 * xij0 + sg1 * xij1);
-            const R tma = -(xij0 * nd0 + xij1 * nd1) * inv_r2;
-            dr += sgn * (dlt2h * cbar * psi * tma * Vb);
+            if (dsph) {
+                // Antuono form (Solver_Normalized_Delta_SPH_SPS.f90:610-636):
+                // psi = 2 (rho_j - rho_i) (x_j - x_i)/r^2 - (grad rho_i + grad rho_j), D += delta h c psi.gradW V
+                const R f = R(2) * drho_ji * inv_r2;
+                const R p0 = -(f * xij0) - sg0, p1 = -(f * xij1) - sg1;
+                dr += sgn * (dla_dh * cbar * (p0 * nd0 + p1 * nd1) * Vb);
+            } else {
+                const R psi = drho_ji + R(0.5) * (sg0 * xij0 + sg1 * xij1);
+                const R tma = -(xij0 * nd0 + xij1 * nd1) * inv_r2;
+                dr += sgn * (dlt2h * cbar * psi * tma * Vb);
+            }
         }
         cont.add(dr);
         // particle shifting sum (Shift_particle_position.f90:97-100), FP64:

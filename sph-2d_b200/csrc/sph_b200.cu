@@ -130,7 +130,7 @@ namespace {
 // --- configuration -> kernel parameters (mirrors the oracle's constants) ---
 int derive_params(const sph_config& c, Params& P) {
     if (c.kernel_model != SPH_KERNEL_GAUSSIAN && c.kernel_model != SPH_KERNEL_WENDLAND2) return SPH_E_CONFIG;
-    if (c.solver < SPH_SOLVER_MODLR_DELTA_SPS || c.solver > SPH_SOLVER_MS_HLLC_DELTA) return SPH_E_CONFIG;
+    if (c.solver < SPH_SOLVER_MODLR_DELTA_SPS || c.solver > SPH_SOLVER_DELTA_SPS) return SPH_E_CONFIG;
     if (c.laplacian != 0 && c.laplacian != 1) return SPH_E_CONFIG;
     if (c.eos != SPH_EOS_TAIT && c.eos != SPH_EOS_LINEAR) return SPH_E_CONFIG;
     if (c.precision != SPH_PREC_FP64 && c.precision != SPH_PREC_MIXED) return SPH_E_CONFIG;
@@ -147,7 +147,10 @@ int derive_params(const sph_config& c, Params& P) {
     P.kernel_model = c.kernel_model;
     P.solver = c.solver;
     P.muscl = c.solver == SPH_SOLVER_MUSCL_DELTA_SPS;
-    P.xsph = (c.xsph_eps != 0.0 && !P.muscl) ? 1 : 0;
+    P.dsph = c.solver == SPH_SOLVER_DELTA_SPS ? 1 : 0;
+    // XSPH: the modified linear Riemann solvers only (Solver_Normalized_Delta_SPH_SPS.f90:286-322
+    // has it commented out)
+    P.xsph = (c.xsph_eps != 0.0 && !P.muscl && !P.dsph) ? 1 : 0;
     P.ms = (c.solver == SPH_SOLVER_MS_MODLR_DELTA || c.solver == SPH_SOLVER_MS_HLLC_DELTA) ? 1 : 0;
     P.hllc = c.solver == SPH_SOLVER_MS_HLLC_DELTA ? 1 : 0;
     P.laplacian = c.laplacian;

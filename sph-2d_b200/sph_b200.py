@@ -38,6 +38,7 @@ SOLVER_MODLR_DELTA_SPS = 0
 SOLVER_MUSCL_DELTA_SPS = 1
 SOLVER_MS_MODLR_DELTA = 2
 SOLVER_MS_HLLC_DELTA = 3
+SOLVER_DELTA_SPS = 4          # Solver_Normalized_Delta_SPH_SPS (the plain Taylor-Green method)
 INTEGRATOR_RK4_REUSE = 0
 INTEGRATOR_EULER_PC = 1
 EOS_TAIT = 0

@@ -75,6 +75,9 @@ RHS_CASES = [
     ("muscl-jitter-1", dict(n_side=64, solver=S.SOLVER_MUSCL_DELTA_SPS, jitter=0.1, seed=1)),
     ("muscl-jitter-2", dict(n_side=50, solver=S.SOLVER_MUSCL_DELTA_SPS, jitter=0.05, seed=9)),
     ("modlr-renorm-jitter", dict(n_side=64, solver=S.SOLVER_MODLR_DELTA_SPS, jitter=0.1, seed=2)),
+    # the plain method (Solver_Normalized_Delta_SPH_SPS) on its own 100x100 lattice and jittered
+    ("dsph-100", dict(n_side=100, solver=S.SOLVER_DELTA_SPS)),
+    ("dsph-jitter", dict(n_side=64, solver=S.SOLVER_DELTA_SPS, jitter=0.1, seed=6)),
 ]
 
 
@@ -118,6 +121,8 @@ STEP_CASES = [
     ("muscl-48-jitter", dict(n_side=48, solver=S.SOLVER_MUSCL_DELTA_SPS, jitter=0.1, seed=3), 10, None),
     ("modlr-48-lattice", dict(n_side=48, solver=S.SOLVER_MODLR_DELTA_SPS), 10, None),
     ("modlr-48-jitter", dict(n_side=48, solver=S.SOLVER_MODLR_DELTA_SPS, jitter=0.1, seed=4), 10, None),
+    ("dsph-100-lattice", dict(n_side=100, solver=S.SOLVER_DELTA_SPS), 10, None),
+    ("dsph-48-jitter", dict(n_side=48, solver=S.SOLVER_DELTA_SPS, jitter=0.1, seed=7), 10, None),
 ]
 
 
@@ -159,13 +164,14 @@ def test_steps_split_equal_single_call(lib):
         assert np.array_equal(a, b)
 
 
-def test_mixed_precision_velocity_error(lib):
+@pytest.mark.parametrize("solver", [S.SOLVER_MUSCL_DELTA_SPS, S.SOLVER_DELTA_SPS])
+def test_mixed_precision_velocity_error(lib, solver):
     """FP32 pair arithmetic with compensated sums: velocity L2 error vs the FP64 GPU
     step, on the jittered lattice (an exact lattice puts the MUSCL limiter on
     branch ties that round-off decides; see test_oracle.py)."""
     res = {}
     for prec in (S.PREC_FP64, S.PREC_MIXED):
-        case = S.make_tgv(128, solver=S.SOLVER_MUSCL_DELTA_SPS, precision=prec, jitter=0.1, seed=11)
+        case = S.make_tgv(128, solver=solver, precision=prec, jitter=0.1, seed=11)
         dt = S.baseline_dt(case.cfg)
         with S.Simulation(case.cfg, case.n) as sim:
             sim.set_state(case.pos, case.vel, case.rho, case.mass, case.type)
