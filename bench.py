@@ -13,6 +13,13 @@ reported beside it.  e2e: the same step through the C-ABI with host buffers:
 every step uploads x, v, rho (sph_update_state), advances (sph_step) and
 downloads x, v, rho (sph_get_state).
 
+Side reports in the same line (skipped with --skip-accuracy / --skip-adjoint):
+accuracy (mixed vs FP64 velocity L2), adjoint and adjoint_moving_square
+(cost against a forward step, central-difference checks), moving_square (the
+D/100 moving square, mixed and FP64), plain_method (the 100 x 100 plain
+delta-SPH Taylor-Green case to t = 0.5 against the analytic decay) and
+output_streaming (snapshot overhead).
+
 Multi-GPU: the path does not shard (one GPU holds all particles), so
 --gpus N runs N independent replicas (weak scaling, no collective on the data
 path); value = particles x steps of all ranks / max-over-ranks time.
@@ -287,9 +294,10 @@ def run_native(args, rank, world, local):
     if rank == 0 and not args.skip_adjoint:
         adj = adjoint_report(S)
         adj_ms = adjoint_ms_report(S)
-    ms = None
+    ms = plain = None
     if rank == 0 and not args.skip_accuracy:
         ms = moving_square_report(S)
+        plain = plain_method_report(S)
 
     # ---- CPU baseline (rank 0 only, N = 1) ----------------------------------
     cpu = None
@@ -314,6 +322,7 @@ def run_native(args, rank, world, local):
         "adjoint": adj,
         "adjoint_moving_square": adj_ms,
         "moving_square": ms,
+        "plain_method": plain,
         "output_streaming": streaming,
         "passes_ms_per_step": {
             "images": tm.images_ms / steps, "sort_lists": tm.sort_ms / steps,
@@ -566,6 +575,31 @@ def adjoint_ms_report(S):
         "dC_d_coeffs": [float(x) for x in gc], "dC_dnu": g["nu"], "fd": fd,
         "fd_note": f"central differences eps=1e-7 of the FP64 forward over the first {MS_FD_STEPS} steps",
     }
+
+
+def plain_method_report(S, t_end: float = 0.5):
+    """The 100 x 100 Taylor-Green case of the plain method, as the reference runs it
+    on its CPU: Solver_Normalized_Delta_SPH_SPS (normalised delta-SPH + SPS, no
+    Riemann state), Wendland C2 h = 1.3 dx, rho0 = 1, U0 = 1, c0 = 10, Re = 100,
+    Tait gamma 7, dt = 0.25 h / c0, shifting, RK4 with K1 reuse, to t = 0.5
+    (1,539 steps), FP64 on the GPU.  Device-timed particle-steps/s and KE/KE0 at
+    t = 0.5 against the analytic decay exp(-16 pi^2 nu t)."""
+    case = S.make_tgv(100, solver=S.SOLVER_DELTA_SPS, precision=S.PREC_FP64)
+    dt = S.baseline_dt(case.cfg)
+    nsteps = int(round(t_end / dt))
+    with S.Simulation(case.cfg, case.n) as sim:
+        sim.set_state(case.pos, case.vel, case.rho, case.mass, case.type)
+        ke0 = sim.diagnostics().kinetic_energy
+        sim.reset_timings()
+        d = sim.time_iteration(nsteps, dt)
+        tm = sim.timings()
+    t = nsteps * dt
+    ratio = d.kinetic_energy / ke0
+    analytic = float(np.exp(-16 * np.pi ** 2 * case.cfg.nu * t))
+    return {"case": "TGV 100x100, Solver_Normalized_Delta_SPH_SPS, Wendland C2, FP64, dt = 0.25 h/c0",
+            "steps": nsteps, "t_end": t, "particle_steps_per_s": case.n * nsteps / (tm.total_ms / 1e3),
+            "ms_per_step": tm.total_ms / nsteps, "ke_over_ke0": ratio, "ke_analytic": analytic,
+            "ke_rel_err_vs_analytic": (ratio - analytic) / analytic}
 
 
 def moving_square_report(S, steps: int = 200, warmup: int = 3):
