@@ -255,12 +255,25 @@ __device__ __forceinline__ bool pair_allowed(int rule, int ti, int tj) {
 // and an allowed type pair.  The exact support test is repeated at every RHS on
 // the current positions, so the list only has to be a superset of the pairs of
 // the whole step; k_stage checks the displacement bound that guarantees it.
+// The first kListStage entries of each list are staged in shared memory
+// ([entry][thread], conflict-free) and written out row by row after the scan, so
+// the stores of a warp are coalesced; longer lists write the rest directly.
+constexpr int kListStage = 32;
 template <typename R>
-__global__ void k_build_lists(Params P, Sorted<R> D, unsigned* status) {
-    int a = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(128) k_build_lists(Params P, Sorted<R> D, unsigned* status) {
+    __shared__ unsigned stage[kListStage][128];
+    const int tid = threadIdx.x;
+    int a = blockIdx.x * blockDim.x + tid;
     if (a >= P.n_tot) return;
     int ta = D.type[a];
     int cnt = 0;
+    // one list entry: staged, or (past the stage) straight to global memory
+    auto put = [&](int b, unsigned lower) {
+        const unsigned v = (unsigned)b | lower;
+        if (cnt < kListStage) stage[cnt][tid] = v;
+        else if (cnt < P.max_nbr) D.nbr[(size_t)cnt * P.nbr_stride + a] = v;
+        ++cnt;
+    };
     if (ta != SPH_TYPE_ILL && ta != 0) {
         double2 xa = D.pos[a];
         int ida = D.id[a];
@@ -297,11 +310,7 @@ __global__ void k_build_lists(Params P, Sorted<R> D, unsigned* status) {
                     if (check_type && !pair_allowed(P.pair_rule, ta, tb[k])) continue;
                     const double dx = xa.x - xb[k].x, dy = xa.y - xb[k].y;
                     if (dx * dx + dy * dy > P.r2_list) continue;
-                    if (cnt < P.max_nbr) {
-                        const unsigned lower = ida < ib[k] ? 0x80000000u : 0u;
-                        D.nbr[(size_t)cnt * P.nbr_stride + a] = (unsigned)(b + k) | lower;
-                    }
-                    ++cnt;
+                    put(b + k, ida < ib[k] ? 0x80000000u : 0u);
                 }
             }
             for (; b < b1; ++b) {
@@ -310,15 +319,13 @@ __global__ void k_build_lists(Params P, Sorted<R> D, unsigned* status) {
                 const double2 xb = D.pos[b];
                 const double dx = xa.x - xb.x, dy = xa.y - xb.y;
                 if (dx * dx + dy * dy > P.r2_list) continue;
-                if (cnt < P.max_nbr) {
-                    const unsigned lower = ida < D.id[b] ? 0x80000000u : 0u;
-                    D.nbr[(size_t)cnt * P.nbr_stride + a] = (unsigned)b | lower;
-                }
-                ++cnt;
+                put(b, ida < D.id[b] ? 0x80000000u : 0u);
             }
         }
         if (cnt > P.max_nbr) { atomicOr(status, ST_NBR_OVERFLOW); cnt = P.max_nbr; }
     }
+    const int ns = min(cnt, kListStage);
+    for (int e = 0; e < ns; ++e) D.nbr[(size_t)e * P.nbr_stride + a] = stage[e][tid];
     D.nnbr[a] = cnt;
 }
 
