@@ -2,11 +2,14 @@
 // particle gathers, for every pair neighbour, the linear-Riemann flux (with
 // optional MUSCL reconstruction), continuity, pressure force, Monaghan
 // artificial viscosity, Morris laplacian, delta-alpha term, SPS force, XSPH,
-// delta-SPH density diffusion and (on the last RHS of a step) the shifting sum.
+// delta-SPH density diffusion and (on the last RHS of a step, FP64 and
+// moving-square launches) the shifting sum; the mixed Taylor-Green path forms
+// the shifting sum in k_shift_gather after this pass.
 //
 // Reference loops (all in pair order, scattered to pair_i and pair_j):
 //   Solver_Normalized_Modified_Linear_Riemann_Delta_SPS.f90:300-502, 552-583, 627-635
 //   Solver_Normalized_MUSCL_Linear_Riemann_Delta_SPS.f90:458-682, 690-721
+//   Solver_Normalized_Delta_SPH_SPS.f90:324-512, 610-636 (the plain method)
 //   MUSCL_Limiter: function_module.f90:34-80
 //   Shift_particle_position.f90:78-103
 //   assembly: single_step_compute.f90:152-171

@@ -174,6 +174,14 @@ def test_adjoint_rejects_unsupported_configurations(lib):
         with pytest.raises(S.SphError) as e:
             sim.adjoint_backward()
         assert e.value.code == -1
+    # the plain delta-SPH method is not differentiated
+    case = S.make_tgv(16, solver=S.SOLVER_DELTA_SPS)
+    case.cfg.mls_order = 0
+    with S.Simulation(case.cfg, case.n) as sim:
+        sim.set_state(case.pos, case.vel, case.rho, case.mass, case.type)
+        with pytest.raises(S.SphError) as e:
+            sim.adjoint_forward(2, 1e-4, loss=S.LOSS_KINETIC_ENERGY)
+        assert e.value.code == -7
 
 
 def test_adjoint_of_the_mixed_precision_step(lib):
