@@ -833,7 +833,8 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_a(Params P, Sorted<R> D, Ad
 }
 
 // The shifting sum of particle a over the pairs of the RHS state D, in FP64
-// (the forward forms it in the last pass C of a step, k_pass_c<..., SHIFT>):
+// (the forward forms it in the last pass C of a step, k_pass_c<..., SHIFT>, or
+// in k_shift_gather on the mixed Taylor-Green path):
 //   s_a = sum_b phi(d) V_b r,  phi = (1 + R (W/W_dx)^4) G,  r = x_a - x_b.
 template <typename R>
 __global__ void k_shift_sum(Params P, Sorted<R> D, Adj A) {

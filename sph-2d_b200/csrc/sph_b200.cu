@@ -435,13 +435,21 @@ int rhs(sph_handle* h, int last) {
         if (shc) k_pass_c<R, false, true, true><<<nb, 128, 0, h->stream>>>(P, D);
         else k_pass_c<R, false, true, false><<<nb, 128, 0, h->stream>>>(P, D);
     } else if (P.muscl) {
-        if (shc) k_pass_c<R, true, false, true><<<nb, 128, 0, h->stream>>>(P, D);
-        else k_pass_c<R, true, false, false><<<nb, 128, 0, h->stream>>>(P, D);
+        if constexpr (sizeof(R) == 8) {       // the mixed launches never carry the sum
+            if (shc) k_pass_c<R, true, false, true><<<nb, 128, 0, h->stream>>>(P, D);
+            else k_pass_c<R, true, false, false><<<nb, 128, 0, h->stream>>>(P, D);
+        } else {
+            k_pass_c<R, true, false, false><<<nb, 128, 0, h->stream>>>(P, D);
+        }
     } else {
-        if (shc) k_pass_c<R, false, false, true><<<nb, 128, 0, h->stream>>>(P, D);
-        else k_pass_c<R, false, false, false><<<nb, 128, 0, h->stream>>>(P, D);
+        if constexpr (sizeof(R) == 8) {
+            if (shc) k_pass_c<R, false, false, true><<<nb, 128, 0, h->stream>>>(P, D);
+            else k_pass_c<R, false, false, false><<<nb, 128, 0, h->stream>>>(P, D);
+        } else {
+            k_pass_c<R, false, false, false><<<nb, 128, 0, h->stream>>>(P, D);
+        }
     }
-    if (sh && sep) {
+    if constexpr (sizeof(R) == 4) if (sh && sep) {
         // timed with the update: shifting is part of the step's second pass
         tic(h, PH_UPDATE);
         k_shift_gather<R><<<nb, 128, 0, h->stream>>>(P, D);
