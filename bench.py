@@ -555,7 +555,10 @@ def adjoint_ms_report(S):
         gcf = np.einsum("sq,sqk->k", sim.adjoint_motion_gradient(), jac[:nf])
     fd = []
     for k in (0, 1):
-        eps = 1e-7          # the moving-square tests' step (Gaussian: kinks at the cut-off)
+        # the improved Gaussian's RHS jumps where a pair crosses the 3h cut-off; at
+        # 1e-7 on a0 the difference interval shifts one such crossing by a step
+        # (2.8e-4 off), at 1e-8 none (8e-7; at 1e-9 rounding gives 1e-5)
+        eps = 1e-8
         cp, cm = coeffs.copy(), coeffs.copy()
         cp[k] += eps
         cm[k] -= eps
@@ -573,7 +576,7 @@ def adjoint_ms_report(S):
         "adjoint_particle_steps_per_s": case.n * MS_STEPS / t_bwd,
         "backward_device_ms": tb.total_ms, "backward_reverse_kernels_ms": tb.adjoint_ms,
         "dC_d_coeffs": [float(x) for x in gc], "dC_dnu": g["nu"], "fd": fd,
-        "fd_note": f"central differences eps=1e-7 of the FP64 forward over the first {MS_FD_STEPS} steps",
+        "fd_note": f"central differences eps=1e-8 of the FP64 forward over the first {MS_FD_STEPS} steps",
     }
 
 

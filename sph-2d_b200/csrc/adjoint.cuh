@@ -1040,6 +1040,57 @@ __global__ void k_snap_copy(int n, SnapPtrs dst, SnapPtrs src) {
     dst.r_drho[i] = src.r_drho[i]; dst.r_acc[i] = src.r_acc[i]; dst.r_avg[i] = src.r_avg[i];
 }
 
+// The sorted step-start state a reversed step needs (what prepare wrote: the
+// permutation, the sorted master state and records, the cell ranges and the
+// neighbour lists, and the id-order image routing), kept per step of a segment
+// while the segment is re-run and restored by the reverse step instead of
+// re-sorting.  One descriptor per array (a neighbour-list row is an array):
+// words = 4-byte words per particle (per_particle = 1, times n_tot) or in all.
+struct PrepDesc {
+    unsigned* field;
+    long long off;        // word offset in a slot
+    int per_particle;
+    int words;
+    long long pitch;      // > 0: the neighbour lists, row e of particle a at e * pitch + a
+};
+
+// save = 1: arrays -> slot; save = 0: slot -> arrays.  blockIdx.y = descriptor.
+// cnt: the list lengths (the live ones when saving, the slot's copy when
+// restoring, so no launch reads counts it is writing); each particle copies its
+// own entries only.  Arrays whose size is a multiple of 16 bytes move in 16-byte
+// words (the arrays and the slot offsets are 256-byte aligned).
+__global__ void k_prep_copy(const PrepDesc* d, int n_tot, unsigned* slot, int save, const int* cnt) {
+    const PrepDesc c = d[blockIdx.y];
+    unsigned* s = slot + c.off;
+    const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    if (c.pitch > 0) {
+        for (long long a = t0; a < n_tot; a += stride) {
+            const int n = cnt[a];
+            for (int e = 0; e < n; ++e) {
+                const long long k = (long long)e * c.pitch + a;
+                if (save) s[k] = c.field[k];
+                else c.field[k] = s[k];
+            }
+        }
+        return;
+    }
+    const long long total = c.per_particle ? (long long)n_tot * c.words : (long long)c.words;
+    if ((total & 3) == 0) {
+        uint4* f4 = reinterpret_cast<uint4*>(c.field);
+        uint4* s4 = reinterpret_cast<uint4*>(s);
+        for (long long w = t0; w < total / 4; w += stride) {
+            if (save) s4[w] = f4[w];
+            else f4[w] = s4[w];
+        }
+    } else {
+        for (long long w = t0; w < total; w += stride) {
+            if (save) s[w] = c.field[w];
+            else c.field[w] = s[w];
+        }
+    }
+}
+
 // Copy of the stage state (positions and records) into the stage store.
 template <typename R>
 __global__ void k_keep_stage(int n, Sorted<R> D, double2* pos, double4* kin, typename VT<R>::V4* aux) {

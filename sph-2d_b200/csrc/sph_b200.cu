@@ -690,6 +690,14 @@ struct AdjCtx {
     double4* st_kin = nullptr;
     double4* st_aux = nullptr;  // V4 of the pair precision (float4 uses the first half)
     std::vector<int> seg_ntot;  // particles + images of each step of the segment
+    // sorted step-start state of each step of the segment (PrepDesc), kept with
+    // the stage states when memory allows: [stage_slots][prep_words]
+    unsigned* prep = nullptr;
+    long long prep_words = 0;
+    PrepDesc* d_prep = nullptr;    // descriptor table (rebuilt by each forward call)
+    int n_prep = 0, cap_prep = 0;
+    long long prep_nnbr_off = 0;   // slot offset of the saved list lengths
+    std::vector<int> seg_nimg, seg_nlr;
     double2* target = nullptr;
     double* loss_part = nullptr;
     Adj A{};
@@ -763,6 +771,102 @@ struct SchedGuard {
     ~SchedGuard() { h->sched = nullptr; h->sched_n = 0; h->drag_acc = nullptr; }
 };
 
+// The arrays prepare writes for one step (see PrepDesc): per-particle fields of
+// the sorted state, one descriptor per neighbour-list row, the cell ranges and
+// the id-order image routing; slot offsets from the capacities, 256-byte aligned.
+template <typename R>
+std::vector<PrepDesc> prep_table(sph_handle* h, long long* words, long long* nnbr_off = nullptr) {
+    Sorted<R>& D = sorted<R>(h);
+    std::vector<PrepDesc> v;
+    long long off = 0;
+    const long long cap = h->cap_tot;
+    auto add = [&](void* f, int per_particle, long long w, long long pitch = 0) {
+        v.push_back(PrepDesc{(unsigned*)f, off, per_particle, (int)w, pitch});
+        const long long nw = pitch > 0 ? pitch * w : per_particle ? cap * w : w;
+        off += (nw + 63) & ~63LL;
+    };
+    auto pp = [&](void* f, size_t bytes) { add(f, 1, (long long)(bytes / 4)); };
+    pp(D.id, 4); pp(D.slot_of, 4); pp(D.type, 4); pp(D.itype, 4); pp(D.blabel, 4);
+    pp(D.pos, sizeof(*D.pos)); pp(D.pos0, sizeof(*D.pos0)); pp(D.vel0, sizeof(*D.vel0));
+    pp(D.rho0, sizeof(*D.rho0)); pp(D.mass, sizeof(*D.mass)); pp(D.smass, sizeof(*D.smass));
+    pp(D.kin, sizeof(*D.kin)); pp(D.aux, sizeof(*D.aux));
+    pp(D.c_drho, sizeof(*D.c_drho)); pp(D.c_acc, sizeof(*D.c_acc)); pp(D.c_avg, sizeof(*D.c_avg));
+    if (nnbr_off) *nnbr_off = off;
+    pp(D.nnbr, 4);
+    if (sizeof(R) == 4) {
+        pp(D.vol64, sizeof(*D.vol64)); pp(D.kh, sizeof(*D.kh)); pp(D.kl, sizeof(*D.kl)); pp(D.xhl, sizeof(*D.xhl));
+    }
+    // the lists: max_nbr rows at the lists' own pitch (nbr_stride = cap_tot)
+    add(D.nbr, 1, h->P.max_nbr, h->P.nbr_stride);
+    add(D.cell_start, 0, h->ncells);
+    add(D.cell_end, 0, h->ncells);
+    pp(h->S.lr_cnt, 4); pp(h->S.lr_off, 4); pp(h->S.tb_cnt, 4); pp(h->S.tb_off, 4);
+    *words = off;
+    return v;
+}
+
+long long prep_slot_words(sph_handle* h) {
+    long long w = 0;
+    if (h->mixed) prep_table<float>(h, &w);
+    else prep_table<double>(h, &w);
+    return w;
+}
+
+// Upload the descriptor table of the handle's current arrays (the per-call part).
+template <typename R>
+int prep_upload(sph_handle* h) {
+    AdjCtx* X = h->adj;
+    if (!X->prep) return SPH_OK;
+    long long w = 0;
+    std::vector<PrepDesc> v = prep_table<R>(h, &w, &X->prep_nnbr_off);
+    if (w != X->prep_words) return SPH_E_ARG;
+    if (X->cap_prep < (int)v.size()) {
+        int rc = adj_alloc(X, &X->d_prep, v.size());
+        if (rc) return rc;
+        X->cap_prep = (int)v.size();
+    }
+    CK(cudaMemcpyAsync(X->d_prep, v.data(), sizeof(PrepDesc) * v.size(), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    X->n_prep = (int)v.size();
+    return SPH_OK;
+}
+
+// After prepare in the segment re-run: keep what it wrote in slot j.
+int prep_save(sph_handle* h, int j) {
+    AdjCtx* X = h->adj;
+    if (!X->prep) return SPH_OK;
+    const int nt = h->P.n_tot;
+    const int* cnt = h->mixed ? h->D32.nnbr : h->D64.nnbr;
+    k_prep_copy<<<dim3(blocks(nt, 256), X->n_prep), 256, 0, h->stream>>>(
+        X->d_prep, nt, X->prep + (size_t)j * X->prep_words, 1, cnt);
+    CK(cudaGetLastError());
+    h->launches += 1;
+    X->seg_nimg[j] = h->n_img;
+    X->seg_nlr[j] = h->n_lr;
+    return SPH_OK;
+}
+
+// In place of prepare in a reversed step: the sorted step-start state of slot j
+// (the same as a re-sort of the restored step-start state gives, the sort being
+// deterministic).
+int prep_restore(sph_handle* h, int j) {
+    AdjCtx* X = h->adj;
+    Params& P = h->P;
+    P.n_host = h->n_host;
+    h->n_img = X->seg_nimg[j];
+    h->n_lr = X->seg_nlr[j];
+    P.n_tot = h->n_host + h->n_img;
+    tic(h, PH_SORT);
+    unsigned* slot = X->prep + (size_t)j * X->prep_words;
+    k_prep_copy<<<dim3(blocks(P.n_tot, 256), X->n_prep), 256, 0, h->stream>>>(
+        X->d_prep, P.n_tot, slot, 0, (const int*)(slot + X->prep_nnbr_off));
+    CK(cudaGetLastError());
+    h->launches += 1;
+    h->sorted_valid = true;
+    h->staging_valid = false;
+    return SPH_OK;
+}
+
 int adj_prepare_ctx(sph_handle* h, const sph_adj_config* ac) {
     AdjCtx* X = h->adj;
     const int nseg = (ac->nsteps + ac->checkpoint_every - 1) / ac->checkpoint_every;
@@ -804,6 +908,14 @@ int adj_prepare_ctx(sph_handle* h, const sph_adj_config* ac) {
         if ((rc = adj_alloc(X, &X->st_pos, ns)) || (rc = adj_alloc(X, &X->st_kin, ns)) ||
             (rc = adj_alloc(X, &X->st_aux, ns)))
             return rc;
+        // the sorted step-start states, when every step has a stage slot and they
+        // also leave 1 GiB free (else the reverse step re-sorts)
+        const long long pw = prep_slot_words(h);
+        CK(cudaMemGetInfo(&free_b, &total_b));
+        if (X->stage_slots == every && (size_t)pw * 4 * every + (size_t(1) << 30) <= free_b) {
+            if ((rc = adj_alloc(X, &X->prep, (size_t)pw * every))) return rc;
+            X->prep_words = pw;
+        }
     }
     if (h->P.ms && !X->A.gavg) {
         Adj& A = X->A;
@@ -828,13 +940,15 @@ int adj_prepare_ctx(sph_handle* h, const sph_adj_config* ac) {
     X->nsteps = ac->nsteps; X->every = every; X->nseg = nseg; X->loss = ac->loss; X->dt = ac->dt;
     X->n_host = h->n_host;
     X->seg_ntot.assign(every, 0);
+    X->seg_nimg.assign(every, 0);
+    X->seg_nlr.assign(every, 0);
     return SPH_OK;
 }
 
 template <typename R>
 int adjoint_forward(sph_handle* h, const sph_adj_config* ac, double* loss) {
     int rc = adj_prepare_ctx(h, ac);
-    if (rc) return rc;
+    if (rc || (rc = prep_upload<R>(h))) return rc;
     AdjCtx* X = h->adj;
     const int n = h->n_host;
     if (ac->loss == SPH_LOSS_VELOCITY_MISFIT) {
@@ -908,7 +1022,7 @@ int keep_stage(sph_handle* h, int j, int k) {
 template <typename R>
 int step_keep(sph_handle* h, double dt, int j, bool full) {
     int rc = step_begin<R>(h, dt);
-    if (rc || (rc = prepare<R>(h))) return rc;
+    if (rc || (rc = prepare<R>(h)) || (rc = prep_save(h, j))) return rc;
     h->adj->seg_ntot[j] = h->P.n_tot;
     const int first = h->step_count == 0;
     if (first && (rc = rhs<R>(h, 0))) return rc;
@@ -986,7 +1100,7 @@ int adj_step(sph_handle* h, bool first, int j) {
         if ((rc = step_keep<R>(h, dt, 0, false))) return rc;
         j = 0;
     } else {
-        if ((rc = prepare<R>(h))) return rc;
+        if ((rc = X->prep ? prep_restore(h, j) : prepare<R>(h))) return rc;
         if (h->P.n_tot != X->seg_ntot[j]) return SPH_E_ARG;
     }
     const Params& P = h->P;
@@ -1101,7 +1215,7 @@ int adj_step_ms(sph_handle* h, bool first, int j, int jstep) {
         if ((rc = step_keep<R>(h, dt, 0, false))) return rc;
         j = 0;
     } else {
-        if ((rc = step_begin<R>(h, dt)) || (rc = prepare<R>(h))) return rc;
+        if ((rc = step_begin<R>(h, dt)) || (rc = X->prep ? prep_restore(h, j) : prepare<R>(h))) return rc;
         if (h->P.n_tot != X->seg_ntot[j]) return SPH_E_ARG;
     }
     const Params& P = h->P;
