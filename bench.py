@@ -387,6 +387,7 @@ def adjoint_leg(S, precision, solver=None):
         out = {"loss": loss, "forward_s": t_fwd, "forward_checkpointed_s": t_fck, "backward_s": t_bwd,
                "adjoint_over_forward": t_bwd / t_fwd,
                "forward_device_ms": dev_fwd, "backward_device_ms": tb.total_ms,
+               "adjoint_over_forward_device": tb.total_ms / dev_fwd,
                "backward_reverse_kernels_ms": tb.adjoint_ms, "grad": g}
     return case, dt, target, out
 
@@ -434,7 +435,7 @@ def adjoint_report(S):
     _, _, _, md = adjoint_leg(S, S.PREC_FP64, S.SOLVER_MUSCL_DELTA_SPS)
     gm, g64 = m["grad"]["vel0"], d["grad"]["vel0"]
     keep = ("loss", "forward_s", "forward_checkpointed_s", "backward_s", "adjoint_over_forward",
-            "forward_device_ms", "backward_device_ms", "backward_reverse_kernels_ms")
+            "forward_device_ms", "backward_device_ms", "adjoint_over_forward_device", "backward_reverse_kernels_ms")
     return {
         "case": f"TGV {ADJ_SIDE}x{ADJ_SIDE} ({case.n} particles), {ADJ_STEPS} steps, checkpoint every {ADJ_EVERY}, "
                 "velocity-misfit loss vs a target from 8 seeded Fourier modes (0.05 U0); modified linear Riemann "
@@ -533,9 +534,11 @@ def adjoint_ms_report(S):
         for rep in range(2):          # the first round warms up allocations
             reset(sim)
             sim.set_body_motion((coeffs[0], 0.0))
+            sim.reset_timings()
             t0 = time.perf_counter()
             sim.time_iteration(MS_STEPS, dt)
             t_fwd = time.perf_counter() - t0
+            dev_fwd = sim.timings().total_ms
             reset(sim)
             t0 = time.perf_counter()
             L = sim.adjoint_forward(MS_STEPS, dt, checkpoint_every=MS_EVERY, loss=S.LOSS_DRAG, body_motion=motion)
@@ -574,7 +577,8 @@ def adjoint_ms_report(S):
         "adjoint_over_forward": t_bwd / t_fwd,
         "forward_particle_steps_per_s": case.n * MS_STEPS / t_fwd,
         "adjoint_particle_steps_per_s": case.n * MS_STEPS / t_bwd,
-        "backward_device_ms": tb.total_ms, "backward_reverse_kernels_ms": tb.adjoint_ms,
+        "forward_device_ms": dev_fwd, "backward_device_ms": tb.total_ms,
+        "adjoint_over_forward_device": tb.total_ms / dev_fwd, "backward_reverse_kernels_ms": tb.adjoint_ms,
         "dC_d_coeffs": [float(x) for x in gc], "dC_dnu": g["nu"], "fd": fd,
         "fd_note": f"central differences eps=1e-8 of the FP64 forward over the first {MS_FD_STEPS} steps",
     }

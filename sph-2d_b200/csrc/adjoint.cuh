@@ -570,17 +570,28 @@ __global__ void __launch_bounds__(kAdjThreads, MUSCL ? SPH_ADJ_C_MUSCL_MIN_BLOCK
 }
 
 // dL/dnu += sum of the block partials, in block order.
+// Sum over one block (any multiple of 32 threads up to 1024) in a fixed order:
+// shuffles within each warp, then over the warp sums.  The result is in thread 0.
+__device__ __forceinline__ double block_sum(double s, double* red32) {
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) red32[w] = s;
+    __syncthreads();
+    s = 0.0;
+    if (w == 0) {
+        s = lane < (int)(blockDim.x >> 5) ? red32[lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    }
+    __syncthreads();
+    return s;
+}
+
 __global__ void k_adj_nu_sum(int nparts, const double* part, double* acc) {
-    __shared__ double red[256];
+    __shared__ double red[32];
     double s = 0.0;
     for (int i = threadIdx.x; i < nparts; i += blockDim.x) s += part[i];
-    red[threadIdx.x] = s;
-    __syncthreads();
-    for (int w = 128; w > 0; w >>= 1) {
-        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) acc[0] += red[0];
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) acc[0] += s;
 }
 
 // Reverse of the per-particle end of pass A.  shift: the RHS is the last of a
@@ -1523,18 +1534,12 @@ __global__ void k_adj_body_pos(Params P, Sorted<R> D, Adj A, double* part) {
 
 // out[q] += scale * sum_i part[q nparts + i], q < nq, in block order.
 __global__ void k_adj_motion_sum(int nparts, int nq, const double* part, double scale, double* out) {
-    __shared__ double red[256];
+    __shared__ double red[32];
     for (int q = 0; q < nq; ++q) {
         double s = 0.0;
         for (int i = threadIdx.x; i < nparts; i += blockDim.x) s += part[(size_t)q * nparts + i];
-        red[threadIdx.x] = s;
-        __syncthreads();
-        for (int w = 128; w > 0; w >>= 1) {
-            if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
-            __syncthreads();
-        }
-        if (threadIdx.x == 0) out[q] += scale * red[0];
-        __syncthreads();
+        s = block_sum(s, red);
+        if (threadIdx.x == 0) out[q] += scale * s;
     }
 }
 

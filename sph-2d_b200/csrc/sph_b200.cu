@@ -984,7 +984,7 @@ int adjoint_forward(sph_handle* h, const sph_adj_config* ac, double* loss) {
                                                  X->loss_part);
         h->launches += 2;
         CK(cudaMemsetAsync(h->d_diag, 0, sizeof(double), h->stream));
-        k_adj_nu_sum<<<1, 256, 0, h->stream>>>(nparts, X->loss_part, h->d_diag);
+        k_adj_nu_sum<<<1, 1024, 0, h->stream>>>(nparts, X->loss_part, h->d_diag);
         CK(cudaMemcpyAsync(&v, h->d_diag, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     }
     CK(cudaStreamSynchronize(h->stream));
@@ -1133,7 +1133,7 @@ int adj_step(sph_handle* h, bool first, int j) {
     }
     tic(h, PH_ADJ);
     const int nba = blocks((long long)P.n_tot * kAdjLanes, kAdjThreads);
-    k_adj_nu_sum<<<1, 256, 0, h->stream>>>((first ? 4 : 3) * nba, A.nu_part + (first ? 0 : nba), A.nu_acc);
+    k_adj_nu_sum<<<1, 1024, 0, h->stream>>>((first ? 4 : 3) * nba, A.nu_part + (first ? 0 : nba), A.nu_acc);
     k_adj_scatter<R><<<nb, 256, 0, h->stream>>>(P, D, A, first ? 1 : 0);
     h->launches += 2;
     if (h->cfg.periodic) {
@@ -1181,7 +1181,7 @@ int adj_rhs_ms(sph_handle* h, const Sorted<R>& V, int k, int pred, bool drag, in
         double* part = A.nu_part + (size_t)4 * nbc;
         k_mark_body_nbrs<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, V);
         k_adj_drag<R><<<nb, kAdjThreads, 0, h->stream>>>(P, V, A, X->dloss * X->dt, part);
-        k_adj_nu_sum<<<1, 256, 0, h->stream>>>(nb, part, A.nu_acc);
+        k_adj_nu_sum<<<1, 1024, 0, h->stream>>>(nb, part, A.nu_acc);
         h->launches += 3;
     }
     k_adj_point<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, V, A, 0);
@@ -1190,7 +1190,7 @@ int adj_rhs_ms(sph_handle* h, const Sorted<R>& V, int k, int pred, bool drag, in
         const int ngb = blocks((long long)h->n_ghost * 32, kAdjThreads);
         k_adj_ghost_lambda<R><<<ngb, kAdjThreads, 0, h->stream>>>(P, V, A, h->d_ghost_ids, h->n_ghost, h->t_phys,
                                                                   h->body_acc[0], h->body_acc[1], A.mo_part);
-        k_adj_motion_sum<<<1, 256, 0, h->stream>>>(ngb, 4, A.mo_part, 1.0, A.g_motion + 4 * (size_t)jstep);
+        k_adj_motion_sum<<<1, 1024, 0, h->stream>>>(ngb, 4, A.mo_part, 1.0, A.g_motion + 4 * (size_t)jstep);
         k_adj_ghost_water<R><<<148 * 8, kAdjThreads, 0, h->stream>>>(P, V, A, h->body_acc[0], h->body_acc[1]);
         h->launches += 3;
     }
@@ -1233,12 +1233,12 @@ int adj_step_ms(sph_handle* h, bool first, int j, int jstep) {
     }
     tic(h, PH_ADJ);
     const int nba = blocks((long long)P.n_tot * kAdjLanes, kAdjThreads);
-    k_adj_nu_sum<<<1, 256, 0, h->stream>>>((first ? 2 : 1) * nba, A.nu_part + (first ? 0 : nba), A.nu_acc);
+    k_adj_nu_sum<<<1, 1024, 0, h->stream>>>((first ? 2 : 1) * nba, A.nu_part + (first ? 0 : nba), A.nu_acc);
     // with library ghost assignment the body moved by u_body dt at the step start:
     // dL/du_body += dt sum_body dL/dx
     if (P.ghost_assign) {
         k_adj_body_pos<R><<<nb, 256, 0, h->stream>>>(P, D, A, A.mo_part);
-        k_adj_motion_sum<<<1, 256, 0, h->stream>>>(nb, 2, A.mo_part, dt, A.g_motion + 4 * (size_t)jstep);
+        k_adj_motion_sum<<<1, 1024, 0, h->stream>>>(nb, 2, A.mo_part, dt, A.g_motion + 4 * (size_t)jstep);
         h->launches += 2;
     }
     k_adj_scatter<R><<<nb, 256, 0, h->stream>>>(P, D, A, first ? 1 : 0);
