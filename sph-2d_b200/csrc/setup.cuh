@@ -197,10 +197,19 @@ __global__ void k_gather_sorted(Params P, Staging S, Sorted<R> D, const unsigned
     double2 x = S.pos[i];
     D.pos[s] = x;
     D.pos0[s] = x;
-    D.vel0[s] = S.vel[i];
-    D.rho0[s] = S.rho[i];
-    D.mass[s] = S.mass[i];
-    D.smass[s] = S.smass[i];
+    const double2 v = S.vel[i];
+    const double rho = S.rho[i], m = S.mass[i], sm = S.smass[i];
+    D.vel0[s] = v;
+    D.rho0[s] = rho;
+    D.mass[s] = m;
+    D.smass[s] = sm;
+    // neighbour records of the step-start state (formed here from the values
+    // just gathered, instead of a second pass over the sorted arrays)
+    double p, c;
+    eos64(P, rho, p, c);
+    D.kin[s] = make_double4(v.x, v.y, rho, p);
+    D.aux[s] = mk4<R>((R)m, (R)(m / rho), (R)c, (R)sm);
+    store_split(D, s, x, make_double4(v.x, v.y, rho, p));
     if (i < P.n_host) {
         D.c_drho[s] = (R)S.r_drho[i];
         D.c_acc[s] = mk2<R>((R)S.r_acc[i].x, (R)S.r_acc[i].y);
@@ -327,21 +336,6 @@ __global__ void __launch_bounds__(128) k_build_lists(Params P, Sorted<R> D, unsi
     const int ns = min(cnt, kListStage);
     for (int e = 0; e < ns; ++e) D.nbr[(size_t)e * P.nbr_stride + a] = stage[e][tid];
     D.nnbr[a] = cnt;
-}
-
-// --- 7. neighbour records of the step-start state (all particles) ---------
-template <typename R>
-__global__ void k_records(Params P, Sorted<R> D) {
-    int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= P.n_tot) return;
-    double rho = D.rho0[s];
-    double p, c;
-    eos64(P, rho, p, c);
-    double2 v = D.vel0[s];
-    double m = D.mass[s];
-    D.kin[s] = make_double4(v.x, v.y, rho, p);
-    D.aux[s] = mk4<R>((R)m, (R)(m / rho), (R)c, (R)D.smass[s]);
-    store_split(D, s, D.pos[s], make_double4(v.x, v.y, rho, p));
 }
 
 }  // namespace sph

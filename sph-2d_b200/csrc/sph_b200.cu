@@ -396,9 +396,8 @@ int prepare(sph_handle* h) {
     k_cell_ranges<<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P.n_tot, h->keys_out, D.cell_start, D.cell_end,
                                                                 h->dead_key);
     k_build_lists<R><<<blocks(P.n_tot, 128), 128, 0, h->stream>>>(P, D, h->d_status);
-    k_records<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, D);
     CK(cudaGetLastError());
-    h->launches += 5;
+    h->launches += 4;
     h->sorted_valid = true;
     h->staging_valid = false;   // the master state now lives in the sorted arrays
     return SPH_OK;
