@@ -216,3 +216,24 @@ def test_reference_kinetic_energy_trajectory_on_gpu(lib):
             worst_v = max(worst_v, abs(d.max_speed - vmax) / vmax)
     assert worst < 5e-4, worst
     assert worst_v < 5e-3, worst_v
+
+
+@pytest.mark.parametrize("field,value", [("solver", 9), ("kernel_model", 3), ("mls_order", 2), ("shift_n", 3),
+                                         ("cell_skin", 3.0), ("precision", 7), ("integrator", 5)])
+def test_invalid_configuration_is_rejected(lib, field, value):
+    """sph_init validates the configuration before it allocates or launches
+    anything: each out-of-range switch returns SPH_E_CONFIG."""
+    case = S.make_tgv(16)
+    cfg = case.cfg.copy()
+    setattr(cfg, field, value)
+    with pytest.raises(S.SphError) as e:
+        S.Simulation(cfg, case.n)
+    assert e.value.code == -7
+
+
+def test_state_larger_than_capacity_is_rejected(lib):
+    case = S.make_tgv(16)
+    with S.Simulation(case.cfg, case.n - 1) as sim:
+        with pytest.raises(S.SphError) as e:
+            sim.set_state(case.pos, case.vel, case.rho, case.mass, case.type)
+        assert e.value.code == -2
