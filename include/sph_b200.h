@@ -39,7 +39,9 @@ extern "C" {
 #define SPH_E_CAPACITY   -2   /* pair / particle / cell capacity exceeded   */
 #define SPH_E_NONFINITE  -3   /* NaN/Inf produced in the state               */
 #define SPH_E_CUDA       -5   /* a CUDA runtime call failed                  */
-#define SPH_E_TIMEOUT    -6   /* a bounded device wait gave up               */
+#define SPH_E_TIMEOUT    -6   /* reserved: no kernel of this library waits on
+                                 another block, launch or device, so no wait can
+                                 time out; never returned                         */
 #define SPH_E_CONFIG     -7   /* unsupported configuration value             */
 #define SPH_E_DOMAIN     -8   /* a particle left the cell grid               */
 #define SPH_E_SKIN       -9   /* a particle moved further than the cell skin */
