@@ -495,7 +495,8 @@ def adjoint_ms_report(S):
     sum_s dt F_x / (T F0), F0 = rho0 U^2 D / 2.  Forward = time_iteration over
     the same number of steps with the body at its mean speed a0 (the same work
     per step: translation, ghost assignment, RHS, body force).  The
-    gradient with respect to a0 and a1 is checked by central differences on the
+    gradient with respect to a0 and the four Fourier coefficients is checked by
+    central differences on the
     first 200 steps of the same case: the improved Gaussian's gradient does not
     vanish at its 3h cut-off, so the right-hand side jumps whenever a pair
     crosses the support, and over thousands of steps so many crossings move by
@@ -557,7 +558,7 @@ def adjoint_ms_report(S):
         sim.adjoint_backward(scale)
         gcf = np.einsum("sq,sqk->k", sim.adjoint_motion_gradient(), jac[:nf])
     fd = []
-    for k in (0, 1):
+    for k in range(len(coeffs)):
         # the improved Gaussian's RHS jumps where a pair crosses the 3h cut-off; at
         # 1e-7 on a0 the difference interval shifts one such crossing by a step
         # (2.8e-4 off), at 1e-8 none (8e-7; at 1e-9 rounding gives 1e-5)
