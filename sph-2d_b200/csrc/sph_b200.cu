@@ -474,11 +474,11 @@ int rhs(sph_handle* h, int last) {
 }
 
 template <typename R>
-int stage(sph_handle* h, int st, double dt, int use_carried, int do_shift) {
+int stage(sph_handle* h, int st, double dt, int use_carried, int do_shift, int to_staging = 0) {
     const Params& P = h->P;
     tic(h, PH_UPDATE);
     k_stage<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, sorted<R>(h), st, dt, use_carried, do_shift,
-                                                             h->d_status);
+                                                             h->d_status, h->S, to_staging);
     CK(cudaGetLastError());
     h->launches += 1;
     return SPH_OK;
@@ -544,6 +544,10 @@ int run_steps(sph_handle* h, int nsteps, double dt) {
         // density re-initialisation after every mls_every-th step (1-based step number)
         const bool mls = h->P.mls_order != 0 && (h->step_count + 1) % h->P.mls_every == 0;
         const int shift_now = mls ? 0 : h->cfg.shifting;
+        // the Taylor-Green driver's final stage keeps the id-order staging current
+        // (the moving-square ghost assignment and MLS change the sorted state
+        // after or outside it)
+        const int to_staging = (!h->P.ms && !h->P.ghost_assign && !mls) ? 1 : 0;
         if (first) { rc = rhs<R>(h, 0); if (rc) return rc; }
         if (h->cfg.integrator == SPH_INTEGRATOR_EULER_PC) {
             rc = stage<R>(h, 10, dt, first ? 0 : 1, 0); if (rc) return rc;
@@ -556,7 +560,8 @@ int run_steps(sph_handle* h, int nsteps, double dt) {
             rc = rhs<R>(h, 0); if (rc) return rc;
             rc = stage<R>(h, 2, dt, 0, 0); if (rc) return rc;
             rc = rhs<R>(h, 1); if (rc) return rc;
-            rc = stage<R>(h, 3, dt, 0, shift_now); if (rc) return rc;
+            rc = stage<R>(h, 3, dt, 0, shift_now, to_staging); if (rc) return rc;
+            if (to_staging) h->staging_valid = true;
         }
         if (mls && (rc = reinit_density<R>(h, h->cfg.shifting))) return rc;
         tic(h, -1);

@@ -39,8 +39,12 @@ __device__ __forceinline__ void apply_shift(const Params& P, const Sorted<R>& D,
 }
 
 template <typename R>
+// to_staging (final stages of the Taylor-Green driver): also write the new
+// master state and carried rates of each host particle to the id-order staging
+// arrays, exactly what k_unsort would copy there, so the next step's set-up and
+// a state read need no unsort pass (static fields are unchanged in staging).
 __global__ void k_stage(Params P, Sorted<R> D, int stage, double dt, int use_carried, int do_shift,
-                        unsigned* status) {
+                        unsigned* status, Staging S, int to_staging) {
     using V2 = typename VT<R>::V2;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= P.n_tot) return;
@@ -120,6 +124,18 @@ __global__ void k_stage(Params P, Sorted<R> D, int stage, double dt, int use_car
         D.vel0[s] = make_double2(u, v);
         D.rho0[s] = rho;
         D.pos[s] = make_double2(x, y);
+        if (to_staging) {
+            const int i = D.id[s];
+            if (i < P.n_host) {
+                S.pos[i] = make_double2(x, y);
+                S.vel[i] = make_double2(u, v);
+                S.rho[i] = rho;
+                // the carried rates as k_unsort reads them back (rounded to R)
+                S.r_drho[i] = (double)(R)dr;
+                S.r_acc[i] = make_double2((double)(R)ax, (double)(R)ay);
+                S.r_avg[i] = make_double2((double)(R)gx, (double)(R)gy);
+            }
+        }
     } else {
         D.pos[s] = make_double2(x, y);
     }
