@@ -21,7 +21,7 @@ struct Staging {
     double* r_drho;
     double2* r_acc;
     double2* r_avg;
-    int* cnt;         // image counts / scan scratch
+    int* cnt;         // scratch pair that sizes the image scan's temporary storage
     int* off;
     // image counts and offsets of this step, kept for routing image adjoints:
     // left/right images of host i sit at n_host + lr_off[i] + k (k < lr_cnt[i]),
@@ -31,11 +31,6 @@ struct Staging {
     int* tb_cnt;
     int* tb_off;
 };
-
-__global__ void k_copy_int2(int n, const int* a, const int* b, int* a2, int* b2) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) { a2[i] = a[i]; b2[i] = b[i]; }
-}
 
 // --- 1. periodic wrap (Distribute_Period_Boundary_Particle.f90:56-90) -------
 __global__ void k_wrap(Params P, Staging S) {
@@ -53,7 +48,9 @@ __global__ void k_wrap(Params P, Staging S) {
 // --- 2. images: count per source, then emit at scanned offsets -------------
 // axis 0: left/right images of the host particles (:98-148),
 // axis 1: bottom/top images of host particles and left/right images (:156-206).
-__global__ void k_img_count(Params P, Staging S, int n_src, int axis) {
+// cnt: the routing counts of this axis (lr_cnt / tb_cnt), scanned in place into
+// the routing offsets (lr_off / tb_off) that k_img_emit reads
+__global__ void k_img_count(Params P, Staging S, int n_src, int axis, int* cnt) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_src) return;
     int c = 0;
@@ -63,7 +60,7 @@ __global__ void k_img_count(Params P, Staging S, int n_src, int axis) {
         if (x <= (lo + P.band) && x >= lo) c++;
         if (x >= (hi - P.band) && x <= hi) c++;
     }
-    S.cnt[i] = c;
+    cnt[i] = c;
 }
 
 __global__ void k_img_emit(Params P, Staging S, int n_src, int axis, int base, const int* off) {

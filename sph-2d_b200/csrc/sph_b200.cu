@@ -358,30 +358,28 @@ int prepare(sph_handle* h) {
     int n_img = 0;
     if (h->cfg.periodic) {
         k_wrap<<<blocks(h->n_host, 256), 256, 0, h->stream>>>(P, h->S);
-        // left/right images of the host particles
-        k_img_count<<<blocks(h->n_host, 256), 256, 0, h->stream>>>(P, h->S, h->n_host, 0);
+        // left/right images of the host particles; the counts and offsets are
+        // kept for routing image adjoints back to their sources
+        k_img_count<<<blocks(h->n_host, 256), 256, 0, h->stream>>>(P, h->S, h->n_host, 0, h->S.lr_cnt);
         int n_lr = 0;
-        rc = scan_total(h, h->S.cnt, h->S.off, h->n_host, &n_lr);
+        rc = scan_total(h, h->S.lr_cnt, h->S.lr_off, h->n_host, &n_lr);
         if (rc) return rc;
         if (h->n_host + n_lr > h->cap_tot) return SPH_E_CAPACITY;
-        k_img_emit<<<blocks(h->n_host, 256), 256, 0, h->stream>>>(P, h->S, h->n_host, 0, h->n_host, h->S.off);
-        k_copy_int2<<<blocks(h->n_host, 256), 256, 0, h->stream>>>(h->n_host, h->S.cnt, h->S.off, h->S.lr_cnt,
-                                                                    h->S.lr_off);
+        k_img_emit<<<blocks(h->n_host, 256), 256, 0, h->stream>>>(P, h->S, h->n_host, 0, h->n_host, h->S.lr_off);
         // bottom/top images of host particles and left/right images
         const int n_src = h->n_host + n_lr;
-        k_img_count<<<blocks(n_src, 256), 256, 0, h->stream>>>(P, h->S, n_src, 1);
+        k_img_count<<<blocks(n_src, 256), 256, 0, h->stream>>>(P, h->S, n_src, 1, h->S.tb_cnt);
         int n_tb = 0;
-        rc = scan_total(h, h->S.cnt, h->S.off, n_src, &n_tb);
+        rc = scan_total(h, h->S.tb_cnt, h->S.tb_off, n_src, &n_tb);
         if (rc) return rc;
         if (n_src + n_tb > h->cap_tot) return SPH_E_CAPACITY;
-        k_img_emit<<<blocks(n_src, 256), 256, 0, h->stream>>>(P, h->S, n_src, 1, n_src, h->S.off);
-        k_copy_int2<<<blocks(n_src, 256), 256, 0, h->stream>>>(n_src, h->S.cnt, h->S.off, h->S.tb_cnt, h->S.tb_off);
+        k_img_emit<<<blocks(n_src, 256), 256, 0, h->stream>>>(P, h->S, n_src, 1, n_src, h->S.tb_off);
         h->n_lr = n_lr;
         n_img = n_lr + n_tb;
         CK(cudaGetLastError());
     }
     h->n_img = n_img;
-    h->launches += h->cfg.periodic ? 7 : 0;
+    h->launches += h->cfg.periodic ? 5 : 0;
     P.n_tot = h->n_host + n_img;
     tic(h, PH_SORT);
     Sorted<R>& D = sorted<R>(h);
