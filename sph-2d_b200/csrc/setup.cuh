@@ -32,17 +32,16 @@ struct Staging {
     int* tb_off;
 };
 
-// --- 1. periodic wrap (Distribute_Period_Boundary_Particle.f90:56-90) -------
-__global__ void k_wrap(Params P, Staging S) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.n_host || S.type[i] == SPH_TYPE_ILL) return;
-    double2 x = S.pos[i];
-    double Lx = P.box_hi[0] - P.box_lo[0], Ly = P.box_hi[1] - P.box_lo[1];
+// --- 1. periodic wrap (Distribute_Period_Boundary_Particle.f90:56-90), done by
+// the first image count below: a host particle outside the box re-enters on the
+// opposite side before its images are counted.
+__device__ __forceinline__ double2 wrap_position(const Params& P, double2 x) {
+    const double Lx = P.box_hi[0] - P.box_lo[0], Ly = P.box_hi[1] - P.box_lo[1];
     if (x.x > P.box_hi[0]) x.x = x.x - Lx;
     else if (x.x < P.box_lo[0]) x.x = x.x + Lx;
     if (x.y > P.box_hi[1]) x.y = x.y - Ly;
     else if (x.y < P.box_lo[1]) x.y = x.y + Ly;
-    S.pos[i] = x;
+    return x;
 }
 
 // --- 2. images: count per source, then emit at scanned offsets -------------
@@ -50,12 +49,19 @@ __global__ void k_wrap(Params P, Staging S) {
 // axis 1: bottom/top images of host particles and left/right images (:156-206).
 // cnt: the routing counts of this axis (lr_cnt / tb_cnt), scanned in place into
 // the routing offsets (lr_off / tb_off) that k_img_emit reads
+// axis 0 (sources = the host particles) wraps the positions first.
 __global__ void k_img_count(Params P, Staging S, int n_src, int axis, int* cnt) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_src) return;
     int c = 0;
     if (S.type[i] != SPH_TYPE_ILL) {
-        double x = axis == 0 ? S.pos[i].x : S.pos[i].y;
+        double2 xy = S.pos[i];
+        if (axis == 0) {
+            const double2 w = wrap_position(P, xy);
+            if (w.x != xy.x || w.y != xy.y) S.pos[i] = w;
+            xy = w;
+        }
+        double x = axis == 0 ? xy.x : xy.y;
         double lo = P.box_lo[axis], hi = P.box_hi[axis];
         if (x <= (lo + P.band) && x >= lo) c++;
         if (x >= (hi - P.band) && x <= hi) c++;

@@ -357,7 +357,6 @@ int prepare(sph_handle* h) {
     tic(h, PH_IMAGES);
     int n_img = 0;
     if (h->cfg.periodic) {
-        k_wrap<<<blocks(h->n_host, 256), 256, 0, h->stream>>>(P, h->S);
         // left/right images of the host particles; the counts and offsets are
         // kept for routing image adjoints back to their sources
         k_img_count<<<blocks(h->n_host, 256), 256, 0, h->stream>>>(P, h->S, h->n_host, 0, h->S.lr_cnt);
@@ -379,7 +378,7 @@ int prepare(sph_handle* h) {
         CK(cudaGetLastError());
     }
     h->n_img = n_img;
-    h->launches += h->cfg.periodic ? 5 : 0;
+    h->launches += h->cfg.periodic ? 4 : 0;
     P.n_tot = h->n_host + n_img;
     tic(h, PH_SORT);
     Sorted<R>& D = sorted<R>(h);
