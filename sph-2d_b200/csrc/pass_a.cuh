@@ -204,12 +204,14 @@ void launch_pass_a(const Params& P, const Sorted<R>& D, int nb, cudaStream_t st)
 // or |x_j-x_i| < 1.414h and acos(n.(x_j-x_i)/|x_j-x_i|) <= pi/4.
 // Both criteria only accept j within 2h <= support, so the list covers them.
 template <typename R>
+// Grid-stride over the particles: candidates are rare, so most threads only
+// read a flag byte, and a grid of 148 x 8 blocks does that with little block
+// scheduling.
 __global__ void k_surface(Params P, Sorted<R> D) {
     using V4 = typename VT<R>::V4;
-    const int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= P.n_tot) return;
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < P.n_tot; a += gridDim.x * blockDim.x) {
     uint8_t fl = D.flags[a];
-    if (!(fl & 4)) return;
+    if (!(fl & 4)) continue;
     const int nn = D.npairs[a];
     const double2 xa = D.pos[a];
     // sum_dwdx (:155-156) recomputed here (candidates are rare)
@@ -248,20 +250,31 @@ __global__ void k_surface(Params P, Sorted<R> D) {
         }
     }
     D.flags[a] = surface ? (uint8_t)(fl | 1) : (uint8_t)(fl & ~1);
+    }
 }
 
 // Near-free-surface flags (Define_freesurface...f90:418-440): every pair
 // neighbour of a surface particle.  Idempotent byte stores, no atomics needed.
 template <typename R>
 __global__ void k_near(Params P, Sorted<R> D) {
-    const int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= P.n_tot) return;
-    if (!(D.flags[a] & 1)) return;
-    const int nn = D.npairs[a];
-    for (int e = 0; e < nn; ++e) {
-        const int b = (int)(D.pairs[(size_t)e * P.nbr_stride + a] & 0x7fffffffu);
-        D.flags[b] |= 2;
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < P.n_tot; a += gridDim.x * blockDim.x) {
+        if (!(D.flags[a] & 1)) continue;
+        const int nn = D.npairs[a];
+        for (int e = 0; e < nn; ++e) {
+            const int b = (int)(D.pairs[(size_t)e * P.nbr_stride + a] & 0x7fffffffu);
+            D.flags[b] |= 2;
+        }
     }
+}
+
+// The free-surface test and the near-surface flags of one RHS.
+template <typename R>
+void launch_surface(const Params& P, const Sorted<R>& D, cudaStream_t st) {
+    int nb = (P.n_tot + 127) / 128;
+    if (nb > 148 * 8) nb = 148 * 8;
+    if (nb == 0) return;
+    k_surface<R><<<nb, 128, 0, st>>>(P, D);
+    k_near<R><<<nb, 128, 0, st>>>(P, D);
 }
 
 }  // namespace sph

@@ -419,8 +419,7 @@ int rhs(sph_handle* h, int last) {
     tic(h, PH_A);
     launch_pass_a<R, true>(P, D, nb, h->stream);
     tic(h, PH_SURF);
-    k_surface<R><<<nb, 128, 0, h->stream>>>(P, D);
-    k_near<R><<<nb, 128, 0, h->stream>>>(P, D);
+    launch_surface<R>(P, D, h->stream);
     tic(h, PH_C);
     // the mixed Taylor-Green path forms the shifting sum in k_shift_gather after
     // pass C; the FP64 and moving-square launches form it inside pass C
@@ -1065,8 +1064,7 @@ int adj_rhs(sph_handle* h, const Sorted<R>& V, int k, int stage, bool shift = fa
     if (!shift) {
         tic(h, PH_A);
         launch_pass_a<R, false>(P, V, nb, h->stream);
-        k_surface<R><<<nb, 128, 0, h->stream>>>(P, V);
-        k_near<R><<<nb, 128, 0, h->stream>>>(P, V);
+        launch_surface<R>(P, V, h->stream);
         h->launches += 3;
     }
     tic(h, PH_ADJ);
@@ -1115,8 +1113,7 @@ int adj_step(sph_handle* h, bool first, int j) {
         const int nba = blocks(P.n_tot, 128);
         tic(h, PH_A);
         launch_pass_a<R, false>(P, V, nba, h->stream);
-        k_surface<R><<<nba, 128, 0, h->stream>>>(P, V);
-        k_near<R><<<nba, 128, 0, h->stream>>>(P, V);
+        launch_surface<R>(P, V, h->stream);
         tic(h, PH_ADJ);
         k_shift_sum<R><<<nb, 256, 0, h->stream>>>(P, V, A);
         h->launches += 4;
@@ -1173,8 +1170,7 @@ int adj_rhs_ms(sph_handle* h, const Sorted<R>& V, int k, int pred, bool drag, in
         h->launches += 1;
     }
     launch_pass_a<R, false>(P, V, nb, h->stream);
-    k_surface<R><<<nb, 128, 0, h->stream>>>(P, V);
-    k_near<R><<<nb, 128, 0, h->stream>>>(P, V);
+    launch_surface<R>(P, V, h->stream);
     tic(h, PH_ADJ);
     CK(cudaMemsetAsync(V.nflag, 0, (size_t)P.n_tot, h->stream));
     k_adj_c<R, true><<<nbc, kAdjThreads, 0, h->stream>>>(P, V, A, A.lr[k], A.la[k], A.nu_part + (size_t)k * nbc);
