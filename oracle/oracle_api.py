@@ -1,7 +1,8 @@
 """ctypes binding of the CPU oracle (oracle/liboracle.so).
 
 TEST INFRASTRUCTURE: imported only by tests/, __graft_entry__.smoke() and the
-CPU-baseline legs of bench.py, as the checker.  The product path never loads it.
+CPU-baseline legs of bench.py, as the reference results to compare against.  The
+product path never loads it.
 """
 from __future__ import annotations
 

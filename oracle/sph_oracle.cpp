@@ -1,6 +1,6 @@
 // sph_oracle.cpp -- CPU restatement of SPH-2D's weakly-compressible time step.
 //
-// TEST INFRASTRUCTURE ONLY.  This file is the checker that libsph_b200 is
+// TEST INFRASTRUCTURE ONLY.  This file is the oracle that libsph_b200 is
 // compared against; it is never linked into, loaded by or called from the
 // product path.  Only tests/, __graft_entry__.smoke() and the cpu_baseline /
 // --impl reference legs of bench.py may load it.
