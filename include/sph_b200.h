@@ -295,10 +295,15 @@ int sph_reset_timings(sph_handle* h);
  * The search works in a fixed static device array (about 2.4 MiB per GPU that
  * loads the library, held until exit) and calls no cudaMalloc / cudaFree:
  * at most 65536 particles and 65536 background cells of edge kernel_scale*h
- * over grid_lo..grid_hi; larger inputs return SPH_E_CAPACITY.  Calls share that
- * array: GPU work of two calls must not overlap.  The first call on a device
- * resolves the array's address (cudaGetSymbolAddress); make it before any
- * stream capture.  cfg->periodic is ignored (no images are generated). */
+ * over grid_lo..grid_hi; larger inputs return SPH_E_CAPACITY.  At most 256
+ * pairs (i, j > i) per particle: beyond that it returns SPH_E_CAPACITY with
+ * *pair_number = -1.  pair_cap = 0 counts only (SPH_OK); a pair_cap below the
+ * count fills the first pair_cap pairs and returns SPH_E_CAPACITY.  Calls share
+ * that array: GPU work of two calls must not overlap.  The first call on a
+ * device resolves the array's address (cudaGetSymbolAddress) and keeps it for
+ * the life of that device context; make it before any stream capture, and do
+ * not call this entry point on a device after cudaDeviceReset.
+ * cfg->periodic is ignored (no images are generated). */
 int sph_find_particle_pair_noalloc(const sph_config* cfg, int n, const double* d_pos, const int* d_type,
                                    long long pair_cap, int* d_pair_i, int* d_pair_j, double* d_w,
                                    double* d_dwdx, long long* pair_number, void* stream);

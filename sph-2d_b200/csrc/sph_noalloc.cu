@@ -18,10 +18,16 @@
 // call clears what must start at zero.  Two calls whose GPU work overlaps
 // (different host threads, or different streams without ordering between them)
 // race on the array and give wrong results: serialise them.
+// At most kMaxPairsPerParticle pairs (i, j > i) per particle: beyond that the
+// call returns SPH_E_CAPACITY with *pair_number = -1 (a larger pair_cap does
+// not help).
 // The first call on a device resolves the array's device address with
 // cudaGetSymbolAddress (the host-side symbol is only a stand-in, not a device
 // address) and caches it per device; make that first call before any stream
-// capture.
+// capture.  The cached address belongs to the device context of that first
+// call: after cudaDeviceReset the module is loaded again and the cache is
+// stale, so a process that resets a device must not call this entry point on
+// it afterwards.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -41,6 +47,7 @@ constexpr int kMaxParticles = 65536;
 constexpr int kMaxCells = 65536;
 constexpr int kScanThreads = 1024;
 constexpr int kMaxDevices = 64;
+constexpr int kMaxPairsPerParticle = 256;   // pairs (i, j > i) one thread sorts by j
 
 // scratch layout (byte offsets)
 constexpr size_t kOffCellOf = 0;                                               // int[kMaxParticles]
@@ -180,7 +187,7 @@ __global__ void na_pairs(Params P, int n, const double* pos, const int* type, Sc
     const int cx = c % P.gnx, cy = c / P.gnx;
     const double xi = pos[i], yi = pos[n + i];
     const int ti = type[i];
-    int js[256];
+    int js[kMaxPairsPerParticle];
     int m = 0;
     long long cnt = 0;
     for (int gy = max(cy - 1, 0); gy <= min(cy + 1, P.gny - 1); ++gy) {
@@ -193,7 +200,7 @@ __global__ void na_pairs(Params P, int n, const double* pos, const int* type, Sc
                 double d;
                 if (!in_support(P, xi - pos[j], yi - pos[n + j], d)) continue;
                 ++cnt;
-                if (EMIT && m < 256) {
+                if (EMIT && m < kMaxPairsPerParticle) {
                     int q = m++;
                     while (q > 0 && js[q - 1] > j) { js[q] = js[q - 1]; --q; }
                     js[q] = j;
@@ -203,7 +210,7 @@ __global__ void na_pairs(Params P, int n, const double* pos, const int* type, Sc
     }
     if (!EMIT) {
         s.pair_count[i] = cnt;
-        if (cnt > 256) atomicOr((unsigned long long*)&s.totals[1], (unsigned long long)ST_PAIR_OVERFLOW);
+        if (cnt > kMaxPairsPerParticle) atomicOr((unsigned long long*)&s.totals[1], (unsigned long long)ST_PAIR_OVERFLOW);
         return;
     }
     long long o = s.pair_off[i];
@@ -262,16 +269,23 @@ extern "C" int sph_find_particle_pair_noalloc(const sph_config* cfg, int n, cons
     na_scatter<<<nb, 128, 0, st>>>(n, s);
     na_pairs<false><<<nb, 128, 0, st>>>(P, n, d_pos, d_type, s, 0, nullptr, nullptr, nullptr, nullptr);
     na_scan_pairs<<<1, kScanThreads, 0, st>>>(n, s);
+    // a rejected launch (an invalid stream, say) must not let the copy below
+    // return the totals an earlier call left in the array
+    if (cudaGetLastError() != cudaSuccess) return SPH_E_CUDA;
     long long totals[2] = {0, 0};
     if (cudaMemcpyAsync(totals, s.totals, sizeof(totals), cudaMemcpyDeviceToHost, st) != cudaSuccess) return SPH_E_CUDA;
     if (cudaStreamSynchronize(st) != cudaSuccess) return SPH_E_CUDA;
     *pair_number = totals[0];
     if (totals[1] & ST_DOMAIN) return SPH_E_DOMAIN;
-    if (totals[1] & ST_PAIR_OVERFLOW) return SPH_E_CAPACITY;
-    if (pair_cap > 0) {
-        na_pairs<true><<<nb, 128, 0, st>>>(P, n, d_pos, d_type, s, pair_cap, d_pair_i, d_pair_j, d_w, d_dwdx);
-        if (cudaGetLastError() != cudaSuccess) return SPH_E_CUDA;
-        if (cudaStreamSynchronize(st) != cudaSuccess) return SPH_E_CUDA;
+    if (totals[1] & ST_PAIR_OVERFLOW) {
+        // more than kMaxPairsPerParticle pairs (i, j > i) for one particle: no
+        // pair_cap helps, so the count is reported as -1
+        *pair_number = -1;
+        return SPH_E_CAPACITY;
     }
+    if (pair_cap <= 0) return SPH_OK;       // count only, as sph_find_particle_pair
+    na_pairs<true><<<nb, 128, 0, st>>>(P, n, d_pos, d_type, s, pair_cap, d_pair_i, d_pair_j, d_w, d_dwdx);
+    if (cudaGetLastError() != cudaSuccess) return SPH_E_CUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return SPH_E_CUDA;
     return totals[0] > pair_cap ? SPH_E_CAPACITY : SPH_OK;
 }
