@@ -63,6 +63,9 @@ def load():
                                    ctypes.c_double, ctypes.c_int, dp, dp, dp, dp, dp]
     lib.oracle_tangent_ms.argtypes = [cp, ctypes.c_int, dp, dp, dp, dp, ip, ip, ip, ctypes.c_double, ctypes.c_int,
                                       ctypes.c_double, dp, ctypes.c_int, dp, dp, dp, dp, ctypes.c_double, dp, dp]
+    lib.oracle_set_muscl_gradient_scale.argtypes = [ctypes.c_double]
+    lib.oracle_muscl_limiter.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double, dp, dp]
+    lib.oracle_hllc_state.argtypes = [cp, dp, dp]
     _lib = lib
     return lib
 
@@ -250,3 +253,26 @@ def set_ghost_state(labels, body_vel=(0.0, 0.0), body_acc=(0.0, 0.0), t: float =
     bv = np.ascontiguousarray(body_vel, np.float64)
     ba = np.ascontiguousarray(body_acc, np.float64)
     load().oracle_set_ghost_state(lb.shape[0], _p(lb, ctypes.c_int), _p(bv), _p(ba), float(t))
+
+
+def set_muscl_gradient_scale(scale: float):
+    """Factor on the MUSCL reconstruction gradients (grad p, grad u, grad v) of
+    the following oracle RHS evaluations; 1 is the solver as written."""
+    load().oracle_set_muscl_gradient_scale(float(scale))
+
+
+def muscl_limiter(di: float, dj: float, dij: float):
+    li = ctypes.c_double(0.0); lj = ctypes.c_double(0.0)
+    load().oracle_muscl_limiter(float(di), float(dj), float(dij), ctypes.byref(li), ctypes.byref(lj))
+    return li.value, lj.value
+
+
+def hllc_state(cfg: SphConfig, vi, vj, e, rho_i, rho_j, c_i, c_j, p_i, p_j):
+    """The oracle's HLLC pair state (v*, P*) for one pair; e is the unit vector
+    from particle i to particle j."""
+    inp = np.array([vi[0], vi[1], vj[0], vj[1], e[0], e[1], rho_i, rho_j, c_i, c_j, p_i, p_j], np.float64)
+    out = np.zeros(3)
+    rc = load().oracle_hllc_state(ctypes.byref(cfg), _p(inp), _p(out))
+    if rc != 0:
+        raise RuntimeError("oracle_hllc_state failed")
+    return out[:2].copy(), float(out[2])

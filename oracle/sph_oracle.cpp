@@ -65,6 +65,10 @@ struct Consts {
 
 Consts g_K;
 sph_config g_cfg;
+// Test hook (oracle_set_muscl_gradient_scale): factor on the MUSCL reconstruction
+// gradients grad p, grad u, grad v; 1 everywhere except in the pin tests, where 0
+// turns the MUSCL solver's Riemann states into the unreconstructed ones.
+double g_muscl_grad_scale = 1.0;
 
 inline double pw3(double x) { return x * x * x; }
 inline double pw4(double x) { double x2 = x * x; return x2 * x2; }
@@ -734,6 +738,42 @@ void riemann_solver(const Particles& P, Rhs& R, bool muscl, bool dsph) {
     }
 }
 
+// The HLLC pair state of Moving_Square.../Solver_Normalized_HLLC_Riemann_Delta.f90:207-322:
+// velocities rotated into the pair frame (normal e = (x_j - x_i)/|x_j - x_i|),
+// acoustic star velocity and pressure (:225-228), rho* from the linear equation of
+// state (:230), wave speeds with the shock factor guarded by rho_K > rho* (:239-278),
+// the state sampled at x/t = the mean normal velocity (:281-317), then rotated back,
+// P* = c0^2 (rho_HLLC - rho0) + p_b (:321-322).
+void hllc_state(const double vI[2], const double vJ[2], const double vbar[2], const double e[2], double rL,
+                double rR, double cL, double cR, double PL, double PR, double vs[2], double& Ps) {
+    const sph_config& C = g_cfg;
+    const double T[2][2] = {{e[0], e[1]}, {-e[1], e[0]}};
+    const double VL[2] = {T[0][0] * vI[0] + T[0][1] * vI[1], T[1][0] * vI[0] + T[1][1] * vI[1]};
+    const double VR[2] = {T[0][0] * vJ[0] + T[0][1] * vJ[1], T[1][0] * vJ[0] + T[1][1] * vJ[1]};
+    const double V0 = T[0][0] * vbar[0] + T[0][1] * vbar[1];
+    const double Us = (VR[0] * cL * rL + VL[0] * cR * rR + PL - PR) / (rL * cL + rR * cR);
+    double Pst = (PR * cL * rL + PL * cR * rR - cL * rL * cR * rR * (VR[0] - VL[0])) / (rL * cL + rR * cR);
+    const double rst = (Pst - C.background_p) / C.c0sq + C.rho0;
+    double QL = 1.0, QR = 1.0;
+    if (!(Pst <= PL) && rL > rst) QL = std::sqrt((rst / rL) * (Pst - PL) / (rL - rst)) / cL;
+    const double SL = VL[0] - cL * QL;
+    if (!(Pst <= PR) && rR > rst) QR = std::sqrt((rst / rR) * (Pst - PR) / (rR - rst)) / cR;
+    const double SR = VR[0] + cR * QR;
+    const double Sst = Us, xt = V0;
+    double rH, VH[2];
+    if (SL > xt) { rH = rL; VH[0] = VL[0]; VH[1] = VL[1]; }
+    else if (Sst >= xt && xt >= SL) {
+        double q = rL * ((SL - VL[0]) / (SL - Sst));
+        rH = q; VH[0] = (Sst * q) / rH; VH[1] = (VL[1] * q) / rH;
+    } else if (SR >= xt && xt >= Sst) {
+        double q = rR * ((SR - VR[0]) / (SR - Sst));
+        rH = q; VH[0] = (Sst * q) / rH; VH[1] = (VR[1] * q) / rH;
+    } else { rH = rR; VH[0] = VR[0]; VH[1] = VR[1]; }
+    vs[0] = T[0][0] * VH[0] + T[1][0] * VH[1];
+    vs[1] = T[0][1] * VH[0] + T[1][1] * VH[1];
+    Ps = C.c0sq * (rH - C.rho0) + C.background_p;
+}
+
 // The moving-square solvers: Moving_Square.../Solver_Normalized_Modified_Linear_Riemann_Delta.f90
 // and Solver_Normalized_HLLC_Riemann_Delta.f90 (no SPS; XSPH average velocity
 // computed first and added to the continuity flux; laplacianTerm switch), with
@@ -787,33 +827,7 @@ void ms_riemann_solver(const Particles& P, Rhs& R, bool hllc) {
             double bR = std::min(3.0 * (std::max((UL - UR), 0.0)), cbar);
             Ps = Pbar + 0.5 * bR * rbar * (UL - UR);
         } else {
-            // Solver_Normalized_HLLC_Riemann_Delta.f90:207-322
-            const double T[2][2] = {{e[0], e[1]}, {-e[1], e[0]}};
-            const double VL[2] = {T[0][0] * vI[0] + T[0][1] * vI[1], T[1][0] * vI[0] + T[1][1] * vI[1]};
-            const double VR[2] = {T[0][0] * vJ[0] + T[0][1] * vJ[1], T[1][0] * vJ[0] + T[1][1] * vJ[1]};
-            const double V0 = T[0][0] * vbar[0] + T[0][1] * vbar[1];
-            const double rL = ri, rR = rj, cL = R.c[i], cR = R.c[j];
-            const double Us = (VR[0] * cL * rL + VL[0] * cR * rR + PL - PR) / (rL * cL + rR * cR);
-            double Pst = (PR * cL * rL + PL * cR * rR - cL * rL * cR * rR * (VR[0] - VL[0])) / (rL * cL + rR * cR);
-            const double rst = (Pst - C.background_p) / C.c0sq + C.rho0;
-            double QL = 1.0, QR = 1.0;
-            if (!(Pst <= PL) && rL > rst) QL = std::sqrt((rst / rL) * (Pst - PL) / (rL - rst)) / cL;
-            const double SL = VL[0] - cL * QL;
-            if (!(Pst <= PR) && rR > rst) QR = std::sqrt((rst / rR) * (Pst - PR) / (rR - rst)) / cR;
-            const double SR = VR[0] + cR * QR;
-            const double Sst = Us, xt = V0;
-            double rH, VH[2];
-            if (SL > xt) { rH = rL; VH[0] = VL[0]; VH[1] = VL[1]; }
-            else if (Sst >= xt && xt >= SL) {
-                double q = rL * ((SL - VL[0]) / (SL - Sst));
-                rH = q; VH[0] = (Sst * q) / rH; VH[1] = (VL[1] * q) / rH;
-            } else if (SR >= xt && xt >= Sst) {
-                double q = rR * ((SR - VR[0]) / (SR - Sst));
-                rH = q; VH[0] = (Sst * q) / rH; VH[1] = (VR[1] * q) / rH;
-            } else { rH = rR; VH[0] = VR[0]; VH[1] = VR[1]; }
-            vs[0] = T[0][0] * VH[0] + T[1][0] * VH[1];
-            vs[1] = T[0][1] * VH[0] + T[1][1] * VH[1];
-            Ps = C.c0sq * (rH - C.rho0) + C.background_p;
+            hllc_state(vI, vJ, vbar, e, ri, rj, R.c[i], R.c[j], PL, PR, vs, Ps);
         }
         double vIs[2], vJs[2], IPs, JPs;
         if (R.near[i] == 1) { vIs[0] = vbar[0]; vIs[1] = vbar[1]; IPs = Pbar; }
@@ -1056,7 +1070,16 @@ void single_step_compute(Particles& P, Rhs& R) {
         return;
     }
     const bool muscl = g_cfg.solver == SPH_SOLVER_MUSCL_DELTA_SPS;
-    if (muscl) gradients(P, R, true);
+    if (muscl) {
+        gradients(P, R, true);
+        if (g_muscl_grad_scale != 1.0)       // test hook: scale the reconstruction gradients
+            for (int c = 0; c < 2; ++c)
+                for (int i = 0; i < n; ++i) {
+                    R.gp[c][i] *= g_muscl_grad_scale;
+                    R.gu[c][i] *= g_muscl_grad_scale;
+                    R.gv[c][i] *= g_muscl_grad_scale;
+                }
+    }
     sps_stress(P, R);
     riemann_solver(P, R, muscl, g_cfg.solver == SPH_SOLVER_DELTA_SPS);
 }
@@ -1479,6 +1502,28 @@ void oracle_set_ghost_state(int n, const int* labels, const double* bvel, const 
     for (int k = 0; k < 2; ++k) { g_bvel[k] = bvel ? bvel[k] : 0.0; g_bacc[k] = bacc ? bacc[k] : 0.0; }
     g_time = t;
     g_n_host = n;
+}
+
+// Test hooks for the pins of the MUSCL and HLLC paths (tests/test_oracle_pins.py).
+void oracle_set_muscl_gradient_scale(double s) { g_muscl_grad_scale = s; }
+
+void oracle_muscl_limiter(double di, double dj, double dij, double* li, double* lj) {
+    muscl_limiter(di, dj, dij, *li, *lj);
+}
+
+// The HLLC pair state for one pair: in[0..1] v_i, in[2..3] v_j, in[4..5] the unit
+// vector from i to j, in[6..11] rho_i, rho_j, c_i, c_j, p_i, p_j; out[0..1] v*, out[2] P*.
+// The configuration supplies c0^2, rho0 and the background pressure.
+int oracle_hllc_state(const sph_config* cfg, const double* in, double* out) {
+    if (!cfg || !in || !out) return -1;
+    g_cfg = *cfg;
+    derive_consts(*cfg);
+    const double vI[2] = {in[0], in[1]}, vJ[2] = {in[2], in[3]}, e[2] = {in[4], in[5]};
+    const double vbar[2] = {(vI[0] + vJ[0]) / 2.0, (vI[1] + vJ[1]) / 2.0};
+    double vs[2], Ps;
+    hllc_state(vI, vJ, vbar, e, in[6], in[7], in[8], in[9], in[10], in[11], vs, Ps);
+    out[0] = vs[0]; out[1] = vs[1]; out[2] = Ps;
+    return 0;
 }
 
 int oracle_threads(int nthreads) {
