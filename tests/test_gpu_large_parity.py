@@ -1,0 +1,120 @@
+"""Parity at the sizes of the benchmark cases.
+
+* The pair check of the 1024^2 / 2048^2 Taylor-Green case: positions jittered by
+  a seeded uniform +/-0.1 dx, the sorted pair set (periodic images included)
+  bit-exact against the oracle's find_particle_pair
+  (Taylor_Green_Vortex/find_particle_pair.f90:64-123), seeds 1-3.
+* One FP64 right-hand side of the benchmark solver (MUSCL linear Riemann +
+  delta-SPH + SPS, Wendland C2) at 1024^2 on the jittered lattice, <= 1e-10.
+* One FP64 right-hand side of the HLLC solver on the moving square at D/100
+  (D = 1 in a [0,10] x [0,5] tank, 4 ghost layers), <= 1e-10
+  (Moving_Square.../Solver_Normalized_HLLC_Riemann_Delta.f90).
+* The moving square at D/100 for 200 Euler predictor-corrector steps in mixed
+  precision against FP64, at Re = 50, 100 and 150 (nu = U D / Re,
+  Moving_Square.../Information_Module.f90:44): velocity L2 <= 1e-5.
+"""
+import numpy as np
+import pytest
+
+import sph_b200 as S
+
+pytestmark = pytest.mark.gpu
+
+
+def relerr(a, b):
+    den = np.abs(b).max()
+    return np.abs(a - b).max() / (den if den > 0 else 1.0)
+
+
+def sorted_keys(pi, pj):
+    return np.sort(pi.astype(np.int64) * (1 << 31) + pj.astype(np.int64))
+
+
+@pytest.mark.parametrize("n_side", [1024, 2048])
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_pair_set_bit_exact_benchmark_size(lib, oracle, n_side, seed):
+    case = S.make_tgv(n_side, jitter=0.1, seed=seed)
+    ext = oracle.periodic_images(case.cfg, case.pos, case.vel, case.rho, case.mass, case.type)
+    cap = 12 * ext[2].size
+    ref = oracle.find_particle_pair(case.cfg, ext[0], ext[4], pair_cap=cap)
+    kr = sorted_keys(ref["pair_i"], ref["pair_j"])
+    ref = None
+    with S.Simulation(case.cfg, case.n) as sim:
+        sim.set_state(case.pos, case.vel, case.rho, case.mass, case.type)
+        got = sim.find_particle_pair(cap, want_kernel=False)
+    assert got["pair_number"] == kr.size
+    kg = sorted_keys(got["pair_i"], got["pair_j"])
+    assert np.array_equal(kg, kr)
+    # about ten pairs per particle at h = 1.3 dx, support 2h
+    assert 9.5 * case.n < kr.size < 10.5 * case.n
+
+
+def test_rhs_fp64_parity_benchmark_size(lib, oracle):
+    case = S.make_tgv(1024, solver=S.SOLVER_MUSCL_DELTA_SPS, jitter=0.1, seed=1)
+    ext = oracle.periodic_images(case.cfg, case.pos, case.vel, case.rho, case.mass, case.type)[:5]
+    ref = oracle.rhs(case.cfg, *ext)
+    n, m = case.n, ext[2].size
+    with S.Simulation(case.cfg, case.n) as sim:
+        sim.set_state(case.pos, case.vel, case.rho, case.mass, case.type)
+        got = sim.single_step_compute()
+        grads = sim.field(S.FIELD_GRADS)
+    assert relerr(got["drhodt"], ref["drhodt"][:n]) < 1e-10
+    assert relerr(got["acc"], np.concatenate([ref["acc"][:n], ref["acc"][m:m + n]])) < 1e-10
+    assert np.array_equal(got["fs"], ref["fs"][:n])
+    for f in range(4):
+        want = np.concatenate([ref["grads"][2 * f * m:2 * f * m + n],
+                               ref["grads"][(2 * f + 1) * m:(2 * f + 1) * m + n]])
+        assert relerr(grads[2 * f * n:(2 * f + 2) * n], want) < 1e-10, f
+
+
+def _ms_d100(solver, precision=S.PREC_FP64, re=100.0, jitter=0.0, seed=0):
+    case, ity = S.make_moving_square(dx=0.01, lx=10.0, ly=5.0, D=1.0, U=1.0, solver=solver, precision=precision,
+                                     jitter=jitter, seed=seed)
+    case.cfg.nu = 1.0 * 1.0 / re
+    return case, ity
+
+
+def test_hllc_rhs_parity_moving_square_d100(lib, oracle):
+    case, ity = _ms_d100(S.SOLVER_MS_HLLC_DELTA, jitter=0.1, seed=2)
+    # a seeded velocity field in the water so that the pair states cover
+    # compressions and expansions everywhere, not only at the body
+    rng = np.random.default_rng(5)
+    water = case.type == S.TYPE_WATER
+    vel = case.vel.copy()
+    vel[:case.n][water] += rng.uniform(-0.05, 0.05, water.sum())
+    vel[case.n:][water] += rng.uniform(-0.05, 0.05, water.sum())
+    assert case.n > 500_000
+    ref = oracle.rhs(case.cfg, case.pos, vel, case.rho, case.mass, case.type)
+    bf_ref = oracle.rhs_body_force(case.cfg, case.pos, vel, case.rho, case.mass, case.type, ity)
+    with S.Simulation(case.cfg, case.n) as sim:
+        sim.set_state(case.pos, vel, case.rho, case.mass, case.type)
+        sim.set_initial_type(ity)
+        got = sim.single_step_compute()
+        bf = np.array(sim.diagnostics().body_force[:])
+    assert relerr(got["drhodt"], ref["drhodt"]) < 1e-10
+    assert relerr(got["acc"], ref["acc"]) < 1e-10
+    assert relerr(got["avg_vel"], ref["avg_vel"]) < 1e-10
+    assert np.abs(bf - bf_ref).max() <= 1e-10 * np.abs(bf_ref).max()
+
+
+@pytest.mark.parametrize("re", [50.0, 100.0, 150.0])
+def test_moving_square_mixed_vs_fp64(lib, re):
+    """D/100, HLLC + delta-SPH, ghost assignment with the body at U = 1, shifting,
+    MLS every 40 steps, 200 steps: the mixed-precision velocity against the FP64
+    run's."""
+    res = {}
+    for prec in (S.PREC_FP64, S.PREC_MIXED):
+        case, ity = _ms_d100(S.SOLVER_MS_HLLC_DELTA, precision=prec, re=re)
+        case.cfg.ghost_assign = 1
+        dt = 0.25 * case.cfg.h / np.sqrt(case.cfg.c0sq)
+        with S.Simulation(case.cfg, case.n) as sim:
+            sim.set_state(case.pos, case.vel, case.rho, case.mass, case.type)
+            sim.set_initial_type(ity)
+            sim.set_boundary_labels(S.moving_square_labels(case, ity))
+            sim.set_body_motion((1.0, 0.0))
+            sim.time_iteration(200, dt)
+            res[prec] = sim.get_state()[1]
+    water = np.concatenate([case.type == S.TYPE_WATER] * 2)
+    v64, v32 = res[S.PREC_FP64][water], res[S.PREC_MIXED][water]
+    l2 = np.linalg.norm(v32 - v64) / np.linalg.norm(v64)
+    assert l2 <= 1e-5, l2
