@@ -85,7 +85,7 @@ struct sph_handle {
     int* d_int = nullptr;           // small int scratch
     double* d_part = nullptr;       // reduction partials
     double* d_diag = nullptr;
-    double* d_xfer = nullptr;       // column-major transfer scratch [cap_host * 4]
+    double* d_xfer = nullptr;       // column-major transfer scratch [cap_host * 6]
     double* d_export = nullptr;     // k_export output (lazy)
     long long* d_off64 = nullptr;   // pair offsets (lazy)
     int* d_cnt_id = nullptr;
@@ -1400,7 +1400,7 @@ int init_impl(const sph_config* cfg, int n_capacity, sph_handle** out) {
     CK(dalloc(&h->d_status, 1)); CK(cudaMemset(h->d_status, 0, sizeof(unsigned)));
     CK(dalloc(&h->d_int, 4));
     CK(dalloc(&h->d_part, 2 * 148 * 4)); CK(dalloc(&h->d_diag, 2));
-    CK(dalloc(&h->d_xfer, (size_t)4 * h->cap_host));
+    CK(dalloc(&h->d_xfer, (size_t)6 * h->cap_host));
     if (cfg->mls_order) CK(dalloc(&h->d_mls, cap));
     if (h->mixed) rc = alloc_sorted(h->D32, cap, h->P.max_nbr, h->ncells);
     else rc = alloc_sorted(h->D64, cap, h->P.max_nbr, h->ncells);
@@ -1413,33 +1413,18 @@ template <typename R>
 int get_state_impl(sph_handle* h, int n, double* pos, double* vel, double* rho, double* press) {
     int rc = unsort<R>(h);
     if (rc) return rc;
-    if (pos) {
-        k_deinterleave<<<blocks(n, 256), 256, 0, h->stream>>>(n, h->S.pos, h->d_xfer);
-        h->launches += 1;
-        CK(cudaMemcpyAsync(pos, h->d_xfer, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, h->stream));
-        CK(cudaStreamSynchronize(h->stream));
-    }
-    if (vel) {
-        k_deinterleave<<<blocks(n, 256), 256, 0, h->stream>>>(n, h->S.vel, h->d_xfer);
-        h->launches += 1;
-        CK(cudaMemcpyAsync(vel, h->d_xfer, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, h->stream));
-        CK(cudaStreamSynchronize(h->stream));
-    }
-    if (rho || press) {
-        std::vector<double> tmp;
-        double* r = rho;
-        if (!r) { tmp.resize(n); r = tmp.data(); }
-        CK(cudaMemcpyAsync(r, h->S.rho, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
-        CK(cudaStreamSynchronize(h->stream));
-        if (press) {
-            const Params& P = h->P;
-            for (int i = 0; i < n; ++i) {
-                double x = r[i] / P.rho0;
-                double x2 = x * x, x4 = x2 * x2;
-                press[i] = P.eos == SPH_EOS_TAIT ? P.eos_b * (x4 * x2 * x - 1.0) + P.pb : P.c0sq * (r[i] - P.rho0) + P.pb;
-            }
-        }
-    }
+    // one pass packs x, v (column-major), rho and the pressure (status_equation
+    // on the device) into the transfer buffer; the requested blocks are then
+    // copied back with a single wait at the end
+    k_snapshot<<<blocks(n, 256), 256, 0, h->stream>>>(h->P, n, h->S.pos, h->S.vel, h->S.rho, h->d_xfer);
+    CK(cudaGetLastError());
+    h->launches += 1;
+    const size_t nn = (size_t)n;
+    if (pos) CK(cudaMemcpyAsync(pos, h->d_xfer, sizeof(double) * 2 * nn, cudaMemcpyDeviceToHost, h->stream));
+    if (vel) CK(cudaMemcpyAsync(vel, h->d_xfer + 2 * nn, sizeof(double) * 2 * nn, cudaMemcpyDeviceToHost, h->stream));
+    if (rho) CK(cudaMemcpyAsync(rho, h->d_xfer + 4 * nn, sizeof(double) * nn, cudaMemcpyDeviceToHost, h->stream));
+    if (press) CK(cudaMemcpyAsync(press, h->d_xfer + 5 * nn, sizeof(double) * nn, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
     return SPH_OK;
 }
 
@@ -1527,6 +1512,9 @@ int sph_update_state(sph_handle* h, int n, const double* pos, const double* vel,
     k_interleave<<<blocks(n, 256), 256, 0, h->stream>>>(n, h->d_xfer + 2 * (size_t)n, h->S.vel);
     CK(cudaMemcpyAsync(h->S.rho, rho, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
     CK(cudaGetLastError());
+    // the copies from page-locked buffers run asynchronously: finish them before
+    // returning, since the caller owns (and may refill) its arrays afterwards
+    CK(cudaStreamSynchronize(h->stream));
     h->launches += 2;
     h->staging_valid = true;
     h->sorted_valid = false;
