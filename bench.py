@@ -4,7 +4,11 @@ Workload: the 2048 x 2048 Taylor-Green vortex (4,194,304 particles), MUSCL
 linear-Riemann + delta-SPH + SPS solver, Wendland C2 (h = 1.3 dx), true 2x2
 renormalisation, periodic images, RK4 with K1 reuse (3 RHS per step after the
 first), particle shifting.  A "step" is one time step of that integrator over
-all particles.  Synthetic data: the analytic Taylor-Green initial field.
+all particles.  Synthetic data: the analytic Taylor-Green initial field on the
+lattice jittered by a seeded uniform +/-0.1 dx (seed 1) -- the state on which
+the mixed path meets the 1e-5 velocity bound; on the exact lattice the MUSCL
+limiter sits on ties that round-off decides, and that lattice is timed as a
+side report (lattice_exact).
 
 Headline value: particle-steps/s of the mixed-precision step (FP32 pair
 arithmetic, compensated sums, FP64 state), inputs resident on the device,
@@ -25,7 +29,8 @@ Multi-GPU: the path does not shard (one GPU holds all particles), so
 path); value = particles x steps of all ranks / max-over-ranks time.
 
 --impl reference: the CPU restatement of the reference (oracle/, OpenMP over
-particles) on the host cores, on a bounded sample of the same workload.
+particles) on the host cores, on bounded samples of the same workload (512^2
+and 256^2 of the same jittered case, --steps steps each) and a serial leg.
 """
 from __future__ import annotations
 
@@ -48,8 +53,20 @@ sys.path.insert(0, os.path.join(ROOT, "sph-2d_b200"))
 METRIC = "particle-steps/s at 4.2M TGV: mixed vs FP64 GPU at <=1e-5 L2; adjoint/fwd cost"
 UNIT = "particle-steps/s"
 N_SIDE = 2048
-WORKLOAD = ("Taylor-Green vortex 2048x2048 (4,194,304 particles), MUSCL linear-Riemann + delta-SPH + SPS, "
-            "Wendland C2 h=1.3dx, rho0=1, c0=10, Re=100, RK4 with K1 reuse (3 RHS/step), shifting, periodic images")
+JITTER, JITTER_SEED = 0.1, 1
+WORKLOAD = ("Taylor-Green vortex 2048x2048 (4,194,304 particles) on the lattice jittered +-0.1dx (seed 1), "
+            "MUSCL linear-Riemann + delta-SPH + SPS, Wendland C2 h=1.3dx, rho0=1, c0=10, Re=100, "
+            "RK4 with K1 reuse (3 RHS/step), shifting, periodic images")
+
+
+def bench_config(n_side: int, world: int) -> dict:
+    """The `config` object of both arms (the native step and the CPU reference)."""
+    import sph_b200 as S
+    cfg = S.tgv_baseline_config(n_side, S.SOLVER_MUSCL_DELTA_SPS, S.PREC_MIXED)
+    return {"workload": WORKLOAD, "particles": n_side * n_side, "rhs_per_step": 3, "dt": S.baseline_dt(cfg),
+            "lattice": f"jittered +-{JITTER}dx, seed {JITTER_SEED}",
+            "l2": "state (~1.4 GB) larger than L2 (126 MB), no flush needed",
+            "parallelism": f"replicas x{world}"}
 
 
 def parse():
@@ -188,7 +205,7 @@ def run_native(args, rank, world, local):
     results = {}
     clocks_info = None
     for prec in (S.PREC_MIXED, S.PREC_FP64):
-        case = S.make_tgv(n_side, solver=S.SOLVER_MUSCL_DELTA_SPS, precision=prec)
+        case = S.make_tgv(n_side, solver=S.SOLVER_MUSCL_DELTA_SPS, precision=prec, jitter=JITTER, seed=JITTER_SEED)
         dt = S.baseline_dt(case.cfg)
         sim = S.Simulation(case.cfg, case.n)
         sim.set_state(case.pos, case.vel, case.rho, case.mass, case.type)
@@ -209,7 +226,9 @@ def run_native(args, rank, world, local):
         if clk:
             clocks_info = clk.stop()
         dev_ms = max_over_ranks(tm.total_ms)
-        results[prec] = dict(sim=sim, case=case, dt=dt, dev_ms=dev_ms, wall_s=wall, tm=tm, diag=diag)
+        # the velocity of the state that was timed (warm-up + timed steps)
+        vel_end = sim.get_state()[1] if rank == 0 else None
+        results[prec] = dict(sim=sim, case=case, dt=dt, dev_ms=dev_ms, wall_s=wall, tm=tm, diag=diag, vel=vel_end)
         if prec == S.PREC_FP64:
             sim.close()
 
@@ -251,24 +270,30 @@ def run_native(args, rank, world, local):
     if rank == 0 and not args.skip_accuracy:
         streaming = streaming_report(S, sim, n, mixed["dt"])
 
-    # ---- accuracy: mixed vs FP64 on the jittered lattice ----------------------
+    # ---- accuracy: mixed vs FP64 on the timed state -----------------------------
     accuracy = None
+    if rank == 0:
+        vm, vd = mixed["vel"], fp64["vel"]
+        accuracy = {"timed_state": {
+            "velocity_l2_mixed_vs_fp64": float(np.linalg.norm(vm - vd) / np.linalg.norm(vd)),
+            "steps": args.warmup + steps,
+            "case": "the timed runs themselves: the same jittered initial state, warm-up + timed steps"}}
     if not args.skip_accuracy and rank == 0:
-        # the benchmark's own size, on a jittered lattice: on the exact lattice the
-        # MUSCL limiter sits on ties that round-off decides, and FP64 runs one ulp
-        # apart already differ by 2.5e-4 after 100 steps
-        acc_side = n_side
+        # the same initial state over 100 steps (the horizon of the 1e-5 bound);
+        # on the exact lattice the MUSCL limiter sits on ties that round-off
+        # decides, and FP64 runs one ulp apart already differ by 2.5e-4 there
         acc_steps = 100
         v = {}
         for prec in (S.PREC_FP64, S.PREC_MIXED):
-            c = S.make_tgv(acc_side, solver=S.SOLVER_MUSCL_DELTA_SPS, precision=prec, jitter=0.1, seed=1)
+            c = S.make_tgv(n_side, solver=S.SOLVER_MUSCL_DELTA_SPS, precision=prec, jitter=JITTER, seed=JITTER_SEED)
             with S.Simulation(c.cfg, c.n) as s2:
                 s2.set_state(c.pos, c.vel, c.rho, c.mass, c.type)
                 s2.time_iteration(acc_steps, S.baseline_dt(c.cfg))
                 v[prec] = s2.get_state()[1]
         l2 = float(np.linalg.norm(v[S.PREC_MIXED] - v[S.PREC_FP64]) / np.linalg.norm(v[S.PREC_FP64]))
-        accuracy = {"velocity_l2_mixed_vs_fp64": l2, "steps": acc_steps,
-                    "case": f"TGV {acc_side}x{acc_side}, lattice jittered +-0.1dx (seed 1), same solver"}
+        accuracy.update({"velocity_l2_mixed_vs_fp64": l2, "steps": acc_steps,
+                         "case": f"TGV {n_side}x{n_side}, the timed initial state (lattice jittered "
+                                 f"+-{JITTER}dx, seed {JITTER_SEED}), same solver"})
 
     # ---- roofline of the dominant kernel (pass C) ----------------------------
     pk, pk_kind = peaks()
@@ -297,15 +322,16 @@ def run_native(args, rank, world, local):
     if rank == 0 and not args.skip_adjoint:
         adj = adjoint_report(S)
         adj_ms = adjoint_ms_report(S)
-    ms = plain = None
+    ms = plain = exact = None
     if rank == 0 and not args.skip_accuracy:
+        exact = exact_lattice_report(S, n_side)
         ms = moving_square_report(S)
         plain = plain_method_report(S)
 
     # ---- CPU baseline (rank 0 only, N = 1) ----------------------------------
     cpu = None
     if rank == 0 and world == 1:
-        cpu = cpu_reference(steps=2, warmup=1)
+        cpu = cpu_reference(steps=steps, warmup=1, sides=(256,), serial=True)
 
     mixed["sim"].close()
     if rank != 0:
@@ -314,10 +340,8 @@ def run_native(args, rank, world, local):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": args.warmup,
         "ms_per_step": mixed["dev_ms"] / steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 pair arithmetic + f64 state (mixed)", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "particles": n, "images": int(mixed["diag"].n_images),
-                   "rhs_per_step": 3, "dt": mixed["dt"], "precision": "mixed",
-                   "l2": "state (~1.4 GB) larger than L2 (126 MB), no flush needed",
-                   "parallelism": f"replicas x{world}"},
+        "config": bench_config(n_side, world),
+        "images": int(mixed["diag"].n_images),
         "fp64": {"value": value64, "unit": UNIT, "ms_per_step": fp64["dev_ms"] / steps,
                  "mixed_over_fp64": value / value64},
         "accuracy": accuracy,
@@ -326,6 +350,7 @@ def run_native(args, rank, world, local):
         "adjoint_moving_square": adj_ms,
         "moving_square": ms,
         "plain_method": plain,
+        "lattice_exact": exact,
         "output_streaming": streaming,
         "passes_ms_per_step": {
             "images": tm.images_ms / steps, "sort_lists": tm.sort_ms / steps,
@@ -656,25 +681,67 @@ def moving_square_report(S, steps: int = 200, warmup: int = 3):
     return out
 
 
-def cpu_reference(steps: int, warmup: int, n_side: int = 256):
-    """The oracle (CPU restatement of the reference, OpenMP) on a bounded sample:
-    the same solver and physics on a 256 x 256 lattice."""
+def cpu_reference(steps: int, warmup: int, sides=(256,), serial: bool = True):
+    """The oracle (CPU restatement of the reference) on bounded samples of the
+    workload: the same solver, physics and jittered lattice at `sides` x `sides`
+    particles (h = 1.3 dx at every size, so the work per particle is that of the
+    2048^2 case), `steps` timed steps after `warmup` (at least the 4-RHS first
+    step) with OpenMP over particles on all host threads, and a serial leg
+    (1 thread, 128^2, a few steps).  The value is the rate of the largest sample."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle_api as O
     import sph_b200 as S
     O.build()
     threads = O.threads(os.cpu_count() or 1)
-    case = S.make_tgv(n_side, solver=S.SOLVER_MUSCL_DELTA_SPS)
-    dt = S.baseline_dt(case.cfg)
-    sim = O.OracleSim(case.cfg, case.pos, case.vel, case.rho, case.mass, case.type)
-    sim.run(max(warmup, 1), dt)        # first step has 4 RHS: keep it out of the timing
-    t0 = time.perf_counter()
-    sim.run(steps, dt)
-    el = time.perf_counter() - t0
-    return {"value": case.n * steps / el, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"TGV {n_side}x{n_side} ({case.n} particles), {steps} steps after {max(warmup, 1)} warm-up, "
-                      f"same solver, FP64, {threads} OpenMP threads; per-particle cost is size-independent",
-            "seconds": el}
+
+    def leg(n_side, nsteps):
+        case = S.make_tgv(n_side, solver=S.SOLVER_MUSCL_DELTA_SPS, jitter=JITTER, seed=JITTER_SEED)
+        dt = S.baseline_dt(case.cfg)
+        sim = O.OracleSim(case.cfg, case.pos, case.vel, case.rho, case.mass, case.type)
+        sim.run(max(warmup, 1), dt)        # the first step has 4 RHS: keep it out of the timing
+        t0 = time.perf_counter()
+        sim.run(nsteps, dt)
+        el = time.perf_counter() - t0
+        return {"n_side": n_side, "particles": case.n, "steps": nsteps, "seconds": el,
+                "particle_steps_per_s": case.n * nsteps / el}
+
+    legs = [leg(ns, steps) for ns in sides]
+    out = {"value": legs[-1]["particle_steps_per_s"], "unit": UNIT, "cores": threads, "kind": "port",
+           "sample": (f"TGV {legs[-1]['n_side']}^2 ({legs[-1]['particles']} particles) on the jittered lattice "
+                      f"(+-{JITTER}dx, seed {JITTER_SEED}), {steps} steps after {max(warmup, 1)} warm-up, same solver, "
+                      f"FP64, {threads} OpenMP threads"),
+           "seconds": legs[-1]["seconds"], "sizes": legs,
+           "per_particle_note": "the rate per particle at each sample size in `sizes` (h = 1.3 dx everywhere)"}
+    if serial:
+        O.threads(1)
+        try:
+            out["serial"] = dict(leg(128, min(steps, 3)), cores=1)
+        finally:
+            O.threads(threads)
+    return out
+
+
+def exact_lattice_report(S, n_side: int, steps: int = 20, warmup: int = 3):
+    """The same benchmark step on the exact (unjittered) lattice: device-timed
+    particle-steps/s of the mixed and FP64 paths and their velocity difference
+    after warm-up + timed steps (MUSCL limiter ties there are decided by
+    round-off, so that difference is not bounded by 1e-5)."""
+    out, vel = {}, {}
+    for name, prec in (("mixed", S.PREC_MIXED), ("fp64", S.PREC_FP64)):
+        case = S.make_tgv(n_side, solver=S.SOLVER_MUSCL_DELTA_SPS, precision=prec)
+        dt = S.baseline_dt(case.cfg)
+        with S.Simulation(case.cfg, case.n) as sim:
+            sim.set_state(case.pos, case.vel, case.rho, case.mass, case.type)
+            sim.time_iteration(warmup, dt)
+            sim.reset_timings()
+            sim.time_iteration(steps, dt)
+            tm = sim.timings()
+            vel[name] = sim.get_state()[1]
+        out[name] = {"particle_steps_per_s": case.n * steps / (tm.total_ms / 1e3), "ms_per_step": tm.total_ms / steps}
+    out["mixed_over_fp64"] = out["mixed"]["particle_steps_per_s"] / out["fp64"]["particle_steps_per_s"]
+    out["velocity_l2_mixed_vs_fp64"] = float(np.linalg.norm(vel["mixed"] - vel["fp64"]) / np.linalg.norm(vel["fp64"]))
+    out["case"] = f"TGV {n_side}x{n_side} exact lattice, same solver, {steps} steps after {warmup}, device-timed"
+    return out
 
 
 def main():
@@ -683,14 +750,16 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return 0
-        steps = max(1, min(args.steps, 4))
+        steps = max(1, args.steps)
         t0 = time.perf_counter()
-        cpu = cpu_reference(steps=steps, warmup=max(1, min(args.warmup, 2)))
+        # bounded samples of the workload (512^2 gives the value, 256^2 shows the
+        # rate per particle does not depend on the sample size) and a serial leg
+        cpu = cpu_reference(steps=steps, warmup=1, sides=(256, 512), serial=True)
         el = time.perf_counter() - t0
         line = {"metric": METRIC, "value": cpu["value"], "unit": UNIT, "n_gpus": world, "steps": steps,
                 "warmup": args.warmup, "ms_per_step": cpu["seconds"] / steps * 1e3, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-                "config": {"workload": WORKLOAD, "sample": cpu["sample"]},
+                "config": bench_config(args.n_side, world),
                 "cpu_baseline": cpu,
                 "e2e": {"value": cpu["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
                 "wall_s": el}
