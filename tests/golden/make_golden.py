@@ -7,14 +7,14 @@ Reads (only when run, in a checkout that has the reference mounted):
   Taylor_Green_Vortex/Maximum_velocity_magnitude.dat      max |u|/U every 100 steps
 Writes tests/golden/tgv_reference.npz (every 10th particle row and the first
 50 rows of both time series).  The tests never read the reference tree.
+
+Usage: python tests/golden/make_golden.py <path of the reference checkout>
 """
 import os
 import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-TGV = os.path.join(REF, "Taylor_Green_Vortex")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
@@ -32,11 +32,14 @@ def rows(path, ncol):
 
 
 def main():
-    init = rows(os.path.join(TGV, "Initial_particle_information.dat"), 6)
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <path of the reference checkout>")
+    tgv = os.path.join(sys.argv[1], "Taylor_Green_Vortex")
+    init = rows(os.path.join(tgv, "Initial_particle_information.dat"), 6)
     assert init.shape == (10000, 6), init.shape
     idx = np.arange(0, 10000, 10)
-    ke = rows(os.path.join(TGV, "Kinetic_energy.dat"), 2)[:50]
-    vmax = rows(os.path.join(TGV, "Maximum_velocity_magnitude.dat"), 2)[:50]
+    ke = rows(os.path.join(tgv, "Kinetic_energy.dat"), 2)[:50]
+    vmax = rows(os.path.join(tgv, "Maximum_velocity_magnitude.dat"), 2)[:50]
     np.savez_compressed(os.path.join(HERE, "tgv_reference.npz"), init_index=idx, init_rows=init[idx],
                         kinetic_energy=ke, max_velocity=vmax)
     print("wrote", os.path.join(HERE, "tgv_reference.npz"))
