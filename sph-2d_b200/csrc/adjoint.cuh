@@ -1377,8 +1377,16 @@ __device__ __forceinline__ void ghost_water_one(const Params& P, const Sorted<R>
     const double hg = P.ghost_h;
     double x0b = 0, x1b = 0, ub = 0, vb = 0, pb = 0, rb = 0;
     const int gx0 = max(cx - P.ghost_cells, 0), gx1 = min(cx + P.ghost_cells, P.gnx - 1);
-    for_cell_runs(P, D.cell_start, D.cell_end, gx0, gx1, max(cy - P.ghost_cells, 0),
-                  min(cy + P.ghost_cells, P.gny - 1), [&](int lo, int hi) {
+    for (int gy = max(cy - P.ghost_cells, 0); gy <= min(cy + P.ghost_cells, P.gny - 1); ++gy) {
+        const int row = gy * P.gnx;
+        int lo = -1, hi = -1;
+        for (int gx = gx0; gx <= gx1; ++gx) {
+            const int b0 = D.cell_start[row + gx];
+            if (b0 < 0) continue;
+            if (lo < 0) lo = b0;
+            hi = D.cell_end[row + gx];
+        }
+        if (lo < 0) continue;
         for (int s = lo + lane; s < hi; s += 32) {
             if (D.type[s] != SPH_TYPE_FIX_GHOST || D.id[s] >= P.n_host) continue;
             const double2 x = D.pos[s];
@@ -1410,7 +1418,7 @@ __device__ __forceinline__ void ghost_water_one(const Params& P, const Sorted<R>
             x0b -= k * dx + cg * gxe;
             x1b -= k * dy + cg * gye;
         }
-    });
+    }
     x0b = warp_sum(x0b); x1b = warp_sum(x1b); ub = warp_sum(ub); vb = warp_sum(vb);
     pb = warp_sum(pb); rb = warp_sum(rb);
     if (lane != 0) return;

@@ -186,8 +186,8 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? SPH_PASS_A_F32_BLOCKS : 
     D.nb3[a] = mk4<R>(gr[5], gr[6], gr[7], R(0));
     const R fv = fra;
     D.fra_v[a] = fv;
-    uint8_t fl = integrated(P, ta) ? (uint8_t)8 : (uint8_t)0;   // bit 3: rates assembled (read by pair partners)
-    if (P.free_surface && ta == SPH_TYPE_WATER && (double)fv <= P.fs_thr) fl |= 4;  // surface candidate (:123)
+    uint8_t fl = 0;
+    if (P.free_surface && ta == SPH_TYPE_WATER && (double)fv <= P.fs_thr) fl = 4;   // surface candidate (:123)
     D.flags[a] = fl;
     if (MS) D.avg[a] = mk2<R>(xs0, xs1);
 }

@@ -74,10 +74,9 @@ struct Side {
 #ifndef SPH_PASS_C_SHIFT_BLOCKS
 #define SPH_PASS_C_SHIFT_BLOCKS 4
 #endif
-// The gather for particle a (a < n_tot); the body of k_pass_c, also run by the
-// blocks of k_pass_c_tile that cannot hold their pairs in shared memory.
 template <typename R, bool MUSCL, bool MS, bool SHIFT>
-__device__ __forceinline__ void pass_c_gather(const Params& P, const Sorted<R>& D, const int a) {
+__global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIFT_BLOCKS : 4) : 3)
+    k_pass_c(Params P, Sorted<R> D) {
     using V4 = typename VT<R>::V4;
     using A = typename Acc<R>::T;
     constexpr bool F32 = sizeof(R) == 4;
@@ -88,6 +87,8 @@ __device__ __forceinline__ void pass_c_gather(const Params& P, const Sorted<R>& 
     // neighbour's FP64 position (and FP64 volume) instead of its hi/lo position
     // and takes the FP32 difference as the rounding of the FP64 one
     constexpr bool X64 = !HL || SHIFT;
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= P.n_tot) return;
     const int ta = D.type[a];
     const int nn = D.npairs[a];
     const double2 xa = X64 ? D.pos[a] : make_double2(0.0, 0.0);
@@ -410,14 +411,6 @@ __device__ __forceinline__ void pass_c_gather(const Params& P, const Sorted<R>& 
         const double c = -P.shift_beta * (P.h * P.h);
         D.shift[a] = make_double2(c * (b64.x * shx + b64.y * shy), c * (b64.z * shx + b64.w * shy));
     }
-}
-
-template <typename R, bool MUSCL, bool MS, bool SHIFT>
-__global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIFT_BLOCKS : 4) : 3)
-    k_pass_c(Params P, Sorted<R> D) {
-    const int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= P.n_tot) return;
-    pass_c_gather<R, MUSCL, MS, SHIFT>(P, D, a);
 }
 
 // The particle shifting sum of the mixed Taylor-Green path as a gather of its

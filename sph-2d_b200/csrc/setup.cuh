@@ -93,52 +93,7 @@ __global__ void k_img_emit(Params P, Staging S, int n_src, int axis, int base, c
     }
 }
 
-// --- 3. cell keys ------------------------------------------------------------
-// Cells of edge >= list radius, ordered in super-rows of kSuperRow cell rows:
-// super-row by super-row, column by column inside a super-row, bottom to top
-// inside a column.  A run of consecutive sorted slots then covers a patch
-// kSuperRow cells high instead of a strip one cell high, so more of a
-// particle's neighbours fall inside the same block of consecutive slots (pass
-// C evaluates those pairs once per block; 76 % of the pairs at h = 1.3 dx with
-// two rows, 59 % with one).
-constexpr int kSuperRow = 2;
-
-__host__ __device__ __forceinline__ unsigned cell_key(const Params& P, int cx, int cy) {
-    return (unsigned)((cy / kSuperRow) * (P.gnx * kSuperRow) + cx * kSuperRow + (cy % kSuperRow));
-}
-
-// Number of cell keys (the super-rows padded to kSuperRow rows).
-__host__ __forceinline__ long long cell_key_count(const Params& P) {
-    return (long long)((P.gny + kSuperRow - 1) / kSuperRow) * kSuperRow * P.gnx;
-}
-
-// The slot ranges of the particles in the cells [gx0, gx1] x [gy0, gy1]: fn(lo,
-// hi) for runs of consecutive keys (a whole super-row slice is one run; a
-// partial one gives one run per column), each run's particles being the
-// contiguous slots lo..hi-1.  Empty cells hold cell_start = -1.
-template <typename F>
-__device__ __forceinline__ void for_cell_runs(const Params& P, const int* cell_start, const int* cell_end, int gx0,
-                                              int gx1, int gy0, int gy1, F&& fn) {
-    auto run = [&](unsigned k0, unsigned k1) {
-        int lo = -1, hi = -1;
-        for (unsigned k = k0; k <= k1; ++k) {
-            const int st = cell_start[k];
-            if (st < 0) continue;
-            if (lo < 0) lo = st;
-            hi = cell_end[k];
-        }
-        if (lo >= 0) fn(lo, hi);
-    };
-    for (int R = gy0 / kSuperRow; R <= gy1 / kSuperRow; ++R) {
-        const int r0 = max(gy0, R * kSuperRow), r1 = min(gy1, R * kSuperRow + kSuperRow - 1);
-        if (r0 == R * kSuperRow && r1 == R * kSuperRow + kSuperRow - 1) {
-            run(cell_key(P, gx0, r0), cell_key(P, gx1, r1));
-        } else {
-            for (int gx = gx0; gx <= gx1; ++gx) run(cell_key(P, gx, r0), cell_key(P, gx, r1));
-        }
-    }
-}
-
+// --- 3. cell keys (row-major cells of edge >= list radius) -----------------
 __global__ void k_cell_keys(Params P, const double2* pos, const int* type, unsigned* keys, unsigned* vals,
                             unsigned* status, unsigned dead_key) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -154,7 +109,7 @@ __global__ void k_cell_keys(Params P, const double2* pos, const int* type, unsig
         keys[i] = dead_key;
         return;
     }
-    keys[i] = cell_key(P, cx, cy);
+    keys[i] = (unsigned)(cy * P.gnx + cx);
 }
 
 // Device-side arrays in cell-sorted order (templated on the pair precision).
@@ -184,7 +139,7 @@ struct Sorted {
     V4* binv;         // B^-1 (11, 12, 21, 22) in the pair precision
     double4* binv64;  // B^-1 in FP64 (applied to the FP64 shifting sum)
     R* fra_v;
-    uint8_t* flags;   // bit0 surface, bit1 near surface, bit2 surface candidate, bit3 integrated (water)
+    uint8_t* flags;   // bit0 surface, bit1 near surface, bit2 surface candidate
     // rates of the current RHS
     R* drho;
     V2* acc;
@@ -338,9 +293,17 @@ __global__ void __launch_bounds__(128) k_build_lists(Params P, Sorted<R> D, unsi
         int x0 = max(cx - 1, 0), x1 = min(cx + 1, P.gnx - 1);
         // with the one-fluid rule every pair of a water particle is allowed
         const bool check_type = !(P.pair_rule == SPH_PAIRS_ONE_FLUID && ta == SPH_TYPE_WATER);
-        // the 3x3 cells as runs of contiguous slots of the sorted order
-        for_cell_runs(P, D.cell_start, D.cell_end, x0, x1, max(cy - 1, 0), min(cy + 1, P.gny - 1),
-                      [&](int b0, int b1) {
+        for (int gy = max(cy - 1, 0); gy <= min(cy + 1, P.gny - 1); ++gy) {
+            // the cells x0..x1 of a row are consecutive keys, so their particles
+            // form one contiguous range of the sorted order
+            const int row = gy * P.gnx;
+            int b0 = -1, b1 = -1;
+            for (int gx = x0; gx <= x1; ++gx) {
+                const int st = D.cell_start[row + gx];
+                if (st < 0) continue;
+                if (b0 < 0) b0 = st;
+                b1 = D.cell_end[row + gx];
+            }
             // candidates four at a time: their loads are issued together, then
             // tested in order (the list is the same as a one-by-one scan)
             int b = b0;
@@ -370,7 +333,7 @@ __global__ void __launch_bounds__(128) k_build_lists(Params P, Sorted<R> D, unsi
                 if (dx * dx + dy * dy > P.r2_list) continue;
                 put(b, ida < D.id[b] ? 0x80000000u : 0u);
             }
-        });
+        }
         if (cnt > P.max_nbr) { atomicOr(status, ST_NBR_OVERFLOW); cnt = P.max_nbr; }
     }
     const int ns = min(cnt, kListStage);

@@ -23,7 +23,6 @@
 #include <vector>
 
 #include "adjoint.cuh"
-#include "pass_c_tile.cuh"
 
 using namespace sph;
 
@@ -223,7 +222,7 @@ int derive_params(const sph_config& c, Params& P) {
     P.gnx = (int)ceil((c.grid_hi[0] - c.grid_lo[0]) / rl) + 3;
     P.gny = (int)ceil((c.grid_hi[1] - c.grid_lo[1]) / rl) + 3;
     if (!(c.grid_hi[0] > c.grid_lo[0]) || !(c.grid_hi[1] > c.grid_lo[1])) return SPH_E_CONFIG;
-    if ((long long)P.gnx * (P.gny + 1) > (1LL << 30)) return SPH_E_CONFIG;
+    if ((long long)P.gnx * P.gny > (1LL << 30)) return SPH_E_CONFIG;
     // neighbour-list capacity: twice the lattice count inside the list radius
     const double lat = pi * (rl / c.dx) * (rl / c.dx);
     int mn = (int)ceil(2.0 * lat) + 16;
@@ -431,14 +430,11 @@ int rhs(sph_handle* h, int last) {
         if (shc) k_pass_c<R, false, true, true><<<nb, 128, 0, h->stream>>>(P, D);
         else k_pass_c<R, false, true, false><<<nb, 128, 0, h->stream>>>(P, D);
     } else if (P.muscl) {
-        // the benchmark solver: pairs inside a block evaluated once (the FP64
-        // launch that also forms the shifting sum keeps the gather)
-        const int nbt = blocks(P.n_tot, kTileThreads);
         if constexpr (sizeof(R) == 8) {       // the mixed launches never carry the sum
             if (shc) k_pass_c<R, true, false, true><<<nb, 128, 0, h->stream>>>(P, D);
-            else k_pass_c_tile<R><<<nbt, kTileThreads, pass_c_tile_smem<R>(), h->stream>>>(P, D);
+            else k_pass_c<R, true, false, false><<<nb, 128, 0, h->stream>>>(P, D);
         } else {
-            k_pass_c_tile<R><<<nbt, kTileThreads, pass_c_tile_smem<R>(), h->stream>>>(P, D);
+            k_pass_c<R, true, false, false><<<nb, 128, 0, h->stream>>>(P, D);
         }
     } else {
         if constexpr (sizeof(R) == 8) {
@@ -1369,16 +1365,11 @@ int init_impl(const sph_config* cfg, int n_capacity, sph_handle** out) {
     }
     h->cap_tot = h->cap_host + h->cap_img;
     const int cap = h->cap_tot;
-    h->ncells = (int)cell_key_count(h->P);
+    h->ncells = h->P.gnx * h->P.gny;
     h->key_bits = 1;
     while ((1LL << h->key_bits) <= (long long)h->ncells) h->key_bits++;
     h->dead_key = (unsigned)((1ULL << h->key_bits) - 1);
     h->P.nbr_stride = cap;
-    // the tile pass keeps its pairs and the partners' terms in shared memory
-    CK(cudaFuncSetAttribute(k_pass_c_tile<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)pass_c_tile_smem<float>()));
-    CK(cudaFuncSetAttribute(k_pass_c_tile<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)pass_c_tile_smem<double>()));
     CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&h->snap_ready, cudaEventDisableTiming));

@@ -317,8 +317,16 @@ __device__ __forceinline__ void ghost_visit_warp(const Params& P, const Sorted<R
     const int cx = (int)floor((x.x - P.gx0) / P.cs), cy = (int)floor((x.y - P.gy0) / P.cs);
     const double hg = P.ghost_h;
     const int gx0 = max(cx - P.ghost_cells, 0), gx1 = min(cx + P.ghost_cells, P.gnx - 1);
-    for_cell_runs(P, D.cell_start, D.cell_end, gx0, gx1, max(cy - P.ghost_cells, 0),
-                  min(cy + P.ghost_cells, P.gny - 1), [&](int lo, int hi) {
+    for (int gy = max(cy - P.ghost_cells, 0); gy <= min(cy + P.ghost_cells, P.gny - 1); ++gy) {
+        const int row = gy * P.gnx;
+        int lo = -1, hi = -1;
+        for (int gx = gx0; gx <= gx1; ++gx) {
+            const int b0 = D.cell_start[row + gx];
+            if (b0 < 0) continue;
+            if (lo < 0) lo = b0;
+            hi = D.cell_end[row + gx];
+        }
+        if (lo < 0) continue;
         for (int b = lo + lane; b < hi; b += 32) {
             if (D.type[b] == SPH_TYPE_FIX_GHOST) continue;
             const double2 xb = D.pos[b];
@@ -336,7 +344,7 @@ __device__ __forceinline__ void ghost_visit_warp(const Params& P, const Sorted<R
             }
             fn(b, dx, dy, q, w);
         }
-    });
+    }
 }
 
 // Sum over the warp, lane 0's association order, broadcast to every lane (so
