@@ -35,19 +35,24 @@ namespace sph {
 
 template <typename R>
 __device__ __forceinline__ void muscl_limiter(R di, R dj, R dij, R& li, R& lj) {
-    // the two sign branches of the reference written with selects (the same
-    // values, bit for bit, including the sign of the zero increments), so the
-    // lanes of a warp do not diverge
+    // The reference's two sign branches folded into one: with s = sign(dj)
+    // (+1 when dj > 0, else -1) the dj <= 0 branch is the dj > 0 branch applied
+    // to (-di, -dj) and negated, since min and max swap under negation:
+    //   lim = s max(0, max(min(1.3 s di, s dj), min(s di, 1.3 s dj))),
+    //   lim < dij/2 (dj <= 0) <=> s lim > s dij/2,  di < dj <=> s di > s dj.
+    // The same values as the branches (zero increments may carry the other
+    // sign), one min/max chain, no divergence between the lanes of a warp.
     const R b = R(1.3);
-    const R bdi = b * di, bdj = b * dj;
-    const bool pos = dj > R(0);
-    const R lim = pos ? max(R(0), max(min(bdi, dj), min(di, bdj))) : min(R(0), min(max(bdi, dj), max(di, bdj)));
+    const R s = dj > R(0) ? R(1) : R(-1);
+    const R sdi = s * di, sdj = s * dj;
+    const R m = max(R(0), max(min(b * sdi, sdj), min(sdi, b * sdj)));     // s * lim >= 0
     const R half = R(0.5) * dij;
-    const bool big = (pos ? (lim > half) : (lim < half)) && fabs(lim) > R(0);
-    const bool first = pos ? (di > dj) : (di < dj);
-    const R on = dij * R(0.5), off = dij * R(0);
-    li = big ? (first ? on : off) : lim;
-    lj = big ? (first ? off : on) : lim;
+    const bool big = m > s * half && m > R(0);
+    const bool first = sdi > sdj;
+    const R lim = s * m;
+    const R off = dij * R(0);
+    li = big ? (first ? half : off) : lim;
+    lj = big ? (first ? off : half) : lim;
 }
 
 __device__ __forceinline__ double rcp(double x) { return 1.0 / x; }
