@@ -96,6 +96,10 @@ __device__ __forceinline__ bool in_support(const Params& P, double dx, double dy
     return d <= P.r_cut && d >= P.cut_min;
 }
 
+// A product rounded on its own (never fused into a following add).
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+
 // TwoSum (Knuth) compensated accumulation for the FP32 sums.
 struct CSum {
     float s, c;

@@ -193,27 +193,31 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIF
             inv_d = R(1) / d;
         }
         if (!PRE) load_records(b, T);
+        // the pair's i and j members (only the moving-square HLLC state reads
+        // them; everything else is formed from a's and b's records directly)
         const Side<R>& I = a_is_i ? S : T;
         const Side<R>& J = a_is_i ? T : S;
         const R sgn = a_is_i ? R(1) : R(-1);
-        // position_difference_ij = x_i - x_j (find_particle_pair.f90:79-107)
-        R xij0, xij1;
-        if (HL) { xij0 = (R)(a_is_i ? dxf : -dxf); xij1 = (R)(a_is_i ? dyf : -dyf); }
-        else { xij0 = (R)(a_is_i ? dxd : -dxd); xij1 = (R)(a_is_i ? dyd : -dyd); }
-        // pair differences: FP64, or hi/lo in FP32
-        R du, dv, dp, drho_ji, rho_i, rho_j, rho_b;
+        // position_difference_ij = x_i - x_j (find_particle_pair.f90:79-107) = sgn (x_a - x_b)
+        R xab0, xab1;
+        if (HL) { xab0 = (R)dxf; xab1 = (R)dyf; }
+        else { xab0 = (R)dxd; xab1 = (R)dyd; }
+        const R xij0 = sgn * xab0, xij1 = sgn * xab1;
+        // pair differences, FP64 or hi/lo in FP32, formed as a - b and oriented
+        // by sgn: b - a is exactly -(a - b), so both members of the pair get the
+        // same bits, and sums such as rho_i + rho_j are a's plus b's
+        R du, dv, dp, drho_ji, rho_a_, rho_b;
         if (HL) {
-            du = (R)((I.kh.x - J.kh.x) + (I.kl.x - J.kl.x));
-            dv = (R)((I.kh.y - J.kh.y) + (I.kl.y - J.kl.y));
-            dp = (R)((I.kh.w - J.kh.w) + (I.kl.w - J.kl.w));
-            drho_ji = (R)((J.kh.z - I.kh.z) + (J.kl.z - I.kl.z));
-            rho_i = (R)I.kh.z; rho_j = (R)J.kh.z; rho_b = (R)T.kh.z;
+            du = sgn * (R)((S.kh.x - T.kh.x) + (S.kl.x - T.kl.x));
+            dv = sgn * (R)((S.kh.y - T.kh.y) + (S.kl.y - T.kl.y));
+            dp = sgn * (R)((S.kh.w - T.kh.w) + (S.kl.w - T.kl.w));
+            drho_ji = -(sgn * (R)((S.kh.z - T.kh.z) + (S.kl.z - T.kl.z)));
+            rho_a_ = (R)S.kh.z; rho_b = (R)T.kh.z;
         } else {
-            du = (R)(I.kin.x - J.kin.x); dv = (R)(I.kin.y - J.kin.y);
-            dp = (R)(I.kin.w - J.kin.w);
-            drho_ji = (R)(J.kin.z - I.kin.z);
-            rho_i = (R)I.kin.z; rho_j = (R)J.kin.z;
-            rho_b = (R)T.kin.z;
+            du = sgn * (R)(S.kin.x - T.kin.x); dv = sgn * (R)(S.kin.y - T.kin.y);
+            dp = sgn * (R)(S.kin.w - T.kin.w);
+            drho_ji = -(sgn * (R)(S.kin.z - T.kin.z));
+            rho_a_ = (R)S.kin.z; rho_b = (R)T.kin.z;
         }
         // compute_kernel: W and dwdx(k) = g (x_i - x_j)
         R w, g;
@@ -235,26 +239,31 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIF
         // Normalized_dwdx of this particle's side: B_a^-1 dwdx(k)
         const R nd0 = bi.x * dw0 + bi.y * dw1;
         const R nd1 = bi.z * dw0 + bi.w * dw1;
-        const R cbar = R(0.5) * (I.aux.z + J.aux.z);
-        const R rbar = R(0.5) * (rho_i + rho_j);
+        const R cbar = R(0.5) * (S.aux.z + T.aux.z);
+        const R rbar = R(0.5) * (rho_a_ + rho_b);
         const R inv_rbar = rcp(rbar);
         const R e0 = -xij0 * inv_d, e1 = -xij1 * inv_d;     // x_j - x_i direction (both solvers)
         // Riemann states.  li/lj are the MUSCL reconstruction increments
         // (function_module.f90:34-80); the modified solver has none.
         R lpi = R(0), lpj = R(0), lui = R(0), luj = R(0), lvi = R(0), lvj = R(0);
         if (MUSCL) {
-            const R x0 = -xij0, x1 = -xij1;          // j - i
+            // DelPhi_i = 0.5 grad phi_i.(x_j - x_i), DelPhi_j = -0.5 grad phi_j.(x_j - x_i):
+            // with ga = 0.5 grad phi_a.(x_a - x_b), gb = 0.5 grad phi_b.(x_a - x_b),
+            // (DelPhi_i, DelPhi_j) = (-ga, gb) when a is pair_i and (gb, -ga) when it is
+            // pair_j.  The products are rounded separately and fused in a fixed order,
+            // so both members of the pair form the same bits.
             // nb2 = (grad rho y, grad p x, grad p y, grad u x), nb3 = (grad u y, grad v x, grad v y, 0)
-            muscl_limiter<R>(R(0.5) * (I.nb2.y * x0 + I.nb2.z * x1), R(-0.5) * (J.nb2.y * x0 + J.nb2.z * x1), -dp,
-                             lpi, lpj);
-            muscl_limiter<R>(R(0.5) * (I.nb2.w * x0 + I.nb3.x * x1), R(-0.5) * (J.nb2.w * x0 + J.nb3.x * x1), -du,
-                             lui, luj);
-            muscl_limiter<R>(R(0.5) * (I.nb3.y * x0 + I.nb3.z * x1), R(-0.5) * (J.nb3.y * x0 + J.nb3.z * x1), -dv,
-                             lvi, lvj);
+            auto half_dot = [&](R g0, R g1) { return R(0.5) * fma(g1, xab1, mul_rn(g0, xab0)); };
+            const R gpa = half_dot(S.nb2.y, S.nb2.z), gpb = half_dot(T.nb2.y, T.nb2.z);
+            const R gua = half_dot(S.nb2.w, S.nb3.x), gub = half_dot(T.nb2.w, T.nb3.x);
+            const R gva = half_dot(S.nb3.y, S.nb3.z), gvb = half_dot(T.nb3.y, T.nb3.z);
+            muscl_limiter<R>(a_is_i ? -gpa : gpb, a_is_i ? gpb : -gpa, -dp, lpi, lpj);
+            muscl_limiter<R>(a_is_i ? -gua : gub, a_is_i ? gub : -gua, -du, lui, luj);
+            muscl_limiter<R>(a_is_i ? -gva : gvb, a_is_i ? gvb : -gva, -dv, lvi, lvj);
         }
         // U_L - U_R and P_L - P_R from the differences
         const R dU = (du + lui + luj) * e0 + (dv + lvi + lvj) * e1;
-        const R Pbar = HL ? R(0.5) * ((R)I.kh.w + (R)J.kh.w) : R(0.5) * ((R)I.kin.w + (R)J.kin.w);
+        const R Pbar = HL ? R(0.5) * ((R)S.kh.w + (R)T.kh.w) : R(0.5) * ((R)S.kin.w + (R)T.kin.w);
         R PA, wa0, wa1;          // this side's star pressure and velocity minus star velocity
         if (a_is_i) { wa0 = R(0.5) * du + lui; wa1 = R(0.5) * dv + lvi; }
         else { wa0 = R(-0.5) * du - luj; wa1 = R(-0.5) * dv - lvj; }
@@ -298,7 +307,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIF
             } else { rH = rR; VH0 = VR0; VH1 = VR1; }
             const double vs0 = ed0 * VH0 - ed1 * VH1, vs1 = ed1 * VH0 + ed0 * VH1;
             PA = (R)(P.c0sq * (rH - P.rho0) + P.pb);
-            const double4& K = a_is_i ? I.kin : J.kin;
+            const double4& K = S.kin;
             wa0 = (R)(K.x - vs0);
             wa1 = (R)(K.y - vs1);
         }
@@ -341,7 +350,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIF
         // SPS force, unnormalised dwdx and the neighbour's SPS mass (:450-492);
         // the reference does not reset temp_p between x and y (kept with quirks)
         if (!MS) {
-            const R sxx = I.nb1.x + J.nb1.x, sxy = I.nb1.y + J.nb1.y, syy = I.nb1.z + J.nb1.z;
+            const R sxx = S.nb1.x + T.nb1.x, sxy = S.nb1.y + T.nb1.y, syy = S.nb1.z + T.nb1.z;
             R tp = (sxx * dw0 + sxy * dw1) * rho_ij;
             const R smb = T.aux.w;
             tx += smb * tp;
@@ -353,13 +362,13 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIF
         accy.add(sgn * ty);
         // XSPH average velocity (:495-500; modified solver only)
         if (!MUSCL && !MS && P.xsph) {
-            const R f = eps2 * mb * rcp(rho_i + rho_j) * w;
+            const R f = eps2 * mb * rcp(rho_a_ + rho_b) * w;
             xsx -= sgn * (f * du);
             xsy -= sgn * (f * dv);
         }
         // delta-SPH density diffusion (:552-583): psi = (rho_j - rho_i) - 0.5 (grad rho_i + grad rho_j).(x_j - x_i)
         if (water) {
-            const R sg0 = I.nb1.w + J.nb1.w, sg1 = I.nb2.x + J.nb2.x;
+            const R sg0 = S.nb1.w + T.nb1.w, sg1 = S.nb2.x + T.nb2.x;
             if (dsph) {
                 // Antuono form (Solver_Normalized_Delta_SPH_SPS.f90:610-636):
                 // psi = 2 (rho_j - rho_i) (x_j - x_i)/r^2 - (grad rho_i + grad rho_j), D += delta h c psi.gradW V
