@@ -55,8 +55,13 @@ __device__ __forceinline__ void muscl_limiter(R di, R dj, R dij, R& li, R& lj) {
     lj = big ? (first ? off : half) : lim;
 }
 
+// Reciprocal and quotient in the pair loop: exact in FP64; in FP32 the fast
+// forms (__fdividef, a few ulp), whose error is far below the rounding the
+// mixed path already accepts in each FP32 pair term.
 __device__ __forceinline__ double rcp(double x) { return 1.0 / x; }
-__device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ float rcp(float x) { return __fdividef(1.0f, x); }
+__device__ __forceinline__ double quot(double a, double b) { return a / b; }
+__device__ __forceinline__ float quot(float a, float b) { return __fdividef(a, b); }
 
 // Per-particle state a thread needs for one side of a pair.
 template <typename R>
@@ -327,7 +332,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIF
         const R inv_r2 = inv_d * inv_d;
         const R vx = du * xij0 + dv * xij1;
         if (vx < R(0)) {
-            const R phi1 = hbar * vx / (d * d + fh2);
+            const R phi1 = quot(hbar * vx, d * d + fh2);
             const R Pi = (-alpha * cbar * phi1 + beta * (phi1 * phi1)) * inv_rbar;
             tx += mb * (-Pi * nd0);
             ty += mb * (-Pi * nd1);
