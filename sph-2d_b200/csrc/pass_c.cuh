@@ -90,9 +90,9 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIF
     using V4 = typename VT<R>::V4;
     using A = typename Acc<R>::T;
     constexpr bool F32 = sizeof(R) == 4;
-    // hi/lo records: the mixed Taylor-Green variants (the moving-square ones keep
-    // the FP64 records, which their FP64 HLLC state needs)
-    constexpr bool HL = F32 && !MS;
+    // hi/lo records: every mixed variant (the moving-square HLLC state is then
+    // formed in FP32 from differences, below)
+    constexpr bool HL = F32;
     // the shifting sum needs the FP64 position differences: that launch reads the
     // neighbour's FP64 position (and FP64 volume) instead of its hi/lo position
     // and takes the FP32 difference as the rounding of the FP64 one
@@ -281,9 +281,64 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIF
             if (!near_a) { wa0 -= sU * e0; wa1 -= sU * e1; }
         } else if (near_a) {
             PA = Pbar;
+        } else if (HL) {
+            // The HLLC state of Moving_Square.../Solver_Normalized_HLLC_Riemann_Delta.f90:207-322
+            // written in differences, so that FP32 keeps the accuracy of the hi/lo pair
+            // differences (rho* and P* = c0^2 (rho_HLLC - rho0) are otherwise differences of
+            // O(1) numbers).  Pair frame e (i to j) and t = (-e1, e0); dV = VR0 - VL0 =
+            // -(du, dv).e; C_K = rho_K c_K; the reference's contact speed
+            // U* = (VR0 C_L + VL0 C_R + P_L - P_R)/(C_L + C_R) gives
+            //   sL = U* - VL0 = (C_L dV + dp)/(C_L + C_R),  sR = U* - VR0 = (dp - C_R dV)/(C_L + C_R),
+            //   P* - P_L = -C_L (dp + C_R dV)/(C_L + C_R);
+            // the state sampled at V0 = (VL0 + VR0)/2, V0 - VL0 = VR0 - V0 = dV/2, gives
+            //   rho_HLLC - rho0 = (rho_K - rho0) [+ rho_K (U* - V_K0)/(S_K - U*) in the star regions]
+            // and v_K - v* as components along e and t.
+            const R rL = a_is_i ? rho_a_ : rho_b, rR = a_is_i ? rho_b : rho_a_;
+            const R cL = a_is_i ? (R)S.aux.z : (R)T.aux.z, cR = a_is_i ? (R)T.aux.z : (R)S.aux.z;
+            const R rho0f = (R)P.rho0;
+            const R dra = (R)((S.kh.z - (float)rho0f) + S.kl.z), drb = (R)((T.kh.z - (float)rho0f) + T.kl.z);
+            const R drL = a_is_i ? dra : drb, drR = a_is_i ? drb : dra;   // rho - rho0
+            const R CL = rL * cL, CR = rR * cR;
+            const R iC = rcp(CL + CR);
+            const R dV = -(e0 * du + e1 * dv);
+            const R sL = (CL * dV + dp) * iC;
+            const R sR = (dp - CR * dV) * iC;
+            const R dPL = -(CL * (dp + CR * dV)) * iC;     // P* - P_L
+            const R dPR = dPL + dp;                        // P* - P_R
+            // shock factor (:243-275): taken when P* > P_K and rho_K > rho*.  With the linear
+            // equation of state rho_K - rho* = -(P* - P_K)/c0^2, so the branch is never taken.
+            R QL = R(1), QR = R(1);
+            if (P.eos != SPH_EOS_LINEAR) {
+                const R ic0 = (R)(1.0 / P.c0sq), pbf = (R)P.pb;
+                const R pa_ = (R)(S.kh.w + S.kl.w), pbb = (R)(T.kh.w + T.kl.w);
+                const R pL = a_is_i ? pa_ : pbb, pR = a_is_i ? pbb : pa_;
+                const R gL = drL - (pL - pbf) * ic0 - dPL * ic0;     // rho_L - rho*
+                const R gR = drR - (pR - pbf) * ic0 - dPR * ic0;     // rho_R - rho*
+                if (dPL > R(0) && gL > R(0)) QL = sqrt(((rL - gL) / rL) * dPL / gL) / cL;
+                if (dPR > R(0) && gR > R(0)) QR = sqrt(((rR - gR) / rR) * dPR / gR) / cR;
+            }
+            const R sLm = -cL * QL, sRm = cR * QR;         // S_L - VL0, S_R - VR0
+            const R hdV = R(0.5) * dV;
+            const R tdv = e1 * du - e0 * dv;               // VR1 - VL1
+            R dH, aI, bI, aJ, bJ;       // rho_HLLC - rho0; v_i - v* = aI e + bI t, v_j - v* = aJ e + bJ t
+            if (sLm > hdV) {                                        // S_L > V0: the left state
+                dH = drL; aI = R(0); bI = R(0); aJ = dV; bJ = tdv;
+            } else if (sL - hdV >= R(0) && hdV >= sLm) {            // U* >= V0 >= S_L
+                dH = drL + rL * quot(sL, sLm - sL);
+                aI = -sL; bI = R(0); aJ = -sR; bJ = tdv;
+            } else if (sRm >= -hdV && sL - hdV <= R(0)) {           // S_R >= V0 >= U*
+                dH = drR + rR * quot(sR, sRm - sR);
+                aI = -sL; bI = -tdv; aJ = -sR; bJ = R(0);
+            } else {                                                // the right state
+                dH = drR; aI = -dV; bI = -tdv; aJ = R(0); bJ = R(0);
+            }
+            PA = (R)P.c0sq * dH + (R)P.pb;
+            const R al = a_is_i ? aI : aJ, be = a_is_i ? bI : bJ;
+            wa0 = al * e0 - be * e1;
+            wa1 = al * e1 + be * e0;
         } else {
             // HLLC in the pair frame (Moving_Square.../Solver_Normalized_HLLC_Riemann_Delta.f90:207-322),
-            // in FP64 in both paths: rho* and P* = c0^2 (rho_HLLC - rho0) are differences of O(1) numbers
+            // FP64 path: the reference's own operations
             const double ed0 = -(a_is_i ? dxd : -dxd) / sqrt(dxd * dxd + dyd * dyd);
             const double ed1 = -(a_is_i ? dyd : -dyd) / sqrt(dxd * dxd + dyd * dyd);
             const double uI = I.kin.x, vI = I.kin.y, uJ = J.kin.x, vJ = J.kin.y;
