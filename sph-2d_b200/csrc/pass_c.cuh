@@ -55,13 +55,13 @@ __device__ __forceinline__ void muscl_limiter(R di, R dj, R dij, R& li, R& lj) {
     lj = big ? (first ? off : half) : lim;
 }
 
-// Reciprocal and quotient in the pair loop: exact in FP64; in FP32 the fast
-// forms (__fdividef, a few ulp), whose error is far below the rounding the
-// mixed path already accepts in each FP32 pair term.
+// Reciprocal and quotient in the pair loop, correctly rounded in both
+// precisions (the fast FP32 forms, __fdividef, made mixed pass C slower:
+// 3.46 -> 3.85 ms per step at 2048^2).
 __device__ __forceinline__ double rcp(double x) { return 1.0 / x; }
-__device__ __forceinline__ float rcp(float x) { return __fdividef(1.0f, x); }
-__device__ __forceinline__ double quot(double a, double b) { return a / b; }
-__device__ __forceinline__ float quot(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
+template <typename R>
+__device__ __forceinline__ R quot(R a, R b) { return a / b; }
 
 // Per-particle state a thread needs for one side of a pair.
 template <typename R>
@@ -84,8 +84,11 @@ struct Side {
 #ifndef SPH_PASS_C_SHIFT_BLOCKS
 #define SPH_PASS_C_SHIFT_BLOCKS 4
 #endif
+#ifndef SPH_PASS_C_F32_BLOCKS
+#define SPH_PASS_C_F32_BLOCKS 4
+#endif
 template <typename R, bool MUSCL, bool MS, bool SHIFT>
-__global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIFT_BLOCKS : 4) : 3)
+__global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIFT_BLOCKS : SPH_PASS_C_F32_BLOCKS) : 3)
     k_pass_c(Params P, Sorted<R> D) {
     using V4 = typename VT<R>::V4;
     using A = typename Acc<R>::T;
