@@ -329,8 +329,10 @@ int sph_find_particle_pair_noalloc(const sph_config* cfg, int n, const double* d
  *    SPH_SOLVER_MUSCL_DELTA_SPS) with the RK4 driver, with or without particle
  *    shifting (the limiter, the capped shift and its density correction are
  *    differentiated on the branch the forward took);
- *  - the moving-square modified linear Riemann solver (SPH_SOLVER_MS_MODLR_DELTA,
- *    Morris laplacian, XSPH velocities in the continuity flux) with the Euler
+ *  - the moving-square modified linear Riemann and HLLC solvers
+ *    (SPH_SOLVER_MS_MODLR_DELTA, SPH_SOLVER_MS_HLLC_DELTA; Morris laplacian,
+ *    XSPH velocities in the continuity flux; the HLLC state on the sampled
+ *    region and wave speeds the forward took) with the Euler
  *    predictor-corrector driver, with the library's ghost assignment
  *    (ghost_assign = 1: the reverse runs through the Shepard interpolation onto
  *    the wall and body ghosts) or with caller-given ghost states; without

@@ -230,8 +230,9 @@ __device__ __forceinline__ void muscl_limiter_rev(double di, double dj, double d
 
 // Reverse of the contribution of b to particle a (a water particle) with the
 // adjoints lr (of drho_a) and (l0, l1) (of acc_a).  MS: the moving-square
-// modified solver (Moving_Square.../Solver_Normalized_Modified_Linear_Riemann_Delta.f90
-// :169-230): w also carries avg_a - avg_b (XSPH inside the continuity flux), no SPS.
+// solvers (Moving_Square.../Solver_Normalized_Modified_Linear_Riemann_Delta.f90
+// :169-230, and with P.hllc Solver_Normalized_HLLC_Riemann_Delta.f90:207-322):
+// w also carries avg_a - avg_b (XSPH inside the continuity flux), no SPS.
 // MUSCL: the MUSCL linear-Riemann solver (Solver_Normalized_MUSCL_Linear_Riemann_Delta_SPS.f90:
 // 470-502): the limited reconstructions of p, u, v enter U_L - U_R, P_L - P_R and
 // this side's v - v*; a_lower: a is the reference's pair index i (the lower id),
@@ -280,7 +281,43 @@ __device__ __forceinline__ void rev_pair(const Params& P, const PSide& A, const 
     bool take_m3 = false;
     // this side's reconstruction increment: + l_i as i, - l_j as j
     const double su = MUSCL ? (a_lower ? lui : -luj) : 0.0, sv = MUSCL ? (a_lower ? lvi : -lvj) : 0.0;
-    if (A.near) {
+    // HLLC (moving-square solver, Moving_Square.../Solver_Normalized_HLLC_Riemann_Delta.f90:
+    // 207-322), written in differences: with the pair frame e = (x_j - x_i)/d,
+    // t = (-e1, e0), dV = VR0 - VL0 = (u_a - u_b).r/d and tdv = VR1 - VL1 =
+    // (r0 (v_a - v_b) - r1 (u_a - u_b))/d (both independent of the orientation),
+    // C_K = rho_K c_K, the contact speed U* = (VR0 C_L + VL0 C_R + P_L - P_R)/(C_L + C_R):
+    //   sL = U* - VL0 = (C_L dV + dp_ij)/(C_L + C_R), sR = U* - VR0 = (dp_ij - C_R dV)/(C_L + C_R);
+    // the state sampled at the mean normal velocity in one of four regions (taken
+    // as the forward took it; the shock factor is 1, its branch being unreachable
+    // when the pressure follows the density), rho_HLLC - rho0 = rho_K - rho0
+    // [+ rho_K (U* - V_K0)/(S_K - U*)], and v_a - v* = al e + be t.
+    const bool hllc = MS && P.hllc && !A.near;
+    const double sIh = a_lower ? 1.0 : -1.0;
+    double hdVh = 0, htdv = 0, hrL = 0, hrR = 0, hcL = 0, hcR = 0, hCL = 0, hCR = 0, hiC = 0, hsL = 0, hsR = 0;
+    double hal = 0, hbe = 0, he0 = 0, he1 = 0;
+    int hreg = 0;
+    if (hllc) {
+        hdVh = vx * id;
+        htdv = (r0 * du1 - r1 * du0) * id;
+        const double dpp = sIh * dp;
+        hrL = a_lower ? A.rho : B.rho; hrR = a_lower ? B.rho : A.rho;
+        hcL = a_lower ? A.c : B.c; hcR = a_lower ? B.c : A.c;
+        hCL = hrL * hcL; hCR = hrR * hcR; hiC = 1.0 / (hCL + hCR);
+        hsL = (hCL * hdVh + dpp) * hiC;
+        hsR = (dpp - hCR * hdVh) * hiC;
+        const double hh = 0.5 * hdVh;
+        hreg = (-hcL > hh) ? 0 : (hsL - hh >= 0.0 && hh >= -hcL) ? 1 : (hcR >= -hh && hsL - hh <= 0.0) ? 2 : 3;
+        double dH, aI, bI, aJ, bJ;
+        if (hreg == 0) { dH = hrL - P.rho0; aI = 0.0; bI = 0.0; aJ = hdVh; bJ = htdv; }
+        else if (hreg == 1) { dH = hrL - P.rho0 + hrL * hsL / (-hcL - hsL); aI = -hsL; bI = 0.0; aJ = -hsR; bJ = htdv; }
+        else if (hreg == 2) { dH = hrR - P.rho0 + hrR * hsR / (hcR - hsR); aI = -hsL; bI = -htdv; aJ = -hsR; bJ = 0.0; }
+        else { dH = hrR - P.rho0; aI = -hdVh; bI = -htdv; aJ = 0.0; bJ = 0.0; }
+        hal = a_lower ? aI : aJ; hbe = a_lower ? bI : bJ;
+        he0 = -sIh * r0 * id; he1 = -sIh * r1 * id;
+        PA = P.c0sq * dH + P.pb;
+        w0 = hal * he0 - hbe * he1;
+        w1 = hal * he1 + hbe * he0;
+    } else if (A.near) {
         PA = Pbar; w0 = 0.5 * du0 + su; w1 = 0.5 * du1 + sv;
     } else {
         const double m3 = 3.0 * fmax(dU, 0.0);
@@ -382,14 +419,58 @@ __device__ __forceinline__ void rev_pair(const Params& P, const PSide& A, const 
             r0b += 0.5 * psib * sg0; r1b += 0.5 * psib * sg1;
         }
     }
-    du0b += 0.5 * w0b; du1b += 0.5 * w1b;
+    if (!hllc) { du0b += 0.5 * w0b; du1b += 0.5 * w1b; }
     o.avg0 = w0b; o.avg1 = w1b;
     double luib = 0, lujb = 0, lvib = 0, lvjb = 0, Spb = 0, Sub = 0, Svb = 0;
     if (MUSCL) {
         if (a_lower) { luib += w0b; lvib += w1b; } else { lujb -= w0b; lvjb -= w1b; }
     }
-    Pbarb += PAb0;
-    if (!A.near) {
+    double hcab = 0.0, hcbb = 0.0;
+    if (hllc) {
+        // reverse of the HLLC state above, region as taken
+        const double dHb = P.c0sq * PAb0;
+        const double alb = w0b * he0 + w1b * he1, beb = -w0b * he1 + w1b * he0;
+        const double e0b = w0b * hal + w1b * hbe, e1b = -w0b * hbe + w1b * hal;
+        double sLb = 0, sRb = 0, dVb = 0, tdvb = 0, rLb = 0, rRb = 0, cLb = 0, cRb = 0;
+        if (hreg == 0) {
+            rLb += dHb;
+            if (!a_lower) { dVb += alb; tdvb += beb; }
+        } else if (hreg == 1) {
+            const double Dd = -hcL - hsL, iD2 = 1.0 / (Dd * Dd);
+            rLb += dHb * (1.0 + hsL / Dd);
+            sLb += dHb * hrL * (-hcL) * iD2;
+            cLb += dHb * hrL * hsL * iD2;
+            if (a_lower) sLb -= alb; else { sRb -= alb; tdvb += beb; }
+        } else if (hreg == 2) {
+            const double Dd = hcR - hsR, iD2 = 1.0 / (Dd * Dd);
+            rRb += dHb * (1.0 + hsR / Dd);
+            sRb += dHb * hrR * hcR * iD2;
+            cRb -= dHb * hrR * hsR * iD2;
+            if (a_lower) { sLb -= alb; tdvb -= beb; } else sRb -= alb;
+        } else {
+            rRb += dHb;
+            if (a_lower) { dVb -= alb; tdvb -= beb; }
+        }
+        dVb += (sLb * hCL - sRb * hCR) * hiC;
+        const double dppb = (sLb + sRb) * hiC;
+        const double CLb = (sLb * (hdVh - hsL) - sRb * hsR) * hiC;
+        const double CRb = (-sLb * hsL - sRb * (hdVh + hsR)) * hiC;
+        rLb += CLb * hcL; cLb += CLb * hrL;
+        rRb += CRb * hcR; cRb += CRb * hrR;
+        dpb += sIh * dppb;
+        vxb += dVb * id;
+        db -= hdVh * id * dVb;
+        du1b += tdvb * r0 * id; du0b -= tdvb * r1 * id;
+        r0b += tdvb * du1 * id; r1b -= tdvb * du0 * id;
+        db -= htdv * id * tdvb;
+        r0b -= sIh * id * e0b; r1b -= sIh * id * e1b;
+        db += sIh * (r0 * e0b + r1 * e1b) * id * id;
+        if (a_lower) { rab += rLb; rbb += rRb; hcab = cLb; hcbb = cRb; }
+        else { rab += rRb; rbb += rLb; hcab = cRb; hcbb = cLb; }
+    } else {
+        Pbarb += PAb0;
+    }
+    if (!A.near && !hllc) {
         const double kkb = w0b * r0 + w1b * r1;
         r0b += kk * w0b; r1b += kk * w1b;
         dpb += kkb * (0.5 * irbar * ic0) * id;
@@ -456,7 +537,7 @@ __device__ __forceinline__ void rev_pair(const Params& P, const PSide& A, const 
     o.x0 = r0b; o.x1 = r1b;
     o.u = du0b; o.v = du1b;
     o.pa = 0.5 * Pbarb + dpb; o.pb = 0.5 * Pbarb - dpb;
-    o.ca = 0.5 * cbarb; o.cb = 0.5 * cbarb;
+    o.ca = 0.5 * cbarb + hcab; o.cb = 0.5 * cbarb + hcbb;
     o.ra = rab + 0.5 * rbarb; o.rb = rbb + 0.5 * rbarb;
     o.Vb = Vbb;
 }

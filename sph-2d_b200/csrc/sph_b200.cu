@@ -754,7 +754,9 @@ int adj_config_ok(const sph_handle* h, int loss) {
     if (P.ms) {
         // moving-square modified linear solver, Morris laplacian, Euler predictor-corrector
         if (h->cfg.shifting) return SPH_E_CONFIG;
-        if (h->cfg.solver != SPH_SOLVER_MS_MODLR_DELTA || P.laplacian != 1) return SPH_E_CONFIG;
+        if ((h->cfg.solver != SPH_SOLVER_MS_MODLR_DELTA && h->cfg.solver != SPH_SOLVER_MS_HLLC_DELTA) ||
+            P.laplacian != 1)
+            return SPH_E_CONFIG;
         if (h->cfg.integrator != SPH_INTEGRATOR_EULER_PC || h->cfg.periodic) return SPH_E_CONFIG;
     } else {
         if ((h->cfg.solver != SPH_SOLVER_MODLR_DELTA_SPS && h->cfg.solver != SPH_SOLVER_MUSCL_DELTA_SPS) || P.xsph)
