@@ -21,7 +21,7 @@
 // Scope: (1) Taylor-Green: the modified linear Riemann and the MUSCL linear
 // Riemann delta-SPH + SPS solvers, RK4 with the K1 reuse, periodic images
 // (oracle_tangent); (2) moving square:
-// the modified linear Riemann solver with XSPH in the continuity flux, the
+// the modified linear Riemann and the HLLC solvers with XSPH in the continuity flux, the
 // fixed-ghost assignment, the body force and the Euler predictor-corrector with
 // a per-step body motion (oracle_tangent_ms).  Either kernel, with or without
 // renormalisation, with or without shifting in (1) and without in (2), no
@@ -524,7 +524,8 @@ int run(const sph_config& cfg, int n, const T* x0, const T* y0, const T* u0, con
 
 // ---------------------------------------------------------------------------
 // Moving-square step (Moving_Square_Cylinder_Flow/...): the modified linear
-// Riemann solver with the XSPH velocity inside the continuity flux
+// Riemann solver, or the HLLC solver (Solver_Normalized_HLLC_Riemann_Delta.f90),
+// with the XSPH velocity inside the continuity flux
 // (Solver_Normalized_Modified_Linear_Riemann_Delta.f90:100-336), the fixed-ghost
 // assignment (Assign_boundary_particles.f90:611-941, MLS order 1), the body force
 // (Calculate_Body_Force.f90:53-142) and the Euler predictor-corrector with the
@@ -534,6 +535,38 @@ int run(const sph_config& cfg, int n, const T* x0, const T* y0, const T* u0, con
 // ms_riemann_solver / assign_ghosts / body_force / run_step_euler_pc, with the
 // masses as scalars of type T (the ghost masses are interpolated).
 // ---------------------------------------------------------------------------
+// The HLLC pair state of Moving_Square.../Solver_Normalized_HLLC_Riemann_Delta.f90:207-322
+// (the same operations as sph_oracle.cpp's hllc_state), on scalars of type T:
+// branches on the values, derivatives through the taken branch.
+template <class T>
+void hllc_state_t(const sph_config& C, const T vI[2], const T vJ[2], const T vbar[2], const T e[2], const T& rL,
+                  const T& rR, const T& cL, const T& cR, const T& PL, const T& PR, T vs[2], T& Ps) {
+    const T Tm[2][2] = {{e[0], e[1]}, {-e[1], e[0]}};
+    const T VL[2] = {Tm[0][0] * vI[0] + Tm[0][1] * vI[1], Tm[1][0] * vI[0] + Tm[1][1] * vI[1]};
+    const T VR[2] = {Tm[0][0] * vJ[0] + Tm[0][1] * vJ[1], Tm[1][0] * vJ[0] + Tm[1][1] * vJ[1]};
+    const T V0 = Tm[0][0] * vbar[0] + Tm[0][1] * vbar[1];
+    const T Us = (VR[0] * cL * rL + VL[0] * cR * rR + PL - PR) / (rL * cL + rR * cR);
+    const T Pst = (PR * cL * rL + PL * cR * rR - cL * rL * cR * rR * (VR[0] - VL[0])) / (rL * cL + rR * cR);
+    const T rst = (Pst - C.background_p) / C.c0sq + C.rho0;
+    T QL(1.0), QR(1.0);
+    if (!(val(Pst) <= val(PL)) && val(rL) > val(rst)) QL = sqrt((rst / rL) * (Pst - PL) / (rL - rst)) / cL;
+    const T SL = VL[0] - cL * QL;
+    if (!(val(Pst) <= val(PR)) && val(rR) > val(rst)) QR = sqrt((rst / rR) * (Pst - PR) / (rR - rst)) / cR;
+    const T SR = VR[0] + cR * QR;
+    T rH, VH[2];
+    if (val(SL) > val(V0)) { rH = rL; VH[0] = VL[0]; VH[1] = VL[1]; }
+    else if (val(Us) >= val(V0) && val(V0) >= val(SL)) {
+        const T q = rL * ((SL - VL[0]) / (SL - Us));
+        rH = q; VH[0] = (Us * q) / rH; VH[1] = (VL[1] * q) / rH;
+    } else if (val(SR) >= val(V0) && val(V0) >= val(Us)) {
+        const T q = rR * ((SR - VR[0]) / (SR - Us));
+        rH = q; VH[0] = (Us * q) / rH; VH[1] = (VR[1] * q) / rH;
+    } else { rH = rR; VH[0] = VR[0]; VH[1] = VR[1]; }
+    vs[0] = Tm[0][0] * VH[0] + Tm[1][0] * VH[1];
+    vs[1] = Tm[0][1] * VH[0] + Tm[1][1] * VH[1];
+    Ps = C.c0sq * (rH - C.rho0) + C.background_p;
+}
+
 template <class T>
 struct MSParts {
     std::vector<T> x, y, u, v, rho, mass;
@@ -717,14 +750,22 @@ struct MSModel {
             const T r2 = dx0[k] * dx0[k] + dx1[k] * dx1[k];
             const T d = sqrt(r2);
             const T e0 = -dx0[k] / d, e1 = -dx1[k] / d;
-            const T UL = P.u[i] * e0 + P.v[i] * e1, UR = P.u[j] * e0 + P.v[j] * e1;
-            const T Ubar = (UL + UR) / 2.0;
-            const T Us = Ubar + 0.5 * (p[i] - p[j]) / (rbar * K.sqrt_c0);
-            const T vs0 = (Us - Ubar) * e0 + vbar0, vs1 = (Us - Ubar) * e1 + vbar1;
-            const T dU = UL - UR;
-            const T m3 = val(dU) > 0.0 ? 3.0 * dU : T(0.0);
-            const T bR = val(m3) < val(cbar) ? m3 : cbar;
-            const T Ps = Pbar + 0.5 * bR * rbar * dU;
+            T vs0, vs1, Ps;
+            if (C.solver == SPH_SOLVER_MS_HLLC_DELTA) {
+                const T vI[2] = {P.u[i], P.v[i]}, vJ[2] = {P.u[j], P.v[j]}, vb[2] = {vbar0, vbar1}, ee[2] = {e0, e1};
+                T vs[2];
+                hllc_state_t(C, vI, vJ, vb, ee, ri, rj, c[i], c[j], p[i], p[j], vs, Ps);
+                vs0 = vs[0]; vs1 = vs[1];
+            } else {
+                const T UL = P.u[i] * e0 + P.v[i] * e1, UR = P.u[j] * e0 + P.v[j] * e1;
+                const T Ubar = (UL + UR) / 2.0;
+                const T Us = Ubar + 0.5 * (p[i] - p[j]) / (rbar * K.sqrt_c0);
+                vs0 = (Us - Ubar) * e0 + vbar0; vs1 = (Us - Ubar) * e1 + vbar1;
+                const T dU = UL - UR;
+                const T m3 = val(dU) > 0.0 ? 3.0 * dU : T(0.0);
+                const T bR = val(m3) < val(cbar) ? m3 : cbar;
+                Ps = Pbar + 0.5 * bR * rbar * dU;
+            }
             const T vdi0 = P.u[i] - vs0 + avg[0][i] - avg[0][j], vdi1 = P.v[i] - vs1 + avg[1][i] - avg[1][j];
             const T vdj0 = P.u[j] - vs0 + avg[0][j] - avg[0][i], vdj1 = P.v[j] - vs1 + avg[1][j] - avg[1][i];
             const T tmi = vdi0 * ni0[k] + vdi1 * ni1[k];
@@ -925,7 +966,8 @@ int oracle_tangent_ms(const sph_config* cfg, int n, const double* pos, const dou
                       double* out) {
     if (!cfg || !pos || !vel || !rho || !mass || !type || !itype || !motion || !out || n <= 0 || nsteps <= 0)
         return SPH_E_ARG;
-    if (cfg->solver != SPH_SOLVER_MS_MODLR_DELTA || cfg->integrator != SPH_INTEGRATOR_EULER_PC || cfg->shifting ||
+    if ((cfg->solver != SPH_SOLVER_MS_MODLR_DELTA && cfg->solver != SPH_SOLVER_MS_HLLC_DELTA) ||
+        cfg->integrator != SPH_INTEGRATOR_EULER_PC || cfg->shifting ||
         cfg->mls_order != 0 || cfg->laplacian != 1 || cfg->free_surface || cfg->periodic)
         return SPH_E_CONFIG;
     for (int i = 0; i < n; ++i)

@@ -2,8 +2,10 @@
 sph_adjoint_backward / sph_adjoint_motion_gradient) against central finite
 differences of the FP64 forward run on the GPU.
 
-The case: the moving-square modified linear Riemann solver (XSPH velocities in
-the continuity flux, Morris laplacian) with the Euler predictor-corrector, the
+The case: the moving-square modified linear Riemann solver, and the HLLC solver
+(Solver_Normalized_HLLC_Riemann_Delta.f90, its state reversed on the sampled
+region and wave speeds the forward took), with XSPH velocities in the
+continuity flux, the Morris laplacian and the Euler predictor-corrector, the
 library's ghost assignment at every RHS (Shepard interpolation onto the wall
 and body ghosts, mirrored wall velocities, the shock-release branch) and the
 body moved by a per-step schedule.  Losses: the drag impulse sum_s dt F_x and
@@ -29,8 +31,11 @@ NSTEPS = 16
 REL_TOL = 1e-4
 
 
-def _case(jitter=0.05, seed=41, ghost_assign=1):
-    case, ity = S.make_moving_square(solver=S.SOLVER_MS_MODLR_DELTA, jitter=jitter, seed=seed)
+SOLVERS = [S.SOLVER_MS_MODLR_DELTA, S.SOLVER_MS_HLLC_DELTA]
+
+
+def _case(jitter=0.05, seed=41, ghost_assign=1, solver=S.SOLVER_MS_MODLR_DELTA):
+    case, ity = S.make_moving_square(solver=solver, jitter=jitter, seed=seed)
     water = np.r_[case.type, case.type] == S.TYPE_WATER
     case.vel = case.vel + np.where(water, S.fourier_perturbation(case.pos, n_modes=6, amp=0.2, seed=seed), 0.0)
     cfg = case.cfg
@@ -86,10 +91,12 @@ def test_drag_loss_is_the_sum_of_the_step_forces(lib):
     assert L != 0.0
 
 
-@pytest.mark.parametrize("loss", [S.LOSS_DRAG, S.LOSS_KINETIC_ENERGY])
-def test_motion_gradient_matches_central_differences(lib, loss):
+@pytest.mark.parametrize("solver,loss", [(S.SOLVER_MS_MODLR_DELTA, S.LOSS_DRAG),
+                                         (S.SOLVER_MS_MODLR_DELTA, S.LOSS_KINETIC_ENERGY),
+                                         (S.SOLVER_MS_HLLC_DELTA, S.LOSS_DRAG)])
+def test_motion_gradient_matches_central_differences(lib, solver, loss):
     """dL/d(amplitude) of the impulsive start and dL/d(Fourier coefficients)."""
-    case, ity, lab, dt = _case()
+    case, ity, lab, dt = _case(solver=solver)
     period = NSTEPS * dt
     coeffs = np.array([0.5, 0.4, -0.2, 0.15, 0.1])
     motion, jac = S.body_motion_schedule(coeffs, NSTEPS, dt, period=period)
@@ -108,8 +115,9 @@ def test_motion_gradient_matches_central_differences(lib, loss):
         _check(gc[k], fd, f"motion coefficient {k}")
 
 
-def test_drag_gradient_velocity_and_viscosity(lib):
-    case, ity, lab, dt = _case()
+@pytest.mark.parametrize("solver", SOLVERS)
+def test_drag_gradient_velocity_and_viscosity(lib, solver):
+    case, ity, lab, dt = _case(solver=solver)
     motion, _ = S.body_motion_schedule([1.0], NSTEPS, dt)
     L, g, gm, _, _ = _grad(case, ity, lab, dt, motion, S.LOSS_DRAG)
     n = case.n
@@ -166,7 +174,7 @@ def test_moving_square_adjoint_independent_of_checkpoint_interval(lib):
 def test_moving_square_adjoint_rejects_unsupported(lib):
     case, ity, lab, dt = _case()
     cfg = case.cfg.copy()
-    cfg.solver = S.SOLVER_MS_HLLC_DELTA
+    cfg.laplacian = 0          # the Monaghan-form laplacian has no reverse
     with _sim(case, ity, lab, cfg) as sim:
         with pytest.raises(S.SphError) as e:
             sim.adjoint_forward(2, dt, loss=S.LOSS_DRAG)
@@ -182,14 +190,14 @@ def test_moving_square_adjoint_rejects_unsupported(lib):
         assert e.value.code == -7
 
 
+@pytest.mark.parametrize("solver", SOLVERS)
 @pytest.mark.parametrize("loss", [S.LOSS_DRAG, S.LOSS_KINETIC_ENERGY])
-def test_moving_square_adjoint_matches_cpu_tangent_linear_reference(lib, oracle, loss):
+def test_moving_square_adjoint_matches_cpu_tangent_linear_reference(lib, oracle, loss, solver):
     """g.delta from the GPU adjoint against the FP64 CPU tangent-linear model of
     the same steps (oracle/sph_tangent.cpp, oracle_tangent_ms) along directions
     in the initial velocity, position and density, the viscosity and the body
     motion: both are exact derivatives of the same discrete map (1e-8)."""
-    case, ity = S.make_moving_square(dx=0.1, lx=2.0, ly=1.0, D=0.4, solver=S.SOLVER_MS_MODLR_DELTA,
-                                     jitter=0.05, seed=8)
+    case, ity = S.make_moving_square(dx=0.1, lx=2.0, ly=1.0, D=0.4, solver=solver, jitter=0.05, seed=8)
     water = np.r_[case.type, case.type] == S.TYPE_WATER
     case.vel = case.vel + np.where(water, S.fourier_perturbation(case.pos, n_modes=4, amp=0.2, seed=8), 0.0)
     cfg = case.cfg

@@ -12,9 +12,11 @@ import sph_b200 as S
 NSTEPS = 5
 
 
-def _case():
-    case, ity = S.make_moving_square(dx=0.1, lx=2.0, ly=1.0, D=0.4, solver=S.SOLVER_MS_MODLR_DELTA,
-                                     jitter=0.05, seed=7)
+SOLVERS = [S.SOLVER_MS_MODLR_DELTA, S.SOLVER_MS_HLLC_DELTA]
+
+
+def _case(solver=S.SOLVER_MS_MODLR_DELTA):
+    case, ity = S.make_moving_square(dx=0.1, lx=2.0, ly=1.0, D=0.4, solver=solver, jitter=0.05, seed=7)
     water = np.r_[case.type, case.type] == S.TYPE_WATER
     case.vel = case.vel + np.where(water, S.fourier_perturbation(case.pos, n_modes=4, amp=0.2, seed=7), 0.0)
     cfg = case.cfg
@@ -32,8 +34,9 @@ def _tangent(oracle, case, ity, lab, dt, motion, loss, cfg=None, **d):
                              ity, lab, 0.0, NSTEPS, dt, motion, loss, **d)
 
 
-def test_tangent_ms_value_path_reproduces_the_oracle(oracle):
-    case, ity, lab, dt, motion = _case()
+@pytest.mark.parametrize("solver", SOLVERS)
+def test_tangent_ms_value_path_reproduces_the_oracle(oracle, solver):
+    case, ity, lab, dt, motion = _case(solver)
     ke, _ = _tangent(oracle, case, ity, lab, dt, motion, S.LOSS_KINETIC_ENERGY)
     drag, _ = _tangent(oracle, case, ity, lab, dt, motion, S.LOSS_DRAG)
     sim = oracle.OracleSim(case.cfg, case.pos, case.vel, case.rho, case.mass, case.type)
@@ -52,9 +55,10 @@ def test_tangent_ms_value_path_reproduces_the_oracle(oracle):
     assert drag != 0.0
 
 
+@pytest.mark.parametrize("solver", SOLVERS)
 @pytest.mark.parametrize("loss", [S.LOSS_DRAG, S.LOSS_KINETIC_ENERGY])
-def test_tangent_ms_matches_its_central_differences(oracle, loss):
-    case, ity, lab, dt, motion = _case()
+def test_tangent_ms_matches_its_central_differences(oracle, loss, solver):
+    case, ity, lab, dt, motion = _case(solver)
     rng = np.random.default_rng(2)
     dmo = np.zeros_like(motion)
     dmo[:, 0] = rng.standard_normal(NSTEPS)
@@ -89,6 +93,6 @@ def test_tangent_ms_matches_its_central_differences(oracle, loss):
 def test_tangent_ms_rejects_configurations_outside_its_scope(oracle):
     case, ity, lab, dt, motion = _case()
     cfg = case.cfg.copy()
-    cfg.solver = S.SOLVER_MS_HLLC_DELTA
+    cfg.shifting = 1
     with pytest.raises(RuntimeError):
         _tangent(oracle, case, ity, lab, dt, motion, S.LOSS_DRAG, cfg=cfg)
