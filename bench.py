@@ -182,6 +182,12 @@ PASS_C_BYTES_MIXED = 16 + 32 + 16 + 48 + 16 + 1 + 4 + 8 + 8
 PASS_C_BYTES_FP64 = 16 + 32 + 32 + 96 + 32 + 1 + 8 + 16 + 16 + 16
 
 
+def passes(tm, steps: int) -> dict:
+    """Device time per step of each phase of the step (sph_timings)."""
+    return {"images": tm.images_ms / steps, "sort_lists": tm.sort_ms / steps, "pass_a": tm.pass_a_ms / steps,
+            "surface": tm.surface_ms / steps, "pass_c": tm.pass_c_ms / steps, "update": tm.update_ms / steps}
+
+
 def run_native(args, rank, world, local):
     import torch
     torch.cuda.set_device(local)
@@ -343,6 +349,7 @@ def run_native(args, rank, world, local):
         "config": bench_config(n_side, world),
         "images": int(mixed["diag"].n_images),
         "fp64": {"value": value64, "unit": UNIT, "ms_per_step": fp64["dev_ms"] / steps,
+                 "passes_ms_per_step": passes(fp64["tm"], steps),
                  "mixed_over_fp64": value / value64},
         "accuracy": accuracy,
         "adjoint_over_forward": adj["adjoint_over_forward"] if adj else None,
@@ -352,10 +359,7 @@ def run_native(args, rank, world, local):
         "plain_method": plain,
         "lattice_exact": exact,
         "output_streaming": streaming,
-        "passes_ms_per_step": {
-            "images": tm.images_ms / steps, "sort_lists": tm.sort_ms / steps,
-            "pass_a": tm.pass_a_ms / steps, "surface": tm.surface_ms / steps,
-            "pass_c": tm.pass_c_ms / steps, "update": tm.update_ms / steps},
+        "passes_ms_per_step": passes(tm, steps),
         "roofline": roof,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
