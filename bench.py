@@ -668,7 +668,9 @@ def moving_square_report(S, steps: int = 200, warmup: int = 3):
             sim.set_time(0.0)
             sim.time_iteration(warmup, dt)
             sim.reset_timings()
-            d = sim.time_iteration(steps, dt)
+            sim.time_iteration(steps // 2, dt)
+            vel[name + "_half"] = sim.get_state()[1]
+            d = sim.time_iteration(steps - steps // 2, dt)
             tm = sim.timings()
             vel[name] = sim.get_state()[1]
         out[name] = {"particle_steps_per_s": case.n * steps / (tm.total_ms / 1e3),
@@ -679,6 +681,9 @@ def moving_square_report(S, steps: int = 200, warmup: int = 3):
     dv = vel["mixed"][water] - vel["fp64"][water]
     out["mixed_over_fp64"] = out["mixed"]["particle_steps_per_s"] / out["fp64"]["particle_steps_per_s"]
     out["velocity_l2_mixed_vs_fp64"] = float(np.linalg.norm(dv) / np.linalg.norm(vel["fp64"][water]))
+    dvh = vel["mixed_half"][water] - vel["fp64_half"][water]
+    out["velocity_l2_mixed_vs_fp64_half"] = float(np.linalg.norm(dvh) / np.linalg.norm(vel["fp64_half"][water]))
+    out["velocity_l2_steps"] = [warmup + steps // 2, warmup + steps]
     out["case"] = (f"moving square D=1 in [0,10]x[0,5], dx=D/100 ({n} particles incl. ghosts), HLLC + delta-SPH, "
                    f"Re=100, impulsive U=1, ghost assignment, body force every step, Euler PC, shifting, MLS every "
                    f"40 steps; {steps} steps after {warmup}, device-timed")
