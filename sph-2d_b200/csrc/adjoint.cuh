@@ -237,7 +237,7 @@ __device__ __forceinline__ void muscl_limiter_rev(double di, double dj, double d
 // 470-502): the limited reconstructions of p, u, v enter U_L - U_R, P_L - P_R and
 // this side's v - v*; a_lower: a is the reference's pair index i (the lower id),
 // which fixes the limiter's sides.
-template <bool MS = false, bool MUSCL = false>
+template <bool MS = false, bool MUSCL = false, bool HLLC = false>
 __device__ __forceinline__ void rev_pair(const Params& P, const PSide& A, const PSide& B, double lr, double l0,
                                          double l1, PBar& o, bool a_lower = true) {
     const double r0 = A.x.x - B.x.x, r1 = A.x.y - B.x.y;
@@ -291,7 +291,7 @@ __device__ __forceinline__ void rev_pair(const Params& P, const PSide& A, const 
     // as the forward took it; the shock factor is 1, its branch being unreachable
     // when the pressure follows the density), rho_HLLC - rho0 = rho_K - rho0
     // [+ rho_K (U* - V_K0)/(S_K - U*)], and v_a - v* = al e + be t.
-    const bool hllc = MS && P.hllc && !A.near;
+    const bool hllc = MS && HLLC && !A.near;
     const double sIh = a_lower ? 1.0 : -1.0;
     double hdVh = 0, htdv = 0, hrL = 0, hrR = 0, hcL = 0, hcR = 0, hCL = 0, hCR = 0, hiC = 0, hsL = 0, hsR = 0;
     double hal = 0, hbe = 0, he0 = 0, he1 = 0;
@@ -559,7 +559,9 @@ __device__ __forceinline__ void rev_pair(const Params& P, const PSide& A, const 
 #define SPH_ADJ_C_MUSCL_MIN_BLOCKS 2 // the limiter reverses need more than 168
 #endif
 constexpr int kAdjLanes = SPH_ADJ_LANES;     // 2 or 4
-template <typename R, bool MS = false, bool MUSCL = false>
+// HLLC: the moving-square HLLC solver (a variant of its own, so that the
+// modified solver's reverse carries none of its registers).
+template <typename R, bool MS = false, bool MUSCL = false, bool HLLC = false>
 __global__ void __launch_bounds__(kAdjThreads, MUSCL ? SPH_ADJ_C_MUSCL_MIN_BLOCKS : SPH_ADJ_C_MIN_BLOCKS) k_adj_c(Params P, Sorted<R> D, Adj A, const double* lr,
                                                         const double2* la, double* nu_part) {
     __shared__ double red[kAdjThreads];
@@ -592,7 +594,7 @@ __global__ void __launch_bounds__(kAdjThreads, MUSCL ? SPH_ADJ_C_MUSCL_MIN_BLOCK
             const PSide Sa = load_side<R, MS, MUSCL>(D, acc_at);
             const PSide Sb = load_side<R, MS, MUSCL>(D, other);
             PBar o;
-            rev_pair<MS, MUSCL>(P, Sa, Sb, l_r, l_a.x, l_a.y, o, role ? !c_lower : c_lower);
+            rev_pair<MS, MUSCL, HLLC>(P, Sa, Sb, l_r, l_a.x, l_a.y, o, role ? !c_lower : c_lower);
             v[0] += sg * o.x0; v[1] += sg * o.x1; v[2] += sg * o.u; v[3] += sg * o.v;
             v[4] += role ? o.pb : o.pa;
             v[5] += role ? o.cb : o.ca;

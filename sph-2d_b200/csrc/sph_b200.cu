@@ -1175,7 +1175,11 @@ int adj_rhs_ms(sph_handle* h, const Sorted<R>& V, int k, int pred, bool drag, in
     launch_surface<R>(P, V, h->stream);
     tic(h, PH_ADJ);
     CK(cudaMemsetAsync(V.nflag, 0, (size_t)P.n_tot, h->stream));
-    k_adj_c<R, true><<<nbc, kAdjThreads, 0, h->stream>>>(P, V, A, A.lr[k], A.la[k], A.nu_part + (size_t)k * nbc);
+    if (P.hllc)
+        k_adj_c<R, true, false, true><<<nbc, kAdjThreads, 0, h->stream>>>(P, V, A, A.lr[k], A.la[k],
+                                                                          A.nu_part + (size_t)k * nbc);
+    else
+        k_adj_c<R, true><<<nbc, kAdjThreads, 0, h->stream>>>(P, V, A, A.lr[k], A.la[k], A.nu_part + (size_t)k * nbc);
     if (drag) {
         double* part = A.nu_part + (size_t)4 * nbc;
         k_mark_body_nbrs<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, V);
