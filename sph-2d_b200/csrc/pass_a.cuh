@@ -270,6 +270,9 @@ __global__ void k_near(Params P, Sorted<R> D) {
 // The free-surface test and the near-surface flags of one RHS.
 template <typename R>
 void launch_surface(const Params& P, const Sorted<R>& D, cudaStream_t st) {
+    // without free-surface detection pass A marks no candidate, so both kernels
+    // would only read flags
+    if (!P.free_surface) return;
     int nb = (P.n_tot + 127) / 128;
     if (nb > 148 * 8) nb = 148 * 8;
     if (nb == 0) return;

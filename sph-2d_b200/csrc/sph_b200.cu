@@ -451,7 +451,7 @@ int rhs(sph_handle* h, int last) {
         h->launches += 1;
     }
     CK(cudaGetLastError());
-    h->launches += 4;
+    h->launches += P.free_surface ? 4 : 2;
     if (P.has_body && (last || h->bf_every_rhs)) {
         const int nbf = blocks(P.n_tot, kRedThreads);      // <= blocks(cap_tot), the partial buffer size
         double* fin = h->d_bf + (size_t)6 * blocks(h->cap_tot, kRedThreads);
@@ -1118,7 +1118,7 @@ int adj_step(sph_handle* h, bool first, int j) {
         launch_surface<R>(P, V, h->stream);
         tic(h, PH_ADJ);
         k_shift_sum<R><<<nb, 256, 0, h->stream>>>(P, V, A);
-        h->launches += 4;
+        h->launches += P.free_surface ? 4 : 2;
     }
     tic(h, PH_ADJ);
     k_adj_stage3<R><<<nb, 256, 0, h->stream>>>(P, D, A, dt, shift ? 1 : 0);
