@@ -77,6 +77,8 @@ struct Adj {
     double* sm;          // adjoint of the mass of the state the reversed RHS was evaluated on
     double4* glam;       // ghost Shepard multipliers (p, u, v, m) / sum W
     double* glamw;       //   and of the normalisation
+    double4* gint;       // the forward's interpolated ghost (p, u, v, m) of the reversed RHS
+    double* gsw;         //   and its weight sum sum W V
     double* mo_part;     // per-block partials of the body-motion adjoints
     double* g_motion;    // [4 nsteps] dL/d(body velocity, body acceleration) of each step
 };
@@ -1373,26 +1375,11 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_ghost_lambda(Params P, Sort
         const int s = D.slot_of[ghost_ids[wg]];
         const bool body = D.itype[s] == SPH_TYPE_BODY;
         const double gxe = P.grav[0] + (body ? bax : 0.0), gye = P.grav[1] + (body ? bay : 0.0);
-        double sw = 0.0, sp = 0.0, su = 0.0, sv = 0.0, sm = 0.0;
-        int cnt = 0;
-        ghost_visit_warp(P, D, s, [&](int b, double dx, double dy, double, double w) {
-            const double4 kb = D.kin[b];
-            const double mb = D.mass[b];
-            const double W = w * (mb / kb.z);
-            sw += W;
-            sp += kb.w * W + kb.z * W * (gxe * dx + gye * dy);
-            su += kb.x * W;
-            sv += kb.y * W;
-            sm += mb * W;
-            ++cnt;
-        });
-        sw = warp_sum(sw); sp = warp_sum(sp); su = warp_sum(su); sv = warp_sum(sv); sm = warp_sum(sm);
-        cnt = warp_sum(cnt);
-        double pint = 0.0, uint = 0.0, vint = 0.0, m = 0.0;
-        if (cnt >= 3) {
-            const double inv = 1.0 / sw;
-            pint = sp * inv; uint = su * inv; vint = sv * inv; m = sm * inv;
-        }
+        // the interpolated values and the weight sum, as the forward assignment of
+        // this RHS formed them (k_assign_ghosts kept them in gint / gsw)
+        const double4 gi = A.gint[s];
+        const double sw = A.gsw[s];
+        const double pint = gi.x, uint = gi.y, vint = gi.z, m = gi.w;
         double lp = 0, lu = 0, lv = 0, lm = 0, lw = 0, xs0 = 0, xs1 = 0;
         if (m != 0.0) {
             const double2 ou = A.su[s];

@@ -926,6 +926,7 @@ int adj_prepare_ctx(sph_handle* h, const sph_adj_config* ac) {
         if ((rc = adj_alloc(X, &A.lg[0], nt)) || (rc = adj_alloc(X, &A.lg[1], nt)) ||
             (rc = adj_alloc(X, &A.lk_g, nh)) || (rc = adj_alloc(X, &A.gavg, nt)) || (rc = adj_alloc(X, &A.sm, nt)) ||
             (rc = adj_alloc(X, &A.glam, nt)) || (rc = adj_alloc(X, &A.glamw, nt)) ||
+            (rc = adj_alloc(X, &A.gint, nt)) || (rc = adj_alloc(X, &A.gsw, nt)) ||
             // per-block partials: k_adj_ghost_lambda (4 per block of 4 ghosts), k_adj_body_pos (2 per block of 256)
             (rc = adj_alloc(X, &A.mo_part, std::max((size_t)4 * blocks((long long)nh * 32, kAdjThreads),
                                                     (size_t)2 * blocks((long long)nt, 256)))) ||
@@ -1168,7 +1169,7 @@ int adj_rhs_ms(sph_handle* h, const Sorted<R>& V, int k, int pred, bool drag, in
     if (ghosts) {
         k_assign_ghosts<R><<<blocks((long long)h->n_ghost * 32, 128), 128, 0, h->stream>>>(
             P, V, h->d_ghost_ids, h->n_ghost, h->t_phys, h->body_vel[0], h->body_vel[1], h->body_acc[0],
-            h->body_acc[1]);
+            h->body_acc[1], A.gint, A.gsw);
         h->launches += 1;
     }
     launch_pass_a<R, false>(P, V, nb, h->stream);

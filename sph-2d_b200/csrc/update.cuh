@@ -373,8 +373,11 @@ __device__ __forceinline__ int warp_sum(int v) {
 // One warp per ghost (ghost_ids: the host ghosts in id order, n_ghost of them),
 // the lanes splitting the neighbours; the sums are reduced in a fixed order.
 template <typename R>
+// gint / gsw (may be null): the interpolated (p, u, v, m) and the weight sum
+// sum W V of each ghost slot, kept for the reverse (k_adj_ghost_lambda).
 __global__ void k_assign_ghosts(Params P, Sorted<R> D, const int* ghost_ids, int n_ghost, double t, double bvx,
-                                double bvy, double bax, double bay) {
+                                double bvy, double bax, double bay, double4* gint = nullptr,
+                                double* gsw = nullptr) {
     const int wg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (wg >= n_ghost) return;                       // whole warps
     const int s = D.slot_of[ghost_ids[wg]];
@@ -401,6 +404,10 @@ __global__ void k_assign_ghosts(Params P, Sorted<R> D, const int* ghost_ids, int
     if (cnt >= 3) {
         const double inv = 1.0 / sw;
         pint = sp * inv; uint = su * inv; vint = sv * inv; m = sm * inv;
+    }
+    if (gint) {
+        gint[s] = make_double4(pint, uint, vint, m);
+        gsw[s] = sw;
     }
     double u, v, p = 0.0;
     if (body) {
