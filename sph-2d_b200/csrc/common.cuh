@@ -100,21 +100,7 @@ __device__ __forceinline__ bool in_support(const Params& P, double dx, double dy
 __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
 
-// TwoSum (Knuth) compensated accumulation for the FP32 sums.
-struct CSum {
-    float s, c;
-    __device__ __forceinline__ void init() { s = 0.f; c = 0.f; }
-    __device__ __forceinline__ void add(float x) {
-        float t = __fadd_rn(s, x);
-        float bp = __fsub_rn(t, s);
-        float e = __fadd_rn(__fsub_rn(s, __fsub_rn(t, bp)), __fsub_rn(x, bp));
-        s = t;
-        c = __fadd_rn(c, e);
-    }
-    __device__ __forceinline__ float val() const { return __fadd_rn(s, c); }
-};
-
-// Plain accumulator for the FP64 path (same interface).
+// Plain accumulator for the FP64 path.
 struct DSum {
     double s;
     __device__ __forceinline__ void init() { s = 0.0; }
@@ -122,9 +108,19 @@ struct DSum {
     __device__ __forceinline__ double val() const { return s; }
 };
 
+// The mixed path's sums: FP32 terms added in FP64 (one conversion and one FP64
+// add per term; a compensated FP32 TwoSum takes seven FP32 operations for a
+// sum of about the same accuracy).
+struct WSum {
+    double s;
+    __device__ __forceinline__ void init() { s = 0.0; }
+    __device__ __forceinline__ void add(float x) { s += (double)x; }
+    __device__ __forceinline__ float val() const { return (float)s; }
+};
+
 template <typename R> struct Acc;
 template <> struct Acc<double> { using T = DSum; };
-template <> struct Acc<float> { using T = CSum; };
+template <> struct Acc<float> { using T = WSum; };
 
 // compute_kernel for one pair: W and grad_a W(x_a - x_b) = f(d) (x_a - x_b).
 // Improved Gaussian: Taylor_Green_Vortex/compute_kernel.f90:122-134.

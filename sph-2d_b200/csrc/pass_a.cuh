@@ -183,7 +183,9 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? SPH_PASS_A_F32_BLOCKS : 
     }
     D.nb1[a] = mk4<R>(txx, txy, tyy, gr[0]);
     D.nb2[a] = mk4<R>(gr[1], gr[2], gr[3], gr[4]);
-    D.nb3[a] = mk4<R>(gr[5], gr[6], gr[7], R(0));
+    // FP32 records: w = 1/rho (rounded FP32 reciprocal of the FP32 density),
+    // which pass C reads instead of forming it for every pair
+    D.nb3[a] = mk4<R>(gr[5], gr[6], gr[7], F32 ? (R)__frcp_rn((float)rho_a) : R(0));
     const R fv = fra;
     D.fra_v[a] = fv;
     uint8_t fl = 0;

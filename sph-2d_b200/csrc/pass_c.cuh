@@ -23,8 +23,8 @@
 // orders agree to round-off.
 //
 // Precision: R = double is the FP64 path.  R = float is the mixed path: FP32
-// pair arithmetic with reciprocal/rsqrt instead of divisions, compensated
-// (TwoSum) sums for the acceleration and the density rate, and the shifting
+// pair arithmetic with reciprocal/rsqrt instead of divisions, FP64 sums of
+// the FP32 terms for the acceleration and the density rate, and the shifting
 // sum in FP64 (its terms are O(h/10) each and cancel to a displacement that
 // is orders of magnitude smaller, so FP32 rounding there would inject position
 // noise every step into the unstable lattice modes the shifting excites).
@@ -53,6 +53,24 @@ __device__ __forceinline__ void muscl_limiter(R di, R dj, R dij, R& li, R& lj) {
     const R off = dij * R(0);
     li = big ? (first ? half : off) : lim;
     lj = big ? (first ? off : half) : lim;
+}
+
+// The FP32 form: multiplying by s = +-1 is a flip of the sign bit (taken from
+// dj), and s dj = |dj|.  dj = +0 takes s = +1 instead of -1; both give m = 0,
+// big = false and li = lj = 0, so the values are those of the form above
+// (a zero increment may carry the other sign).
+template <>
+__device__ __forceinline__ void muscl_limiter<float>(float di, float dj, float dij, float& li, float& lj) {
+    const float b = 1.3f;
+    const unsigned sb = __float_as_uint(dj) & 0x80000000u;
+    const float sdi = __uint_as_float(__float_as_uint(di) ^ sb), sdj = fabsf(dj);
+    const float m = fmaxf(0.f, fmaxf(fminf(b * sdi, sdj), fminf(sdi, b * sdj)));
+    const float half = 0.5f * dij;
+    const bool big = m > __uint_as_float(__float_as_uint(half) ^ sb) && m > 0.f;
+    const bool first = sdi > sdj;
+    const float lim = __uint_as_float(__float_as_uint(m) ^ sb);
+    li = big ? (first ? half : 0.f) : lim;
+    lj = big ? (first ? 0.f : half) : lim;
 }
 
 // Reciprocal and quotient in the pair loop, correctly rounded in both
@@ -134,7 +152,9 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIF
     const R dla_dh = (R)(P.delta * P.h);
     const R dla_h = (R)(P.delta_alpha * P.h);
     const R eps2 = (R)(2.0 * P.eps);
-    const R inv_rho_a = rcp(rho_a);
+    // 1/rho: the FP32 MUSCL records carry it (nb3.w, the same rounded reciprocal)
+    constexpr bool RREC = F32 && MUSCL;
+    const R inv_rho_a = RREC ? (R)S.nb3.w : rcp(rho_a);
     const R rho0_over_rho_a = (R)P.rho0 * inv_rho_a;
 
     A cont, accx, accy;
@@ -260,7 +280,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIF
             // (DelPhi_i, DelPhi_j) = (-ga, gb) when a is pair_i and (gb, -ga) when it is
             // pair_j.  The products are rounded separately and fused in a fixed order,
             // so both members of the pair form the same bits.
-            // nb2 = (grad rho y, grad p x, grad p y, grad u x), nb3 = (grad u y, grad v x, grad v y, 0)
+            // nb2 = (grad rho y, grad p x, grad p y, grad u x), nb3 = (grad u y, grad v x, grad v y, 1/rho)
             auto half_dot = [&](R g0, R g1) { return R(0.5) * fma(g1, xab1, mul_rn(g0, xab0)); };
             const R gpa = half_dot(S.nb2.y, S.nb2.z), gpb = half_dot(T.nb2.y, T.nb2.z);
             const R gua = half_dot(S.nb2.w, S.nb3.x), gub = half_dot(T.nb2.w, T.nb3.x);
@@ -383,7 +403,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIF
         // continuity (:360-369)
         R dr = R(2) * rho_a * Vb * (sgn * (wa0 * nd0 + wa1 * nd1));
         // pressure force (:374-388)
-        const R rho_ij = inv_rho_a * rcp(rho_b);
+        const R rho_ij = inv_rho_a * (RREC ? (R)T.nb3.w : rcp(rho_b));
         const R fp = R(-2) * PA * rho_ij * mb;
         R tx = fp * nd0, ty = fp * nd1;
         // artificial viscosity (:392-417)

@@ -135,7 +135,7 @@ struct Sorted {
     V4* aux;          // m, V = m/rho, c, smass                      -- neighbour record 2
     V4* nb1;          // tau_xx, tau_xy, tau_yy, grad rho x          -- neighbour record 3
     V4* nb2;          // grad rho y, grad p x, grad p y, grad u x     -- neighbour record 4
-    V4* nb3;          // grad u y, grad v x, grad v y, 0             -- neighbour record 5 (MUSCL)
+    V4* nb3;          // grad u y, grad v x, grad v y, 1/rho (FP32) or 0 -- neighbour record 5 (MUSCL)
     V4* binv;         // B^-1 (11, 12, 21, 22) in the pair precision
     double4* binv64;  // B^-1 in FP64 (applied to the FP64 shifting sum)
     R* fra_v;
