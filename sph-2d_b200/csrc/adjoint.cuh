@@ -153,18 +153,19 @@ __device__ __forceinline__ PSide load_side(const Sorted<R>& D, int s) {
     o.c = (double)ax.z;
     o.sm = (double)ax.w;
     const typename VT<R>::V4 n1 = D.nb1[s];
-    o.t0 = (double)n1.x; o.t1 = (double)n1.y; o.t2 = (double)n1.z; o.g0 = (double)n1.w;
-    o.g1 = (double)D.nb2[s].x;
+    const double gs = grad_scale<R>();
+    o.t0 = (double)n1.x; o.t1 = (double)n1.y; o.t2 = (double)n1.z; o.g0 = gs * n1.w;
+    o.g1 = gs * D.nb2[s].x;
     o.bi = D.binv64[s];
     o.water = D.type[s] == SPH_TYPE_WATER;
     o.near = (D.flags[s] & 2) != 0;
     o.ax = o.ay = 0.0;
     o.gp0 = o.gp1 = o.gu0 = o.gu1 = o.gv0 = o.gv1 = 0.0;
     if (MUSCL) {
-        // nb2 = (grad rho y, grad p x, grad p y, grad u x), nb3 = (grad u y, grad v x, grad v y, 0)
+        // nb2 = (grad rho y, grad p x, grad p y, grad u x), nb3 = (grad u y, grad v x, grad v y, .)
         const typename VT<R>::V4 n2 = D.nb2[s], n3 = D.nb3[s];
-        o.gp0 = (double)n2.y; o.gp1 = (double)n2.z; o.gu0 = (double)n2.w; o.gu1 = (double)n3.x;
-        o.gv0 = (double)n3.y; o.gv1 = (double)n3.z;
+        o.gp0 = gs * n2.y; o.gp1 = gs * n2.z; o.gu0 = gs * n2.w; o.gu1 = gs * n3.x;
+        o.gv0 = gs * n3.y; o.gv1 = gs * n3.z;
     }
     if (MS) {
         const typename VT<R>::V2 g = D.avg[s];
@@ -690,9 +691,10 @@ __global__ void k_adj_point(Params P, Sorted<R> D, Adj A, int shift) {
     const double4 bi = D.binv64[a];
     const typename VT<R>::V4 n1 = D.nb1[a], n2 = D.nb2[a], n3 = D.nb3[a];
     // normalised gradients of pass A: rho (n1.w, n2.x), u (n2.w, n3.x), v (n3.y, n3.z)
-    const double gr0 = (double)n1.w, gr1 = (double)n2.x;
-    const double gu0 = (double)n2.w, gu1 = (double)n3.x;
-    const double gv0 = (double)n3.y, gv1 = (double)n3.z;
+    const double gs = grad_scale<R>();
+    const double gr0 = gs * n1.w, gr1 = gs * n2.x;
+    const double gu0 = gs * n2.w, gu1 = gs * n3.x;
+    const double gv0 = gs * n3.y, gv1 = gs * n3.z;
     double2 ggr = A.ggr[a];
     double4 gbs = make_double4(0, 0, 0, 0);
     if (shift) {
@@ -1023,7 +1025,7 @@ __global__ void k_adj_stage3(Params P, Sorted<R> D, Adj A, double dt, int shift)
             const double amp = sqrt(d0 * d0 + d1 * d1);
             const bool capped = amp > P.shift_max;
             const double dc0 = capped ? d0 / amp * P.shift_max : d0, dc1 = capped ? d1 / amp * P.shift_max : d1;
-            const double g0 = (double)D.nb1[s].w, g1 = (double)D.nb2[s].x;
+            const double g0 = grad_scale<R>() * D.nb1[s].w, g1 = grad_scale<R>() * D.nb2[s].x;
             // x' = x + dc, rho' = rho + g.dc
             const double b0 = lx.x + lrho * g0, b1 = lx.y + lrho * g1;
             sg = make_double2(lrho * dc0, lrho * dc1);

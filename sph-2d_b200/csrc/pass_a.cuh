@@ -181,10 +181,13 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? SPH_PASS_A_F32_BLOCKS : 
         txy = (R)((nut * sxy) * rho);
         tyy = (R)((2 * nut * syy - kk - blin) * rho);
     }
+    // FP32 records: the gradients halved (exact), since pass C uses only
+    // 1/2 grad phi, and w = 1/rho (rounded FP32 reciprocal of the FP32 density),
+    // which pass C reads instead of forming it for every pair
+    if (F32)
+        for (int c = 0; c < 8; ++c) gr[c] *= R(0.5);
     D.nb1[a] = mk4<R>(txx, txy, tyy, gr[0]);
     D.nb2[a] = mk4<R>(gr[1], gr[2], gr[3], gr[4]);
-    // FP32 records: w = 1/rho (rounded FP32 reciprocal of the FP32 density),
-    // which pass C reads instead of forming it for every pair
     D.nb3[a] = mk4<R>(gr[5], gr[6], gr[7], F32 ? (R)__frcp_rn((float)rho_a) : R(0));
     const R fv = fra;
     D.fra_v[a] = fv;

@@ -145,6 +145,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIF
 
     const R hbar = (R)P.h;
     const R inv_h = (R)(1.0 / P.h);
+    const R gk = (R)((P.kernel_model == SPH_KERNEL_GAUSSIAN ? -2.0 : -5.0) * P.kfactor / (P.h * P.h));
     const R inv_sqc0 = (R)(1.0 / P.sqrt_c0);
     const R nu2 = (R)(2.0 * P.nu), alpha = (R)P.alpha, beta = (R)P.beta;
     const R fh2 = (R)((P.fai * P.h) * (P.fai * P.h));
@@ -156,6 +157,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIF
     constexpr bool RREC = F32 && MUSCL;
     const R inv_rho_a = RREC ? (R)S.nb3.w : rcp(rho_a);
     const R rho0_over_rho_a = (R)P.rho0 * inv_rho_a;
+    const R dla_rho = dla_h * rho0_over_rho_a;
 
     A cont, accx, accy;
     cont.init(); accx.init(); accy.init();
@@ -247,7 +249,8 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIF
             drho_ji = -(sgn * (R)(S.kin.z - T.kin.z));
             rho_a_ = (R)S.kin.z; rho_b = (R)T.kin.z;
         }
-        // compute_kernel: W and dwdx(k) = g (x_i - x_j)
+        // compute_kernel: W and dwdx(k) = g (x_i - x_j).  FP32: g with
+        // q/(d h) = 1/h^2 folded into a constant (gk)
         R w, g;
         {
             const R q = d * inv_h;
@@ -255,12 +258,12 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIF
             if (P.kernel_model == SPH_KERNEL_GAUSSIAN) {
                 const R ex = exp(-(q * q));
                 w = (ex - (R)P.gauss_e9) * kf;
-                g = ex * (R(-2) * q) * inv_d * inv_h * kf;
+                g = F32 ? ex * gk : ex * (R(-2) * q) * inv_d * inv_h * kf;
             } else {
                 const R t = R(1) - R(0.5) * q;
                 const R t3 = t * t * t;
                 w = kf * (R(1) + R(2) * q) * (t3 * t);
-                g = kf * (R(-5) * q * t3) * inv_d * inv_h;
+                g = F32 ? t3 * gk : kf * (R(-5) * q * t3) * inv_d * inv_h;
             }
         }
         const R dw0 = g * xij0, dw1 = g * xij1;
@@ -280,8 +283,10 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIF
             // (DelPhi_i, DelPhi_j) = (-ga, gb) when a is pair_i and (gb, -ga) when it is
             // pair_j.  The products are rounded separately and fused in a fixed order,
             // so both members of the pair form the same bits.
-            // nb2 = (grad rho y, grad p x, grad p y, grad u x), nb3 = (grad u y, grad v x, grad v y, 1/rho)
-            auto half_dot = [&](R g0, R g1) { return R(0.5) * fma(g1, xab1, mul_rn(g0, xab0)); };
+            // nb2 = (grad rho y, grad p x, grad p y, grad u x), nb3 = (grad u y, grad v x, grad v y, 1/rho),
+            // the gradients halved in the FP32 records
+            // (the FP32 records hold 1/2 grad phi, so the halving is already done, exactly)
+            auto half_dot = [&](R g0, R g1) { return (F32 ? R(1) : R(0.5)) * fma(g1, xab1, mul_rn(g0, xab0)); };
             const R gpa = half_dot(S.nb2.y, S.nb2.z), gpb = half_dot(T.nb2.y, T.nb2.z);
             const R gua = half_dot(S.nb2.w, S.nb3.x), gub = half_dot(T.nb2.w, T.nb3.x);
             const R gva = half_dot(S.nb3.y, S.nb3.z), gvb = half_dot(T.nb3.y, T.nb3.z);
@@ -415,9 +420,11 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIF
             tx += mb * (-Pi * nd0);
             ty += mb * (-Pi * nd1);
         }
+        // (x_i - x_j).B^-1 dwdx / r^2, shared by the laplacian and delta-SPH (FP32)
+        const R xnd = (xij0 * nd0 + xij1 * nd1) * inv_r2;
         if (!MS || P.laplacian == 1) {
             // Morris laplacian (:432-436)
-            const R lf = Vb * nu2 * (xij0 * nd0 + xij1 * nd1) * inv_r2;
+            const R lf = F32 ? Vb * nu2 * xnd : Vb * nu2 * (xij0 * nd0 + xij1 * nd1) * inv_r2;
             tx += lf * du;
             ty += lf * dv;
         } else {
@@ -427,7 +434,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIF
             ty += lf * nd1;
         }
         // delta-alpha artificial internal acceleration (:442-446)
-        const R tt = dla_h * cbar * vx * inv_r2 * rho0_over_rho_a * Vb;
+        const R tt = F32 ? dla_rho * cbar * (vx * inv_r2) * Vb : dla_h * cbar * vx * inv_r2 * rho0_over_rho_a * Vb;
         tx += tt * nd0;
         ty += tt * nd1;
         // SPS force, unnormalised dwdx and the neighbour's SPS mass (:450-492);
@@ -456,11 +463,12 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIF
                 // Antuono form (Solver_Normalized_Delta_SPH_SPS.f90:610-636):
                 // psi = 2 (rho_j - rho_i) (x_j - x_i)/r^2 - (grad rho_i + grad rho_j), D += delta h c psi.gradW V
                 const R f = R(2) * drho_ji * inv_r2;
-                const R p0 = -(f * xij0) - sg0, p1 = -(f * xij1) - sg1;
+                const R gsc = F32 ? R(2) : R(1);      // FP32 records: 1/2 grad rho
+                const R p0 = -(f * xij0) - gsc * sg0, p1 = -(f * xij1) - gsc * sg1;
                 dr += sgn * (dla_dh * cbar * (p0 * nd0 + p1 * nd1) * Vb);
             } else {
-                const R psi = drho_ji + R(0.5) * (sg0 * xij0 + sg1 * xij1);
-                const R tma = -(xij0 * nd0 + xij1 * nd1) * inv_r2;
+                const R psi = drho_ji + (F32 ? R(1) : R(0.5)) * (sg0 * xij0 + sg1 * xij1);
+                const R tma = F32 ? -xnd : -(xij0 * nd0 + xij1 * nd1) * inv_r2;
                 dr += sgn * (dlt2h * cbar * psi * tma * Vb);
             }
         }

@@ -136,6 +136,7 @@ struct Sorted {
     V4* nb1;          // tau_xx, tau_xy, tau_yy, grad rho x          -- neighbour record 3
     V4* nb2;          // grad rho y, grad p x, grad p y, grad u x     -- neighbour record 4
     V4* nb3;          // grad u y, grad v x, grad v y, 1/rho (FP32) or 0 -- neighbour record 5 (MUSCL)
+                      // (the FP32 records hold the gradients halved: grad_scale<R>())
     V4* binv;         // B^-1 (11, 12, 21, 22) in the pair precision
     double4* binv64;  // B^-1 in FP64 (applied to the FP64 shifting sum)
     R* fra_v;
@@ -172,6 +173,11 @@ struct Sorted {
     float4* kl;       //               (lo)
     float4* xhl;      // x hi, y hi, x lo, y lo
 };
+
+// Factor from the stored gradient records (nb1.w, nb2, nb3.xyz) to the
+// gradients: the FP32 records hold 1/2 grad phi (pass C uses only that).
+template <typename R>
+__host__ __device__ constexpr double grad_scale() { return sizeof(R) == 4 ? 2.0 : 1.0; }
 
 // Hi/lo split of the records a particle's pass-C neighbours read (mixed path).
 template <typename R>

@@ -34,8 +34,8 @@ __device__ __forceinline__ void apply_shift(const Params& P, const Sorted<R>& D,
     if (amp > P.shift_max) { s0 = s0 / amp * P.shift_max; s1 = s1 / amp * P.shift_max; }
     x = x + s0;
     y = y + s1;
-    rho = rho + (double)D.nb1[s].w * s0;
-    rho = rho + (double)D.nb2[s].x * s1;
+    rho = rho + grad_scale<R>() * D.nb1[s].w * s0;
+    rho = rho + grad_scale<R>() * D.nb2[s].x * s1;
 }
 
 template <typename R>
@@ -668,12 +668,13 @@ __global__ void k_export(Params P, Sorted<R> D, double* out) {
     out[6 * n + i] = (D.flags[s] & 2) ? 1.0 : 0.0;
     out[7 * n + i] = (double)D.fra_v[s];
     auto bi = D.binv[s]; auto n1 = D.nb1[s]; auto n2 = D.nb2[s]; auto n3 = D.nb3[s];
+    const double gs = grad_scale<R>();
     out[8 * n + i] = (double)bi.x; out[9 * n + i] = (double)bi.y; out[10 * n + i] = (double)bi.z; out[11 * n + i] = (double)bi.w;
     out[12 * n + i] = (double)n1.x; out[13 * n + i] = (double)n1.y; out[14 * n + i] = (double)n1.z;
-    out[15 * n + i] = (double)n1.w; out[16 * n + i] = (double)n2.x;
-    out[17 * n + i] = (double)n2.y; out[18 * n + i] = (double)n2.z;
-    out[19 * n + i] = (double)n2.w; out[20 * n + i] = (double)n3.x;
-    out[21 * n + i] = (double)n3.y; out[22 * n + i] = (double)n3.z;
+    out[15 * n + i] = gs * n1.w; out[16 * n + i] = gs * n2.x;
+    out[17 * n + i] = gs * n2.y; out[18 * n + i] = gs * n2.z;
+    out[19 * n + i] = gs * n2.w; out[20 * n + i] = gs * n3.x;
+    out[21 * n + i] = gs * n3.y; out[22 * n + i] = gs * n3.z;
 }
 
 }  // namespace sph
