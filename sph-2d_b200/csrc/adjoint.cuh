@@ -837,11 +837,16 @@ __device__ __forceinline__ void rev_rawsum(double r0, double r1, double id, doub
 // m) are written to sx, su, sr, sm for the ghost reverse and the stage reverse
 // that follow.
 // MUSCL: also pass A's raw grad p sum, p = p(rho) by the equation of state.
+// kAdjLanes lanes per particle: lane q takes pairs q, q + kAdjLanes, ...; the
+// lanes' partial sums are added by shuffles in a fixed order.
 template <typename R, bool MS = false, bool MUSCL = false>
 __global__ void __launch_bounds__(kAdjThreads) k_adj_a(Params P, Sorted<R> D, Adj A, int stage, double dt,
                                                        const double2* lg) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= P.n_tot) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c0 = t / kAdjLanes, lane = t & (kAdjLanes - 1);
+    // every lane of the warp takes part in the shuffles below
+    const bool live = c0 < P.n_tot;
+    const int c = live ? c0 : 0;
     const double2 xc = D.pos[c];
     const double4 kc = D.kin[c];
     const double mc = D.mass[c];
@@ -855,8 +860,8 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_a(Params P, Sorted<R> D, Ad
         const double2 g = A.gavg[c], l = lg[c];
         lac = make_double2(g.x + l.x, g.y + l.y);
     }
-    const int nn = D.npairs[c];
-    for (int e = 0; e < nn; ++e) {
+    const int nn = live ? D.npairs[c] : 0;
+    for (int e = lane; e < nn; e += kAdjLanes) {
         const int b = (int)(D.pairs[(size_t)e * P.nbr_stride + c] & 0x7fffffffu);
         const double2 xb = D.pos[b];
         const double4 kb = D.kin[b];
@@ -913,6 +918,16 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_a(Params P, Sorted<R> D, Ad
             Vb += G * S;
         }
     }
+    double v[8] = {x0b, x1b, ub, vb, rb, Vb, mb_, pb_};
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        if (!MS && q == 6) continue;
+        if (!MUSCL && q == 7) continue;
+        v[q] += __shfl_xor_sync(0xffffffffu, v[q], 1);
+        if (kAdjLanes == 4) v[q] += __shfl_xor_sync(0xffffffffu, v[q], 2);
+    }
+    if (!live || lane != 0) return;
+    x0b = v[0]; x1b = v[1]; ub = v[2]; vb = v[3]; rb = v[4]; Vb = v[5]; mb_ = v[6]; pb_ = v[7];
     const double2 sx = A.sx[c], su = A.su[c];
     if (MS) {
         A.sx[c] = make_double2(sx.x + x0b, sx.y + x1b);

@@ -1081,8 +1081,8 @@ int adj_rhs(sph_handle* h, const Sorted<R>& V, int k, int stage, bool shift = fa
         h->launches += 1;
     }
     k_adj_point<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, V, A, shift ? 1 : 0);
-    if (P.muscl) k_adj_a<R, false, true><<<nb, kAdjThreads, 0, h->stream>>>(P, V, A, stage, X->dt, nullptr);
-    else k_adj_a<R><<<nb, kAdjThreads, 0, h->stream>>>(P, V, A, stage, X->dt, nullptr);
+    if (P.muscl) k_adj_a<R, false, true><<<nbc, kAdjThreads, 0, h->stream>>>(P, V, A, stage, X->dt, nullptr);
+    else k_adj_a<R><<<nbc, kAdjThreads, 0, h->stream>>>(P, V, A, stage, X->dt, nullptr);
     CK(cudaGetLastError());
     h->launches += 3;
     return SPH_OK;
@@ -1189,7 +1189,7 @@ int adj_rhs_ms(sph_handle* h, const Sorted<R>& V, int k, int pred, bool drag, in
         h->launches += 3;
     }
     k_adj_point<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, V, A, 0);
-    k_adj_a<R, true><<<nb, kAdjThreads, 0, h->stream>>>(P, V, A, 0, X->dt, A.lg[k]);
+    k_adj_a<R, true><<<nbc, kAdjThreads, 0, h->stream>>>(P, V, A, 0, X->dt, A.lg[k]);
     if (ghosts) {
         const int ngb = blocks((long long)h->n_ghost * 32, kAdjThreads);
         k_adj_ghost_lambda<R><<<ngb, kAdjThreads, 0, h->stream>>>(P, V, A, h->d_ghost_ids, h->n_ghost, h->t_phys,
