@@ -400,9 +400,14 @@ int prepare(sph_handle* h) {
     return SPH_OK;
 }
 
-// One RHS evaluation on the current stage state.
 template <typename R>
-int rhs(sph_handle* h, int last) {
+int keep_stage(sph_handle* h, int j, int k);
+
+// One RHS evaluation on the current stage state.  keep_j >= 0 (the adjoint's
+// segment re-run): the ghost interpolation sums go to gint / gsw and the state
+// after the ghost assignment to stage slot keep_j.
+template <typename R>
+int rhs(sph_handle* h, int last, int keep_j = -1, double4* gint = nullptr, double* gsw = nullptr) {
     const Params& P = h->P;
     Sorted<R>& D = sorted<R>(h);
     const int nb = blocks(P.n_tot, 128);
@@ -412,9 +417,13 @@ int rhs(sph_handle* h, int last) {
         if (h->n_ghost > 0) {
             k_assign_ghosts<R><<<blocks((long long)h->n_ghost * 32, 128), 128, 0, h->stream>>>(
                 P, D, h->d_ghost_ids, h->n_ghost, h->t_phys, h->body_vel[0], h->body_vel[1], h->body_acc[0],
-                h->body_acc[1]);
+                h->body_acc[1], gint, gsw);
             h->launches += 1;
         }
+    }
+    if (keep_j >= 0) {
+        int rc = keep_stage<R>(h, keep_j, 0);
+        if (rc) return rc;
     }
     tic(h, PH_A);
     launch_pass_a<R, true>(P, D, nb, h->stream);
@@ -698,6 +707,26 @@ struct AdjCtx {
     int n_prep = 0, cap_prep = 0;
     long long prep_nnbr_off = 0;   // slot offset of the saved list lengths
     std::vector<int> seg_nimg, seg_nlr;
+    // moving square: what the corrector RHS of each step of the segment computed
+    // before pass C (the ghost interpolation sums, pass A's pair list, B^-1,
+    // gradient records, flags and XSPH velocity), written there by the segment
+    // re-run and read by the reverse step instead of re-running the ghost
+    // assignment, pass A and the surface tests (allocated with the sorted-state
+    // slots when they also leave 1 GiB free).  Per slot: pairs [max_nbr][cap_tot],
+    // the rest [cap_tot]; the pair-precision arrays as bytes.
+    bool pa = false;
+    unsigned* pa_pairs = nullptr;
+    int* pa_npairs = nullptr;
+    unsigned char* pa_binv = nullptr;
+    unsigned char* pa_nb1 = nullptr;
+    unsigned char* pa_nb2 = nullptr;
+    unsigned char* pa_fra = nullptr;
+    unsigned char* pa_avg = nullptr;
+    uint8_t* pa_flags = nullptr;
+    double4* pa_binv64 = nullptr;
+    double4* pa_gint = nullptr;
+    double* pa_gsw = nullptr;
+    std::vector<char> seg_kept;  // the corrector RHS of step j ran in the re-run into slot j
     double2* target = nullptr;
     double* loss_part = nullptr;
     Adj A{};
@@ -798,11 +827,12 @@ std::vector<PrepDesc> prep_table(sph_handle* h, long long* words, long long* nnb
     if (sizeof(R) == 4) {
         pp(D.vol64, sizeof(*D.vol64)); pp(D.kh, sizeof(*D.kh)); pp(D.kl, sizeof(*D.kl)); pp(D.xhl, sizeof(*D.xhl));
     }
-    // the lists: max_nbr rows at the lists' own pitch (nbr_stride = cap_tot)
-    add(D.nbr, 1, h->P.max_nbr, h->P.nbr_stride);
     add(D.cell_start, 0, h->ncells);
     add(D.cell_end, 0, h->ncells);
     pp(h->S.lr_cnt, 4); pp(h->S.lr_off, 4); pp(h->S.tb_cnt, 4); pp(h->S.tb_off, 4);
+    // the lists, last (a reverse step that does not re-run pass A skips them):
+    // max_nbr rows at the lists' own pitch (nbr_stride = cap_tot)
+    add(D.nbr, 1, h->P.max_nbr, h->P.nbr_stride);
     *words = off;
     return v;
 }
@@ -833,13 +863,14 @@ int prep_upload(sph_handle* h) {
     return SPH_OK;
 }
 
-// After prepare in the segment re-run: keep what it wrote in slot j.
-int prep_save(sph_handle* h, int j) {
+// After prepare in the segment re-run: keep what it wrote in slot j (lists =
+// false: without the neighbour lists, the last descriptor).
+int prep_save(sph_handle* h, int j, bool lists = true) {
     AdjCtx* X = h->adj;
     if (!X->prep) return SPH_OK;
     const int nt = h->P.n_tot;
     const int* cnt = h->mixed ? h->D32.nnbr : h->D64.nnbr;
-    k_prep_copy<<<dim3(blocks(nt, 256), X->n_prep), 256, 0, h->stream>>>(
+    k_prep_copy<<<dim3(blocks(nt, 256), X->n_prep - (lists ? 0 : 1)), 256, 0, h->stream>>>(
         X->d_prep, nt, X->prep + (size_t)j * X->prep_words, 1, cnt);
     CK(cudaGetLastError());
     h->launches += 1;
@@ -850,8 +881,8 @@ int prep_save(sph_handle* h, int j) {
 
 // In place of prepare in a reversed step: the sorted step-start state of slot j
 // (the same as a re-sort of the restored step-start state gives, the sort being
-// deterministic).
-int prep_restore(sph_handle* h, int j) {
+// deterministic); lists = false: without the neighbour lists.
+int prep_restore(sph_handle* h, int j, bool lists = true) {
     AdjCtx* X = h->adj;
     Params& P = h->P;
     P.n_host = h->n_host;
@@ -860,7 +891,7 @@ int prep_restore(sph_handle* h, int j) {
     P.n_tot = h->n_host + h->n_img;
     tic(h, PH_SORT);
     unsigned* slot = X->prep + (size_t)j * X->prep_words;
-    k_prep_copy<<<dim3(blocks(P.n_tot, 256), X->n_prep), 256, 0, h->stream>>>(
+    k_prep_copy<<<dim3(blocks(P.n_tot, 256), X->n_prep - (lists ? 0 : 1)), 256, 0, h->stream>>>(
         X->d_prep, P.n_tot, slot, 0, (const int*)(slot + X->prep_nnbr_off));
     CK(cudaGetLastError());
     h->launches += 1;
@@ -918,6 +949,25 @@ int adj_prepare_ctx(sph_handle* h, const sph_adj_config* ac) {
             if ((rc = adj_alloc(X, &X->prep, (size_t)pw * every))) return rc;
             X->prep_words = pw;
         }
+        // (FP64 forward only: the mixed forward's pass A reads the hi/lo records,
+        // the reverse step's re-run the FP64 state)
+        if (h->P.ms && X->prep && !h->mixed) {
+            const size_t rs = h->mixed ? sizeof(float) : sizeof(double);
+            const size_t per_pa = nt * ((size_t)h->P.max_nbr * 4 + 4 + 3 * 4 * rs + rs + 2 * rs + 1 +
+                                        sizeof(double4) * 2 + sizeof(double));
+            CK(cudaMemGetInfo(&free_b, &total_b));
+            if (per_pa * every + (size_t(1) << 30) <= free_b) {
+                const size_t ne = nt * every;
+                if ((rc = adj_alloc(X, &X->pa_pairs, ne * h->P.max_nbr)) || (rc = adj_alloc(X, &X->pa_npairs, ne)) ||
+                    (rc = adj_alloc(X, &X->pa_binv, ne * 4 * rs)) || (rc = adj_alloc(X, &X->pa_nb1, ne * 4 * rs)) ||
+                    (rc = adj_alloc(X, &X->pa_nb2, ne * 4 * rs)) || (rc = adj_alloc(X, &X->pa_fra, ne * rs)) ||
+                    (rc = adj_alloc(X, &X->pa_avg, ne * 2 * rs)) || (rc = adj_alloc(X, &X->pa_flags, ne)) ||
+                    (rc = adj_alloc(X, &X->pa_binv64, ne)) || (rc = adj_alloc(X, &X->pa_gint, ne)) ||
+                    (rc = adj_alloc(X, &X->pa_gsw, ne)))
+                    return rc;
+                X->pa = true;
+            }
+        }
     }
     if (h->P.ms && !X->A.gavg) {
         Adj& A = X->A;
@@ -945,6 +995,7 @@ int adj_prepare_ctx(sph_handle* h, const sph_adj_config* ac) {
     X->seg_ntot.assign(every, 0);
     X->seg_nimg.assign(every, 0);
     X->seg_nlr.assign(every, 0);
+    X->seg_kept.assign(every, 0);
     return SPH_OK;
 }
 
@@ -1008,6 +1059,36 @@ Sorted<R> stage_view(sph_handle* h, int j, int k) {
     return V;
 }
 
+// The sorted arrays V with what pass A writes (and the surface tests update)
+// taken from pass-A slot j.
+template <typename R>
+Sorted<R> pa_view(sph_handle* h, Sorted<R> V, int j) {
+    using V4 = typename VT<R>::V4;
+    using V2 = typename VT<R>::V2;
+    AdjCtx* X = h->adj;
+    const size_t o = (size_t)j * X->cap_tot;
+    V.pairs = X->pa_pairs + o * h->P.max_nbr;
+    V.npairs = X->pa_npairs + o;
+    V.binv = reinterpret_cast<V4*>(X->pa_binv) + o;
+    V.nb1 = reinterpret_cast<V4*>(X->pa_nb1) + o;
+    V.nb2 = reinterpret_cast<V4*>(X->pa_nb2) + o;
+    V.fra_v = reinterpret_cast<R*>(X->pa_fra) + o;
+    V.avg = reinterpret_cast<V2*>(X->pa_avg) + o;
+    V.flags = X->pa_flags + o;
+    V.binv64 = X->pa_binv64 + o;
+    return V;
+}
+
+// While a kept corrector RHS and its stage run in the segment re-run, the
+// handle's sorted arrays point at pass-A slot j; the destructor points them back.
+template <typename R>
+struct PaSwap {
+    Sorted<R>& D;
+    Sorted<R> saved;
+    PaSwap(sph_handle* h, int j) : D(sorted<R>(h)), saved(D) { D = pa_view<R>(h, D, j); }
+    ~PaSwap() { D = saved; }
+};
+
 // Copy the current stage state into stage slot j, state k.
 template <typename R>
 int keep_stage(sph_handle* h, int j, int k) {
@@ -1024,17 +1105,37 @@ int keep_stage(sph_handle* h, int j, int k) {
 // full = false the step stops after the last kept state (all the reverse needs).
 template <typename R>
 int step_keep(sph_handle* h, double dt, int j, bool full) {
-    int rc = step_begin<R>(h, dt);
-    if (rc || (rc = prepare<R>(h)) || (rc = prep_save(h, j))) return rc;
-    h->adj->seg_ntot[j] = h->P.n_tot;
     const int first = h->step_count == 0;
+    // the corrector RHS of a moving-square step that runs here fills pass-A slot j,
+    // and its reverse step re-runs no pass A, so it needs no neighbour lists
+    const bool keep_pa = h->adj->pa && full && !first && h->cfg.integrator == SPH_INTEGRATOR_EULER_PC;
+    int rc = step_begin<R>(h, dt);
+    if (rc || (rc = prepare<R>(h)) || (rc = prep_save(h, j, !keep_pa))) return rc;
+    h->adj->seg_ntot[j] = h->P.n_tot;
     if (first && (rc = rhs<R>(h, 0))) return rc;
     if (h->cfg.integrator == SPH_INTEGRATOR_EULER_PC) {
-        if ((rc = stage<R>(h, 10, dt, first ? 0 : 1, 0)) || (rc = keep_stage<R>(h, j, 0))) return rc;
-        if (full) {
-            if ((rc = rhs<R>(h, 1)) || (rc = stage<R>(h, 11, dt, 0, 0))) return rc;
+        AdjCtx* X = h->adj;
+        X->seg_kept[j] = 0;
+        if ((rc = stage<R>(h, 10, dt, first ? 0 : 1, 0))) return rc;
+        if (keep_pa) {
+            // the corrector RHS writes what pass A computes into pass-A slot j,
+            // for the reverse step to read
+            const size_t o = (size_t)j * X->cap_tot;
+            {
+                PaSwap<R> sw(h, j);
+                if ((rc = rhs<R>(h, 1, j, X->pa_gint + o, X->pa_gsw + o)) || (rc = stage<R>(h, 11, dt, 0, 0)))
+                    return rc;
+            }
+            X->seg_kept[j] = 1;
             h->step_count++;
             h->n_steps++;
+        } else {
+            if ((rc = keep_stage<R>(h, j, 0))) return rc;
+            if (full) {
+                if ((rc = rhs<R>(h, 1)) || (rc = stage<R>(h, 11, dt, 0, 0))) return rc;
+                h->step_count++;
+                h->n_steps++;
+            }
         }
         tic(h, -1);
         if (h->ev_used > 4096) timing_flush(h);
@@ -1158,22 +1259,30 @@ int adj_step(sph_handle* h, bool first, int j) {
 // assignment, and of the predictor (pred = 1) or the step-start accumulation.
 // The body-motion adjoints of the RHS go to g_motion[4 jstep ..].
 template <typename R>
-int adj_rhs_ms(sph_handle* h, const Sorted<R>& V, int k, int pred, bool drag, int jstep) {
+int adj_rhs_ms(sph_handle* h, const Sorted<R>& V, int k, int pred, bool drag, int jstep, int kept_j = -1) {
     const Params& P = h->P;
     AdjCtx* X = h->adj;
-    Adj& A = X->A;
+    Adj A = X->A;
     const int nb = blocks(P.n_tot, kAdjThreads);
     const int nbc = blocks((long long)P.n_tot * kAdjLanes, kAdjThreads);
     const bool ghosts = P.ghost_assign && h->n_ghost > 0;
-    tic(h, PH_A);
-    if (ghosts) {
-        k_assign_ghosts<R><<<blocks((long long)h->n_ghost * 32, 128), 128, 0, h->stream>>>(
-            P, V, h->d_ghost_ids, h->n_ghost, h->t_phys, h->body_vel[0], h->body_vel[1], h->body_acc[0],
-            h->body_acc[1], A.gint, A.gsw);
-        h->launches += 1;
+    if (kept_j >= 0) {
+        // the segment re-run left this RHS's assigned ghosts in the stage slot and
+        // its interpolation sums and pass-A outputs in pass-A slot kept_j (V)
+        const size_t o = (size_t)kept_j * X->cap_tot;
+        A.gint = X->pa_gint + o;
+        A.gsw = X->pa_gsw + o;
+    } else {
+        tic(h, PH_A);
+        if (ghosts) {
+            k_assign_ghosts<R><<<blocks((long long)h->n_ghost * 32, 128), 128, 0, h->stream>>>(
+                P, V, h->d_ghost_ids, h->n_ghost, h->t_phys, h->body_vel[0], h->body_vel[1], h->body_acc[0],
+                h->body_acc[1], A.gint, A.gsw);
+            h->launches += 1;
+        }
+        launch_pass_a<R, false>(P, V, nb, h->stream);
+        launch_surface<R>(P, V, h->stream);
     }
-    launch_pass_a<R, false>(P, V, nb, h->stream);
-    launch_surface<R>(P, V, h->stream);
     tic(h, PH_ADJ);
     CK(cudaMemsetAsync(V.nflag, 0, (size_t)P.n_tot, h->stream));
     if (P.hllc)
@@ -1219,7 +1328,8 @@ int adj_step_ms(sph_handle* h, bool first, int j, int jstep) {
         if ((rc = step_keep<R>(h, dt, 0, false))) return rc;
         j = 0;
     } else {
-        if ((rc = step_begin<R>(h, dt)) || (rc = X->prep ? prep_restore(h, j) : prepare<R>(h))) return rc;
+        const bool lists = !(X->pa && X->seg_kept[j]);
+        if ((rc = step_begin<R>(h, dt)) || (rc = X->prep ? prep_restore(h, j, lists) : prepare<R>(h))) return rc;
         if (h->P.n_tot != X->seg_ntot[j]) return SPH_E_ARG;
     }
     const Params& P = h->P;
@@ -1228,7 +1338,9 @@ int adj_step_ms(sph_handle* h, bool first, int j, int jstep) {
     tic(h, PH_ADJ);
     k_adj_stage_end_ms<R><<<nb, 256, 0, h->stream>>>(P, D, A, dt);
     h->launches += 1;
-    if ((rc = adj_rhs_ms<R>(h, stage_view<R>(h, j, 0), 1, 1, X->loss == SPH_LOSS_DRAG, jstep))) return rc;
+    const bool kept = X->pa && X->seg_kept[j];
+    const Sorted<R> V = kept ? pa_view<R>(h, stage_view<R>(h, j, 0), j) : stage_view<R>(h, j, 0);
+    if ((rc = adj_rhs_ms<R>(h, V, 1, 1, X->loss == SPH_LOSS_DRAG, jstep, kept ? j : -1))) return rc;
     if (first) {
         // the fresh K1 of the first step was evaluated on the step-start state
         k_adj_load<R><<<nb, 256, 0, h->stream>>>(P, D, nullptr, nullptr);
