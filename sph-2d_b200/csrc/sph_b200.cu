@@ -1272,6 +1272,11 @@ int adj_rhs_ms(sph_handle* h, const Sorted<R>& V, int k, int pred, bool drag, in
         const size_t o = (size_t)kept_j * X->cap_tot;
         A.gint = X->pa_gint + o;
         A.gsw = X->pa_gsw + o;
+        if (ghosts) {
+            // the ghosts' mass and step-start arrays as that assignment set them
+            k_ghost_refill<R><<<blocks(h->n_ghost, 256), 256, 0, h->stream>>>(V, h->d_ghost_ids, h->n_ghost);
+            h->launches += 1;
+        }
     } else {
         tic(h, PH_A);
         if (ghosts) {

@@ -450,6 +450,22 @@ __global__ void k_assign_ghosts(Params P, Sorted<R> D, const int* ghost_ids, int
     store_split(D, s, x, make_double4(u, v, rho, p));
 }
 
+// The per-particle arrays k_assign_ghosts writes besides the records (mass,
+// SPS mass, step-start velocity and density), set again from the records of a
+// state that already holds the assigned ghosts (FP64 records: aux.x = m exactly).
+template <typename R>
+__global__ void k_ghost_refill(Sorted<R> D, const int* ghost_ids, int n_ghost) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n_ghost) return;
+    const int s = D.slot_of[ghost_ids[g]];
+    const double4 k = D.kin[s];
+    const double m = (double)D.aux[s].x;
+    D.mass[s] = m;
+    D.smass[s] = m;
+    D.vel0[s] = make_double2(k.x, k.y);
+    D.rho0[s] = k.z;
+}
+
 // Kinetic energy and max |v| of the water host particles
 // (Sampling_subroutine.f90:346-356): deterministic two-level reduction in FP64.
 constexpr int kRedThreads = 256;
