@@ -73,6 +73,22 @@ __device__ __forceinline__ void muscl_limiter<float>(float di, float dj, float d
     lj = big ? (first ? 0.f : half) : lim;
 }
 
+// The same FP32 limiter with its results as a pair term uses them: the sum
+// L = li + lj (half when one increment is clamped to dij/2, else 2 lim) and the
+// increment of this particle's side (li when it is pair_i, else lj).
+__device__ __forceinline__ void muscl_limiter_sum(float di, float dj, float dij, bool a_is_i, float& L, float& own) {
+    const float b = 1.3f;
+    const unsigned sb = __float_as_uint(dj) & 0x80000000u;
+    const float sdi = __uint_as_float(__float_as_uint(di) ^ sb), sdj = fabsf(dj);
+    const float m = fmaxf(0.f, fmaxf(fminf(b * sdi, sdj), fminf(sdi, b * sdj)));
+    const float half = 0.5f * dij;
+    const bool big = m > __uint_as_float(__float_as_uint(half) ^ sb) && m > 0.f;
+    const bool first = sdi > sdj;
+    const float lim = __uint_as_float(__float_as_uint(m) ^ sb);
+    L = big ? half : 2.f * lim;
+    own = big ? (first == a_is_i ? half : 0.f) : lim;
+}
+
 // Reciprocal and quotient in the pair loop, correctly rounded in both
 // precisions (the fast FP32 forms, __fdividef, made mixed pass C slower:
 // 3.46 -> 3.85 ms per step at 2048^2).
@@ -228,20 +244,28 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIF
         const Side<R>& I = a_is_i ? S : T;
         const Side<R>& J = a_is_i ? T : S;
         const R sgn = a_is_i ? R(1) : R(-1);
-        // position_difference_ij = x_i - x_j (find_particle_pair.f90:79-107) = sgn (x_a - x_b)
+        // AB (the mixed MUSCL Taylor-Green launch): the pair terms are formed in a's
+        // frame, x_a - x_b and phi_a - phi_b, instead of the pair's i/j frame.
+        // Negation is exact, so a term odd in the orientation takes the i/j-frame
+        // bits times sgn and the sgn of the final sums cancels it: sgn stays only
+        // where the MUSCL limiter needs the i/j frame.
+        constexpr bool AB = F32 && MUSCL && !MS;
+        // position_difference_ij = x_i - x_j (find_particle_pair.f90:79-107) = sgn (x_a - x_b);
+        // xij: that, or x_a - x_b in AB
         R xab0, xab1;
         if (HL) { xab0 = (R)dxf; xab1 = (R)dyf; }
         else { xab0 = (R)dxd; xab1 = (R)dyd; }
-        const R xij0 = sgn * xab0, xij1 = sgn * xab1;
+        const R xij0 = AB ? xab0 : sgn * xab0, xij1 = AB ? xab1 : sgn * xab1;
+        const R fsg = AB ? R(1) : sgn;      // the orientation of the frame's sums
         // pair differences, FP64 or hi/lo in FP32, formed as a - b and oriented
         // by sgn: b - a is exactly -(a - b), so both members of the pair get the
         // same bits, and sums such as rho_i + rho_j are a's plus b's
         R du, dv, dp, drho_ji, rho_a_, rho_b;
         if (HL) {
-            du = sgn * (R)((S.kh.x - T.kh.x) + (S.kl.x - T.kl.x));
-            dv = sgn * (R)((S.kh.y - T.kh.y) + (S.kl.y - T.kl.y));
-            dp = sgn * (R)((S.kh.w - T.kh.w) + (S.kl.w - T.kl.w));
-            drho_ji = -(sgn * (R)((S.kh.z - T.kh.z) + (S.kl.z - T.kl.z)));
+            du = fsg * (R)((S.kh.x - T.kh.x) + (S.kl.x - T.kl.x));
+            dv = fsg * (R)((S.kh.y - T.kh.y) + (S.kl.y - T.kl.y));
+            dp = fsg * (R)((S.kh.w - T.kh.w) + (S.kl.w - T.kl.w));
+            drho_ji = -(fsg * (R)((S.kh.z - T.kh.z) + (S.kl.z - T.kl.z)));
             rho_a_ = (R)S.kh.z; rho_b = (R)T.kh.z;
         } else {
             du = sgn * (R)(S.kin.x - T.kin.x); dv = sgn * (R)(S.kin.y - T.kin.y);
@@ -290,18 +314,34 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIF
             const R gpa = half_dot(S.nb2.y, S.nb2.z), gpb = half_dot(T.nb2.y, T.nb2.z);
             const R gua = half_dot(S.nb2.w, S.nb3.x), gub = half_dot(T.nb2.w, T.nb3.x);
             const R gva = half_dot(S.nb3.y, S.nb3.z), gvb = half_dot(T.nb3.y, T.nb3.z);
-            muscl_limiter<R>(a_is_i ? -gpa : gpb, a_is_i ? gpb : -gpa, -dp, lpi, lpj);
-            muscl_limiter<R>(a_is_i ? -gua : gub, a_is_i ? gub : -gua, -du, lui, luj);
-            muscl_limiter<R>(a_is_i ? -gva : gvb, a_is_i ? gvb : -gva, -dv, lvi, lvj);
+            if constexpr (AB) {
+                // the limiter in the i/j frame (dij = phi_j - phi_i = -sgn (phi_a - phi_b)),
+                // its sum and own-side increment taken back to a's frame by sgn;
+                // lpi etc. then hold sgn L and the own increment (lpj, luj, lvj unused)
+                float L, own;
+                muscl_limiter_sum(a_is_i ? -gpa : gpb, a_is_i ? gpb : -gpa, -(sgn * dp), a_is_i, L, own);
+                lpi = sgn * L;
+                muscl_limiter_sum(a_is_i ? -gua : gub, a_is_i ? gub : -gua, -(sgn * du), a_is_i, L, own);
+                lui = sgn * L; luj = sgn * own;
+                muscl_limiter_sum(a_is_i ? -gva : gvb, a_is_i ? gvb : -gva, -(sgn * dv), a_is_i, L, own);
+                lvi = sgn * L; lvj = sgn * own;
+            } else {
+                muscl_limiter<R>(a_is_i ? -gpa : gpb, a_is_i ? gpb : -gpa, -dp, lpi, lpj);
+                muscl_limiter<R>(a_is_i ? -gua : gub, a_is_i ? gub : -gua, -du, lui, luj);
+                muscl_limiter<R>(a_is_i ? -gva : gvb, a_is_i ? gvb : -gva, -dv, lvi, lvj);
+            }
         }
-        // U_L - U_R and P_L - P_R from the differences
-        const R dU = (du + lui + luj) * e0 + (dv + lvi + lvj) * e1;
+        // U_L - U_R and P_L - P_R from the differences (AB: the frame's e0, e1 and
+        // differences; the product is the i/j frame's)
+        const R dU = AB ? (du + lui) * e0 + (dv + lvi) * e1 : (du + lui + luj) * e0 + (dv + lvi + lvj) * e1;
         const R Pbar = HL ? R(0.5) * ((R)S.kh.w + (R)T.kh.w) : R(0.5) * ((R)S.kin.w + (R)T.kin.w);
         R PA, wa0, wa1;          // this side's star pressure and velocity minus star velocity
-        if (a_is_i) { wa0 = R(0.5) * du + lui; wa1 = R(0.5) * dv + lvi; }
+        if (AB) { wa0 = R(0.5) * du + luj; wa1 = R(0.5) * dv + lvj; }
+        else if (a_is_i) { wa0 = R(0.5) * du + lui; wa1 = R(0.5) * dv + lvi; }
         else { wa0 = R(-0.5) * du - luj; wa1 = R(-0.5) * dv - lvj; }
         if (!MS || !P.hllc) {
-            const R dP = dp + lpi + lpj;
+            // AB: dP and U* - Ubar in a's frame; sU e is the i/j frame's product
+            const R dP = AB ? dp + lpi : dp + lpi + lpj;
             const R sU = R(0.5) * dP * (inv_rbar * inv_sqc0);               // U* - Ubar
             const R bR = min(R(3) * (max(dU, R(0))), cbar);
             const R Ps = Pbar + R(0.5) * bR * rbar * dU;
@@ -406,7 +446,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIF
         }
         const R Vb = T.aux.y, mb = T.aux.x;
         // continuity (:360-369)
-        R dr = R(2) * rho_a * Vb * (sgn * (wa0 * nd0 + wa1 * nd1));
+        R dr = R(2) * rho_a * Vb * (fsg * (wa0 * nd0 + wa1 * nd1));
         // pressure force (:374-388)
         const R rho_ij = inv_rho_a * (RREC ? (R)T.nb3.w : rcp(rho_b));
         const R fp = R(-2) * PA * rho_ij * mb;
@@ -448,8 +488,8 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIF
             tp = (tp + syy * dw1 + sxy * dw0) * rho_ij;
             ty += smb * tp;
         }
-        accx.add(sgn * tx);
-        accy.add(sgn * ty);
+        accx.add(fsg * tx);
+        accy.add(fsg * ty);
         // XSPH average velocity (:495-500; modified solver only)
         if (!MUSCL && !MS && P.xsph) {
             const R f = eps2 * mb * rcp(rho_a_ + rho_b) * w;
@@ -469,7 +509,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIF
             } else {
                 const R psi = drho_ji + (F32 ? R(1) : R(0.5)) * (sg0 * xij0 + sg1 * xij1);
                 const R tma = F32 ? -xnd : -(xij0 * nd0 + xij1 * nd1) * inv_r2;
-                dr += sgn * (dlt2h * cbar * psi * tma * Vb);
+                dr += fsg * (dlt2h * cbar * psi * tma * Vb);
             }
         }
         cont.add(dr);
