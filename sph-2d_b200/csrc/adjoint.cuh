@@ -1117,6 +1117,15 @@ __global__ void k_adj_route(int n_src, int base, const int* cnt, const int* off,
     A.lx[s] = x; A.lv[s] = v; A.lrho[s] = r;
 }
 
+// The hi/lo records of the mixed path formed from the FP64 state of V (as the
+// forward's stages write them).
+template <typename R>
+__global__ void k_resplit(int n, Sorted<R> D) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    store_split(D, s, D.pos[s], D.kin[s]);
+}
+
 // Stage state -> the arrays the RHS reads (positions, kinematic and auxiliary records).
 template <typename R>
 __global__ void k_adj_load(Params P, Sorted<R> D, const double2* pos, const double4* kin) {

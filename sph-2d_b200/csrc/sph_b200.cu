@@ -715,11 +715,13 @@ struct AdjCtx {
     // slots when they also leave 1 GiB free).  Per slot: pairs [max_nbr][cap_tot],
     // the rest [cap_tot]; the pair-precision arrays as bytes.
     bool pa = false;
+    int pa_per_step = 0;         // pass-A slots per step: 1 (Euler PC corrector) or 3 (RK4 RHS 2-4)
     unsigned* pa_pairs = nullptr;
     int* pa_npairs = nullptr;
     unsigned char* pa_binv = nullptr;
     unsigned char* pa_nb1 = nullptr;
     unsigned char* pa_nb2 = nullptr;
+    unsigned char* pa_nb3 = nullptr;   // Taylor-Green only (MUSCL gradients, 1/rho)
     unsigned char* pa_fra = nullptr;
     unsigned char* pa_avg = nullptr;
     uint8_t* pa_flags = nullptr;
@@ -951,21 +953,26 @@ int adj_prepare_ctx(sph_handle* h, const sph_adj_config* ac) {
         }
         // (FP64 forward only: the mixed forward's pass A reads the hi/lo records,
         // the reverse step's re-run the FP64 state)
-        if (h->P.ms && X->prep && !h->mixed) {
+        // (the moving square: FP64 forward only)
+        if (X->prep && (!h->P.ms || !h->mixed)) {
+            const bool ms = h->P.ms != 0;
+            const int per = ms ? 1 : 3;
             const size_t rs = h->mixed ? sizeof(float) : sizeof(double);
-            const size_t per_pa = nt * ((size_t)h->P.max_nbr * 4 + 4 + 3 * 4 * rs + rs + 2 * rs + 1 +
-                                        sizeof(double4) * 2 + sizeof(double));
+            const size_t per_pa = nt * ((size_t)h->P.max_nbr * 4 + 4 + (ms ? 3 : 4) * 4 * rs + rs + 2 * rs + 1 +
+                                        sizeof(double4) + (ms ? sizeof(double4) + sizeof(double) : 0));
             CK(cudaMemGetInfo(&free_b, &total_b));
-            if (per_pa * every + (size_t(1) << 30) <= free_b) {
-                const size_t ne = nt * every;
+            if (per_pa * every * per + (size_t(1) << 30) <= free_b) {
+                const size_t ne = nt * every * per;
                 if ((rc = adj_alloc(X, &X->pa_pairs, ne * h->P.max_nbr)) || (rc = adj_alloc(X, &X->pa_npairs, ne)) ||
                     (rc = adj_alloc(X, &X->pa_binv, ne * 4 * rs)) || (rc = adj_alloc(X, &X->pa_nb1, ne * 4 * rs)) ||
                     (rc = adj_alloc(X, &X->pa_nb2, ne * 4 * rs)) || (rc = adj_alloc(X, &X->pa_fra, ne * rs)) ||
                     (rc = adj_alloc(X, &X->pa_avg, ne * 2 * rs)) || (rc = adj_alloc(X, &X->pa_flags, ne)) ||
-                    (rc = adj_alloc(X, &X->pa_binv64, ne)) || (rc = adj_alloc(X, &X->pa_gint, ne)) ||
-                    (rc = adj_alloc(X, &X->pa_gsw, ne)))
+                    (rc = adj_alloc(X, &X->pa_binv64, ne)))
                     return rc;
+                if (ms && ((rc = adj_alloc(X, &X->pa_gint, ne)) || (rc = adj_alloc(X, &X->pa_gsw, ne)))) return rc;
+                if (!ms && (rc = adj_alloc(X, &X->pa_nb3, ne * 4 * rs))) return rc;
                 X->pa = true;
+                X->pa_per_step = per;
             }
         }
     }
@@ -1076,6 +1083,7 @@ Sorted<R> pa_view(sph_handle* h, Sorted<R> V, int j) {
     V.avg = reinterpret_cast<V2*>(X->pa_avg) + o;
     V.flags = X->pa_flags + o;
     V.binv64 = X->pa_binv64 + o;
+    if (X->pa_nb3) V.nb3 = reinterpret_cast<V4*>(X->pa_nb3) + o;
     return V;
 }
 
@@ -1085,7 +1093,9 @@ template <typename R>
 struct PaSwap {
     Sorted<R>& D;
     Sorted<R> saved;
-    PaSwap(sph_handle* h, int j) : D(sorted<R>(h)), saved(D) { D = pa_view<R>(h, D, j); }
+    PaSwap(sph_handle* h, int j, bool on = true) : D(sorted<R>(h)), saved(D) {
+        if (on) D = pa_view<R>(h, D, j);
+    }
     ~PaSwap() { D = saved; }
 };
 
@@ -1106,9 +1116,10 @@ int keep_stage(sph_handle* h, int j, int k) {
 template <typename R>
 int step_keep(sph_handle* h, double dt, int j, bool full) {
     const int first = h->step_count == 0;
-    // the corrector RHS of a moving-square step that runs here fills pass-A slot j,
-    // and its reverse step re-runs no pass A, so it needs no neighbour lists
-    const bool keep_pa = h->adj->pa && full && !first && h->cfg.integrator == SPH_INTEGRATOR_EULER_PC;
+    // the RHS evaluations of a step that runs here in full (the moving square's
+    // corrector; the Runge-Kutta RHS 2-4) fill its pass-A slots, and its reverse
+    // step re-runs no pass A, so it needs no neighbour lists
+    const bool keep_pa = h->adj->pa && full && !first;
     int rc = step_begin<R>(h, dt);
     if (rc || (rc = prepare<R>(h)) || (rc = prep_save(h, j, !keep_pa))) return rc;
     h->adj->seg_ntot[j] = h->P.n_tot;
@@ -1141,11 +1152,25 @@ int step_keep(sph_handle* h, double dt, int j, bool full) {
         if (h->ev_used > 4096) timing_flush(h);
         return SPH_OK;
     }
+    // RK4: RHS k + 1 (k = 0, 1, 2) on stage state S(k+1) and the stage it feeds
+    // write pass A's outputs into pass-A slot 3 j + k when the step is kept
+    h->adj->seg_kept[j] = keep_pa ? 1 : 0;
     if ((rc = stage<R>(h, 0, dt, first ? 0 : 1, 0)) || (rc = keep_stage<R>(h, j, 0))) return rc;
-    if ((rc = rhs<R>(h, 0)) || (rc = stage<R>(h, 1, dt, 0, 0)) || (rc = keep_stage<R>(h, j, 1))) return rc;
-    if ((rc = rhs<R>(h, 0)) || (rc = stage<R>(h, 2, dt, 0, 0)) || (rc = keep_stage<R>(h, j, 2))) return rc;
+    {
+        PaSwap<R> sw(h, 3 * j, keep_pa);
+        if ((rc = rhs<R>(h, 0)) || (rc = stage<R>(h, 1, dt, 0, 0))) return rc;
+    }
+    if ((rc = keep_stage<R>(h, j, 1))) return rc;
+    {
+        PaSwap<R> sw(h, 3 * j + 1, keep_pa);
+        if ((rc = rhs<R>(h, 0)) || (rc = stage<R>(h, 2, dt, 0, 0))) return rc;
+    }
+    if ((rc = keep_stage<R>(h, j, 2))) return rc;
     if (full) {
-        if ((rc = rhs<R>(h, 1)) || (rc = stage<R>(h, 3, dt, 0, h->cfg.shifting))) return rc;
+        {
+            PaSwap<R> sw(h, 3 * j + 2, keep_pa);
+            if ((rc = rhs<R>(h, 1)) || (rc = stage<R>(h, 3, dt, 0, h->cfg.shifting))) return rc;
+        }
         h->step_count++;
         h->n_steps++;
     }
@@ -1154,22 +1179,38 @@ int step_keep(sph_handle* h, double dt, int j, bool full) {
     return SPH_OK;
 }
 
+// Pass A and the surface tests re-run on a kept stage state V, as the forward
+// ran them: the mixed forward reads the hi/lo records, which are formed here
+// from V's FP64 state first (the same records the forward's stage wrote).
+template <typename R>
+void adj_pass_a(sph_handle* h, const Sorted<R>& V) {
+    const Params& P = h->P;
+    const int nb = blocks(P.n_tot, 128);
+    if constexpr (sizeof(R) == 4) {
+        k_resplit<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P.n_tot, V);
+        launch_pass_a<R, true>(P, V, nb, h->stream);
+        h->launches += 1;
+    } else {
+        launch_pass_a<R, false>(P, V, nb, h->stream);
+    }
+    launch_surface<R>(P, V, h->stream);
+    h->launches += P.free_surface ? 3 : 1;
+}
+
 // Reverse of one RHS evaluation on the stage state V, with the rate adjoints
 // of RHS k of the step; stage = the stage that produced V (-1: the step start).
 // shift: the last RHS of a step with particle shifting (pass A already re-run by
 // adj_step, the step-end reverse left smu / shgr / shbi).
 template <typename R>
-int adj_rhs(sph_handle* h, const Sorted<R>& V, int k, int stage, bool shift = false) {
+int adj_rhs(sph_handle* h, const Sorted<R>& V, int k, int stage, bool shift = false, bool kept = false) {
     const Params& P = h->P;
     AdjCtx* X = h->adj;
     Adj& A = X->A;
     const int nb = blocks(P.n_tot, kAdjThreads);
     const int nbc = blocks((long long)P.n_tot * kAdjLanes, kAdjThreads);
-    if (!shift) {
+    if (!shift && !kept) {
         tic(h, PH_A);
-        launch_pass_a<R, false>(P, V, nb, h->stream);
-        launch_surface<R>(P, V, h->stream);
-        h->launches += 3;
+        adj_pass_a<R>(h, V);
     }
     tic(h, PH_ADJ);
     if (P.muscl)
@@ -1203,30 +1244,35 @@ int adj_step(sph_handle* h, bool first, int j) {
         if ((rc = step_keep<R>(h, dt, 0, false))) return rc;
         j = 0;
     } else {
-        if ((rc = X->prep ? prep_restore(h, j) : prepare<R>(h))) return rc;
+        if ((rc = X->prep ? prep_restore(h, j, !(X->pa && X->seg_kept[j])) : prepare<R>(h))) return rc;
         if (h->P.n_tot != X->seg_ntot[j]) return SPH_E_ARG;
     }
     const Params& P = h->P;
     Sorted<R>& D = sorted<R>(h);
     const int nb = blocks(P.n_tot, 256);
     const bool shift = h->cfg.shifting != 0;
+    // kept: the segment re-run left the pass-A outputs of RHS k + 1 in pass-A slot 3 j + k
+    const bool kept = X->pa && X->seg_kept[j];
+    auto view = [&](int k) {
+        return kept ? pa_view<R>(h, stage_view<R>(h, j, k), 3 * j + k) : stage_view<R>(h, j, k);
+    };
     if (shift) {
         // the step end's shift reads the last RHS's pass A (B^-1, grad rho, flags)
         // and its shifting sum: re-form them on the kept state S3 first
-        const Sorted<R> V = stage_view<R>(h, j, 2);
-        const int nba = blocks(P.n_tot, 128);
-        tic(h, PH_A);
-        launch_pass_a<R, false>(P, V, nba, h->stream);
-        launch_surface<R>(P, V, h->stream);
+        const Sorted<R> V = view(2);
+        if (!kept) {
+            tic(h, PH_A);
+            adj_pass_a<R>(h, V);
+        }
         tic(h, PH_ADJ);
         k_shift_sum<R><<<nb, 256, 0, h->stream>>>(P, V, A);
-        h->launches += P.free_surface ? 4 : 2;
+        h->launches += 1;
     }
     tic(h, PH_ADJ);
     k_adj_stage3<R><<<nb, 256, 0, h->stream>>>(P, D, A, dt, shift ? 1 : 0);
     h->launches += 1;
     for (int k = 2; k >= 0; --k)
-        if ((rc = adj_rhs<R>(h, stage_view<R>(h, j, k), k + 1, k, shift && k == 2))) return rc;
+        if ((rc = adj_rhs<R>(h, view(k), k + 1, k, shift && k == 2, kept))) return rc;
     if (first) {
         // the fresh K1 of the first step was evaluated on the step-start state
         k_adj_load<R><<<nb, 256, 0, h->stream>>>(P, D, nullptr, nullptr);
