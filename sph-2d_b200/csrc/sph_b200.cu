@@ -1269,7 +1269,9 @@ int adj_step(sph_handle* h, bool first, int j) {
         h->launches += 1;
     }
     tic(h, PH_ADJ);
-    k_adj_stage3<R><<<nb, 256, 0, h->stream>>>(P, D, A, dt, shift ? 1 : 0);
+    // the step end's shift reads the last RHS's flags, B^-1 and grad rho (kept:
+    // from pass-A slot 3 j + 2; else the re-run above left them in the arrays)
+    k_adj_stage3<R><<<nb, 256, 0, h->stream>>>(P, kept ? pa_view<R>(h, D, 3 * j + 2) : D, A, dt, shift ? 1 : 0);
     h->launches += 1;
     for (int k = 2; k >= 0; --k)
         if ((rc = adj_rhs<R>(h, view(k), k + 1, k, shift && k == 2, kept))) return rc;
