@@ -322,6 +322,14 @@ int sph_find_particle_pair_noalloc(const sph_config* cfg, int n, const double* d
  * of the artificial-viscosity switch).  The handle's state after the backward
  * pass is the forward's final state.
  *
+ * Device memory: besides the checkpoints, the handle keeps, while a segment
+ * is reversed, the stage states of each of its steps, their sorted states
+ * and, where that leaves 1 GiB free, what pass A computed for each RHS the
+ * re-run evaluated (per step of a segment: about 20 bytes times max_nbr plus
+ * 200 bytes per particle slot for each such RHS, three for the Runge-Kutta
+ * driver and one for the Euler predictor-corrector).  When memory is short it
+ * keeps less and recomputes instead; the gradient is the same either way.
+ *
  * Supported configurations (others return SPH_E_CONFIG), either kernel, with
  * or without renormalisation, without MLS density re-initialisation:
  *  - the normalised modified linear Riemann and MUSCL linear Riemann delta-SPH
