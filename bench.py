@@ -513,7 +513,7 @@ def streaming_report(S, sim, n, dt, chunks: int = 4, every: int = 5):
             "note": "wall clock, mixed 2048^2 step; sph_step calls of `every` steps each"}
 
 
-MS_DX, MS_STEPS, MS_EVERY, MS_FD_STEPS = 0.02, 2000, 64, 200
+MS_DX, MS_STEPS, MS_EVERY, MS_FD_STEPS, MS_FD_STEPS_WENDLAND = 0.02, 2000, 64, 200, 1000
 MS_COEFFS = (1.0, 0.2, -0.1, 0.05, 0.02)
 
 
@@ -529,7 +529,9 @@ def adjoint_ms_report(S):
     per step: translation, ghost assignment, RHS, body force).  The
     gradient with respect to a0 and the four Fourier coefficients is checked by
     central differences on the
-    first 200 steps of the same case: the improved Gaussian's gradient does not
+    first 200 steps of the same case, and on 1,000 steps of the case with the
+    Wendland C2 kernel, whose gradient vanishes at its cut-off: the improved
+    Gaussian's gradient does not
     vanish at its 3h cut-off, so the right-hand side jumps whenever a pair
     crosses the support, and over thousands of steps so many crossings move by
     a step inside any difference interval that the difference quotient no
@@ -601,6 +603,35 @@ def adjoint_ms_report(S):
         f = (loss_of(S.body_motion_schedule(cp, MS_STEPS, dt, period=T)[0][:nf], nf)
              - loss_of(S.body_motion_schedule(cm, MS_STEPS, dt, period=T)[0][:nf], nf)) / (2 * eps)
         fd.append({"coefficient": k, "adjoint": float(gcf[k]), "fd": f, "rel_err": abs(gcf[k] - f) / abs(f)})
+    # half the run's length with the Wendland C2 kernel (h = 1.3 dx, support 2h): its
+    # gradient is zero at the cut-off, so pairs crossing it put no jumps into the
+    # right-hand side and the difference quotient keeps measuring the derivative
+    cfg_w = cfg.copy()
+    cfg_w.kernel_model, cfg_w.kernel_scale, cfg_w.h = S.KERNEL_WENDLAND2, 2.0, 1.3 * cfg.dx
+    dt_w = 0.25 * cfg_w.h / np.sqrt(cfg_w.c0sq)
+    nw = MS_FD_STEPS_WENDLAND
+    mo_w, jac_w = S.body_motion_schedule(coeffs, MS_STEPS, dt_w, period=MS_STEPS * dt_w)
+    scale_w = 1.0 / (MS_STEPS * dt_w * 0.5 * cfg.rho0)
+
+    def loss_w(c):
+        with S.Simulation(cfg_w, case.n) as sim:
+            reset(sim)
+            mo = S.body_motion_schedule(c, MS_STEPS, dt_w, period=MS_STEPS * dt_w)[0][:nw]
+            return scale_w * sim.adjoint_forward(nw, dt_w, checkpoint_every=MS_EVERY, loss=S.LOSS_DRAG, body_motion=mo)
+
+    with S.Simulation(cfg_w, case.n) as sim:
+        reset(sim)
+        sim.adjoint_forward(nw, dt_w, checkpoint_every=MS_EVERY, loss=S.LOSS_DRAG, body_motion=mo_w[:nw])
+        sim.adjoint_backward(scale_w)
+        gw = np.einsum("sq,sqk->k", sim.adjoint_motion_gradient(), jac_w[:nw])
+    fd_w = []
+    for k in (0, 2):
+        eps = 1e-6
+        cp, cm = coeffs.copy(), coeffs.copy()
+        cp[k] += eps
+        cm[k] -= eps
+        f = (loss_w(cp) - loss_w(cm)) / (2 * eps)
+        fd_w.append({"coefficient": k, "adjoint": float(gw[k]), "fd": f, "rel_err": abs(gw[k] - f) / abs(f)})
     return {
         "case": f"moving square D=1 in [0,10]x[0,5], dx=D/50 ({case.n} particles incl. ghosts), Re=100, "
                 f"MS modified linear Riemann + delta-SPH, ghost assignment, Euler PC, FP64, {MS_STEPS} steps, "
@@ -614,6 +645,9 @@ def adjoint_ms_report(S):
         "adjoint_over_forward_device": tb.total_ms / dev_fwd, "backward_reverse_kernels_ms": tb.adjoint_ms,
         "dC_d_coeffs": [float(x) for x in gc], "dC_dnu": g["nu"], "fd": fd,
         "fd_note": f"central differences eps=1e-8 of the FP64 forward over the first {MS_FD_STEPS} steps",
+        "fd_wendland": fd_w,
+        "fd_wendland_note": (f"the same case with the Wendland C2 kernel (h = 1.3 dx), {MS_FD_STEPS_WENDLAND} steps, "
+                             "central differences eps=1e-6 of coefficients 0 and 2"),
     }
 
 
