@@ -291,6 +291,9 @@ struct Model {
         }
         // MUSCL: normalised gradients of p, u, v (Solver_Normalized_MUSCL_Linear_Riemann_Delta_SPS.f90:151-185)
         const bool muscl = C.solver == SPH_SOLVER_MUSCL_DELTA_SPS;
+        // the plain delta-SPH method (Solver_Normalized_Delta_SPH_SPS.f90:335-374,
+        // 610-636): no Riemann state (v* = v-bar, P* = P-bar), Antuono's diffusion
+        const bool dsph = C.solver == SPH_SOLVER_DELTA_SPS;
         std::vector<T> gp[2], gu[2], gv[2];
         if (muscl) {
             for (int q = 0; q < 2; ++q) { gp[q].assign(n, T(0.0)); gu[q].assign(n, T(0.0)); gv[q].assign(n, T(0.0)); }
@@ -339,9 +342,10 @@ struct Model {
             const T dU = UL - UR;
             const T m3 = val(dU) > 0.0 ? 3.0 * dU : T(0.0);
             const T bR = val(m3) < val(cbar) ? m3 : cbar;
-            const T Ps = Pbar + 0.5 * bR * rbar * dU;
-            const T tmi = (uI - vs0) * ni0[k] + (vI - vs1) * ni1[k];
-            const T tmj = -((uJ - vs0) * nj0[k] + (vJ - vs1) * nj1[k]);
+            const T Ps = dsph ? Pbar : Pbar + 0.5 * bR * rbar * dU;
+            const T ws0 = dsph ? vbar0 : vs0, ws1 = dsph ? vbar1 : vs1;
+            const T tmi = (uI - ws0) * ni0[k] + (vI - ws1) * ni1[k];
+            const T tmj = -((uJ - ws0) * nj0[k] + (vJ - ws1) * nj1[k]);
             cont[i] += 2.0 * ri * Vj * tmi;
             cont[j] += 2.0 * rj * Vi * tmj;
             const T rij = 1.0 / (ri * rj);
@@ -386,9 +390,15 @@ struct Model {
             const T pd0 = -dx0[k], pd1 = -dx1[k];
             const T r2 = pd0 * pd0 + pd1 * pd1;
             const T dr = -(P.rho[i] - P.rho[j]);
+            const T cbar = (c[i] + c[j]) / 2.0;
+            if (dsph) {
+                const T ps0 = 2.0 * dr / r2 * pd0 - (g0[i] + g0[j]), ps1 = 2.0 * dr / r2 * pd1 - (g1[i] + g1[j]);
+                corr[i] += C.delta * hb * cbar * (ps0 * ni0[k] + ps1 * ni1[k]) * vol[j];
+                corr[j] -= C.delta * hb * cbar * (ps0 * nj0[k] + ps1 * nj1[k]) * vol[i];
+                continue;
+            }
             const T psi = dr - 0.5 * ((g0[i] + g0[j]) * pd0 + (g1[i] + g1[j]) * pd1);
             const T tmi = (pd0 * ni0[k] + pd1 * ni1[k]) / r2, tmj = (pd0 * nj0[k] + pd1 * nj1[k]) / r2;
-            const T cbar = (c[i] + c[j]) / 2.0;
             corr[i] += 2.0 * C.delta * hb * cbar * psi * tmi * vol[j];
             corr[j] -= 2.0 * C.delta * hb * cbar * psi * tmj * vol[i];
         }
@@ -800,9 +810,9 @@ struct MSModel {
             const T pd0 = -dx0[k], pd1 = -dx1[k];
             const T r2 = pd0 * pd0 + pd1 * pd1;
             const T dr = -(P.rho[i] - P.rho[j]);
+            const T cbar = (c[i] + c[j]) / 2.0;
             const T psi = dr - 0.5 * ((g0[i] + g0[j]) * pd0 + (g1[i] + g1[j]) * pd1);
             const T tmi = (pd0 * ni0[k] + pd1 * ni1[k]) / r2, tmj = (pd0 * nj0[k] + pd1 * nj1[k]) / r2;
-            const T cbar = (c[i] + c[j]) / 2.0;
             corr[i] += 2.0 * C.delta * hb * cbar * psi * tmi * vol[j];
             corr[j] += -(2.0 * C.delta * hb * cbar * psi * tmj * vol[i]);
         }
@@ -917,7 +927,8 @@ int oracle_tangent(const sph_config* cfg, int n, const double* pos, const double
                    double dnu, int nsteps, double dt, int loss, const double* target_vel, double* out,
                    double* pos_out, double* vel_out, double* rho_out) {
     if (!cfg || !pos || !vel || !rho || !mass || !type || !out || n <= 0 || nsteps <= 0) return SPH_E_ARG;
-    if ((cfg->solver != SPH_SOLVER_MODLR_DELTA_SPS && cfg->solver != SPH_SOLVER_MUSCL_DELTA_SPS) ||
+    if ((cfg->solver != SPH_SOLVER_MODLR_DELTA_SPS && cfg->solver != SPH_SOLVER_MUSCL_DELTA_SPS &&
+         cfg->solver != SPH_SOLVER_DELTA_SPS) ||
         cfg->integrator != SPH_INTEGRATOR_RK4_REUSE ||
         cfg->xsph_eps != 0.0 || cfg->pair_rule != SPH_PAIRS_ONE_FLUID || cfg->mls_order != 0)
         return SPH_E_CONFIG;

@@ -320,7 +320,9 @@ __device__ __forceinline__ void rev_pair(const Params& P, const PSide& A, const 
         PA = P.c0sq * dH + P.pb;
         w0 = hal * he0 - hbe * he1;
         w1 = hal * he1 + hbe * he0;
-    } else if (A.near) {
+    } else if (A.near || P.dsph) {
+        // the pair-mean state: near the free surface, and for every pair of the
+        // plain delta-SPH method (Solver_Normalized_Delta_SPH_SPS.f90:335-374)
         PA = Pbar; w0 = 0.5 * du0 + su; w1 = 0.5 * du1 + sv;
     } else {
         const double m3 = 3.0 * fmax(dU, 0.0);
@@ -407,7 +409,22 @@ __device__ __forceinline__ void rev_pair(const Params& P, const PSide& A, const 
         Gb += 2.0 * A.rho * B.V * WN * lr;
         w0b = k2 * n0; w1b = k2 * n1;
         n0b += k2 * w0; n1b += k2 * w1;
-        if (A.water) {
+        if (A.water && P.dsph) {
+            // Antuono form (Solver_Normalized_Delta_SPH_SPS.f90:610-636) in a's frame:
+            // D_a += delta h cbar G V_b Y, Y = 2 (rho_a - rho_b) s/d^2 - (grad rho_a + grad rho_b).n
+            const double K = P.delta * P.h * lr;
+            const double sg0 = A.g0 + B.g0, sg1 = A.g1 + B.g1;
+            const double Y = 2.0 * drho * s * id2 - (sg0 * n0 + sg1 * n1);
+            cbarb += K * G * B.V * Y;
+            Gb += K * cbar * B.V * Y;
+            Vbb += K * cbar * G * Y;
+            const double Yb = K * cbar * G * B.V;
+            rab += 2.0 * s * id2 * Yb; rbb -= 2.0 * s * id2 * Yb;
+            sb += 2.0 * drho * id2 * Yb;
+            db -= 4.0 * drho * s * id2 * id * Yb;
+            o.g0 = -n0 * Yb; o.g1 = -n1 * Yb;
+            n0b -= sg0 * Yb; n1b -= sg1 * Yb;
+        } else if (A.water) {
             const double T2 = 2.0 * P.delta * P.h * lr;
             const double sg0 = A.g0 + B.g0, sg1 = A.g1 + B.g1;
             const double psi = -drho + 0.5 * (sg0 * r0 + sg1 * r1);
@@ -473,7 +490,7 @@ __device__ __forceinline__ void rev_pair(const Params& P, const PSide& A, const 
     } else {
         Pbarb += PAb0;
     }
-    if (!A.near && !hllc) {
+    if (!A.near && !P.dsph && !hllc) {
         const double kkb = w0b * r0 + w1b * r1;
         r0b += kk * w0b; r1b += kk * w1b;
         dpb += kkb * (0.5 * irbar * ic0) * id;

@@ -790,7 +790,9 @@ int adj_config_ok(const sph_handle* h, int loss) {
             return SPH_E_CONFIG;
         if (h->cfg.integrator != SPH_INTEGRATOR_EULER_PC || h->cfg.periodic) return SPH_E_CONFIG;
     } else {
-        if ((h->cfg.solver != SPH_SOLVER_MODLR_DELTA_SPS && h->cfg.solver != SPH_SOLVER_MUSCL_DELTA_SPS) || P.xsph)
+        if ((h->cfg.solver != SPH_SOLVER_MODLR_DELTA_SPS && h->cfg.solver != SPH_SOLVER_MUSCL_DELTA_SPS &&
+             h->cfg.solver != SPH_SOLVER_DELTA_SPS) ||
+            P.xsph)
             return SPH_E_CONFIG;
         if (h->cfg.integrator != SPH_INTEGRATOR_RK4_REUSE) return SPH_E_CONFIG;
     }

@@ -41,6 +41,11 @@ def _case(kind):
     Taylor-Green case shifts every step); the others switch it off."""
     if kind.startswith("muscl"):
         case = S.make_tgv(32, solver=S.SOLVER_MUSCL_DELTA_SPS, jitter=0.05, seed=13)
+    elif kind.startswith("plain"):
+        # the plain delta-SPH method (Solver_Normalized_Delta_SPH_SPS.f90): the
+        # pair-mean state for every pair and Antuono's density diffusion
+        case = S.make_tgv(32, solver=S.SOLVER_DELTA_SPS, jitter=0.05, seed=14)
+        case.cfg.xsph_eps = 0.0
     elif kind.startswith("wendland-renorm"):
         case = S.make_tgv(32, solver=S.SOLVER_MODLR_DELTA_SPS, jitter=0.05, seed=11)
     else:
@@ -100,7 +105,7 @@ def _check(ad, fd, what):
 
 
 @pytest.mark.parametrize("kind", ["wendland-renorm", "reference-gaussian", "wendland-renorm-shift",
-                                  "reference-gaussian-shift", "muscl", "muscl-shift"])
+                                  "reference-gaussian-shift", "muscl", "muscl-shift", "plain", "plain-shift"])
 @pytest.mark.parametrize("pre_steps", [0, 3])
 def test_adjoint_matches_central_differences(lib, kind, pre_steps):
     case = _case(kind)
@@ -174,9 +179,10 @@ def test_adjoint_rejects_unsupported_configurations(lib):
         with pytest.raises(S.SphError) as e:
             sim.adjoint_backward()
         assert e.value.code == -1
-    # the plain delta-SPH method is not differentiated
-    case = S.make_tgv(16, solver=S.SOLVER_DELTA_SPS)
+    # the modified solver with XSPH velocities is not differentiated
+    case = S.make_tgv(16, solver=S.SOLVER_MODLR_DELTA_SPS)
     case.cfg.mls_order = 0
+    case.cfg.xsph_eps = 0.5
     with S.Simulation(case.cfg, case.n) as sim:
         sim.set_state(case.pos, case.vel, case.rho, case.mass, case.type)
         with pytest.raises(S.SphError) as e:
@@ -200,7 +206,7 @@ def test_adjoint_of_the_mixed_precision_step(lib):
 
 
 @pytest.mark.parametrize("kind", ["wendland-renorm", "reference-gaussian", "wendland-renorm-shift",
-                                  "reference-gaussian-shift", "muscl", "muscl-shift"])
+                                  "reference-gaussian-shift", "muscl", "muscl-shift", "plain", "plain-shift"])
 def test_adjoint_matches_cpu_tangent_linear_reference(lib, oracle, kind):
     """g.delta from the GPU adjoint against the FP64 CPU tangent-linear model of
     the same steps (oracle/sph_tangent.cpp, forward-mode derivative with the

@@ -10,6 +10,10 @@ import sph_b200 as S
 def _case(kind):
     if kind.startswith("muscl"):
         case = S.make_tgv(24, solver=S.SOLVER_MUSCL_DELTA_SPS, jitter=0.05, seed=6)
+    elif kind.startswith("plain"):
+        # the plain delta-SPH method (Solver_Normalized_Delta_SPH_SPS.f90)
+        case = S.make_tgv(24, solver=S.SOLVER_DELTA_SPS, jitter=0.05, seed=8)
+        case.cfg.xsph_eps = 0.0
     elif kind.startswith("wendland-renorm"):
         case = S.make_tgv(24, solver=S.SOLVER_MODLR_DELTA_SPS, jitter=0.05, seed=3)
     else:
@@ -20,7 +24,7 @@ def _case(kind):
 
 
 KINDS = ["wendland-renorm", "reference-gaussian", "wendland-renorm-shift", "reference-gaussian-shift", "muscl",
-         "muscl-shift"]
+         "muscl-shift", "plain", "plain-shift"]
 
 
 @pytest.mark.parametrize("kind", KINDS)
