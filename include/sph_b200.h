@@ -69,7 +69,7 @@ extern "C" {
 #define SPH_PAIRS_NO_SAME_BND 1 /* MS  Find_particle_pair.f90:73-75 drop -2/-2, -3/-3, -201/-201 */
 
 #define SPH_PREC_FP64   0   /* every field and pair term in FP64                     */
-#define SPH_PREC_MIXED  1   /* FP32 pair arithmetic + compensated sums, FP64 state   */
+#define SPH_PREC_MIXED  1   /* FP32 pair arithmetic summed in FP64, FP64 state         */
 
 #define SPH_INTEGRATOR_RK4_REUSE 0 /* time_iteration.f90:781-1159 (3 RHS/step after step 1) */
 #define SPH_INTEGRATOR_EULER_PC  1 /* Moving_Square.../SPH_Time_Iteration.f90:304-334, Iteration_Method 2 (1 RHS/step) */
@@ -333,8 +333,9 @@ int sph_find_particle_pair_noalloc(const sph_config* cfg, int n, const double* d
  * Supported configurations (others return SPH_E_CONFIG), either kernel, with
  * or without renormalisation, without MLS density re-initialisation:
  *  - the normalised modified linear Riemann and MUSCL linear Riemann delta-SPH
- *    + SPS solvers (SPH_SOLVER_MODLR_DELTA_SPS without XSPH,
- *    SPH_SOLVER_MUSCL_DELTA_SPS) with the RK4 driver, with or without particle
+ *    + SPS solvers and the plain delta-SPH method (SPH_SOLVER_MODLR_DELTA_SPS
+ *    without XSPH, SPH_SOLVER_MUSCL_DELTA_SPS, SPH_SOLVER_DELTA_SPS) with the
+ *    RK4 driver, with or without particle
  *    shifting (the limiter, the capped shift and its density correction are
  *    differentiated on the branch the forward took);
  *  - the moving-square modified linear Riemann and HLLC solvers
