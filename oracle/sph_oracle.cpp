@@ -1292,6 +1292,36 @@ void mls_reinit(Particles& P, int n_host) {
     for (int i = 0; i < n_host; ++i) P.rho[i] = rho_new[i];
 }
 
+// RefreshDensity_MLS_Order = 1 (Taylor_Green_Vortex/Reinitialize_particle_density.f90:71-92,
+// Moving_Square.../Reinitialize_particle_density.f90:66-88) on the pair list and
+// volumes of the step's last RHS: for pairs of particles of the same type,
+// rho_i += m_j w_ij / sum_w(i) for water particles, sum_w(i) = sum_j w_ij V_j over
+// the same pairs (Define_freesurface_and_Normailized_derivates.f90:87-91).  Other
+// particles keep their density.
+void mls_order1(Particles& P, int n_host, const Rhs& R) {
+    const PairList& L = R.L;
+    std::vector<double> sw(P.n, 0.0), rho(P.n, 0.0);
+    for (size_t k = 0; k < L.size(); ++k) {
+        const int i = L.pi[k], j = L.pj[k];
+        if (P.type[i] != P.type[j]) continue;
+        sw[i] += L.w[k] * R.vol[j];
+        sw[j] += L.w[k] * R.vol[i];
+    }
+    for (size_t k = 0; k < L.size(); ++k) {
+        const int i = L.pi[k], j = L.pj[k];
+        if (P.type[i] != P.type[j]) continue;
+        if (P.type[i] == SPH_TYPE_WATER) rho[i] += P.mass[j] * L.w[k] / sw[i];
+        if (P.type[j] == SPH_TYPE_WATER) rho[j] += P.mass[i] * L.w[k] / sw[j];
+    }
+    for (int i = 0; i < n_host; ++i)
+        if (P.type[i] == SPH_TYPE_WATER) P.rho[i] = rho[i];
+}
+
+void reinit_density(Particles& P, int n_host, const Rhs& R) {
+    if (g_cfg.mls_order == 1) mls_order1(P, n_host, R);
+    else mls_reinit(P, n_host);
+}
+
 struct Sim {
     sph_config cfg;
     Particles H;                      // host particles
@@ -1360,7 +1390,7 @@ void run_step_euler_pc(Sim& S, double dt) {
     S.racc1.assign(R.acc[1].begin(), R.acc[1].begin() + n);
     S.ravg0.assign(R.avg[0].begin(), R.avg[0].begin() + n);
     S.ravg1.assign(R.avg[1].begin(), R.avg[1].begin() + n);
-    if (g_cfg.mls_order && (S.step + 1) % g_cfg.mls_every == 0) mls_reinit(P, n);
+    if (g_cfg.mls_order && (S.step + 1) % g_cfg.mls_every == 0) reinit_density(P, n, R);
     if (g_cfg.shifting) shift_particles(P, n, R);
     for (int i = 0; i < n; ++i) {
         S.H.x[i] = P.x[i]; S.H.y[i] = P.y[i]; S.H.u[i] = P.u[i]; S.H.v[i] = P.v[i]; S.H.rho[i] = P.rho[i];
@@ -1449,7 +1479,7 @@ void run_step(Sim& S, double dt) {
     S.ravg0.assign(R.avg[0].begin(), R.avg[0].begin() + n);
     S.ravg1.assign(R.avg[1].begin(), R.avg[1].begin() + n);
     // Reinitialize_particle_density every MLS_time_step steps, before shifting (:673-682)
-    if (g_cfg.mls_order && (S.step + 1) % g_cfg.mls_every == 0) mls_reinit(P, n);
+    if (g_cfg.mls_order && (S.step + 1) % g_cfg.mls_every == 0) reinit_density(P, n, R);
     if (g_cfg.shifting) shift_particles(P, n, R);
     // copy the host particles back (images are discarded)
     for (int i = 0; i < n; ++i) {

@@ -138,7 +138,7 @@ int derive_params(const sph_config& c, Params& P) {
     if (!(c.h > 0) || !(c.kernel_scale >= 2.0) || !(c.dx > 0) || !(c.rho0 > 0) || !(c.c0sq > 0)) return SPH_E_CONFIG;
     if (c.cell_skin < 0 || c.cell_skin > 2) return SPH_E_CONFIG;
     if (c.shift_n != 4) return SPH_E_CONFIG;
-    if (c.mls_order != 0 && c.mls_order != 3 && c.mls_order != 6) return SPH_E_CONFIG;
+    if (c.mls_order != 0 && c.mls_order != 1 && c.mls_order != 3 && c.mls_order != 6) return SPH_E_CONFIG;
     if (c.mls_order != 0 && (c.mls_every < 1 || !(c.mls_alpha >= 0))) return SPH_E_CONFIG;
     if (c.ghost_assign != 0 && c.ghost_assign != 1) return SPH_E_CONFIG;
     if (c.ghost_assign && (!(c.ghost_h_factor > 0) || (c.wall_bc != 0 && c.wall_bc != 1))) return SPH_E_CONFIG;
@@ -505,11 +505,24 @@ int reinit_density(sph_handle* h, int do_shift) {
     Sorted<R>& D = sorted<R>(h);
     const int nb = blocks(P.n_tot, 128);
     tic(h, PH_UPDATE);
+    // (order 1 formed its densities on the step's last RHS: mls1_on_last_rhs)
     if (P.mls_order == 6) k_mls<R, 6><<<nb, 128, 0, h->stream>>>(P, D, h->d_mls);
-    else k_mls<R, 3><<<nb, 128, 0, h->stream>>>(P, D, h->d_mls);
+    else if (P.mls_order == 3) k_mls<R, 3><<<nb, 128, 0, h->stream>>>(P, D, h->d_mls);
     k_finish_mls<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, D, h->d_mls, do_shift, h->d_status);
     CK(cudaGetLastError());
-    h->launches += 2;
+    h->launches += P.mls_order == 1 ? 1 : 2;
+    return SPH_OK;
+}
+
+// MLS order 1 reads the pair list and state of the step's last RHS: formed right
+// after it, before the stage that ends the step moves the particles.
+template <typename R>
+int mls1_on_last_rhs(sph_handle* h) {
+    const Params& P = h->P;
+    tic(h, PH_UPDATE);
+    k_mls1<R><<<blocks(P.n_tot, 128), 128, 0, h->stream>>>(P, sorted<R>(h), h->d_mls);
+    CK(cudaGetLastError());
+    h->launches += 1;
     return SPH_OK;
 }
 
@@ -554,9 +567,11 @@ int run_steps(sph_handle* h, int nsteps, double dt) {
         // after or outside it)
         const int to_staging = (!h->P.ms && !h->P.ghost_assign && !mls) ? 1 : 0;
         if (first) { rc = rhs<R>(h, 0); if (rc) return rc; }
+        const bool mls1 = mls && h->P.mls_order == 1;
         if (h->cfg.integrator == SPH_INTEGRATOR_EULER_PC) {
             rc = stage<R>(h, 10, dt, first ? 0 : 1, 0); if (rc) return rc;
             rc = rhs<R>(h, 1); if (rc) return rc;
+            if (mls1 && (rc = mls1_on_last_rhs<R>(h))) return rc;
             rc = stage<R>(h, 11, dt, 0, shift_now); if (rc) return rc;
         } else {
             rc = stage<R>(h, 0, dt, first ? 0 : 1, 0); if (rc) return rc;
@@ -565,6 +580,7 @@ int run_steps(sph_handle* h, int nsteps, double dt) {
             rc = rhs<R>(h, 0); if (rc) return rc;
             rc = stage<R>(h, 2, dt, 0, 0); if (rc) return rc;
             rc = rhs<R>(h, 1); if (rc) return rc;
+            if (mls1 && (rc = mls1_on_last_rhs<R>(h))) return rc;
             rc = stage<R>(h, 3, dt, 0, shift_now, to_staging); if (rc) return rc;
             if (to_staging) h->staging_valid = true;
         }

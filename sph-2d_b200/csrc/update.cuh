@@ -262,6 +262,38 @@ __global__ void k_mls(Params P, Sorted<R> D, double* rho_new) {
     rho_new[a] = out;
 }
 
+// RefreshDensity_MLS_Order = 1 (Taylor_Green_Vortex/Reinitialize_particle_density.f90:71-92,
+// Moving_Square.../Reinitialize_particle_density.f90:66-88), evaluated on the
+// step's last RHS (its pair list and state, which the reference's pair arrays
+// and volumes still hold when it runs): for a water particle a,
+//   rho_a = sum_b m_b W_ab / sum_b W_ab V_b
+// over the pairs with a neighbour of a's type (sum_w,
+// Define_freesurface_and_Normailized_derivates.f90:87-91), in FP64.
+template <typename R>
+__global__ void k_mls1(Params P, Sorted<R> D, double* rho_new) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= P.n_tot) return;
+    rho_new[a] = D.kin[a].z;
+    const int ta = D.type[a];
+    if (ta != SPH_TYPE_WATER || D.id[a] >= P.n_host) return;
+    const double2 xa = D.pos[a];
+    double sw = 0.0, sm = 0.0;
+    const int nn = D.npairs[a];
+    for (int e = 0; e < nn; ++e) {
+        const int b = (int)(D.pairs[(size_t)e * P.nbr_stride + a] & 0x7fffffffu);
+        if (D.type[b] != ta) continue;
+        const double2 xb = D.pos[b];
+        const double px = xa.x - xb.x, py = xa.y - xb.y;
+        const double d = __dsqrt_rn(__dadd_rn(__dmul_rn(px, px), __dmul_rn(py, py)));
+        double w, gx, gy;
+        kernel_w_dw<double>(P, d, px, py, w, gx, gy);
+        const double mb = D.mass[b];
+        sw += w * (mb / D.kin[b].z);
+        sm += mb * w;
+    }
+    rho_new[a] = sm / sw;
+}
+
 // The re-initialised density replaces the integrated one; then the shift of the
 // step (when on) is applied, as the reference's driver calls the two in turn.
 template <typename R>

@@ -1,8 +1,9 @@
 """GPU parity of the MLS density re-initialisation (Reinitialize_particle_density)
 against the oracle: several steps with a re-initialisation every few steps, on
 the Taylor-Green case (quadratic MLS, the reference's shipped setting, and with
-the benchmark's MUSCL solver) and on the moving-square case (linear MLS,
-Euler predictor-corrector), FP64, 1e-10 norm-wise."""
+the benchmark's MUSCL solver; order 1, the Shepard-normalised mass sum over the
+last RHS's same-type pairs) and on the moving-square case (linear MLS and
+order 1, Euler predictor-corrector), FP64, 1e-10 norm-wise."""
 import numpy as np
 import pytest
 
@@ -29,7 +30,8 @@ def _run_both(oracle, case, nsteps, dt, itype=None):
     return got, ref.state()
 
 
-@pytest.mark.parametrize("name", ["reference-order6", "muscl-order6", "modlr-order3"])
+@pytest.mark.parametrize("name", ["reference-order6", "muscl-order6", "modlr-order3", "muscl-order1",
+                                  "reference-order1"])
 def test_reinitialisation_tgv(lib, oracle, name):
     if name == "reference-order6":
         case = S.make_tgv(40, reference=True, jitter=0.05, seed=21)
@@ -39,7 +41,7 @@ def test_reinitialisation_tgv(lib, oracle, name):
         case = S.make_tgv(40, solver=solver, jitter=0.05, seed=22)
         case.cfg.mls_alpha = 1e-4
         dt = S.baseline_dt(case.cfg)
-    case.cfg.mls_order = 3 if name == "modlr-order3" else 6
+    case.cfg.mls_order = 3 if name == "modlr-order3" else 1 if name.endswith("order1") else 6
     case.cfg.mls_every = 3
     (pos, vel, rho, _), (rpos, rvel, rrho, _) = _run_both(oracle, case, 7, dt)
     assert relerr(rho - case.cfg.rho0, rrho - case.cfg.rho0) < 1e-10
@@ -55,8 +57,10 @@ def test_reinitialisation_tgv(lib, oracle, name):
     assert relerr(rho0 - case.cfg.rho0, rrho - case.cfg.rho0) > 1e-6
 
 
-def test_reinitialisation_moving_square(lib, oracle):
+@pytest.mark.parametrize("order", [3, 1])
+def test_reinitialisation_moving_square(lib, oracle, order):
     case, ity = S.make_moving_square(solver=S.SOLVER_MS_HLLC_DELTA, jitter=0.05, seed=23)
+    case.cfg.mls_order = order
     case.cfg.mls_every = 3
     dt = 0.25 * case.cfg.h / np.sqrt(case.cfg.c0sq)
     (pos, vel, rho, _), (rpos, rvel, rrho, _) = _run_both(oracle, case, 7, dt, ity)
