@@ -115,8 +115,9 @@ typedef struct sph_config {
     int    free_surface;      /* Has_FreeSurface_Or_Not: 1 detect free-surface particles, 0 none */
     /* MLS density re-initialisation (Reinitialize_particle_density), run after the
      * integrator update and before shifting of every mls_every-th step:
-     * mls_order 0 off, 3 linear or 6 quadratic moving least squares
-     * (RefreshDensity_MLS_Order; order 1 is not built and returns SPH_E_CONFIG),
+     * mls_order 0 off, 1 the Shepard-normalised mass sum over the step's last
+     * pair list (sum m_j W_ij / sum W_ij V_j over same-type pairs), 3 linear or
+     * 6 quadratic moving least squares (RefreshDensity_MLS_Order),
      * mls_every = MLS_time_step / RefreshDensity_time_step,
      * mls_alpha = slighted_modified_alpha (the moment matrix gets alpha^3 on its diagonal). */
     int    mls_order;
