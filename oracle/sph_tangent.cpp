@@ -24,8 +24,8 @@
 // the modified linear Riemann and the HLLC solvers with XSPH in the continuity flux, the
 // fixed-ghost assignment, the body force and the Euler predictor-corrector with
 // a per-step body motion (oracle_tangent_ms).  Either kernel, with or without
-// renormalisation, with or without shifting in (1) and without in (2), no
-// density re-initialisation, no free-surface particles.  Other inputs return SPH_E_CONFIG.  The pair search is a plain
+// renormalisation, with or without shifting in (1) and without in (2), density
+// re-initialisation (orders 1, 3, 6) in (1) only, no free-surface particles.  Other inputs return SPH_E_CONFIG.  The pair search is a plain
 // double loop (small cases only).
 
 #include <cmath>
@@ -198,7 +198,7 @@ struct Model {
     // this RHS's pairs, sh[0..1][i] = -beta h^2 sum_j (1 + R (w/w_dx)^4) V_j
     // B_i^-1 grad_i W, and the normalised density gradient gr[0..1].
     int rhs(const Parts<T>& P, std::vector<T>& drho, std::vector<T>& acc0, std::vector<T>& acc1,
-            std::vector<T>* sh = nullptr, std::vector<T>* gr = nullptr) const {
+            std::vector<T>* sh = nullptr, std::vector<T>* gr = nullptr, std::vector<T>* o1 = nullptr) const {
         const int n = P.n;
         std::vector<T> p(n), c(n), vol(n);
         for (int i = 0; i < n; ++i) { eos(P.rho[i], p[i], c[i]); vol[i] = P.mass[i] / P.rho[i]; }
@@ -221,6 +221,23 @@ struct Model {
             dx0[k] = P.x[i] - P.x[j]; dx1[k] = P.y[i] - P.y[j];
             const T d = sqrt(dx0[k] * dx0[k] + dx1[k] * dx1[k]);
             kernel(d, dx0[k], dx1[k], hb, w[k], dw0[k], dw1[k]);
+        }
+        if (o1) {
+            // RefreshDensity_MLS_Order = 1 on this RHS's pairs (Reinitialize_particle_density.f90:71-92):
+            // rho_i = sum m_j w_ij / sum_w(i), sum_w(i) = sum w_ij V_j, same-type pairs
+            std::vector<T> sw(n, T(0.0)), acc(n, T(0.0));
+            for (size_t k = 0; k < np; ++k) {
+                const int i = pi[k], j = pj[k];
+                if (P.type[i] != P.type[j]) continue;
+                sw[i] += w[k] * vol[j]; sw[j] += w[k] * vol[i];
+            }
+            for (size_t k = 0; k < np; ++k) {
+                const int i = pi[k], j = pj[k];
+                if (P.type[i] != P.type[j]) continue;
+                if (P.type[i] == SPH_TYPE_WATER) acc[i] += P.mass[j] * w[k] / sw[i];
+                if (P.type[j] == SPH_TYPE_WATER) acc[j] += P.mass[i] * w[k] / sw[j];
+            }
+            *o1 = acc;
         }
         // volume fraction: free-surface candidates are outside this model's scope
         if (C.free_surface) {
@@ -425,6 +442,64 @@ struct Model {
         return SPH_OK;
     }
 
+    // Reinitialize_particle_density, orders 3 and 6 (Reinitialize_particle_density.f90:
+    // 98-181, MLS_Interpolation_In_Subdomain_Domain.f90:96-285) for the water
+    // particles among the first n, from every particle within the support at the
+    // current positions: rho_i = c.r with A c = e_1, A = sum W p p^T + alpha^3 I,
+    // r = sum rho_j W p, p = (1, dx, dy[, dx^2, dx dy, dy^2]), (dx, dy) = (x_j - x_i)/h;
+    // Shepard weights W / sum W when A is singular or, at order 6, with at most 8
+    // neighbours.  A c = e_1 by Gaussian elimination (A is symmetric positive
+    // definite; the oracle inverts it by Gauss-Jordan, the same c to rounding).
+    void mls(Parts<T>& P, int n) const {
+        const int m = C.mls_order;
+        const double hb = (C.h + C.h) / 2.0, rcut = C.kernel_scale * hb;
+        const double a3 = C.mls_alpha * C.mls_alpha * C.mls_alpha;
+        std::vector<T> out(n);
+        for (int i = 0; i < n; ++i) {
+            out[i] = P.rho[i];
+            if (P.type[i] != SPH_TYPE_WATER) continue;
+            T A[6][7], r[6];
+            for (int a = 0; a < 6; ++a) { r[a] = T(0.0); for (int b = 0; b < 7; ++b) A[a][b] = T(0.0); }
+            T sw(0.0), srw(0.0);
+            int k = 0;
+            for (int j = 0; j < P.n; ++j) {
+                const T px = P.x[i] - P.x[j], py = P.y[i] - P.y[j];
+                const double d0 = std::sqrt(val(px) * val(px) + val(py) * val(py));
+                if (!(d0 <= rcut) || !(d0 >= K.cut_min)) continue;
+                T w, g0, g1;
+                kernel(sqrt(px * px + py * py), px, py, hb, w, g0, g1);
+                const T dx = -px / C.h, dy = -py / C.h;
+                const T p[6] = {T(1.0), dx, dy, dx * dx, dx * dy, dy * dy};
+                for (int a = 0; a < m; ++a) {
+                    for (int b = 0; b < m; ++b) A[a][b] += w * p[a] * p[b];
+                    r[a] += P.rho[j] * w * p[a];
+                }
+                sw += w; srw += P.rho[j] * w;
+                ++k;
+            }
+            for (int a = 0; a < m; ++a) { A[a][a] += a3; A[a][m] = T(a == 0 ? 1.0 : 0.0); }
+            bool ok = true;
+            for (int c = 0; c < m && ok; ++c) {
+                if (!(val(A[c][c]) > 0.0)) { ok = false; break; }
+                for (int q = c + 1; q < m; ++q) {
+                    const T f = A[q][c] / A[c][c];
+                    for (int b = c; b <= m; ++b) A[q][b] -= f * A[c][b];
+                }
+            }
+            if (!ok || (m == 6 && k <= 8)) { out[i] = srw / sw; continue; }
+            T cs[6];
+            for (int a = m - 1; a >= 0; --a) {
+                T t = A[a][m];
+                for (int b = a + 1; b < m; ++b) t -= A[a][b] * cs[b];
+                cs[a] = t / A[a][a];
+            }
+            T rho(0.0);
+            for (int a = 0; a < m; ++a) rho += cs[a] * r[a];
+            out[i] = rho;
+        }
+        for (int i = 0; i < n; ++i) P.rho[i] = out[i];
+    }
+
     // Distribute_Period_Boundary_Particle (:56-206): wrap, then left/right images
     // of the hosts and bottom/top images of hosts and left/right images.
     void images(std::vector<T>& hx, std::vector<T>& hy, const std::vector<T>& hu, const std::vector<T>& hv,
@@ -484,7 +559,9 @@ int run(const sph_config& cfg, int n, const T* x0, const T* y0, const T* u0, con
             for (int i = 0; i < n; ++i) { dr[i] = cr[i]; a0[i] = ca0[i]; a1[i] = ca1[i]; }
         }
         std::vector<T> Kr(n), Ka0(n), Ka1(n), Kv0(n), Kv1(n);
-        std::vector<T> sh[2], gr[2];
+        std::vector<T> sh[2], gr[2], o1;
+        // density re-initialisation after every mls_every-th step (1-based)
+        const bool mls_step = cfg.mls_order != 0 && (s + 1) % cfg.mls_every == 0;
         // stages (time_iteration.f90:942-1047): water particles only
         for (int st = 0; st < 3; ++st) {
             const double f = st < 2 ? 0.5 * dt : dt;
@@ -499,7 +576,9 @@ int run(const sph_config& cfg, int n, const T* x0, const T* y0, const T* u0, con
                 Kr[i] += wgt * dr[i]; Ka0[i] += wgt * a0[i]; Ka1[i] += wgt * a1[i];
                 Kv0[i] += wgt * P.u[i]; Kv1[i] += wgt * P.v[i];
             }
-            if ((rc = M.rhs(P, dr, a0, a1, st == 2 && cfg.shifting ? sh : nullptr, gr))) return rc;
+            if ((rc = M.rhs(P, dr, a0, a1, st == 2 && cfg.shifting ? sh : nullptr, gr,
+                            st == 2 && mls_step && cfg.mls_order == 1 ? &o1 : nullptr)))
+                return rc;
         }
         for (int i = 0; i < n; ++i) {
             if (P.type[i] != SPH_TYPE_WATER) continue;
@@ -508,6 +587,14 @@ int run(const sph_config& cfg, int n, const T* x0, const T* y0, const T* u0, con
             P.x[i] = B0.x[i] + (Kv0[i] + P.u[i]) * dt / 6.0 + 0.5 * dt * dt * a0[i];
             P.v[i] = B0.v[i] + (Ka1[i] + a1[i]) * dt / 6.0;
             P.y[i] = B0.y[i] + (Kv1[i] + P.v[i]) * dt / 6.0 + 0.5 * dt * dt * a1[i];
+        }
+        if (mls_step) {
+            if (cfg.mls_order == 1) {
+                for (int i = 0; i < n; ++i)
+                    if (P.type[i] == SPH_TYPE_WATER) P.rho[i] = o1[i];
+            } else {
+                M.mls(P, n);
+            }
         }
         if (cfg.shifting) {
             // Shift_particle_position.f90:97-136 on the last RHS's pairs: capped
@@ -930,7 +1017,7 @@ int oracle_tangent(const sph_config* cfg, int n, const double* pos, const double
     if ((cfg->solver != SPH_SOLVER_MODLR_DELTA_SPS && cfg->solver != SPH_SOLVER_MUSCL_DELTA_SPS &&
          cfg->solver != SPH_SOLVER_DELTA_SPS) ||
         cfg->integrator != SPH_INTEGRATOR_RK4_REUSE ||
-        cfg->xsph_eps != 0.0 || cfg->pair_rule != SPH_PAIRS_ONE_FLUID || cfg->mls_order != 0)
+        cfg->xsph_eps != 0.0 || cfg->pair_rule != SPH_PAIRS_ONE_FLUID)
         return SPH_E_CONFIG;
     if (loss == SPH_LOSS_VELOCITY_MISFIT && !target_vel) return SPH_E_ARG;
     std::vector<Dual> x(n), y(n), u(n), v(n), r(n);
