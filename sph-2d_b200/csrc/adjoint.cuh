@@ -1030,23 +1030,14 @@ __global__ void k_adj_shift(Params P, Sorted<R> D, Adj A) {
     A.sr[c] -= Vc * A.irho[c] * Vb_;
 }
 
-// Reverse of stage 3 (the step end) from the id-order adjoints of the end state
-// and of the carried rates.  Non-integrated host particles keep their state.
-// With shift: the step end also moved the water particles that are not near
-// the surface by the capped shift cap(delta), delta = -beta h^2 B^-1 s (s from
-// k_shift_sum), and corrected rho by grad rho . cap(delta)
-// (Shift_particle_position.f90:97-136): its reverse leaves the adjoints of s
-// (smu), grad rho (shgr) and B^-1 (shbi) of the last RHS; the cap is the branch
-// the forward took.
+// Reverse of the step end's capped shift and density correction for slot s
+// (x' = x + dc, rho' = rho + grad rho.dc, dc the capped shift of the last RHS):
+// the adjoints of the shift sum, grad rho and B^-1 go to smu, shgr, shbi.
 template <typename R>
-__global__ void k_adj_stage3(Params P, Sorted<R> D, Adj A, double dt, int shift) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= P.n_tot) return;
-    const int i = D.id[s];
-    double2 lx = make_double2(0, 0), lv = make_double2(0, 0);
-    double lrho = 0.0;
-    if (i < P.n_host) { lx = A.lx[i]; lv = A.lv[i]; lrho = A.lrho[i]; }
-    if (shift) {
+__device__ __forceinline__ void shift_reverse(const Params& P, const Sorted<R>& D, const Adj& A, int s, int i,
+                                              double2 lx, double lrho) {
+    // (the shift moves the water particles that are not near the surface)
+    {
         double2 mu = make_double2(0, 0), sg = make_double2(0, 0);
         double4 sb = make_double4(0, 0, 0, 0);
         if (i < P.n_host && D.type[s] == SPH_TYPE_WATER && !(D.flags[s] & 2)) {
@@ -1073,6 +1064,30 @@ __global__ void k_adj_stage3(Params P, Sorted<R> D, Adj A, double dt, int shift)
         }
         A.smu[s] = mu; A.shgr[s] = sg; A.shbi[s] = sb;
     }
+}
+
+// Reverse of stage 3 (the step end) from the id-order adjoints of the end state
+// and of the carried rates.  Non-integrated host particles keep their state.
+// With shift: the step end also moved the water particles that are not near
+// the surface by the capped shift cap(delta), delta = -beta h^2 B^-1 s (s from
+// k_shift_sum), and corrected rho by grad rho . cap(delta)
+// (Shift_particle_position.f90:97-136): its reverse leaves the adjoints of s
+// (smu), grad rho (shgr) and B^-1 (shbi) of the last RHS; the cap is the branch
+// the forward took.
+template <typename R>
+__global__ void k_adj_stage3(Params P, Sorted<R> D, Adj A, double dt, int shift, const double2* ox = nullptr,
+                             const double* orho = nullptr) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= P.n_tot) return;
+    const int i = D.id[s];
+    double2 lx = make_double2(0, 0), lv = make_double2(0, 0);
+    double lrho = 0.0;
+    if (i < P.n_host) { lx = A.lx[i]; lv = A.lv[i]; lrho = A.lrho[i]; }
+    // ox / orho: the adjoint of the last stage's positions and densities when the
+    // step ended with the density re-initialisation (its reverse and that of the
+    // shift after it already ran: k_adj_mls_end, k_adj_mls_own, k_adj_mls_nbr)
+    if (ox) { lx = ox[s]; lrho = orho[s]; shift = 0; }
+    if (shift) shift_reverse<R>(P, D, A, s, i, lx, lrho);
     for (int k = 0; k < 4; ++k) { A.lr[k][s] = 0.0; A.la[k][s] = make_double2(0, 0); }
     A.lxe[s] = make_double2(0, 0);
     if (i < P.n_host && integrated(P, D.type[s])) {
@@ -1098,6 +1113,242 @@ __global__ void k_adj_stage3(Params P, Sorted<R> D, Adj A, double dt, int shift)
         A.av0[s] = lv;
         A.ar0[s] = lrho;
     }
+}
+
+
+// ---- reverse of the density re-initialisation (moving least squares) -------
+// The forward (k_mls, Taylor-Green variant) forms, for a water host a and its
+// neighbours b within the support at the state the step's last stage produced,
+//   A = sum W_b p_b p_b^T + alpha^3 I,  r = sum rho_b W_b p_b,  rho_a' = c.r,  A c = e_1,
+// p_b = (1, dx, dy[, dx^2, dx dy, dy^2]), (dx, dy) = (x_b - x_a)/h, W_b = W(|x_a - x_b|),
+// or rho_a' = sum rho_b W_b / S, S = sum W_b, when A is singular or (order 6) a
+// has at most 8 neighbours.  With lam the adjoint of rho_a' and y = A^-1 (lam r):
+//   rho_b-bar += lam W_b (c.p_b),   W_b-bar = (c.p_b)(lam rho_b - y.p_b),
+//   p_b-bar = lam rho_b W_b c - W_b ((c.p_b) y + (y.p_b) c)
+// (Shepard: rho_b-bar += lam W_b / S, W_b-bar = lam (rho_b - rho_a') / S), then
+// through p_b to x_b - x_a and through W_b to |x_a - x_b|.
+
+// The Cholesky factor of k_mls's solve (the same operations in the same order,
+// so c = A^-1 e_1 takes the forward's bits) and a solve with it.
+template <int M>
+__device__ __forceinline__ bool mls_chol(const double (&A)[M * (M + 1) / 2], double (&L)[M * (M + 1) / 2]) {
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+#pragma unroll
+        for (int j = 0; j <= i; ++j) {
+            double sum = A[i * (i + 1) / 2 + j];
+#pragma unroll
+            for (int k = 0; k < j; ++k) sum -= L[i * (i + 1) / 2 + k] * L[j * (j + 1) / 2 + k];
+            if (i == j) {
+                if (!(sum > 0.0)) return false;
+                L[i * (i + 1) / 2 + i] = sqrt(sum);
+            } else {
+                L[i * (i + 1) / 2 + j] = sum / L[j * (j + 1) / 2 + j];
+            }
+        }
+    }
+    return true;
+}
+
+template <int M>
+__device__ __forceinline__ void mls_solve(const double (&L)[M * (M + 1) / 2], const double (&b)[M], double (&x)[M]) {
+    double y[M];
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+        double sum = b[i];
+#pragma unroll
+        for (int k = 0; k < i; ++k) sum -= L[i * (i + 1) / 2 + k] * y[k];
+        y[i] = sum / L[i * (i + 1) / 2 + i];
+    }
+#pragma unroll
+    for (int i = M - 1; i >= 0; --i) {
+        double sum = y[i];
+#pragma unroll
+        for (int k = i + 1; k < M; ++k) sum -= L[k * (k + 1) / 2 + i] * x[k];
+        x[i] = sum / L[i * (i + 1) / 2 + i];
+    }
+}
+
+// p-bar -> (dx, dy)-bar
+template <int M>
+__device__ __forceinline__ void mls_pbar_to_d(const double (&pb)[6], double dx, double dy, double& dxb, double& dyb) {
+    dxb = pb[1];
+    dyb = pb[2];
+    if (M == 6) {
+        dxb += 2.0 * dx * pb[3] + dy * pb[4];
+        dyb += dx * pb[4] + 2.0 * dy * pb[5];
+    }
+}
+
+// The step end's adjoint split for the reverse of a step that ended with the
+// density re-initialisation: the shift after it reversed (as in k_adj_stage3),
+// then the positions' adjoint (xe) and the adjoint of the re-initialised
+// density (lam) per slot.
+template <typename R>
+__global__ void k_adj_mls_end(Params P, Sorted<R> D, Adj A, int shift, double2* xe, double* lam) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= P.n_tot) return;
+    const int i = D.id[s];
+    double2 lx = make_double2(0, 0);
+    double lrho = 0.0;
+    if (i < P.n_host) { lx = A.lx[i]; lrho = A.lrho[i]; }
+    if (shift) shift_reverse<R>(P, D, A, s, i, lx, lrho);
+    xe[s] = lx;
+    lam[s] = lrho;
+}
+
+// Per owner a (a water host): A, r and the solve of k_mls on the state V the
+// last stage produced, y = A^-1 (lam_a r), and the adjoint of x_a through its
+// own sum.  cy[15 a ..]: c (0-5), y (6-11), mode (12: 0 not an owner, 1 the
+// moving-least-squares weights, 2 Shepard), S (13), rho_a' (14).
+template <typename R, int M>
+__global__ void k_adj_mls_own(Params P, Sorted<R> V, const double* lam, double* cy, double2* xown) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= P.n_tot) return;
+    double* o = cy + (size_t)15 * a;
+    o[12] = 0.0;
+    xown[a] = make_double2(0.0, 0.0);
+    if (V.type[a] != SPH_TYPE_WATER || V.id[a] >= P.n_host) return;
+    const double2 xa = V.pos[a];
+    const double inv_h = 1.0 / P.h;
+    double Am[M * (M + 1) / 2], r[M];
+#pragma unroll
+    for (int k = 0; k < M * (M + 1) / 2; ++k) Am[k] = 0.0;
+#pragma unroll
+    for (int k = 0; k < M; ++k) r[k] = 0.0;
+    double sw = 0.0, srw = 0.0;
+    int cnt = 0;
+    const int nn = V.nnbr[a];
+    for (int e = 0; e < nn; ++e) {
+        const int b = (int)(V.nbr[(size_t)e * P.nbr_stride + a] & 0x7fffffffu);
+        const double2 xb = V.pos[b];
+        const double px = xa.x - xb.x, py = xa.y - xb.y;
+        double d;
+        if (!in_support(P, px, py, d)) continue;
+        double w, gx, gy;
+        kernel_w_dw<double>(P, d, px, py, w, gx, gy);
+        const double rho_b = V.kin[b].z;
+        double p[M];
+        const double dx = -px * inv_h, dy = -py * inv_h;
+        p[0] = 1.0; p[1] = dx; p[2] = dy;
+        if (M == 6) { p[3 % M] = dx * dx; p[4 % M] = dx * dy; p[5 % M] = dy * dy; }
+#pragma unroll
+        for (int i = 0; i < M; ++i) {
+            const double wp = w * p[i];
+#pragma unroll
+            for (int j = 0; j <= i; ++j) Am[i * (i + 1) / 2 + j] += wp * p[j];
+            r[i] += rho_b * wp;
+        }
+        sw += w;
+        srw += rho_b * w;
+        ++cnt;
+    }
+#pragma unroll
+    for (int i = 0; i < M; ++i) Am[i * (i + 1) / 2 + i] += P.mls_alpha3;
+    const double lm = lam[a];
+    double L[M * (M + 1) / 2], c[M], y[M];
+    const bool ok = !(M == 6 && cnt <= 8) && mls_chol<M>(Am, L);
+    const double out = srw / sw;
+    if (ok) {
+        double e1[M], lr[M];
+#pragma unroll
+        for (int i = 0; i < M; ++i) { e1[i] = i == 0 ? 1.0 : 0.0; lr[i] = lm * r[i]; }
+        mls_solve<M>(L, e1, c);
+        mls_solve<M>(L, lr, y);
+#pragma unroll
+        for (int i = 0; i < M; ++i) { o[i] = c[i]; o[6 + i] = y[i]; }
+        o[12] = 1.0;
+    } else {
+        o[12] = 2.0;
+        o[13] = sw;
+        o[14] = out;
+    }
+    double xb0 = 0.0, xb1 = 0.0;
+    for (int e = 0; e < nn; ++e) {
+        const int b = (int)(V.nbr[(size_t)e * P.nbr_stride + a] & 0x7fffffffu);
+        const double2 xb = V.pos[b];
+        const double px = xa.x - xb.x, py = xa.y - xb.y;
+        double d;
+        if (!in_support(P, px, py, d)) continue;
+        double w, gx, gy;
+        kernel_w_dw<double>(P, d, px, py, w, gx, gy);
+        const double rho_b = V.kin[b].z;
+        double Wb;
+        if (ok) {
+            const double dx = -px * inv_h, dy = -py * inv_h;
+            double p[6] = {1.0, dx, dy, dx * dx, dx * dy, dy * dy};
+            double cp = 0.0, yp = 0.0;
+#pragma unroll
+            for (int i = 0; i < M; ++i) { cp += c[i] * p[i]; yp += y[i] * p[i]; }
+            Wb = cp * (lm * rho_b - yp);
+            double pb[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+            for (int i = 0; i < M; ++i) pb[i] = lm * rho_b * w * c[i] - w * (yp * c[i] + cp * y[i]);
+            double dxb, dyb;
+            mls_pbar_to_d<M>(pb, dx, dy, dxb, dyb);
+            xb0 -= dxb * inv_h; xb1 -= dyb * inv_h;       // (dx, dy) = (x_b - x_a)/h
+        } else {
+            Wb = lm * (rho_b - out) / sw;
+        }
+        xb0 += Wb * gx; xb1 += Wb * gy;                   // grad_a W = (gx, gy)
+    }
+    xown[a] = make_double2(xb0, xb1);
+}
+
+// Per particle q: its position and density adjoints through the re-initialised
+// densities of the owners a it is a neighbour of (gathered over q's list, which
+// holds every such a), plus the step end's (xe) and the owner's own part (xown);
+// a particle that is not an owner keeps its density, rho' = rho.
+template <typename R, int M>
+__global__ void k_adj_mls_nbr(Params P, Sorted<R> V, const double* lam, const double* cy, const double2* xown,
+                              const double2* xe, double2* ox, double* orho) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= P.n_tot) return;
+    const double2 xq = V.pos[q];
+    const double rho_q = V.kin[q].z;
+    const bool owner = V.type[q] == SPH_TYPE_WATER && V.id[q] < P.n_host;
+    const double inv_h = 1.0 / P.h;
+    const double2 x0 = xe[q], x1 = xown[q];
+    double xb0 = x0.x + x1.x, xb1 = x0.y + x1.y;
+    double rb = owner ? 0.0 : lam[q];
+    const int nn = V.nnbr[q];
+    for (int e = 0; e < nn; ++e) {
+        const int a = (int)(V.nbr[(size_t)e * P.nbr_stride + q] & 0x7fffffffu);
+        const double* o = cy + (size_t)15 * a;
+        const double mode = o[12];
+        if (mode == 0.0) continue;
+        const double2 xa = V.pos[a];
+        const double px = xa.x - xq.x, py = xa.y - xq.y;
+        double d;
+        if (!in_support(P, px, py, d)) continue;
+        double w, gx, gy;
+        kernel_w_dw<double>(P, d, px, py, w, gx, gy);
+        const double lm = lam[a];
+        double Wb;
+        if (mode == 1.0) {
+            const double dx = -px * inv_h, dy = -py * inv_h;
+            double p[6] = {1.0, dx, dy, dx * dx, dx * dy, dy * dy};
+            double c[M], y[M];
+            double cp = 0.0, yp = 0.0;
+#pragma unroll
+            for (int i = 0; i < M; ++i) { c[i] = o[i]; y[i] = o[6 + i]; cp += c[i] * p[i]; yp += y[i] * p[i]; }
+            rb += lm * w * cp;
+            Wb = cp * (lm * rho_q - yp);
+            double pb[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+            for (int i = 0; i < M; ++i) pb[i] = lm * rho_q * w * c[i] - w * (yp * c[i] + cp * y[i]);
+            double dxb, dyb;
+            mls_pbar_to_d<M>(pb, dx, dy, dxb, dyb);
+            xb0 += dxb * inv_h; xb1 += dyb * inv_h;
+        } else {
+            const double S = o[13], out = o[14];
+            rb += lm * w / S;
+            Wb = lm * (rho_q - out) / S;
+        }
+        xb0 -= Wb * gx; xb1 -= Wb * gy;                   // grad_q W = -grad_a W
+    }
+    ox[q] = make_double2(xb0, xb1);
+    orho[q] = rb;
 }
 
 // Sorted step-start adjoints -> id order; the K1 adjoint goes to the previous step.

@@ -707,10 +707,19 @@ struct AdjCtx {
     int cap_ck = 0, cap_seg = 0, cap_host = 0, cap_tot = 0;
     Snap ck;                   // checkpoints [nseg + 1] (the last: the final state)
     Snap seg;                  // step-start states of the segment being reversed
-    // stage states S1..S3 in sorted order, [stage_slots][3][cap_tot]: one slot per
+    // stage states S1..S3 in sorted order (and, with density re-initialisation,
+    // the state the step's last stage produced before it), [stage_slots][nst][cap_tot]: one slot per
     // step of the segment when memory allows (kept while the segment is re-run),
     // else one slot that each reversed step recomputes
     int stage_slots = 0;
+    int nst = 3;                // states per stage slot
+    // reverse of the density re-initialisation (moving least squares, orders 3 and 6)
+    double2* mls_x = nullptr;   // adjoint of the positions it read, per slot
+    double* mls_r = nullptr;    //   and of the densities
+    double* mls_lam = nullptr;  // adjoint of the densities it produced
+    double* mls_cy = nullptr;   // per owner: c = A^-1 e_1, y = A^-1 (lam r), (mode, sum W, out) [15]
+    double2* mls_xe = nullptr;  // the step end's position adjoint (after the shift's reverse)
+    double2* mls_xo = nullptr;  // an owner's position adjoint through its own sum
     double2* st_pos = nullptr;
     double4* st_kin = nullptr;
     double4* st_aux = nullptr;  // V4 of the pair precision (float4 uses the first half)
@@ -797,7 +806,9 @@ int snap_io(sph_handle* h, const Snap& s, int k, int n, bool save) {
 
 int adj_config_ok(const sph_handle* h, int loss) {
     const Params& P = h->P;
-    if (P.mls_order) return SPH_E_CONFIG;
+    // density re-initialisation: moving least squares (orders 3, 6) with the
+    // Taylor-Green driver
+    if (P.mls_order && (P.ms || P.mls_order == 1)) return SPH_E_CONFIG;
     if (P.ms) {
         // moving-square modified linear solver, Morris laplacian, Euler predictor-corrector
         if (h->cfg.shifting) return SPH_E_CONFIG;
@@ -953,11 +964,12 @@ int adj_prepare_ctx(sph_handle* h, const sph_adj_config* ac) {
             (rc = adj_alloc(X, &A.lrho, nt)) || (rc = adj_alloc(X, &A.lk_r, nh)) || (rc = adj_alloc(X, &A.lk_a, nh)))
             return rc;
         // stage states: every step of a segment if that leaves 1 GiB free, else one
-        const size_t per_slot = 3 * nt * (sizeof(double2) + 2 * sizeof(double4));
+        X->nst = h->P.mls_order ? 4 : 3;
+        const size_t per_slot = (size_t)X->nst * nt * (sizeof(double2) + 2 * sizeof(double4));
         size_t free_b = 0, total_b = 0;
         CK(cudaMemGetInfo(&free_b, &total_b));
         X->stage_slots = (per_slot * every + (size_t(1) << 30) <= free_b) ? every : 1;
-        const size_t ns = (size_t)X->stage_slots * 3 * nt;
+        const size_t ns = (size_t)X->stage_slots * X->nst * nt;
         if ((rc = adj_alloc(X, &X->st_pos, ns)) || (rc = adj_alloc(X, &X->st_kin, ns)) ||
             (rc = adj_alloc(X, &X->st_aux, ns)))
             return rc;
@@ -994,6 +1006,14 @@ int adj_prepare_ctx(sph_handle* h, const sph_adj_config* ac) {
             }
         }
     }
+    if (h->P.mls_order && !X->mls_x) {
+        const size_t nt = (size_t)X->cap_tot;
+        int rc;
+        if ((rc = adj_alloc(X, &X->mls_x, nt)) || (rc = adj_alloc(X, &X->mls_r, nt)) ||
+            (rc = adj_alloc(X, &X->mls_lam, nt)) || (rc = adj_alloc(X, &X->mls_cy, nt * 15)) ||
+            (rc = adj_alloc(X, &X->mls_xe, nt)) || (rc = adj_alloc(X, &X->mls_xo, nt)))
+            return rc;
+    }
     if (h->P.ms && !X->A.gavg) {
         Adj& A = X->A;
         const size_t nh = (size_t)X->cap_host, nt = (size_t)X->cap_tot;
@@ -1029,6 +1049,9 @@ int adjoint_forward(sph_handle* h, const sph_adj_config* ac, double* loss) {
     int rc = adj_prepare_ctx(h, ac);
     if (rc || (rc = prep_upload<R>(h))) return rc;
     AdjCtx* X = h->adj;
+    // with density re-initialisation every step of a segment keeps its states
+    // (the reverse of a re-initialised step reads the state before it)
+    if (h->P.mls_order && X->stage_slots < X->every) return SPH_E_CAPACITY;
     const int n = h->n_host;
     if (ac->loss == SPH_LOSS_VELOCITY_MISFIT) {
         CK(cudaMemcpyAsync(h->d_xfer, ac->target_vel, sizeof(double) * 2 * n, cudaMemcpyHostToDevice, h->stream));
@@ -1077,7 +1100,7 @@ template <typename R>
 Sorted<R> stage_view(sph_handle* h, int j, int k) {
     AdjCtx* X = h->adj;
     Sorted<R> V = sorted<R>(h);
-    const size_t o = ((size_t)j * 3 + k) * (size_t)X->cap_tot;
+    const size_t o = ((size_t)j * X->nst + k) * (size_t)X->cap_tot;
     V.pos = X->st_pos + o;
     V.kin = X->st_kin + o;
     V.aux = reinterpret_cast<typename VT<R>::V4*>(X->st_aux + o);
@@ -1134,10 +1157,15 @@ int keep_stage(sph_handle* h, int j, int k) {
 template <typename R>
 int step_keep(sph_handle* h, double dt, int j, bool full) {
     const int first = h->step_count == 0;
+    // density re-initialisation after this step (1-based step number): the step
+    // runs in full, and its reverse reads the state the last stage produced
+    // (stage slot state 3) and the neighbour lists
+    const bool mls = h->P.mls_order != 0 && (h->step_count + 1) % h->P.mls_every == 0;
+    if (mls) full = true;
     // the RHS evaluations of a step that runs here in full (the moving square's
     // corrector; the Runge-Kutta RHS 2-4) fill its pass-A slots, and its reverse
     // step re-runs no pass A, so it needs no neighbour lists
-    const bool keep_pa = h->adj->pa && full && !first;
+    const bool keep_pa = h->adj->pa && full && !first && !mls;
     int rc = step_begin<R>(h, dt);
     if (rc || (rc = prepare<R>(h)) || (rc = prep_save(h, j, !keep_pa))) return rc;
     h->adj->seg_ntot[j] = h->P.n_tot;
@@ -1187,8 +1215,9 @@ int step_keep(sph_handle* h, double dt, int j, bool full) {
     if (full) {
         {
             PaSwap<R> sw(h, 3 * j + 2, keep_pa);
-            if ((rc = rhs<R>(h, 1)) || (rc = stage<R>(h, 3, dt, 0, h->cfg.shifting))) return rc;
+            if ((rc = rhs<R>(h, 1)) || (rc = stage<R>(h, 3, dt, 0, mls ? 0 : h->cfg.shifting))) return rc;
         }
+        if (mls && ((rc = keep_stage<R>(h, j, 3)) || (rc = reinit_density<R>(h, h->cfg.shifting)))) return rc;
         h->step_count++;
         h->n_steps++;
     }
@@ -1287,10 +1316,32 @@ int adj_step(sph_handle* h, bool first, int j) {
         h->launches += 1;
     }
     tic(h, PH_ADJ);
-    // the step end's shift reads the last RHS's flags, B^-1 and grad rho (kept:
-    // from pass-A slot 3 j + 2; else the re-run above left them in the arrays)
-    k_adj_stage3<R><<<nb, 256, 0, h->stream>>>(P, kept ? pa_view<R>(h, D, 3 * j + 2) : D, A, dt, shift ? 1 : 0);
-    h->launches += 1;
+    // a step that ended with the density re-initialisation (never a kept one)
+    const bool mls = P.mls_order != 0 && (h->step_count + 1) % P.mls_every == 0;
+    if (mls) {
+        // the shift's reverse, then that of the re-initialisation on the state the
+        // last stage produced (stage slot state 3) over the step's lists
+        const Sorted<R> V3 = stage_view<R>(h, j, 3);
+        const int nbo = blocks(P.n_tot, 128);
+        k_adj_mls_end<R><<<nb, 256, 0, h->stream>>>(P, D, A, shift ? 1 : 0, X->mls_xe, X->mls_lam);
+        if (P.mls_order == 6) {
+            k_adj_mls_own<R, 6><<<nbo, 128, 0, h->stream>>>(P, V3, X->mls_lam, X->mls_cy, X->mls_xo);
+            k_adj_mls_nbr<R, 6><<<nbo, 128, 0, h->stream>>>(P, V3, X->mls_lam, X->mls_cy, X->mls_xo, X->mls_xe,
+                                                             X->mls_x, X->mls_r);
+        } else {
+            k_adj_mls_own<R, 3><<<nbo, 128, 0, h->stream>>>(P, V3, X->mls_lam, X->mls_cy, X->mls_xo);
+            k_adj_mls_nbr<R, 3><<<nbo, 128, 0, h->stream>>>(P, V3, X->mls_lam, X->mls_cy, X->mls_xo, X->mls_xe,
+                                                             X->mls_x, X->mls_r);
+        }
+        k_adj_stage3<R><<<nb, 256, 0, h->stream>>>(P, D, A, dt, 0, X->mls_x, X->mls_r);
+        h->launches += 4;
+    } else {
+        // the step end's shift reads the last RHS's flags, B^-1 and grad rho (kept:
+        // from pass-A slot 3 j + 2; else the re-run above left them in the arrays)
+        k_adj_stage3<R><<<nb, 256, 0, h->stream>>>(P, kept ? pa_view<R>(h, D, 3 * j + 2) : D, A, dt,
+                                                     shift ? 1 : 0);
+        h->launches += 1;
+    }
     for (int k = 2; k >= 0; --k)
         if ((rc = adj_rhs<R>(h, view(k), k + 1, k, shift && k == 2, kept))) return rc;
     if (first) {

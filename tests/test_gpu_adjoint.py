@@ -52,6 +52,12 @@ def _case(kind):
         case = S.make_tgv(32, reference=True, jitter=0.05, seed=12)
     case.cfg.shifting = 1 if kind.endswith("-shift") else 0
     case.cfg.mls_order = 0
+    if "-mls" in kind:
+        # density re-initialisation (moving least squares, order 3 or 6) after
+        # every fourth step: steps 4, 8 and 12 of the run
+        case.cfg.mls_order = int(kind.split("-mls")[1][0])
+        case.cfg.mls_every = 4
+        case.cfg.mls_alpha = 1e-4
     return case
 
 
@@ -105,7 +111,8 @@ def _check(ad, fd, what):
 
 
 @pytest.mark.parametrize("kind", ["wendland-renorm", "reference-gaussian", "wendland-renorm-shift",
-                                  "reference-gaussian-shift", "muscl", "muscl-shift", "plain", "plain-shift"])
+                                  "reference-gaussian-shift", "muscl", "muscl-shift", "plain", "plain-shift",
+                                  "reference-gaussian-mls6", "wendland-renorm-mls3-shift", "muscl-mls6"])
 @pytest.mark.parametrize("pre_steps", [0, 3])
 def test_adjoint_matches_central_differences(lib, kind, pre_steps):
     case = _case(kind)
@@ -170,7 +177,7 @@ def test_adjoint_independent_of_checkpoint_interval(lib):
 
 def test_adjoint_rejects_unsupported_configurations(lib):
     case = S.make_tgv(16, solver=S.SOLVER_MUSCL_DELTA_SPS)
-    case.cfg.mls_order = 6                    # density re-initialisation: not differentiated
+    case.cfg.mls_order = 1                    # order-1 re-initialisation: not differentiated
     with S.Simulation(case.cfg, case.n) as sim:
         sim.set_state(case.pos, case.vel, case.rho, case.mass, case.type)
         with pytest.raises(S.SphError) as e:
@@ -206,7 +213,8 @@ def test_adjoint_of_the_mixed_precision_step(lib):
 
 
 @pytest.mark.parametrize("kind", ["wendland-renorm", "reference-gaussian", "wendland-renorm-shift",
-                                  "reference-gaussian-shift", "muscl", "muscl-shift", "plain", "plain-shift"])
+                                  "reference-gaussian-shift", "muscl", "muscl-shift", "plain", "plain-shift",
+                                  "reference-gaussian-mls6", "wendland-renorm-mls3-shift", "muscl-mls6"])
 def test_adjoint_matches_cpu_tangent_linear_reference(lib, oracle, kind):
     """g.delta from the GPU adjoint against the FP64 CPU tangent-linear model of
     the same steps (oracle/sph_tangent.cpp, forward-mode derivative with the
