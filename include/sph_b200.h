@@ -332,13 +332,17 @@ int sph_find_particle_pair_noalloc(const sph_config* cfg, int n, const double* d
  * keeps less and recomputes instead; the gradient is the same either way.
  *
  * Supported configurations (others return SPH_E_CONFIG), either kernel, with
- * or without renormalisation, without MLS density re-initialisation:
+ * or without renormalisation:
  *  - the normalised modified linear Riemann and MUSCL linear Riemann delta-SPH
  *    + SPS solvers and the plain delta-SPH method (SPH_SOLVER_MODLR_DELTA_SPS
  *    without XSPH, SPH_SOLVER_MUSCL_DELTA_SPS, SPH_SOLVER_DELTA_SPS) with the
  *    RK4 driver, with or without particle
  *    shifting (the limiter, the capped shift and its density correction are
- *    differentiated on the branch the forward took);
+ *    differentiated on the branch the forward took), with or without the
+ *    moving-least-squares density re-initialisation (mls_order 3 or 6; its
+ *    Shepard fallback differentiated where the forward took it); with the
+ *    re-initialisation every step of a checkpoint segment must keep its states,
+ *    else sph_adjoint_forward returns SPH_E_CAPACITY (lower checkpoint_every);
  *  - the moving-square modified linear Riemann and HLLC solvers
  *    (SPH_SOLVER_MS_MODLR_DELTA, SPH_SOLVER_MS_HLLC_DELTA; Morris laplacian,
  *    XSPH velocities in the continuity flux; the HLLC state on the sampled
@@ -346,7 +350,7 @@ int sph_find_particle_pair_noalloc(const sph_config* cfg, int n, const double* d
  *    predictor-corrector driver, with the library's ghost assignment
  *    (ghost_assign = 1: the reverse runs through the Shepard interpolation onto
  *    the wall and body ghosts) or with caller-given ghost states; without
- *    particle shifting.
+ *    particle shifting or density re-initialisation.
  * The reverse kernels compute in FP64 for both precisions of the forward step.
  *
  * Body motion: with body_motion set, step k of the forward run (k = 0 ..
