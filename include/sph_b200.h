@@ -190,10 +190,12 @@ int sph_update_state(sph_handle* h, int n, const double* pos, const double* vel,
 int sph_set_initial_type(sph_handle* h, int n, const int* initial_type);
 
 /* subdomain_Boundary_particle_type for the n host particles: -6 horizontal
- * wall, -7 corner ("center"), -8 vertical wall, 0 anything else
- * (Moving_Square.../Initial_Particle_From_First_Step.f90:220-300).  Used by the
- * ghost assignment; the radius free-slip label -9 (cylinder walls) is not
- * supported (SPH_E_CONFIG). */
+ * wall, -7 corner ("center"), -8 vertical wall, -9 along the cylinder, 0
+ * anything else (Moving_Square.../Initial_Particle_From_First_Step.f90:220-300).
+ * Used by the ghost assignment.  A -9 ghost keeps its interpolated velocity, as
+ * in the reference: its radius_free_slip call (Assign_boundary_particles.f90:905,
+ * Function_Module.f90:929-960) reads and writes the global particle arrays,
+ * at the subdomain index and at fix_ghost_name, not the ghost's own velocity. */
 int sph_set_boundary_labels(sph_handle* h, int n, const int* labels);
 
 /* Custom_velocity and Custom_accleration of Body_Motion_Solver

@@ -1778,8 +1778,6 @@ int sph_set_initial_type(sph_handle* h, int n, const int* initial_type) {
 
 int sph_set_boundary_labels(sph_handle* h, int n, const int* labels) {
     if (!h || n != h->n_host || n <= 0 || !labels) return SPH_E_ARG;
-    for (int i = 0; i < n; ++i)
-        if (labels[i] == -9) return SPH_E_CONFIG;     // radius free slip: not built
     CK(cudaSetDevice(h->device));
     int rc = h->mixed ? unsort<float>(h) : unsort<double>(h);
     if (rc) return rc;
