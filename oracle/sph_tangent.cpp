@@ -24,9 +24,10 @@
 // the modified linear Riemann and the HLLC solvers with XSPH in the continuity flux, the
 // fixed-ghost assignment, the body force and the Euler predictor-corrector with
 // a per-step body motion (oracle_tangent_ms).  Either kernel, with or without
-// renormalisation, with or without shifting in (1) and without in (2), density
-// re-initialisation (orders 1, 3, 6) in (1) only, no free-surface particles.  Other inputs return SPH_E_CONFIG.  The pair search is a plain
-// double loop (small cases only).
+// renormalisation, with or without shifting (the capped shift on the last
+// RHS's pairs, exponent 4 in (2)), density re-initialisation (orders 1, 3, 6)
+// in (1) only, no free-surface particles.  Other inputs return SPH_E_CONFIG.
+// The pair search is a plain double loop (small cases only).
 
 #include <cmath>
 #include <cstring>
@@ -761,7 +762,8 @@ struct MSModel {
 
     // single_step_compute of the moving square: the rates of every particle and,
     // when fx is given, the x body force of this RHS.
-    int rhs(MSParts<T>& P, std::vector<T>& drho, std::vector<T>* acc, std::vector<T>* avg, T* fx) const {
+    int rhs(MSParts<T>& P, std::vector<T>& drho, std::vector<T>* acc, std::vector<T>* avg, T* fx,
+            std::vector<T>* sh = nullptr, std::vector<T>* gr = nullptr) const {
         const sph_config& C = M.C;
         const TConsts& K = M.K;
         const T& nu = M.nu;
@@ -910,6 +912,22 @@ struct MSModel {
             acc[0][i] = a0[i]; acc[1][i] = a1[i];
             drho[i] = drho[i] + corr[i];
         }
+        if (sh) {
+            // the particle shift on this RHS's pairs (Shift_particle_position.f90:56-100),
+            // sh[0..1][i] = -beta h^2 sum_j (1 + R (w/w_dx)^4) V_j B_i^-1 grad_i W, and
+            // the normalised density gradient gr[0..1]
+            sh[0].assign(n, T(0.0)); sh[1].assign(n, T(0.0));
+            const double h2 = C.h * C.h;
+            for (size_t k = 0; k < np; ++k) {
+                const int i = pi[k], j = pj[k];
+                const T r = w[k] / K.w_dx;
+                const T r2 = r * r;
+                const T f = C.shift_beta * h2 * (1.0 + C.shift_R * (r2 * r2));
+                sh[0][i] += -(f * ni0[k] * vol[j]); sh[1][i] += -(f * ni1[k] * vol[j]);
+                sh[0][j] += f * nj0[k] * vol[i]; sh[1][j] += f * nj1[k] * vol[i];
+            }
+            gr[0] = g0; gr[1] = g1;
+        }
         if (fx) {
             // Calculate_Body_Force, x component of the total (Morris laplacian)
             std::vector<T> bp(n, T(0.0)), bv(n, T(0.0));
@@ -982,7 +1000,8 @@ int run_ms(const sph_config& cfg, MSParts<T>& H, const T& nu, const std::vector<
             P.v[i] = B0.v[i] + dt * a[1][i];
         }
         T fx;
-        if ((rc = S.rhs(P, dr, a, g, &fx))) return rc;
+        std::vector<T> sh[2], gr[2];
+        if ((rc = S.rhs(P, dr, a, g, &fx, cfg.shifting ? sh : nullptr, gr))) return rc;
         drag = drag + dt * fx;
         for (int i = 0; i < n; ++i) {
             if (P.type[i] != SPH_TYPE_WATER) continue;
@@ -991,6 +1010,19 @@ int run_ms(const sph_config& cfg, MSParts<T>& H, const T& nu, const std::vector<
             P.y[i] = B0.y[i] + 0.5 * dt * (P.v[i] + tv1[i]) + g[1][i] * dt + 0.5 * a[1][i] * (dt * dt);
             P.u[i] = B0.u[i] + 0.5 * dt * (a[0][i] + ta0[i]);
             P.v[i] = B0.v[i] + 0.5 * dt * (a[1][i] + ta1[i]);
+        }
+        if (cfg.shifting) {
+            // the capped shift of the water particles (none is near a free surface
+            // here) and the first-order density correction
+            for (int i = 0; i < n; ++i) {
+                if (P.type[i] != SPH_TYPE_WATER) continue;
+                T s0 = sh[0][i], s1 = sh[1][i];
+                const T amp = sqrt(s0 * s0 + s1 * s1);
+                if (val(amp) > cfg.shift_max) { s0 = s0 / amp * cfg.shift_max; s1 = s1 / amp * cfg.shift_max; }
+                P.x[i] = P.x[i] + s0; P.y[i] = P.y[i] + s1;
+                P.rho[i] = P.rho[i] + gr[0][i] * s0;
+                P.rho[i] = P.rho[i] + gr[1][i] * s1;
+            }
         }
         rdrho = dr; racc[0] = a[0]; racc[1] = a[1]; ravg[0] = g[0]; ravg[1] = g[1];
         for (int i = 0; i < n; ++i) {
@@ -1065,7 +1097,7 @@ int oracle_tangent_ms(const sph_config* cfg, int n, const double* pos, const dou
     if (!cfg || !pos || !vel || !rho || !mass || !type || !itype || !motion || !out || n <= 0 || nsteps <= 0)
         return SPH_E_ARG;
     if ((cfg->solver != SPH_SOLVER_MS_MODLR_DELTA && cfg->solver != SPH_SOLVER_MS_HLLC_DELTA) ||
-        cfg->integrator != SPH_INTEGRATOR_EULER_PC || cfg->shifting ||
+        cfg->integrator != SPH_INTEGRATOR_EULER_PC || (cfg->shifting && cfg->shift_n != 4) ||
         cfg->mls_order != 0 || cfg->laplacian != 1 || cfg->free_surface || cfg->periodic)
         return SPH_E_CONFIG;
     for (int i = 0; i < n; ++i)
