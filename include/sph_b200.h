@@ -351,8 +351,10 @@ int sph_find_particle_pair_noalloc(const sph_config* cfg, int n, const double* d
  *    region and wave speeds the forward took) with the Euler
  *    predictor-corrector driver, with the library's ghost assignment
  *    (ghost_assign = 1: the reverse runs through the Shepard interpolation onto
- *    the wall and body ghosts) or with caller-given ghost states; without
- *    particle shifting or density re-initialisation.
+ *    the wall and body ghosts) or with caller-given ghost states, with or
+ *    without particle shifting after the corrector (the capped shift of the
+ *    corrector RHS over its pairs, ghosts included); without density
+ *    re-initialisation.
  * The reverse kernels compute in FP64 for both precisions of the forward step.
  *
  * Body motion: with body_motion set, step k of the forward run (k = 0 ..

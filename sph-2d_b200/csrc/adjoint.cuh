@@ -1028,6 +1028,8 @@ __global__ void k_adj_shift(Params P, Sorted<R> D, Adj A) {
     const double2 sx = A.sx[c];
     A.sx[c] = make_double2(sx.x + x0b, sx.y + x1b);
     A.sr[c] -= Vc * A.irho[c] * Vb_;
+    // the moving square's assigned ghosts also carry a mass adjoint (V = m / rho)
+    if (P.ms) A.sm[c] += Vb_ * A.irho[c];
 }
 
 // Reverse of the step end's capped shift and density correction for slot s
@@ -1818,14 +1820,19 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_ghost_water(Params P, Sorte
 //   x'   = x0 + (up + v0) dt/2 + g2 dt + a2 dt^2/2,   carried (d2, a2, g2),
 // up the predicted velocity.  Rates of RHS 0 (the predictor's, K1) and RHS 1
 // (the corrector's); lxe keeps the adjoint of up for the predictor reverse.
+// With shift: the step end then moved the water particles by the capped shift
+// of the corrector RHS and corrected their density (as at the end of the
+// Runge-Kutta step, k_adj_stage3); its reverse leaves smu, shgr, shbi, and D
+// carries that RHS's pass-A outputs.
 template <typename R>
-__global__ void k_adj_stage_end_ms(Params P, Sorted<R> D, Adj A, double dt) {
+__global__ void k_adj_stage_end_ms(Params P, Sorted<R> D, Adj A, double dt, int shift) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= P.n_tot) return;
     const int i = D.id[s];
     double2 lx = make_double2(0, 0), lv = make_double2(0, 0);
     double lrho = 0.0;
     if (i < P.n_host) { lx = A.lx[i]; lv = A.lv[i]; lrho = A.lrho[i]; }
+    if (shift) shift_reverse<R>(P, D, A, s, i, lx, lrho);
     for (int k = 0; k < 2; ++k) {
         A.lr[k][s] = 0.0; A.la[k][s] = make_double2(0, 0); A.lg[k][s] = make_double2(0, 0);
     }

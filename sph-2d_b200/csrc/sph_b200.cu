@@ -810,8 +810,8 @@ int adj_config_ok(const sph_handle* h, int loss) {
     // Taylor-Green driver
     if (P.mls_order && (P.ms || P.mls_order == 1)) return SPH_E_CONFIG;
     if (P.ms) {
-        // moving-square modified linear solver, Morris laplacian, Euler predictor-corrector
-        if (h->cfg.shifting) return SPH_E_CONFIG;
+        // moving-square modified linear or HLLC solver, Morris laplacian, Euler
+        // predictor-corrector, with or without shifting
         if ((h->cfg.solver != SPH_SOLVER_MS_MODLR_DELTA && h->cfg.solver != SPH_SOLVER_MS_HLLC_DELTA) ||
             P.laplacian != 1)
             return SPH_E_CONFIG;
@@ -1180,7 +1180,8 @@ int step_keep(sph_handle* h, double dt, int j, bool full) {
             const size_t o = (size_t)j * X->cap_tot;
             {
                 PaSwap<R> sw(h, j);
-                if ((rc = rhs<R>(h, 1, j, X->pa_gint + o, X->pa_gsw + o)) || (rc = stage<R>(h, 11, dt, 0, 0)))
+                if ((rc = rhs<R>(h, 1, j, X->pa_gint + o, X->pa_gsw + o)) ||
+                    (rc = stage<R>(h, 11, dt, 0, h->cfg.shifting)))
                     return rc;
             }
             X->seg_kept[j] = 1;
@@ -1189,7 +1190,7 @@ int step_keep(sph_handle* h, double dt, int j, bool full) {
         } else {
             if ((rc = keep_stage<R>(h, j, 0))) return rc;
             if (full) {
-                if ((rc = rhs<R>(h, 1)) || (rc = stage<R>(h, 11, dt, 0, 0))) return rc;
+                if ((rc = rhs<R>(h, 1)) || (rc = stage<R>(h, 11, dt, 0, h->cfg.shifting))) return rc;
                 h->step_count++;
                 h->n_steps++;
             }
@@ -1368,15 +1369,45 @@ int adj_step(sph_handle* h, bool first, int j) {
     return SPH_OK;
 }
 
+// The forward values a moving-square RHS's reverse reads, on the state V: the
+// ghost assignment and pass A re-run (the same values as in the forward run),
+// or, for a kept corrector RHS (kept_j >= 0), the ghosts' mass and step-start
+// arrays refilled from what the segment re-run left.
+template <typename R>
+void adj_rhs_ms_values(sph_handle* h, const Sorted<R>& V, int kept_j) {
+    const Params& P = h->P;
+    AdjCtx* X = h->adj;
+    const bool ghosts = P.ghost_assign && h->n_ghost > 0;
+    if (kept_j >= 0) {
+        if (ghosts) {
+            k_ghost_refill<R><<<blocks(h->n_ghost, 256), 256, 0, h->stream>>>(V, h->d_ghost_ids, h->n_ghost);
+            h->launches += 1;
+        }
+        return;
+    }
+    tic(h, PH_A);
+    if (ghosts) {
+        k_assign_ghosts<R><<<blocks((long long)h->n_ghost * 32, 128), 128, 0, h->stream>>>(
+            P, V, h->d_ghost_ids, h->n_ghost, h->t_phys, h->body_vel[0], h->body_vel[1], h->body_acc[0],
+            h->body_acc[1], X->A.gint, X->A.gsw);
+        h->launches += 1;
+    }
+    launch_pass_a<R, false>(P, V, blocks(P.n_tot, kAdjThreads), h->stream);
+    launch_surface<R>(P, V, h->stream);
+}
+
 // Reverse of one moving-square RHS evaluation on the state V with the rate
 // adjoints of RHS k of the step (0: the predictor's K1, 1: the corrector's):
-// the ghost assignment and pass A are re-run on V (the same values as in the
-// forward run), then the reverse of pass C (and of the step's drag term), of the
+// the forward values first (adj_rhs_ms_values, unless shift: adj_step_ms formed
+// them before the step end's reverse), then the reverse of pass C (and of the
+// step's drag term), of the shifting sums (shift: the corrector RHS of a step
+// with particle shifting, whose step-end reverse left smu / shgr / shbi), of the
 // per-particle end of pass A, of its pair sums and XSPH velocity, of the ghost
 // assignment, and of the predictor (pred = 1) or the step-start accumulation.
 // The body-motion adjoints of the RHS go to g_motion[4 jstep ..].
 template <typename R>
-int adj_rhs_ms(sph_handle* h, const Sorted<R>& V, int k, int pred, bool drag, int jstep, int kept_j = -1) {
+int adj_rhs_ms(sph_handle* h, const Sorted<R>& V, int k, int pred, bool drag, int jstep, int kept_j = -1,
+               bool shift = false) {
     const Params& P = h->P;
     AdjCtx* X = h->adj;
     Adj A = X->A;
@@ -1389,22 +1420,8 @@ int adj_rhs_ms(sph_handle* h, const Sorted<R>& V, int k, int pred, bool drag, in
         const size_t o = (size_t)kept_j * X->cap_tot;
         A.gint = X->pa_gint + o;
         A.gsw = X->pa_gsw + o;
-        if (ghosts) {
-            // the ghosts' mass and step-start arrays as that assignment set them
-            k_ghost_refill<R><<<blocks(h->n_ghost, 256), 256, 0, h->stream>>>(V, h->d_ghost_ids, h->n_ghost);
-            h->launches += 1;
-        }
-    } else {
-        tic(h, PH_A);
-        if (ghosts) {
-            k_assign_ghosts<R><<<blocks((long long)h->n_ghost * 32, 128), 128, 0, h->stream>>>(
-                P, V, h->d_ghost_ids, h->n_ghost, h->t_phys, h->body_vel[0], h->body_vel[1], h->body_acc[0],
-                h->body_acc[1], A.gint, A.gsw);
-            h->launches += 1;
-        }
-        launch_pass_a<R, false>(P, V, nb, h->stream);
-        launch_surface<R>(P, V, h->stream);
     }
+    if (!shift) adj_rhs_ms_values<R>(h, V, kept_j);
     tic(h, PH_ADJ);
     CK(cudaMemsetAsync(V.nflag, 0, (size_t)P.n_tot, h->stream));
     if (P.hllc)
@@ -1412,6 +1429,10 @@ int adj_rhs_ms(sph_handle* h, const Sorted<R>& V, int k, int pred, bool drag, in
                                                                           A.nu_part + (size_t)k * nbc);
     else
         k_adj_c<R, true><<<nbc, kAdjThreads, 0, h->stream>>>(P, V, A, A.lr[k], A.la[k], A.nu_part + (size_t)k * nbc);
+    if (shift) {
+        k_adj_shift<R><<<nb, kAdjThreads, 0, h->stream>>>(P, V, A);
+        h->launches += 1;
+    }
     if (drag) {
         double* part = A.nu_part + (size_t)4 * nbc;
         k_mark_body_nbrs<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, V);
@@ -1419,7 +1440,7 @@ int adj_rhs_ms(sph_handle* h, const Sorted<R>& V, int k, int pred, bool drag, in
         k_adj_nu_sum<<<1, 1024, 0, h->stream>>>(nb, part, A.nu_acc);
         h->launches += 3;
     }
-    k_adj_point<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, V, A, 0);
+    k_adj_point<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, V, A, shift ? 1 : 0);
     k_adj_a<R, true><<<nbc, kAdjThreads, 0, h->stream>>>(P, V, A, 0, X->dt, A.lg[k]);
     if (ghosts) {
         const int ngb = blocks((long long)h->n_ghost * 32, kAdjThreads);
@@ -1457,12 +1478,22 @@ int adj_step_ms(sph_handle* h, bool first, int j, int jstep) {
     const Params& P = h->P;
     Sorted<R>& D = sorted<R>(h);
     const int nb = blocks(P.n_tot, 256);
-    tic(h, PH_ADJ);
-    k_adj_stage_end_ms<R><<<nb, 256, 0, h->stream>>>(P, D, A, dt);
-    h->launches += 1;
     const bool kept = X->pa && X->seg_kept[j];
     const Sorted<R> V = kept ? pa_view<R>(h, stage_view<R>(h, j, 0), j) : stage_view<R>(h, j, 0);
-    if ((rc = adj_rhs_ms<R>(h, V, 1, 1, X->loss == SPH_LOSS_DRAG, jstep, kept ? j : -1))) return rc;
+    const bool shift = h->cfg.shifting != 0;
+    if (shift) {
+        // the step end's shift reads the corrector RHS's pass A (B^-1, grad rho,
+        // flags) and its shifting sum over the assigned ghosts: re-form them first
+        adj_rhs_ms_values<R>(h, V, kept ? j : -1);
+        tic(h, PH_ADJ);
+        k_shift_sum<R><<<nb, 256, 0, h->stream>>>(P, V, A);
+        h->launches += 1;
+    }
+    tic(h, PH_ADJ);
+    k_adj_stage_end_ms<R><<<nb, 256, 0, h->stream>>>(P, shift && kept ? pa_view<R>(h, D, j) : D, A, dt,
+                                                      shift ? 1 : 0);
+    h->launches += 1;
+    if ((rc = adj_rhs_ms<R>(h, V, 1, 1, X->loss == SPH_LOSS_DRAG, jstep, kept ? j : -1, shift))) return rc;
     if (first) {
         // the fresh K1 of the first step was evaluated on the step-start state
         k_adj_load<R><<<nb, 256, 0, h->stream>>>(P, D, nullptr, nullptr);

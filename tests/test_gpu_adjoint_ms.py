@@ -171,6 +171,50 @@ def test_moving_square_adjoint_independent_of_checkpoint_interval(lib):
         assert np.array_equal(got[2], ref[2])
 
 
+@pytest.mark.parametrize("solver", SOLVERS)
+def test_shifting_adjoint_matches_central_differences(lib, solver):
+    """Particle shifting after every corrector (Shift_particle_position.f90:
+    56-136 on the corrector RHS's pairs, ghosts included): drag gradient in two
+    motion coefficients and one velocity direction, and the same gradient at
+    every checkpoint interval (1: every corrector RHS kept from the segment
+    re-run; 16: all re-formed in the reverse step)."""
+    case, ity, lab, dt = _case(solver=solver)
+    case.cfg.shifting = 1
+    period = NSTEPS * dt
+    coeffs = np.array([0.5, 0.4, -0.2])
+    motion, jac = S.body_motion_schedule(coeffs, NSTEPS, dt, period=period)
+    L, g, gm, end, after = _grad(case, ity, lab, dt, motion, S.LOSS_DRAG)
+    assert all(np.array_equal(a, b) for a, b in zip(end, after))
+    with _sim(case, ity, lab) as sim:
+        L0 = sim.adjoint_forward(NSTEPS, dt, checkpoint_every=NSTEPS, loss=S.LOSS_DRAG, body_motion=motion)
+    assert L0 == L
+    case.cfg.shifting = 0
+    assert _loss(case, ity, lab, dt, motion, S.LOSS_DRAG) != L
+    case.cfg.shifting = 1
+    gc = np.einsum("sq,sqk->k", gm, jac)
+    for k in (0, 2):
+        eps = 1e-7
+        cp, cm = coeffs.copy(), coeffs.copy()
+        cp[k] += eps
+        cm[k] -= eps
+        fd = (_loss(case, ity, lab, dt, S.body_motion_schedule(cp, NSTEPS, dt, period=period)[0], S.LOSS_DRAG)
+              - _loss(case, ity, lab, dt, S.body_motion_schedule(cm, NSTEPS, dt, period=period)[0],
+                      S.LOSS_DRAG)) / (2 * eps)
+        _check(gc[k], fd, f"motion coefficient {k}")
+    rng = np.random.default_rng(320)
+    d = rng.standard_normal(2 * case.n) * 0.1
+    eps = 1e-7
+    fd = (_loss(case, ity, lab, dt, motion, S.LOSS_DRAG, vel=eps * d)
+          - _loss(case, ity, lab, dt, motion, S.LOSS_DRAG, vel=-eps * d)) / (2 * eps)
+    _check(float(g["vel0"] @ d), fd, "velocity direction")
+    for every in (1, NSTEPS):
+        got = _grad(case, ity, lab, dt, motion, S.LOSS_DRAG, every=every)
+        assert got[0] == L
+        for key in ("vel0", "rho0", "pos0"):
+            assert np.array_equal(got[1][key], g[key]), (every, key)
+        assert np.array_equal(got[2], gm)
+
+
 def test_moving_square_adjoint_rejects_unsupported(lib):
     case, ity, lab, dt = _case()
     cfg = case.cfg.copy()
@@ -190,18 +234,20 @@ def test_moving_square_adjoint_rejects_unsupported(lib):
         assert e.value.code == -7
 
 
+@pytest.mark.parametrize("shifting", [0, 1])
 @pytest.mark.parametrize("solver", SOLVERS)
 @pytest.mark.parametrize("loss", [S.LOSS_DRAG, S.LOSS_KINETIC_ENERGY])
-def test_moving_square_adjoint_matches_cpu_tangent_linear_reference(lib, oracle, loss, solver):
+def test_moving_square_adjoint_matches_cpu_tangent_linear_reference(lib, oracle, loss, solver, shifting):
     """g.delta from the GPU adjoint against the FP64 CPU tangent-linear model of
     the same steps (oracle/sph_tangent.cpp, oracle_tangent_ms) along directions
     in the initial velocity, position and density, the viscosity and the body
-    motion: both are exact derivatives of the same discrete map (1e-8)."""
+    motion: both are exact derivatives of the same discrete map (1e-8).  With
+    shifting, each step ends with the capped shift of the corrector RHS."""
     case, ity = S.make_moving_square(dx=0.1, lx=2.0, ly=1.0, D=0.4, solver=solver, jitter=0.05, seed=8)
     water = np.r_[case.type, case.type] == S.TYPE_WATER
     case.vel = case.vel + np.where(water, S.fourier_perturbation(case.pos, n_modes=4, amp=0.2, seed=8), 0.0)
     cfg = case.cfg
-    cfg.ghost_assign, cfg.shifting, cfg.mls_order = 1, 0, 0
+    cfg.ghost_assign, cfg.shifting, cfg.mls_order = 1, shifting, 0
     lab = S.moving_square_labels(case, ity)
     dt = 0.25 * cfg.h / np.sqrt(cfg.c0sq)
     motion, _ = S.body_motion_schedule([0.5, 0.3, -0.1], NSTEPS, dt, period=NSTEPS * dt)
