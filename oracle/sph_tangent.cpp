@@ -25,8 +25,8 @@
 // fixed-ghost assignment, the body force and the Euler predictor-corrector with
 // a per-step body motion (oracle_tangent_ms).  Either kernel, with or without
 // renormalisation, with or without shifting (the capped shift on the last
-// RHS's pairs, exponent 4 in (2)), density re-initialisation (orders 1, 3, 6)
-// in (1) only, no free-surface particles.  Other inputs return SPH_E_CONFIG.
+// RHS's pairs, exponent 4 in (2)), density re-initialisation (orders 1, 3, 6
+// in (1); 3, 6 in (2)), no free-surface particles.  Other inputs return SPH_E_CONFIG.
 // The pair search is a plain double loop (small cases only).
 
 #include <cmath>
@@ -760,6 +760,68 @@ struct MSModel {
         }
     }
 
+    // Reinitialize_particle_density, orders 3 and 6, moving-square variant
+    // (Moving_Square.../Reinitialize_particle_density.f90:92-200 with
+    // SPH_Subroutine_Module.f90:2565-2792) on the state after the corrector, the
+    // ghosts as the corrector RHS assigned them: for a water particle i every
+    // particle j within the support, i itself included, weighted by W_ij V_j,
+    // V_j = m_j / rho_j; rho_i = c.r with A c = e_1, A = sum W V p p^T + alpha^3 I,
+    // r = sum rho_j W V p; Shepard weights when A is singular (no few-neighbour
+    // fallback); the old density where the result is NaN.
+    void mls(MSParts<T>& P) const {
+        const sph_config& C = M.C;
+        const int m = C.mls_order;
+        const double hb = (C.h + C.h) / 2.0, rcut = C.kernel_scale * hb;
+        const double a3 = C.mls_alpha * C.mls_alpha * C.mls_alpha;
+        std::vector<T> out(P.n);
+        for (int i = 0; i < P.n; ++i) {
+            out[i] = P.rho[i];
+            if (P.type[i] != SPH_TYPE_WATER) continue;
+            T A[6][7], r[6];
+            for (int a = 0; a < 6; ++a) { r[a] = T(0.0); for (int b = 0; b < 7; ++b) A[a][b] = T(0.0); }
+            T sw(0.0), srw(0.0);
+            for (int j = 0; j < P.n; ++j) {
+                const T px = P.x[i] - P.x[j], py = P.y[i] - P.y[j];
+                const double d0 = std::sqrt(val(px) * val(px) + val(py) * val(py));
+                if (!(d0 <= rcut)) continue;
+                T w, g0, g1;
+                // the particle itself: distance 0 with no derivative
+                M.kernel(j == i ? T(0.0) : sqrt(px * px + py * py), px, py, hb, w, g0, g1);
+                w = w * (P.mass[j] / P.rho[j]);
+                const T dx = -px / C.h, dy = -py / C.h;
+                const T p[6] = {T(1.0), dx, dy, dx * dx, dx * dy, dy * dy};
+                for (int a = 0; a < m; ++a) {
+                    for (int b = 0; b < m; ++b) A[a][b] += w * p[a] * p[b];
+                    r[a] += P.rho[j] * w * p[a];
+                }
+                sw += w; srw += P.rho[j] * w;
+            }
+            for (int a = 0; a < m; ++a) { A[a][a] += a3; A[a][m] = T(a == 0 ? 1.0 : 0.0); }
+            bool ok = true;
+            for (int c = 0; c < m && ok; ++c) {
+                if (!(val(A[c][c]) > 0.0)) { ok = false; break; }
+                for (int q = c + 1; q < m; ++q) {
+                    const T f = A[q][c] / A[c][c];
+                    for (int b = c; b <= m; ++b) A[q][b] -= f * A[c][b];
+                }
+            }
+            T rho(0.0);
+            if (!ok) {
+                rho = srw / sw;
+            } else {
+                T cs[6];
+                for (int a = m - 1; a >= 0; --a) {
+                    T t = A[a][m];
+                    for (int b = a + 1; b < m; ++b) t -= A[a][b] * cs[b];
+                    cs[a] = t / A[a][a];
+                }
+                for (int a = 0; a < m; ++a) rho += cs[a] * r[a];
+            }
+            if (!std::isnan(val(rho))) out[i] = rho;
+        }
+        for (int i = 0; i < P.n; ++i) P.rho[i] = out[i];
+    }
+
     // single_step_compute of the moving square: the rates of every particle and,
     // when fx is given, the x body force of this RHS.
     int rhs(MSParts<T>& P, std::vector<T>& drho, std::vector<T>* acc, std::vector<T>* avg, T* fx,
@@ -1011,6 +1073,9 @@ int run_ms(const sph_config& cfg, MSParts<T>& H, const T& nu, const std::vector<
             P.u[i] = B0.u[i] + 0.5 * dt * (a[0][i] + ta0[i]);
             P.v[i] = B0.v[i] + 0.5 * dt * (a[1][i] + ta1[i]);
         }
+        // density re-initialisation after every mls_every-th step (1-based), before
+        // the shift
+        if (cfg.mls_order != 0 && (s + 1) % cfg.mls_every == 0) S.mls(P);
         if (cfg.shifting) {
             // the capped shift of the water particles (none is near a free surface
             // here) and the first-order density correction
@@ -1098,7 +1163,7 @@ int oracle_tangent_ms(const sph_config* cfg, int n, const double* pos, const dou
         return SPH_E_ARG;
     if ((cfg->solver != SPH_SOLVER_MS_MODLR_DELTA && cfg->solver != SPH_SOLVER_MS_HLLC_DELTA) ||
         cfg->integrator != SPH_INTEGRATOR_EULER_PC || (cfg->shifting && cfg->shift_n != 4) ||
-        cfg->mls_order != 0 || cfg->laplacian != 1 || cfg->free_surface || cfg->periodic)
+        cfg->mls_order == 1 || cfg->laplacian != 1 || cfg->free_surface || cfg->periodic)
         return SPH_E_CONFIG;
     for (int i = 0; i < n; ++i)
         if (type[i] <= SPH_TYPE_INLET) return SPH_E_CONFIG;

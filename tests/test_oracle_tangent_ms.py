@@ -2,8 +2,9 @@
 oracle_tangent_ms), the CPU reference of the moving-square adjoint: its value
 path must reproduce the oracle's Euler predictor-corrector steps with ghost
 assignment and a per-step body motion (final kinetic energy and the drag
-impulse), with and without the particle shift after the corrector, and its
-directional derivatives must match central differences of
+impulse), with and without the particle shift after the corrector and the
+moving-least-squares density re-initialisation (orders 3 and 6, every second
+step), and its directional derivatives must match central differences of
 its own value path."""
 import numpy as np
 import pytest
@@ -16,14 +17,14 @@ NSTEPS = 5
 SOLVERS = [S.SOLVER_MS_MODLR_DELTA, S.SOLVER_MS_HLLC_DELTA]
 
 
-def _case(solver=S.SOLVER_MS_MODLR_DELTA, shifting=0):
+def _case(solver=S.SOLVER_MS_MODLR_DELTA, shifting=0, mls_order=0):
     case, ity = S.make_moving_square(dx=0.1, lx=2.0, ly=1.0, D=0.4, solver=solver, jitter=0.05, seed=7)
     water = np.r_[case.type, case.type] == S.TYPE_WATER
     case.vel = case.vel + np.where(water, S.fourier_perturbation(case.pos, n_modes=4, amp=0.2, seed=7), 0.0)
     cfg = case.cfg
     cfg.ghost_assign = 1
     cfg.shifting = shifting
-    cfg.mls_order = 0
+    cfg.mls_order, cfg.mls_every = mls_order, 2
     lab = S.moving_square_labels(case, ity)
     dt = 0.25 * cfg.h / np.sqrt(cfg.c0sq)
     motion, _ = S.body_motion_schedule([0.5, 0.3, -0.1], NSTEPS, dt, period=NSTEPS * dt)
@@ -35,10 +36,13 @@ def _tangent(oracle, case, ity, lab, dt, motion, loss, cfg=None, **d):
                              ity, lab, 0.0, NSTEPS, dt, motion, loss, **d)
 
 
-@pytest.mark.parametrize("shifting", [0, 1])
+VARIANTS = [(0, 0), (1, 0), (0, 3), (1, 6)]      # (shifting, mls_order)
+
+
+@pytest.mark.parametrize("shifting,mls_order", VARIANTS)
 @pytest.mark.parametrize("solver", SOLVERS)
-def test_tangent_ms_value_path_reproduces_the_oracle(oracle, solver, shifting):
-    case, ity, lab, dt, motion = _case(solver, shifting)
+def test_tangent_ms_value_path_reproduces_the_oracle(oracle, solver, shifting, mls_order):
+    case, ity, lab, dt, motion = _case(solver, shifting, mls_order)
     ke, _ = _tangent(oracle, case, ity, lab, dt, motion, S.LOSS_KINETIC_ENERGY)
     drag, _ = _tangent(oracle, case, ity, lab, dt, motion, S.LOSS_DRAG)
     sim = oracle.OracleSim(case.cfg, case.pos, case.vel, case.rho, case.mass, case.type)
@@ -57,11 +61,11 @@ def test_tangent_ms_value_path_reproduces_the_oracle(oracle, solver, shifting):
     assert drag != 0.0
 
 
-@pytest.mark.parametrize("shifting", [0, 1])
+@pytest.mark.parametrize("shifting,mls_order", VARIANTS)
 @pytest.mark.parametrize("solver", SOLVERS)
 @pytest.mark.parametrize("loss", [S.LOSS_DRAG, S.LOSS_KINETIC_ENERGY])
-def test_tangent_ms_matches_its_central_differences(oracle, loss, solver, shifting):
-    case, ity, lab, dt, motion = _case(solver, shifting)
+def test_tangent_ms_matches_its_central_differences(oracle, loss, solver, shifting, mls_order):
+    case, ity, lab, dt, motion = _case(solver, shifting, mls_order)
     rng = np.random.default_rng(2)
     dmo = np.zeros_like(motion)
     dmo[:, 0] = rng.standard_normal(NSTEPS)
@@ -95,7 +99,7 @@ def test_tangent_ms_matches_its_central_differences(oracle, loss, solver, shifti
 
 def test_tangent_ms_rejects_configurations_outside_its_scope(oracle):
     case, ity, lab, dt, motion = _case()
-    for field, value in (("mls_order", 3), ("free_surface", 1)):
+    for field, value in (("mls_order", 1), ("free_surface", 1)):
         cfg = case.cfg.copy()
         setattr(cfg, field, value)
         with pytest.raises(RuntimeError):
