@@ -353,8 +353,11 @@ int sph_find_particle_pair_noalloc(const sph_config* cfg, int n, const double* d
  *    (ghost_assign = 1: the reverse runs through the Shepard interpolation onto
  *    the wall and body ghosts) or with caller-given ghost states, with or
  *    without particle shifting after the corrector (the capped shift of the
- *    corrector RHS over its pairs, ghosts included); without density
- *    re-initialisation.
+ *    corrector RHS over its pairs, ghosts included), with or without the
+ *    moving-least-squares density re-initialisation (mls_order 3 or 6, the
+ *    moving-square variant: W V weights, the particle itself counted, the
+ *    ghosts' density and mass as the corrector RHS assigned them).
+ * Density re-initialisation of order 1 returns SPH_E_CONFIG.
  * The reverse kernels compute in FP64 for both precisions of the forward step.
  *
  * Body motion: with body_motion set, step k of the forward run (k = 0 ..

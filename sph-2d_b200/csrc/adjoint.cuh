@@ -1129,6 +1129,12 @@ __global__ void k_adj_stage3(Params P, Sorted<R> D, Adj A, double dt, int shift,
 //   p_b-bar = lam rho_b W_b c - W_b ((c.p_b) y + (y.p_b) c)
 // (Shepard: rho_b-bar += lam W_b / S, W_b-bar = lam (rho_b - rho_a') / S), then
 // through p_b to x_b - x_a and through W_b to |x_a - x_b|.
+// The moving-square variant weights by W_b V_b, V_b = m_b / rho_b, counts a
+// itself (distance 0: no position derivative), tests only d <= r_cut, has no
+// few-neighbour fallback and keeps rho_a where the result is NaN: the formulas
+// above with W_b V_b in place of W_b, whose adjoint then reaches W_b (times
+// V_b), rho_b (times -W_b V_b / rho_b) and m_b (times W_b / rho_b; the ghosts'
+// assigned mass).
 
 // The Cholesky factor of k_mls's solve (the same operations in the same order,
 // so c = A^-1 e_1 takes the forward's bits) and a solve with it.
@@ -1199,16 +1205,25 @@ __global__ void k_adj_mls_end(Params P, Sorted<R> D, Adj A, int shift, double2* 
     lam[s] = lrho;
 }
 
+// The pair test of the re-initialisation: the support of the pair search, or
+// (moving square) d <= r_cut alone.
+__device__ __forceinline__ bool mls_in(const Params& P, double px, double py, double& d) {
+    const bool in = in_support(P, px, py, d);
+    return P.ms ? d <= P.r_cut : in;
+}
+
 // Per owner a (a water host): A, r and the solve of k_mls on the state V the
 // last stage produced, y = A^-1 (lam_a r), and the adjoint of x_a through its
-// own sum.  cy[15 a ..]: c (0-5), y (6-11), mode (12: 0 not an owner, 1 the
-// moving-least-squares weights, 2 Shepard), S (13), rho_a' (14).
+// own sum.  cy[16 a ..]: c (0-5), y (6-11), mode (12: 0 not an owner or the
+// density kept, 1 the moving-least-squares weights, 2 Shepard), S (13),
+// rho_a' (14), the adjoint of rho_a through a's own term (15, moving square).
 template <typename R, int M>
 __global__ void k_adj_mls_own(Params P, Sorted<R> V, const double* lam, double* cy, double2* xown) {
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= P.n_tot) return;
-    double* o = cy + (size_t)15 * a;
+    double* o = cy + (size_t)16 * a;
     o[12] = 0.0;
+    o[15] = 0.0;
     xown[a] = make_double2(0.0, 0.0);
     if (V.type[a] != SPH_TYPE_WATER || V.id[a] >= P.n_host) return;
     const double2 xa = V.pos[a];
@@ -1221,15 +1236,17 @@ __global__ void k_adj_mls_own(Params P, Sorted<R> V, const double* lam, double* 
     double sw = 0.0, srw = 0.0;
     int cnt = 0;
     const int nn = V.nnbr[a];
-    for (int e = 0; e < nn; ++e) {
-        const int b = (int)(V.nbr[(size_t)e * P.nbr_stride + a] & 0x7fffffffu);
+    // (the moving-square variant: a itself first, e = -1)
+    for (int e = P.ms ? -1 : 0; e < nn; ++e) {
+        const int b = e < 0 ? a : (int)(V.nbr[(size_t)e * P.nbr_stride + a] & 0x7fffffffu);
         const double2 xb = V.pos[b];
         const double px = xa.x - xb.x, py = xa.y - xb.y;
         double d;
-        if (!in_support(P, px, py, d)) continue;
+        if (!mls_in(P, px, py, d)) continue;
         double w, gx, gy;
         kernel_w_dw<double>(P, d, px, py, w, gx, gy);
         const double rho_b = V.kin[b].z;
+        if (P.ms) w *= V.mass[b] / rho_b;
         double p[M];
         const double dx = -px * inv_h, dy = -py * inv_h;
         p[0] = 1.0; p[1] = dx; p[2] = dy;
@@ -1249,7 +1266,7 @@ __global__ void k_adj_mls_own(Params P, Sorted<R> V, const double* lam, double* 
     for (int i = 0; i < M; ++i) Am[i * (i + 1) / 2 + i] += P.mls_alpha3;
     const double lm = lam[a];
     double L[M * (M + 1) / 2], c[M], y[M];
-    const bool ok = !(M == 6 && cnt <= 8) && mls_chol<M>(Am, L);
+    const bool ok = !(!P.ms && M == 6 && cnt <= 8) && mls_chol<M>(Am, L);
     const double out = srw / sw;
     if (ok) {
         double e1[M], lr[M];
@@ -1257,13 +1274,28 @@ __global__ void k_adj_mls_own(Params P, Sorted<R> V, const double* lam, double* 
         for (int i = 0; i < M; ++i) { e1[i] = i == 0 ? 1.0 : 0.0; lr[i] = lm * r[i]; }
         mls_solve<M>(L, e1, c);
         mls_solve<M>(L, lr, y);
+        double cr = 0.0;
 #pragma unroll
-        for (int i = 0; i < M; ++i) { o[i] = c[i]; o[6 + i] = y[i]; }
+        for (int i = 0; i < M; ++i) { o[i] = c[i]; o[6 + i] = y[i]; cr += c[i] * r[i]; }
         o[12] = 1.0;
+        // (the moving square keeps the old density where the result is NaN)
+        if (P.ms && isnan(cr)) { o[12] = 0.0; return; }
     } else {
+        if (P.ms && isnan(out)) return;
         o[12] = 2.0;
         o[13] = sw;
         o[14] = out;
+    }
+    if (P.ms) {
+        // a's own term: W(0) V_a with p = e_1, no position derivative
+        double d0;
+        mls_in(P, 0.0, 0.0, d0);
+        double w, gx, gy;
+        kernel_w_dw<double>(P, d0, 0.0, 0.0, w, gx, gy);
+        const double rho_a = V.kin[a].z;
+        const double wt = w * (V.mass[a] / rho_a);
+        const double Wt = ok ? c[0] * (lm * rho_a - y[0]) : lm * (rho_a - out) / sw;
+        o[15] = (ok ? lm * wt * c[0] : lm * wt / sw) - Wt * wt / rho_a;
     }
     double xb0 = 0.0, xb1 = 0.0;
     for (int e = 0; e < nn; ++e) {
@@ -1271,10 +1303,12 @@ __global__ void k_adj_mls_own(Params P, Sorted<R> V, const double* lam, double* 
         const double2 xb = V.pos[b];
         const double px = xa.x - xb.x, py = xa.y - xb.y;
         double d;
-        if (!in_support(P, px, py, d)) continue;
+        if (!mls_in(P, px, py, d)) continue;
         double w, gx, gy;
         kernel_w_dw<double>(P, d, px, py, w, gx, gy);
         const double rho_b = V.kin[b].z;
+        const double f = P.ms ? V.mass[b] / rho_b : 1.0;     // the weight W f
+        const double wt = w * f;
         double Wb;
         if (ok) {
             const double dx = -px * inv_h, dy = -py * inv_h;
@@ -1282,15 +1316,15 @@ __global__ void k_adj_mls_own(Params P, Sorted<R> V, const double* lam, double* 
             double cp = 0.0, yp = 0.0;
 #pragma unroll
             for (int i = 0; i < M; ++i) { cp += c[i] * p[i]; yp += y[i] * p[i]; }
-            Wb = cp * (lm * rho_b - yp);
+            Wb = cp * (lm * rho_b - yp) * f;
             double pb[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll
-            for (int i = 0; i < M; ++i) pb[i] = lm * rho_b * w * c[i] - w * (yp * c[i] + cp * y[i]);
+            for (int i = 0; i < M; ++i) pb[i] = lm * rho_b * wt * c[i] - wt * (yp * c[i] + cp * y[i]);
             double dxb, dyb;
             mls_pbar_to_d<M>(pb, dx, dy, dxb, dyb);
             xb0 -= dxb * inv_h; xb1 -= dyb * inv_h;       // (dx, dy) = (x_b - x_a)/h
         } else {
-            Wb = lm * (rho_b - out) / sw;
+            Wb = lm * (rho_b - out) / sw * f;
         }
         xb0 += Wb * gx; xb1 += Wb * gy;                   // grad_a W = (gx, gy)
     }
@@ -1300,33 +1334,39 @@ __global__ void k_adj_mls_own(Params P, Sorted<R> V, const double* lam, double* 
 // Per particle q: its position and density adjoints through the re-initialised
 // densities of the owners a it is a neighbour of (gathered over q's list, which
 // holds every such a), plus the step end's (xe) and the owner's own part (xown);
-// a particle that is not an owner keeps its density, rho' = rho.
+// a particle that is not an owner keeps its density, rho' = rho.  Moving
+// square: an owner's own term (cy[16 q + 15]) is added, and for the ghosts the
+// adjoints of the density and mass they carried (as the corrector RHS assigned
+// them) go to gm instead of orho (their density passes through: orho = lam).
 template <typename R, int M>
 __global__ void k_adj_mls_nbr(Params P, Sorted<R> V, const double* lam, const double* cy, const double2* xown,
-                              const double2* xe, double2* ox, double* orho) {
+                              const double2* xe, double2* ox, double* orho, double2* gm) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= P.n_tot) return;
     const double2 xq = V.pos[q];
     const double rho_q = V.kin[q].z;
-    const bool owner = V.type[q] == SPH_TYPE_WATER && V.id[q] < P.n_host;
+    const bool water = V.type[q] == SPH_TYPE_WATER;
+    const bool owner = water && V.id[q] < P.n_host && cy[(size_t)16 * q + 12] != 0.0;
+    const double fq = P.ms ? V.mass[q] / rho_q : 1.0;
     const double inv_h = 1.0 / P.h;
     const double2 x0 = xe[q], x1 = xown[q];
     double xb0 = x0.x + x1.x, xb1 = x0.y + x1.y;
-    double rb = owner ? 0.0 : lam[q];
+    double rb = 0.0, mb = 0.0;
     const int nn = V.nnbr[q];
     for (int e = 0; e < nn; ++e) {
         const int a = (int)(V.nbr[(size_t)e * P.nbr_stride + q] & 0x7fffffffu);
-        const double* o = cy + (size_t)15 * a;
+        const double* o = cy + (size_t)16 * a;
         const double mode = o[12];
         if (mode == 0.0) continue;
         const double2 xa = V.pos[a];
         const double px = xa.x - xq.x, py = xa.y - xq.y;
         double d;
-        if (!in_support(P, px, py, d)) continue;
+        if (!mls_in(P, px, py, d)) continue;
         double w, gx, gy;
         kernel_w_dw<double>(P, d, px, py, w, gx, gy);
+        const double wt = w * fq;
         const double lm = lam[a];
-        double Wb;
+        double Wt;                                         // the adjoint of the weight W fq
         if (mode == 1.0) {
             const double dx = -px * inv_h, dy = -py * inv_h;
             double p[6] = {1.0, dx, dy, dx * dx, dx * dy, dy * dy};
@@ -1334,23 +1374,47 @@ __global__ void k_adj_mls_nbr(Params P, Sorted<R> V, const double* lam, const do
             double cp = 0.0, yp = 0.0;
 #pragma unroll
             for (int i = 0; i < M; ++i) { c[i] = o[i]; y[i] = o[6 + i]; cp += c[i] * p[i]; yp += y[i] * p[i]; }
-            rb += lm * w * cp;
-            Wb = cp * (lm * rho_q - yp);
+            rb += lm * wt * cp;
+            Wt = cp * (lm * rho_q - yp);
             double pb[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll
-            for (int i = 0; i < M; ++i) pb[i] = lm * rho_q * w * c[i] - w * (yp * c[i] + cp * y[i]);
+            for (int i = 0; i < M; ++i) pb[i] = lm * rho_q * wt * c[i] - wt * (yp * c[i] + cp * y[i]);
             double dxb, dyb;
             mls_pbar_to_d<M>(pb, dx, dy, dxb, dyb);
             xb0 += dxb * inv_h; xb1 += dyb * inv_h;
         } else {
             const double S = o[13], out = o[14];
-            rb += lm * w / S;
-            Wb = lm * (rho_q - out) / S;
+            rb += lm * wt / S;
+            Wt = lm * (rho_q - out) / S;
         }
+        if (P.ms) {
+            rb -= Wt * wt / rho_q;                         // V_q = m_q / rho_q
+            mb += Wt * w / rho_q;
+        }
+        const double Wb = Wt * fq;
         xb0 -= Wb * gx; xb1 -= Wb * gy;                   // grad_q W = -grad_a W
     }
+    if (owner) rb += cy[(size_t)16 * q + 15];
     ox[q] = make_double2(xb0, xb1);
-    orho[q] = rb;
+    if (P.ms && !water) {
+        orho[q] = lam[q];
+        gm[q] = make_double2(rb, mb);
+    } else {
+        orho[q] = owner ? rb : rb + lam[q];
+        if (gm) gm[q] = make_double2(0.0, 0.0);
+    }
+}
+
+// The moving square's ghosts: the adjoints of the density and mass they carried
+// into the re-initialisation (gm) join those of the corrector RHS that assigned
+// them, after k_adj_c has formed the latter.
+template <typename R>
+__global__ void k_adj_add_ghost_rm(Params P, Sorted<R> D, Adj A, const double2* gm) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= P.n_tot || D.type[s] == SPH_TYPE_WATER) return;
+    const double2 g = gm[s];
+    A.sr[s] += g.x;
+    A.sm[s] += g.y;
 }
 
 // Sorted step-start adjoints -> id order; the K1 adjoint goes to the previous step.
@@ -1825,13 +1889,17 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_ghost_water(Params P, Sorte
 // Runge-Kutta step, k_adj_stage3); its reverse leaves smu, shgr, shbi, and D
 // carries that RHS's pass-A outputs.
 template <typename R>
-__global__ void k_adj_stage_end_ms(Params P, Sorted<R> D, Adj A, double dt, int shift) {
+__global__ void k_adj_stage_end_ms(Params P, Sorted<R> D, Adj A, double dt, int shift, const double2* ox = nullptr,
+                                   const double* orho = nullptr) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= P.n_tot) return;
     const int i = D.id[s];
     double2 lx = make_double2(0, 0), lv = make_double2(0, 0);
     double lrho = 0.0;
     if (i < P.n_host) { lx = A.lx[i]; lv = A.lv[i]; lrho = A.lrho[i]; }
+    // ox / orho: the adjoint of the corrected positions and densities when the
+    // step ended with the density re-initialisation (as in k_adj_stage3)
+    if (ox) { lx = ox[s]; lrho = orho[s]; shift = 0; }
     if (shift) shift_reverse<R>(P, D, A, s, i, lx, lrho);
     for (int k = 0; k < 2; ++k) {
         A.lr[k][s] = 0.0; A.la[k][s] = make_double2(0, 0); A.lg[k][s] = make_double2(0, 0);

@@ -717,9 +717,10 @@ struct AdjCtx {
     double2* mls_x = nullptr;   // adjoint of the positions it read, per slot
     double* mls_r = nullptr;    //   and of the densities
     double* mls_lam = nullptr;  // adjoint of the densities it produced
-    double* mls_cy = nullptr;   // per owner: c = A^-1 e_1, y = A^-1 (lam r), (mode, sum W, out) [15]
+    double* mls_cy = nullptr;   // per owner: c = A^-1 e_1, y = A^-1 (lam r), (mode, sum W, out, own) [16]
     double2* mls_xe = nullptr;  // the step end's position adjoint (after the shift's reverse)
     double2* mls_xo = nullptr;  // an owner's position adjoint through its own sum
+    double2* mls_gm = nullptr;  // moving square: the ghosts' density and mass adjoints through it
     double2* st_pos = nullptr;
     double4* st_kin = nullptr;
     double4* st_aux = nullptr;  // V4 of the pair precision (float4 uses the first half)
@@ -806,9 +807,8 @@ int snap_io(sph_handle* h, const Snap& s, int k, int n, bool save) {
 
 int adj_config_ok(const sph_handle* h, int loss) {
     const Params& P = h->P;
-    // density re-initialisation: moving least squares (orders 3, 6) with the
-    // Taylor-Green driver
-    if (P.mls_order && (P.ms || P.mls_order == 1)) return SPH_E_CONFIG;
+    // density re-initialisation: moving least squares (orders 3, 6)
+    if (P.mls_order == 1) return SPH_E_CONFIG;
     if (P.ms) {
         // moving-square modified linear or HLLC solver, Morris laplacian, Euler
         // predictor-corrector, with or without shifting
@@ -1010,8 +1010,9 @@ int adj_prepare_ctx(sph_handle* h, const sph_adj_config* ac) {
         const size_t nt = (size_t)X->cap_tot;
         int rc;
         if ((rc = adj_alloc(X, &X->mls_x, nt)) || (rc = adj_alloc(X, &X->mls_r, nt)) ||
-            (rc = adj_alloc(X, &X->mls_lam, nt)) || (rc = adj_alloc(X, &X->mls_cy, nt * 15)) ||
-            (rc = adj_alloc(X, &X->mls_xe, nt)) || (rc = adj_alloc(X, &X->mls_xo, nt)))
+            (rc = adj_alloc(X, &X->mls_lam, nt)) || (rc = adj_alloc(X, &X->mls_cy, nt * 16)) ||
+            (rc = adj_alloc(X, &X->mls_xe, nt)) || (rc = adj_alloc(X, &X->mls_xo, nt)) ||
+            (rc = adj_alloc(X, &X->mls_gm, nt)))
             return rc;
     }
     if (h->P.ms && !X->A.gavg) {
@@ -1190,7 +1191,10 @@ int step_keep(sph_handle* h, double dt, int j, bool full) {
         } else {
             if ((rc = keep_stage<R>(h, j, 0))) return rc;
             if (full) {
-                if ((rc = rhs<R>(h, 1)) || (rc = stage<R>(h, 11, dt, 0, h->cfg.shifting))) return rc;
+                if ((rc = rhs<R>(h, 1)) || (rc = stage<R>(h, 11, dt, 0, mls ? 0 : h->cfg.shifting))) return rc;
+                // the re-initialisation reads the corrected state (stage slot state 3)
+                if (mls && ((rc = keep_stage<R>(h, j, 3)) || (rc = reinit_density<R>(h, h->cfg.shifting))))
+                    return rc;
                 h->step_count++;
                 h->n_steps++;
             }
@@ -1328,11 +1332,11 @@ int adj_step(sph_handle* h, bool first, int j) {
         if (P.mls_order == 6) {
             k_adj_mls_own<R, 6><<<nbo, 128, 0, h->stream>>>(P, V3, X->mls_lam, X->mls_cy, X->mls_xo);
             k_adj_mls_nbr<R, 6><<<nbo, 128, 0, h->stream>>>(P, V3, X->mls_lam, X->mls_cy, X->mls_xo, X->mls_xe,
-                                                             X->mls_x, X->mls_r);
+                                                             X->mls_x, X->mls_r, nullptr);
         } else {
             k_adj_mls_own<R, 3><<<nbo, 128, 0, h->stream>>>(P, V3, X->mls_lam, X->mls_cy, X->mls_xo);
             k_adj_mls_nbr<R, 3><<<nbo, 128, 0, h->stream>>>(P, V3, X->mls_lam, X->mls_cy, X->mls_xo, X->mls_xe,
-                                                             X->mls_x, X->mls_r);
+                                                             X->mls_x, X->mls_r, nullptr);
         }
         k_adj_stage3<R><<<nb, 256, 0, h->stream>>>(P, D, A, dt, 0, X->mls_x, X->mls_r);
         h->launches += 4;
@@ -1398,16 +1402,18 @@ void adj_rhs_ms_values(sph_handle* h, const Sorted<R>& V, int kept_j) {
 
 // Reverse of one moving-square RHS evaluation on the state V with the rate
 // adjoints of RHS k of the step (0: the predictor's K1, 1: the corrector's):
-// the forward values first (adj_rhs_ms_values, unless shift: adj_step_ms formed
+// the forward values first (adj_rhs_ms_values, unless pre: adj_step_ms formed
 // them before the step end's reverse), then the reverse of pass C (and of the
 // step's drag term), of the shifting sums (shift: the corrector RHS of a step
-// with particle shifting, whose step-end reverse left smu / shgr / shbi), of the
-// per-particle end of pass A, of its pair sums and XSPH velocity, of the ghost
-// assignment, and of the predictor (pred = 1) or the step-start accumulation.
-// The body-motion adjoints of the RHS go to g_motion[4 jstep ..].
+// with particle shifting, whose step-end reverse left smu / shgr / shbi), the
+// ghosts' density and mass adjoints through the step's density
+// re-initialisation (gm, when it ran), the reverse of the per-particle end of
+// pass A, of its pair sums and XSPH velocity, of the ghost assignment, and of
+// the predictor (pred = 1) or the step-start accumulation.  The body-motion
+// adjoints of the RHS go to g_motion[4 jstep ..].
 template <typename R>
 int adj_rhs_ms(sph_handle* h, const Sorted<R>& V, int k, int pred, bool drag, int jstep, int kept_j = -1,
-               bool shift = false) {
+               bool pre = false, bool shift = false, const double2* gm = nullptr) {
     const Params& P = h->P;
     AdjCtx* X = h->adj;
     Adj A = X->A;
@@ -1421,7 +1427,7 @@ int adj_rhs_ms(sph_handle* h, const Sorted<R>& V, int k, int pred, bool drag, in
         A.gint = X->pa_gint + o;
         A.gsw = X->pa_gsw + o;
     }
-    if (!shift) adj_rhs_ms_values<R>(h, V, kept_j);
+    if (!pre) adj_rhs_ms_values<R>(h, V, kept_j);
     tic(h, PH_ADJ);
     CK(cudaMemsetAsync(V.nflag, 0, (size_t)P.n_tot, h->stream));
     if (P.hllc)
@@ -1431,6 +1437,10 @@ int adj_rhs_ms(sph_handle* h, const Sorted<R>& V, int k, int pred, bool drag, in
         k_adj_c<R, true><<<nbc, kAdjThreads, 0, h->stream>>>(P, V, A, A.lr[k], A.la[k], A.nu_part + (size_t)k * nbc);
     if (shift) {
         k_adj_shift<R><<<nb, kAdjThreads, 0, h->stream>>>(P, V, A);
+        h->launches += 1;
+    }
+    if (gm) {
+        k_adj_add_ghost_rm<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, V, A, gm);
         h->launches += 1;
     }
     if (drag) {
@@ -1481,19 +1491,47 @@ int adj_step_ms(sph_handle* h, bool first, int j, int jstep) {
     const bool kept = X->pa && X->seg_kept[j];
     const Sorted<R> V = kept ? pa_view<R>(h, stage_view<R>(h, j, 0), j) : stage_view<R>(h, j, 0);
     const bool shift = h->cfg.shifting != 0;
-    if (shift) {
+    // a step that ended with the density re-initialisation (never a kept one)
+    const bool mls = P.mls_order != 0 && (h->step_count + 1) % P.mls_every == 0;
+    const bool pre = shift || mls;
+    if (pre) {
         // the step end's shift reads the corrector RHS's pass A (B^-1, grad rho,
-        // flags) and its shifting sum over the assigned ghosts: re-form them first
+        // flags) and its shifting sum over the assigned ghosts, the
+        // re-initialisation the ghosts' mass as that RHS assigned it: re-form them
+        // first
         adj_rhs_ms_values<R>(h, V, kept ? j : -1);
         tic(h, PH_ADJ);
-        k_shift_sum<R><<<nb, 256, 0, h->stream>>>(P, V, A);
-        h->launches += 1;
+        if (shift) {
+            k_shift_sum<R><<<nb, 256, 0, h->stream>>>(P, V, A);
+            h->launches += 1;
+        }
     }
     tic(h, PH_ADJ);
-    k_adj_stage_end_ms<R><<<nb, 256, 0, h->stream>>>(P, shift && kept ? pa_view<R>(h, D, j) : D, A, dt,
-                                                      shift ? 1 : 0);
-    h->launches += 1;
-    if ((rc = adj_rhs_ms<R>(h, V, 1, 1, X->loss == SPH_LOSS_DRAG, jstep, kept ? j : -1, shift))) return rc;
+    if (mls) {
+        // the shift's reverse, then that of the re-initialisation on the corrected
+        // state (stage slot state 3) over the step's lists
+        const Sorted<R> V3 = stage_view<R>(h, j, 3);
+        const int nbo = blocks(P.n_tot, 128);
+        k_adj_mls_end<R><<<nb, 256, 0, h->stream>>>(P, D, A, shift ? 1 : 0, X->mls_xe, X->mls_lam);
+        if (P.mls_order == 6) {
+            k_adj_mls_own<R, 6><<<nbo, 128, 0, h->stream>>>(P, V3, X->mls_lam, X->mls_cy, X->mls_xo);
+            k_adj_mls_nbr<R, 6><<<nbo, 128, 0, h->stream>>>(P, V3, X->mls_lam, X->mls_cy, X->mls_xo, X->mls_xe,
+                                                             X->mls_x, X->mls_r, X->mls_gm);
+        } else {
+            k_adj_mls_own<R, 3><<<nbo, 128, 0, h->stream>>>(P, V3, X->mls_lam, X->mls_cy, X->mls_xo);
+            k_adj_mls_nbr<R, 3><<<nbo, 128, 0, h->stream>>>(P, V3, X->mls_lam, X->mls_cy, X->mls_xo, X->mls_xe,
+                                                             X->mls_x, X->mls_r, X->mls_gm);
+        }
+        k_adj_stage_end_ms<R><<<nb, 256, 0, h->stream>>>(P, D, A, dt, 0, X->mls_x, X->mls_r);
+        h->launches += 4;
+    } else {
+        k_adj_stage_end_ms<R><<<nb, 256, 0, h->stream>>>(P, shift && kept ? pa_view<R>(h, D, j) : D, A, dt,
+                                                          shift ? 1 : 0);
+        h->launches += 1;
+    }
+    if ((rc = adj_rhs_ms<R>(h, V, 1, 1, X->loss == SPH_LOSS_DRAG, jstep, kept ? j : -1, pre, shift,
+                            mls ? X->mls_gm : nullptr)))
+        return rc;
     if (first) {
         // the fresh K1 of the first step was evaluated on the step-start state
         k_adj_load<R><<<nb, 256, 0, h->stream>>>(P, D, nullptr, nullptr);

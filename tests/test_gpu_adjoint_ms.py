@@ -171,15 +171,20 @@ def test_moving_square_adjoint_independent_of_checkpoint_interval(lib):
         assert np.array_equal(got[2], ref[2])
 
 
-@pytest.mark.parametrize("solver", SOLVERS)
-def test_shifting_adjoint_matches_central_differences(lib, solver):
+@pytest.mark.parametrize("solver,shifting,mls_order", [(S.SOLVER_MS_MODLR_DELTA, 1, 0), (S.SOLVER_MS_HLLC_DELTA, 1, 0),
+                                                      (S.SOLVER_MS_MODLR_DELTA, 0, 3),
+                                                      (S.SOLVER_MS_HLLC_DELTA, 1, 6)])
+def test_shifting_and_mls_adjoint_matches_central_differences(lib, solver, shifting, mls_order):
     """Particle shifting after every corrector (Shift_particle_position.f90:
-    56-136 on the corrector RHS's pairs, ghosts included): drag gradient in two
-    motion coefficients and one velocity direction, and the same gradient at
-    every checkpoint interval (1: every corrector RHS kept from the segment
-    re-run; 16: all re-formed in the reverse step)."""
+    56-136 on the corrector RHS's pairs, ghosts included) and the density
+    re-initialisation every fourth step (Moving_Square.../
+    Reinitialize_particle_density.f90:92-200): drag gradient in two motion
+    coefficients and one velocity direction, and the same gradient at every
+    checkpoint interval (1: every corrector RHS kept from the segment re-run;
+    16: all re-formed in the reverse step)."""
     case, ity, lab, dt = _case(solver=solver)
-    case.cfg.shifting = 1
+    case.cfg.shifting = shifting
+    case.cfg.mls_order, case.cfg.mls_every = mls_order, 4
     period = NSTEPS * dt
     coeffs = np.array([0.5, 0.4, -0.2])
     motion, jac = S.body_motion_schedule(coeffs, NSTEPS, dt, period=period)
@@ -188,9 +193,9 @@ def test_shifting_adjoint_matches_central_differences(lib, solver):
     with _sim(case, ity, lab) as sim:
         L0 = sim.adjoint_forward(NSTEPS, dt, checkpoint_every=NSTEPS, loss=S.LOSS_DRAG, body_motion=motion)
     assert L0 == L
-    case.cfg.shifting = 0
+    case.cfg.shifting, case.cfg.mls_order = 0, 0
     assert _loss(case, ity, lab, dt, motion, S.LOSS_DRAG) != L
-    case.cfg.shifting = 1
+    case.cfg.shifting, case.cfg.mls_order = shifting, mls_order
     gc = np.einsum("sq,sqk->k", gm, jac)
     for k in (0, 2):
         eps = 1e-7
@@ -234,20 +239,24 @@ def test_moving_square_adjoint_rejects_unsupported(lib):
         assert e.value.code == -7
 
 
-@pytest.mark.parametrize("shifting", [0, 1])
+@pytest.mark.parametrize("shifting,mls_order", [(0, 0), (1, 0), (0, 3), (1, 6)])
 @pytest.mark.parametrize("solver", SOLVERS)
 @pytest.mark.parametrize("loss", [S.LOSS_DRAG, S.LOSS_KINETIC_ENERGY])
-def test_moving_square_adjoint_matches_cpu_tangent_linear_reference(lib, oracle, loss, solver, shifting):
+def test_moving_square_adjoint_matches_cpu_tangent_linear_reference(lib, oracle, loss, solver, shifting,
+                                                                     mls_order):
     """g.delta from the GPU adjoint against the FP64 CPU tangent-linear model of
     the same steps (oracle/sph_tangent.cpp, oracle_tangent_ms) along directions
     in the initial velocity, position and density, the viscosity and the body
     motion: both are exact derivatives of the same discrete map (1e-8).  With
-    shifting, each step ends with the capped shift of the corrector RHS."""
+    shifting, each step ends with the capped shift of the corrector RHS; with
+    mls_order, every fourth step re-initialises the density first (the
+    moving-square variant: W V weights over every particle in the support, the
+    ghosts with the density and mass the corrector RHS assigned them)."""
     case, ity = S.make_moving_square(dx=0.1, lx=2.0, ly=1.0, D=0.4, solver=solver, jitter=0.05, seed=8)
     water = np.r_[case.type, case.type] == S.TYPE_WATER
     case.vel = case.vel + np.where(water, S.fourier_perturbation(case.pos, n_modes=4, amp=0.2, seed=8), 0.0)
     cfg = case.cfg
-    cfg.ghost_assign, cfg.shifting, cfg.mls_order = 1, shifting, 0
+    cfg.ghost_assign, cfg.shifting, cfg.mls_order, cfg.mls_every = 1, shifting, mls_order, 4
     lab = S.moving_square_labels(case, ity)
     dt = 0.25 * cfg.h / np.sqrt(cfg.c0sq)
     motion, _ = S.body_motion_schedule([0.5, 0.3, -0.1], NSTEPS, dt, period=NSTEPS * dt)
