@@ -21,17 +21,30 @@ namespace sph {
 // HLREC: in the mixed path, read the hi/lo float records (position, u, v, rho, p)
 // instead of the FP64 ones and form the pair differences in FP32 from them
 // (see store_split); the adjoint, which runs this pass on stored stage states
-// that carry only the FP64 records, uses HLREC = false.  MS: the moving-square
-// solvers (P.ms), whose XSPH sum is formed here; compile-time so that the
-// Taylor-Green launches carry none of its registers.
+// that carry only the FP64 records, uses HLREC = false.  The Taylor-Green
+// launch forms the differences of u, v, rho and p from the hi parts alone (the
+// position difference keeps hi + lo: the kernel and B need it to the FP32
+// rounding of the FP64 difference): each gradient term is an FP32 product
+// summed in FP32, and at 2048^2 dropping the lo record took this pass from
+// 2.07 to 1.87 ms per step (1.80 at 8 blocks per SM) while the velocity L2
+// against FP64 after 100 steps went from 2.78e-6 to 2.83e-6 and the density
+// error (relative to its variation) from 2.46e-5 to 2.70e-5.  MS: the
+// moving-square solvers (P.ms), whose XSPH sum is formed here and which keep
+// the hi + lo differences; compile-time so that the Taylor-Green launches carry
+// none of its registers.
 #ifndef SPH_PASS_A_F32_BLOCKS
-#define SPH_PASS_A_F32_BLOCKS 7
+#define SPH_PASS_A_F32_BLOCKS 8
+#endif
+#ifndef SPH_PASS_A_F32_MS_BLOCKS
+#define SPH_PASS_A_F32_MS_BLOCKS 7
 #endif
 template <typename R, bool HLREC, bool MS>
-__global__ void __launch_bounds__(128, sizeof(R) == 4 ? SPH_PASS_A_F32_BLOCKS : 4) k_pass_a(Params P, Sorted<R> D) {
+__global__ void __launch_bounds__(128, sizeof(R) == 4 ? (MS ? SPH_PASS_A_F32_MS_BLOCKS : SPH_PASS_A_F32_BLOCKS) : 4)
+    k_pass_a(Params P, Sorted<R> D) {
     using V4 = typename VT<R>::V4;
     constexpr bool F32 = sizeof(R) == 4;
     constexpr bool HL = HLREC && F32;
+    constexpr bool LO = HL && MS;        // the lo parts of u, v, rho, p
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= P.n_tot) return;
     const int ta = D.type[a];
@@ -40,7 +53,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? SPH_PASS_A_F32_BLOCKS : 
     const double4 ka = HL ? make_double4(0.0, 0.0, __ldg(&D.kin[a].z), 0.0) : D.kin[a];
     const float4 xa_hl = HL ? D.xhl[a] : make_float4(0.f, 0.f, 0.f, 0.f);
     const float4 kah = HL ? D.kh[a] : make_float4(0.f, 0.f, 0.f, 0.f);
-    const float4 kal = HL ? D.kl[a] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 kal = LO ? D.kl[a] : make_float4(0.f, 0.f, 0.f, 0.f);
     const double rho_a = ka.z;
     // the sums of this pass have no large cancellation (differences of smooth
     // fields, or B ~ I), so FP32 accumulates them directly in the mixed path
@@ -64,7 +77,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? SPH_PASS_A_F32_BLOCKS : 
     float4 xbhl_n = make_float4(0.f, 0.f, 0.f, 0.f), kbh_n = xbhl_n, kbl_n = xbhl_n;
     R vb_n = R(0);
     auto fetch = [&](int bb) {
-        if (HL) { xbhl_n = __ldg(&D.xhl[bb]); kbh_n = __ldg(&D.kh[bb]); kbl_n = __ldg(&D.kl[bb]); }
+        if (HL) { xbhl_n = __ldg(&D.xhl[bb]); kbh_n = __ldg(&D.kh[bb]); if (LO) kbl_n = __ldg(&D.kl[bb]); }
         else { xb_n = __ldg(&D.pos[bb]); kb_n = D.kin[bb]; }
         vb_n = D.aux[bb].y;
     };
@@ -117,11 +130,16 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? SPH_PASS_A_F32_BLOCKS : 
         }
         // differences of the records (b minus a): FP64, or hi/lo in FP32
         R drho, du, dv, dp;
-        if (HL) {
+        if (LO) {
             drho = (R)((kbh.z - kah.z) + (kbl.z - kal.z));
             du = (R)((kbh.x - kah.x) + (kbl.x - kal.x));
             dv = (R)((kbh.y - kah.y) + (kbl.y - kal.y));
             dp = (R)((kbh.w - kah.w) + (kbl.w - kal.w));
+        } else if (HL) {
+            drho = (R)(kbh.z - kah.z);
+            du = (R)(kbh.x - kah.x);
+            dv = (R)(kbh.y - kah.y);
+            dp = (R)(kbh.w - kah.w);
         } else {
             drho = (R)(kb.z - ka.z);
             du = (R)(kb.x - ka.x); dv = (R)(kb.y - ka.y);
