@@ -341,8 +341,9 @@ int sph_find_particle_pair_noalloc(const sph_config* cfg, int n, const double* d
  *    RK4 driver, with or without particle
  *    shifting (the limiter, the capped shift and its density correction are
  *    differentiated on the branch the forward took), with or without the
- *    moving-least-squares density re-initialisation (mls_order 3 or 6; its
- *    Shepard fallback differentiated where the forward took it); with the
+ *    density re-initialisation (mls_order 3 or 6, moving least squares, its
+ *    Shepard fallback differentiated where the forward took it; mls_order 1,
+ *    the Shepard density on the last RHS's pairs); with the
  *    re-initialisation every step of a checkpoint segment must keep its states,
  *    else sph_adjoint_forward returns SPH_E_CAPACITY (lower checkpoint_every);
  *  - the moving-square modified linear Riemann and HLLC solvers
@@ -354,10 +355,9 @@ int sph_find_particle_pair_noalloc(const sph_config* cfg, int n, const double* d
  *    the wall and body ghosts) or with caller-given ghost states, with or
  *    without particle shifting after the corrector (the capped shift of the
  *    corrector RHS over its pairs, ghosts included), with or without the
- *    moving-least-squares density re-initialisation (mls_order 3 or 6, the
- *    moving-square variant: W V weights, the particle itself counted, the
- *    ghosts' density and mass as the corrector RHS assigned them).
- * Density re-initialisation of order 1 returns SPH_E_CONFIG.
+ *    density re-initialisation (mls_order 3 or 6, the moving-square variant:
+ *    W V weights, the particle itself counted, the ghosts' density and mass as
+ *    the corrector RHS assigned them; mls_order 1 on the corrector RHS's pairs).
  * The reverse kernels compute in FP64 for both precisions of the forward step.
  *
  * Body motion: with body_motion set, step k of the forward run (k = 0 ..

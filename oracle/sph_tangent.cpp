@@ -25,8 +25,8 @@
 // fixed-ghost assignment, the body force and the Euler predictor-corrector with
 // a per-step body motion (oracle_tangent_ms).  Either kernel, with or without
 // renormalisation, with or without shifting (the capped shift on the last
-// RHS's pairs, exponent 4 in (2)), density re-initialisation (orders 1, 3, 6
-// in (1); 3, 6 in (2)), no free-surface particles.  Other inputs return SPH_E_CONFIG.
+// RHS's pairs, exponent 4 in (2)), density re-initialisation (orders 1, 3, 6),
+// no free-surface particles.  Other inputs return SPH_E_CONFIG.
 // The pair search is a plain double loop (small cases only).
 
 #include <cmath>
@@ -825,7 +825,7 @@ struct MSModel {
     // single_step_compute of the moving square: the rates of every particle and,
     // when fx is given, the x body force of this RHS.
     int rhs(MSParts<T>& P, std::vector<T>& drho, std::vector<T>* acc, std::vector<T>* avg, T* fx,
-            std::vector<T>* sh = nullptr, std::vector<T>* gr = nullptr) const {
+            std::vector<T>* sh = nullptr, std::vector<T>* gr = nullptr, std::vector<T>* o1 = nullptr) const {
         const sph_config& C = M.C;
         const TConsts& K = M.K;
         const T& nu = M.nu;
@@ -855,6 +855,24 @@ struct MSModel {
             dx0[k] = P.x[i] - P.x[j]; dx1[k] = P.y[i] - P.y[j];
             const T d = sqrt(dx0[k] * dx0[k] + dx1[k] * dx1[k]);
             M.kernel(d, dx0[k], dx1[k], hb, w[k], dw0[k], dw1[k]);
+        }
+        if (o1) {
+            // RefreshDensity_MLS_Order = 1 on this RHS's pairs (Moving_Square.../
+            // Reinitialize_particle_density.f90:66-88): rho_i = sum m_j w_ij / sum_w(i),
+            // sum_w(i) = sum w_ij V_j over the same-type pairs
+            std::vector<T> sw(n, T(0.0)), a1(n, T(0.0));
+            for (size_t k = 0; k < np; ++k) {
+                const int i = pi[k], j = pj[k];
+                if (P.type[i] != P.type[j]) continue;
+                sw[i] += w[k] * vol[j]; sw[j] += w[k] * vol[i];
+            }
+            for (size_t k = 0; k < np; ++k) {
+                const int i = pi[k], j = pj[k];
+                if (P.type[i] != P.type[j]) continue;
+                if (P.type[i] == SPH_TYPE_WATER) a1[i] += P.mass[j] * w[k] / sw[i];
+                if (P.type[j] == SPH_TYPE_WATER) a1[j] += P.mass[i] * w[k] / sw[j];
+            }
+            *o1 = a1;
         }
         std::vector<T> bi[4];
         for (int q = 0; q < 4; ++q) bi[q].assign(n, T(q == 0 || q == 3 ? 1.0 : 0.0));
@@ -1062,8 +1080,11 @@ int run_ms(const sph_config& cfg, MSParts<T>& H, const T& nu, const std::vector<
             P.v[i] = B0.v[i] + dt * a[1][i];
         }
         T fx;
-        std::vector<T> sh[2], gr[2];
-        if ((rc = S.rhs(P, dr, a, g, &fx, cfg.shifting ? sh : nullptr, gr))) return rc;
+        std::vector<T> sh[2], gr[2], o1;
+        const bool mls_step = cfg.mls_order != 0 && (s + 1) % cfg.mls_every == 0;
+        if ((rc = S.rhs(P, dr, a, g, &fx, cfg.shifting ? sh : nullptr, gr,
+                        mls_step && cfg.mls_order == 1 ? &o1 : nullptr)))
+            return rc;
         drag = drag + dt * fx;
         for (int i = 0; i < n; ++i) {
             if (P.type[i] != SPH_TYPE_WATER) continue;
@@ -1075,7 +1096,14 @@ int run_ms(const sph_config& cfg, MSParts<T>& H, const T& nu, const std::vector<
         }
         // density re-initialisation after every mls_every-th step (1-based), before
         // the shift
-        if (cfg.mls_order != 0 && (s + 1) % cfg.mls_every == 0) S.mls(P);
+        if (mls_step) {
+            if (cfg.mls_order == 1) {
+                for (int i = 0; i < n; ++i)
+                    if (P.type[i] == SPH_TYPE_WATER) P.rho[i] = o1[i];
+            } else {
+                S.mls(P);
+            }
+        }
         if (cfg.shifting) {
             // the capped shift of the water particles (none is near a free surface
             // here) and the first-order density correction
@@ -1163,7 +1191,7 @@ int oracle_tangent_ms(const sph_config* cfg, int n, const double* pos, const dou
         return SPH_E_ARG;
     if ((cfg->solver != SPH_SOLVER_MS_MODLR_DELTA && cfg->solver != SPH_SOLVER_MS_HLLC_DELTA) ||
         cfg->integrator != SPH_INTEGRATOR_EULER_PC || (cfg->shifting && cfg->shift_n != 4) ||
-        cfg->mls_order == 1 || cfg->laplacian != 1 || cfg->free_surface || cfg->periodic)
+        cfg->laplacian != 1 || cfg->free_surface || cfg->periodic)
         return SPH_E_CONFIG;
     for (int i = 0; i < n; ++i)
         if (type[i] <= SPH_TYPE_INLET) return SPH_E_CONFIG;

@@ -1417,6 +1417,101 @@ __global__ void k_adj_add_ghost_rm(Params P, Sorted<R> D, Adj A, const double2* 
     A.sm[s] += g.y;
 }
 
+// ---- reverse of the order-1 re-initialisation --------------------------------
+// The forward (k_mls1) forms, on the state of the step's last RHS and over its
+// pair list, for a water host a:
+//   rho_a' = S_m / S_w,  S_m = sum_b m_b W_ab,  S_w = sum_b W_ab V_b,  V_b = m_b / rho_b,
+// over the pairs with a neighbour b of a's type; the stage that ends the step
+// then discards a's integrated density.  With lam the adjoint of rho_a':
+//   W_ab-bar = lam m_b (1 - rho_a' / rho_b) / S_w,
+//   rho_b-bar += lam rho_a' W_ab m_b / (S_w rho_b^2).
+
+// The step end's split: the positions' adjoint passes through to the last
+// stage, a water host's density adjoint goes to the re-initialisation alone
+// (its integrated density was replaced), the others' pass through.
+template <typename R>
+__global__ void k_adj_mls1_end(Params P, Sorted<R> D, const double2* xe, const double* lam, double2* ox,
+                               double* orho) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= P.n_tot) return;
+    ox[s] = xe[s];
+    orho[s] = (D.type[s] == SPH_TYPE_WATER && D.id[s] < P.n_host) ? 0.0 : lam[s];
+}
+
+// Per owner a on the last RHS's state V: S_w and rho_a' with k_mls1's operations
+// (cy[16 a ..]: mode 12 = 2 for an owner, S_w 13, rho_a' 14).
+template <typename R>
+__global__ void k_adj_mls1_own(Params P, Sorted<R> V, double* cy) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= P.n_tot) return;
+    double* o = cy + (size_t)16 * a;
+    o[12] = 0.0;
+    const int ta = V.type[a];
+    if (ta != SPH_TYPE_WATER || V.id[a] >= P.n_host) return;
+    const double2 xa = V.pos[a];
+    double sw = 0.0, sm = 0.0;
+    const int nn = V.npairs[a];
+    for (int e = 0; e < nn; ++e) {
+        const int b = (int)(V.pairs[(size_t)e * P.nbr_stride + a] & 0x7fffffffu);
+        if (V.type[b] != ta) continue;
+        const double2 xb = V.pos[b];
+        const double px = xa.x - xb.x, py = xa.y - xb.y;
+        const double d = __dsqrt_rn(__dadd_rn(__dmul_rn(px, px), __dmul_rn(py, py)));
+        double w, gx, gy;
+        kernel_w_dw<double>(P, d, px, py, w, gx, gy);
+        const double mb = V.mass[b];
+        sw += w * (mb / V.kin[b].z);
+        sm += mb * w;
+    }
+    o[12] = 2.0;
+    o[13] = sw;
+    o[14] = sm / sw;
+}
+
+// Per particle q of the last RHS's state: the adjoints of its position and
+// density through its own order-1 density and those of the owners in its pair
+// list, added to sx and sr (after k_adj_c has formed the RHS's own).
+template <typename R>
+__global__ void k_adj_mls1_nbr(Params P, Sorted<R> V, Adj A, const double* lam, const double* cy) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= P.n_tot) return;
+    const int tq = V.type[q];
+    const double2 xq = V.pos[q];
+    const double rho_q = V.kin[q].z, m_q = V.mass[q];
+    const double* oq = cy + (size_t)16 * q;
+    const bool own = oq[12] != 0.0;
+    const double lq = own ? lam[q] : 0.0, swq = own ? oq[13] : 1.0, rq = own ? oq[14] : 0.0;
+    double x0b = 0.0, x1b = 0.0, rb = 0.0;
+    const int nn = V.npairs[q];
+    for (int e = 0; e < nn; ++e) {
+        const int b = (int)(V.pairs[(size_t)e * P.nbr_stride + q] & 0x7fffffffu);
+        if (V.type[b] != tq) continue;
+        const double* ob = cy + (size_t)16 * b;
+        const bool bown = ob[12] != 0.0;
+        if (!own && !bown) continue;
+        const double2 xb = V.pos[b];
+        const double px = xq.x - xb.x, py = xq.y - xb.y;
+        const double d = __dsqrt_rn(__dadd_rn(__dmul_rn(px, px), __dmul_rn(py, py)));
+        double w, gx, gy;
+        kernel_w_dw<double>(P, d, px, py, w, gx, gy);      // grad_q W = (gx, gy)
+        double Wb = 0.0;
+        if (own) {
+            const double rho_b = V.kin[b].z;
+            Wb += lq * V.mass[b] * (1.0 - rq / rho_b) / swq;
+        }
+        if (bown) {
+            const double lb = lam[b], swb = ob[13], rbp = ob[14];
+            Wb += lb * m_q * (1.0 - rbp / rho_q) / swb;
+            rb += lb * rbp * w * m_q / (swb * (rho_q * rho_q));
+        }
+        x0b += Wb * gx;
+        x1b += Wb * gy;
+    }
+    const double2 sx = A.sx[q];
+    A.sx[q] = make_double2(sx.x + x0b, sx.y + x1b);
+    A.sr[q] += rb;
+}
+
 // Sorted step-start adjoints -> id order; the K1 adjoint goes to the previous step.
 template <typename R>
 __global__ void k_adj_scatter(Params P, Sorted<R> D, Adj A, int first) {

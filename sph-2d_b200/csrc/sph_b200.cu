@@ -807,8 +807,6 @@ int snap_io(sph_handle* h, const Snap& s, int k, int n, bool save) {
 
 int adj_config_ok(const sph_handle* h, int loss) {
     const Params& P = h->P;
-    // density re-initialisation: moving least squares (orders 3, 6)
-    if (P.mls_order == 1) return SPH_E_CONFIG;
     if (P.ms) {
         // moving-square modified linear or HLLC solver, Morris laplacian, Euler
         // predictor-corrector, with or without shifting
@@ -1162,6 +1160,7 @@ int step_keep(sph_handle* h, double dt, int j, bool full) {
     // runs in full, and its reverse reads the state the last stage produced
     // (stage slot state 3) and the neighbour lists
     const bool mls = h->P.mls_order != 0 && (h->step_count + 1) % h->P.mls_every == 0;
+    const bool mls1 = mls && h->P.mls_order == 1;   // formed on the last RHS, before the final stage
     if (mls) full = true;
     // the RHS evaluations of a step that runs here in full (the moving square's
     // corrector; the Runge-Kutta RHS 2-4) fill its pass-A slots, and its reverse
@@ -1191,7 +1190,9 @@ int step_keep(sph_handle* h, double dt, int j, bool full) {
         } else {
             if ((rc = keep_stage<R>(h, j, 0))) return rc;
             if (full) {
-                if ((rc = rhs<R>(h, 1)) || (rc = stage<R>(h, 11, dt, 0, mls ? 0 : h->cfg.shifting))) return rc;
+                if ((rc = rhs<R>(h, 1)) || (mls1 && (rc = mls1_on_last_rhs<R>(h))) ||
+                    (rc = stage<R>(h, 11, dt, 0, mls ? 0 : h->cfg.shifting)))
+                    return rc;
                 // the re-initialisation reads the corrected state (stage slot state 3)
                 if (mls && ((rc = keep_stage<R>(h, j, 3)) || (rc = reinit_density<R>(h, h->cfg.shifting))))
                     return rc;
@@ -1220,7 +1221,9 @@ int step_keep(sph_handle* h, double dt, int j, bool full) {
     if (full) {
         {
             PaSwap<R> sw(h, 3 * j + 2, keep_pa);
-            if ((rc = rhs<R>(h, 1)) || (rc = stage<R>(h, 3, dt, 0, mls ? 0 : h->cfg.shifting))) return rc;
+            if ((rc = rhs<R>(h, 1)) || (mls1 && (rc = mls1_on_last_rhs<R>(h))) ||
+                (rc = stage<R>(h, 3, dt, 0, mls ? 0 : h->cfg.shifting)))
+                return rc;
         }
         if (mls && ((rc = keep_stage<R>(h, j, 3)) || (rc = reinit_density<R>(h, h->cfg.shifting)))) return rc;
         h->step_count++;
@@ -1253,8 +1256,11 @@ void adj_pass_a(sph_handle* h, const Sorted<R>& V) {
 // of RHS k of the step; stage = the stage that produced V (-1: the step start).
 // shift: the last RHS of a step with particle shifting (pass A already re-run by
 // adj_step, the step-end reverse left smu / shgr / shbi).
+// mls1: the last RHS of a step that ended with the order-1 re-initialisation,
+// formed on this RHS's state and pairs (its reverse follows k_adj_c).
 template <typename R>
-int adj_rhs(sph_handle* h, const Sorted<R>& V, int k, int stage, bool shift = false, bool kept = false) {
+int adj_rhs(sph_handle* h, const Sorted<R>& V, int k, int stage, bool shift = false, bool kept = false,
+            bool mls1 = false) {
     const Params& P = h->P;
     AdjCtx* X = h->adj;
     Adj& A = X->A;
@@ -1273,6 +1279,11 @@ int adj_rhs(sph_handle* h, const Sorted<R>& V, int k, int stage, bool shift = fa
     if (shift) {
         k_adj_shift<R><<<nb, kAdjThreads, 0, h->stream>>>(P, V, A);
         h->launches += 1;
+    }
+    if (mls1) {
+        k_adj_mls1_own<R><<<blocks(P.n_tot, 128), 128, 0, h->stream>>>(P, V, X->mls_cy);
+        k_adj_mls1_nbr<R><<<blocks(P.n_tot, 128), 128, 0, h->stream>>>(P, V, A, X->mls_lam, X->mls_cy);
+        h->launches += 2;
     }
     k_adj_point<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, V, A, shift ? 1 : 0);
     if (P.muscl) k_adj_a<R, false, true><<<nbc, kAdjThreads, 0, h->stream>>>(P, V, A, stage, X->dt, nullptr);
@@ -1323,7 +1334,15 @@ int adj_step(sph_handle* h, bool first, int j) {
     tic(h, PH_ADJ);
     // a step that ended with the density re-initialisation (never a kept one)
     const bool mls = P.mls_order != 0 && (h->step_count + 1) % P.mls_every == 0;
-    if (mls) {
+    const bool mls1 = mls && P.mls_order == 1;
+    if (mls1) {
+        // the shift's reverse; the positions pass through to the last stage, the
+        // re-initialised densities' adjoint waits for the last RHS's reverse
+        k_adj_mls_end<R><<<nb, 256, 0, h->stream>>>(P, D, A, shift ? 1 : 0, X->mls_xe, X->mls_lam);
+        k_adj_mls1_end<R><<<nb, 256, 0, h->stream>>>(P, D, X->mls_xe, X->mls_lam, X->mls_x, X->mls_r);
+        k_adj_stage3<R><<<nb, 256, 0, h->stream>>>(P, D, A, dt, 0, X->mls_x, X->mls_r);
+        h->launches += 3;
+    } else if (mls) {
         // the shift's reverse, then that of the re-initialisation on the state the
         // last stage produced (stage slot state 3) over the step's lists
         const Sorted<R> V3 = stage_view<R>(h, j, 3);
@@ -1348,7 +1367,7 @@ int adj_step(sph_handle* h, bool first, int j) {
         h->launches += 1;
     }
     for (int k = 2; k >= 0; --k)
-        if ((rc = adj_rhs<R>(h, view(k), k + 1, k, shift && k == 2, kept))) return rc;
+        if ((rc = adj_rhs<R>(h, view(k), k + 1, k, shift && k == 2, kept, mls1 && k == 2))) return rc;
     if (first) {
         // the fresh K1 of the first step was evaluated on the step-start state
         k_adj_load<R><<<nb, 256, 0, h->stream>>>(P, D, nullptr, nullptr);
@@ -1413,7 +1432,7 @@ void adj_rhs_ms_values(sph_handle* h, const Sorted<R>& V, int kept_j) {
 // adjoints of the RHS go to g_motion[4 jstep ..].
 template <typename R>
 int adj_rhs_ms(sph_handle* h, const Sorted<R>& V, int k, int pred, bool drag, int jstep, int kept_j = -1,
-               bool pre = false, bool shift = false, const double2* gm = nullptr) {
+               bool pre = false, bool shift = false, const double2* gm = nullptr, bool mls1 = false) {
     const Params& P = h->P;
     AdjCtx* X = h->adj;
     Adj A = X->A;
@@ -1442,6 +1461,11 @@ int adj_rhs_ms(sph_handle* h, const Sorted<R>& V, int k, int pred, bool drag, in
     if (gm) {
         k_adj_add_ghost_rm<R><<<blocks(P.n_tot, 256), 256, 0, h->stream>>>(P, V, A, gm);
         h->launches += 1;
+    }
+    if (mls1) {
+        k_adj_mls1_own<R><<<blocks(P.n_tot, 128), 128, 0, h->stream>>>(P, V, X->mls_cy);
+        k_adj_mls1_nbr<R><<<blocks(P.n_tot, 128), 128, 0, h->stream>>>(P, V, A, X->mls_lam, X->mls_cy);
+        h->launches += 2;
     }
     if (drag) {
         double* part = A.nu_part + (size_t)4 * nbc;
@@ -1507,7 +1531,14 @@ int adj_step_ms(sph_handle* h, bool first, int j, int jstep) {
         }
     }
     tic(h, PH_ADJ);
-    if (mls) {
+    const bool mls1 = mls && P.mls_order == 1;
+    if (mls1) {
+        // as in adj_step: the densities' adjoint goes to the corrector RHS's reverse
+        k_adj_mls_end<R><<<nb, 256, 0, h->stream>>>(P, D, A, shift ? 1 : 0, X->mls_xe, X->mls_lam);
+        k_adj_mls1_end<R><<<nb, 256, 0, h->stream>>>(P, D, X->mls_xe, X->mls_lam, X->mls_x, X->mls_r);
+        k_adj_stage_end_ms<R><<<nb, 256, 0, h->stream>>>(P, D, A, dt, 0, X->mls_x, X->mls_r);
+        h->launches += 3;
+    } else if (mls) {
         // the shift's reverse, then that of the re-initialisation on the corrected
         // state (stage slot state 3) over the step's lists
         const Sorted<R> V3 = stage_view<R>(h, j, 3);
@@ -1530,7 +1561,7 @@ int adj_step_ms(sph_handle* h, bool first, int j, int jstep) {
         h->launches += 1;
     }
     if ((rc = adj_rhs_ms<R>(h, V, 1, 1, X->loss == SPH_LOSS_DRAG, jstep, kept ? j : -1, pre, shift,
-                            mls ? X->mls_gm : nullptr)))
+                            mls && !mls1 ? X->mls_gm : nullptr, mls1)))
         return rc;
     if (first) {
         // the fresh K1 of the first step was evaluated on the step-start state

@@ -117,7 +117,8 @@ def _check(ad, fd, what):
 
 @pytest.mark.parametrize("kind", ["wendland-renorm", "reference-gaussian", "wendland-renorm-shift",
                                   "reference-gaussian-shift", "muscl", "muscl-shift", "plain", "plain-shift",
-                                  "reference-gaussian-mls6", "wendland-renorm-mls3-shift", "muscl-mls6"])
+                                  "reference-gaussian-mls6", "wendland-renorm-mls3-shift", "muscl-mls6",
+                                  "wendland-renorm-mls1", "muscl-mls1-shift"])
 @pytest.mark.parametrize("pre_steps", [0, 3])
 def test_adjoint_matches_central_differences(lib, kind, pre_steps):
     case = _case(kind)
@@ -182,7 +183,7 @@ def test_adjoint_independent_of_checkpoint_interval(lib):
 
 def test_adjoint_rejects_unsupported_configurations(lib):
     case = S.make_tgv(16, solver=S.SOLVER_MUSCL_DELTA_SPS)
-    case.cfg.mls_order = 1                    # order-1 re-initialisation: not differentiated
+    case.cfg.integrator = S.INTEGRATOR_EULER_PC   # the Taylor-Green solvers: RK4 only
     with S.Simulation(case.cfg, case.n) as sim:
         sim.set_state(case.pos, case.vel, case.rho, case.mass, case.type)
         with pytest.raises(S.SphError) as e:
@@ -219,7 +220,8 @@ def test_adjoint_of_the_mixed_precision_step(lib):
 
 @pytest.mark.parametrize("kind", ["wendland-renorm", "reference-gaussian", "wendland-renorm-shift",
                                   "reference-gaussian-shift", "muscl", "muscl-shift", "plain", "plain-shift",
-                                  "reference-gaussian-mls6", "wendland-renorm-mls3-shift", "muscl-mls6"])
+                                  "reference-gaussian-mls6", "wendland-renorm-mls3-shift", "muscl-mls6",
+                                  "wendland-renorm-mls1", "muscl-mls1-shift"])
 def test_adjoint_matches_cpu_tangent_linear_reference(lib, oracle, kind):
     """g.delta from the GPU adjoint against the FP64 CPU tangent-linear model of
     the same steps (oracle/sph_tangent.cpp, forward-mode derivative with the

@@ -173,7 +173,7 @@ def test_moving_square_adjoint_independent_of_checkpoint_interval(lib):
 
 @pytest.mark.parametrize("solver,shifting,mls_order", [(S.SOLVER_MS_MODLR_DELTA, 1, 0), (S.SOLVER_MS_HLLC_DELTA, 1, 0),
                                                       (S.SOLVER_MS_MODLR_DELTA, 0, 3),
-                                                      (S.SOLVER_MS_HLLC_DELTA, 1, 6)])
+                                                      (S.SOLVER_MS_HLLC_DELTA, 1, 6), (S.SOLVER_MS_MODLR_DELTA, 0, 1)])
 def test_shifting_and_mls_adjoint_matches_central_differences(lib, solver, shifting, mls_order):
     """Particle shifting after every corrector (Shift_particle_position.f90:
     56-136 on the corrector RHS's pairs, ghosts included) and the density
@@ -239,7 +239,7 @@ def test_moving_square_adjoint_rejects_unsupported(lib):
         assert e.value.code == -7
 
 
-@pytest.mark.parametrize("shifting,mls_order", [(0, 0), (1, 0), (0, 3), (1, 6)])
+@pytest.mark.parametrize("shifting,mls_order", [(0, 0), (1, 0), (0, 3), (1, 6), (1, 1)])
 @pytest.mark.parametrize("solver", SOLVERS)
 @pytest.mark.parametrize("loss", [S.LOSS_DRAG, S.LOSS_KINETIC_ENERGY])
 def test_moving_square_adjoint_matches_cpu_tangent_linear_reference(lib, oracle, loss, solver, shifting,
@@ -249,9 +249,10 @@ def test_moving_square_adjoint_matches_cpu_tangent_linear_reference(lib, oracle,
     in the initial velocity, position and density, the viscosity and the body
     motion: both are exact derivatives of the same discrete map (1e-8).  With
     shifting, each step ends with the capped shift of the corrector RHS; with
-    mls_order, every fourth step re-initialises the density first (the
-    moving-square variant: W V weights over every particle in the support, the
-    ghosts with the density and mass the corrector RHS assigned them)."""
+    mls_order, every fourth step re-initialises the density first (orders 3, 6:
+    the moving-square variant, W V weights over every particle in the support,
+    the ghosts with the density and mass the corrector RHS assigned them;
+    order 1: the Shepard density over the corrector RHS's water pairs)."""
     case, ity = S.make_moving_square(dx=0.1, lx=2.0, ly=1.0, D=0.4, solver=solver, jitter=0.05, seed=8)
     water = np.r_[case.type, case.type] == S.TYPE_WATER
     case.vel = case.vel + np.where(water, S.fourier_perturbation(case.pos, n_modes=4, amp=0.2, seed=8), 0.0)

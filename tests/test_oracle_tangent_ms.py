@@ -3,8 +3,7 @@ oracle_tangent_ms), the CPU reference of the moving-square adjoint: its value
 path must reproduce the oracle's Euler predictor-corrector steps with ghost
 assignment and a per-step body motion (final kinetic energy and the drag
 impulse), with and without the particle shift after the corrector and the
-moving-least-squares density re-initialisation (orders 3 and 6, every second
-step), and its directional derivatives must match central differences of
+density re-initialisation (orders 1, 3 and 6, every second step), and its directional derivatives must match central differences of
 its own value path."""
 import numpy as np
 import pytest
@@ -36,7 +35,7 @@ def _tangent(oracle, case, ity, lab, dt, motion, loss, cfg=None, **d):
                              ity, lab, 0.0, NSTEPS, dt, motion, loss, **d)
 
 
-VARIANTS = [(0, 0), (1, 0), (0, 3), (1, 6)]      # (shifting, mls_order)
+VARIANTS = [(0, 0), (1, 0), (0, 3), (1, 6), (1, 1)]      # (shifting, mls_order)
 
 
 @pytest.mark.parametrize("shifting,mls_order", VARIANTS)
@@ -99,7 +98,7 @@ def test_tangent_ms_matches_its_central_differences(oracle, loss, solver, shifti
 
 def test_tangent_ms_rejects_configurations_outside_its_scope(oracle):
     case, ity, lab, dt, motion = _case()
-    for field, value in (("mls_order", 1), ("free_surface", 1)):
+    for field, value in (("laplacian", 0), ("free_surface", 1)):
         cfg = case.cfg.copy()
         setattr(cfg, field, value)
         with pytest.raises(RuntimeError):
