@@ -89,13 +89,18 @@ __device__ __forceinline__ void muscl_limiter_sum(float di, float dj, float dij,
     own = big ? (first == a_is_i ? half : 0.f) : lim;
 }
 
-// Reciprocal and quotient in the pair loop, correctly rounded in both
-// precisions (the fast FP32 forms, __fdividef, made mixed pass C slower:
-// 3.46 -> 3.85 ms per step at 2048^2).
+// Reciprocal and quotient in the pair loop: correctly rounded, except the
+// FP32 1/rho-bar and artificial-viscosity quotient (fast_quot: __fdividef,
+// about 2 ulp).  Fast forms everywhere made mixed pass C slower (3.46 -> 3.85 ms
+// per step at 2048^2: fewer instructions between the neighbour-record loads);
+// these two alone took it from 2.80 to 2.75 ms with the velocity L2 against
+// FP64 unchanged (2.78e-6 after 100 steps).
 __device__ __forceinline__ double rcp(double x) { return 1.0 / x; }
 __device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
 template <typename R>
 __device__ __forceinline__ R quot(R a, R b) { return a / b; }
+__device__ __forceinline__ double fast_quot(double a, double b) { return a / b; }
+__device__ __forceinline__ float fast_quot(float a, float b) { return __fdividef(a, b); }
 
 // Per-particle state a thread needs for one side of a pair.
 template <typename R>
@@ -296,7 +301,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIF
         const R nd1 = bi.z * dw0 + bi.w * dw1;
         const R cbar = R(0.5) * (S.aux.z + T.aux.z);
         const R rbar = R(0.5) * (rho_a_ + rho_b);
-        const R inv_rbar = rcp(rbar);
+        const R inv_rbar = fast_quot(R(1), rbar);
         const R e0 = -xij0 * inv_d, e1 = -xij1 * inv_d;     // x_j - x_i direction (both solvers)
         // Riemann states.  li/lj are the MUSCL reconstruction increments
         // (function_module.f90:34-80); the modified solver has none.
@@ -455,7 +460,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? (SHIFT ? SPH_PASS_C_SHIF
         const R inv_r2 = inv_d * inv_d;
         const R vx = du * xij0 + dv * xij1;
         if (vx < R(0)) {
-            const R phi1 = quot(hbar * vx, d * d + fh2);
+            const R phi1 = fast_quot(hbar * vx, d * d + fh2);
             const R Pi = (-alpha * cbar * phi1 + beta * (phi1 * phi1)) * inv_rbar;
             tx += mb * (-Pi * nd0);
             ty += mb * (-Pi * nd1);
