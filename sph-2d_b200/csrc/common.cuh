@@ -32,6 +32,8 @@ struct Params {
     // kernel / pair search
     double h, r_cut, cut_min, kfactor, gauss_e9, q_zero;
     double r2_list;          // squared neighbour-list radius (support * (1 + skin))
+    float r2_list32;         // the same for the mixed path's FP32 test on the hi positions,
+                             // widened to cover their rounding (a superset of the FP64 list)
     // equation of state
     double rho0, c0sq, sqrt_c0, eos_b, pb;
     int eos;

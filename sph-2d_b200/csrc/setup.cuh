@@ -292,8 +292,13 @@ __global__ void __launch_bounds__(128) k_build_lists(Params P, Sorted<R> D, unsi
         else if (cnt < P.max_nbr) D.nbr[(size_t)cnt * P.nbr_stride + a] = v;
         ++cnt;
     };
+    // the mixed path tests the FP32 hi positions against the widened radius
+    // r2_list32 (a superset of the FP64 list, see derive_params)
+    constexpr bool F32 = sizeof(R) == 4;
+    const float2* xh = reinterpret_cast<const float2*>(D.xhl);     // (x hi, y hi) at 2 s
     if (ta != SPH_TYPE_ILL && ta != 0) {
         double2 xa = D.pos[a];
+        const float2 xa_h = F32 ? xh[2 * (size_t)a] : make_float2(0.f, 0.f);
         int ida = D.id[a];
         int cx = (int)floor((xa.x - P.gx0) / P.cs), cy = (int)floor((xa.y - P.gy0) / P.cs);
         int x0 = max(cx - 1, 0), x1 = min(cx + 1, P.gnx - 1);
@@ -315,10 +320,12 @@ __global__ void __launch_bounds__(128) k_build_lists(Params P, Sorted<R> D, unsi
             int b = b0;
             for (; b + 4 <= b1; b += 4) {
                 double2 xb[4];
+                float2 xbh[4];
                 int tb[4], ib[4];
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
-                    xb[k] = __ldg(&D.pos[b + k]);
+                    if (F32) xbh[k] = __ldg(&xh[2 * (size_t)(b + k)]);
+                    else xb[k] = __ldg(&D.pos[b + k]);
                     ib[k] = __ldg(&D.id[b + k]);
                     tb[k] = check_type ? __ldg(&D.type[b + k]) : 0;
                 }
@@ -326,17 +333,28 @@ __global__ void __launch_bounds__(128) k_build_lists(Params P, Sorted<R> D, unsi
                 for (int k = 0; k < 4; ++k) {
                     if (b + k == a) continue;
                     if (check_type && !pair_allowed(P.pair_rule, ta, tb[k])) continue;
-                    const double dx = xa.x - xb[k].x, dy = xa.y - xb[k].y;
-                    if (dx * dx + dy * dy > P.r2_list) continue;
+                    if (F32) {
+                        const float dx = xa_h.x - xbh[k].x, dy = xa_h.y - xbh[k].y;
+                        if (dx * dx + dy * dy > P.r2_list32) continue;
+                    } else {
+                        const double dx = xa.x - xb[k].x, dy = xa.y - xb[k].y;
+                        if (dx * dx + dy * dy > P.r2_list) continue;
+                    }
                     put(b + k, ida < ib[k] ? 0x80000000u : 0u);
                 }
             }
             for (; b < b1; ++b) {
                 if (b == a) continue;
                 if (check_type && !pair_allowed(P.pair_rule, ta, D.type[b])) continue;
-                const double2 xb = D.pos[b];
-                const double dx = xa.x - xb.x, dy = xa.y - xb.y;
-                if (dx * dx + dy * dy > P.r2_list) continue;
+                if (F32) {
+                    const float2 xbh = xh[2 * (size_t)b];
+                    const float dx = xa_h.x - xbh.x, dy = xa_h.y - xbh.y;
+                    if (dx * dx + dy * dy > P.r2_list32) continue;
+                } else {
+                    const double2 xb = D.pos[b];
+                    const double dx = xa.x - xb.x, dy = xa.y - xb.y;
+                    if (dx * dx + dy * dy > P.r2_list) continue;
+                }
                 put(b, ida < D.id[b] ? 0x80000000u : 0u);
             }
         }

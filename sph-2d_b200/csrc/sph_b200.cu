@@ -221,6 +221,19 @@ int derive_params(const sph_config& c, Params& P) {
     P.gy0 = c.grid_lo[1] - rl;
     P.gnx = (int)ceil((c.grid_hi[0] - c.grid_lo[0]) / rl) + 3;
     P.gny = (int)ceil((c.grid_hi[1] - c.grid_lo[1]) / rl) + 3;
+    // The mixed list build tests |x_a - x_b| on the FP32 hi positions: each is
+    // within 2^-24 |x| of the FP64 one and the FP32 difference within 2^-24 of
+    // its magnitude, so each computed component is within 2^-22 X of the FP64
+    // one (X = the largest coordinate on the grid) and the distance within
+    // 2^-21 X; the radius widened by that and the square by (1 + 2^-19) keeps
+    // every FP64 list member (the extra candidates fail the exact support tests
+    // of the passes that read the list).
+    {
+        const double X = fmax(fmax(fabs(P.gx0), fabs(P.gx0 + P.gnx * P.cs)),
+                              fmax(fabs(P.gy0), fabs(P.gy0 + P.gny * P.cs)));
+        const double r32 = rl + X * 0x1p-21;
+        P.r2_list32 = (float)(r32 * r32 * (1.0 + 0x1p-19));
+    }
     if (!(c.grid_hi[0] > c.grid_lo[0]) || !(c.grid_hi[1] > c.grid_lo[1])) return SPH_E_CONFIG;
     if ((long long)P.gnx * P.gny > (1LL << 30)) return SPH_E_CONFIG;
     // neighbour-list capacity: twice the lattice count inside the list radius
