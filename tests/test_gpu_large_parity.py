@@ -51,6 +51,15 @@ def test_pair_set_bit_exact_benchmark_size(lib, oracle, n_side, seed):
     assert np.array_equal(kg, kr)
     # about ten pairs per particle at h = 1.3 dx, support 2h
     assert 9.5 * case.n < kr.size < 10.5 * case.n
+    if seed == 1:
+        # the mixed path builds its neighbour lists from the FP32 hi positions
+        # against a widened radius; the exact support test then gives the same set
+        cfg = case.cfg.copy()
+        cfg.precision = S.PREC_MIXED
+        with S.Simulation(cfg, case.n) as sim:
+            sim.set_state(case.pos, case.vel, case.rho, case.mass, case.type)
+            got = sim.find_particle_pair(cap, want_kernel=False)
+        assert np.array_equal(sorted_keys(got["pair_i"], got["pair_j"]), kr)
 
 
 def test_rhs_fp64_parity_benchmark_size(lib, oracle):
